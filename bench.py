@@ -1,0 +1,335 @@
+"""Benchmark of the LorenzoQuant(3-D, REL 1e-3, radius 32768, zigzag) ->
+Bitshuffle(16 KiB, element width 2) -> RZE(16 KiB, 4 levels) chain on a
+512^3 FP32 field (seeded Gaussian random field, P(k) ~ k^-3, mean 0, std 1,
+0.1% of cells set to +-1e3).
+
+One step = one compression and one decompression of the field, inputs
+resident in HBM.  `value` is the compression throughput (uncompressed bytes /
+device time); the decompression throughput, both roofline fractions, the
+end-to-end (host buffers, copies inside the timed region) figures, the CPU
+baseline and clock samples sit beside it in the same JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank compresses its own field (no data exchange: the
+path shards by field); timings are maxed over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+DIMS = (512, 512, 512)
+EB, RADIUS, ZIGZAG, OUTLIER_CAP = 1e-3, 32768, True, 0.1
+SEED = 1002
+METRIC = "comp/decomp GB/s and % HBM roofline at fixed eb"
+WORKLOAD = ("LorenzoQuant3D(REL 1e-3, r 32768, zigzag)->Bitshuffle(16384,ew2)->RZE(16384,4) "
+            "on 512^3 f32 GRF k^-3 + 0.1% +-1e3 spikes")
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 6:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
+        mx = max((float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- CPU side
+
+def cpu_baseline(steps: int = 1):
+    """The oracle (OpenMP C restatement of the reference stage math) on a
+    bounded sample of the workload: a 512x512x64 slab of the same field."""
+    import numpy as np
+    import torch
+
+    from fzgpumodules_b200 import fields
+    from oracle import oracle as O
+    x = fields.grf((64, 512, 512), seed=SEED, spike_frac=1e-3).reshape(-1).numpy()
+    dims = (512, 512, 64)
+    cap = int(np.ceil(x.size * OUTLIER_CAP))
+    O.lib()
+    tc, td = [], []
+    size = 0
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        vb = O.value_base(x, O.REL)
+        abs_eb, r, e2 = O.resolve_eb(EB, O.REL, vb)
+        codes, err, idx, cnt = O.lq_fwd(x, dims, r, RADIUS, ZIGZAG, cap=cap)
+        stream = O.rze_encode(O.bitshuffle(codes, 16384, 2))
+        t1 = time.perf_counter()
+        c2 = O.bitshuffle(O.rze_decode(stream), 16384, 2, inverse=True).view(np.uint16)
+        y = O.lq_inv(c2, err, idx, dims, e2, ZIGZAG)
+        t2 = time.perf_counter()
+        tc.append(t1 - t0)
+        td.append(t2 - t1)
+        size = stream.size + 8 * len(idx) + 4
+    nbytes = x.size * 4
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"compress_gbs": nbytes / np.median(tc) / 1e9, "decompress_gbs": nbytes / np.median(td) / 1e9,
+            "cores": cores, "sample": "512x512x64 slab of the 512^3 field (64 MiB), oracle chain",
+            "ratio": nbytes / size}
+
+
+def run_reference(args, world, rank):
+    """The reference arm: the reference's stage math on the host cores (the
+    reference ships no CPU implementation of this path, so the oracle port)."""
+    if rank != 0:
+        return
+    res = [cpu_baseline(1) for _ in range(args.warmup + args.steps)][args.warmup:]
+    import numpy as np
+    comp = float(np.median([r["compress_gbs"] for r in res]))
+    dec = float(np.median([r["decompress_gbs"] for r in res]))
+    line = {"metric": METRIC, "value": comp, "unit": "GB/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD + " (CPU sample 512x512x64)"},
+            "decompress": {"value": dec, "unit": "GB/s"},
+            "cpu_baseline": {"value": comp, "unit": "GB/s", "cores": res[0]["cores"], "kind": "port",
+                             "sample": res[0]["sample"]},
+            "e2e": {"value": comp, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU side
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from fzgpumodules_b200 import fields, kernels
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    nz, ny, nx = DIMS[2], DIMS[1], DIMS[0]
+    x = fields.grf((nz, ny, nx), seed=SEED + rank, spike_frac=1e-3, device=dev).reshape(-1)
+    n = x.numel()
+    nbytes = 4 * n
+    ws = kernels.Workspace()
+    out = kernels.lq_bs_rze_compress(x, DIMS, EB, kernels.REL, RADIUS, ZIGZAG, OUTLIER_CAP, ws=ws)
+    torch.cuda.synchronize()
+    size = int(out["rze_size"].item())
+    abs_eb = float(out["eb_state"][1].item())
+    y = kernels.lq_bs_rze_decompress(out["rze"], size, out["err"], out["idx"], out["count"],
+                                     out["cap"], n, DIMS, abs_eb, ZIGZAG, ws=ws)
+    torch.cuda.synchronize()
+    maxerr = float((y - x).abs().max().item())
+    n_out = int(out["count"].item())
+    comp_bytes = size + 8 * min(n_out, out["cap"]) + 4  # RZE stream + outlier segments + count
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    s = torch.cuda.current_stream()
+
+    def one(kind):
+        flush.zero_()  # evict L2 between timed iterations (outside the events)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        if kind == "c":
+            kernels.lq_bs_rze_compress(x, DIMS, EB, kernels.REL, RADIUS, ZIGZAG, OUTLIER_CAP, ws=ws, out=out)
+        else:
+            kernels.lq_bs_rze_decompress(out["rze"], size, out["err"], out["idx"], out["count"],
+                                         out["cap"], n, DIMS, abs_eb, ZIGZAG,
+                                         flags=kernels.NO_SYNC, ws=ws, out=y)
+        e1.record(s)
+        return e0, e1
+
+    for _ in range(args.warmup):
+        one("c"), one("d")
+    barrier(world)
+    ev_c, ev_d = [], []
+    with ClockSampler(local) as clk:
+        t_wall = time.perf_counter()
+        for _ in range(args.steps):
+            ev_c.append(one("c"))
+            ev_d.append(one("d"))
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    barrier(world)
+    st = ws.status()
+    tc = [a.elapsed_time(b) / 1e3 for a, b in ev_c]
+    td = [a.elapsed_time(b) / 1e3 for a, b in ev_d]
+    t_c = max_over_ranks(float(np.mean(tc)), world)
+    t_d = max_over_ranks(float(np.mean(td)), world)
+
+    # end to end through the C ABI with host buffers: H2D of the field, compress,
+    # D2H of the compressed segments; H2D of the segments, decompress, D2H of the field
+    hx = x.cpu().pin_memory()
+    hy = torch.empty_like(hx).pin_memory()
+    hs = torch.empty(size, dtype=torch.uint8).pin_memory()
+    dx = torch.empty_like(x)
+    e2e_c, e2e_d = [], []
+    for it in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dx.copy_(hx, non_blocking=True)
+        o2 = kernels.lq_bs_rze_compress(dx, DIMS, EB, kernels.REL, RADIUS, ZIGZAG, OUTLIER_CAP, ws=ws, out=out)
+        sz = int(o2["rze_size"].item())  # D2H of the stream size
+        hs[:sz].copy_(o2["rze"][:sz], non_blocking=True)
+        herr = o2["err"][: n_out].to("cpu", non_blocking=True)
+        hidx = o2["idx"][: n_out].to("cpu", non_blocking=True)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        drze = hs[:sz].to(dev, non_blocking=True)
+        derr = herr.to(dev, non_blocking=True)
+        didx = hidx.to(dev, non_blocking=True)
+        kernels.lq_bs_rze_decompress(drze, sz, derr if n_out else out["err"], didx if n_out else out["idx"],
+                                     out["count"], out["cap"], n, DIMS, abs_eb, ZIGZAG,
+                                     flags=kernels.NO_SYNC, ws=ws, out=y)
+        hy.copy_(y, non_blocking=True)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if it >= args.warmup:
+            e2e_c.append(t1 - t0)
+            e2e_d.append(t2 - t1)
+    e2e_t = max_over_ranks(float(np.mean(e2e_c)), world)
+    e2e_td = max_over_ranks(float(np.mean(e2e_d)), world)
+
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    algo_c = nbytes + comp_bytes   # read f32 field + write compressed segments
+    algo_d = comp_bytes + nbytes   # read compressed segments + write f32 field
+    ach_c = algo_c / t_c / 1e9
+    ach_d = algo_d / t_d / 1e9
+    cpu = cpu_baseline(1) if (world == 1 and not args.no_cpu) else None
+    line = {
+        "metric": METRIC, "value": world * nbytes / t_c / 1e9, "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": (t_c + t_d) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "dims": list(DIMS), "eb": EB, "eb_mode": "REL",
+                   "radius": RADIUS, "zigzag": ZIGZAG, "outlier_capacity": OUTLIER_CAP,
+                   "l2": "input 512 MiB > L2, plus a 256 MiB L2 flush before every timed call",
+                   "parallelism": f"replicas x{world}"},
+        "compress": {"gbs": nbytes / t_c / 1e9, "ms": t_c * 1e3, "ratio": nbytes / comp_bytes,
+                     "compressed_bytes": comp_bytes, "outliers": n_out},
+        "decompress": {"value": world * nbytes / t_d / 1e9, "unit": "GB/s", "ms": t_d * 1e3,
+                       "max_abs_err": maxerr, "abs_eb": abs_eb,
+                       "roofline": {"bound": "hbm", "achieved": ach_d, "peak": peak, "unit": "GB/s",
+                                    "frac": ach_d / peak, "traffic": None, "peak_kind": peak_kind}},
+        "roofline": {"bound": "hbm", "achieved": ach_c, "peak": peak, "unit": "GB/s",
+                     "frac": ach_c / peak, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "lq_chunk_kernel<3,fused> (+ value-base scan)"},
+        "e2e": {"value": world * nbytes / e2e_t / 1e9, "unit": "GB/s",
+                "h2d_bytes_per_step": nbytes + comp_bytes, "d2h_bytes_per_step": comp_bytes + nbytes + 8,
+                "compress_gbs": nbytes / e2e_t / 1e9, "decompress_gbs": nbytes / e2e_td / 1e9},
+        "gpu_launches": args.steps * (3 + 3),
+        "clocks": clk.summary(),
+        "status": st,
+        "wall_s_timed": t_wall,
+    }
+    if cpu:
+        line["cpu_baseline"] = {"value": cpu["compress_gbs"], "unit": "GB/s", "cores": cpu["cores"],
+                                "kind": "port", "sample": cpu["sample"],
+                                "decompress_gbs": cpu["decompress_gbs"]}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world, rank, local = dist_setup() if args.impl == "ours" else (
+        int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,71 @@
+"""Loader for libfzb.so, the sm_100a kernels behind the C ABI in include/fzb.h.
+
+The library is built in-tree (``python -m fzgpumodules_b200.build`` or
+``__graft_entry__.build()``).  There is no CPU fallback: a missing library is
+an ImportError-level failure, not a silent downgrade.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libfzb.so")
+HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "fzb.h")
+
+_lib = None
+
+
+class FzbError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        msg = lib().fzb_status_string(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{what}: {msg} (status {status})" if what else msg)
+
+
+def header_symbols() -> list[str]:
+    """Names of the functions include/fzb.h declares."""
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(fzb_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing; build it with __graft_entry__.build()")
+        L = C.CDLL(LIB_PATH)
+        p, u64, sz, i32, u32, f32 = C.c_void_p, C.c_uint64, C.c_size_t, C.c_int, C.c_uint32, C.c_float
+        L.fzb_version.restype = i32
+        L.fzb_status_string.restype = C.c_char_p
+        L.fzb_status_string.argtypes = [i32]
+        L.fzb_workspace_bytes.restype = sz
+        L.fzb_workspace_bytes.argtypes = [u64]
+        L.fzb_workspace_status.restype = i32
+        L.fzb_workspace_status.argtypes = [p, p]
+        L.fzb_lq_forward.restype = i32
+        L.fzb_lq_forward.argtypes = [p, u64, p, f32, i32, f32, u32, i32, p, p, p, u64, p, p, p, sz, p]
+        L.fzb_lq_inverse.restype = i32
+        L.fzb_lq_inverse.argtypes = [p, p, p, p, u64, u64, p, f32, i32, p, p, sz, p]
+        L.fzb_bitshuffle.restype = i32
+        L.fzb_bitshuffle.argtypes = [p, u64, u32, i32, i32, p, p]
+        L.fzb_rze_max_bytes.restype = u64
+        L.fzb_rze_max_bytes.argtypes = [u64]
+        L.fzb_rze_encode.restype = i32
+        L.fzb_rze_encode.argtypes = [p, u64, p, p, p, sz, p]
+        L.fzb_rze_decode.restype = i32
+        L.fzb_rze_decode.argtypes = [p, u64, u64, p, p, sz, p]
+        L.fzb_lq_bs_rze_compress.restype = i32
+        L.fzb_lq_bs_rze_compress.argtypes = [p, u64, p, f32, i32, f32, u32, i32, p, p, u64, p, p, p, p, p, sz, p]
+        L.fzb_lq_bs_rze_decompress.restype = i32
+        L.fzb_lq_bs_rze_decompress.argtypes = [p, u64, p, p, p, u64, u64, p, f32, i32, p, C.c_uint, p, sz, p]
+        _lib = L
+    return _lib
+
+
+def check(status: int, what: str = "") -> None:
+    if status != 0:
+        raise FzbError(status, what)

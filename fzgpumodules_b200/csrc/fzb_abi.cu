@@ -1,0 +1,449 @@
+// fzb_abi.cu -- the extern "C" boundary (include/fzb.h).  Host-side
+// argument checking, workspace carving and kernel launches; no allocation.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+
+#include "../../include/fzb.h"
+#include "fzb_kernels.cuh"
+
+using namespace fzb;
+
+namespace {
+
+constexpr int kVersion = 100;
+constexpr size_t kCtrlBytes = 256;   // err, ticket, scalars
+constexpr int kMaxParts = 1024;      // min/max partials
+
+struct Work {
+    uint32_t* err;
+    uint32_t* ticket;
+    float* inv_scalars;
+    float* pmin;
+    float* pmax;
+    unsigned long long* st_outl;
+    unsigned long long* st_bytes;
+    unsigned long long* in_off;
+    uint32_t* ostart;
+    uint16_t* codes;   // 2 * n_total bytes: codes staging for the exact inverse
+    size_t need;
+};
+
+inline size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+inline uint64_t chunks_of(uint64_t n_total) { return (n_total + kChunkCodes - 1) / kChunkCodes; }
+
+Work carve(void* base, uint64_t n_total) {
+    Work w{};
+    const uint64_t nch = chunks_of(n_total) + 1;
+    uint8_t* p = static_cast<uint8_t*>(base);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        uint8_t* q = p ? p + off : nullptr;
+        off += align256(bytes);
+        return q;
+    };
+    uint8_t* ctrl = take(kCtrlBytes);
+    w.err = reinterpret_cast<uint32_t*>(ctrl);
+    w.ticket = reinterpret_cast<uint32_t*>(ctrl ? ctrl + 4 : nullptr);
+    w.inv_scalars = reinterpret_cast<float*>(ctrl ? ctrl + 64 : nullptr);
+    w.pmin = reinterpret_cast<float*>(take(sizeof(float) * kMaxParts));
+    w.pmax = reinterpret_cast<float*>(take(sizeof(float) * kMaxParts));
+    w.st_outl = reinterpret_cast<unsigned long long*>(take(8 * nch));
+    w.st_bytes = reinterpret_cast<unsigned long long*>(take(8 * nch));
+    w.in_off = reinterpret_cast<unsigned long long*>(take(8 * (nch + 1)));
+    w.ostart = reinterpret_cast<uint32_t*>(take(4 * (nch + 1)));
+    w.codes = reinterpret_cast<uint16_t*>(take(2 * (n_total + kChunkCodes)));
+    w.need = off;
+    return w;
+}
+
+inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
+
+#define CK(call)                                          \
+    do {                                                  \
+        if ((call) != cudaSuccess) return FZB_E_CUDA;     \
+    } while (0)
+
+struct Geometry {
+    uint32_t nx, ny, nz, ndim, nfield;
+};
+
+int geometry(uint64_t n_total, const uint32_t dims[3], Geometry* g) {
+    if (n_total == 0 || n_total >= (1ull << 31) || dims == nullptr) return FZB_E_INVALID;
+    uint32_t ny = dims[1] ? dims[1] : 1, nz = dims[2] ? dims[2] : 1;
+    uint64_t nx = dims[0];
+    if (nx == 0) nx = n_total / ((uint64_t)ny * nz);  // LorenzoQuantStage infers x
+    const uint64_t nf = nx * ny * nz;
+    if (nx == 0 || nf == 0 || nf > n_total) return FZB_E_INVALID;
+    g->nx = (uint32_t)nx;
+    g->ny = ny;
+    g->nz = nz;
+    g->nfield = (uint32_t)nf;
+    g->ndim = nz > 1 ? 3 : (ny > 1 ? 2 : 1);  // LorenzoQuantStage::ndim()
+    return FZB_OK;
+}
+
+// Dynamic shared memory of the chunk kernel: the staged windows, at least
+// the RZE working set when fused.
+size_t lq_smem_bytes(const Geometry& g, bool fused) {
+    auto gran = [](uint64_t len) { return (((len + 3) / 4 + 1) + 7) & ~(uint64_t)7; };
+    uint64_t per_plane;
+    if (g.ndim == 1) per_plane = gran(kChunkCodes + 1);
+    else if (g.nx <= kChunkCodes) per_plane = gran((uint64_t)g.nx + 1 + kChunkCodes);
+    else per_plane = 2 * gran(kChunkCodes + 1);
+    const uint64_t planes = (g.ndim == 3) ? 2 : 1;
+    size_t bytes = (size_t)(per_plane * planes * 16);
+    const size_t rze_set = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
+    if (fused && bytes < rze_set) bytes = rze_set;
+    return bytes;
+}
+
+int launch_lq(const Geometry& g, bool fused, const FwdArgs& a, size_t smem, uint32_t grid,
+              cudaStream_t s) {
+    const bool rowal = (g.ndim == 1) || (g.nx % 32 == 0);
+    return launch_lq_chunk((int)g.ndim, fused, rowal, a, smem, grid, s) == 0 ? FZB_OK : FZB_E_CUDA;
+}
+
+// Resolves abs_eb / ebx2_r on the device into eb_state (no host sync).
+int resolve_eb(const float* d_in, uint64_t n_total, float eb, int mode, float value_base,
+               const Work& w, float* d_eb_state, cudaStream_t s) {
+    if (mode != FZB_ABS && !(value_base > 0.0f)) {
+        uint64_t blocks = (n_total + 1023) / 1024;
+        int parts = (int)(blocks < (uint64_t)kMaxParts ? blocks : kMaxParts);
+        if (parts < 1) parts = 1;
+        minmax_kernel<<<parts, 256, 0, s>>>(d_in, n_total, w.pmin, w.pmax);
+        CK(cudaGetLastError());
+        resolve_eb_kernel<<<1, 32, 0, s>>>(w.pmin, w.pmax, parts, mode, eb, 0.0f, d_eb_state);
+    } else {
+        resolve_eb_kernel<<<1, 32, 0, s>>>(nullptr, nullptr, 0, mode, eb, value_base, d_eb_state);
+    }
+    CK(cudaGetLastError());
+    return FZB_OK;
+}
+
+int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32_t dims[3],
+                   float eb, int eb_mode, float value_base, uint32_t radius, int zigzag,
+                   uint16_t* d_codes, float* d_err, uint32_t* d_idx, uint64_t cap,
+                   uint32_t* d_count, void* d_rze, uint64_t* d_rze_size, float* d_eb_state,
+                   void* d_work, size_t work_bytes, void* stream) {
+    Geometry g;
+    int rc = geometry(n_total, dims, &g);
+    if (rc) return rc;
+    if (!d_in || !d_count || !d_eb_state || (cap && (!d_err || !d_idx))) return FZB_E_INVALID;
+    if (fused ? (!d_rze || !d_rze_size) : !d_codes) return FZB_E_INVALID;
+    if (eb_mode < FZB_ABS || eb_mode > FZB_NOA || !(eb > 0.0f)) return FZB_E_INVALID;
+    Work w = carve(d_work, n_total);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    const uint64_t nch = chunks_of(n_total);
+    CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
+    CK(cudaMemsetAsync(w.st_outl, 0, 8 * nch, s));
+    if (fused) CK(cudaMemsetAsync(w.st_bytes, 0, 8 * nch, s));
+    rc = resolve_eb(d_in, n_total, eb, eb_mode, value_base, w, d_eb_state, s);
+    if (rc) return rc;
+    FwdArgs a{};
+    a.in = d_in;
+    a.n_total = (uint32_t)n_total;
+    a.nfield = g.nfield;
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.nz = g.nz;
+    a.plane = g.nx * g.ny;
+    a.ebx2_r = d_eb_state + 2;
+    a.radius = (float)(uint16_t)radius;  // the kernel compares against TCode(radius)
+    a.zigzag = zigzag;
+    a.two_piece = (g.ndim >= 2 && g.nx > (uint32_t)kChunkCodes) ? 1 : 0;
+    a.codes = d_codes;
+    a.out_err = d_err;
+    a.out_idx = d_idx;
+    a.cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
+    a.out_count = d_count;
+    a.rze = static_cast<uint8_t*>(d_rze);
+    a.n_chunks = (uint32_t)nch;
+    a.codes_bytes = (uint32_t)(2 * n_total);
+    a.rze_size = reinterpret_cast<unsigned long long*>(d_rze_size);
+    a.st_outl = w.st_outl;
+    a.st_bytes = w.st_bytes;
+    a.ticket = w.ticket;
+    a.err = w.err;
+    return launch_lq(g, fused, a, lq_smem_bytes(g, fused), (uint32_t)nch, s);
+}
+
+InvArgs inv_args(const Work& w, const Geometry& g, uint64_t n_total) {
+    InvArgs a{};
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.nz = g.nz;
+    a.plane = g.nx * g.ny;
+    a.nfield = g.nfield;
+    a.n_total = (uint32_t)n_total;
+    a.err = w.err;
+    a.in_off = w.in_off;
+    a.ostart = w.ostart;
+    return a;
+}
+
+// memset(out) + scatter + tile kernels (the exact path).
+int exact_inverse(const InvArgs& a, const Geometry& g, cudaStream_t s) {
+    CK(cudaMemsetAsync(a.out, 0, sizeof(float) * (size_t)a.n_total, s));
+    if (a.cap) {
+        uint32_t blocks = (uint32_t)((a.cap + 255) / 256);
+        if (blocks > 4096) blocks = 4096;
+        scatter_outliers_kernel<<<blocks, 256, 0, s>>>(a);
+        CK(cudaGetLastError());
+    }
+    if (g.ndim == 1) {
+        lq_inverse_1d_kernel<<<(g.nfield + 1023) / 1024, 256, 0, s>>>(a);
+    } else if (g.ndim == 2) {
+        dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32, 1);
+        lq_inverse_2d_kernel<<<grid, 128, 0, s>>>(a);
+    } else {
+        dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + 7) / 8);
+        lq_inverse_3d_kernel<<<grid, 256, 0, s>>>(a);
+    }
+    CK(cudaGetLastError());
+    return FZB_OK;
+}
+
+int read_status(const Work& w, cudaStream_t s, uint32_t* bits) {
+    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpy(bits, w.err, 4, cudaMemcpyDeviceToHost));
+    return FZB_OK;
+}
+
+int status_of(uint32_t bits) {
+    if (bits & kErrMalformed) return FZB_E_MALFORMED;
+    if (bits & kErrLookbackTimeout) return FZB_E_TIMEOUT;
+    return FZB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fzb_version(void) { return kVersion; }
+
+const char* fzb_status_string(int st) {
+    switch (st) {
+        case FZB_OK: return "ok";
+        case FZB_E_INVALID: return "invalid argument or unsupported configuration";
+        case FZB_E_CUDA: return "CUDA runtime error";
+        case FZB_E_WORKSPACE: return "workspace too small";
+        case FZB_E_CAPACITY: return "output buffer too small";
+        case FZB_E_MALFORMED: return "malformed compressed input";
+        case FZB_E_TIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+size_t fzb_workspace_bytes(uint64_t n_total) { return carve(nullptr, n_total).need; }
+
+int fzb_workspace_status(void* d_work, void* stream) {
+    if (!d_work) return FZB_E_INVALID;
+    uint32_t* err = static_cast<uint32_t*>(d_work);
+    uint32_t bits = 0;
+    CK(cudaStreamSynchronize(S(stream)));
+    CK(cudaMemcpy(&bits, err, 4, cudaMemcpyDeviceToHost));
+    CK(cudaMemset(err, 0, 4));
+    return status_of(bits);
+}
+
+int fzb_lq_forward(const float* d_in, uint64_t n_total, const uint32_t dims[3], float eb,
+                   int eb_mode, float value_base, uint32_t radius, int zigzag, uint16_t* d_codes,
+                   float* d_err, uint32_t* d_idx, uint64_t cap, uint32_t* d_count,
+                   float* d_eb_state, void* d_work, size_t work_bytes, void* stream) {
+    return forward_common(false, d_in, n_total, dims, eb, eb_mode, value_base, radius, zigzag,
+                          d_codes, d_err, d_idx, cap, d_count, nullptr, nullptr, d_eb_state,
+                          d_work, work_bytes, stream);
+}
+
+int fzb_lq_bs_rze_compress(const float* d_in, uint64_t n_total, const uint32_t dims[3], float eb,
+                           int eb_mode, float value_base, uint32_t radius, int zigzag,
+                           float* d_err, uint32_t* d_idx, uint64_t cap, uint32_t* d_count,
+                           void* d_rze, uint64_t* d_rze_size, float* d_eb_state, void* d_work,
+                           size_t work_bytes, void* stream) {
+    return forward_common(true, d_in, n_total, dims, eb, eb_mode, value_base, radius, zigzag,
+                          nullptr, d_err, d_idx, cap, d_count, d_rze, d_rze_size, d_eb_state,
+                          d_work, work_bytes, stream);
+}
+
+int fzb_lq_inverse(const uint16_t* d_codes, const float* d_err, const uint32_t* d_idx,
+                   const uint32_t* d_count, uint64_t cap, uint64_t n_total, const uint32_t dims[3],
+                   float abs_eb, int zigzag, float* d_out, void* d_work, size_t work_bytes,
+                   void* stream) {
+    Geometry g;
+    int rc = geometry(n_total, dims, &g);
+    if (rc) return rc;
+    if (!d_codes || !d_out || !d_count || (cap && (!d_err || !d_idx))) return FZB_E_INVALID;
+    Work w = carve(d_work, n_total);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
+    InvArgs a = inv_args(w, g, n_total);
+    a.codes = const_cast<uint16_t*>(d_codes);
+    a.out_err = d_err;
+    a.out_idx = d_idx;
+    a.out_count = d_count;
+    a.cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
+    a.ebx2 = 2.0f * abs_eb;
+    a.zigzag = zigzag;
+    a.out = d_out;
+    return exact_inverse(a, g, s);
+}
+
+int fzb_bitshuffle(const void* d_in, uint64_t bytes, uint32_t block, int ew, int inverse,
+                   void* d_out, void* stream) {
+    if (!d_in || !d_out || (ew != 1 && ew != 2)) return FZB_E_INVALID;
+    if (block == 0 || block % (1024u * (uint32_t)ew) != 0) return FZB_E_INVALID;
+    cudaStream_t s = S(stream);
+    const uint64_t nfull = bytes / block;
+    const uint8_t* in = static_cast<const uint8_t*>(d_in);
+    uint8_t* out = static_cast<uint8_t*>(d_out);
+    if (nfull) {
+        if (ew == 2 && block == (uint32_t)kChunkBytes &&
+            ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0) {
+            bitshuffle2_kernel<<<(unsigned)nfull, kThreads, 0, s>>>(in, out, inverse);
+        } else {
+            const uint32_t nchunk = block / (uint32_t)ew;
+            bitshuffle_ballot_kernel<<<(unsigned)nfull, nchunk < 1024 ? nchunk : 1024, 0, s>>>(
+                in, out, block, ew, inverse);
+        }
+        CK(cudaGetLastError());
+    }
+    const uint64_t tail = bytes - nfull * block;
+    if (tail) CK(cudaMemcpyAsync(out + nfull * block, in + nfull * block, tail,
+                                 cudaMemcpyDeviceToDevice, s));
+    return FZB_OK;
+}
+
+uint64_t fzb_rze_max_bytes(uint64_t bytes) {
+    const uint64_t nch = (bytes + kChunkBytes - 1) / kChunkBytes;
+    return 8 + 4 * nch + nch * (uint64_t)kChunkBytes + 4;
+}
+
+int fzb_rze_encode(const void* d_in, uint64_t bytes, void* d_out, uint64_t* d_out_size,
+                   void* d_work, size_t work_bytes, void* stream) {
+    if (!d_in || !d_out || !d_out_size || bytes == 0 || bytes >= (1ull << 32)) return FZB_E_INVALID;
+    const uint64_t n_equiv = (bytes + 1) / 2;
+    Work w = carve(d_work, n_equiv);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    const uint64_t nch = (bytes + kChunkBytes - 1) / kChunkBytes;
+    CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
+    CK(cudaMemsetAsync(w.st_bytes, 0, 8 * nch, s));
+    RzeEncArgs a{};
+    a.in = static_cast<const uint8_t*>(d_in);
+    a.bytes = bytes;
+    a.out = static_cast<uint8_t*>(d_out);
+    a.n_chunks = (uint32_t)nch;
+    a.out_size = reinterpret_cast<unsigned long long*>(d_out_size);
+    a.st_bytes = w.st_bytes;
+    a.ticket = w.ticket;
+    a.err = w.err;
+    const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
+    CK(cudaFuncSetAttribute(rze_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    rze_encode_kernel<<<(unsigned)nch, kThreads, smem, s>>>(a);
+    CK(cudaGetLastError());
+    return FZB_OK;
+}
+
+int fzb_rze_decode(const void* d_in, uint64_t in_bytes, uint64_t orig_bytes, void* d_out,
+                   void* d_work, size_t work_bytes, void* stream) {
+    if (!d_in || !d_out || orig_bytes == 0 || orig_bytes >= (1ull << 32)) return FZB_E_INVALID;
+    const uint64_t nch = (orig_bytes + kChunkBytes - 1) / kChunkBytes;
+    if (in_bytes < 8 + 4 * nch) return FZB_E_MALFORMED;
+    const uint64_t n_equiv = (orig_bytes + 1) / 2;
+    Work w = carve(d_work, n_equiv);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
+    rze_prepass_kernel<<<1, 1024, 0, s>>>(static_cast<const uint8_t*>(d_in), in_bytes, (uint32_t)nch,
+                                          (uint32_t)orig_bytes, w.in_off, w.err);
+    CK(cudaGetLastError());
+    InvArgs a{};
+    a.rze = static_cast<const uint8_t*>(d_in);
+    a.rze_bytes = in_bytes;
+    a.in_off = w.in_off;
+    a.n_chunks = (uint32_t)nch;
+    a.orig_bytes = (uint32_t)orig_bytes;
+    a.bytes_out = static_cast<uint8_t*>(d_out);
+    a.err = w.err;
+    const int smem = kChunkBytes * 2 + 16 + 2048 + 256 + 32;
+    CK(cudaFuncSetAttribute(rze_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    rze_decode_kernel<<<(unsigned)nch, kThreads, smem, s>>>(a);
+    CK(cudaGetLastError());
+    return FZB_OK;
+}
+
+int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float* d_err,
+                             const uint32_t* d_idx, const uint32_t* d_count, uint64_t cap,
+                             uint64_t n_total, const uint32_t dims[3], float abs_eb, int zigzag,
+                             float* d_out, unsigned flags, void* d_work, size_t work_bytes,
+                             void* stream) {
+    Geometry g;
+    int rc = geometry(n_total, dims, &g);
+    if (rc) return rc;
+    if (!d_rze || !d_out || !d_count || (cap && (!d_err || !d_idx))) return FZB_E_INVALID;
+    const uint64_t nch = chunks_of(n_total);
+    if (rze_bytes < 8 + 4 * nch) return FZB_E_MALFORMED;
+    Work w = carve(d_work, n_total);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
+    rze_prepass_kernel<<<1, 1024, 0, s>>>(static_cast<const uint8_t*>(d_rze), rze_bytes, (uint32_t)nch,
+                                          (uint32_t)(2 * n_total), w.in_off, w.err);
+    CK(cudaGetLastError());
+    InvArgs a = inv_args(w, g, n_total);
+    a.rze = static_cast<const uint8_t*>(d_rze);
+    a.rze_bytes = rze_bytes;
+    a.n_chunks = (uint32_t)nch;
+    a.orig_bytes = (uint32_t)(2 * n_total);
+    a.out_err = d_err;
+    a.out_idx = d_idx;
+    a.out_count = d_count;
+    a.cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
+    a.ebx2 = 2.0f * abs_eb;
+    a.zigzag = zigzag;
+    a.shuffled = 1;
+    a.out = d_out;
+
+    const uint32_t nx = g.nx;
+    const bool pow2 = nx >= 8 && nx <= 1024 && (nx & (nx - 1)) == 0;
+    const uint32_t R = pow2 ? (uint32_t)kChunkCodes / nx : 0;
+    const bool fused = !(flags & FZB_FORCE_EXACT) && g.ndim == 3 && pow2 && g.ny % R == 0;
+    if (fused) {
+        outlier_ranges_kernel<<<(unsigned)((nch + 256) / 256 + 1), 256, 0, s>>>(
+            d_idx, d_count, a.cap, (uint32_t)nch, w.ostart, w.err);
+        CK(cudaGetLastError());
+        const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32 + 4 * kChunkCodes;
+        CK(cudaFuncSetAttribute(fused_inverse_3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem));
+        dim3 grid(g.ny / R, (g.nz + 7) / 8, 1);
+        fused_inverse_3d_kernel<<<grid, kThreads, smem, s>>>(a);
+        CK(cudaGetLastError());
+        if (n_total > g.nfield)
+            CK(cudaMemsetAsync(d_out + g.nfield, 0, sizeof(float) * (n_total - g.nfield), s));
+        if (flags & FZB_NO_SYNC) return FZB_OK;
+        uint32_t bits = 0;
+        rc = read_status(w, s, &bits);
+        if (rc) return rc;
+        if (bits & (kErrMalformed | kErrLookbackTimeout)) return status_of(bits);
+        if (!(bits & (kErrInexact | kErrUnsorted))) return FZB_OK;
+        CK(cudaMemsetAsync(w.err, 0, 4, s));  // rerun exactly below
+    }
+    a.codes = w.codes;
+    const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
+    CK(cudaFuncSetAttribute(rze_decode_codes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            smem));
+    rze_decode_codes_kernel<<<(unsigned)nch, kThreads, smem, s>>>(a);
+    CK(cudaGetLastError());
+    rc = exact_inverse(a, g, s);
+    if (rc || (flags & FZB_NO_SYNC)) return rc;
+    uint32_t bits = 0;
+    rc = read_status(w, s, &bits);
+    return rc ? rc : status_of(bits);
+}
+
+}  // extern "C"

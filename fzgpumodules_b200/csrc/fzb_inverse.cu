@@ -1,0 +1,425 @@
+// fzb_inverse.cu -- inverse kernels: RZE stream prepass, chunk decode
+// (bytes, or bytes + Bitshuffle inverse -> codes), outlier scatter, the
+// exact tile-local Lorenzo inverse (1-D/2-D/3-D) and the fused single-pass
+// RZE -> Bitshuffle -> 3-D Lorenzo inverse.
+#include "fzb_kernels.cuh"
+
+namespace fzb {
+
+// ---------------------------------------------------------------------------
+// Payload offsets of every chunk of an RZE stream (rze_stage.cu:871-900),
+// one CTA of 1024 threads.  in_off[n] receives the end of the payload.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __restrict__ rze,
+                                                           uint64_t rze_bytes, uint32_t n_expect,
+                                                           uint32_t orig_expect,
+                                                           unsigned long long* __restrict__ in_off,
+                                                           uint32_t* err) {
+    __shared__ unsigned long long s[1024];
+    const uint32_t* h = reinterpret_cast<const uint32_t*>(rze);
+    const uint32_t n = n_expect;
+    const uint64_t hdr = 8ull + 4ull * n;
+    if (h[0] != orig_expect || h[1] != n_expect || hdr > rze_bytes) {
+        // inconsistent header: flag it and point every chunk at the header end
+        if (threadIdx.x == 0) atomicOr(err, kErrMalformed);
+        for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) in_off[i] = rze_bytes + 1;
+        return;
+    }
+    const uint32_t per = (n + 1023) / 1024;
+    const uint32_t b = threadIdx.x * per, e = min(n, b + per);
+    unsigned long long sum = 0;
+    for (uint32_t i = b; i < e; i++) sum += h[2 + i] & 0x7fffffffu;
+    s[threadIdx.x] = sum;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+        unsigned long long v = (threadIdx.x >= (unsigned)d) ? s[threadIdx.x - d] : 0ull;
+        __syncthreads();
+        s[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned long long run = hdr + s[threadIdx.x] - sum;
+    for (uint32_t i = b; i < e; i++) {
+        in_off[i] = run;
+        run += h[2 + i] & 0x7fffffffu;
+    }
+    if (threadIdx.x == 1023) {
+        in_off[n] = hdr + s[1023];
+        if (hdr + s[1023] > rze_bytes) atomicOr(err, kErrMalformed);
+    }
+}
+
+// Per-chunk start of the (index-sorted) outlier list, and a sortedness check.
+__global__ void outlier_ranges_kernel(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ count,
+                                      uint32_t cap, uint32_t n_chunks, uint32_t* __restrict__ ostart,
+                                      uint32_t* err) {
+    const uint32_t nout = min(*count, cap);
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t c = tid; c <= n_chunks; c += stride) {
+        const uint64_t key = (uint64_t)c * kChunkCodes;
+        uint32_t lo = 0, hi = nout;
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if ((uint64_t)idx[mid] < key) lo = mid + 1;
+            else hi = mid;
+        }
+        ostart[c] = lo;
+    }
+    for (uint32_t i = tid; i + 1 < nout; i += stride)
+        if (idx[i] >= idx[i + 1]) atomicOr(err, kErrUnsorted);
+}
+
+__device__ __forceinline__ RzeDecSmem dec_smem(uint8_t* base, uint32_t* ws) {
+    RzeDecSmem sm;
+    sm.C = base;
+    sm.S = reinterpret_cast<uint32_t*>(base + kChunkBytes + 16);
+    sm.bm1 = reinterpret_cast<uint32_t*>(base + 2 * kChunkBytes + 16);
+    sm.bm2 = base + 2 * kChunkBytes + 16 + 2048;
+    sm.bm3 = base + 2 * kChunkBytes + 16 + 2048 + 256;
+    sm.ws = ws;
+    return sm;
+}
+constexpr int kDecSmemBytes = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
+
+__device__ __forceinline__ bool chunk_src(const InvArgs& a, uint32_t c, uint32_t* e, int* osz,
+                                          const uint8_t** src) {
+    *e = reinterpret_cast<const uint32_t*>(a.rze + 8)[c];
+    *osz = (c + 1 < a.n_chunks) ? kChunkBytes : (int)(a.orig_bytes - c * (uint32_t)kChunkBytes);
+    const uint64_t off = a.in_off[c];
+    *src = a.rze + off;
+    return off + (*e & 0x7fffffffu) <= a.rze_bytes;
+}
+
+// Plain RZE decode: one CTA per chunk, decoded bytes to bytes_out.
+__global__ void __launch_bounds__(kThreads) rze_decode_kernel(InvArgs a) {
+    extern __shared__ float4 smraw[];
+    __shared__ uint32_t s_ws[16];
+    const uint32_t c = blockIdx.x;
+    const RzeDecSmem sm = dec_smem(reinterpret_cast<uint8_t*>(smraw), s_ws);
+    uint32_t e;
+    int osz;
+    const uint8_t* src;
+    if (!chunk_src(a, c, &e, &osz, &src)) {
+        if (threadIdx.x == 0) atomicOr(a.err, kErrMalformed);
+        e = 2;  // decode as zeros
+    }
+    rze_decode_chunk(src, e, osz, sm, a.err);
+    uint8_t* dst = a.bytes_out + (size_t)c * kChunkBytes;
+    if (osz == kChunkBytes && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+        const uint4* s4 = reinterpret_cast<const uint4*>(sm.S);
+        uint4* d4 = reinterpret_cast<uint4*>(dst);
+        for (int i = threadIdx.x; i < kChunkBytes / 16; i += kThreads) d4[i] = s4[i];
+    } else {
+        const uint8_t* Sb = reinterpret_cast<const uint8_t*>(sm.S);
+        for (int i = threadIdx.x; i < osz; i += kThreads) dst[i] = Sb[i];
+    }
+}
+
+// RZE decode + Bitshuffle inverse: one CTA per chunk, codes to a.codes.
+__global__ void __launch_bounds__(kThreads) rze_decode_codes_kernel(InvArgs a) {
+    extern __shared__ float4 smraw[];
+    __shared__ uint32_t s_ws[16];
+    const uint32_t c = blockIdx.x;
+    const RzeDecSmem sm = dec_smem(reinterpret_cast<uint8_t*>(smraw), s_ws);
+    uint32_t e;
+    int osz;
+    const uint8_t* src;
+    if (!chunk_src(a, c, &e, &osz, &src)) {
+        if (threadIdx.x == 0) atomicOr(a.err, kErrMalformed);
+        e = 2;
+    }
+    rze_decode_chunk(src, e, osz, sm, a.err);
+    const int t = threadIdx.x;
+    if (osz == kChunkBytes) {
+        uint32_t x[16];
+        if (a.shuffled) {
+#pragma unroll
+            for (int b = 0; b < 16; b++) x[b] = sm.S[(15 - b) * 256 + t];
+            transpose16x2(x);
+            uint32_t rw[16];
+#pragma unroll
+            for (int l = 0; l < 8; l++) rw[l] = __byte_perm(x[2 * l], x[2 * l + 1], 0x5410);
+#pragma unroll
+            for (int l = 8; l < 16; l++) rw[l] = __byte_perm(x[2 * l - 16], x[2 * l - 15], 0x7632);
+#pragma unroll
+            for (int l = 0; l < 16; l++) x[l] = rw[l];
+        } else {
+#pragma unroll
+            for (int l = 0; l < 16; l++) x[l] = sm.S[16 * t + l];
+        }
+        uint4* d4 = reinterpret_cast<uint4*>(a.codes + (size_t)c * kChunkCodes + 32 * t);
+#pragma unroll
+        for (int v = 0; v < 4; v++) d4[v] = make_uint4(x[4 * v], x[4 * v + 1], x[4 * v + 2], x[4 * v + 3]);
+    } else {  // tail block: stored unshuffled
+        uint8_t* dst = reinterpret_cast<uint8_t*>(a.codes) + (size_t)c * kChunkBytes;
+        const uint8_t* Sb = reinterpret_cast<const uint8_t*>(sm.S);
+        for (int i = t; i < osz; i += kThreads) dst[i] = Sb[i];
+    }
+}
+
+// out must be zeroed; writes each outlier's delta at its index
+// (lorenzo_quant_kernels.cuh:23-40).
+__global__ void scatter_outliers_kernel(InvArgs a) {
+    const uint32_t n = min(*a.out_count, a.cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = a.out_idx[i];
+        if (k < a.n_total) a.out[k] = a.out_err[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Exact inverse kernels.  `out` holds the scattered outlier deltas (zero
+// elsewhere); each tile is reconstructed with the reference's add tree.
+// ---------------------------------------------------------------------------
+
+// 1-D: 1024-element tiles, thread t owns elements 4t..4t+3
+// (lorenzo_quant.cu:155-244).
+__global__ void __launch_bounds__(256) lq_inverse_1d_kernel(InvArgs a) {
+    __shared__ float s_w[8];
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint64_t base = (uint64_t)blockIdx.x * 1024 + 4 * t;
+    const float ebx2 = a.ebx2;
+    const bool zz = a.zigzag != 0;
+    float v[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const uint64_t g = base + i;
+        v[i] = (g < a.nfield) ? __fadd_rn(a.out[g], decode_code(a.codes[g], zz)) : 0.0f;
+    }
+#pragma unroll
+    for (int i = 1; i < 4; i++) v[i] = __fadd_rn(v[i], v[i - 1]);
+    float ts = v[3];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        float n = __shfl_up_sync(0xffffffffu, ts, d);
+        if ((int)lane >= d) ts = __fadd_rn(ts, n);
+    }
+    float pre = __shfl_up_sync(0xffffffffu, ts, 1);
+    if (lane > 0) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) v[i] = __fadd_rn(v[i], pre);
+    }
+    if (lane == 31) s_w[warp] = v[3];
+    __syncthreads();
+    if (warp > 0) {
+        float w[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[i] = s_w[i];
+        // Hillis-Steele over the 8 warp totals, evaluated as a tree
+#pragma unroll
+        for (int d = 1; d < 8; d <<= 1)
+#pragma unroll
+            for (int i = 7; i >= 1; i--)
+                if (i >= d) w[i] = __fadd_rn(w[i], w[i - d]);
+        const float add = w[warp - 1];
+#pragma unroll
+        for (int i = 0; i < 4; i++) v[i] = __fadd_rn(v[i], add);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const uint64_t g = base + i;
+        if (g < a.nfield) a.out[g] = __fmul_rn(v[i], ebx2);
+    }
+}
+
+// 2-D: 32x32 tiles, 128 threads = 32 x 4 row groups of 8
+// (lorenzo_quant_nd.cu:112-190).
+__global__ void __launch_bounds__(128) lq_inverse_2d_kernel(InvArgs a) {
+    __shared__ float s_tot[4][32];
+    const uint32_t lx = threadIdx.x & 31, wy = threadIdx.x >> 5;
+    const uint32_t gx = blockIdx.x * 32 + lx, gy0 = blockIdx.y * 32 + wy * 8;
+    const float ebx2 = a.ebx2;
+    const bool zz = a.zigzag != 0;
+    float v[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const uint32_t gy = gy0 + i;
+        v[i] = 0.0f;
+        if (gx < a.nx && gy < a.ny) {
+            const uint64_t g = (uint64_t)gy * a.nx + gx;
+            v[i] = __fadd_rn(a.out[g], decode_code(a.codes[g], zz));
+        }
+    }
+#pragma unroll
+    for (int i = 1; i < 8; i++) v[i] = __fadd_rn(v[i], v[i - 1]);
+    s_tot[wy][lx] = v[7];
+    __syncthreads();
+    if (wy > 0) {
+        const float t0 = s_tot[0][lx];
+        const float t1 = __fadd_rn(t0, s_tot[1][lx]);
+        const float add = (wy == 1) ? t0 : (wy == 2) ? t1 : __fadd_rn(t1, s_tot[2][lx]);
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = __fadd_rn(v[i], add);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            float n = __shfl_up_sync(0xffffffffu, v[i], d);
+            if ((int)lx >= d) v[i] = __fadd_rn(v[i], n);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const uint32_t gy = gy0 + i;
+        if (gx < a.nx && gy < a.ny) a.out[(uint64_t)gy * a.nx + gx] = __fmul_rn(v[i], ebx2);
+    }
+}
+
+// 3-D: one CTA per 32x8x8 brick (four 8x8x8 tiles); thread (x, z) scans y
+// sequentially and x as an 8-lane Hillis-Steele, then thread (x, y) runs the
+// z Hillis-Steele tree in registers (lorenzo_quant_nd.cu:281-364).
+__global__ void __launch_bounds__(256) lq_inverse_3d_kernel(InvArgs a) {
+    __shared__ float V[8][8][33];  // [z][y][x]
+    const uint32_t lx = threadIdx.x & 31, lz = threadIdx.x >> 5;
+    const uint32_t gx = blockIdx.x * 32 + lx, gy0 = blockIdx.y * 8, gz = blockIdx.z * 8 + lz;
+    const float ebx2 = a.ebx2;
+    const bool zz = a.zigzag != 0;
+    float v[8];
+#pragma unroll
+    for (int y = 0; y < 8; y++) {
+        v[y] = 0.0f;
+        const uint32_t gy = gy0 + y;
+        if (gx < a.nx && gy < a.ny && gz < a.nz) {
+            const uint64_t g = ((uint64_t)gz * a.ny + gy) * a.nx + gx;
+            v[y] = __fadd_rn(a.out[g], decode_code(a.codes[g], zz));
+        }
+    }
+#pragma unroll
+    for (int y = 1; y < 8; y++) v[y] = __fadd_rn(v[y], v[y - 1]);
+    const uint32_t tx = lx & 7;
+#pragma unroll
+    for (int y = 0; y < 8; y++) {
+#pragma unroll
+        for (int d = 1; d < 8; d <<= 1) {
+            float n = __shfl_up_sync(0xffffffffu, v[y], d, 8);
+            if ((int)tx >= d) v[y] = __fadd_rn(v[y], n);
+        }
+        V[lz][y][lx] = v[y];
+    }
+    __syncthreads();
+    const uint32_t ly = lz;  // second phase: thread (x, y)
+    float w[8];
+#pragma unroll
+    for (int z = 0; z < 8; z++) w[z] = V[z][ly][lx];
+#pragma unroll
+    for (int d = 1; d < 8; d <<= 1)
+#pragma unroll
+        for (int z = 7; z >= 1; z--)
+            if (z >= d) w[z] = __fadd_rn(w[z], w[z - d]);
+    const uint32_t gy = gy0 + ly;
+#pragma unroll
+    for (int z = 0; z < 8; z++) {
+        const uint32_t gzz = blockIdx.z * 8 + z;
+        if (gx < a.nx && gy < a.ny && gzz < a.nz)
+            a.out[((uint64_t)gzz * a.ny + gy) * a.nx + gx] = __fmul_rn(w[z], ebx2);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused inverse for 3-D fields whose 8192-code chunks are R = 8192/nx whole
+// rows (nx a power of two <= 1024, ny % R == 0).  One CTA per (R-row slab,
+// 8-plane z tile): for each plane it decodes the chunk (RZE -> Bitshuffle
+// inverse -> deltas in shared memory), adds that chunk's outliers, scans y
+// and x with the reference's add tree and keeps a running z sum in
+// registers.  The running z sum equals the reference's z Hillis-Steele tree
+// whenever every partial sum is an integer below 2^24; each column checks
+// sum |v| < 2^23 and otherwise raises kErrInexact so the host reruns the
+// exact kernels.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int dswz(int m) {  // swizzled float index in D
+    const int g = m >> 2;
+    return ((g ^ ((g >> 3) & 7)) << 2) | (m & 3);
+}
+
+__global__ void __launch_bounds__(kThreads) fused_inverse_3d_kernel(InvArgs a) {
+    extern __shared__ float4 smraw[];
+    __shared__ uint32_t s_ws[16];
+    if (*a.err & (kErrUnsorted | kErrMalformed)) return;
+    uint8_t* base = reinterpret_cast<uint8_t*>(smraw);
+    const RzeDecSmem sm = dec_smem(base, s_ws);
+    float* D = reinterpret_cast<float*>(base + kDecSmemBytes);
+    const int t = threadIdx.x;
+    const uint32_t nx = a.nx, R = kChunkCodes / nx, slabs = a.ny / R;
+    const uint32_t s = blockIdx.x, zt = blockIdx.y;
+    const uint32_t lognx = 31 - __clz(nx);
+    const float ebx2 = a.ebx2;
+    const bool zz = a.zigzag != 0;
+    const uint32_t nout = min(*a.out_count, a.cap);
+
+    float acc[4][8], gsum[4][8];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int y = 0; y < 8; y++) acc[i][y] = gsum[i][y] = 0.0f;
+    bool inexact = false;
+
+    const uint32_t z0 = zt * 8, z1 = min(z0 + 8, a.nz);
+    for (uint32_t z = z0; z < z1; z++) {
+        const uint32_t c = z * slabs + s;
+        uint32_t e;
+        int osz;
+        const uint8_t* src;
+        if (!chunk_src(a, c, &e, &osz, &src)) {
+            if (t == 0) atomicOr(a.err, kErrMalformed);
+            e = 2;
+        }
+        rze_decode_chunk(src, e, osz, sm, a.err);
+        {   // Bitshuffle inverse + code -> float delta, thread t owns codes 32t..
+            uint32_t x[16];
+#pragma unroll
+            for (int b = 0; b < 16; b++) x[b] = sm.S[(15 - b) * 256 + t];
+            transpose16x2(x);
+            float4* D4 = reinterpret_cast<float4*>(D);
+#pragma unroll
+            for (int g = 0; g < 8; g++) {
+                float f[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int E = 4 * g + k;
+                    f[k] = decode_code((x[E & 15] >> (16 * (E >> 4))) & 0xffffu, zz);
+                }
+                const int gi = 8 * t + g;
+                D4[gi ^ ((gi >> 3) & 7)] = make_float4(f[0], f[1], f[2], f[3]);
+            }
+        }
+        __syncthreads();
+        {   // outliers of this chunk: delta = outlier + decoded code
+            const uint32_t o0 = a.ostart[c], o1 = min(a.ostart[c + 1], nout);
+            const uint32_t kbase = c * (uint32_t)kChunkCodes;
+            for (uint32_t i = o0 + t; i < o1; i += kThreads) {
+                const int m = (int)(a.out_idx[i] - kbase);
+                D[dswz(m)] = __fadd_rn(a.out_err[i], D[dswz(m)]);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t col = t + kThreads * i;
+            const uint32_t ytile = col >> lognx, x = col & (nx - 1);
+            float v[8];
+#pragma unroll
+            for (int y = 0; y < 8; y++) v[y] = D[dswz((int)(((ytile * 8 + y) << lognx) + x))];
+#pragma unroll
+            for (int y = 1; y < 8; y++) v[y] = __fadd_rn(v[y], v[y - 1]);
+            const uint32_t tx = x & 7;
+#pragma unroll
+            for (int y = 0; y < 8; y++) {
+#pragma unroll
+                for (int d = 1; d < 8; d <<= 1) {
+                    float n = __shfl_up_sync(0xffffffffu, v[y], d, 8);
+                    if ((int)tx >= d) v[y] = __fadd_rn(v[y], n);
+                }
+                acc[i][y] = __fadd_rn(acc[i][y], v[y]);
+                gsum[i][y] = __fadd_rn(gsum[i][y], fabsf(v[y]));
+                inexact |= !(gsum[i][y] < 8388608.0f);
+                const uint32_t gy = s * R + ytile * 8 + y;
+                a.out[((uint64_t)z * a.ny + gy) * nx + x] = __fmul_rn(acc[i][y], ebx2);
+            }
+        }
+        __syncthreads();
+    }
+    if (__any_sync(0xffffffffu, inexact) && (t & 31) == 0) atomicOr(a.err, kErrInexact);
+}
+
+}  // namespace fzb

@@ -1,0 +1,91 @@
+// fzb_kernels.cuh -- kernel argument blocks and declarations shared by the
+// kernel translation units and the C-ABI layer.
+#pragma once
+
+#include "fzb_rze.cuh"
+
+namespace fzb {
+
+struct FwdArgs {
+    const float* in;
+    uint32_t n_total;  // elements in the code domain (>= nfield when padded)
+    uint32_t nfield;   // nx * ny * nz
+    uint32_t nx, ny, nz;
+    uint32_t plane;        // nx * ny
+    const float* ebx2_r;   // device scalar
+    float radius;
+    int zigzag;
+    int two_piece;         // separate windows for q(k) and q(k - nx)
+    uint16_t* codes;       // codes-only output
+    float* out_err;
+    uint32_t* out_idx;
+    uint32_t cap;
+    uint32_t* out_count;
+    uint8_t* rze;          // fused output stream
+    uint32_t n_chunks;
+    uint32_t codes_bytes;
+    unsigned long long* rze_size;
+    unsigned long long* st_outl;
+    unsigned long long* st_bytes;
+    uint32_t* ticket;
+    uint32_t* err;
+};
+
+struct RzeEncArgs {
+    const uint8_t* in;
+    uint64_t bytes;
+    uint8_t* out;
+    uint32_t n_chunks;
+    unsigned long long* out_size;
+    unsigned long long* st_bytes;
+    uint32_t* ticket;
+    uint32_t* err;
+};
+
+// Inverse-side arguments.
+struct InvArgs {
+    const uint8_t* rze;           // RZE stream (fused / codes path)
+    uint64_t rze_bytes;
+    const unsigned long long* in_off;  // per-chunk payload offsets (prepass)
+    uint32_t n_chunks;
+    uint32_t orig_bytes;          // RZE original byte count
+    uint16_t* codes;              // codes output (codes path)
+    uint8_t* bytes_out;           // plain RZE decode output
+    const float* out_err;
+    const uint32_t* out_idx;
+    const uint32_t* out_count;
+    uint32_t cap;
+    const uint32_t* ostart;       // per-chunk outlier start (n_chunks + 1)
+    uint32_t nx, ny, nz, plane, nfield, n_total;
+    float ebx2;                   // 2 * abs_eb
+    int zigzag;
+    int shuffled;                 // full chunks are bitshuffled (ew = 2)
+    float* out;
+    uint32_t* err;
+};
+
+__global__ void minmax_kernel(const float* x, uint64_t n, float* pmin, float* pmax);
+__global__ void resolve_eb_kernel(const float* pmin, const float* pmax, int nparts, int mode,
+                                  float user_eb, float vb_given, float* st);
+// Launches the chunk kernel instance for (ndim, fused, row-aligned); returns
+// a cudaError_t value.
+int launch_lq_chunk(int ndim, bool fused, bool rowal, const FwdArgs& a, size_t smem,
+                    unsigned grid, cudaStream_t s);
+__global__ void bitshuffle2_kernel(const uint8_t* in, uint8_t* out, int inverse);
+__global__ void bitshuffle_ballot_kernel(const uint8_t* in, uint8_t* out, uint32_t block, int ew,
+                                         int inverse);
+__global__ void rze_encode_kernel(RzeEncArgs a);
+
+__global__ void rze_prepass_kernel(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect,
+                                   uint32_t orig_expect, unsigned long long* in_off, uint32_t* err);
+__global__ void outlier_ranges_kernel(const uint32_t* idx, const uint32_t* count, uint32_t cap,
+                                      uint32_t n_chunks, uint32_t* ostart, uint32_t* err);
+__global__ void rze_decode_kernel(InvArgs a);
+__global__ void rze_decode_codes_kernel(InvArgs a);
+__global__ void scatter_outliers_kernel(InvArgs a);
+__global__ void lq_inverse_1d_kernel(InvArgs a);
+__global__ void lq_inverse_2d_kernel(InvArgs a);
+__global__ void lq_inverse_3d_kernel(InvArgs a);
+__global__ void fused_inverse_3d_kernel(InvArgs a);
+
+}  // namespace fzb

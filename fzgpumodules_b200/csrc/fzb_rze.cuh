@@ -1,0 +1,274 @@
+// fzb_rze.cuh -- block-level RZE chunk encoder/decoder (256 threads).
+//
+// Format of one chunk (modules/coders/rze/rze_stage.cu:324-445):
+//   [nonzero bytes][non-repeated bm1 bytes][non-repeated bm2 bytes]
+//   [non-repeated bm3 bytes][bm4, 4 bytes][u16 input size]
+// bmL+1 marks the bytes of bmL that differ from their predecessor (byte 0
+// compared with 0); bm1 marks nonzero input bytes.  An all-zero chunk is the
+// 2-byte size tag alone; a chunk that overflows any level is stored raw and
+// its header size word carries bit 31.
+//
+// Work split: thread t owns input bytes [64t, 64t+64) (bm1 bytes 8t..8t+7 =
+// bm2 byte t); level 3 is one ballot per warp, level 4 one ballot in warp 0.
+#pragma once
+
+#include "fzb_common.cuh"
+
+namespace fzb {
+
+struct RzeSmem {
+    uint32_t* S;    // 4096 words: chunk bytes (zero past in_size)
+    uint8_t* O;     // >= kChunkBytes + 8 bytes: encoded chunk
+    uint32_t* bm1;  // 512 words
+    uint8_t* bm2;   // 256 bytes
+    uint32_t* bm3;  // 8 words
+    uint32_t* ws;   // 16 words scan workspace
+};
+
+// Encodes the chunk held in sm.S (in_size bytes, rest zero).  Returns the
+// header size word (bit 31 = stored raw; then the payload is S itself).
+// Uniform across the block; ends with a barrier.
+__device__ static uint32_t rze_encode_chunk(const RzeSmem& sm, int in_size) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t raw_word = 0x80000000u | (uint32_t)in_size;
+
+    uint32_t w[16];
+    uint64_t M = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        w[i] = sm.S[16 * t + i];
+        M |= (uint64_t)nz_nibble(w[i]) << (4 * i);
+    }
+    uint32_t nzT;
+    uint32_t off1 = block_excl_scan((uint32_t)__popcll(M), sm.ws, &nzT);
+    if (nzT == 0) {
+        if (t == 0) {
+            sm.O[0] = (uint8_t)(in_size & 0xff);
+            sm.O[1] = (uint8_t)((in_size >> 8) & 0xff);
+        }
+        __syncthreads();
+        return 2u;
+    }
+    const int b1 = (in_size + 7) >> 3;
+    if ((int)nzT >= kRzeAvail || (int)nzT > kRzeAvail - b1) return raw_word;
+
+    {   // level 1 payload: nonzero bytes in byte order
+        uint32_t pos = off1;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            uint32_t nib = (uint32_t)(M >> (4 * i)) & 15u;
+            const uint32_t wv = w[i];
+            while (nib) {
+                int b = __ffs(nib) - 1;
+                nib &= nib - 1;
+                sm.O[pos++] = (uint8_t)(wv >> (8 * b));
+            }
+        }
+    }
+    sm.bm1[2 * t] = (uint32_t)M;
+    sm.bm1[2 * t + 1] = (uint32_t)(M >> 32);
+    __syncthreads();
+
+    // level 2: RE of bm1 (b1 bytes); this thread's bytes are M
+    uint32_t m2;
+    {
+        uint32_t prev = (t > 0) ? (uint32_t)reinterpret_cast<const uint8_t*>(sm.bm1)[8 * t - 1] : 0u;
+        uint64_t diff = M ^ ((M << 8) | (uint64_t)prev);
+        m2 = nz_byte_mask64(diff);
+        int valid = b1 - 8 * t;
+        m2 &= (valid >= 8) ? 0xffu : (valid <= 0 ? 0u : ((1u << valid) - 1u));
+    }
+    uint32_t n2T;
+    uint32_t off2 = block_excl_scan((uint32_t)__popc(m2), sm.ws, &n2T);
+    int wpos = (int)(nzT + n2T);
+    if (wpos >= kRzeAvail) return raw_word;
+    {
+        uint32_t m = m2, pos = nzT + off2;
+        while (m) {
+            int b = __ffs(m) - 1;
+            m &= m - 1;
+            sm.O[pos++] = (uint8_t)(M >> (8 * b));
+        }
+    }
+    sm.bm2[t] = (uint8_t)m2;
+    __syncthreads();
+
+    // level 3: RE of bm2 (b2 bytes); bm2 byte t is m2
+    const int b2 = (b1 + 7) >> 3;
+    if (wpos >= kRzeAvail || wpos > kRzeAvail - b2) return raw_word;
+    uint32_t p3 = (t > 0) ? (uint32_t)sm.bm2[t - 1] : 0u;
+    bool nr3 = (t < b2) && (m2 != p3);
+    uint32_t bal = __ballot_sync(0xffffffffu, nr3);
+    if (lane == 0) sm.bm3[warp] = bal;
+    uint32_t n3T;
+    uint32_t off3 = block_excl_scan(nr3 ? 1u : 0u, sm.ws, &n3T);  // has barriers
+    if (nr3) sm.O[wpos + off3] = (uint8_t)m2;
+    wpos += (int)n3T;
+    if (wpos >= kRzeAvail) return raw_word;
+
+    // level 4: RE of bm3 (b3 <= 32 bytes), bm4 stored raw
+    const int b3 = (b2 + 7) >> 3;
+    if (wpos >= kRzeAvail - 4 || wpos > (kRzeAvail - 4) - b3) return raw_word;
+    if (warp == 0) {
+        const uint8_t* b3p = reinterpret_cast<const uint8_t*>(sm.bm3);
+        uint32_t byte = b3p[lane];
+        uint32_t pb = lane ? (uint32_t)b3p[lane - 1] : 0u;
+        bool nr4 = (lane < b3) && (byte != pb);
+        uint32_t bm4 = __ballot_sync(0xffffffffu, nr4);
+        if (nr4) sm.O[wpos + __popc(bm4 & ((1u << lane) - 1u))] = (uint8_t)byte;
+        if (lane == 0) sm.ws[12] = bm4;
+    }
+    __syncthreads();
+    const uint32_t bm4 = sm.ws[12];
+    wpos += __popc(bm4);
+    if (wpos >= kRzeAvail - 4) return raw_word;
+    if (t == 0) {
+        sm.O[wpos + 0] = (uint8_t)(bm4);
+        sm.O[wpos + 1] = (uint8_t)(bm4 >> 8);
+        sm.O[wpos + 2] = (uint8_t)(bm4 >> 16);
+        sm.O[wpos + 3] = (uint8_t)(bm4 >> 24);
+        sm.O[wpos + 4] = (uint8_t)(in_size & 0xff);
+        sm.O[wpos + 5] = (uint8_t)((in_size >> 8) & 0xff);
+    }
+    __syncthreads();
+    return (uint32_t)(wpos + 6);
+}
+
+// Copies `len` bytes from shared memory `src` to global `dst` (any byte
+// alignment).  Words shared with a neighbouring chunk are written bytewise so
+// concurrent chunks never overwrite each other's bytes.
+__device__ __forceinline__ void copy_out_bytes(uint8_t* dst, const uint8_t* src, uint32_t len) {
+    if (len == 0) return;
+    const uintptr_t d0 = reinterpret_cast<uintptr_t>(dst);
+    const uintptr_t d1 = d0 + len;
+    const uintptr_t a0 = (d0 + 3) & ~(uintptr_t)3;  // first full word
+    const uintptr_t a1 = d1 & ~(uintptr_t)3;        // end of last full word
+    if (a0 >= a1) {
+        for (uint32_t i = threadIdx.x; i < len; i += kThreads) dst[i] = src[i];
+        return;
+    }
+    const uint32_t head = (uint32_t)(a0 - d0), tail = (uint32_t)(d1 - a1);
+    if (threadIdx.x < head) dst[threadIdx.x] = src[threadIdx.x];
+    if (threadIdx.x < tail) dst[(a1 - d0) + threadIdx.x] = src[(a1 - d0) + threadIdx.x];
+    const uint32_t nwords = (uint32_t)((a1 - a0) >> 2);
+    uint32_t* dw = reinterpret_cast<uint32_t*>(a0);
+    const uint8_t* s = src + head;
+    for (uint32_t i = threadIdx.x; i < nwords; i += kThreads) {
+        const uint8_t* p = s + 4 * i;
+        dw[i] = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+    }
+}
+
+struct RzeDecSmem {
+    uint8_t* C;     // >= kChunkBytes + 8: staged compressed chunk
+    uint32_t* S;    // 4096 words: decoded chunk bytes
+    uint32_t* bm1;  // 512 words
+    uint8_t* bm2;   // 256 bytes
+    uint8_t* bm3;   // 32 bytes
+    uint32_t* ws;   // 16 words
+};
+
+// Decodes one chunk (header word `e`, `osz` original bytes) from global
+// `src` into sm.S (bytes past osz zeroed).  Sets kErrMalformed on an
+// inconsistent chunk (and leaves zeros).  Ends with a barrier.
+__device__ static void rze_decode_chunk(const uint8_t* __restrict__ src, uint32_t e, int osz,
+                                 const RzeDecSmem& sm, uint32_t* err) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t comp = e & 0x7fffffffu;
+    uint8_t* Sb = reinterpret_cast<uint8_t*>(sm.S);
+    if (e & 0x80000000u) {  // raw chunk: copy the original bytes
+        const int n = min((int)comp, osz);
+        if (n != osz && t == 0) atomicOr(err, kErrMalformed);
+        for (int i = t; i < kChunkBytes; i += kThreads) Sb[i] = (i < n) ? src[i] : 0;
+        __syncthreads();
+        return;
+    }
+    if (comp <= 2) {  // all-zero chunk
+        for (int i = t; i < kChunkBytes / 4; i += kThreads) sm.S[i] = 0;
+        __syncthreads();
+        return;
+    }
+    if (comp > (uint32_t)kChunkBytes || comp < 7u) {
+        if (t == 0) atomicOr(err, kErrMalformed);
+        for (int i = t; i < kChunkBytes / 4; i += kThreads) sm.S[i] = 0;
+        __syncthreads();
+        return;
+    }
+    // stage the compressed bytes (aligned word loads, unaligned start)
+    {
+        const uintptr_t s0 = reinterpret_cast<uintptr_t>(src);
+        const uintptr_t a0 = s0 & ~(uintptr_t)3;
+        const uint32_t lead = (uint32_t)(s0 - a0);
+        const uint32_t nw = (lead + comp + 3) >> 2;
+        const uint32_t* sw = reinterpret_cast<const uint32_t*>(a0);
+        for (uint32_t i = t; i < nw; i += kThreads) {
+            uint32_t v = __ldg(sw + i);
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                int32_t pos = (int32_t)(4 * i + b) - (int32_t)lead;
+                if (pos >= 0 && pos < (int32_t)comp) sm.C[pos] = (uint8_t)(v >> (8 * b));
+            }
+        }
+    }
+    __syncthreads();
+    const int b1 = (osz + 7) >> 3, b2 = (b1 + 7) >> 3, b3 = (b2 + 7) >> 3;
+    const int bm4_start = (int)comp - 6;
+    const uint32_t bm4 = (uint32_t)sm.C[bm4_start] | ((uint32_t)sm.C[bm4_start + 1] << 8) |
+                         ((uint32_t)sm.C[bm4_start + 2] << 16) | ((uint32_t)sm.C[bm4_start + 3] << 24);
+    const int s3 = bm4_start - __popc(bm4);
+    bool bad = s3 < 0;
+    // bm3 from bm4: byte l = data3[rank(l)-1] if any set bit at <= l
+    if (warp == 0) {
+        uint32_t r = __popc(bm4 & (0xffffffffu >> (31 - lane)));
+        uint32_t v = (r && lane < b3 && !bad) ? sm.C[s3 + (int)r - 1] : 0u;
+        sm.bm3[lane] = (uint8_t)v;
+        uint32_t pc = __popc(v);
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) pc += __shfl_xor_sync(0xffffffffu, pc, d);
+        if (lane == 0) sm.ws[12] = pc;
+    }
+    __syncthreads();
+    const int s2 = s3 - (int)sm.ws[12];
+    bad = bad || s2 < 0;
+    // bm2 from bm3: thread t produces bm2 byte t from bm3 bit t
+    {
+        const uint32_t* b3w = reinterpret_cast<const uint32_t*>(sm.bm3);
+        uint32_t r = 0;
+        for (int k = 0; k < (t >> 5); k++) r += __popc(b3w[k]);
+        r += __popc(b3w[t >> 5] & (0xffffffffu >> (31 - lane)));
+        uint32_t v = (r && t < b2 && !bad) ? sm.C[s2 + (int)r - 1] : 0u;
+        sm.bm2[t] = (uint8_t)v;
+        uint32_t n2;
+        const uint32_t ex = block_excl_scan((uint32_t)__popc(v), sm.ws, &n2);
+        const int s1 = s2 - (int)n2;
+        bad = bad || s1 < 0;
+        // bm1 from bm2: thread t produces bm1 bytes 8t..8t+7 from bm2 byte t
+        uint64_t M = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            uint32_t rk = ex + __popc(v & (0xffu >> (7 - k)));
+            uint32_t byte = (rk && (8 * t + k) < b1 && !bad) ? sm.C[s1 + (int)rk - 1] : 0u;
+            M |= (uint64_t)byte << (8 * k);
+        }
+        // level-1 zero elimination: bytes 64t..64t+63 from bits of M
+        uint32_t nzT;
+        uint32_t pos = block_excl_scan((uint32_t)__popcll(M), sm.ws, &nzT);
+        bad = bad || ((int)nzT != s1);
+        if (bad) M = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            uint32_t nib = (uint32_t)(M >> (4 * i)) & 15u;
+            uint32_t wv = 0;
+            while (nib) {
+                int b = __ffs(nib) - 1;
+                nib &= nib - 1;
+                wv |= (uint32_t)sm.C[pos++] << (8 * b);
+            }
+            sm.S[16 * t + i] = wv;
+        }
+    }
+    if (bad && t == 0) atomicOr(err, kErrMalformed);
+    __syncthreads();
+}
+
+}  // namespace fzb

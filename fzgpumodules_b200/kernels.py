@@ -1,0 +1,166 @@
+"""Thin Python calls into the C ABI (include/fzb.h) on torch CUDA tensors.
+
+torch supplies device memory and the current stream; every byte of stage
+math runs in libfzb.so.  Each function mirrors one reference stage
+``execute`` (cited beside it) and returns torch tensors on the same device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import torch
+
+from ._lib import check, lib
+
+ABS, REL, NOA = 0, 1, 2
+NO_SYNC, FORCE_EXACT = 1, 2
+CHUNK_CODES = 8192
+CHUNK_BYTES = 16384
+
+
+def _ptr(t: torch.Tensor | None):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(device=None):
+    return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _dims(dims) -> C.Array:
+    d = list(dims) + [1, 1, 1]
+    return (C.c_uint32 * 3)(int(d[0]), int(d[1]), int(d[2]))
+
+
+class Workspace:
+    """Reusable device workspace sized with fzb_workspace_bytes()."""
+
+    def __init__(self):
+        self.buf: torch.Tensor | None = None
+
+    def get(self, n_total: int, device) -> tuple[C.c_void_p, int]:
+        need = int(lib().fzb_workspace_bytes(int(n_total)))
+        if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
+            self.buf = torch.empty(need, dtype=torch.uint8, device=device)
+        return _ptr(self.buf), self.buf.numel()
+
+    def status(self) -> int:
+        if self.buf is None:
+            return 0
+        return int(lib().fzb_workspace_status(_ptr(self.buf), _stream(self.buf.device)))
+
+
+_default_ws = Workspace()
+
+
+def max_outliers(n: int, capacity: float) -> int:
+    """LorenzoQuantStage::getMaxOutlierCount (lorenzo_quant.h)."""
+    return int(math.ceil(n * float(capacity)))
+
+
+def lq_forward(x: torch.Tensor, dims, eb: float, mode: int = ABS, radius: int = 32768,
+               zigzag: bool = False, outlier_capacity: float = 0.2, value_base: float = 0.0,
+               ws: Workspace | None = None):
+    """LorenzoQuantStage<float,uint16_t> forward (lorenzo_quant.cu:583-719)."""
+    ws = ws or _default_ws
+    n = x.numel()
+    cap = max_outliers(n, outlier_capacity)
+    dev = x.device
+    codes = torch.empty(n, dtype=torch.uint16, device=dev)
+    err = torch.empty(max(cap, 1), dtype=torch.float32, device=dev)
+    idx = torch.empty(max(cap, 1), dtype=torch.int32, device=dev)
+    count = torch.zeros(1, dtype=torch.int32, device=dev)
+    eb_state = torch.zeros(4, dtype=torch.float32, device=dev)
+    wp, wn = ws.get(n, dev)
+    check(lib().fzb_lq_forward(_ptr(x), n, _dims(dims), eb, mode, value_base, radius, int(zigzag),
+                               _ptr(codes), _ptr(err), _ptr(idx), cap, _ptr(count), _ptr(eb_state),
+                               wp, wn, _stream(dev)), "fzb_lq_forward")
+    return dict(codes=codes, err=err, idx=idx, count=count, eb_state=eb_state, cap=cap)
+
+
+def lq_inverse(codes, err, idx, count, cap: int, dims, abs_eb: float, zigzag: bool = False,
+               ws: Workspace | None = None):
+    """LorenzoQuantStage inverse (lorenzo_quant.cu:494-581)."""
+    ws = ws or _default_ws
+    n = codes.numel()
+    dev = codes.device
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    wp, wn = ws.get(n, dev)
+    check(lib().fzb_lq_inverse(_ptr(codes), _ptr(err), _ptr(idx), _ptr(count), cap, n, _dims(dims),
+                               abs_eb, int(zigzag), _ptr(out), wp, wn, _stream(dev)), "fzb_lq_inverse")
+    return out
+
+
+def bitshuffle(data: torch.Tensor, block: int = CHUNK_BYTES, ew: int = 2, inverse: bool = False):
+    """BitshuffleStage::execute (bitshuffle_stage.cu:355-475)."""
+    src = data.view(torch.uint8).reshape(-1)
+    out = torch.empty_like(src)
+    check(lib().fzb_bitshuffle(_ptr(src), src.numel(), block, ew, int(inverse), _ptr(out),
+                               _stream(src.device)), "fzb_bitshuffle")
+    return out
+
+
+def rze_encode(data: torch.Tensor, ws: Workspace | None = None, trim: bool = True):
+    """RZEStage forward (rze_stage.cu:774-843).  Returns (stream, size_tensor)."""
+    ws = ws or _default_ws
+    src = data.view(torch.uint8).reshape(-1)
+    nb = src.numel()
+    out = torch.empty(int(lib().fzb_rze_max_bytes(nb)), dtype=torch.uint8, device=src.device)
+    size = torch.zeros(1, dtype=torch.int64, device=src.device)
+    wp, wn = ws.get((nb + 1) // 2, src.device)
+    check(lib().fzb_rze_encode(_ptr(src), nb, _ptr(out), _ptr(size), wp, wn, _stream(src.device)),
+          "fzb_rze_encode")
+    if trim:
+        return out[: int(size.item())], size
+    return out, size
+
+
+def rze_decode(stream: torch.Tensor, orig_bytes: int, ws: Workspace | None = None):
+    """RZEStage inverse (rze_stage.cu:846-994)."""
+    ws = ws or _default_ws
+    src = stream.view(torch.uint8).reshape(-1)
+    out = torch.empty(orig_bytes, dtype=torch.uint8, device=src.device)
+    wp, wn = ws.get((orig_bytes + 1) // 2, src.device)
+    check(lib().fzb_rze_decode(_ptr(src), src.numel(), orig_bytes, _ptr(out), wp, wn,
+                               _stream(src.device)), "fzb_rze_decode")
+    return out
+
+
+def lq_bs_rze_compress(x: torch.Tensor, dims, eb: float, mode: int = ABS, radius: int = 32768,
+                       zigzag: bool = False, outlier_capacity: float = 0.2,
+                       value_base: float = 0.0, ws: Workspace | None = None, out=None):
+    """Fused LorenzoQuant -> Bitshuffle -> RZE.  Returns a dict of device
+    tensors (rze stream at capacity, rze_size, outlier buffers, eb_state)."""
+    ws = ws or _default_ws
+    n = x.numel()
+    cap = max_outliers(n, outlier_capacity)
+    dev = x.device
+    if out is None:
+        out = dict(
+            rze=torch.empty(int(lib().fzb_rze_max_bytes(2 * n)), dtype=torch.uint8, device=dev),
+            rze_size=torch.zeros(1, dtype=torch.int64, device=dev),
+            err=torch.empty(max(cap, 1), dtype=torch.float32, device=dev),
+            idx=torch.empty(max(cap, 1), dtype=torch.int32, device=dev),
+            count=torch.zeros(1, dtype=torch.int32, device=dev),
+            eb_state=torch.zeros(4, dtype=torch.float32, device=dev),
+            cap=cap)
+    wp, wn = ws.get(n, dev)
+    check(lib().fzb_lq_bs_rze_compress(
+        _ptr(x), n, _dims(dims), eb, mode, value_base, radius, int(zigzag), _ptr(out["err"]),
+        _ptr(out["idx"]), cap, _ptr(out["count"]), _ptr(out["rze"]), _ptr(out["rze_size"]),
+        _ptr(out["eb_state"]), wp, wn, _stream(dev)), "fzb_lq_bs_rze_compress")
+    return out
+
+
+def lq_bs_rze_decompress(rze: torch.Tensor, rze_bytes: int, err, idx, count, cap: int, n: int,
+                         dims, abs_eb: float, zigzag: bool = False, flags: int = 0,
+                         ws: Workspace | None = None, out=None):
+    ws = ws or _default_ws
+    dev = rze.device
+    if out is None:
+        out = torch.empty(n, dtype=torch.float32, device=dev)
+    wp, wn = ws.get(n, dev)
+    check(lib().fzb_lq_bs_rze_decompress(
+        _ptr(rze), rze_bytes, _ptr(err), _ptr(idx), _ptr(count), cap, n, _dims(dims), abs_eb,
+        int(zigzag), _ptr(out), flags, wp, wn, _stream(dev)), "fzb_lq_bs_rze_decompress")
+    return out

@@ -1,0 +1,120 @@
+/*
+ * fzb.h -- C ABI of the B200 (sm_100a) FZGPUModules hot path.
+ *
+ * Every entry point takes caller-owned device pointers, sizes, a caller-owned
+ * device workspace (size from the matching *_workspace_bytes query) and a
+ * CUDA stream passed as void*.  Nothing here allocates device memory.
+ * Return value: FZB_OK (0) or a negative FZB_E_* status.  Unless a function
+ * says otherwise it only enqueues work; device-side faults (malformed
+ * streams, look-back timeouts) are latched in the workspace and reported by
+ * fzb_workspace_status().
+ *
+ * Each declaration names the reference interface it replaces (paths within
+ * the FZGPUModules source tree).
+ */
+#ifndef FZB_H
+#define FZB_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FZB_OK 0
+#define FZB_E_INVALID (-1)     /* bad argument / unsupported configuration   */
+#define FZB_E_CUDA (-2)        /* a CUDA runtime call failed                 */
+#define FZB_E_WORKSPACE (-3)   /* workspace too small                        */
+#define FZB_E_CAPACITY (-4)    /* output buffer too small                    */
+#define FZB_E_MALFORMED (-5)   /* compressed input is inconsistent           */
+#define FZB_E_TIMEOUT (-6)     /* a bounded device wait gave up              */
+
+/* Error-bound modes (modules/fused/lorenzo_quant/lorenzo_quant.h:30-34). */
+#define FZB_ABS 0
+#define FZB_REL 1
+#define FZB_NOA 2
+
+/* fzb_*_decompress flags */
+#define FZB_NO_SYNC 1u        /* do not wait for / check the device status */
+#define FZB_FORCE_EXACT 2u    /* skip the fused inverse, run the exact kernels */
+
+int fzb_version(void);
+const char* fzb_status_string(int status);
+
+/* Workspace for any entry point over n_total Lorenzo elements (or
+ * 2*n_total bytes for the byte-stream coders). */
+size_t fzb_workspace_bytes(uint64_t n_total);
+
+/* Synchronises `stream` and returns the status latched in the workspace
+ * (FZB_OK, FZB_E_MALFORMED or FZB_E_TIMEOUT), then clears it. */
+int fzb_workspace_status(void* d_work, void* stream);
+
+/* Device scalar block written by the forward entry points:
+ * eb_state[0] value_base, [1] abs_eb, [2] ebx2_r, [3] ebx2
+ * (lorenzo_quant.cu:612-644, predictor_utils.cuh:74-117). */
+
+/* LorenzoQuantStage<float,uint16_t>::execute, forward
+ * (modules/fused/lorenzo_quant/lorenzo_quant.cu:583-719; kernels
+ * lorenzo_quant.cu:262-364, lorenzo_quant_nd.cu:29-105,199-274).
+ * dims = {nx, ny, nz} (x fastest); ndim follows LorenzoQuantStage::ndim().
+ * value_base > 0 skips the REL/NOA scan (setValueBase).  Outliers are
+ * written sorted by index; *d_count receives the total found (may exceed
+ * cap; only cap are stored). */
+int fzb_lq_forward(const float* d_in, uint64_t n_total, const uint32_t dims[3],
+                   float eb, int eb_mode, float value_base, uint32_t radius, int zigzag,
+                   uint16_t* d_codes, float* d_err, uint32_t* d_idx, uint64_t cap,
+                   uint32_t* d_count, float* d_eb_state,
+                   void* d_work, size_t work_bytes, void* stream);
+
+/* LorenzoQuantStage inverse (lorenzo_quant.cu:494-581, scatter
+ * lorenzo_quant_kernels.cuh:23-40, dequantize lorenzo_quant.cu:155-244,
+ * lorenzo_quant_nd.cu:112-190,281-364).  abs_eb is the header's error_bound. */
+int fzb_lq_inverse(const uint16_t* d_codes, const float* d_err, const uint32_t* d_idx,
+                   const uint32_t* d_count, uint64_t cap, uint64_t n_total,
+                   const uint32_t dims[3], float abs_eb, int zigzag, float* d_out,
+                   void* d_work, size_t work_bytes, void* stream);
+
+/* BitshuffleStage::execute (modules/shufflers/bitshuffle/bitshuffle_stage.cu
+ * :355-475).  ew = 1 or 2; block a positive multiple of 1024*ew. */
+int fzb_bitshuffle(const void* d_in, uint64_t bytes, uint32_t block, int ew, int inverse,
+                   void* d_out, void* stream);
+
+/* RZEStage::execute forward (modules/coders/rze/rze_stage.cu:774-843).
+ * d_out must hold fzb_rze_max_bytes(bytes); *d_out_size (device u64)
+ * receives the stream size (padded to 4 bytes). */
+uint64_t fzb_rze_max_bytes(uint64_t bytes);
+int fzb_rze_encode(const void* d_in, uint64_t bytes, void* d_out, uint64_t* d_out_size,
+                   void* d_work, size_t work_bytes, void* stream);
+
+/* RZEStage::execute inverse (rze_stage.cu:846-994) without host round
+ * trips: orig_bytes is the size recorded at compression (RZE header
+ * cached_orig_bytes, rze_stage.h:175-184). */
+int fzb_rze_decode(const void* d_in, uint64_t in_bytes, uint64_t orig_bytes, void* d_out,
+                   void* d_work, size_t work_bytes, void* stream);
+
+/* Fused LorenzoQuant -> Bitshuffle(16384 B, ew 2) -> RZE(16384 B, 4 levels)
+ * compression in one pass (the chain lorenzo_quant.cu:583-719 ->
+ * bitshuffle_stage.cu:355-475 -> rze_stage.cu:774-843).  Outputs are the
+ * pipeline's sinks: the outlier buffers and the RZE stream. */
+int fzb_lq_bs_rze_compress(const float* d_in, uint64_t n_total, const uint32_t dims[3],
+                           float eb, int eb_mode, float value_base, uint32_t radius, int zigzag,
+                           float* d_err, uint32_t* d_idx, uint64_t cap, uint32_t* d_count,
+                           void* d_rze, uint64_t* d_rze_size, float* d_eb_state,
+                           void* d_work, size_t work_bytes, void* stream);
+
+/* Inverse of the chain (rze_stage.cu:846-994 -> bitshuffle_stage.cu:325-349
+ * -> lorenzo_quant.cu:494-581).  Single pass for 3-D fields whose rows tile
+ * a 16 KiB chunk exactly; otherwise decode-to-codes + exact inverse.
+ * Unless FZB_NO_SYNC is given it synchronises, verifies the device status
+ * and reruns the exact kernels when the fused pass reported it left the
+ * exact-integer regime. */
+int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float* d_err,
+                             const uint32_t* d_idx, const uint32_t* d_count, uint64_t cap,
+                             uint64_t n_total, const uint32_t dims[3], float abs_eb, int zigzag,
+                             float* d_out, unsigned flags,
+                             void* d_work, size_t work_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

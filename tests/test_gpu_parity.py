@@ -1,0 +1,268 @@
+"""GPU parity: libfzb.so kernels vs the CPU oracle (bit-exact) and vs the
+reference's own stage kernels built from its sources (oracle/_ref), on the
+same seeded inputs."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+K = None
+
+
+def kern():
+    global K
+    if K is None:
+        from fzgpumodules_b200 import kernels
+        K = kernels
+    return K
+
+
+def _field(n, seed, kind="smooth"):
+    rng = np.random.default_rng(seed)
+    if kind == "smooth":
+        x = np.cumsum(rng.normal(size=n)).astype(np.float32)
+        x /= np.abs(x).max()
+        return x.astype(np.float32)
+    if kind == "noise":
+        return rng.normal(size=n).astype(np.float32)
+    if kind == "spiky":
+        x = np.cumsum(rng.normal(size=n) * 0.01).astype(np.float32)
+        pos = rng.choice(n, max(1, n // 500), replace=False)
+        x[pos] = rng.choice([-1e3, 1e3], pos.size)
+        return x.astype(np.float32)
+    raise ValueError(kind)
+
+
+def _g(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def _h(t):
+    return t.cpu().numpy()
+
+
+def _oracle_forward(x, dims, eb, mode, radius, zz, cap, value_base=0.0):
+    vb = value_base if value_base > 0 else (O.value_base(x, mode) if mode else 0.0)
+    abs_eb, r, e2 = O.resolve_eb(eb, mode, vb)
+    codes, err, idx, cnt = O.lq_fwd(x, dims, r, radius, zz, cap=cap, n_total=x.size)
+    return codes, err, idx, cnt, abs_eb, r, e2, vb
+
+
+GEOMS = [
+    (10000, 1, 1), (8192 * 3 + 77, 1, 1),         # 1-D (+ partial chunk)
+    (100, 70, 1), (37, 19, 1), (256, 96, 1),      # 2-D odd / row-aligned
+    (9000, 3, 1),                                  # 2-D rows wider than a chunk
+    (33, 17, 11), (64, 32, 16), (512, 16, 16),    # 3-D odd / row-aligned
+    (96, 40, 9),                                   # 3-D chunks spanning planes
+]
+
+
+@pytest.mark.parametrize("dims", GEOMS)
+@pytest.mark.parametrize("mode,zz,radius,kind", [
+    (O.ABS, False, 32768, "smooth"), (O.REL, True, 32768, "spiky"),
+    (O.ABS, True, 512, "spiky"), (O.NOA, False, 64, "noise")])
+def test_lq_forward_matches_oracle(cuda, dims, mode, zz, radius, kind):
+    n = int(np.prod(dims))
+    x = _field(n, 11, kind)
+    cap = int(np.ceil(n * 0.2))
+    codes, err, idx, cnt, abs_eb, r, e2, vb = _oracle_forward(x, dims, 1e-3, mode, radius, zz, cap)
+    out = kern().lq_forward(_g(x, cuda), dims, 1e-3, mode, radius, zz, 0.2)
+    st = _h(out["eb_state"])
+    assert st[1] == abs_eb and st[2] == r and st[3] == e2
+    assert np.array_equal(_h(out["codes"]), codes)
+    gcnt = int(_h(out["count"])[0])
+    assert gcnt == cnt
+    k = min(cnt, cap)
+    assert np.array_equal(_h(out["idx"])[:k].view(np.uint32), idx)
+    assert np.array_equal(_h(out["err"])[:k].view(np.uint32), err.view(np.uint32))
+
+
+@pytest.mark.parametrize("dims", GEOMS)
+def test_lq_inverse_matches_oracle(cuda, dims):
+    n = int(np.prod(dims))
+    x = _field(n, 12, "spiky")
+    cap = n
+    codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-3, O.ABS, 512, True, cap)
+    y = O.lq_inv(codes, err, idx, dims, e2, True)
+    dc = kern().lq_inverse(_g(codes, cuda), _g(np.append(err, 0), cuda),
+                           _g(np.append(idx, 0).astype(np.int32), cuda),
+                           _g(np.int32([cnt]), cuda), cap, dims, float(abs_eb), True)
+    assert np.array_equal(_h(dc).view(np.uint32), y.view(np.uint32))
+    assert np.max(np.abs(y - x)) <= 1e-3 * 1.01
+
+
+@pytest.mark.parametrize("ew", [1, 2])
+def test_bitshuffle_matches_oracle(cuda, ew):
+    rng = np.random.default_rng(13)
+    d = rng.integers(0, 256, 16384 * 5 + 300, dtype=np.uint8)
+    d[: 16384] &= 0x3
+    s = kern().bitshuffle(_g(d, cuda), 16384, ew)
+    assert np.array_equal(_h(s), O.bitshuffle(d, 16384, ew))
+    back = kern().bitshuffle(s, 16384, ew, inverse=True)
+    assert np.array_equal(_h(back), d)
+    s2 = kern().bitshuffle(_g(d[: 8192 * 3], cuda), 8192, ew)  # non-default block
+    assert np.array_equal(_h(s2), O.bitshuffle(d[: 8192 * 3], 8192, ew))
+
+
+def _byte_cases():
+    rng = np.random.default_rng(14)
+    sparse = np.zeros(16384 * 7, np.uint8)
+    sparse[rng.choice(sparse.size, 900, replace=False)] = rng.integers(1, 256, 900)
+    return {
+        "zeros": np.zeros(16384 * 2, np.uint8),
+        "random": rng.integers(0, 256, 16384 * 3, dtype=np.uint8),
+        "sparse": sparse,
+        "runs": np.repeat(rng.integers(0, 4, 400, dtype=np.uint8), 330),
+        "partial": rng.integers(0, 3, 3000, dtype=np.uint8),
+        "mixed": np.concatenate([np.zeros(16384, np.uint8), rng.integers(0, 256, 16384, dtype=np.uint8),
+                                 np.repeat(np.uint8([1, 2, 3]), 5001)]),
+        "near_raw": (rng.random(16384 * 2) < 0.93).astype(np.uint8) * rng.integers(1, 256, 16384 * 2, dtype=np.uint8),
+    }
+
+
+@pytest.mark.parametrize("kind", list(_byte_cases().keys()))
+def test_rze_matches_oracle(cuda, kind):
+    d = _byte_cases()[kind]
+    ref = O.rze_encode(d)
+    enc, size = kern().rze_encode(_g(d, cuda))
+    assert int(size.item()) == ref.size
+    assert np.array_equal(_h(enc), ref)
+    dec = kern().rze_decode(enc, d.size)
+    assert np.array_equal(_h(dec), d)
+
+
+FUSED_GEOMS = [(512, 16, 16), (64, 32, 24), (33, 17, 11), (256, 96, 1), (8192 * 2 + 5, 1, 1),
+               (1024, 8, 9), (96, 40, 9)]
+
+
+@pytest.mark.parametrize("dims", FUSED_GEOMS)
+@pytest.mark.parametrize("mode,zz,radius,kind", [
+    (O.REL, True, 32768, "spiky"), (O.ABS, True, 512, "spiky"), (O.ABS, False, 32768, "noise")])
+def test_fused_compress_matches_oracle_chain(cuda, dims, mode, zz, radius, kind):
+    n = int(np.prod(dims))
+    x = _field(n, 15, kind)
+    cap = int(np.ceil(n * 0.1))
+    codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-3, mode, radius, zz, cap)
+    stream = O.rze_encode(O.bitshuffle(codes, 16384, 2))
+    out = kern().lq_bs_rze_compress(_g(x, cuda), dims, 1e-3, mode, radius, zz, 0.1)
+    size = int(_h(out["rze_size"])[0])
+    assert size == stream.size
+    assert np.array_equal(_h(out["rze"])[:size], stream)
+    assert int(_h(out["count"])[0]) == cnt
+    k = min(cnt, cap)
+    assert np.array_equal(_h(out["idx"])[:k].view(np.uint32), idx)
+    assert np.array_equal(_h(out["err"])[:k].view(np.uint32), err.view(np.uint32))
+    # inverse: fused single pass (when the geometry allows) and the exact path
+    y = O.lq_inv(codes, err, idx, dims, e2, zz)
+    for flags in (0, kern().FORCE_EXACT):
+        dec = kern().lq_bs_rze_decompress(out["rze"], size, out["err"], out["idx"], out["count"],
+                                          out["cap"], n, dims, float(abs_eb), zz, flags=flags)
+        assert np.array_equal(_h(dec).view(np.uint32), y.view(np.uint32)), f"flags={flags}"
+
+
+def test_fused_decompress_exactness_fallback(cuda):
+    # huge deltas leave the exact-integer regime: the fused inverse must flag
+    # it and the host must rerun the exact kernels (same bits as the oracle)
+    dims = (64, 16, 16)
+    n = int(np.prod(dims))
+    rng = np.random.default_rng(16)
+    x = (rng.normal(size=n) * 1e4).astype(np.float32)
+    cap = n
+    codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-4, O.ABS, 32768, True, cap)
+    y = O.lq_inv(codes, err, idx, dims, e2, True)
+    out = kern().lq_bs_rze_compress(_g(x, cuda), dims, 1e-4, O.ABS, 32768, True, 1.0)
+    size = int(_h(out["rze_size"])[0])
+    dec = kern().lq_bs_rze_decompress(out["rze"], size, out["err"], out["idx"], out["count"],
+                                      out["cap"], n, dims, float(abs_eb), True)
+    assert np.array_equal(_h(dec).view(np.uint32), y.view(np.uint32))
+
+
+def test_malformed_stream_reports_error(cuda):
+    d = _byte_cases()["sparse"]
+    enc, size = kern().rze_encode(_g(d, cuda))
+    bad = enc.clone()
+    bad[8:12] = torch.tensor([0xff, 0xff, 0x00, 0x00], dtype=torch.uint8, device=cuda)  # chunk 0 size
+    with pytest.raises(Exception):
+        kern().rze_decode(bad, d.size)
+        st = kern()._default_ws.status()
+        if st != 0:
+            raise RuntimeError(st)
+
+
+# ----------------------------------------------------------- reference kernels
+
+def _ref():
+    if not os.path.exists(O.REF_STAGES):
+        pytest.skip("reference stage build absent")
+    L = C.CDLL(O.REF_STAGES)
+    L.ref_last_error.restype = C.c_char_p
+    return L
+
+
+def _vp(t):
+    return C.c_void_p(t.data_ptr())
+
+
+REF_GEOMS = [(10000, 1, 1), (100, 70, 1), (33, 17, 11), (512, 16, 16), (256, 96, 1)]
+
+
+@pytest.mark.parametrize("dims", REF_GEOMS)
+@pytest.mark.parametrize("mode,zz,radius,kind", [
+    (O.REL, True, 32768, "spiky"), (O.ABS, True, 512, "spiky"), (O.NOA, False, 32768, "smooth")])
+def test_reference_kernels_match_oracle_and_ours(cuda, dims, mode, zz, radius, kind):
+    L = _ref()
+    n = int(np.prod(dims))
+    x = _field(n, 17, kind)
+    cap = int(np.ceil(n * 0.2))
+    dx = _g(x, cuda)
+    codes = torch.empty(n, dtype=torch.int16, device=cuda)
+    err = torch.empty(cap, dtype=torch.float32, device=cuda)
+    idx = torch.empty(cap, dtype=torch.int32, device=cuda)
+    cnt = torch.zeros(1, dtype=torch.int32, device=cuda)
+    hdr = (C.c_uint8 * 128)()
+    nx, ny, nz = dims
+    rc = L.ref_lq_fwd(_vp(dx), C.c_size_t(n), C.c_size_t(nx), C.c_size_t(ny), C.c_size_t(nz),
+                      C.c_float(1e-3), mode, radius, C.c_float(0.2), int(zz), _vp(codes), _vp(err),
+                      _vp(idx), _vp(cnt), hdr)
+    assert rc == 0, L.ref_last_error()
+    rcnt = int(_h(cnt)[0])
+    ocodes, oerr, oidx, ocnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-3, mode, radius, zz, cap)
+    assert rcnt == ocnt
+    assert np.array_equal(_h(codes).view(np.uint16), ocodes)
+    k = min(rcnt, cap)
+    order = np.argsort(_h(idx)[:k].view(np.uint32), kind="stable")
+    assert np.array_equal(_h(idx)[:k].view(np.uint32)[order], oidx)  # same set, sorted
+    assert np.array_equal(_h(err)[:k].view(np.uint32)[order], oerr.view(np.uint32))
+    hv = np.frombuffer(bytes(hdr), np.uint8)
+    assert hv[:4].view(np.float32)[0] == abs_eb  # header error_bound
+    # reference inverse on its own outputs == oracle inverse == ours
+    out = torch.empty(n, dtype=torch.float32, device=cuda)
+    rc = L.ref_lq_inv(_vp(codes), _vp(err), _vp(idx), _vp(cnt), C.c_size_t(n), C.c_size_t(cap),
+                      hdr, _vp(out))
+    assert rc == 0, L.ref_last_error()
+    y = O.lq_inv(ocodes, oerr, oidx, dims, e2, zz)
+    assert np.array_equal(_h(out).view(np.uint32), y.view(np.uint32))
+
+
+@pytest.mark.parametrize("kind", ["sparse", "random", "partial", "mixed", "near_raw"])
+def test_reference_rze_and_bitshuffle_match(cuda, kind):
+    L = _ref()
+    d = _byte_cases()[kind]
+    n = d.size
+    din = _g(d, cuda)
+    out = torch.zeros(int(O.lib().orc_rze_max_bytes(n)) + 64, dtype=torch.uint8, device=cuda)
+    nb = C.c_size_t(0)
+    rc = L.ref_rze_encode(_vp(din), C.c_size_t(n), _vp(out), C.byref(nb))
+    assert rc == 0, L.ref_last_error()
+    ref_stream = _h(out)[: nb.value]
+    assert np.array_equal(ref_stream, O.rze_encode(d))
+    if n % 16384 == 0:
+        bs = torch.empty_like(din)
+        assert L.ref_bitshuffle(_vp(din), C.c_size_t(n), 16384, 2, 0, _vp(bs)) == 0
+        assert np.array_equal(_h(bs), O.bitshuffle(d, 16384, 2))
