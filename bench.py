@@ -60,7 +60,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
@@ -220,11 +220,12 @@ def run_ours(args, world, rank, local):
         e1.record(s)
         return e0, e1
 
-    for _ in range(args.warmup):
-        one("c"), one("d")
-    barrier(world)
     ev_c, ev_d = [], []
     with ClockSampler(local) as clk:
+        time.sleep(0.3)  # let the sampler start before the timed region
+        for _ in range(args.warmup):
+            one("c"), one("d")
+        barrier(world)
         t_wall = time.perf_counter()
         for _ in range(args.steps):
             ev_c.append(one("c"))
@@ -315,7 +316,7 @@ def run_ours(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

@@ -56,17 +56,25 @@ __global__ void __launch_bounds__(256) minmax_kernel(const float* __restrict__ x
 
 // EbState layout (device): [0] value_base, [1] abs_eb, [2] ebx2_r, [3] ebx2.
 // nparts == 0: value_base = vb_given (ABS, or a caller-provided base).
+// Launched with one warp.
 __global__ void resolve_eb_kernel(const float* __restrict__ pmin, const float* __restrict__ pmax,
                                   int nparts, int mode, float user_eb, float vb_given,
                                   float* __restrict__ st) {
-    if (threadIdx.x != 0) return;
     float vb = (mode != 0) ? vb_given : 0.0f;
+    float lo = INFINITY, hi = -INFINITY;
     if (mode != 0 && nparts > 0) {
-        float lo = pmin[0], hi = pmax[0];
-        for (int i = 1; i < nparts; i++) {
+        for (int i = threadIdx.x; i < nparts; i += 32) {
             lo = fminf(lo, pmin[i]);
             hi = fmaxf(hi, pmax[i]);
         }
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+            lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+            hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+        }
+    }
+    if (threadIdx.x != 0) return;
+    if (mode != 0 && nparts > 0) {
         if (mode == 2) {
             vb = __fsub_rn(hi, lo);
         } else {
@@ -128,48 +136,68 @@ __device__ __forceinline__ void load_window(float4* Q, const Win& w, const float
             if (gi < w.ngran) {
                 const long long g = w.gbase + 4LL * gi;
                 float4 v = buf[i];
-                // positions outside the field stage as 0 (never read by a valid element)
-                v.x = (g + 0 >= 0 && g + 0 < (long long)nfield) ? q_of(v.x, r) : 0.0f;
-                v.y = (g + 1 >= 0 && g + 1 < (long long)nfield) ? q_of(v.y, r) : 0.0f;
-                v.z = (g + 2 >= 0 && g + 2 < (long long)nfield) ? q_of(v.z, r) : 0.0f;
-                v.w = (g + 3 >= 0 && g + 3 < (long long)nfield) ? q_of(v.w, r) : 0.0f;
+                if (g >= 0 && g + 4 <= (long long)nfield) {
+                    v.x = q_of(v.x, r);
+                    v.y = q_of(v.y, r);
+                    v.z = q_of(v.z, r);
+                    v.w = q_of(v.w, r);
+                } else {  // field edge: positions outside stage as 0 (never read by a valid element)
+                    v.x = (g + 0 >= 0 && g + 0 < (long long)nfield) ? q_of(v.x, r) : 0.0f;
+                    v.y = (g + 1 >= 0 && g + 1 < (long long)nfield) ? q_of(v.y, r) : 0.0f;
+                    v.z = (g + 2 >= 0 && g + 2 < (long long)nfield) ? q_of(v.z, r) : 0.0f;
+                    v.w = (g + 3 >= 0 && g + 3 < (long long)nfield) ? q_of(v.w, r) : 0.0f;
+                }
                 Q[w.soff + swz(gi)] = v;
             }
         }
     }
 }
 
+// Windows a chunk needs: q(k) (cur) and q(k - nx) (up) for plane z and, in
+// 3-D when some element has z % 8 != 0, for plane z - 1.  Union mode covers
+// cur and up with one window per plane; rows wider than a chunk use two.
 struct Roles {
-    Win w[4];
-    int nw;
-    int cur[2], up[2];  // window index per plane (0 = z, 1 = z-1)
+    Win cur0, up0, cur1, up1;
+    bool two, z;  // separate up windows / plane z-1 present
 };
 
-// Windows needed by a chunk [i0, i0+cnt).  Union mode covers q(k) and
-// q(k-nx) with one window per plane; wide rows use two.
+__device__ __forceinline__ Win make_win(long long start, long long end, int& soff) {
+    const long long gb = start >= 0 ? (start & ~3LL) : -(((-start) + 3) & ~3LL);
+    const int ng = (int)((end - gb + 3) >> 2);
+    Win w{gb, ng, soff};
+    soff += (ng + 7) & ~7;
+    return w;
+}
+
 __device__ __forceinline__ void make_roles(const FwdArgs& a, int ndim, uint32_t i0, uint32_t cnt,
                                            bool need_z, Roles& R) {
-    R.nw = 0;
     int soff = 0;
-    auto add = [&](long long start, long long end) -> int {
-        long long gb = start >= 0 ? (start & ~3LL) : -(((-start) + 3) & ~3LL);
-        int ng = (int)((end - gb + 3) >> 2);
-        R.w[R.nw] = Win{gb, ng, soff};
-        soff += (ng + 7) & ~7;
-        return R.nw++;
-    };
-    const int planes = (ndim == 3 && need_z) ? 2 : 1;
-    for (int p = 0; p < planes; p++) {
+    R.two = (ndim >= 2) && a.two_piece;
+    R.z = (ndim == 3) && need_z;
+    for (int p = 0; p < (R.z ? 2 : 1); p++) {
         const long long sh = p ? (long long)a.plane : 0;
-        const long long s = (long long)i0 - sh, e = (long long)i0 + cnt - sh;
+        const long long s0 = (long long)i0 - sh, e0 = (long long)i0 + cnt - sh;
+        Win cur, up;
         if (ndim == 1) {
-            R.cur[p] = R.up[p] = add(s - 1, e);
-        } else if (!a.two_piece) {
-            R.cur[p] = R.up[p] = add(s - (long long)a.nx - 1, e);
+            cur = up = make_win(s0 - 1, e0, soff);
+        } else if (!R.two) {
+            cur = up = make_win(s0 - (long long)a.nx - 1, e0, soff);
         } else {
-            R.up[p] = add(s - (long long)a.nx - 1, e - (long long)a.nx);
-            R.cur[p] = add(s - 1, e);
+            up = make_win(s0 - (long long)a.nx - 1, e0 - (long long)a.nx, soff);
+            cur = make_win(s0 - 1, e0, soff);
         }
+        if (p == 0) { R.cur0 = cur; R.up0 = up; }
+        else { R.cur1 = cur; R.up1 = up; }
+    }
+}
+
+__device__ __forceinline__ void load_roles(float4* Q, const Roles& R, const float* in, uint32_t nfield,
+                                           float r, bool vec_ok) {
+    load_window(Q, R.cur0, in, nfield, r, vec_ok);
+    if (R.two) load_window(Q, R.up0, in, nfield, r, vec_ok);
+    if (R.z) {
+        load_window(Q, R.cur1, in, nfield, r, vec_ok);
+        if (R.two) load_window(Q, R.up1, in, nfield, r, vec_ok);
     }
 }
 
@@ -187,14 +215,14 @@ template <int NDIM>
 __device__ __forceinline__ float delta_at(const FwdArgs& a, const float4* Q, const Roles& R,
                                           uint32_t k) {
     if (NDIM == 1) {
-        const float q = qread(Q, R.w[R.cur[0]], k);
-        return (k & 1023u) ? __fsub_rn(q, qread(Q, R.w[R.cur[0]], (long long)k - 1)) : q;
+        const float q = qread(Q, R.cur0, k);
+        return (k & 1023u) ? __fsub_rn(q, qread(Q, R.cur0, (long long)k - 1)) : q;
     }
     const uint32_t z = (NDIM == 3) ? k / a.plane : 0u;
     const uint32_t rem = k - z * a.plane;
     const uint32_t y = rem / a.nx, x = rem - y * a.nx;
-    const Win& wc = R.w[R.cur[0]];
-    const Win& wu = R.w[R.up[0]];
+    const Win& wc = R.cur0;
+    const Win& wu = R.up0;
     const long long ku = (long long)k - a.nx;
     if (NDIM == 2) {
         const uint32_t tx = x & 31u, ty = y & 31u;
@@ -211,8 +239,8 @@ __device__ __forceinline__ float delta_at(const FwdArgs& a, const float4* Q, con
         float v = qread(Q, w, kk);
         return tz ? __fsub_rn(v, qread(Q, *wz, kkz)) : v;
     };
-    const Win* wcz = tz ? &R.w[R.cur[1]] : nullptr;
-    const Win* wuz = tz ? &R.w[R.up[1]] : nullptr;
+    const Win* wcz = &R.cur1;
+    const Win* wuz = &R.up1;
     float b0 = A(wc, k, kz, wcz);
     if (tx) b0 = __fsub_rn(b0, A(wc, (long long)k - 1, kz - 1, wcz));
     if (!ty) return b0;
@@ -270,6 +298,98 @@ __device__ __forceinline__ void rze_place_chunk(uint8_t* __restrict__ out, uint3
     }
 }
 
+// Row-vector path: one thread, 32 consecutive elements of one row, all
+// operands staged in shared memory.  TZ/TY say whether the z / y predecessor
+// lies inside the tile (z % 8 != 0, y % 8 != 0; 2-D: y % 32 != 0).
+struct GroupIn {
+    const float4 *Qc, *Qu, *Qcz, *Quz;
+    int rc, ru, rcz, ruz;
+    float p0;
+    uint32_t j0;
+    float radius;
+};
+
+template <bool ZZ>
+__device__ __forceinline__ uint32_t code_of(float c) {
+    const int iv = __float2int_rz(c);
+    if (ZZ) {
+        const int s = (int)(int16_t)iv;
+        return (((uint32_t)s << 1) ^ (uint32_t)(s >> 15)) & 0xffffu;
+    }
+    return (uint32_t)iv & 0xffffu;
+}
+
+__device__ __forceinline__ void unpack4(float4 v, float* d) {
+    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+}
+
+template <int NDIM, bool ZZ, bool TZ, bool TY>
+__device__ __forceinline__ void group_codes(const GroupIn& g, uint32_t (&x)[16], uint32_t& om) {
+    float p0 = g.p0, p1 = 0.0f;  // carried a00 / a01 (3-D), v0 (2-D), q (1-D)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        float qc[16], qu[16], qcz[16], quz[16];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            unpack4(g.Qc[swz(g.rc + 4 * h + k)], qc + 4 * k);
+            if (NDIM >= 2 && TY) unpack4(g.Qu[swz(g.ru + 4 * h + k)], qu + 4 * k);
+            if (NDIM == 3 && TZ) {
+                unpack4(g.Qcz[swz(g.rcz + 4 * h + k)], qcz + 4 * k);
+                if (TY) unpack4(g.Quz[swz(g.ruz + 4 * h + k)], quz + 4 * k);
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 16; e++) {
+            const int E = 16 * h + e;
+            float cc;
+            if (NDIM == 3) {
+                const float a00 = TZ ? __fsub_rn(qc[e], qcz[e]) : qc[e];
+                const float b0 = (E & 7) ? __fsub_rn(a00, p0) : a00;
+                p0 = a00;
+                if (TY) {
+                    const float a01 = TZ ? __fsub_rn(qu[e], quz[e]) : qu[e];
+                    const float b1 = (E & 7) ? __fsub_rn(a01, p1) : a01;
+                    p1 = a01;
+                    cc = __fsub_rn(b0, b1);
+                } else {
+                    cc = b0;
+                }
+            } else if (NDIM == 2) {
+                const float v0 = TY ? __fsub_rn(qc[e], qu[e]) : qc[e];
+                cc = E ? __fsub_rn(v0, p0) : v0;
+                p0 = v0;
+            } else {
+                cc = ((g.j0 + E) & 1023u) ? __fsub_rn(qc[e], p0) : qc[e];
+                p0 = qc[e];
+            }
+            const bool qz = fabsf(cc) < g.radius;
+            const uint32_t code = qz ? code_of<ZZ>(cc) : 0u;
+            om |= (qz ? 0u : 1u) << E;
+            if (h == 0) x[e] = code;
+            else x[e] = __byte_perm(x[e], code, 0x5410);
+        }
+    }
+}
+
+template <int NDIM, bool ZZ>
+__device__ __forceinline__ void group_dispatch(const GroupIn& g, bool tz, bool ty, uint32_t (&x)[16],
+                                               uint32_t& om) {
+    if (NDIM == 3) {
+        if (tz) {
+            if (ty) group_codes<NDIM, ZZ, true, true>(g, x, om);
+            else group_codes<NDIM, ZZ, true, false>(g, x, om);
+        } else {
+            if (ty) group_codes<NDIM, ZZ, false, true>(g, x, om);
+            else group_codes<NDIM, ZZ, false, false>(g, x, om);
+        }
+    } else if (NDIM == 2) {
+        if (ty) group_codes<NDIM, ZZ, false, true>(g, x, om);
+        else group_codes<NDIM, ZZ, false, false>(g, x, om);
+    } else {
+        group_codes<NDIM, ZZ, false, false>(g, x, om);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // The chunk kernel.  FUSED=false writes codes; FUSED=true bitshuffles them
 // (16 KiB blocks, element width 2, ballot layout) and RZE-encodes the block
@@ -278,7 +398,7 @@ __device__ __forceinline__ void rze_place_chunk(uint8_t* __restrict__ out, uint3
 // ---------------------------------------------------------------------------
 
 template <int NDIM, bool FUSED, bool ROWAL>
-__global__ void __launch_bounds__(kThreads) lq_chunk_kernel(FwdArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) lq_chunk_kernel(FwdArgs a) {
     extern __shared__ float4 Q[];
     __shared__ uint32_t s_ws[16];
     __shared__ uint32_t s_chunk;
@@ -301,7 +421,7 @@ __global__ void __launch_bounds__(kThreads) lq_chunk_kernel(FwdArgs a) {
     Roles R;
     make_roles(a, NDIM, i0, cnt, need_z, R);
     const bool vec_ok = (reinterpret_cast<uintptr_t>(a.in) & 15) == 0;
-    for (int i = 0; i < R.nw; i++) load_window(Q, R.w[i], a.in, a.nfield, r, vec_ok);
+    load_roles(Q, R, a.in, a.nfield, r, vec_ok);
     __syncthreads();
 
     // ---- pass 1: codes of this thread's 32 consecutive elements ----
@@ -310,79 +430,37 @@ __global__ void __launch_bounds__(kThreads) lq_chunk_kernel(FwdArgs a) {
     uint32_t x[16];
 #pragma unroll
     for (int l = 0; l < 16; l++) x[l] = 0;
-    uint32_t nout = 0;
     // row-vector path only for whole groups; partial groups use the element path
     const bool whole = ROWAL && (j0 + 32 <= cnt) && (k0 + 32 <= a.nfield);
+    uint32_t om = 0;  // outlier bit per element
     if (whole) {
-        {
-            uint32_t ty = 0, tz = 0;
-            if (NDIM == 3) {
-                const uint32_t z = k0 / a.plane, y = (k0 - z * a.plane) / a.nx;
-                ty = y & 7u;
-                tz = z & 7u;
-            } else if (NDIM == 2) {
-                ty = (k0 / a.nx) & 31u;
-            }
-            const float4* Qc = Q + R.w[R.cur[0]].soff;
-            const float4* Qu = Q + R.w[R.up[0]].soff;
-            const int rc = (int)(((long long)k0 - R.w[R.cur[0]].gbase) >> 2);
-            const int ru = (int)(((long long)k0 - a.nx - R.w[R.up[0]].gbase) >> 2);
-            const float4* Qcz = Qc;
-            const float4* Quz = Qu;
-            int rcz = 0, ruz = 0;
-            if (NDIM == 3 && tz) {
-                Qcz = Q + R.w[R.cur[1]].soff;
-                Quz = Q + R.w[R.up[1]].soff;
-                rcz = (int)(((long long)k0 - a.plane - R.w[R.cur[1]].gbase) >> 2);
-                ruz = (int)(((long long)k0 - a.plane - a.nx - R.w[R.up[1]].gbase) >> 2);
-            }
-            float p0 = 0.f, p1 = 0.f;  // carried a00 / a01 (3-D), v0 (2-D), q (1-D)
-            if (NDIM == 1 && (j0 & 1023u)) p0 = qread(Q, R.w[R.cur[0]], (long long)k0 - 1);
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                float qc[16], qu[16], qcz[16], quz[16];
-#pragma unroll
-                for (int g = 0; g < 4; g++) {
-                    float4 v = Qc[swz(rc + 4 * h + g)];
-                    qc[4 * g] = v.x; qc[4 * g + 1] = v.y; qc[4 * g + 2] = v.z; qc[4 * g + 3] = v.w;
-                    if (NDIM >= 2) {
-                        float4 u = Qu[swz(ru + 4 * h + g)];
-                        qu[4 * g] = u.x; qu[4 * g + 1] = u.y; qu[4 * g + 2] = u.z; qu[4 * g + 3] = u.w;
-                    }
-                    if (NDIM == 3 && tz) {
-                        float4 vz = Qcz[swz(rcz + 4 * h + g)];
-                        float4 uz = Quz[swz(ruz + 4 * h + g)];
-                        qcz[4 * g] = vz.x; qcz[4 * g + 1] = vz.y; qcz[4 * g + 2] = vz.z; qcz[4 * g + 3] = vz.w;
-                        quz[4 * g] = uz.x; quz[4 * g + 1] = uz.y; quz[4 * g + 2] = uz.z; quz[4 * g + 3] = uz.w;
-                    }
-                }
-#pragma unroll
-                for (int e = 0; e < 16; e++) {
-                    const int E = 16 * h + e;
-                    float cc;
-                    if (NDIM == 3) {
-                        float a00 = tz ? __fsub_rn(qc[e], qcz[e]) : qc[e];
-                        float a01 = tz ? __fsub_rn(qu[e], quz[e]) : qu[e];
-                        float b0 = (E & 7) ? __fsub_rn(a00, p0) : a00;
-                        float b1 = (E & 7) ? __fsub_rn(a01, p1) : a01;
-                        cc = ty ? __fsub_rn(b0, b1) : b0;
-                        p0 = a00;
-                        p1 = a01;
-                    } else if (NDIM == 2) {
-                        float v0 = ty ? __fsub_rn(qc[e], qu[e]) : qc[e];
-                        cc = E ? __fsub_rn(v0, p0) : v0;
-                        p0 = v0;
-                    } else {
-                        cc = ((j0 + E) & 1023u) ? __fsub_rn(qc[e], p0) : qc[e];
-                        p0 = qc[e];
-                    }
-                    const bool qz = fabsf(cc) < a.radius;
-                    const uint32_t code = qz ? encode_code(cc, zz) : 0u;
-                    nout += qz ? 0u : 1u;
-                    x[e] |= code << (16 * h);
-                }
-            }
+        uint32_t ty = 0, tz = 0;
+        if (NDIM == 3) {
+            const uint32_t z = k0 / a.plane, y = (k0 - z * a.plane) / a.nx;
+            ty = y & 7u;
+            tz = z & 7u;
+        } else if (NDIM == 2) {
+            ty = (k0 / a.nx) & 31u;
         }
+        GroupIn g;
+        g.Qc = Q + R.cur0.soff;
+        g.Qu = Q + R.up0.soff;
+        g.rc = (int)(((long long)k0 - R.cur0.gbase) >> 2);
+        g.ru = (int)(((long long)k0 - a.nx - R.up0.gbase) >> 2);
+        g.Qcz = g.Qc;
+        g.Quz = g.Qu;
+        g.rcz = g.ruz = 0;
+        if (NDIM == 3 && tz) {
+            g.Qcz = Q + R.cur1.soff;
+            g.Quz = Q + R.up1.soff;
+            g.rcz = (int)(((long long)k0 - a.plane - R.cur1.gbase) >> 2);
+            g.ruz = (int)(((long long)k0 - a.plane - a.nx - R.up1.gbase) >> 2);
+        }
+        g.p0 = (NDIM == 1 && (j0 & 1023u)) ? qread(Q, R.cur0, (long long)k0 - 1) : 0.0f;
+        g.j0 = j0;
+        g.radius = a.radius;
+        if (zz) group_dispatch<NDIM, true>(g, tz != 0, ty != 0, x, om);
+        else group_dispatch<NDIM, false>(g, tz != 0, ty != 0, x, om);
     } else if (j0 < cnt && k0 < a.nfield) {
         for (int E = 0; E < 32; E++) {
             const uint32_t k = k0 + E;
@@ -390,13 +468,14 @@ __global__ void __launch_bounds__(kThreads) lq_chunk_kernel(FwdArgs a) {
                 const float cc = delta_at<NDIM>(a, Q, R, k);
                 const bool qz = fabsf(cc) < a.radius;
                 const uint32_t code = qz ? encode_code(cc, zz) : 0u;
-                nout += qz ? 0u : 1u;
+                om |= (qz ? 0u : 1u) << E;
 #pragma unroll
                 for (int l = 0; l < 16; l++)
                     if (l == (E & 15)) x[l] |= code << (16 * (E >> 4));
             }
         }
     }
+    const uint32_t nout = __popc(om);
 
     // ---- outliers: block scan + look-back for their global offset ----
     uint32_t ototal;

@@ -90,7 +90,7 @@ def test_lq_inverse_matches_oracle(cuda, dims):
     cap = n
     codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-3, O.ABS, 512, True, cap)
     y = O.lq_inv(codes, err, idx, dims, e2, True)
-    dc = kern().lq_inverse(_g(codes, cuda), _g(np.append(err, 0), cuda),
+    dc = kern().lq_inverse(_g(codes, cuda), _g(np.append(err, np.float32(0)), cuda),
                            _g(np.append(idx, 0).astype(np.int32), cuda),
                            _g(np.int32([cnt]), cuda), cap, dims, float(abs_eb), True)
     assert np.array_equal(_h(dc).view(np.uint32), y.view(np.uint32))
