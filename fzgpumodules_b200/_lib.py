@@ -43,7 +43,7 @@ def lib():
         L.fzb_status_string.restype = C.c_char_p
         L.fzb_status_string.argtypes = [i32]
         L.fzb_workspace_bytes.restype = sz
-        L.fzb_workspace_bytes.argtypes = [u64]
+        L.fzb_workspace_bytes.argtypes = [u64, u64]
         L.fzb_workspace_status.restype = i32
         L.fzb_workspace_status.argtypes = [p, p]
         L.fzb_lq_forward.restype = i32

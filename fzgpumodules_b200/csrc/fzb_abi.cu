@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 
 #include "../../include/fzb.h"
@@ -18,15 +19,19 @@ constexpr int kMaxParts = 1024;      // min/max partials
 
 struct Work {
     uint32_t* err;
-    uint32_t* ticket;
-    float* inv_scalars;
+    uint32_t* ostage_ctr;
+    unsigned int* mm_done;
     float* pmin;
     float* pmax;
-    unsigned long long* st_outl;
-    unsigned long long* st_bytes;
-    unsigned long long* in_off;
-    uint32_t* ostart;
-    uint16_t* codes;   // 2 * n_total bytes: codes staging for the exact inverse
+    unsigned long long* in_off;   // decode: payload offsets; encode: pay_off
+    uint32_t* ostart;             // decode: per-chunk outlier start; encode: ofin
+    uint32_t* sizes;
+    uint32_t* ocnt;
+    uint32_t* obase;
+    uint16_t* codes;   // 2 * n_total bytes: chunk slots (encode) / codes (exact inverse)
+    float* ostage_err;
+    uint32_t* ostage_idx;
+    uint64_t ostage_cap;
     size_t need;
 };
 
@@ -34,7 +39,7 @@ inline size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 inline uint64_t chunks_of(uint64_t n_total) { return (n_total + kChunkCodes - 1) / kChunkCodes; }
 
-Work carve(void* base, uint64_t n_total) {
+Work carve(void* base, uint64_t n_total, uint64_t cap) {
     Work w{};
     const uint64_t nch = chunks_of(n_total) + 1;
     uint8_t* p = static_cast<uint8_t*>(base);
@@ -46,20 +51,31 @@ Work carve(void* base, uint64_t n_total) {
     };
     uint8_t* ctrl = take(kCtrlBytes);
     w.err = reinterpret_cast<uint32_t*>(ctrl);
-    w.ticket = reinterpret_cast<uint32_t*>(ctrl ? ctrl + 4 : nullptr);
-    w.inv_scalars = reinterpret_cast<float*>(ctrl ? ctrl + 64 : nullptr);
+    w.ostage_ctr = reinterpret_cast<uint32_t*>(ctrl ? ctrl + 4 : nullptr);
+    w.mm_done = reinterpret_cast<unsigned int*>(ctrl ? ctrl + 8 : nullptr);
     w.pmin = reinterpret_cast<float*>(take(sizeof(float) * kMaxParts));
     w.pmax = reinterpret_cast<float*>(take(sizeof(float) * kMaxParts));
-    w.st_outl = reinterpret_cast<unsigned long long*>(take(8 * nch));
-    w.st_bytes = reinterpret_cast<unsigned long long*>(take(8 * nch));
     w.in_off = reinterpret_cast<unsigned long long*>(take(8 * (nch + 1)));
     w.ostart = reinterpret_cast<uint32_t*>(take(4 * (nch + 1)));
-    w.codes = reinterpret_cast<uint16_t*>(take(2 * (n_total + kChunkCodes)));
+    w.sizes = reinterpret_cast<uint32_t*>(take(4 * nch));
+    w.ocnt = reinterpret_cast<uint32_t*>(take(4 * nch));
+    w.obase = reinterpret_cast<uint32_t*>(take(4 * nch));
+    w.codes = reinterpret_cast<uint16_t*>(take(2 * (n_total + kChunkCodes) + 64));
+    w.ostage_cap = cap;
+    w.ostage_err = reinterpret_cast<float*>(take(4 * (cap + 1)));
+    w.ostage_idx = reinterpret_cast<uint32_t*>(take(4 * (cap + 1)));
     w.need = off;
     return w;
 }
 
 inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
+
+// FZB_DISABLE_SLAB=1 routes 3-D fused compression through the per-chunk
+// kernel (both produce identical bytes; tests exercise each).
+inline unsigned flags_env() {
+    const char* v = getenv("FZB_DISABLE_SLAB");
+    return (v && v[0] == '1') ? 1u : 0u;
+}
 
 #define CK(call)                                          \
     do {                                                  \
@@ -110,14 +126,17 @@ int launch_lq(const Geometry& g, bool fused, const FwdArgs& a, size_t smem, uint
 int resolve_eb(const float* d_in, uint64_t n_total, float eb, int mode, float value_base,
                const Work& w, float* d_eb_state, cudaStream_t s) {
     if (mode != FZB_ABS && !(value_base > 0.0f)) {
-        uint64_t blocks = (n_total + 1023) / 1024;
-        int parts = (int)(blocks < (uint64_t)kMaxParts ? blocks : kMaxParts);
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        uint64_t want = (n_total / 4 + 255) / 256;
+        int parts = (int)(want < (uint64_t)(4 * sms) ? want : (uint64_t)(4 * sms));
         if (parts < 1) parts = 1;
-        minmax_kernel<<<parts, 256, 0, s>>>(d_in, n_total, w.pmin, w.pmax);
-        CK(cudaGetLastError());
-        resolve_eb_kernel<<<1, 32, 0, s>>>(w.pmin, w.pmax, parts, mode, eb, 0.0f, d_eb_state);
+        if (parts > kMaxParts) parts = kMaxParts;
+        minmax_kernel<<<parts, 256, 0, s>>>(d_in, n_total, w.pmin, w.pmax, w.mm_done, mode, eb,
+                                            d_eb_state);
     } else {
-        resolve_eb_kernel<<<1, 32, 0, s>>>(nullptr, nullptr, 0, mode, eb, value_base, d_eb_state);
+        resolve_eb_kernel<<<1, 32, 0, s>>>(mode, eb, value_base, d_eb_state);
     }
     CK(cudaGetLastError());
     return FZB_OK;
@@ -134,13 +153,11 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
     if (!d_in || !d_count || !d_eb_state || (cap && (!d_err || !d_idx))) return FZB_E_INVALID;
     if (fused ? (!d_rze || !d_rze_size) : !d_codes) return FZB_E_INVALID;
     if (eb_mode < FZB_ABS || eb_mode > FZB_NOA || !(eb > 0.0f)) return FZB_E_INVALID;
-    Work w = carve(d_work, n_total);
+    Work w = carve(d_work, n_total, cap);
     if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
     cudaStream_t s = S(stream);
     const uint64_t nch = chunks_of(n_total);
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
-    CK(cudaMemsetAsync(w.st_outl, 0, 8 * nch, s));
-    if (fused) CK(cudaMemsetAsync(w.st_bytes, 0, 8 * nch, s));
     rc = resolve_eb(d_in, n_total, eb, eb_mode, value_base, w, d_eb_state, s);
     if (rc) return rc;
     FwdArgs a{};
@@ -156,19 +173,52 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
     a.zigzag = zigzag;
     a.two_piece = (g.ndim >= 2 && g.nx > (uint32_t)kChunkCodes) ? 1 : 0;
     a.codes = d_codes;
-    a.out_err = d_err;
-    a.out_idx = d_idx;
-    a.cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
-    a.out_count = d_count;
-    a.rze = static_cast<uint8_t*>(d_rze);
     a.n_chunks = (uint32_t)nch;
-    a.codes_bytes = (uint32_t)(2 * n_total);
-    a.rze_size = reinterpret_cast<unsigned long long*>(d_rze_size);
-    a.st_outl = w.st_outl;
-    a.st_bytes = w.st_bytes;
-    a.ticket = w.ticket;
+    a.slots = reinterpret_cast<uint8_t*>(w.codes);
+    a.sizes = w.sizes;
+    a.ocnt = w.ocnt;
+    a.obase = w.obase;
+    a.ostage_ctr = w.ostage_ctr;
+    a.ostage_err = w.ostage_err;
+    a.ostage_idx = w.ostage_idx;
+    a.ostage_cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
     a.err = w.err;
-    return launch_lq(g, fused, a, lq_smem_bytes(g, fused), (uint32_t)nch, s);
+    const uint32_t nx = g.nx;
+    const bool slab = fused && g.ndim == 3 && nx >= 32 && nx <= 1024 && (nx & (nx - 1)) == 0 &&
+                      g.ny % ((uint32_t)kChunkCodes / nx) == 0 && g.nfield == n_total &&
+                      !(flags_env() & 1);
+    if (slab) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        rc = launch_lq3d_slab(a, (unsigned)(2 * sms), s) == 0 ? FZB_OK : FZB_E_CUDA;
+    } else {
+        rc = launch_lq(g, fused, a, lq_smem_bytes(g, fused), (uint32_t)nch, s);
+    }
+    if (rc) return rc;
+    AsmArgs m{};
+    m.slots = a.slots;
+    m.sizes = fused ? w.sizes : nullptr;
+    m.n_chunks = (uint32_t)nch;
+    m.orig_bytes = (uint32_t)(2 * n_total);
+    m.out = static_cast<uint8_t*>(d_rze);
+    m.out_size = reinterpret_cast<unsigned long long*>(d_rze_size);
+    m.pay_off = w.in_off;
+    m.ocnt = w.ocnt;
+    m.obase = w.obase;
+    m.ofin = w.ostart;
+    m.ostage_err = w.ostage_err;
+    m.ostage_idx = w.ostage_idx;
+    m.ostage_cap = a.ostage_cap;
+    m.out_err = d_err;
+    m.out_idx = d_idx;
+    m.cap = a.ostage_cap;
+    m.out_count = d_count;
+    assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
+    CK(cudaGetLastError());
+    assemble_copy_kernel<<<(unsigned)nch, 256, 0, s>>>(m);
+    CK(cudaGetLastError());
+    return FZB_OK;
 }
 
 InvArgs inv_args(const Work& w, const Geometry& g, uint64_t n_total) {
@@ -238,7 +288,7 @@ const char* fzb_status_string(int st) {
     }
 }
 
-size_t fzb_workspace_bytes(uint64_t n_total) { return carve(nullptr, n_total).need; }
+size_t fzb_workspace_bytes(uint64_t n_total, uint64_t cap) { return carve(nullptr, n_total, cap).need; }
 
 int fzb_workspace_status(void* d_work, void* stream) {
     if (!d_work) return FZB_E_INVALID;
@@ -277,7 +327,7 @@ int fzb_lq_inverse(const uint16_t* d_codes, const float* d_err, const uint32_t* 
     int rc = geometry(n_total, dims, &g);
     if (rc) return rc;
     if (!d_codes || !d_out || !d_count || (cap && (!d_err || !d_idx))) return FZB_E_INVALID;
-    Work w = carve(d_work, n_total);
+    Work w = carve(d_work, n_total, 0);
     if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
     cudaStream_t s = S(stream);
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
@@ -327,24 +377,31 @@ int fzb_rze_encode(const void* d_in, uint64_t bytes, void* d_out, uint64_t* d_ou
                    void* d_work, size_t work_bytes, void* stream) {
     if (!d_in || !d_out || !d_out_size || bytes == 0 || bytes >= (1ull << 32)) return FZB_E_INVALID;
     const uint64_t n_equiv = (bytes + 1) / 2;
-    Work w = carve(d_work, n_equiv);
+    Work w = carve(d_work, n_equiv, 0);
     if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
     cudaStream_t s = S(stream);
     const uint64_t nch = (bytes + kChunkBytes - 1) / kChunkBytes;
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
-    CK(cudaMemsetAsync(w.st_bytes, 0, 8 * nch, s));
     RzeEncArgs a{};
     a.in = static_cast<const uint8_t*>(d_in);
     a.bytes = bytes;
-    a.out = static_cast<uint8_t*>(d_out);
-    a.n_chunks = (uint32_t)nch;
-    a.out_size = reinterpret_cast<unsigned long long*>(d_out_size);
-    a.st_bytes = w.st_bytes;
-    a.ticket = w.ticket;
-    a.err = w.err;
+    a.slots = reinterpret_cast<uint8_t*>(w.codes);
+    a.sizes = w.sizes;
     const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
     CK(cudaFuncSetAttribute(rze_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     rze_encode_kernel<<<(unsigned)nch, kThreads, smem, s>>>(a);
+    CK(cudaGetLastError());
+    AsmArgs m{};
+    m.slots = a.slots;
+    m.sizes = w.sizes;
+    m.n_chunks = (uint32_t)nch;
+    m.orig_bytes = (uint32_t)bytes;
+    m.out = static_cast<uint8_t*>(d_out);
+    m.out_size = reinterpret_cast<unsigned long long*>(d_out_size);
+    m.pay_off = w.in_off;
+    assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
+    CK(cudaGetLastError());
+    assemble_copy_kernel<<<(unsigned)nch, 256, 0, s>>>(m);
     CK(cudaGetLastError());
     return FZB_OK;
 }
@@ -355,7 +412,7 @@ int fzb_rze_decode(const void* d_in, uint64_t in_bytes, uint64_t orig_bytes, voi
     const uint64_t nch = (orig_bytes + kChunkBytes - 1) / kChunkBytes;
     if (in_bytes < 8 + 4 * nch) return FZB_E_MALFORMED;
     const uint64_t n_equiv = (orig_bytes + 1) / 2;
-    Work w = carve(d_work, n_equiv);
+    Work w = carve(d_work, n_equiv, 0);
     if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
     cudaStream_t s = S(stream);
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
@@ -388,7 +445,7 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
     if (!d_rze || !d_out || !d_count || (cap && (!d_err || !d_idx))) return FZB_E_INVALID;
     const uint64_t nch = chunks_of(n_total);
     if (rze_bytes < 8 + 4 * nch) return FZB_E_MALFORMED;
-    Work w = carve(d_work, n_total);
+    Work w = carve(d_work, n_total, 0);
     if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
     cudaStream_t s = S(stream);
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));

@@ -146,26 +146,30 @@ __device__ __forceinline__ uint64_t lb_load(const unsigned long long* p) {
     return v;
 }
 
-// Called by warp 0 of the CTA owning `chunk`.  Publishes `agg`, walks back
-// to the nearest inclusive prefix, publishes this chunk's inclusive prefix
-// and returns the exclusive prefix (identical in all lanes).
-__device__ __noinline__ static uint64_t lookback(unsigned long long* st, uint32_t chunk, uint64_t agg,
-                             uint32_t* err) {
-    const int lane = threadIdx.x & 31;
+// Called by all kThreads threads of the CTA owning `chunk`: one round trip
+// inspects 256 predecessors.  Publishes `agg`, walks back to the nearest
+// inclusive prefix, publishes this chunk's inclusive prefix and returns the
+// exclusive prefix (identical in all threads).  `red` needs 2*(kThreads/32)+2
+// u64 of shared memory.
+__device__ __noinline__ static uint64_t lookback(unsigned long long* st, uint32_t chunk,
+                                                 uint64_t agg, uint32_t* err,
+                                                 unsigned long long* red) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    constexpr int W = kThreads / 32;
     if (chunk == 0) {
-        if (lane == 0) lb_store(st, kFlagPre | agg);
+        if (t == 0) lb_store(st, kFlagPre | agg);
         return 0;
     }
-    if (lane == 0) lb_store(st + chunk, kFlagAgg | agg);
+    if (t == 0) lb_store(st + chunk, kFlagAgg | agg);
     uint64_t excl = 0;
     int64_t base = (int64_t)chunk - 1;
     bool timed_out = false;
     while (true) {
-        int64_t idx = base - lane;
-        uint64_t s = kFlagPre;  // lanes before chunk 0 read as an empty prefix
+        const int64_t idx = base - t;
+        uint64_t s = kFlagPre;  // positions before chunk 0 read as an empty prefix
         if (idx >= 0) {
             int spins = 0;
-            do {
+            while (true) {
                 s = lb_load(st + idx);
                 if ((s >> 62) != 0) break;
                 if (++spins > kSpinLimit) {
@@ -173,23 +177,31 @@ __device__ __noinline__ static uint64_t lookback(unsigned long long* st, uint32_
                     s = kFlagPre;
                     break;
                 }
-                __nanosleep(64);
-            } while (true);
+                __nanosleep(32);
+            }
         }
-        uint32_t pre = __ballot_sync(0xffffffffu, (s >> 62) == 2);
-        uint64_t v = s & kValMask;
-        if (pre) {
-            int k = __ffs(pre) - 1;
-            if (lane > k) v = 0;
-        }
+        // nearest inclusive prefix: smallest t whose status carries one
+        const uint32_t pre = __ballot_sync(0xffffffffu, (s >> 62) == 2);
+        if (lane == 0) red[warp] = pre ? (unsigned long long)(warp * 32 + __ffs(pre) - 1) : 1000ull;
+        __syncthreads();
+        unsigned long long tmin = 1000ull;
+#pragma unroll
+        for (int w = 0; w < W; w++) tmin = min(tmin, red[w]);
+        uint64_t v = ((unsigned long long)t <= tmin) ? (s & kValMask) : 0ull;
 #pragma unroll
         for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
-        excl += v;
-        if (pre) break;
-        base -= 32;
+        if (lane == 0) red[W + warp] = v;
+        __syncthreads();
+        uint64_t sum = 0;
+#pragma unroll
+        for (int w = 0; w < W; w++) sum += red[W + w];
+        excl += sum;
+        __syncthreads();
+        if (tmin < 1000ull) break;
+        base -= kThreads;
     }
-    if (__any_sync(0xffffffffu, timed_out) && lane == 0) atomicOr(err, kErrLookbackTimeout);
-    if (lane == 0) lb_store(st + chunk, kFlagPre | ((excl + agg) & kValMask));
+    if (timed_out) atomicOr(err, kErrLookbackTimeout);
+    if (t == 0) lb_store(st + chunk, kFlagPre | ((excl + agg) & kValMask));
     return excl;
 }
 

@@ -3,9 +3,10 @@
 // stream), standalone Bitshuffle and RZE encode.
 //
 // One CTA of 256 threads per 8192-element chunk (= one 16 KiB Bitshuffle
-// block = one RZE chunk).  Chunks are claimed through a ticket counter so the
-// decoupled look-back that places outliers and compressed bytes only waits on
-// chunks that are already running.
+// block = one RZE chunk).  Placement is two-phase so no chunk ever waits on
+// another: each chunk writes its encoded bytes to a fixed slot and its
+// outliers to staging, then assemble_scan/assemble_copy build the ordered
+// stream and outlier list.
 #include "fzb_kernels.cuh"
 
 namespace fzb {
@@ -15,23 +16,58 @@ namespace fzb {
 // device, so REL/NOA need no host round trip.
 // ---------------------------------------------------------------------------
 
+// Grid-stride min/max with four independent 16-byte loads in flight per
+// thread; the last block to finish reduces the partials and resolves
+// abs_eb / ebx2_r into st (lorenzo_quant.cu:612-644).  st layout:
+// [0] value_base, [1] abs_eb, [2] ebx2_r, [3] ebx2.
+__device__ __forceinline__ void resolve_eb_store(float lo, float hi, int mode, float user_eb,
+                                                 float vb, bool have_minmax, float* st) {
+    if (mode != 0 && have_minmax) {
+        if (mode == 2) {
+            vb = __fsub_rn(hi, lo);
+        } else {
+            const float al = lo < 0.0f ? -lo : lo, ah = hi < 0.0f ? -hi : hi;
+            vb = al > ah ? al : ah;
+        }
+    }
+    if (mode == 0) vb = 0.0f;
+    // ABS, or value_base <= 0 -> fall back to ABS
+    const float abs_eb = (mode == 0 || !(vb > 0.0f)) ? user_eb : __fmul_rn(user_eb, vb);
+    st[0] = vb;
+    st[1] = abs_eb;
+    st[2] = __fdiv_rn(1.0f, __fmul_rn(2.0f, abs_eb));
+    st[3] = __fmul_rn(2.0f, abs_eb);
+}
+
 __global__ void __launch_bounds__(256) minmax_kernel(const float* __restrict__ x, uint64_t n,
                                                      float* __restrict__ pmin,
-                                                     float* __restrict__ pmax) {
+                                                     float* __restrict__ pmax,
+                                                     unsigned int* __restrict__ done, int mode,
+                                                     float user_eb, float* __restrict__ st) {
     float lo = INFINITY, hi = -INFINITY;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * 4;
     const bool vec = ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
-    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4; i < n; i += stride) {
-        if (vec && i + 4 <= n) {
-            float4 v = __ldg(reinterpret_cast<const float4*>(x + i));
-            lo = fminf(lo, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
-            hi = fmaxf(hi, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
-        } else {
-            for (uint64_t k = i; k < n && k < i + 4; k++) {
-                lo = fminf(lo, x[k]);
-                hi = fmaxf(hi, x[k]);
-            }
+    const uint64_t nv = vec ? n / 4 : 0;
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < nv; i += 4 * stride) {
+        float4 v[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[k] = __ldg(x4 + i + k * stride);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            lo = fminf(lo, fminf(fminf(v[k].x, v[k].y), fminf(v[k].z, v[k].w)));
+            hi = fmaxf(hi, fmaxf(fmaxf(v[k].x, v[k].y), fmaxf(v[k].z, v[k].w)));
         }
+    }
+    for (; i < nv; i += stride) {
+        const float4 v = __ldg(x4 + i);
+        lo = fminf(lo, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
+        hi = fmaxf(hi, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+    }
+    for (uint64_t k = 4 * nv + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        lo = fminf(lo, x[k]);
+        hi = fmaxf(hi, x[k]);
     }
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) {
@@ -39,6 +75,7 @@ __global__ void __launch_bounds__(256) minmax_kernel(const float* __restrict__ x
         hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, d));
     }
     __shared__ float slo[8], shi[8];
+    __shared__ bool s_last;
     if ((threadIdx.x & 31) == 0) {
         slo[threadIdx.x >> 5] = lo;
         shi[threadIdx.x >> 5] = hi;
@@ -51,43 +88,41 @@ __global__ void __launch_bounds__(256) minmax_kernel(const float* __restrict__ x
         }
         pmin[blockIdx.x] = lo;
         pmax[blockIdx.x] = hi;
+        __threadfence();
+        s_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    lo = INFINITY;
+    hi = -INFINITY;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        lo = fminf(lo, __ldcg(pmin + b));
+        hi = fmaxf(hi, __ldcg(pmax + b));
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        slo[threadIdx.x >> 5] = lo;
+        shi[threadIdx.x >> 5] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; w++) {
+            lo = fminf(lo, slo[w]);
+            hi = fmaxf(hi, shi[w]);
+        }
+        resolve_eb_store(lo, hi, mode, user_eb, 0.0f, true, st);
+        *done = 0;  // ready for the next launch
     }
 }
 
-// EbState layout (device): [0] value_base, [1] abs_eb, [2] ebx2_r, [3] ebx2.
-// nparts == 0: value_base = vb_given (ABS, or a caller-provided base).
-// Launched with one warp.
-__global__ void resolve_eb_kernel(const float* __restrict__ pmin, const float* __restrict__ pmax,
-                                  int nparts, int mode, float user_eb, float vb_given,
-                                  float* __restrict__ st) {
-    float vb = (mode != 0) ? vb_given : 0.0f;
-    float lo = INFINITY, hi = -INFINITY;
-    if (mode != 0 && nparts > 0) {
-        for (int i = threadIdx.x; i < nparts; i += 32) {
-            lo = fminf(lo, pmin[i]);
-            hi = fmaxf(hi, pmax[i]);
-        }
-#pragma unroll
-        for (int d = 16; d >= 1; d >>= 1) {
-            lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, d));
-            hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, d));
-        }
-    }
-    if (threadIdx.x != 0) return;
-    if (mode != 0 && nparts > 0) {
-        if (mode == 2) {
-            vb = __fsub_rn(hi, lo);
-        } else {
-            float al = lo < 0.0f ? -lo : lo, ah = hi < 0.0f ? -hi : hi;
-            vb = al > ah ? al : ah;
-        }
-    }
-    // lorenzo_quant.cu:612-644: ABS, or value_base <= 0 -> fall back to ABS
-    float abs_eb = (mode == 0 || !(vb > 0.0f)) ? user_eb : __fmul_rn(user_eb, vb);
-    st[0] = vb;
-    st[1] = abs_eb;
-    st[2] = __fdiv_rn(1.0f, __fmul_rn(2.0f, abs_eb));
-    st[3] = __fmul_rn(2.0f, abs_eb);
+// Error-bound resolution without a scan (ABS, or a caller-provided base).
+__global__ void resolve_eb_kernel(int mode, float user_eb, float vb_given, float* __restrict__ st) {
+    if (threadIdx.x == 0) resolve_eb_store(0.f, 0.f, mode, user_eb, vb_given, false, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -266,35 +301,119 @@ __device__ __forceinline__ void raw_to_packed(const uint32_t (&rw)[16], uint32_t
     }
 }
 
-// Shared epilogue: look-back for the compressed byte offset, copy out,
-// header words, trailing pad.  `sw` is the chunk's size word.
-__device__ __forceinline__ void rze_place_chunk(uint8_t* __restrict__ out, uint32_t n_chunks,
-                                                uint32_t orig_bytes, uint32_t c, uint32_t sw,
-                                                const uint8_t* payload,
-                                                unsigned long long* st, uint32_t* err,
-                                                unsigned long long* out_size,
-                                                unsigned long long* s_b) {
+// Writes a chunk's encoded bytes (S when stored raw, else O) to its 16 KiB
+// slot and its size word to sizes[c].
+__device__ __forceinline__ void write_slot(uint8_t* __restrict__ slots, uint32_t* __restrict__ sizes,
+                                           uint32_t c, uint32_t sw, const uint8_t* payload) {
     const uint32_t clean = sw & 0x7fffffffu;
-    if (threadIdx.x < 32) {
-        uint64_t ex = lookback(st, c, clean, err);
-        if (threadIdx.x == 0) *s_b = ex;
-    }
-    __syncthreads();
-    const uint64_t boff = *s_b;
-    const uint64_t hdr = 8ull + 4ull * n_chunks;
-    copy_out_bytes(out + hdr + boff, payload, clean);
-    if (threadIdx.x == 0) {
-        reinterpret_cast<uint32_t*>(out + 8)[c] = sw;
-        if (c == 0) {
-            reinterpret_cast<uint32_t*>(out)[0] = orig_bytes;
-            reinterpret_cast<uint32_t*>(out)[1] = n_chunks;
+    uint4* d4 = reinterpret_cast<uint4*>(slots + (size_t)c * kChunkBytes);
+    const uint4* s4 = reinterpret_cast<const uint4*>(payload);
+    for (uint32_t i = threadIdx.x; i < (clean + 15) / 16; i += kThreads) d4[i] = s4[i];
+    if (threadIdx.x == 0) sizes[c] = sw;
+}
+
+// Exclusive scans over chunks (one CTA of 1024 threads): payload offsets,
+// outlier offsets, RZE header, total sizes.
+__global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) {
+    __shared__ unsigned long long sp[1024];
+    __shared__ unsigned int so[1024];
+    const uint32_t n = a.n_chunks, t = threadIdx.x;
+    const uint32_t per = (n + 1023) / 1024;
+    const uint32_t b = t * per, e = min(n, b + per);
+    // outliers that found room in staging (an overflowing run keeps those,
+    // the count still reports every outlier found)
+    auto staged = [&](uint32_t i) -> uint32_t {
+        const uint32_t b0 = a.obase[i], n0 = a.ocnt[i];
+        return b0 >= a.ostage_cap ? 0u : min(n0, a.ostage_cap - b0);
+    };
+    unsigned long long ps = 0;
+    unsigned int os = 0, ot = 0;
+    for (uint32_t i = b; i < e; i++) {
+        if (a.sizes) ps += a.sizes[i] & 0x7fffffffu;
+        if (a.ocnt) {
+            os += staged(i);
+            ot += a.ocnt[i];
         }
     }
-    if (c == n_chunks - 1) {
-        const uint64_t total = hdr + boff + clean;
-        const uint64_t padded = (total + 3) & ~3ull;
-        if (threadIdx.x < padded - total) out[total + threadIdx.x] = 0;
-        if (threadIdx.x == 0) *out_size = padded;
+    sp[t] = ps;
+    so[t] = os;
+    __shared__ unsigned int s_tot;
+    if (t == 0) s_tot = 0;
+    __syncthreads();
+    if (a.ocnt) atomicAdd(&s_tot, ot);
+    for (int d = 1; d < 1024; d <<= 1) {
+        unsigned long long vp = (t >= (unsigned)d) ? sp[t - d] : 0ull;
+        unsigned int vo = (t >= (unsigned)d) ? so[t - d] : 0u;
+        __syncthreads();
+        sp[t] += vp;
+        so[t] += vo;
+        __syncthreads();
+    }
+    unsigned long long rp = sp[t] - ps;
+    unsigned int ro = so[t] - os;
+    uint32_t* hdr = reinterpret_cast<uint32_t*>(a.out);
+    for (uint32_t i = b; i < e; i++) {
+        if (a.sizes) {
+            a.pay_off[i] = rp;
+            rp += a.sizes[i] & 0x7fffffffu;
+            hdr[2 + i] = a.sizes[i];
+        }
+        if (a.ocnt) {
+            a.ofin[i] = ro;
+            ro += staged(i);
+        }
+    }
+    if (t == 1023) {
+        if (a.sizes) {
+            hdr[0] = a.orig_bytes;
+            hdr[1] = n;
+            const unsigned long long total = 8ull + 4ull * n + sp[1023];
+            const unsigned long long padded = (total + 3) & ~3ull;
+            for (unsigned long long i = total; i < padded; i++) a.out[i] = 0;
+            *a.out_size = padded;
+        }
+        if (a.ocnt) *a.out_count = s_tot;
+    }
+}
+
+// One CTA per chunk: payload from its slot to the final stream position
+// (any byte alignment), and its outliers from staging to their sorted
+// position (chunks are index ranges and each chunk's block is sorted).
+__global__ void __launch_bounds__(256) assemble_copy_kernel(AsmArgs a) {
+    const uint32_t c = blockIdx.x;
+    if (a.sizes) {
+        const uint32_t len = a.sizes[c] & 0x7fffffffu;
+        uint8_t* dst = a.out + 8ull + 4ull * a.n_chunks + a.pay_off[c];
+        const uint8_t* src = a.slots + (size_t)c * kChunkBytes;
+        const uint32_t* s32 = reinterpret_cast<const uint32_t*>(src);
+        const uintptr_t d0 = reinterpret_cast<uintptr_t>(dst), d1 = d0 + len;
+        const uintptr_t a0 = (d0 + 3) & ~(uintptr_t)3, a1 = d1 & ~(uintptr_t)3;
+        if (a0 >= a1) {
+            for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) dst[i] = src[i];
+        } else {
+            const uint32_t head = (uint32_t)(a0 - d0), tail = (uint32_t)(d1 - a1);
+            if (threadIdx.x < head) dst[threadIdx.x] = src[threadIdx.x];
+            if (threadIdx.x < tail) dst[(a1 - d0) + threadIdx.x] = src[(a1 - d0) + threadIdx.x];
+            uint32_t* dw = reinterpret_cast<uint32_t*>(a0);
+            const uint32_t nw = (uint32_t)((a1 - a0) >> 2), r = head & 3;
+            for (uint32_t i = threadIdx.x; i < nw; i += blockDim.x) {
+                const uint32_t w0 = (head + 4 * i) >> 2;  // source word of destination word i
+                const uint32_t lo = __ldg(s32 + w0);
+                const uint32_t hi = r ? __ldg(s32 + w0 + 1) : 0u;
+                dw[i] = r ? __funnelshift_r(lo, hi, 8 * r) : lo;
+            }
+        }
+    }
+    if (a.ocnt) {
+        const uint32_t b = a.obase[c], f = a.ofin[c];
+        const uint32_t n = b >= a.ostage_cap ? 0u : min(a.ocnt[c], a.ostage_cap - b);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t s = b + i, d = f + i;
+            if (d < a.cap) {
+                a.out_err[d] = a.ostage_err[s];
+                a.out_idx[d] = a.ostage_idx[s];
+            }
+        }
     }
 }
 
@@ -401,12 +520,9 @@ template <int NDIM, bool FUSED, bool ROWAL>
 __global__ void __launch_bounds__(kThreads, 3) lq_chunk_kernel(FwdArgs a) {
     extern __shared__ float4 Q[];
     __shared__ uint32_t s_ws[16];
-    __shared__ uint32_t s_chunk;
-    __shared__ unsigned long long s_b;
+    __shared__ uint32_t s_obase;
     const int t = threadIdx.x;
-    if (t == 0) s_chunk = atomicAdd(a.ticket, 1u);
-    __syncthreads();
-    const uint32_t c = s_chunk;
+    const uint32_t c = blockIdx.x;
     const uint32_t i0 = c * (uint32_t)kChunkCodes;
     const uint32_t cnt = min((uint32_t)kChunkCodes, a.n_total - i0);
     const float r = *a.ebx2_r;
@@ -477,32 +593,32 @@ __global__ void __launch_bounds__(kThreads, 3) lq_chunk_kernel(FwdArgs a) {
     }
     const uint32_t nout = __popc(om);
 
-    // ---- outliers: block scan + look-back for their global offset ----
+    // ---- outliers: block scan, one staging allocation per chunk ----
     uint32_t ototal;
     const uint32_t ooff = block_excl_scan(nout, s_ws, &ototal);
-    if (t < 32) {
-        uint64_t ex = lookback(a.st_outl, c, ototal, a.err);
-        if (t == 0) s_b = ex;
+    if (t == 0) {
+        const uint32_t b = ototal ? atomicAdd(a.ostage_ctr, ototal) : 0u;
+        a.obase[c] = b;
+        a.ocnt[c] = ototal;
+        s_obase = b;
     }
     __syncthreads();
-    const uint64_t obase = s_b;
-    if (nout) {  // pass 2: recompute this thread's deltas and store outliers
-        uint64_t pos = obase + ooff;
+    if (nout) {  // pass 2: recompute this thread's deltas and stage its outliers
+        uint32_t pos = s_obase + ooff;
         for (int E = 0; E < 32; E++) {
             const uint32_t k = k0 + E;
             if (j0 + E < cnt && k < a.nfield) {
                 const float cc = delta_at<NDIM>(a, Q, R, k);
                 if (!(fabsf(cc) < a.radius)) {
-                    if (pos < a.cap) {
-                        a.out_err[pos] = cc;
-                        a.out_idx[pos] = k;
+                    if (pos < a.ostage_cap) {
+                        a.ostage_err[pos] = cc;
+                        a.ostage_idx[pos] = k;
                     }
                     pos++;
                 }
             }
         }
     }
-    if (c == a.n_chunks - 1 && t == 0) *a.out_count = (uint32_t)((obase + ototal) < 0xffffffffull ? (obase + ototal) : 0xffffffffull);
 
     if (!FUSED) {
         uint32_t rw[16];
@@ -543,9 +659,193 @@ __global__ void __launch_bounds__(kThreads, 3) lq_chunk_kernel(FwdArgs a) {
     }
     __syncthreads();
     const uint32_t sw = rze_encode_chunk(sm, (int)(2 * cnt));
-    rze_place_chunk(a.rze, a.n_chunks, a.codes_bytes, c, sw,
-                    (sw >> 31) ? reinterpret_cast<const uint8_t*>(sm.S) : sm.O, a.st_bytes, a.err,
-                    a.rze_size, &s_b);
+    write_slot(a.slots, a.sizes, c, sw, (sw >> 31) ? reinterpret_cast<const uint8_t*>(sm.S) : sm.O);
+}
+
+// ---------------------------------------------------------------------------
+// Slab-column kernel for 3-D fields whose chunks are R = 8192/nx whole rows
+// (nx a power of two in [32, 1024], ny % R == 0, no padding).  A work unit is
+// one R-row slab across one 8-plane z tile; its chunks are produced plane by
+// plane.  Every element is rounded once (plane z-1's q stays in registers),
+// no halo is read (slab and tile origins have y % 8 == 0 and z % 8 == 0), and
+// plane z+1 is prefetched into registers while plane z is encoded.  Units
+// run last-to-first so the tail of the field, still in L2 after the
+// value-base scan, is consumed first.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int gswz(int g) { return g ^ ((g >> 3) & 7); }
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <bool ZZ>
+__global__ void __launch_bounds__(kThreads, 2) lq3d_slab_kernel(FwdArgs a, uint32_t slabs,
+                                                               uint32_t units) {
+    extern __shared__ float4 smem4[];
+    __shared__ uint32_t s_ws[16];
+    __shared__ uint32_t s_obase;
+    uint8_t* base = reinterpret_cast<uint8_t*>(smem4);
+    float4* A4 = smem4;                       // A plane: 8192 floats, swizzled granules
+    float4* Rw = smem4 + kChunkCodes / 4;     // raw plane prefetch: 8192 floats, swizzled
+    const float* Af = reinterpret_cast<const float*>(smem4);
+    RzeSmem sm;
+    uint8_t* rz = base + 8 * kChunkCodes;
+    sm.S = reinterpret_cast<uint32_t*>(rz);
+    sm.O = rz + kChunkBytes;
+    sm.bm1 = reinterpret_cast<uint32_t*>(rz + 2 * kChunkBytes + 16);
+    sm.bm2 = rz + 2 * kChunkBytes + 16 + 2048;
+    sm.bm3 = reinterpret_cast<uint32_t*>(rz + 2 * kChunkBytes + 16 + 2048 + 256);
+    sm.ws = s_ws;
+
+    const int t = threadIdx.x;
+    const uint32_t nx = a.nx, R = kChunkCodes / nx;
+    const float r = *a.ebx2_r;
+    const uint32_t e0 = 32u * t;             // this thread's 32 elements of the slab plane
+    const uint32_t ty = (e0 / nx) & 7u;      // slab origin has y % 8 == 0
+    const int gup = ((int)e0 - (int)nx) >> 2;
+    auto dswz = [](int m) { const int g = m >> 2; return (gswz(g) << 2) | (m & 3); };
+    auto prefetch = [&](uint32_t z, uint32_t s) {
+        const float4* src = reinterpret_cast<const float4*>(
+            a.in + ((size_t)z * a.ny + (size_t)s * R) * nx + e0);
+#pragma unroll
+        for (int g = 0; g < 8; g++) cp_async16(Rw + gswz(8 * t + g), src + g);
+        cp_async_commit();
+    };
+
+    uint32_t uu = blockIdx.x;
+    if (uu < units) {
+        const uint32_t u = units - 1 - uu;
+        prefetch((u / slabs) * 8, u % slabs);
+    }
+    for (; uu < units; uu += gridDim.x) {
+        const uint32_t u = units - 1 - uu;
+        const uint32_t s = u % slabs, zt = u / slabs;
+        const uint32_t z0 = zt * 8, z1 = min(z0 + 8, a.nz);
+        float qprev[32];
+        for (uint32_t z = z0; z < z1; z++) {
+            const uint32_t c = z * slabs + s;
+            const bool tz = (z != z0);
+            cp_async_wait_all();
+            float4 cur[8];
+#pragma unroll
+            for (int g = 0; g < 8; g++) cur[g] = Rw[gswz(8 * t + g)];
+            // each thread refills only its own granules, so no barrier is needed
+            if (z + 1 < z1) prefetch(z + 1, s);
+            else if (uu + gridDim.x < units) {
+                const uint32_t un = units - 1 - (uu + gridDim.x);
+                prefetch((un / slabs) * 8, un % slabs);
+            }
+            // A = q(z) - q(z-1): the z difference first (lorenzo_quant_nd.cu:236)
+#pragma unroll
+            for (int g = 0; g < 8; g++) {
+                float v[4] = {cur[g].x, cur[g].y, cur[g].z, cur[g].w};
+                float w[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int e = 4 * g + k;
+                    const float q = q_of(v[k], r);
+                    w[k] = tz ? __fsub_rn(q, qprev[e]) : q;
+                    qprev[e] = q;
+                }
+                A4[gswz(8 * t + g)] = make_float4(w[0], w[1], w[2], w[3]);
+            }
+            __syncthreads();
+            // x then y differences (lorenzo_quant_nd.cu:239-246), quantize
+            uint32_t x[16];
+            uint32_t om = 0;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                float av[16], up[16];
+#pragma unroll
+                for (int g = 0; g < 4; g++) {
+                    const float4 w = A4[gswz(8 * t + 4 * h + g)];
+                    av[4 * g] = w.x; av[4 * g + 1] = w.y; av[4 * g + 2] = w.z; av[4 * g + 3] = w.w;
+                    if (ty) {
+                        const float4 q = A4[gswz(gup + 4 * h + g)];
+                        up[4 * g] = q.x; up[4 * g + 1] = q.y; up[4 * g + 2] = q.z; up[4 * g + 3] = q.w;
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const int e = 16 * h + k;
+                    float cc;
+                    const float b0 = (e & 7) ? __fsub_rn(av[k], av[k - 1]) : av[k];
+                    if (ty) {
+                        const float b1 = (e & 7) ? __fsub_rn(up[k], up[k - 1]) : up[k];
+                        cc = __fsub_rn(b0, b1);
+                    } else {
+                        cc = b0;
+                    }
+                    const bool qz = fabsf(cc) < a.radius;
+                    const uint32_t code = qz ? code_of<ZZ>(cc) : 0u;
+                    om |= (qz ? 0u : 1u) << e;
+                    if (h == 0) x[k] = code;
+                    else x[k] = __byte_perm(x[k], code, 0x5410);
+                }
+            }
+            // outliers: one staging allocation per chunk; values recomputed
+            // from the staged A plane (rare path)
+            const uint32_t nout = __popc(om);
+            uint32_t ototal;
+            const uint32_t ooff = block_excl_scan(nout, s_ws, &ototal);
+            if (t == 0) {
+                const uint32_t b = ototal ? atomicAdd(a.ostage_ctr, ototal) : 0u;
+                a.obase[c] = b;
+                a.ocnt[c] = ototal;
+                s_obase = b;
+            }
+            __syncthreads();
+            if (nout) {
+                uint32_t pos = s_obase + ooff;
+                const uint32_t kbase = c * (uint32_t)kChunkCodes + e0;
+                for (int e = 0; e < 32; e++) {
+                    if (!((om >> e) & 1u)) continue;
+                    const int m = (int)e0 + e;
+                    const float a0 = Af[dswz(m)];
+                    const float b0 = (e & 7) ? __fsub_rn(a0, Af[dswz(m - 1)]) : a0;
+                    float cc = b0;
+                    if (ty) {
+                        const float u0 = Af[dswz(m - (int)nx)];
+                        const float b1 = (e & 7) ? __fsub_rn(u0, Af[dswz(m - (int)nx - 1)]) : u0;
+                        cc = __fsub_rn(b0, b1);
+                    }
+                    if (pos < a.ostage_cap) {
+                        a.ostage_err[pos] = cc;
+                        a.ostage_idx[pos] = kbase + e;
+                    }
+                    pos++;
+                }
+            }
+            // Bitshuffle (full chunk) and RZE
+            transpose16x2(x);
+#pragma unroll
+            for (int b = 0; b < 16; b++) sm.S[(15 - b) * 256 + t] = x[b];
+            __syncthreads();
+            const uint32_t sw = rze_encode_chunk(sm, kChunkBytes);
+            write_slot(a.slots, a.sizes, c, sw, (sw >> 31) ? reinterpret_cast<const uint8_t*>(sm.S) : sm.O);
+            __syncthreads();
+        }
+    }
+    cp_async_wait_all();
+}
+
+int launch_lq3d_slab(const FwdArgs& a, unsigned grid, cudaStream_t s) {
+    const size_t smem = 8 * kChunkCodes + 2 * kChunkBytes + 16 + 2048 + 256 + 32;
+    const uint32_t slabs = a.ny / (kChunkCodes / a.nx), units = slabs * ((a.nz + 7) / 8);
+    cudaError_t e;
+    if (a.zigzag) {
+        e = cudaFuncSetAttribute(lq3d_slab_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        lq3d_slab_kernel<true><<<grid, kThreads, smem, s>>>(a, slabs, units);
+    } else {
+        e = cudaFuncSetAttribute(lq3d_slab_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        lq3d_slab_kernel<false><<<grid, kThreads, smem, s>>>(a, slabs, units);
+    }
+    return (int)cudaGetLastError();
 }
 
 template <int NDIM, bool FUSED, bool ROWAL>
@@ -644,12 +944,8 @@ __global__ void bitshuffle_ballot_kernel(const uint8_t* __restrict__ in, uint8_t
 __global__ void __launch_bounds__(kThreads) rze_encode_kernel(RzeEncArgs a) {
     extern __shared__ float4 Q[];
     __shared__ uint32_t s_ws[16];
-    __shared__ uint32_t s_chunk;
-    __shared__ unsigned long long s_b;
     const int t = threadIdx.x;
-    if (t == 0) s_chunk = atomicAdd(a.ticket, 1u);
-    __syncthreads();
-    const uint32_t c = s_chunk;
+    const uint32_t c = blockIdx.x;
     const uint64_t off = (uint64_t)c * kChunkBytes;
     const int in_size = (int)min((uint64_t)kChunkBytes, a.bytes - off);
     uint8_t* base = reinterpret_cast<uint8_t*>(Q);
@@ -671,9 +967,7 @@ __global__ void __launch_bounds__(kThreads) rze_encode_kernel(RzeEncArgs a) {
     }
     __syncthreads();
     const uint32_t sw = rze_encode_chunk(sm, in_size);
-    rze_place_chunk(a.out, a.n_chunks, (uint32_t)a.bytes, c, sw,
-                    (sw >> 31) ? reinterpret_cast<const uint8_t*>(sm.S) : sm.O, a.st_bytes, a.err,
-                    a.out_size, &s_b);
+    write_slot(a.slots, a.sizes, c, sw, (sw >> 31) ? reinterpret_cast<const uint8_t*>(sm.S) : sm.O);
 }
 
 }  // namespace fzb

@@ -21,25 +21,47 @@ struct FwdArgs {
     uint32_t* out_idx;
     uint32_t cap;
     uint32_t* out_count;
-    uint8_t* rze;          // fused output stream
     uint32_t n_chunks;
-    uint32_t codes_bytes;
-    unsigned long long* rze_size;
-    unsigned long long* st_outl;
-    unsigned long long* st_bytes;
-    uint32_t* ticket;
+    // two-phase placement: chunk payloads go to fixed 16 KiB slots and
+    // outliers to an atomically allocated staging area; assemble_* kernels
+    // then write the final, ordered outputs
+    uint8_t* slots;        // n_chunks * 16 KiB (+16)
+    uint32_t* sizes;       // per-chunk RZE size words
+    uint32_t* ocnt;        // per-chunk outlier counts
+    uint32_t* obase;       // per-chunk staging offsets
+    uint32_t* ostage_ctr;
+    float* ostage_err;
+    uint32_t* ostage_idx;
+    uint32_t ostage_cap;
     uint32_t* err;
+};
+
+// Final placement of slot payloads and staged outliers.
+struct AsmArgs {
+    const uint8_t* slots;
+    const uint32_t* sizes;   // null: outliers only
+    uint32_t n_chunks;
+    uint32_t orig_bytes;
+    uint8_t* out;            // RZE stream
+    unsigned long long* out_size;
+    unsigned long long* pay_off;  // n_chunks (scratch)
+    const uint32_t* ocnt;
+    const uint32_t* obase;
+    uint32_t* ofin;          // n_chunks (scratch)
+    const float* ostage_err;
+    const uint32_t* ostage_idx;
+    uint32_t ostage_cap;
+    float* out_err;
+    uint32_t* out_idx;
+    uint32_t cap;
+    uint32_t* out_count;
 };
 
 struct RzeEncArgs {
     const uint8_t* in;
     uint64_t bytes;
-    uint8_t* out;
-    uint32_t n_chunks;
-    unsigned long long* out_size;
-    unsigned long long* st_bytes;
-    uint32_t* ticket;
-    uint32_t* err;
+    uint8_t* slots;
+    uint32_t* sizes;
 };
 
 // Inverse-side arguments.
@@ -64,17 +86,21 @@ struct InvArgs {
     uint32_t* err;
 };
 
-__global__ void minmax_kernel(const float* x, uint64_t n, float* pmin, float* pmax);
-__global__ void resolve_eb_kernel(const float* pmin, const float* pmax, int nparts, int mode,
-                                  float user_eb, float vb_given, float* st);
+__global__ void minmax_kernel(const float* x, uint64_t n, float* pmin, float* pmax,
+                              unsigned int* done, int mode, float user_eb, float* st);
+__global__ void resolve_eb_kernel(int mode, float user_eb, float vb_given, float* st);
 // Launches the chunk kernel instance for (ndim, fused, row-aligned); returns
 // a cudaError_t value.
 int launch_lq_chunk(int ndim, bool fused, bool rowal, const FwdArgs& a, size_t smem,
                     unsigned grid, cudaStream_t s);
+// Slab-column fused 3-D kernel (see fzb_forward.cu); `grid` persistent CTAs.
+int launch_lq3d_slab(const FwdArgs& a, unsigned grid, cudaStream_t s);
 __global__ void bitshuffle2_kernel(const uint8_t* in, uint8_t* out, int inverse);
 __global__ void bitshuffle_ballot_kernel(const uint8_t* in, uint8_t* out, uint32_t block, int ew,
                                          int inverse);
 __global__ void rze_encode_kernel(RzeEncArgs a);
+__global__ void assemble_scan_kernel(AsmArgs a);
+__global__ void assemble_copy_kernel(AsmArgs a);
 
 __global__ void rze_prepass_kernel(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect,
                                    uint32_t orig_expect, unsigned long long* in_off, uint32_t* err);

@@ -38,8 +38,8 @@ class Workspace:
     def __init__(self):
         self.buf: torch.Tensor | None = None
 
-    def get(self, n_total: int, device) -> tuple[C.c_void_p, int]:
-        need = int(lib().fzb_workspace_bytes(int(n_total)))
+    def get(self, n_total: int, device, cap: int = 0) -> tuple[C.c_void_p, int]:
+        need = int(lib().fzb_workspace_bytes(int(n_total), int(cap)))
         if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
             self.buf = torch.empty(need, dtype=torch.uint8, device=device)
         return _ptr(self.buf), self.buf.numel()
@@ -71,7 +71,7 @@ def lq_forward(x: torch.Tensor, dims, eb: float, mode: int = ABS, radius: int = 
     idx = torch.empty(max(cap, 1), dtype=torch.int32, device=dev)
     count = torch.zeros(1, dtype=torch.int32, device=dev)
     eb_state = torch.zeros(4, dtype=torch.float32, device=dev)
-    wp, wn = ws.get(n, dev)
+    wp, wn = ws.get(n, dev, cap)
     check(lib().fzb_lq_forward(_ptr(x), n, _dims(dims), eb, mode, value_base, radius, int(zigzag),
                                _ptr(codes), _ptr(err), _ptr(idx), cap, _ptr(count), _ptr(eb_state),
                                wp, wn, _stream(dev)), "fzb_lq_forward")
@@ -144,7 +144,7 @@ def lq_bs_rze_compress(x: torch.Tensor, dims, eb: float, mode: int = ABS, radius
             count=torch.zeros(1, dtype=torch.int32, device=dev),
             eb_state=torch.zeros(4, dtype=torch.float32, device=dev),
             cap=cap)
-    wp, wn = ws.get(n, dev)
+    wp, wn = ws.get(n, dev, cap)
     check(lib().fzb_lq_bs_rze_compress(
         _ptr(x), n, _dims(dims), eb, mode, value_base, radius, int(zigzag), _ptr(out["err"]),
         _ptr(out["idx"]), cap, _ptr(out["count"]), _ptr(out["rze"]), _ptr(out["rze_size"]),

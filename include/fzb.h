@@ -42,8 +42,9 @@ int fzb_version(void);
 const char* fzb_status_string(int status);
 
 /* Workspace for any entry point over n_total Lorenzo elements (or
- * 2*n_total bytes for the byte-stream coders). */
-size_t fzb_workspace_bytes(uint64_t n_total);
+ * 2*n_total bytes for the byte-stream coders) with room to stage up to
+ * `cap` outliers (the forward entry points' outlier capacity; 0 otherwise). */
+size_t fzb_workspace_bytes(uint64_t n_total, uint64_t cap);
 
 /* Synchronises `stream` and returns the status latched in the workspace
  * (FZB_OK, FZB_E_MALFORMED or FZB_E_TIMEOUT), then clears it. */
@@ -59,7 +60,9 @@ int fzb_workspace_status(void* d_work, void* stream);
  * dims = {nx, ny, nz} (x fastest); ndim follows LorenzoQuantStage::ndim().
  * value_base > 0 skips the REL/NOA scan (setValueBase).  Outliers are
  * written sorted by index; *d_count receives the total found (may exceed
- * cap; only cap are stored). */
+ * cap; only cap are stored, and on such an overflow which ones are kept
+ * depends on execution order, as in the reference).  The workspace must be
+ * sized with fzb_workspace_bytes(n_total, cap). */
 int fzb_lq_forward(const float* d_in, uint64_t n_total, const uint32_t dims[3],
                    float eb, int eb_mode, float value_base, uint32_t radius, int zigzag,
                    uint16_t* d_codes, float* d_err, uint32_t* d_idx, uint64_t cap,

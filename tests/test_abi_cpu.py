@@ -18,7 +18,7 @@ def test_host_only_queries():
     assert L.fzb_version() >= 100
     assert L.fzb_status_string(0) == b"ok"
     assert b"workspace" in L.fzb_status_string(-3)
-    a, b = L.fzb_workspace_bytes(1 << 20), L.fzb_workspace_bytes(1 << 27)
+    a, b = L.fzb_workspace_bytes(1 << 20, 0), L.fzb_workspace_bytes(1 << 27, 1 << 20)
     assert 0 < a < b
     # header + per-chunk sizes + payload bound + pad
     assert L.fzb_rze_max_bytes(16384) == 8 + 4 + 16384 + 4
