@@ -89,6 +89,21 @@ uint64_t fzb_rze_max_bytes(uint64_t bytes);
 int fzb_rze_encode(const void* d_in, uint64_t bytes, void* d_out, uint64_t* d_out_size,
                    void* d_work, size_t work_bytes, void* stream);
 
+/* RZE encode for callers that cannot allocate device memory (a plugin behind
+ * a fixed-signature filter interface that only receives its input and
+ * output buffers, work issued inside a stream capture that must not
+ * allocate, a host callback barred from allocation calls).  No counterpart
+ * in the reference: same output bytes as fzb_rze_encode, but its scratch is
+ * one static device array of fixed size, resident on every device that uses
+ * it until the process exits.  Inputs above FZB_RZE_NOALLOC_MAX_BYTES are
+ * rejected with FZB_E_CAPACITY.  All calls on a device share that array, so
+ * calls whose GPU work overlaps race and must be serialised.  The first call
+ * on each device resolves the array's address; make it before any stream
+ * capture.  Allocates nothing; d_out must hold fzb_rze_max_bytes(bytes). */
+#define FZB_RZE_NOALLOC_MAX_BYTES (8ull << 20)
+int fzb_rze_encode_noalloc(const void* d_in, uint64_t bytes, void* d_out, uint64_t* d_out_size,
+                           void* stream);
+
 /* RZEStage::execute inverse (rze_stage.cu:846-994) without host round
  * trips: orig_bytes is the size recorded at compression (RZE header
  * cached_orig_bytes, rze_stage.h:175-184). */
