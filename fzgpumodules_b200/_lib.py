@@ -62,6 +62,18 @@ def lib():
         L.fzb_lq_bs_rze_compress.argtypes = [p, u64, p, f32, i32, f32, u32, i32, p, p, u64, p, p, p, p, p, sz, p]
         L.fzb_lq_bs_rze_decompress.restype = i32
         L.fzb_lq_bs_rze_decompress.argtypes = [p, u64, p, p, p, u64, u64, p, f32, i32, p, C.c_uint, p, sz, p]
+        L.fzb_rle_max_bytes.restype = u64
+        L.fzb_rle_max_bytes.argtypes = [u64, i32]
+        L.fzb_rle_encode.restype = i32
+        L.fzb_rle_encode.argtypes = [p, u64, i32, p, p, p, sz, p]
+        L.fzb_rle_decode.restype = i32
+        L.fzb_rle_decode.argtypes = [p, u64, i32, p, p, sz, p]
+        L.fzb_bitpack_encode.restype = i32
+        L.fzb_bitpack_encode.argtypes = [p, u64, i32, i32, p, p, p, p, sz, p]
+        L.fzb_bitpack_decode.restype = i32
+        L.fzb_bitpack_decode.argtypes = [p, u64, i32, i32, p, p]
+        L.fzb_rze_encode_noalloc.restype = i32
+        L.fzb_rze_encode_noalloc.argtypes = [p, u64, p, p, p]
         _lib = L
     return _lib
 

@@ -32,6 +32,11 @@ struct Work {
     float* ostage_err;
     uint32_t* ostage_idx;
     uint64_t ostage_cap;
+    uint32_t* big;      // n_total u32 (RLE run starts / offsets)
+    uint32_t* tiles;    // per-4096-element tile scratch
+    uint32_t* total;    // device scalar
+    unsigned int* done; // last-block counter
+    uint8_t* nbits;     // device byte
     size_t need;
 };
 
@@ -64,6 +69,11 @@ Work carve(void* base, uint64_t n_total, uint64_t cap) {
     w.ostage_cap = cap;
     w.ostage_err = reinterpret_cast<float*>(take(4 * (cap + 1)));
     w.ostage_idx = reinterpret_cast<uint32_t*>(take(4 * (cap + 1)));
+    w.big = reinterpret_cast<uint32_t*>(take(4 * (n_total + 64)));
+    w.tiles = reinterpret_cast<uint32_t*>(take(4 * (n_total / 4096 + 64)));
+    w.total = reinterpret_cast<uint32_t*>(ctrl ? ctrl + 12 : nullptr);
+    w.done = reinterpret_cast<unsigned int*>(ctrl ? ctrl + 16 : nullptr);
+    w.nbits = ctrl ? ctrl + 20 : nullptr;
     w.need = off;
     return w;
 }
@@ -501,6 +511,57 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
     uint32_t bits = 0;
     rc = read_status(w, s, &bits);
     return rc ? rc : status_of(bits);
+}
+
+uint64_t fzb_rle_max_bytes(uint64_t n, int elem) {
+    return 4 + ((n * (uint64_t)elem + 3) & ~3ull) + 4 * n;
+}
+
+int fzb_rle_encode(const void* d_in, uint64_t n, int elem, void* d_out, uint64_t* d_out_size,
+                   void* d_work, size_t work_bytes, void* stream) {
+    if (!d_in || !d_out || !d_out_size || (elem != 1 && elem != 2 && elem != 4)) return FZB_E_INVALID;
+    if (n == 0 || n >= (1ull << 31)) return FZB_E_INVALID;
+    Work w = carve(d_work, n, 0);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
+    return launch_rle_encode(d_in, (uint32_t)n, elem, static_cast<uint8_t*>(d_out),
+                             reinterpret_cast<unsigned long long*>(d_out_size), w.tiles, w.big,
+                             w.total, s) == 0 ? FZB_OK : FZB_E_CUDA;
+}
+
+int fzb_rle_decode(const void* d_in, uint64_t n, int elem, void* d_out, void* d_work,
+                   size_t work_bytes, void* stream) {
+    if (!d_in || !d_out || (elem != 1 && elem != 2 && elem != 4)) return FZB_E_INVALID;
+    if (n == 0 || n >= (1ull << 31)) return FZB_E_INVALID;
+    Work w = carve(d_work, n, 0);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
+    return launch_rle_decode(static_cast<const uint8_t*>(d_in), (uint32_t)n, elem, d_out, w.big,
+                             w.tiles, w.total, w.err, s) == 0 ? FZB_OK : FZB_E_CUDA;
+}
+
+int fzb_bitpack_encode(const void* d_in, uint64_t n, int elem, int nbits, void* d_out,
+                       uint8_t* d_nbits, uint64_t* d_out_size, void* d_work, size_t work_bytes,
+                       void* stream) {
+    if (!d_in || !d_out || (elem != 1 && elem != 2 && elem != 4) || n == 0) return FZB_E_INVALID;
+    if (nbits < 0 || nbits > 8 * elem || (nbits & (nbits - 1)) != 0) return FZB_E_INVALID;
+    Work w = carve(d_work, 1, 0);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
+    uint8_t* nb = d_nbits ? d_nbits : w.nbits;
+    return launch_bitpack_encode(d_in, n, elem, nbits, nb, static_cast<uint8_t*>(d_out),
+                                 reinterpret_cast<unsigned long long*>(d_out_size),
+                                 reinterpret_cast<uint32_t*>(w.pmin), w.done, s) == 0 ? FZB_OK : FZB_E_CUDA;
+}
+
+int fzb_bitpack_decode(const void* d_in, uint64_t n, int elem, int nbits, void* d_out, void* stream) {
+    if (!d_in || !d_out || (elem != 1 && elem != 2 && elem != 4) || n == 0) return FZB_E_INVALID;
+    if (nbits <= 0 || nbits > 8 * elem || (nbits & (nbits - 1)) != 0) return FZB_E_INVALID;
+    return launch_bitpack_decode(static_cast<const uint8_t*>(d_in), n, elem, nbits, d_out, S(stream)) == 0
+               ? FZB_OK : FZB_E_CUDA;
 }
 
 }  // extern "C"

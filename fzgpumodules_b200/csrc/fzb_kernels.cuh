@@ -114,4 +114,14 @@ __global__ void lq_inverse_2d_kernel(InvArgs a);
 __global__ void lq_inverse_3d_kernel(InvArgs a);
 __global__ void fused_inverse_3d_kernel(InvArgs a);
 
+// RLE and Bitpack (fzb_coders.cu); return cudaError_t values.
+int launch_rle_encode(const void* in, uint32_t n, int elem, uint8_t* out, unsigned long long* out_size,
+                      uint32_t* tcnt, uint32_t* starts, uint32_t* runs_total, cudaStream_t s);
+int launch_rle_decode(const uint8_t* in, uint32_t n, int elem, void* out, uint32_t* offs,
+                      uint32_t* tile_scratch, uint32_t* total, uint32_t* err, cudaStream_t s);
+int launch_bitpack_encode(const void* in, uint64_t n, int elem, int nbits, uint8_t* nbits_dev,
+                          uint8_t* out, unsigned long long* out_size, uint32_t* pmax,
+                          unsigned int* done, cudaStream_t s);
+int launch_bitpack_decode(const uint8_t* in, uint64_t n, int elem, int nbits, void* out, cudaStream_t s);
+
 }  // namespace fzb

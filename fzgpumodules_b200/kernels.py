@@ -164,3 +164,57 @@ def lq_bs_rze_decompress(rze: torch.Tensor, rze_bytes: int, err, idx, count, cap
         _ptr(rze), rze_bytes, _ptr(err), _ptr(idx), _ptr(count), cap, n, _dims(dims), abs_eb,
         int(zigzag), _ptr(out), flags, wp, wn, _stream(dev)), "fzb_lq_bs_rze_decompress")
     return out
+
+
+def _elem(t: torch.Tensor) -> int:
+    return t.element_size()
+
+
+def rle_encode(data: torch.Tensor, ws: Workspace | None = None, trim: bool = True):
+    """RLEStage<T> forward (rle.cu:261-384).  Returns (stream, size_tensor)."""
+    ws = ws or _default_ws
+    src = data.reshape(-1)
+    n, e = src.numel(), _elem(src)
+    out = torch.empty(int(lib().fzb_rle_max_bytes(n, e)), dtype=torch.uint8, device=src.device)
+    size = torch.zeros(1, dtype=torch.int64, device=src.device)
+    wp, wn = ws.get(n, src.device)
+    check(lib().fzb_rle_encode(_ptr(src), n, e, _ptr(out), _ptr(size), wp, wn, _stream(src.device)),
+          "fzb_rle_encode")
+    if trim:
+        return out[: int(size.item())], size
+    return out, size
+
+
+def rle_decode(stream: torch.Tensor, n: int, dtype=torch.uint16, ws: Workspace | None = None,
+               out: torch.Tensor | None = None):
+    """RLEStage<T> inverse (rle.cu:196-259)."""
+    ws = ws or _default_ws
+    src = stream.view(torch.uint8).reshape(-1)
+    if out is None:
+        out = torch.empty(n, dtype=dtype, device=src.device)
+    wp, wn = ws.get(n, src.device)
+    check(lib().fzb_rle_decode(_ptr(src), n, _elem(out), _ptr(out), wp, wn, _stream(src.device)),
+          "fzb_rle_decode")
+    return out
+
+
+def bitpack_encode(data: torch.Tensor, nbits: int = 0, ws: Workspace | None = None):
+    """BitpackStage<T> forward (bitpack_stage.cu:169-244).  nbits 0 = detect.
+    Returns (packed bytes, nbits used)."""
+    ws = ws or _default_ws
+    src = data.reshape(-1)
+    n, e = src.numel(), _elem(src)
+    out = torch.empty(n * e, dtype=torch.uint8, device=src.device)
+    nb = torch.zeros(1, dtype=torch.uint8, device=src.device)
+    size = torch.zeros(1, dtype=torch.int64, device=src.device)
+    wp, wn = ws.get(1, src.device)
+    check(lib().fzb_bitpack_encode(_ptr(src), n, e, nbits, _ptr(out), _ptr(nb), _ptr(size), wp, wn,
+                                   _stream(src.device)), "fzb_bitpack_encode")
+    return out[: int(size.item())], int(nb.item())
+
+
+def bitpack_decode(packed: torch.Tensor, n: int, nbits: int, dtype=torch.uint16):
+    out = torch.empty(n, dtype=dtype, device=packed.device)
+    check(lib().fzb_bitpack_decode(_ptr(packed), n, _elem(out), nbits, _ptr(out),
+                                   _stream(packed.device)), "fzb_bitpack_decode")
+    return out

@@ -132,6 +132,29 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
                              float* d_out, unsigned flags,
                              void* d_work, size_t work_bytes, void* stream);
 
+/* RLEStage<T>::execute forward (modules/coders/rle/rle.cu:261-384), element
+ * width elem = 1, 2 or 4 bytes.  Wire format [u32 runs][values, padded to 4
+ * bytes with zeros][u32 lengths] (rle.h:22).  d_out must hold
+ * fzb_rle_max_bytes(n, elem); *d_out_size (device u64) receives the size. */
+uint64_t fzb_rle_max_bytes(uint64_t n, int elem);
+int fzb_rle_encode(const void* d_in, uint64_t n, int elem, void* d_out, uint64_t* d_out_size,
+                   void* d_work, size_t work_bytes, void* stream);
+
+/* RLEStage<T> inverse (rle.cu:196-259) into n elements (the element count the
+ * stage header records, rle.h:123-131).  Run lengths that do not add up to n
+ * are reported as FZB_E_MALFORMED by fzb_workspace_status(). */
+int fzb_rle_decode(const void* d_in, uint64_t n, int elem, void* d_out, void* d_work,
+                   size_t work_bytes, void* stream);
+
+/* BitpackStage<T>::execute (modules/coders/bitpack/bitpack_stage.cu:169-244):
+ * nbits a power of two <= 8*elem, or 0 to detect it from the maximum
+ * (setAutoDetect, :118-124); the nbits used is written to *d_nbits (device
+ * byte, optional) and the packed size to *d_out_size (device u64, optional). */
+int fzb_bitpack_encode(const void* d_in, uint64_t n, int elem, int nbits, void* d_out,
+                       uint8_t* d_nbits, uint64_t* d_out_size, void* d_work, size_t work_bytes,
+                       void* stream);
+int fzb_bitpack_decode(const void* d_in, uint64_t n, int elem, int nbits, void* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
