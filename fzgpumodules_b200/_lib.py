@@ -72,6 +72,20 @@ def lib():
         L.fzb_bitpack_encode.argtypes = [p, u64, i32, i32, p, p, p, p, sz, p]
         L.fzb_bitpack_decode.restype = i32
         L.fzb_bitpack_decode.argtypes = [p, u64, i32, i32, p, p]
+        L.fzb_huff_workspace_bytes.restype = sz
+        L.fzb_huff_workspace_bytes.argtypes = [u64, u32]
+        L.fzb_huff_max_bytes.restype = u64
+        L.fzb_huff_max_bytes.argtypes = [u64, u32]
+        L.fzb_huff_histogram.restype = i32
+        L.fzb_huff_histogram.argtypes = [p, u64, u32, p, p]
+        L.fzb_huff_book.restype = i32
+        L.fzb_huff_book.argtypes = [p, u32, p, p]
+        L.fzb_huff_encode.restype = i32
+        L.fzb_huff_encode.argtypes = [p, u64, u32, p, p, p, p, p, sz, p]
+        L.fzb_huff_compress.restype = i32
+        L.fzb_huff_compress.argtypes = [p, u64, u32, p, p, p, sz, p]
+        L.fzb_huff_decode.restype = i32
+        L.fzb_huff_decode.argtypes = [p, u64, u64, u32, p, p, sz, p]
         L.fzb_rze_encode_noalloc.restype = i32
         L.fzb_rze_encode_noalloc.argtypes = [p, u64, p, p, p]
         _lib = L

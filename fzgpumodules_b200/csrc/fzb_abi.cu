@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "../../include/fzb.h"
 #include "fzb_kernels.cuh"
@@ -294,6 +295,7 @@ const char* fzb_status_string(int st) {
         case FZB_E_CAPACITY: return "output buffer too small";
         case FZB_E_MALFORMED: return "malformed compressed input";
         case FZB_E_TIMEOUT: return "device wait timed out";
+        case FZB_E_RANGE: return "input symbol outside [0, bklen)";
         default: return "unknown status";
     }
 }
@@ -561,6 +563,145 @@ int fzb_bitpack_decode(const void* d_in, uint64_t n, int elem, int nbits, void* 
     if (!d_in || !d_out || (elem != 1 && elem != 2 && elem != 4) || n == 0) return FZB_E_INVALID;
     if (nbits <= 0 || nbits > 8 * elem || (nbits & (nbits - 1)) != 0) return FZB_E_INVALID;
     return launch_bitpack_decode(static_cast<const uint8_t*>(d_in), n, elem, nbits, d_out, S(stream)) == 0
+               ? FZB_OK : FZB_E_CUDA;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// PHF Huffman (HuffmanStage<uint16_t>, coarse mode).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct HfWork {
+    uint32_t* err;
+    uint32_t* ncell_total;
+    uint32_t* freq;
+    uint32_t* bk4;
+    uint8_t* revbook;
+    uint32_t* par_nbit;
+    uint32_t* par_ncell;
+    uint32_t* par_entry;
+    uint32_t* tiles;
+    uint32_t* slots;
+    size_t need;
+};
+
+inline uint64_t hf_pardeg(uint64_t n) { return (n - 1) / kHfSublen + 1; }
+inline size_t hf_revbook_bytes(uint32_t bklen) { return 256 + 2 * (size_t)bklen; }
+
+// ctrl first, so fzb_workspace_status reads the same error word
+HfWork carve_hf(void* base, uint64_t n, uint32_t bklen) {
+    HfWork w{};
+    const uint64_t pd = hf_pardeg(n);
+    uint8_t* p = static_cast<uint8_t*>(base);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        uint8_t* q = p ? p + off : nullptr;
+        off += align256(bytes);
+        return q;
+    };
+    uint8_t* ctrl = take(kCtrlBytes);
+    w.err = reinterpret_cast<uint32_t*>(ctrl);
+    w.ncell_total = reinterpret_cast<uint32_t*>(ctrl ? ctrl + 4 : nullptr);
+    w.freq = reinterpret_cast<uint32_t*>(take(4 * (size_t)bklen));
+    w.bk4 = reinterpret_cast<uint32_t*>(take(4 * (size_t)bklen));
+    w.revbook = take(hf_revbook_bytes(bklen));
+    w.par_nbit = reinterpret_cast<uint32_t*>(take(4 * pd));
+    w.par_ncell = reinterpret_cast<uint32_t*>(take(4 * pd));
+    w.par_entry = reinterpret_cast<uint32_t*>(take(4 * pd));
+    w.tiles = reinterpret_cast<uint32_t*>(take(4 * (pd / 4096 + 64)));
+    w.slots = reinterpret_cast<uint32_t*>(take(4 * pd * kHfSublen));
+    w.need = off;
+    return w;
+}
+
+inline bool hf_args_ok(uint64_t n, uint32_t bklen) {
+    return n > 0 && n < (1ull << 31) && bklen >= 1 && bklen <= 65535;
+}
+
+inline int sm_count() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t fzb_huff_workspace_bytes(uint64_t n, uint32_t bklen) {
+    if (!hf_args_ok(n, bklen)) return 0;
+    return carve_hf(nullptr, n, bklen).need;
+}
+
+uint64_t fzb_huff_max_bytes(uint64_t n, uint32_t bklen) {
+    if (!hf_args_ok(n, bklen)) return 0;
+    const uint64_t pd = hf_pardeg(n);
+    return 128 + hf_revbook_bytes(bklen) + 8 * pd + 4 * (n + pd) + 16;
+}
+
+int fzb_huff_histogram(const uint16_t* d_in, uint64_t n, uint32_t bklen, uint32_t* d_freq,
+                       void* stream) {
+    if (!d_in || !d_freq || !hf_args_ok(n, bklen)) return FZB_E_INVALID;
+    return launch_hf_histogram(d_in, n, bklen, d_freq, sm_count(), S(stream)) == 0 ? FZB_OK : FZB_E_CUDA;
+}
+
+int fzb_huff_book(const uint32_t* h_freq, uint32_t bklen, uint32_t* h_bk4, uint8_t* h_revbook) {
+    if (!h_freq || !h_bk4 || !h_revbook || bklen < 1 || bklen > 65535) return FZB_E_INVALID;
+    return build_huffman_book(h_freq, bklen, h_bk4, h_revbook) == 0 ? FZB_OK : FZB_E_INVALID;
+}
+
+int fzb_huff_encode(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint32_t* d_bk4,
+                    const uint8_t* d_revbook, void* d_out, uint64_t* d_out_size, void* d_work,
+                    size_t work_bytes, void* stream) {
+    if (!d_in || !d_bk4 || !d_revbook || !d_out || !d_out_size || !hf_args_ok(n, bklen))
+        return FZB_E_INVALID;
+    if (reinterpret_cast<uintptr_t>(d_out) & 3) return FZB_E_INVALID;
+    HfWork w = carve_hf(d_work, n, bklen);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
+    return launch_hf_encode(d_in, n, d_bk4, bklen, d_revbook, static_cast<uint8_t*>(d_out),
+                            reinterpret_cast<unsigned long long*>(d_out_size), w.slots, w.par_nbit,
+                            w.par_ncell, w.par_entry, w.tiles, w.ncell_total, sm_count(), s) == 0
+               ? FZB_OK : FZB_E_CUDA;
+}
+
+int fzb_huff_compress(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_out,
+                      uint64_t* d_out_size, void* d_work, size_t work_bytes, void* stream) {
+    if (!d_in || !d_out || !d_out_size || !hf_args_ok(n, bklen)) return FZB_E_INVALID;
+    if (reinterpret_cast<uintptr_t>(d_out) & 3) return FZB_E_INVALID;
+    HfWork w = carve_hf(d_work, n, bklen);
+    if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    int rc = fzb_huff_histogram(d_in, n, bklen, w.freq, stream);
+    if (rc) return rc;
+    std::vector<uint32_t> freq(bklen), bk4(bklen);
+    std::vector<uint8_t> revbook(hf_revbook_bytes(bklen));
+    CK(cudaMemcpyAsync(freq.data(), w.freq, 4 * (size_t)bklen, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    uint64_t sum = 0;
+    for (uint32_t i = 0; i < bklen; i++) sum += freq[i];
+    if (sum != n) return FZB_E_RANGE;
+    if (build_huffman_book(freq.data(), bklen, bk4.data(), revbook.data()) != 0) return FZB_E_INVALID;
+    // pageable sources: each copy has read its host buffer when the call returns
+    CK(cudaMemcpyAsync(w.bk4, bk4.data(), 4 * (size_t)bklen, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(w.revbook, revbook.data(), revbook.size(), cudaMemcpyHostToDevice, s));
+    return fzb_huff_encode(d_in, n, bklen, w.bk4, w.revbook, d_out, d_out_size, d_work, work_bytes,
+                           stream);
+}
+
+int fzb_huff_decode(const void* d_in, uint64_t in_bytes, uint64_t n, uint32_t bklen, uint16_t* d_out,
+                    void* d_work, size_t work_bytes, void* stream) {
+    if (!d_in || !d_out || !hf_args_ok(n, bklen) || in_bytes < 128) return FZB_E_INVALID;
+    if (reinterpret_cast<uintptr_t>(d_in) & 7) return FZB_E_INVALID;
+    if (!d_work || work_bytes < kCtrlBytes) return FZB_E_WORKSPACE;
+    cudaStream_t s = S(stream);
+    uint32_t* err = static_cast<uint32_t*>(d_work);
+    CK(cudaMemsetAsync(err, 0, kCtrlBytes, s));
+    return launch_hf_decode(static_cast<const uint8_t*>(d_in), in_bytes, n, bklen, d_out, err, s) == 0
                ? FZB_OK : FZB_E_CUDA;
 }
 

@@ -20,14 +20,6 @@ constexpr int kScanTile = 4096;  // elements per CTA in the scan passes
 // (count given or read from *cptr) or the run-length array of an RLE stream
 // (count and position read from the stream's header on the device).
 // ---------------------------------------------------------------------------
-struct ScanSrc {
-    const uint32_t* base;     // plain array
-    const uint32_t* cptr;     // optional device count
-    const uint8_t* rle;       // RLE stream instead of base
-    int elem;                 // RLE value width
-    uint32_t n;               // upper bound of the count
-};
-
 __device__ __forceinline__ const uint32_t* scan_src(const ScanSrc& a, uint32_t* cnt) {
     if (a.rle) {
         const uint32_t R = *reinterpret_cast<const uint32_t*>(a.rle);

@@ -114,6 +114,19 @@ __global__ void lq_inverse_2d_kernel(InvArgs a);
 __global__ void lq_inverse_3d_kernel(InvArgs a);
 __global__ void fused_inverse_3d_kernel(InvArgs a);
 
+// Exclusive scan of u32 values (fzb_coders.cu).  The source is a plain
+// array (count given, or read from *cptr on the device) or the run-length
+// array of an RLE stream.
+struct ScanSrc {
+    const uint32_t* base;     // plain array
+    const uint32_t* cptr;     // optional device count
+    const uint8_t* rle;       // RLE stream instead of base
+    int elem;                 // RLE value width
+    uint32_t n;               // upper bound of the count
+};
+int launch_scan_u32(const ScanSrc& a, uint32_t* out, uint32_t* tile_scratch, uint32_t* total,
+                    cudaStream_t s);
+
 // RLE and Bitpack (fzb_coders.cu); return cudaError_t values.
 int launch_rle_encode(const void* in, uint32_t n, int elem, uint8_t* out, unsigned long long* out_size,
                       uint32_t* tcnt, uint32_t* starts, uint32_t* runs_total, cudaStream_t s);
@@ -123,5 +136,17 @@ int launch_bitpack_encode(const void* in, uint64_t n, int elem, int nbits, uint8
                           uint8_t* out, unsigned long long* out_size, uint32_t* pmax,
                           unsigned int* done, cudaStream_t s);
 int launch_bitpack_decode(const uint8_t* in, uint64_t n, int elem, int nbits, void* out, cudaStream_t s);
+
+// PHF Huffman, coarse mode (fzb_huffman.cu, codebook in fzb_hfbook.cpp).
+constexpr int kHfSublen = 768;
+int launch_hf_histogram(const uint16_t* in, uint64_t n, uint32_t bklen, uint32_t* freq, int sms,
+                        cudaStream_t s);
+int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32_t bklen,
+                     const uint8_t* d_revbook, uint8_t* out, unsigned long long* out_size,
+                     uint32_t* slots, uint32_t* par_nbit, uint32_t* par_ncell, uint32_t* par_entry,
+                     uint32_t* tiles, uint32_t* ncell_total, int sms, cudaStream_t s);
+int launch_hf_decode(const uint8_t* blob, uint64_t blob_bytes, uint64_t n, uint32_t bklen,
+                     uint16_t* out, uint32_t* err, cudaStream_t s);
+int build_huffman_book(const uint32_t* freq, uint32_t bklen, uint32_t* bk4, uint8_t* revbook);
 
 }  // namespace fzb

@@ -11,7 +11,7 @@ import math
 
 import torch
 
-from ._lib import check, lib
+from ._lib import FzbError, check, lib
 
 ABS, REL, NOA = 0, 1, 2
 NO_SYNC, FORCE_EXACT = 1, 2
@@ -40,6 +40,13 @@ class Workspace:
 
     def get(self, n_total: int, device, cap: int = 0) -> tuple[C.c_void_p, int]:
         need = int(lib().fzb_workspace_bytes(int(n_total), int(cap)))
+        if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
+            self.buf = torch.empty(need, dtype=torch.uint8, device=device)
+        return _ptr(self.buf), self.buf.numel()
+
+    def get_bytes(self, need: int, device) -> tuple[C.c_void_p, int]:
+        """Workspace of at least `need` bytes (for the Huffman entry points)."""
+        need = max(int(need), 256)
         if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
             self.buf = torch.empty(need, dtype=torch.uint8, device=device)
         return _ptr(self.buf), self.buf.numel()
@@ -217,4 +224,76 @@ def bitpack_decode(packed: torch.Tensor, n: int, nbits: int, dtype=torch.uint16)
     out = torch.empty(n, dtype=dtype, device=packed.device)
     check(lib().fzb_bitpack_decode(_ptr(packed), n, _elem(out), nbits, _ptr(out),
                                    _stream(packed.device)), "fzb_bitpack_decode")
+    return out
+
+
+# ------------------------------------------------------------------ Huffman
+
+def huff_histogram(codes: torch.Tensor, bklen: int = 1024) -> torch.Tensor:
+    """GPU_histogram_generic (util/histogram/histogram.cu): u32 counts."""
+    src = codes.reshape(-1)
+    freq = torch.empty(bklen, dtype=torch.int32, device=src.device)
+    check(lib().fzb_huff_histogram(_ptr(src), src.numel(), bklen, _ptr(freq), _stream(src.device)),
+          "fzb_huff_histogram")
+    return freq
+
+
+def huff_book(freq, bklen: int = 1024):
+    """phf_CPU_build_canonized_codebook_v2 (phf/hf_bk.cc:84-140) on the host.
+    Returns (bk4 u32[bklen], revbook u8[256 + 2*bklen]) as numpy arrays."""
+    import numpy as np
+    f = np.ascontiguousarray(freq.cpu().numpy() if isinstance(freq, torch.Tensor) else freq).view(np.uint32)
+    bk4 = np.empty(bklen, np.uint32)
+    rb = np.zeros(256 + 2 * bklen, np.uint8)
+    check(lib().fzb_huff_book(f.ctypes.data, bklen, bk4.ctypes.data, rb.ctypes.data), "fzb_huff_book")
+    return bk4, rb
+
+
+def huff_encode(codes: torch.Tensor, bk4, revbook, bklen: int = 1024, ws: Workspace | None = None,
+                trim: bool = True):
+    """GPU_coarse_encode + blob assembly with a given codebook.  Returns
+    (blob, size_tensor)."""
+    import numpy as np
+    ws = ws or _default_ws
+    src = codes.reshape(-1)
+    n, dev = src.numel(), src.device
+    d_bk4 = torch.from_numpy(np.ascontiguousarray(bk4).view(np.int32)).to(dev)
+    d_rb = torch.from_numpy(np.ascontiguousarray(revbook)).to(dev)
+    out = torch.empty(int(lib().fzb_huff_max_bytes(n, bklen)), dtype=torch.uint8, device=dev)
+    size = torch.zeros(1, dtype=torch.int64, device=dev)
+    wp, wn = ws.get_bytes(lib().fzb_huff_workspace_bytes(n, bklen), dev)
+    check(lib().fzb_huff_encode(_ptr(src), n, bklen, _ptr(d_bk4), _ptr(d_rb), _ptr(out), _ptr(size),
+                                wp, wn, _stream(dev)), "fzb_huff_encode")
+    if trim:
+        return out[: int(size.item())], size
+    return out, size
+
+
+def huff_compress(codes: torch.Tensor, bklen: int = 1024, ws: Workspace | None = None,
+                  trim: bool = True):
+    """HuffmanStage<uint16_t>::execute forward (huffman_stage.cu:111-186).
+    Returns (blob, size_tensor)."""
+    ws = ws or _default_ws
+    src = codes.reshape(-1)
+    n, dev = src.numel(), src.device
+    out = torch.empty(int(lib().fzb_huff_max_bytes(n, bklen)), dtype=torch.uint8, device=dev)
+    size = torch.zeros(1, dtype=torch.int64, device=dev)
+    wp, wn = ws.get_bytes(lib().fzb_huff_workspace_bytes(n, bklen), dev)
+    check(lib().fzb_huff_compress(_ptr(src), n, bklen, _ptr(out), _ptr(size), wp, wn, _stream(dev)),
+          "fzb_huff_compress")
+    if trim:
+        return out[: int(size.item())], size
+    return out, size
+
+
+def huff_decode(blob: torch.Tensor, n: int, bklen: int = 1024, ws: Workspace | None = None,
+                out: torch.Tensor | None = None):
+    """HuffmanStage<uint16_t> inverse (phf/hf_kernels.cu:267-298)."""
+    ws = ws or _default_ws
+    src = blob.view(torch.uint8).reshape(-1)
+    if out is None:
+        out = torch.empty(n, dtype=torch.uint16, device=src.device)
+    wp, wn = ws.get_bytes(256, src.device)
+    check(lib().fzb_huff_decode(_ptr(src), src.numel(), n, bklen, _ptr(out), wp, wn,
+                                _stream(src.device)), "fzb_huff_decode")
     return out

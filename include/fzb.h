@@ -28,6 +28,7 @@ extern "C" {
 #define FZB_E_CAPACITY (-4)    /* output buffer too small                    */
 #define FZB_E_MALFORMED (-5)   /* compressed input is inconsistent           */
 #define FZB_E_TIMEOUT (-6)     /* a bounded device wait gave up              */
+#define FZB_E_RANGE (-7)       /* an input symbol is outside the codebook     */
 
 /* Error-bound modes (modules/fused/lorenzo_quant/lorenzo_quant.h:30-34). */
 #define FZB_ABS 0
@@ -154,6 +155,47 @@ int fzb_bitpack_encode(const void* d_in, uint64_t n, int elem, int nbits, void* 
                        uint8_t* d_nbits, uint64_t* d_out_size, void* d_work, size_t work_bytes,
                        void* stream);
 int fzb_bitpack_decode(const void* d_in, uint64_t n, int elem, int nbits, void* d_out, void* stream);
+
+/* PHF Huffman, HuffmanStage<uint16_t> in coarse mode
+ * (modules/coders/huffman/huffman_stage.cu:111-205, phf/hf_hl.cc:25-160).
+ * Blob layout (phf/hf.h:38-44): [128-byte header slot][revbook = int first[32],
+ * int entry[32], u16 keys[bklen]][u32 par_nbit x pardeg][u32 par_entry x
+ * pardeg][u32 bitstream x total_ncell], pardeg = ceil(n / 768).  Header bytes
+ * 64..127 and the upper 16 bits of the first word are written as zero (the
+ * reference leaves encoder scratch there).  bklen is 1..65535. */
+size_t fzb_huff_workspace_bytes(uint64_t n, uint32_t bklen);
+uint64_t fzb_huff_max_bytes(uint64_t n, uint32_t bklen);
+
+/* GPU_histogram_generic (util/histogram/histogram.cu): d_freq[bklen] counts
+ * the symbols of d_in below bklen (larger symbols are skipped). */
+int fzb_huff_histogram(const uint16_t* d_in, uint64_t n, uint32_t bklen, uint32_t* d_freq,
+                       void* stream);
+
+/* phf_CPU_build_canonized_codebook_v2 (phf/hf_bk.cc:84-140), host memory:
+ * h_bk4[bklen] (bits 31..27 length, low 27 canonical code, 0xffffffff for an
+ * absent symbol) and h_revbook[256 + 2*bklen]. */
+int fzb_huff_book(const uint32_t* h_freq, uint32_t bklen, uint32_t* h_bk4, uint8_t* h_revbook);
+
+/* GPU_coarse_encode + memcpy_merge (phf/hf_kernels.cu:59-140,
+ * hf_buf.cc:152-176) with a device codebook: writes the blob to d_out (4-byte
+ * aligned, fzb_huff_max_bytes) and its size to *d_out_size (device u64).
+ * Enqueue only. */
+int fzb_huff_encode(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint32_t* d_bk4,
+                    const uint8_t* d_revbook, void* d_out, uint64_t* d_out_size, void* d_work,
+                    size_t work_bytes, void* stream);
+
+/* HuffmanStage<uint16_t>::execute forward: histogram, one stream
+ * synchronisation to read it (as the reference does), host codebook, encode.
+ * Returns FZB_E_RANGE when a symbol is >= bklen (huffman_stage.cu:151-164). */
+int fzb_huff_compress(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_out,
+                      uint64_t* d_out_size, void* d_work, size_t work_bytes, void* stream);
+
+/* HuffmanStage<uint16_t> inverse (phf/hf_kernels.cu:267-298): decodes the blob
+ * (8-byte aligned) into n symbols.  A header that disagrees with n / bklen or a
+ * bitstream that does not decode to exactly n symbols is reported as
+ * FZB_E_MALFORMED by fzb_workspace_status(); work_bytes >= 256. */
+int fzb_huff_decode(const void* d_in, uint64_t in_bytes, uint64_t n, uint32_t bklen, uint16_t* d_out,
+                    void* d_work, size_t work_bytes, void* stream);
 
 #ifdef __cplusplus
 }

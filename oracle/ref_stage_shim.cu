@@ -166,7 +166,7 @@ extern "C" int ref_bitpack_u16(const uint16_t* d_in, size_t n, int nbits, void* 
 extern "C" int ref_huffman_u16(const uint16_t* d_in, size_t n, int bklen, void* d_out,
                                size_t* out_bytes, uint16_t* d_dec) {
     GUARD_BEGIN
-    MemoryPool pool(MemoryPoolConfig(n * 2, 3.0f));
+    MemoryPool pool(MemoryPoolConfig(n * 2 + (size_t(1) << 22), 3.0f));
     HuffmanStage<uint16_t> st;
     st.setBklen((uint32_t)bklen);
     cudaStream_t s = 0;

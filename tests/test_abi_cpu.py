@@ -35,3 +35,48 @@ def test_invalid_arguments_rejected_before_launch():
     assert rc == -1
     rc = L.fzb_rze_encode(None, 0, None, None, None, 0, None)
     assert rc == -1
+
+
+def test_huffman_host_codebook_matches_oracle_and_reference():
+    """fzb_huff_book is host code: it runs here and must equal the oracle's
+    and (when built) the reference's phf_CPU_build_canonized_codebook_v2."""
+    import numpy as np
+    from fzgpumodules_b200 import kernels as K
+    from oracle import oracle as O
+    rng = np.random.default_rng(7)
+    cases = []
+    for _ in range(60):
+        bk = int(rng.choice([2, 3, 16, 256, 1024, 4096]))
+        f = np.zeros(bk, np.uint32)
+        k = int(rng.integers(1, bk + 1))
+        pos = rng.choice(bk, k, replace=False)
+        f[pos] = rng.geometric(rng.uniform(0.001, 0.5), k).astype(np.uint32) * \
+            rng.integers(1, 1000, k).astype(np.uint32)
+        cases.append((f, bk))
+    fib = [1, 1]
+    while len(fib) < 40:
+        fib.append(fib[-1] + fib[-2])
+    f = np.zeros(1024, np.uint32)
+    f[:40] = fib  # tree deeper than 27: lengths truncated to 28
+    cases.append((f, 1024))
+    f = np.zeros(1024, np.uint32)
+    f[7] = 100  # a single symbol
+    cases.append((f, 1024))
+    for f, bk in cases:
+        a = K.huff_book(f, bk)
+        b = O.huff_book(f, bk)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        if O.ref_hfbook_available():
+            c = O.ref_huff_book(f, bk)
+            assert np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1])
+
+
+def test_huffman_sizes_and_invalid():
+    L = _lib.lib()
+    assert L.fzb_huff_max_bytes(768, 1024) == 128 + 256 + 2048 + 8 + 4 * 769 + 16
+    assert L.fzb_huff_workspace_bytes(0, 1024) == 0
+    assert L.fzb_huff_workspace_bytes(1000, 0) == 0
+    assert L.fzb_huff_workspace_bytes(10 ** 6, 1024) > 4 * 10 ** 6
+    assert L.fzb_huff_compress(None, 10, 1024, None, None, None, 0, None) == -1
+    assert L.fzb_huff_decode(None, 10, 10, 1024, None, None, 0, None) == -1
+    assert L.fzb_status_string(-7) == b"input symbol outside [0, bklen)"
