@@ -28,7 +28,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-DIMS = (512, 512, 512)
+DEFAULT_DIMS = (512, 512, 512)
 EB, RADIUS, ZIGZAG, OUTLIER_CAP = 1e-3, 32768, True, 0.1
 SEED = 1002
 METRIC = "comp/decomp GB/s and % HBM roofline at fixed eb"
@@ -182,6 +182,17 @@ def run_reference(args, world, rank):
 
 # ---------------------------------------------------------------- GPU side
 
+def _traffic(kernel: str):
+    """DRAM bytes per element of `kernel` from the committed ncu summary
+    (profiles/traffic.json: dram__bytes_read.sum + dram__bytes_write.sum of
+    one captured launch divided by the elements it processed), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)[kernel]
+    except Exception:
+        return None
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -189,6 +200,7 @@ def run_ours(args, world, rank, local):
     from fzgpumodules_b200 import fields, kernels
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    DIMS = tuple(args.dims)
     nz, ny, nx = DIMS[2], DIMS[1], DIMS[0]
     x = fields.grf((nz, ny, nx), seed=SEED + rank, spike_frac=1e-3, device=dev).reshape(-1)
     n = x.numel()
@@ -227,11 +239,13 @@ def run_ours(args, world, rank, local):
             one("c"), one("d")
         barrier(world)
         t_wall = time.perf_counter()
-        for _ in range(args.steps):
-            ev_c.append(one("c"))
-            ev_d.append(one("d"))
-        torch.cuda.synchronize()
+        with kernels.Trace() as trace:  # per-kernel CUDA events on the launching stream
+            for _ in range(args.steps):
+                ev_c.append(one("c"))
+                ev_d.append(one("d"))
+            torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall
+        per_kernel = trace.kernels()
     barrier(world)
     st = ws.status()
     tc = [a.elapsed_time(b) / 1e3 for a, b in ev_c]
@@ -239,14 +253,28 @@ def run_ours(args, world, rank, local):
     t_c = max_over_ranks(float(np.mean(tc)), world)
     t_d = max_over_ranks(float(np.mean(td)), world)
 
+    # the dominant kernels, timed by their own events (max over ranks)
+    def kern(name):
+        launches, ms = per_kernel.get(name, (0, 0.0))
+        return launches, max_over_ranks(ms / launches / 1e3 if launches else 0.0, world)
+
+    slab_name = "lq3d_slab_bs_rze" if "lq3d_slab_bs_rze" in per_kernel else "lq_chunk_bs_rze"
+    inv_name = "fused_inverse_3d" if "fused_inverse_3d" in per_kernel else "lq_inverse"
+    n_slab, t_slab = kern(slab_name)
+    n_inv, t_inv = kern(inv_name)
+    launches = sum(v[0] for v in per_kernel.values())
+
     # end to end through the C ABI with host buffers: H2D of the field, compress,
     # D2H of the compressed segments; H2D of the segments, decompress, D2H of the field
     hx = x.cpu().pin_memory()
     hy = torch.empty_like(hx).pin_memory()
     hs = torch.empty(size, dtype=torch.uint8).pin_memory()
     dx = torch.empty_like(x)
-    e2e_c, e2e_d = [], []
-    for it in range(args.warmup + args.steps):
+    e2e_c, e2e_d = [1.0], [1.0]
+    e2e_steps = 0 if args.no_e2e else args.warmup + args.steps
+    if e2e_steps:
+        e2e_c, e2e_d = [], []
+    for it in range(e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         dx.copy_(hx, non_blocking=True)
@@ -277,15 +305,17 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = _peaks()
     algo_c = nbytes + comp_bytes   # read f32 field + write compressed segments
     algo_d = comp_bytes + nbytes   # read compressed segments + write f32 field
-    ach_c = algo_c / t_c / 1e9
-    ach_d = algo_d / t_d / 1e9
+    ach_c = algo_c / t_slab / 1e9 if t_slab else 0.0   # dominant compress kernel
+    ach_d = algo_d / t_inv / 1e9 if t_inv else 0.0     # dominant decompress kernel
+    tr_c, tr_d = _traffic(slab_name), _traffic(inv_name)
     cpu = cpu_baseline(1) if (world == 1 and not args.no_cpu) else None
     line = {
         "metric": METRIC, "value": world * nbytes / t_c / 1e9, "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": (t_c + t_d) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "dims": list(DIMS), "eb": EB, "eb_mode": "REL",
+        "config": {"workload": WORKLOAD if DIMS == DEFAULT_DIMS else WORKLOAD.replace("512^3", "x".join(map(str, DIMS))),
+                   "dims": list(DIMS), "eb": EB, "eb_mode": "REL",
                    "radius": RADIUS, "zigzag": ZIGZAG, "outlier_capacity": OUTLIER_CAP,
                    "l2": "input 512 MiB > L2, plus a 256 MiB L2 flush before every timed call",
                    "parallelism": f"replicas x{world}"},
@@ -294,14 +324,22 @@ def run_ours(args, world, rank, local):
         "decompress": {"value": world * nbytes / t_d / 1e9, "unit": "GB/s", "ms": t_d * 1e3,
                        "max_abs_err": maxerr, "abs_eb": abs_eb,
                        "roofline": {"bound": "hbm", "achieved": ach_d, "peak": peak, "unit": "GB/s",
-                                    "frac": ach_d / peak, "traffic": None, "peak_kind": peak_kind}},
+                                    "frac": ach_d / peak,
+                                    "traffic": tr_d["bytes_per_element"] * n if tr_d else None,
+                                    "algorithmic_bytes": algo_d, "peak_kind": peak_kind,
+                                    "kernel": inv_name, "kernel_ms": t_inv * 1e3, "launches": n_inv,
+                                    "call_frac": (algo_d / t_d / 1e9) / peak}},
         "roofline": {"bound": "hbm", "achieved": ach_c, "peak": peak, "unit": "GB/s",
-                     "frac": ach_c / peak, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "lq_chunk_kernel<3,fused> (+ value-base scan)"},
-        "e2e": {"value": world * nbytes / e2e_t / 1e9, "unit": "GB/s",
+                     "frac": ach_c / peak,
+                     "traffic": tr_c["bytes_per_element"] * n if tr_c else None,
+                     "algorithmic_bytes": algo_c, "peak_kind": peak_kind,
+                     "kernel": slab_name, "kernel_ms": t_slab * 1e3, "launches": n_slab,
+                     "call_frac": (algo_c / t_c / 1e9) / peak},
+        "kernels_ms_per_step": {k: v[1] / args.steps for k, v in per_kernel.items()},
+        "e2e": None if args.no_e2e else {"value": world * nbytes / e2e_t / 1e9, "unit": "GB/s",
                 "h2d_bytes_per_step": nbytes + comp_bytes, "d2h_bytes_per_step": comp_bytes + nbytes + 8,
                 "compress_gbs": nbytes / e2e_t / 1e9, "decompress_gbs": nbytes / e2e_td / 1e9},
-        "gpu_launches": args.steps * (3 + 3),
+        "gpu_launches": launches,
         "clocks": clk.summary(),
         "status": st,
         "wall_s_timed": t_wall,
@@ -320,6 +358,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--dims", type=int, nargs=3, default=list(DEFAULT_DIMS), metavar=("NX", "NY", "NZ"),
+                    help="field extents (x fastest); the default is the 512^3 workload")
     args = ap.parse_args()
     world, rank, local = dist_setup() if args.impl == "ours" else (
         int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)

@@ -72,6 +72,14 @@ def lib():
         L.fzb_bitpack_encode.argtypes = [p, u64, i32, i32, p, p, p, p, sz, p]
         L.fzb_bitpack_decode.restype = i32
         L.fzb_bitpack_decode.argtypes = [p, u64, i32, i32, p, p]
+        L.fzb_trace_enable.restype = i32
+        L.fzb_trace_enable.argtypes = [i32]
+        L.fzb_trace_collect.restype = i32
+        L.fzb_trace_collect.argtypes = []
+        L.fzb_trace_get.restype = i32
+        L.fzb_trace_get.argtypes = [i32, C.c_char_p, sz, p, p]
+        L.fzb_trace_reset.restype = None
+        L.fzb_trace_reset.argtypes = []
         L.fzb_huff_workspace_bytes.restype = sz
         L.fzb_huff_workspace_bytes.argtypes = [u64, u32]
         L.fzb_huff_max_bytes.restype = u64

@@ -144,9 +144,11 @@ int resolve_eb(const float* d_in, uint64_t n_total, float eb, int mode, float va
         int parts = (int)(want < (uint64_t)(4 * sms) ? want : (uint64_t)(4 * sms));
         if (parts < 1) parts = 1;
         if (parts > kMaxParts) parts = kMaxParts;
+        TraceScope ts(s, "minmax_resolve_eb");
         minmax_kernel<<<parts, 256, 0, s>>>(d_in, n_total, w.pmin, w.pmax, w.mm_done, mode, eb,
                                             d_eb_state);
     } else {
+        TraceScope ts(s, "resolve_eb");
         resolve_eb_kernel<<<1, 32, 0, s>>>(mode, eb, value_base, d_eb_state);
     }
     CK(cudaGetLastError());
@@ -202,8 +204,10 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        TraceScope ts(s, "lq3d_slab_bs_rze");
         rc = launch_lq3d_slab(a, (unsigned)(2 * sms), s) == 0 ? FZB_OK : FZB_E_CUDA;
     } else {
+        TraceScope ts(s, fused ? "lq_chunk_bs_rze" : "lq_chunk");
         rc = launch_lq(g, fused, a, lq_smem_bytes(g, fused), (uint32_t)nch, s);
     }
     if (rc) return rc;
@@ -225,9 +229,15 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
     m.out_idx = d_idx;
     m.cap = a.ostage_cap;
     m.out_count = d_count;
-    assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
+    {
+        TraceScope ts(s, "assemble_scan");
+        assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
+    }
     CK(cudaGetLastError());
-    assemble_copy_kernel<<<(unsigned)nch, 256, 0, s>>>(m);
+    {
+        TraceScope ts(s, "assemble_copy");
+        assemble_copy_kernel<<<(unsigned)nch, 256, 0, s>>>(m);
+    }
     CK(cudaGetLastError());
     return FZB_OK;
 }
@@ -252,9 +262,11 @@ int exact_inverse(const InvArgs& a, const Geometry& g, cudaStream_t s) {
     if (a.cap) {
         uint32_t blocks = (uint32_t)((a.cap + 255) / 256);
         if (blocks > 4096) blocks = 4096;
+        TraceScope ts(s, "scatter_outliers");
         scatter_outliers_kernel<<<blocks, 256, 0, s>>>(a);
         CK(cudaGetLastError());
     }
+    TraceScope ts(s, "lq_inverse");
     if (g.ndim == 1) {
         lq_inverse_1d_kernel<<<(g.nfield + 1023) / 1024, 256, 0, s>>>(a);
     } else if (g.ndim == 2) {
@@ -461,8 +473,11 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
     if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
     cudaStream_t s = S(stream);
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
-    rze_prepass_kernel<<<1, 1024, 0, s>>>(static_cast<const uint8_t*>(d_rze), rze_bytes, (uint32_t)nch,
-                                          (uint32_t)(2 * n_total), w.in_off, w.err);
+    {
+        TraceScope ts(s, "rze_prepass");
+        rze_prepass_kernel<<<1, 1024, 0, s>>>(static_cast<const uint8_t*>(d_rze), rze_bytes,
+                                              (uint32_t)nch, (uint32_t)(2 * n_total), w.in_off, w.err);
+    }
     CK(cudaGetLastError());
     InvArgs a = inv_args(w, g, n_total);
     a.rze = static_cast<const uint8_t*>(d_rze);
@@ -483,14 +498,20 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
     const uint32_t R = pow2 ? (uint32_t)kChunkCodes / nx : 0;
     const bool fused = !(flags & FZB_FORCE_EXACT) && g.ndim == 3 && pow2 && g.ny % R == 0;
     if (fused) {
-        outlier_ranges_kernel<<<(unsigned)((nch + 256) / 256 + 1), 256, 0, s>>>(
-            d_idx, d_count, a.cap, (uint32_t)nch, w.ostart, w.err);
+        {
+            TraceScope ts(s, "outlier_ranges");
+            outlier_ranges_kernel<<<(unsigned)((nch + 256) / 256 + 1), 256, 0, s>>>(
+                d_idx, d_count, a.cap, (uint32_t)nch, w.ostart, w.err);
+        }
         CK(cudaGetLastError());
         const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32 + 4 * kChunkCodes;
         CK(cudaFuncSetAttribute(fused_inverse_3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem));
         dim3 grid(g.ny / R, (g.nz + 7) / 8, 1);
-        fused_inverse_3d_kernel<<<grid, kThreads, smem, s>>>(a);
+        {
+            TraceScope ts(s, "fused_inverse_3d");
+            fused_inverse_3d_kernel<<<grid, kThreads, smem, s>>>(a);
+        }
         CK(cudaGetLastError());
         if (n_total > g.nfield)
             CK(cudaMemsetAsync(d_out + g.nfield, 0, sizeof(float) * (n_total - g.nfield), s));
@@ -506,7 +527,10 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
     const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
     CK(cudaFuncSetAttribute(rze_decode_codes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             smem));
-    rze_decode_codes_kernel<<<(unsigned)nch, kThreads, smem, s>>>(a);
+    {
+        TraceScope ts(s, "rze_decode_bitunshuffle");
+        rze_decode_codes_kernel<<<(unsigned)nch, kThreads, smem, s>>>(a);
+    }
     CK(cudaGetLastError());
     rc = exact_inverse(a, g, s);
     if (rc || (flags & FZB_NO_SYNC)) return rc;

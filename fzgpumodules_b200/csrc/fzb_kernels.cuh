@@ -137,6 +137,21 @@ int launch_bitpack_encode(const void* in, uint64_t n, int elem, int nbits, uint8
                           unsigned int* done, cudaStream_t s);
 int launch_bitpack_decode(const uint8_t* in, uint64_t n, int elem, int nbits, void* out, cudaStream_t s);
 
+// Per-kernel CUDA-event timing (fzb_trace.cu): a TraceScope around a launch
+// records an event pair on the launching stream while tracing is enabled.
+extern bool g_trace_on;
+class TraceScope {
+public:
+    TraceScope(cudaStream_t s, const char* name);
+    ~TraceScope();
+    TraceScope(const TraceScope&) = delete;
+    TraceScope& operator=(const TraceScope&) = delete;
+
+private:
+    cudaStream_t s_;
+    cudaEvent_t end_;
+};
+
 // PHF Huffman, coarse mode (fzb_huffman.cu, codebook in fzb_hfbook.cpp).
 constexpr int kHfSublen = 768;
 int launch_hf_histogram(const uint16_t* in, uint64_t n, uint32_t bklen, uint32_t* freq, int sms,

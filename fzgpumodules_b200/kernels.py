@@ -297,3 +297,32 @@ def huff_decode(blob: torch.Tensor, n: int, bklen: int = 1024, ws: Workspace | N
     check(lib().fzb_huff_decode(_ptr(src), src.numel(), n, bklen, _ptr(out), wp, wn,
                                 _stream(src.device)), "fzb_huff_decode")
     return out
+
+
+# ------------------------------------------------------------------ tracing
+
+class Trace:
+    """Per-kernel CUDA-event timing of the library's launches
+    (fzb_trace_*).  Use as a context manager; `kernels()` returns
+    {name: (launches, total_ms)} accumulated while enabled."""
+
+    def __enter__(self):
+        lib().fzb_trace_collect()
+        lib().fzb_trace_reset()
+        lib().fzb_trace_enable(1)
+        return self
+
+    def __exit__(self, *exc):
+        lib().fzb_trace_enable(0)
+
+    @staticmethod
+    def kernels() -> dict:
+        n = lib().fzb_trace_collect()
+        check(min(n, 0), "fzb_trace_collect")
+        out = {}
+        name = C.create_string_buffer(96)
+        launches, ms = C.c_uint64(0), C.c_double(0.0)
+        for i in range(n):
+            check(lib().fzb_trace_get(i, name, 96, C.byref(launches), C.byref(ms)), "fzb_trace_get")
+            out[name.value.decode()] = (int(launches.value), float(ms.value))
+        return out

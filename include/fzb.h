@@ -42,6 +42,18 @@ extern "C" {
 int fzb_version(void);
 const char* fzb_status_string(int status);
 
+/* Per-kernel timing with CUDA events, the library side of the reference's
+ * per-node profiling (Pipeline::enableProfiling / collectTimings,
+ * src/pipeline/dag.cpp:107-116,418-420, include/perf.h:70).  While enabled,
+ * each traced launch records an event pair on its stream.
+ * fzb_trace_collect() waits for them and returns the number of distinct
+ * kernel names accumulated so far (or a negative status); fzb_trace_get()
+ * reads entry i (name, launches, total milliseconds). */
+int fzb_trace_enable(int on);
+int fzb_trace_collect(void);
+int fzb_trace_get(int i, char* name, size_t name_cap, uint64_t* launches, double* total_ms);
+void fzb_trace_reset(void);
+
 /* Workspace for any entry point over n_total Lorenzo elements (or
  * 2*n_total bytes for the byte-stream coders) with room to stage up to
  * `cap` outliers (the forward entry points' outlier capacity; 0 otherwise). */
