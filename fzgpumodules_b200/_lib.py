@@ -72,6 +72,37 @@ def lib():
         L.fzb_bitpack_encode.argtypes = [p, u64, i32, i32, p, p, p, p, sz, p]
         L.fzb_bitpack_decode.restype = i32
         L.fzb_bitpack_decode.argtypes = [p, u64, i32, i32, p, p]
+        L.fzb_concat_bytes.restype = u64
+        L.fzb_concat_bytes.argtypes = [p, i32]
+        L.fzb_concat.restype = i32
+        L.fzb_concat.argtypes = [p, p, i32, p, p]
+        L.fzb_last_error.restype = C.c_char_p
+        L.fzb_last_error.argtypes = []
+        L.fzb_pipeline_create.restype = p
+        L.fzb_pipeline_create.argtypes = [u64, i32, f32]
+        L.fzb_pipeline_destroy.restype = None
+        L.fzb_pipeline_destroy.argtypes = [p]
+        L.fzb_pipeline_set_dims.argtypes = [p, u64, u64, u64]
+        L.fzb_pipeline_add_lorenzo_quant.argtypes = [p, f32, i32, i32, f32, i32, f32]
+        L.fzb_pipeline_add_bitshuffle.argtypes = [p, u32, i32]
+        L.fzb_pipeline_add_rze.argtypes = [p, u32, i32]
+        L.fzb_pipeline_add_rle.argtypes = [p, i32]
+        L.fzb_pipeline_add_huffman.argtypes = [p, u32]
+        L.fzb_pipeline_add_bitpack.argtypes = [p, i32, i32]
+        L.fzb_pipeline_connect.argtypes = [p, i32, i32, C.c_char_p]
+        L.fzb_pipeline_set_fusion.argtypes = [p, i32]
+        L.fzb_pipeline_enable_graph_mode.argtypes = [p, i32]
+        L.fzb_pipeline_enable_profiling.argtypes = [p, i32]
+        L.fzb_pipeline_finalize.argtypes = [p]
+        L.fzb_pipeline_is_fused.argtypes = [p]
+        L.fzb_pipeline_capture_graph.argtypes = [p, p]
+        L.fzb_pipeline_compress.argtypes = [p, p, u64, p, p, p]
+        L.fzb_pipeline_decompress.argtypes = [p, p, u64, p, p, p]
+        L.fzb_pipeline_decompress_into.argtypes = [p, p, u64, p, u64, p, p]
+        L.fzb_pipeline_stage_timings.argtypes = [p, p, i32]
+        L.fzb_pipeline_write_file.argtypes = [p, C.c_char_p, p]
+        L.fzb_decompress_file.argtypes = [C.c_char_p, p, p, p]
+        L.fzb_free.argtypes = [p]
         L.fzb_trace_enable.restype = i32
         L.fzb_trace_enable.argtypes = [i32]
         L.fzb_trace_collect.restype = i32

@@ -640,8 +640,9 @@ HfWork carve_hf(void* base, uint64_t n, uint32_t bklen) {
     return w;
 }
 
+// bklen even keeps every u32 table of the blob 4-byte aligned
 inline bool hf_args_ok(uint64_t n, uint32_t bklen) {
-    return n > 0 && n < (1ull << 31) && bklen >= 1 && bklen <= 65535;
+    return n > 0 && n < (1ull << 31) && bklen >= 2 && bklen <= 65534 && (bklen & 1) == 0;
 }
 
 inline int sm_count() {
@@ -668,7 +669,7 @@ uint64_t fzb_huff_max_bytes(uint64_t n, uint32_t bklen) {
 
 int fzb_huff_histogram(const uint16_t* d_in, uint64_t n, uint32_t bklen, uint32_t* d_freq,
                        void* stream) {
-    if (!d_in || !d_freq || !hf_args_ok(n, bklen)) return FZB_E_INVALID;
+    if (!d_in || !d_freq || n == 0 || n >= (1ull << 31) || bklen < 1 || bklen > 65535) return FZB_E_INVALID;
     return launch_hf_histogram(d_in, n, bklen, d_freq, sm_count(), S(stream)) == 0 ? FZB_OK : FZB_E_CUDA;
 }
 
@@ -720,7 +721,7 @@ int fzb_huff_compress(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_
 int fzb_huff_decode(const void* d_in, uint64_t in_bytes, uint64_t n, uint32_t bklen, uint16_t* d_out,
                     void* d_work, size_t work_bytes, void* stream) {
     if (!d_in || !d_out || !hf_args_ok(n, bklen) || in_bytes < 128) return FZB_E_INVALID;
-    if (reinterpret_cast<uintptr_t>(d_in) & 7) return FZB_E_INVALID;
+    if (reinterpret_cast<uintptr_t>(d_in) & 3) return FZB_E_INVALID;
     if (!d_work || work_bytes < kCtrlBytes) return FZB_E_WORKSPACE;
     cudaStream_t s = S(stream);
     uint32_t* err = static_cast<uint32_t*>(d_work);

@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(128) hf_decode_kernel(const uint8_t* __restric
     const uint32_t* h32 = reinterpret_cast<const uint32_t*>(blob);
     const uint32_t bklen = h32[0] & 0xffffu;
     const bool ok = bklen == bklen_expect && h32[1] == (uint32_t)kSublen && h32[2] == pardeg &&
-                    *reinterpret_cast<const uint64_t*>(blob + 16) == n && e1 == 128 &&
+                    h32[4] == (uint32_t)n && h32[5] == (uint32_t)(n >> 32) && e1 == 128 &&
                     e2 == e1 + 256 + 2 * bklen && e3 == e2 + 4 * pardeg && e4 == e3 + 4 * pardeg &&
                     e4 <= e5 && e5 <= blob_bytes;
     if (!ok) {

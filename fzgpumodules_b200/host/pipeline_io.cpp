@@ -1,0 +1,482 @@
+// pipeline_io.cpp -- decompression (the inverse DAG) and the FZM container:
+// buildHeader / writeToFile / readHeader / decompressFromFile
+// (src/pipeline/compressor_io.cpp:90-706, compressor_inverse_dag.cpp).
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <fstream>
+#include <stdexcept>
+#include <unordered_set>
+
+#include "fz/pipeline.h"
+#include "fzb.h"
+
+namespace fz {
+
+namespace {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+inline size_t pad16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+struct FwdDesc {
+    Stage* stage;
+    std::vector<int> in_ids, out_ids;
+};
+
+using Avail = std::unordered_map<int, std::pair<void*, size_t>>;
+
+std::string hex8(uint32_t v) {
+    char b[16];
+    std::snprintf(b, sizeof(b), "%08X", v);
+    return b;
+}
+
+// The fused inverse applies when the source stage is LorenzoQuant whose codes
+// go through Bitshuffle(16 KiB, ew 2) into RZE(16 KiB, 4 levels) and nothing
+// else reads the intermediates.
+bool fused_inverse(const std::vector<FwdDesc>& fwd, const Avail& avail, int source_buf, MemoryPool* pool,
+                   void* d_result, size_t capacity, size_t* result_size, cudaStream_t stream) {
+    const FwdDesc* lq = nullptr;
+    for (const auto& d : fwd)
+        if (d.in_ids.size() == 1 && d.in_ids[0] == source_buf) lq = &d;
+    if (!lq || lq->out_ids.size() != 4) return false;
+    auto* lqs = dynamic_cast<LorenzoQuantStage<float, uint16_t>*>(lq->stage);
+    if (!lqs) return false;
+    auto consumers = [&](int buf) {
+        std::vector<const FwdDesc*> v;
+        for (const auto& d : fwd)
+            for (int i : d.in_ids)
+                if (i == buf) v.push_back(&d);
+        return v;
+    };
+    const auto c1 = consumers(lq->out_ids[0]);
+    if (c1.size() != 1 || c1[0]->out_ids.size() != 1) return false;
+    auto* bs = dynamic_cast<BitshuffleStage*>(c1[0]->stage);
+    if (!bs || bs->getBlockSize() != 16384 || bs->getElementWidth() != 2) return false;
+    const auto c2 = consumers(c1[0]->out_ids[0]);
+    if (c2.size() != 1 || c2[0]->out_ids.size() != 1) return false;
+    auto* rz = dynamic_cast<RZEStage*>(c2[0]->stage);
+    if (!rz || rz->getChunkSize() != 16384 || rz->getLevels() != 4) return false;
+    for (int i = 1; i < 4; i++)
+        if (!avail.count(lq->out_ids[i])) return false;
+    if (!avail.count(c2[0]->out_ids[0])) return false;
+    const auto& rze = avail.at(c2[0]->out_ids[0]);
+    const auto& err = avail.at(lq->out_ids[1]);
+    const auto& idx = avail.at(lq->out_ids[2]);
+    const auto& cnt = avail.at(lq->out_ids[3]);
+    const size_t n = rz->getCachedOrigBytes() / sizeof(uint16_t);
+    *result_size = n * sizeof(float);
+    if (n == 0) return true;
+    if (*result_size > capacity) throw std::runtime_error("decompress: output buffer too small");
+    const auto d = lqs->getDims();
+    uint32_t dims[3] = {(uint32_t)d[0], (uint32_t)d[1], (uint32_t)d[2]};
+    const size_t need = fzb_workspace_bytes(n, 0);
+    void* w = pool->allocate(need, stream, "inverse_workspace", false);
+    if (!w) throw std::runtime_error("decompress: workspace allocation failed");
+    const int rc = fzb_lq_bs_rze_decompress(rze.first, rze.second, static_cast<const float*>(err.first),
+                                            static_cast<const uint32_t*>(idx.first),
+                                            static_cast<const uint32_t*>(cnt.first), err.second / sizeof(float), n,
+                                            dims, lqs->computedAbsErrorBound(), lqs->getZigzagCodes() ? 1 : 0,
+                                            static_cast<float*>(d_result), 0, w, need, stream);
+    pool->free(w, stream);
+    if (rc) throw std::runtime_error(std::string("LorenzoQuant<-Bitshuffle<-RZE decompress: ") + fzb_status_string(rc));
+    return true;
+}
+
+// Runs the inverse of every stage in reverse topological order.  d_result
+// receives the source buffer's reconstruction.
+void run_inverse(const std::vector<FwdDesc>& fwd, Avail avail, int source_buf, MemoryPool* pool, void* d_result,
+                 size_t capacity, size_t* result_size, cudaStream_t stream, bool allow_fused) {
+    for (const auto& d : fwd) d.stage->setInverse(true);
+    if (allow_fused && fused_inverse(fwd, avail, source_buf, pool, d_result, capacity, result_size, stream)) {
+        cuda_check(cudaStreamSynchronize(stream), "decompress");
+        return;
+    }
+    std::vector<void*> temps;
+    try {
+        for (auto it = fwd.rbegin(); it != fwd.rend(); ++it) {
+            std::vector<void*> in;
+            std::vector<size_t> sizes;
+            for (int id : it->out_ids) {
+                auto a = avail.find(id);
+                if (a == avail.end())
+                    throw std::runtime_error("decompress: buffer " + std::to_string(id) + " of stage '" +
+                                             it->stage->getName() + "' is not available");
+                void* ptr = a->second.first;
+                // container segments are packed unpadded; the coders read
+                // their headers with word loads, so realign odd starts
+                if ((reinterpret_cast<uintptr_t>(ptr) & 15) && a->second.second) {
+                    void* t = pool->allocate(a->second.second, stream, "inverse_realign", false);
+                    if (!t) throw std::runtime_error("decompress: allocation failed");
+                    temps.push_back(t);
+                    cuda_check(cudaMemcpyAsync(t, ptr, a->second.second, cudaMemcpyDeviceToDevice, stream),
+                               "decompress realign");
+                    ptr = t;
+                }
+                in.push_back(ptr);
+                sizes.push_back(a->second.second);
+            }
+            if (it->in_ids.size() != 1)
+                throw std::runtime_error("decompress: stage '" + it->stage->getName() + "' has " +
+                                         std::to_string(it->in_ids.size()) + " inputs; one is supported");
+            const size_t est = it->stage->estimateOutputSizes(sizes).at(0);
+            void* out = nullptr;
+            if (it->in_ids[0] == source_buf) {
+                if (est > capacity) throw std::runtime_error("decompress: output buffer too small");
+                out = d_result;
+            } else {
+                out = est ? pool->allocate(est, stream, "inverse_intermediate", false) : nullptr;
+                if (est && !out) throw std::runtime_error("decompress: allocation failed");
+                temps.push_back(out);
+            }
+            it->stage->execute(stream, pool, in, {out}, sizes);
+            avail[it->in_ids[0]] = {out, it->stage->getActualOutputSize(0)};
+        }
+        cuda_check(cudaStreamSynchronize(stream), "decompress");
+        for (const auto& d : fwd) d.stage->postStreamSync(stream);
+    } catch (...) {
+        cudaStreamSynchronize(stream);
+        for (void* p : temps) pool->free(p, stream);
+        throw;
+    }
+    for (void* p : temps) pool->free(p, stream);
+    *result_size = avail.at(source_buf).second;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- decompress
+
+void Pipeline::runInverse(const std::unordered_map<int, std::pair<void*, size_t>>& outputs, void* d_result,
+                          size_t capacity, size_t* result_size, cudaStream_t stream) {
+    std::vector<FwdDesc> fwd;
+    for (const auto& lv : dag_->getLevels())
+        for (auto* n : lv) fwd.push_back({n->stage, n->input_buffer_ids, n->output_buffer_ids});
+    for (auto& s : stages_) s->saveState();
+    try {
+        run_inverse(fwd, outputs, input_buffer_id_, pool_.get(), d_result, capacity, result_size, stream, fused_);
+    } catch (...) {
+        for (auto& s : stages_) {
+            s->setInverse(false);
+            s->restoreState();
+        }
+        throw;
+    }
+    for (auto& s : stages_) {
+        s->setInverse(false);
+        s->restoreState();
+    }
+    if (original_input_size_ && *result_size > original_input_size_) *result_size = original_input_size_;
+}
+
+void Pipeline::decompress(const void* d_input, size_t input_size, void** d_output, size_t* output_size,
+                          cudaStream_t stream) {
+    if (!finalized_) throw std::runtime_error("Pipeline not finalized");
+    if (meta_.empty()) throw std::runtime_error("decompress() requires compress() to have been called first");
+    std::unordered_map<int, std::pair<void*, size_t>> outs;
+    size_t off = pad16(4 + 8 * meta_.size());
+    for (const auto& m : meta_) {
+        void* p = dag_->getBuffer(m.buffer_id);
+        if (d_input) {
+            if (meta_.size() == 1) p = const_cast<void*>(d_input);
+            else {
+                p = static_cast<uint8_t*>(const_cast<void*>(d_input)) + off;
+                off += pad16(m.actual_size);
+            }
+        }
+        outs[m.buffer_id] = {p, m.actual_size};
+    }
+    if (d_input && meta_.size() > 1 && off > input_size)
+        throw std::runtime_error("decompress(): input (" + std::to_string(input_size) +
+                                 " bytes) is shorter than the compressed layout (" + std::to_string(off) + " bytes)");
+    const size_t cap = input_size_;  // the source bytes (padded)
+    void* d_final = nullptr;
+    if (pool_managed_decomp_) {
+        for (void* p : decomp_outputs_) pool_->free(p, stream);
+        decomp_outputs_.clear();
+        d_final = pool_->allocate(cap, stream, "decomp_output", true);
+        if (!d_final) throw std::runtime_error("Pool allocation for decompress output failed");
+        decomp_outputs_.push_back(d_final);
+    } else {
+        cuda_check(cudaMalloc(&d_final, cap), "cudaMalloc for decompress output");
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    runInverse(outs, d_final, cap, output_size, stream);
+    const auto t1 = std::chrono::steady_clock::now();
+    *d_output = d_final;
+    last_perf_ = PipelinePerfResult();
+    last_perf_.is_compress = false;
+    last_perf_.input_bytes = input_size;
+    last_perf_.output_bytes = *output_size;
+    last_perf_.host_elapsed_ms = last_perf_.dag_elapsed_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();
+}
+
+void Pipeline::decompress(const void* d_input, size_t input_size, void* d_output_buf, size_t output_buf_capacity,
+                          size_t* actual_output_size, cudaStream_t stream) {
+    if (!finalized_) throw std::runtime_error("Pipeline not finalized");
+    if (meta_.empty()) throw std::runtime_error("decompress() requires compress() to have been called first");
+    if (!d_output_buf) throw std::runtime_error("decompress(): null output buffer");
+    std::unordered_map<int, std::pair<void*, size_t>> outs;
+    size_t off = pad16(4 + 8 * meta_.size());
+    for (const auto& m : meta_) {
+        void* p = dag_->getBuffer(m.buffer_id);
+        if (d_input) {
+            if (meta_.size() == 1) p = const_cast<void*>(d_input);
+            else {
+                p = static_cast<uint8_t*>(const_cast<void*>(d_input)) + off;
+                off += pad16(m.actual_size);
+            }
+        }
+        outs[m.buffer_id] = {p, m.actual_size};
+    }
+    (void)input_size;
+    if (output_buf_capacity >= input_size_) {
+        runInverse(outs, d_output_buf, output_buf_capacity, actual_output_size, stream);
+        return;
+    }
+    // the padded reconstruction does not fit: stage it and copy the prefix
+    void* tmp = pool_->allocate(input_size_, stream, "decomp_stage", false);
+    if (!tmp) throw std::runtime_error("decompress staging allocation failed");
+    size_t sz = 0;
+    try {
+        runInverse(outs, tmp, input_size_, &sz, stream);
+    } catch (...) {
+        pool_->free(tmp, stream);
+        throw;
+    }
+    if (sz > output_buf_capacity) {
+        pool_->free(tmp, stream);
+        throw std::runtime_error("decompress(): output (" + std::to_string(sz) + " bytes) exceeds the buffer capacity");
+    }
+    cuda_check(cudaMemcpyAsync(d_output_buf, tmp, sz, cudaMemcpyDeviceToDevice, stream), "decompress copy-out");
+    pool_->free(tmp, stream);
+    *actual_output_size = sz;
+}
+
+// ----------------------------------------------------------------------- FZM
+
+Pipeline::FZMFileHeader Pipeline::buildHeader() const {
+    if (!finalized_) throw std::runtime_error("Cannot build header before finalization");
+    if (meta_.empty()) throw std::runtime_error("Cannot build header before compress() is called");
+    FZMFileHeader fh;
+    fh.core.uncompressed_size = input_size_;
+    fh.core.num_sources = 1;
+    fh.core.source_uncompressed_sizes[0] = input_size_;
+    for (const auto& lv : dag_->getLevels())
+        for (auto* n : lv) {
+            FZMStageInfo si;
+            si.stage_type = (StageType)n->stage->getStageTypeId();
+            si.stage_version = 1;
+            si.num_inputs = (uint8_t)n->input_buffer_ids.size();
+            si.num_outputs = (uint8_t)n->output_buffer_ids.size();
+            for (size_t i = 0; i < n->input_buffer_ids.size() && i < FZM_MAX_STAGE_INPUTS; i++)
+                si.input_buffer_ids[i] = (uint16_t)n->input_buffer_ids[i];
+            for (size_t i = 0; i < n->output_buffer_ids.size() && i < FZM_MAX_STAGE_OUTPUTS; i++)
+                si.output_buffer_ids[i] = (uint16_t)n->output_buffer_ids[i];
+            if (si.num_outputs) si.config_size = (uint32_t)n->stage->serializeHeader(0, si.stage_config, FZM_STAGE_CONFIG_SIZE);
+            fh.stages.push_back(si);
+        }
+    fh.core.num_stages = (uint32_t)fh.stages.size();
+    fh.core.num_buffers = (uint16_t)meta_.size();
+    uint64_t off = 0;
+    for (const auto& m : meta_) {
+        FZMBufferEntry e;
+        e.stage_type = (StageType)m.producer->stage->getStageTypeId();
+        e.stage_version = 1;
+        e.data_type = (DataType)m.producer->stage->getOutputDataType((size_t)m.output_index);
+        e.producer_output_idx = (uint8_t)m.output_index;
+        e.dag_buffer_id = (uint16_t)m.buffer_id;
+        std::strncpy(e.name, m.name.c_str(), FZM_MAX_NAME_LEN - 1);
+        e.data_size = m.actual_size;
+        e.allocated_size = m.allocated_size;
+        e.uncompressed_size = m.actual_size;
+        e.byte_offset = off;
+        e.config_size = (uint32_t)m.producer->stage->serializeHeader((size_t)m.output_index, e.stage_config,
+                                                                     FZM_STAGE_CONFIG_SIZE);
+        off += m.actual_size;
+        fh.buffers.push_back(e);
+    }
+    fh.core.compressed_size = off;
+    fh.core.header_size = fh.core.computeHeaderSize();
+    return fh;
+}
+
+namespace {
+
+uint32_t header_checksum(const Pipeline::FZMFileHeader& fh) {
+    FZMHeaderCore c = fh.core;
+    c.header_checksum = 0;
+    uint32_t crc = crc32Update(0xFFFFFFFFu, &c, sizeof(c));
+    if (!fh.stages.empty()) crc = crc32Update(crc, fh.stages.data(), fh.stages.size() * sizeof(FZMStageInfo));
+    if (!fh.buffers.empty()) crc = crc32Update(crc, fh.buffers.data(), fh.buffers.size() * sizeof(FZMBufferEntry));
+    return crc ^ 0xFFFFFFFFu;
+}
+
+}  // namespace
+
+void Pipeline::writeToFile(const std::string& filename, cudaStream_t stream) {
+    if (!finalized_) throw std::runtime_error("Cannot write to file before finalization");
+    if (!compressed_) throw std::runtime_error("compress() must be called before writeToFile()");
+    FZMFileHeader fh = buildHeader();
+    std::vector<uint8_t> payload(fh.core.compressed_size);
+    size_t off = 0;
+    for (const auto& m : meta_) {
+        if (m.actual_size)
+            cuda_check(cudaMemcpyAsync(payload.data() + off, dag_->getBuffer(m.buffer_id), m.actual_size,
+                                       cudaMemcpyDeviceToHost, stream),
+                       "cudaMemcpyAsync failed");
+        off += m.actual_size;
+    }
+    cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize failed");
+    fh.core.data_checksum = crc32(payload.data(), payload.size());
+    fh.core.flags |= FZM_FLAG_HAS_DATA_CHECKSUM | FZM_FLAG_HAS_HEADER_CHECKSUM;
+    fh.core.header_checksum = header_checksum(fh);
+    std::ofstream f(filename, std::ios::binary);
+    if (!f) throw std::runtime_error("Failed to open file for writing: " + filename);
+    f.write(reinterpret_cast<const char*>(&fh.core), sizeof(fh.core));
+    if (!fh.stages.empty())
+        f.write(reinterpret_cast<const char*>(fh.stages.data()), fh.stages.size() * sizeof(FZMStageInfo));
+    if (!fh.buffers.empty())
+        f.write(reinterpret_cast<const char*>(fh.buffers.data()), fh.buffers.size() * sizeof(FZMBufferEntry));
+    if (!payload.empty()) f.write(reinterpret_cast<const char*>(payload.data()), payload.size());
+    if (!f) throw std::runtime_error("Failed to write file: " + filename);
+}
+
+Pipeline::FZMFileHeader Pipeline::readHeader(const std::string& filename) {
+    std::ifstream f(filename, std::ios::binary);
+    if (!f) throw std::runtime_error("Failed to open file for reading: " + filename);
+    uint32_t magic = 0;
+    uint16_t version = 0;
+    f.read(reinterpret_cast<char*>(&magic), 4);
+    f.read(reinterpret_cast<char*>(&version), 2);
+    if (!f) throw std::runtime_error("Failed to read header from file: " + filename);
+    if (magic != FZM_MAGIC) throw std::runtime_error("Invalid FZM file format (bad magic number)");
+    const uint8_t major = fzmVersionMajor(version), minor = fzmVersionMinor(version);
+    if (major != FZM_VERSION_MAJOR)
+        throw std::runtime_error("Incompatible FZM major version: file has major " + std::to_string(major) +
+                                 ", reader expects major " + std::to_string(FZM_VERSION_MAJOR));
+    const bool exact = minor == FZM_VERSION_MINOR, legacy = minor == 0;
+    f.seekg(0, std::ios::beg);
+    FZMFileHeader fh;
+    fh.core = FZMHeaderCore();
+    std::memset(static_cast<void*>(&fh.core), 0, sizeof(fh.core));
+    f.read(reinterpret_cast<char*>(&fh.core), legacy ? FZM_LEGACY_HEADER_CORE_SIZE : sizeof(FZMHeaderCore));
+    if (!f) throw std::runtime_error("Failed to read header from file: " + filename);
+    if (fh.core.num_stages > FZM_MAX_BUFFERS || fh.core.num_buffers > FZM_MAX_BUFFERS)
+        throw std::runtime_error("FZM header has too many stages/buffers");
+    fh.stages.resize(fh.core.num_stages);
+    if (fh.core.num_stages) {
+        f.read(reinterpret_cast<char*>(fh.stages.data()), fh.core.num_stages * sizeof(FZMStageInfo));
+        if (!f) throw std::runtime_error("Failed to read stage data from file: " + filename);
+    }
+    fh.buffers.resize(fh.core.num_buffers);
+    if (fh.core.num_buffers) {
+        f.read(reinterpret_cast<char*>(fh.buffers.data()), fh.core.num_buffers * sizeof(FZMBufferEntry));
+        if (!f) throw std::runtime_error("Failed to read buffer data from file: " + filename);
+    }
+    if (!legacy && exact && (fh.core.flags & FZM_FLAG_HAS_HEADER_CHECKSUM)) {
+        const uint32_t got = header_checksum(fh);
+        if (got != fh.core.header_checksum)
+            throw std::runtime_error("FZM header checksum mismatch in '" + filename + "': expected 0x" +
+                                     hex8(fh.core.header_checksum) + ", computed 0x" + hex8(got) +
+                                     " — file may be corrupted");
+    }
+    return fh;
+}
+
+void Pipeline::decompressFromFile(const std::string& filename, void** d_output, size_t* output_size,
+                                  cudaStream_t stream, PipelinePerfResult* perf_out, size_t pool_override_bytes) {
+    const auto t0 = std::chrono::steady_clock::now();
+    FZMFileHeader fh = readHeader(filename);
+    std::vector<uint8_t> payload(fh.core.compressed_size);
+    {
+        std::ifstream f(filename, std::ios::binary);
+        if (!f) throw std::runtime_error("Failed to open file for reading: " + filename);
+        f.seekg((std::streamoff)fh.core.header_size, std::ios::beg);
+        if (!payload.empty()) f.read(reinterpret_cast<char*>(payload.data()), payload.size());
+        if (!f) throw std::runtime_error("Failed to read compressed data from file: " + filename);
+    }
+    if (fh.core.flags & FZM_FLAG_HAS_DATA_CHECKSUM) {
+        const uint32_t got = crc32(payload.data(), payload.size());
+        if (got != fh.core.data_checksum)
+            throw std::runtime_error("FZM data checksum mismatch in '" + filename + "': expected 0x" +
+                                     hex8(fh.core.data_checksum) + ", computed 0x" + hex8(got) +
+                                     " — compressed data may be corrupted");
+    }
+    for (const auto& e : fh.buffers)
+        if (e.byte_offset + e.data_size > fh.core.compressed_size)
+            throw std::runtime_error("FZM buffer '" + std::string(e.name, strnlen(e.name, FZM_MAX_NAME_LEN)) +
+                                     "' lies outside the payload");
+    size_t max_u = fh.core.uncompressed_size;
+    for (const auto& e : fh.buffers) max_u = std::max<size_t>(max_u, e.uncompressed_size);
+    const size_t pool_bytes = pool_override_bytes ? pool_override_bytes
+                                                  : (size_t)fh.core.compressed_size + (size_t)(2.5 * (double)max_u) +
+                                                        (32ull << 20);
+    MemoryPool pool(MemoryPoolConfig(pool_bytes, 1.0f));
+    void* d_payload = nullptr;
+    if (!payload.empty()) {
+        d_payload = pool.allocate(payload.size(), stream, "compressed_data_load", false);
+        if (!d_payload) throw std::runtime_error("allocation for the compressed data failed");
+        cuda_check(cudaMemcpyAsync(d_payload, payload.data(), payload.size(), cudaMemcpyHostToDevice, stream),
+                   "cudaMemcpyAsync failed");
+        cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize failed");
+    }
+    std::vector<std::unique_ptr<Stage>> owned;
+    std::vector<FwdDesc> fwd;
+    std::unordered_set<int> produced;
+    for (const auto& si : fh.stages) {
+        owned.emplace_back(createStage(si.stage_type, si.stage_config, si.config_size));
+        FwdDesc d{owned.back().get(), {}, {}};
+        for (int j = 0; j < si.num_inputs && j < (int)FZM_MAX_STAGE_INPUTS; j++)
+            if (si.input_buffer_ids[j] != 0xFFFF) d.in_ids.push_back(si.input_buffer_ids[j]);
+        for (int j = 0; j < si.num_outputs && j < (int)FZM_MAX_STAGE_OUTPUTS; j++)
+            if (si.output_buffer_ids[j] != 0xFFFF) {
+                d.out_ids.push_back(si.output_buffer_ids[j]);
+                produced.insert(si.output_buffer_ids[j]);
+            }
+        fwd.push_back(d);
+    }
+    int source_buf = -1;
+    for (const auto& d : fwd)
+        for (int id : d.in_ids)
+            if (!produced.count(id) && source_buf < 0) source_buf = id;
+    if (source_buf < 0) {
+        if (d_payload) pool.free(d_payload, stream);
+        throw std::runtime_error("decompressFromFile: could not identify any source stage in topology");
+    }
+    Avail avail;
+    for (const auto& e : fh.buffers)
+        avail[(int)e.dag_buffer_id] = {static_cast<uint8_t*>(d_payload) + e.byte_offset, (size_t)e.data_size};
+    size_t src_bytes = fh.core.num_sources && fh.core.source_uncompressed_sizes[0] ? fh.core.source_uncompressed_sizes[0]
+                                                                                   : fh.core.uncompressed_size;
+    void* d_final = nullptr;
+    cuda_check(cudaMalloc(&d_final, src_bytes ? src_bytes : 1), "cudaMalloc for decompressed output failed");
+    size_t got = 0;
+    const auto t1 = std::chrono::steady_clock::now();
+    try {
+        run_inverse(fwd, avail, source_buf, &pool, d_final, src_bytes, &got, stream, true);
+    } catch (...) {
+        cudaStreamSynchronize(stream);
+        cudaFree(d_final);
+        if (d_payload) pool.free(d_payload, stream);
+        throw;
+    }
+    const auto t2 = std::chrono::steady_clock::now();
+    if (d_payload) pool.free(d_payload, stream);
+    cudaStreamSynchronize(stream);
+    *d_output = d_final;
+    *output_size = got;
+    if (perf_out) {
+        *perf_out = PipelinePerfResult();
+        perf_out->is_compress = false;
+        perf_out->input_bytes = fh.core.compressed_size;
+        perf_out->output_bytes = got;
+        perf_out->dag_elapsed_ms = std::chrono::duration<float, std::milli>(t2 - t1).count();
+        perf_out->host_elapsed_ms = std::chrono::duration<float, std::milli>(t2 - t0).count();
+    }
+}
+
+}  // namespace fz

@@ -61,8 +61,10 @@ _default_ws = Workspace()
 
 
 def max_outliers(n: int, capacity: float) -> int:
-    """LorenzoQuantStage::getMaxOutlierCount (lorenzo_quant.h)."""
-    return int(math.ceil(n * float(capacity)))
+    """LorenzoQuantStage::getMaxOutlierCount (lorenzo_quant.h:333-335):
+    ceil(n * capacity) evaluated in single precision."""
+    import numpy as np
+    return int(math.ceil(float(np.float32(n) * np.float32(capacity))))
 
 
 def lq_forward(x: torch.Tensor, dims, eb: float, mode: int = ABS, radius: int = 32768,

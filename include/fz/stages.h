@@ -1,0 +1,474 @@
+// fz/stages.h -- the hot-path stages behind the fz::Stage interface, with
+// the reference's class names, setters, output names and container headers
+// (modules/fused/lorenzo_quant/lorenzo_quant.h, shufflers/bitshuffle/
+// bitshuffle_stage.h, coders/rze/rze_stage.h, coders/rle/rle.h,
+// coders/huffman/huffman_stage.h, coders/bitpack/bitpack_stage.h).  Every
+// stage runs the sm_100a kernels of libfzb through the C ABI in fzb.h; errors
+// are thrown as std::runtime_error, as the reference does.
+#pragma once
+
+#include <array>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <unordered_map>
+#include <vector>
+
+#include "fz/mempool.h"
+#include "fz/stage.h"
+
+namespace fz {
+
+// Device workspace owned by a stage, drawn from the pipeline's pool (or
+// cudaMalloc when the stage runs without a pool) and grown on demand.
+class StageWorkspace {
+public:
+    StageWorkspace() = default;
+    ~StageWorkspace();
+    StageWorkspace(const StageWorkspace&) = delete;
+    StageWorkspace& operator=(const StageWorkspace&) = delete;
+    void* ensure(size_t bytes, MemoryPool* pool, cudaStream_t stream);
+    size_t size() const { return bytes_; }
+    void* get() const { return ptr_; }
+    // Throws when a kernel latched an error (malformed input, a bounded
+    // wait that gave up) in this workspace; clears it.
+    void checkStatus(cudaStream_t stream, const char* what) const;
+
+private:
+    void release();
+    void* ptr_ = nullptr;
+    size_t bytes_ = 0;
+    MemoryPool* pool_ = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// LorenzoQuant (1/2/3-D predict + quantize), float -> uint16 codes + outliers.
+// ---------------------------------------------------------------------------
+enum class ErrorBoundMode : uint8_t { ABS = 0, REL = 1, NOA = 2 };
+
+// 44-byte container record (lorenzo_quant.h:43-67).
+struct LorenzoQuantConfig {
+    float error_bound;       // absolute bound used by the decompressor
+    uint32_t quant_radius;
+    uint32_t num_elements;
+    uint32_t outlier_count;  // stored outliers
+    DataType input_type;
+    DataType code_type;
+    uint8_t ndim;
+    uint8_t eb_mode;
+    uint32_t dim_x;
+    uint32_t dim_y;
+    uint32_t dim_z;
+    float user_eb;
+    float value_base;
+    uint8_t zigzag_codes;
+    uint8_t reserved[3];
+    LorenzoQuantConfig()
+        : error_bound(0.0f), quant_radius(0), num_elements(0), outlier_count(0),
+          input_type(DataType::FLOAT32), code_type(DataType::UINT16), ndim(1), eb_mode(0), dim_x(0),
+          dim_y(1), dim_z(1), user_eb(0.0f), value_base(0.0f), zigzag_codes(0), reserved{0, 0, 0} {}
+};
+static_assert(sizeof(LorenzoQuantConfig) == 44, "LorenzoQuantConfig is 44 bytes");
+
+template <typename TInput = float, typename TCode = uint16_t>
+class LorenzoQuantStage : public Stage {
+    static_assert(std::is_same<TInput, float>::value && std::is_same<TCode, uint16_t>::value,
+                  "the sm_100a kernels implement LorenzoQuantStage<float, uint16_t>");
+
+public:
+    struct Config {
+        float error_bound = 1e-3f;
+        int quant_radius = 32768;
+        float outlier_capacity = 0.2f;
+        std::array<size_t, 3> dims = {0, 1, 1};  // {x, y, z}, x fastest; x = 0 infers x
+        ErrorBoundMode eb_mode = ErrorBoundMode::ABS;
+        float precomputed_value_base = 0.0f;  // > 0 skips the REL/NOA scan
+        bool zigzag_codes = false;
+        Config() = default;
+        Config(TInput eb, TCode radius = 32768, float outlier_cap = 0.2f, std::array<size_t, 3> d = {0, 1, 1})
+            : error_bound(eb), quant_radius(radius), outlier_capacity(outlier_cap), dims(d) {}
+    };
+
+    explicit LorenzoQuantStage(const Config& config = Config());
+
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    void postStreamSync(cudaStream_t stream) override;
+    void onGraphReplay(cudaStream_t) override { pending_ = !is_inverse_ && d_count_ != nullptr; }
+
+    std::string getName() const override { return "LorenzoQuant"; }
+    size_t getNumInputs() const override { return is_inverse_ ? 4 : 1; }
+    size_t getNumOutputs() const override { return is_inverse_ ? 1 : 4; }
+    std::vector<std::string> getOutputNames() const override {
+        return {"codes", "outlier_errors", "outlier_indices", "outlier_count"};
+    }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& input_sizes) const override;
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override;
+    size_t getActualOutputSize(int index) const override {
+        return (index >= 0 && index < (int)actual_.size()) ? actual_[index] : 0;
+    }
+    size_t getExecuteTimeOutputSize(int index) const override {
+        if (is_inverse_) return getActualOutputSize(index);
+        return (index >= 0 && index < (int)at_execute_.size()) ? at_execute_[index] : 0;
+    }
+    void saveState() override { saved_ = actual_; }
+    void restoreState() override { actual_ = saved_; }
+
+    void setErrorBound(TInput eb) { config_.error_bound = eb; }
+    void setQuantRadius(TCode radius) { config_.quant_radius = radius; }
+    void setOutlierCapacity(float capacity) { config_.outlier_capacity = capacity; }
+    void setDims(const std::array<size_t, 3>& dims) override { config_.dims = dims; }
+    void setDims(size_t x, size_t y = 1, size_t z = 1) { config_.dims = {x, y, z}; }
+    void setErrorBoundMode(ErrorBoundMode mode) { config_.eb_mode = mode; }
+    void setValueBase(float value_base) { config_.precomputed_value_base = value_base; }
+    void setZigzagCodes(bool enable) { config_.zigzag_codes = enable; }
+    TInput getErrorBound() const { return config_.error_bound; }
+    TCode getQuantRadius() const { return (TCode)config_.quant_radius; }
+    float getOutlierCapacity() const { return config_.outlier_capacity; }
+    std::array<size_t, 3> getDims() const { return config_.dims; }
+    ErrorBoundMode getErrorBoundMode() const { return config_.eb_mode; }
+    float getValueBase() const { return config_.precomputed_value_base; }
+    bool getZigzagCodes() const { return config_.zigzag_codes; }
+    int ndim() const { return config_.dims[2] > 1 ? 3 : (config_.dims[1] > 1 ? 2 : 1); }
+    void setInverse(bool inverse) override { is_inverse_ = inverse; }
+    bool isInverse() const override { return is_inverse_; }
+
+    uint16_t getStageTypeId() const override { return (uint16_t)StageType::LORENZO_QUANT; }
+    uint8_t getOutputDataType(size_t i) const override;
+    uint8_t getInputDataType(size_t) const override { return (uint8_t)DataType::FLOAT32; }
+    size_t serializeHeader(size_t output_index, uint8_t* buf, size_t max_size) const override;
+    void deserializeHeader(const uint8_t* buf, size_t size) override;
+    size_t getMaxHeaderSize(size_t) const override { return sizeof(LorenzoQuantConfig); }
+
+    // ceil(n * outlier_capacity) in single precision, as the reference
+    // computes it (lorenzo_quant.h:333-335).
+    size_t getMaxOutlierCount(size_t num_elements) const;
+    float computedAbsErrorBound() const { return computed_abs_eb_; }
+    float computedValueBase() const { return computed_value_base_; }
+
+    // The fused LorenzoQuant -> Bitshuffle -> RZE path runs this stage's
+    // forward kernel itself; it reports back what execute() would record.
+    void fusedForward(cudaStream_t stream, MemoryPool* pool, const void* d_in, size_t in_bytes,
+                      void* d_err, void* d_idx, void* d_count, void* d_rze, uint64_t* d_rze_size);
+
+private:
+    void* forwardWorkspace(size_t n, size_t cap, MemoryPool* pool, cudaStream_t stream);
+    Config config_;
+    bool is_inverse_ = false;
+    std::vector<size_t> actual_, saved_, at_execute_;
+    size_t num_elements_ = 0;
+    uint32_t actual_outlier_count_ = 0;
+    float computed_abs_eb_ = 0.0f;
+    float computed_value_base_ = 0.0f;
+    const void* d_count_ = nullptr;  // pending read-back (forward)
+    float* d_eb_state_ = nullptr;    // inside the workspace
+    bool pending_ = false;
+    StageWorkspace ws_;
+};
+
+// ---------------------------------------------------------------------------
+// Bitshuffle (bit-plane transpose per block), size-preserving.
+// ---------------------------------------------------------------------------
+class BitshuffleStage : public Stage {
+public:
+    BitshuffleStage() = default;
+    void setInverse(bool inv) override { is_inverse_ = inv; }
+    bool isInverse() const override { return is_inverse_; }
+    void setBlockSize(size_t bytes) { block_size_ = (uint32_t)bytes; }
+    void setElementWidth(size_t bytes) { element_width_ = (uint8_t)bytes; }
+    size_t getBlockSize() const { return block_size_; }
+    size_t getElementWidth() const { return element_width_; }
+    size_t getRequiredInputAlignment() const override { return block_size_; }
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    std::string getName() const override { return "Bitshuffle"; }
+    size_t getNumInputs() const override { return 1; }
+    size_t getNumOutputs() const override { return 1; }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& s) const override { return {s[0]}; }
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override {
+        return {{"output", actual_}};
+    }
+    size_t getActualOutputSize(int index) const override { return index == 0 ? actual_ : 0; }
+    uint16_t getStageTypeId() const override { return (uint16_t)StageType::BITSHUFFLE; }
+    uint8_t getOutputDataType(size_t) const override { return (uint8_t)DataType::UINT8; }
+    // bitshuffle_stage.h:98-106: [u32 block_size][u8 element_width]
+    size_t serializeHeader(size_t, uint8_t* buf, size_t max_size) const override;
+    void deserializeHeader(const uint8_t* buf, size_t size) override;
+    size_t getMaxHeaderSize(size_t) const override { return 5; }
+    void saveState() override { saved_ = {block_size_, element_width_, actual_}; }
+    void restoreState() override {
+        block_size_ = saved_.block;
+        element_width_ = saved_.ew;
+        actual_ = saved_.actual;
+    }
+    void markFused(size_t bytes) { actual_ = bytes; }
+
+private:
+    struct Saved {
+        uint32_t block = 0;
+        uint8_t ew = 0;
+        size_t actual = 0;
+    };
+    bool is_inverse_ = false;
+    uint32_t block_size_ = 16384;
+    uint8_t element_width_ = 4;  // the reference's default; the path uses 2
+    size_t actual_ = 0;
+    Saved saved_;
+};
+
+// ---------------------------------------------------------------------------
+// RZE (recursive zero-byte elimination over 16 KiB chunks, 4 levels).
+// ---------------------------------------------------------------------------
+class RZEStage : public Stage {
+public:
+    RZEStage() = default;
+    void setInverse(bool inv) override { is_inverse_ = inv; }
+    bool isInverse() const override { return is_inverse_; }
+    bool isGraphCompatible() const override { return !is_inverse_; }
+    void setChunkSize(size_t bytes) { chunk_size_ = (uint32_t)bytes; }
+    void setLevels(int n) { levels_ = (uint8_t)n; }
+    size_t getChunkSize() const { return chunk_size_; }
+    int getLevels() const { return levels_; }
+    uint32_t getCachedOrigBytes() const { return cached_orig_bytes_; }
+    size_t getRequiredInputAlignment() const override { return chunk_size_; }
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    void postStreamSync(cudaStream_t stream) override;
+    void onGraphReplay(cudaStream_t stream) override {
+        if (is_inverse_ || !last_size_) return;
+        d_size_ = last_size_;
+        pending_stream_ = stream;
+    }
+    std::string getName() const override { return "RZE"; }
+    size_t getNumInputs() const override { return 1; }
+    size_t getNumOutputs() const override { return 1; }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& s) const override;
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override {
+        readBack();
+        return {{"output", actual_}};
+    }
+    size_t getActualOutputSize(int index) const override {
+        readBack();
+        return index == 0 ? actual_ : 0;
+    }
+    uint16_t getStageTypeId() const override { return (uint16_t)StageType::RZE; }
+    uint8_t getOutputDataType(size_t) const override { return (uint8_t)DataType::UINT8; }
+    // rze_stage.h:175-184: [u32 chunk_size][u8 levels][u32 original bytes]
+    size_t serializeHeader(size_t, uint8_t* buf, size_t max_size) const override;
+    void deserializeHeader(const uint8_t* buf, size_t size) override;
+    size_t getMaxHeaderSize(size_t) const override { return 9; }
+    size_t estimateScratchBytes(const std::vector<size_t>& s) const override;
+    void saveState() override { saved_ = {chunk_size_, levels_, cached_orig_bytes_}; }
+    void restoreState() override {
+        chunk_size_ = saved_.chunk;
+        levels_ = saved_.levels;
+        cached_orig_bytes_ = saved_.orig;
+    }
+    // Result of the fused path: the stream size lands in *d_size.
+    void markFused(size_t in_bytes, const uint64_t* d_size, cudaStream_t stream);
+
+private:
+    void readBack() const;
+    struct Saved {
+        uint32_t chunk = 0;
+        uint8_t levels = 0;
+        uint32_t orig = 0;
+    };
+    bool is_inverse_ = false;
+    uint32_t chunk_size_ = 16384;
+    uint8_t levels_ = 4;
+    uint32_t cached_orig_bytes_ = 0;
+    mutable size_t actual_ = 0;
+    mutable const uint64_t* d_size_ = nullptr;  // pending read-back
+    const uint64_t* last_size_ = nullptr;       // where the last forward run writes its size
+    mutable cudaStream_t pending_stream_ = nullptr;
+    Saved saved_;
+    StageWorkspace ws_;
+    uint64_t* d_size_own_ = nullptr;  // inside ws_
+};
+
+// ---------------------------------------------------------------------------
+// RLE: [u32 runs][values, padded to 4 B][u32 lengths].
+// ---------------------------------------------------------------------------
+template <typename T>
+class RLEStage : public Stage {
+    static_assert(std::is_same<T, uint8_t>::value || std::is_same<T, uint16_t>::value ||
+                      std::is_same<T, uint32_t>::value || std::is_same<T, int32_t>::value,
+                  "RLEStage element types: uint8_t, uint16_t, uint32_t, int32_t");
+
+public:
+    RLEStage() = default;
+    void setInverse(bool inv) override { is_inverse_ = inv; }
+    bool isInverse() const override { return is_inverse_; }
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    void postStreamSync(cudaStream_t stream) override;
+    void onGraphReplay(cudaStream_t stream) override {
+        if (is_inverse_ || !last_size_) return;
+        d_size_ = last_size_;
+        pending_stream_ = stream;
+    }
+    std::string getName() const override { return "RLE"; }
+    size_t getNumInputs() const override { return 1; }
+    size_t getNumOutputs() const override { return 1; }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& s) const override;
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override {
+        readBack();
+        return {{"output", actual_}};
+    }
+    size_t getActualOutputSize(int index) const override {
+        readBack();
+        return index == 0 ? actual_ : 0;
+    }
+    uint16_t getStageTypeId() const override { return (uint16_t)StageType::RLE; }
+    uint8_t getOutputDataType(size_t) const override { return (uint8_t)dtype(); }
+    uint8_t getInputDataType(size_t) const override { return (uint8_t)dtype(); }
+    // rle.h:123-131: [u8 data type][u32 element count]
+    size_t serializeHeader(size_t, uint8_t* buf, size_t max_size) const override;
+    void deserializeHeader(const uint8_t* buf, size_t size) override;
+    size_t getMaxHeaderSize(size_t) const override { return 5; }
+    size_t estimateScratchBytes(const std::vector<size_t>& s) const override {
+        if (is_inverse_ || s.empty()) return 0;
+        return (s[0] / sizeof(T)) * (1 + 4 + 4 + sizeof(T) + 4);
+    }
+    static DataType dtype();
+
+private:
+    void readBack() const;
+    bool is_inverse_ = false;
+    uint32_t cached_num_elements_ = 0;
+    mutable size_t actual_ = 0;
+    mutable const uint64_t* d_size_ = nullptr;
+    const uint64_t* last_size_ = nullptr;
+    mutable cudaStream_t pending_stream_ = nullptr;
+    StageWorkspace ws_;
+};
+
+// ---------------------------------------------------------------------------
+// PHF Huffman (coarse mode) over 16-bit symbols.
+// ---------------------------------------------------------------------------
+enum class HuffmanEncodeMode { Coarse, Fine };
+
+template <typename T>
+class HuffmanStage : public Stage {
+    static_assert(std::is_same<T, uint16_t>::value, "the sm_100a Huffman coder implements uint16_t symbols");
+
+public:
+    HuffmanStage() = default;
+    void setBklen(uint32_t bklen) { bklen_ = bklen; }
+    uint32_t getBklen() const { return bklen_; }
+    // Fine mode is not built; setting it keeps the coarse format.
+    void setEncodeMode(HuffmanEncodeMode mode) { encode_mode_ = mode; }
+    HuffmanEncodeMode getEncodeMode() const { return encode_mode_; }
+    void setInverse(bool inv) override { is_inverse_ = inv; }
+    bool isInverse() const override { return is_inverse_; }
+    bool isGraphCompatible() const override { return false; }
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    void postStreamSync(cudaStream_t stream) override {
+        if (is_inverse_) ws_.checkStatus(stream, "HuffmanStage (inverse)");
+    }
+    std::string getName() const override { return "Huffman"; }
+    size_t getNumInputs() const override { return 1; }
+    size_t getNumOutputs() const override { return 1; }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& s) const override {
+        if (s.empty()) return {0};
+        return {is_inverse_ ? original_len_ * sizeof(T) : s[0] * 2 + 4096};
+    }
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override {
+        return {{"output", actual_}};
+    }
+    size_t getActualOutputSize(int index) const override { return index == 0 ? actual_ : 0; }
+    uint16_t getStageTypeId() const override { return (uint16_t)StageType::HUFFMAN; }
+    uint8_t getOutputDataType(size_t) const override { return (uint8_t)DataType::UNKNOWN; }
+    uint8_t getInputDataType(size_t) const override { return (uint8_t)DataType::UNKNOWN; }
+    // huffman_stage.h:174-183: [u8 data type][u16 bklen][u64 element count]
+    size_t serializeHeader(size_t, uint8_t* buf, size_t max_size) const override;
+    void deserializeHeader(const uint8_t* buf, size_t size) override;
+    size_t getMaxHeaderSize(size_t) const override { return 11; }
+    void saveState() override { saved_ = {bklen_, original_len_, actual_}; }
+    void restoreState() override {
+        bklen_ = saved_.bklen;
+        original_len_ = saved_.len;
+        actual_ = saved_.actual;
+    }
+
+private:
+    struct Saved {
+        uint32_t bklen = 1024;
+        uint64_t len = 0;
+        size_t actual = 0;
+    };
+    bool is_inverse_ = false;
+    uint32_t bklen_ = 1024;
+    HuffmanEncodeMode encode_mode_ = HuffmanEncodeMode::Coarse;
+    uint64_t original_len_ = 0;
+    size_t actual_ = 0;
+    Saved saved_;
+    StageWorkspace ws_;
+};
+
+// ---------------------------------------------------------------------------
+// Bitpack: low nbits of each element, nbits a power of two (or detected).
+// ---------------------------------------------------------------------------
+template <typename T>
+class BitpackStage : public Stage {
+    static_assert(std::is_same<T, uint8_t>::value || std::is_same<T, uint16_t>::value ||
+                      std::is_same<T, uint32_t>::value,
+                  "BitpackStage: T must be uint8_t, uint16_t or uint32_t");
+
+public:
+    BitpackStage() = default;
+    void setInverse(bool inv) override { is_inverse_ = inv; }
+    bool isInverse() const override { return is_inverse_; }
+    void setNBits(uint8_t nbits);
+    uint8_t getNBits() const { return nbits_; }
+    void setAutoDetect(bool enable) { auto_detect_ = enable; }
+    bool isAutoDetect() const { return auto_detect_; }
+    bool isGraphCompatible() const override { return !auto_detect_; }
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    std::string getName() const override { return "Bitpack"; }
+    size_t getNumInputs() const override { return 1; }
+    size_t getNumOutputs() const override { return 1; }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& s) const override;
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override {
+        return {{"output", actual_}};
+    }
+    size_t getActualOutputSize(int index) const override { return index == 0 ? actual_ : 0; }
+    uint16_t getStageTypeId() const override { return (uint16_t)StageType::BITPACK; }
+    uint8_t getOutputDataType(size_t) const override { return (uint8_t)DataType::UNKNOWN; }
+    uint8_t getInputDataType(size_t) const override { return (uint8_t)DataType::UNKNOWN; }
+    // bitpack_stage.h:160-168: [u8 data type][u8 nbits][u64 element count]
+    size_t serializeHeader(size_t, uint8_t* buf, size_t max_size) const override;
+    void deserializeHeader(const uint8_t* buf, size_t size) override;
+    size_t getMaxHeaderSize(size_t) const override { return 10; }
+    void saveState() override { saved_ = {nbits_, num_elements_, actual_}; }
+    void restoreState() override {
+        nbits_ = saved_.nbits;
+        num_elements_ = saved_.n;
+        actual_ = saved_.actual;
+    }
+
+private:
+    struct Saved {
+        uint8_t nbits = 8 * sizeof(T);
+        uint64_t n = 0;
+        size_t actual = 0;
+    };
+    bool is_inverse_ = false;
+    bool auto_detect_ = false;
+    uint8_t nbits_ = 8 * sizeof(T);
+    uint64_t num_elements_ = 0;
+    size_t actual_ = 0;
+    Saved saved_;
+    StageWorkspace ws_;
+};
+
+// Rebuilds a stage from its container record (stage_factory.h:36-...).  The
+// stage types of this library's path are supported; others throw.
+Stage* createStage(StageType type, const uint8_t* config, size_t config_size);
+
+}  // namespace fz

@@ -174,7 +174,8 @@ int fzb_bitpack_decode(const void* d_in, uint64_t n, int elem, int nbits, void* 
  * int entry[32], u16 keys[bklen]][u32 par_nbit x pardeg][u32 par_entry x
  * pardeg][u32 bitstream x total_ncell], pardeg = ceil(n / 768).  Header bytes
  * 64..127 and the upper 16 bits of the first word are written as zero (the
- * reference leaves encoder scratch there).  bklen is 1..65535. */
+ * reference leaves encoder scratch there).  bklen is even, 2..65534, so every
+ * u32 table of the blob stays 4-byte aligned. */
 size_t fzb_huff_workspace_bytes(uint64_t n, uint32_t bklen);
 uint64_t fzb_huff_max_bytes(uint64_t n, uint32_t bklen);
 
@@ -203,11 +204,70 @@ int fzb_huff_compress(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_
                       uint64_t* d_out_size, void* d_work, size_t work_bytes, void* stream);
 
 /* HuffmanStage<uint16_t> inverse (phf/hf_kernels.cu:267-298): decodes the blob
- * (8-byte aligned) into n symbols.  A header that disagrees with n / bklen or a
+ * (4-byte aligned) into n symbols.  A header that disagrees with n / bklen or a
  * bitstream that does not decode to exactly n symbols is reported as
  * FZB_E_MALFORMED by fzb_workspace_status(); work_bytes >= 256. */
 int fzb_huff_decode(const void* d_in, uint64_t in_bytes, uint64_t n, uint32_t bklen, uint16_t* d_out,
                     void* d_work, size_t work_bytes, void* stream);
+
+/* Pipeline output concatenation (the reference's Pipeline::concatOutputs,
+ * src/pipeline/compressor.cpp:760-875; layout pipeline_utils.h:35-46):
+ * [u32 n][u64 size_i x n] padded to 16 bytes, then segment i padded to 16
+ * bytes, pad bytes zero.  d_out 16-byte aligned, fzb_concat_bytes() long;
+ * d_srcs and sizes are host arrays of n <= FZB_CONCAT_MAX_SEGMENTS. */
+#define FZB_CONCAT_MAX_SEGMENTS 32
+uint64_t fzb_concat_bytes(const uint64_t* sizes, int n);
+int fzb_concat(const void* const* d_srcs, const uint64_t* sizes, int n, void* d_out, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Pipelines: C view of fz::Pipeline (include/fz/pipeline.h), the reference's
+ * Pipeline API (include/pipeline/compressor.h:34-386) for bindings without
+ * C++ interop.  A pipeline is an opaque handle; stages are the indices the
+ * fzb_pipeline_add_* calls return (>= 0).  Errors raised inside the
+ * pipeline return FZB_E_PIPELINE, with the message from fzb_last_error() on
+ * the same thread.  Unlike the kernel entry points these may allocate
+ * (from the pipeline's memory pool) and synchronise, as the reference's do.
+ * ------------------------------------------------------------------------ */
+#define FZB_E_PIPELINE (-8)    /* a pipeline call failed; see fzb_last_error() */
+#define FZB_MINIMAL 0          /* MemoryStrategy::MINIMAL */
+#define FZB_PREALLOCATE 1      /* MemoryStrategy::PREALLOCATE */
+const char* fzb_last_error(void);
+void* fzb_pipeline_create(uint64_t input_hint, int strategy, float pool_multiplier);
+void fzb_pipeline_destroy(void* pipeline);
+int fzb_pipeline_set_dims(void* pipeline, uint64_t x, uint64_t y, uint64_t z);
+/* addStage<LorenzoQuantStage<float,uint16_t>> with Config fields. */
+int fzb_pipeline_add_lorenzo_quant(void* pipeline, float eb, int eb_mode, int radius, float outlier_capacity,
+                                   int zigzag, float value_base);
+int fzb_pipeline_add_bitshuffle(void* pipeline, uint32_t block_size, int element_width);
+int fzb_pipeline_add_rze(void* pipeline, uint32_t chunk_size, int levels);
+int fzb_pipeline_add_rle(void* pipeline, int elem);
+int fzb_pipeline_add_huffman(void* pipeline, uint32_t bklen);
+int fzb_pipeline_add_bitpack(void* pipeline, int elem, int nbits);   /* nbits 0 = setAutoDetect */
+/* connect(dependent, producer, output_name); returns the buffer id. */
+int fzb_pipeline_connect(void* pipeline, int dependent, int producer, const char* output_name);
+/* Fusion of LorenzoQuant -> Bitshuffle -> RZE into one pass (default on). */
+int fzb_pipeline_set_fusion(void* pipeline, int on);
+int fzb_pipeline_enable_graph_mode(void* pipeline, int on);
+int fzb_pipeline_enable_profiling(void* pipeline, int on);
+int fzb_pipeline_finalize(void* pipeline);
+int fzb_pipeline_is_fused(void* pipeline);
+int fzb_pipeline_capture_graph(void* pipeline, void* stream);
+/* compress (pool-owned output, valid until the next compress). */
+int fzb_pipeline_compress(void* pipeline, const void* d_in, uint64_t bytes, void** d_out, uint64_t* out_bytes,
+                          void* stream);
+/* decompress (pool-owned output; d_in NULL = the pipeline's last outputs). */
+int fzb_pipeline_decompress(void* pipeline, const void* d_in, uint64_t bytes, void** d_out, uint64_t* out_bytes,
+                            void* stream);
+int fzb_pipeline_decompress_into(void* pipeline, const void* d_in, uint64_t bytes, void* d_out, uint64_t capacity,
+                                 uint64_t* out_bytes, void* stream);
+/* Per-stage milliseconds of the last profiled compress (enableProfiling);
+ * returns the number of entries written. */
+int fzb_pipeline_stage_timings(void* pipeline, double* ms, int max_entries);
+/* writeToFile: FZM v3.1 with CRC32 checksums (src/pipeline/compressor_io.cpp:178-265). */
+int fzb_pipeline_write_file(void* pipeline, const char* path, void* stream);
+/* Pipeline::decompressFromFile: *d_out is cudaMalloc'd; release it with fzb_free. */
+int fzb_decompress_file(const char* path, void** d_out, uint64_t* out_bytes, void* stream);
+int fzb_free(void* d_ptr);
 
 #ifdef __cplusplus
 }
