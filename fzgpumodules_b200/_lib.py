@@ -76,6 +76,14 @@ def lib():
         L.fzb_concat_bytes.argtypes = [p, i32]
         L.fzb_concat.restype = i32
         L.fzb_concat.argtypes = [p, p, i32, p, p]
+        L.fzb_batch_workspace_bytes.restype = sz
+        L.fzb_batch_workspace_bytes.argtypes = [p, i32]
+        L.fzb_batch_create.restype = p
+        L.fzb_batch_create.argtypes = [p, i32, p, p, sz, p]
+        L.fzb_batch_launch.argtypes = [p, p]
+        L.fzb_batch_destroy.restype = None
+        L.fzb_batch_destroy.argtypes = [p]
+        L.fzb_batch_autotune.argtypes = [p, i32, p, sz, p, p, p]
         L.fzb_last_error.restype = C.c_char_p
         L.fzb_last_error.argtypes = []
         L.fzb_pipeline_create.restype = p

@@ -2,6 +2,7 @@
 // argument checking, workspace carving and kernel launches; no allocation.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -155,6 +156,59 @@ int resolve_eb(const float* d_in, uint64_t n_total, float eb, int mode, float va
     return FZB_OK;
 }
 
+// Chunk-kernel arguments of one field whose workspace is `w`.
+FwdArgs fwd_args(const Geometry& g, const Work& w, const float* d_in, uint64_t n_total, float* d_eb_state,
+                 uint32_t radius, int zigzag, uint16_t* d_codes, uint64_t cap) {
+    FwdArgs a{};
+    a.in = d_in;
+    a.n_total = (uint32_t)n_total;
+    a.nfield = g.nfield;
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.nz = g.nz;
+    a.plane = g.nx * g.ny;
+    a.ebx2_r = d_eb_state + 2;
+    a.radius = (float)(uint16_t)radius;  // the kernel compares against TCode(radius)
+    a.zigzag = zigzag;
+    a.two_piece = (g.ndim >= 2 && g.nx > (uint32_t)kChunkCodes) ? 1 : 0;
+    a.codes = d_codes;
+    a.n_chunks = (uint32_t)chunks_of(n_total);
+    a.slots = reinterpret_cast<uint8_t*>(w.codes);
+    a.sizes = w.sizes;
+    a.ocnt = w.ocnt;
+    a.obase = w.obase;
+    a.ostage_ctr = w.ostage_ctr;
+    a.ostage_err = w.ostage_err;
+    a.ostage_idx = w.ostage_idx;
+    a.ostage_cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
+    a.err = w.err;
+    return a;
+}
+
+// Assembly arguments matching fwd_args().
+AsmArgs asm_args(const Work& w, const FwdArgs& a, bool fused, void* d_rze, uint64_t* d_rze_size, float* d_err,
+                 uint32_t* d_idx, uint32_t* d_count) {
+    AsmArgs m{};
+    m.slots = a.slots;
+    m.sizes = fused ? w.sizes : nullptr;
+    m.n_chunks = a.n_chunks;
+    m.orig_bytes = 2u * a.n_total;
+    m.out = static_cast<uint8_t*>(d_rze);
+    m.out_size = reinterpret_cast<unsigned long long*>(d_rze_size);
+    m.pay_off = w.in_off;
+    m.ocnt = w.ocnt;
+    m.obase = w.obase;
+    m.ofin = w.ostart;
+    m.ostage_err = w.ostage_err;
+    m.ostage_idx = w.ostage_idx;
+    m.ostage_cap = a.ostage_cap;
+    m.out_err = d_err;
+    m.out_idx = d_idx;
+    m.cap = a.ostage_cap;
+    m.out_count = d_count;
+    return m;
+}
+
 int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32_t dims[3],
                    float eb, int eb_mode, float value_base, uint32_t radius, int zigzag,
                    uint16_t* d_codes, float* d_err, uint32_t* d_idx, uint64_t cap,
@@ -173,29 +227,7 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
     rc = resolve_eb(d_in, n_total, eb, eb_mode, value_base, w, d_eb_state, s);
     if (rc) return rc;
-    FwdArgs a{};
-    a.in = d_in;
-    a.n_total = (uint32_t)n_total;
-    a.nfield = g.nfield;
-    a.nx = g.nx;
-    a.ny = g.ny;
-    a.nz = g.nz;
-    a.plane = g.nx * g.ny;
-    a.ebx2_r = d_eb_state + 2;
-    a.radius = (float)(uint16_t)radius;  // the kernel compares against TCode(radius)
-    a.zigzag = zigzag;
-    a.two_piece = (g.ndim >= 2 && g.nx > (uint32_t)kChunkCodes) ? 1 : 0;
-    a.codes = d_codes;
-    a.n_chunks = (uint32_t)nch;
-    a.slots = reinterpret_cast<uint8_t*>(w.codes);
-    a.sizes = w.sizes;
-    a.ocnt = w.ocnt;
-    a.obase = w.obase;
-    a.ostage_ctr = w.ostage_ctr;
-    a.ostage_err = w.ostage_err;
-    a.ostage_idx = w.ostage_idx;
-    a.ostage_cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
-    a.err = w.err;
+    const FwdArgs a = fwd_args(g, w, d_in, n_total, d_eb_state, radius, zigzag, d_codes, cap);
     const uint32_t nx = g.nx;
     const bool slab = fused && g.ndim == 3 && nx >= 32 && nx <= 1024 && (nx & (nx - 1)) == 0 &&
                       g.ny % ((uint32_t)kChunkCodes / nx) == 0 && g.nfield == n_total &&
@@ -211,24 +243,7 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
         rc = launch_lq(g, fused, a, lq_smem_bytes(g, fused), (uint32_t)nch, s);
     }
     if (rc) return rc;
-    AsmArgs m{};
-    m.slots = a.slots;
-    m.sizes = fused ? w.sizes : nullptr;
-    m.n_chunks = (uint32_t)nch;
-    m.orig_bytes = (uint32_t)(2 * n_total);
-    m.out = static_cast<uint8_t*>(d_rze);
-    m.out_size = reinterpret_cast<unsigned long long*>(d_rze_size);
-    m.pay_off = w.in_off;
-    m.ocnt = w.ocnt;
-    m.obase = w.obase;
-    m.ofin = w.ostart;
-    m.ostage_err = w.ostage_err;
-    m.ostage_idx = w.ostage_idx;
-    m.ostage_cap = a.ostage_cap;
-    m.out_err = d_err;
-    m.out_idx = d_idx;
-    m.cap = a.ostage_cap;
-    m.out_count = d_count;
+    const AsmArgs m = asm_args(w, a, fused, d_rze, d_rze_size, d_err, d_idx, d_count);
     {
         TraceScope ts(s, "assemble_scan");
         assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
@@ -728,6 +743,211 @@ int fzb_huff_decode(const void* d_in, uint64_t in_bytes, uint64_t n, uint32_t bk
     CK(cudaMemsetAsync(err, 0, kCtrlBytes, s));
     return launch_hf_decode(static_cast<const uint8_t*>(d_in), in_bytes, n, bklen, d_out, err, s) == 0
                ? FZB_OK : FZB_E_CUDA;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched LorenzoQuant -> Bitshuffle -> RZE over many fields: one reset
+// kernel, one value-base kernel for every field, one persistent chunk
+// kernel over every (field, chunk) unit and two assembly kernels -- five
+// launches whatever the field count, capturable in a CUDA graph.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct BatchPlan {
+    BatchArgs args;
+    uint32_t mm_grid_x;
+    unsigned lq_grid;
+    size_t smem;
+};
+
+struct BatchLayout {
+    size_t desc_bytes;
+    std::vector<size_t> field_off;
+    size_t total;
+};
+
+BatchLayout batch_layout(const fzb_batch_field* f, int nf) {
+    BatchLayout L;
+    L.desc_bytes = align256(sizeof(BatchField) * (size_t)nf) + align256(8ull * nf + 64);
+    size_t off = L.desc_bytes;
+    for (int i = 0; i < nf; i++) {
+        L.field_off.push_back(off);
+        off += align256(carve(nullptr, f[i].n_total, f[i].cap).need);
+    }
+    L.total = off;
+    return L;
+}
+
+int batch_check(const fzb_batch_field& f, Geometry* g) {
+    int rc = geometry(f.n_total, f.dims, g);
+    if (rc) return rc;
+    if (!f.d_in || !f.d_count || !f.d_eb_state || !f.d_rze || !f.d_rze_size) return FZB_E_INVALID;
+    if (f.cap && (!f.d_err || !f.d_idx)) return FZB_E_INVALID;
+    if (f.eb_mode < FZB_ABS || f.eb_mode > FZB_NOA || !(f.eb > 0.0f)) return FZB_E_INVALID;
+    return FZB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t fzb_batch_workspace_bytes(const fzb_batch_field* fields, int nfields) {
+    if (!fields || nfields <= 0) return 0;
+    return batch_layout(fields, nfields).total;
+}
+
+void* fzb_batch_create(const fzb_batch_field* fields, int nfields, const fzb_batch_tuning* tuning, void* d_work,
+                       size_t work_bytes, int* status) {
+    int dummy = 0;
+    int* st = status ? status : &dummy;
+    *st = FZB_E_INVALID;
+    if (!fields || nfields <= 0 || !d_work) return nullptr;
+    const BatchLayout L = batch_layout(fields, nfields);
+    if (work_bytes < L.total) {
+        *st = FZB_E_WORKSPACE;
+        return nullptr;
+    }
+    int dev = 0, sms = 148, max_smem = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    uint8_t* base = static_cast<uint8_t*>(d_work);
+    std::vector<BatchField> hf((size_t)nfields);
+    size_t smem = 0;
+    uint32_t mm_grid = 1;
+    for (int i = 0; i < nfields; i++) {
+        const fzb_batch_field& f = fields[i];
+        Geometry g;
+        const int rc = batch_check(f, &g);
+        if (rc) {
+            *st = rc;
+            return nullptr;
+        }
+        const Work w = carve(base + L.field_off[i], f.n_total, f.cap);
+        BatchField& b = hf[i];
+        b.a = fwd_args(g, w, f.d_in, f.n_total, f.d_eb_state, f.radius, f.zigzag, nullptr, f.cap);
+        b.m = asm_args(w, b.a, true, f.d_rze, f.d_rze_size, f.d_err, f.d_idx, f.d_count);
+        b.in = f.d_in;
+        b.n = f.n_total;
+        b.pmin = w.pmin;
+        b.pmax = w.pmax;
+        b.mm_done = w.mm_done;
+        b.eb_state = f.d_eb_state;
+        b.mode = f.eb_mode;
+        b.user_eb = f.eb;
+        b.vb_given = f.value_base;
+        b.scan = (f.eb_mode != FZB_ABS && !(f.value_base > 0.0f)) ? 1u : 0u;
+        uint64_t want = (f.n_total / 4 + 255) / 256;
+        uint64_t parts = want < (uint64_t)(4 * sms) ? want : (uint64_t)(4 * sms);
+        if (parts < 1) parts = 1;
+        if (parts > (uint64_t)kMaxParts) parts = kMaxParts;
+        b.mm_parts = b.scan ? (uint32_t)parts : 1u;
+        if (b.mm_parts > mm_grid) mm_grid = b.mm_parts;
+        const bool rowal = (g.ndim == 1) || (g.nx % 32 == 0);
+        b.kind = g.ndim == 1 ? 0u : g.ndim == 2 ? (rowal ? 1u : 2u) : (rowal ? 3u : 4u);
+        b.n_chunks = (uint32_t)chunks_of(f.n_total);
+        const size_t sm = lq_smem_bytes(g, true);
+        if (sm > smem) smem = sm;
+    }
+    if ((int)smem > max_smem) {
+        *st = FZB_E_INVALID;
+        return nullptr;
+    }
+    // field order of the unit ranges
+    std::vector<uint32_t> order((size_t)nfields), begin((size_t)nfields);
+    for (int i = 0; i < nfields; i++) order[i] = (uint32_t)i;
+    if (tuning && tuning->order == 1)
+        std::stable_sort(order.begin(), order.end(),
+                         [&](uint32_t x, uint32_t y) { return hf[x].n_chunks > hf[y].n_chunks; });
+    uint64_t units = 0;
+    for (int i = 0; i < nfields; i++) {
+        begin[i] = (uint32_t)units;
+        units += hf[order[i]].n_chunks;
+    }
+    if (units >= (1ull << 31)) return nullptr;
+    // descriptors: [BatchField x n][order x n][begin x n][counter]
+    std::vector<uint8_t> desc(L.desc_bytes, 0);
+    std::memcpy(desc.data(), hf.data(), sizeof(BatchField) * hf.size());
+    const size_t o_order = align256(sizeof(BatchField) * (size_t)nfields);
+    std::memcpy(desc.data() + o_order, order.data(), 4ull * nfields);
+    std::memcpy(desc.data() + o_order + 4ull * nfields, begin.data(), 4ull * nfields);
+    const size_t o_counter = o_order + 8ull * nfields;
+    if (cudaMemcpy(base, desc.data(), desc.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        *st = FZB_E_CUDA;
+        return nullptr;
+    }
+    for (int i = 0; i < nfields; i++)  // control words (scan counters start at zero)
+        if (cudaMemset(base + L.field_off[i], 0, kCtrlBytes) != cudaSuccess) {
+            *st = FZB_E_CUDA;
+            return nullptr;
+        }
+    auto* p = new BatchPlan();
+    p->args.fields = reinterpret_cast<const BatchField*>(base);
+    p->args.nfields = (uint32_t)nfields;
+    p->args.unit_order = reinterpret_cast<const uint32_t*>(base + o_order);
+    p->args.unit_begin = reinterpret_cast<const uint32_t*>(base + o_order + 4ull * nfields);
+    p->args.total_units = (uint32_t)units;
+    p->args.counter = reinterpret_cast<uint32_t*>(base + o_counter);
+    p->mm_grid_x = mm_grid;
+    const int per_sm = (tuning && tuning->ctas_per_sm > 0) ? tuning->ctas_per_sm : 2;
+    const uint64_t grid = (uint64_t)per_sm * (uint64_t)sms;
+    p->lq_grid = (unsigned)(grid < units ? grid : units);
+    if (p->lq_grid == 0) p->lq_grid = 1;
+    p->smem = smem;
+    *st = FZB_OK;
+    return p;
+}
+
+int fzb_batch_launch(void* batch, void* stream) {
+    if (!batch) return FZB_E_INVALID;
+    const BatchPlan* p = static_cast<const BatchPlan*>(batch);
+    cudaStream_t s = S(stream);
+    TraceScope ts(s, "batch_lq_bs_rze");
+    return launch_batch(p->args, p->mm_grid_x, p->lq_grid, p->smem, s) == 0 ? FZB_OK : FZB_E_CUDA;
+}
+
+void fzb_batch_destroy(void* batch) { delete static_cast<BatchPlan*>(batch); }
+
+int fzb_batch_autotune(const fzb_batch_field* fields, int nfields, void* d_work, size_t work_bytes, void* stream,
+                       fzb_batch_tuning* best, float* best_ms) {
+    if (!best) return FZB_E_INVALID;
+    cudaStream_t s = S(stream);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best_t = 1e30f;
+    int rc = FZB_OK;
+    for (int order = 0; order < 2 && rc == FZB_OK; order++)
+        for (int per_sm = 1; per_sm <= 3 && rc == FZB_OK; per_sm++) {
+            fzb_batch_tuning t{per_sm, order};
+            int st = 0;
+            void* p = fzb_batch_create(fields, nfields, &t, d_work, work_bytes, &st);
+            if (!p) {
+                rc = st;
+                break;
+            }
+            float tmin = 1e30f;
+            for (int rep = 0; rep < 3 && rc == FZB_OK; rep++) {  // first run warms up
+                if (cudaEventRecord(e0, s) != cudaSuccess) rc = FZB_E_CUDA;
+                if (rc == FZB_OK) rc = fzb_batch_launch(p, stream);
+                if (rc == FZB_OK && cudaEventRecord(e1, s) != cudaSuccess) rc = FZB_E_CUDA;
+                if (rc == FZB_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = FZB_E_CUDA;
+                float ms = 0;
+                if (rc == FZB_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = FZB_E_CUDA;
+                if (rc == FZB_OK && rep > 0 && ms < tmin) tmin = ms;
+            }
+            fzb_batch_destroy(p);
+            if (rc == FZB_OK && tmin < best_t) {
+                best_t = tmin;
+                *best = t;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best_ms) *best_ms = best_t;
+    return rc;
 }
 
 }  // extern "C"

@@ -39,17 +39,19 @@ __device__ __forceinline__ void resolve_eb_store(float lo, float hi, int mode, f
     st[3] = __fmul_rn(2.0f, abs_eb);
 }
 
-__global__ void __launch_bounds__(256) minmax_kernel(const float* __restrict__ x, uint64_t n,
-                                                     float* __restrict__ pmin,
-                                                     float* __restrict__ pmax,
-                                                     unsigned int* __restrict__ done, int mode,
-                                                     float user_eb, float* __restrict__ st) {
+// Block `blk` of `nblk` cooperating blocks: partial min/max into
+// pmin/pmax[blk]; the last block to finish reduces the partials and resolves
+// the error bound into st, then re-arms `done` for the next launch.
+__device__ __forceinline__ void minmax_body(const float* __restrict__ x, uint64_t n, float* __restrict__ pmin,
+                                            float* __restrict__ pmax, unsigned int* __restrict__ done, int mode,
+                                            float user_eb, float* __restrict__ st, const unsigned blk,
+                                            const unsigned nblk) {
     float lo = INFINITY, hi = -INFINITY;
     const bool vec = ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
     const uint64_t nv = vec ? n / 4 : 0;
     const float4* x4 = reinterpret_cast<const float4*>(x);
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)nblk * blockDim.x;
+    uint64_t i = (uint64_t)blk * blockDim.x + threadIdx.x;
     for (; i + 3 * stride < nv; i += 4 * stride) {
         float4 v[4];
 #pragma unroll
@@ -65,7 +67,7 @@ __global__ void __launch_bounds__(256) minmax_kernel(const float* __restrict__ x
         lo = fminf(lo, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
         hi = fmaxf(hi, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
     }
-    for (uint64_t k = 4 * nv + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    for (uint64_t k = 4 * nv + (uint64_t)blk * blockDim.x + threadIdx.x; k < n; k += stride) {
         lo = fminf(lo, x[k]);
         hi = fmaxf(hi, x[k]);
     }
@@ -86,17 +88,17 @@ __global__ void __launch_bounds__(256) minmax_kernel(const float* __restrict__ x
             lo = fminf(lo, slo[w]);
             hi = fmaxf(hi, shi[w]);
         }
-        pmin[blockIdx.x] = lo;
-        pmax[blockIdx.x] = hi;
+        pmin[blk] = lo;
+        pmax[blk] = hi;
         __threadfence();
-        s_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+        s_last = (atomicAdd(done, 1u) == nblk - 1);
     }
     __syncthreads();
     if (!s_last) return;
     __threadfence();
     lo = INFINITY;
     hi = -INFINITY;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    for (unsigned b = threadIdx.x; b < nblk; b += blockDim.x) {
         lo = fminf(lo, __ldcg(pmin + b));
         hi = fmaxf(hi, __ldcg(pmax + b));
     }
@@ -118,6 +120,13 @@ __global__ void __launch_bounds__(256) minmax_kernel(const float* __restrict__ x
         resolve_eb_store(lo, hi, mode, user_eb, 0.0f, true, st);
         *done = 0;  // ready for the next launch
     }
+}
+
+__global__ void __launch_bounds__(256) minmax_kernel(const float* __restrict__ x, uint64_t n,
+                                                     float* __restrict__ pmin, float* __restrict__ pmax,
+                                                     unsigned int* __restrict__ done, int mode, float user_eb,
+                                                     float* __restrict__ st) {
+    minmax_body(x, n, pmin, pmax, done, mode, user_eb, st, blockIdx.x, gridDim.x);
 }
 
 // Error-bound resolution without a scan (ABS, or a caller-provided base).
@@ -314,7 +323,7 @@ __device__ __forceinline__ void write_slot(uint8_t* __restrict__ slots, uint32_t
 
 // Exclusive scans over chunks (one CTA of 1024 threads): payload offsets,
 // outlier offsets, RZE header, total sizes.
-__global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) {
+__device__ __forceinline__ void assemble_scan_body(const AsmArgs& a) {
     __shared__ unsigned long long sp[1024];
     __shared__ unsigned int so[1024];
     const uint32_t n = a.n_chunks, t = threadIdx.x;
@@ -376,11 +385,12 @@ __global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) {
     }
 }
 
+__global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) { assemble_scan_body(a); }
+
 // One CTA per chunk: payload from its slot to the final stream position
 // (any byte alignment), and its outliers from staging to their sorted
 // position (chunks are index ranges and each chunk's block is sorted).
-__global__ void __launch_bounds__(256) assemble_copy_kernel(AsmArgs a) {
-    const uint32_t c = blockIdx.x;
+__device__ __forceinline__ void assemble_copy_body(const AsmArgs& a, const uint32_t c) {
     if (a.sizes) {
         const uint32_t len = a.sizes[c] & 0x7fffffffu;
         uint8_t* dst = a.out + 8ull + 4ull * a.n_chunks + a.pay_off[c];
@@ -416,6 +426,8 @@ __global__ void __launch_bounds__(256) assemble_copy_kernel(AsmArgs a) {
         }
     }
 }
+
+__global__ void __launch_bounds__(256) assemble_copy_kernel(AsmArgs a) { assemble_copy_body(a, blockIdx.x); }
 
 // Row-vector path: one thread, 32 consecutive elements of one row, all
 // operands staged in shared memory.  TZ/TY say whether the z / y predecessor
@@ -516,13 +528,13 @@ __device__ __forceinline__ void group_dispatch(const GroupIn& g, bool tz, bool t
 // so each thread's 32 codes share (y, z) and the row-vector path applies.
 // ---------------------------------------------------------------------------
 
+// One 8192-code chunk `c` of the field `a` (every thread of the block
+// calls it; it contains block-wide barriers).  Q: dynamic shared memory,
+// s_ws: 16 words, s_obase: one word.
 template <int NDIM, bool FUSED, bool ROWAL>
-__global__ void __launch_bounds__(kThreads, 3) lq_chunk_kernel(FwdArgs a) {
-    extern __shared__ float4 Q[];
-    __shared__ uint32_t s_ws[16];
-    __shared__ uint32_t s_obase;
+__device__ __forceinline__ void lq_chunk_body(const FwdArgs& a, const uint32_t c, float4* Q, uint32_t* s_ws,
+                                              uint32_t& s_obase) {
     const int t = threadIdx.x;
-    const uint32_t c = blockIdx.x;
     const uint32_t i0 = c * (uint32_t)kChunkCodes;
     const uint32_t cnt = min((uint32_t)kChunkCodes, a.n_total - i0);
     const float r = *a.ebx2_r;
@@ -660,6 +672,100 @@ __global__ void __launch_bounds__(kThreads, 3) lq_chunk_kernel(FwdArgs a) {
     __syncthreads();
     const uint32_t sw = rze_encode_chunk(sm, (int)(2 * cnt));
     write_slot(a.slots, a.sizes, c, sw, (sw >> 31) ? reinterpret_cast<const uint8_t*>(sm.S) : sm.O);
+}
+
+template <int NDIM, bool FUSED, bool ROWAL>
+__global__ void __launch_bounds__(kThreads, 3) lq_chunk_kernel(FwdArgs a) {
+    extern __shared__ float4 Q[];
+    __shared__ uint32_t s_ws[16];
+    __shared__ uint32_t s_obase;
+    lq_chunk_body<NDIM, FUSED, ROWAL>(a, blockIdx.x, Q, s_ws, s_obase);
+}
+
+// ---------------------------------------------------------------------------
+// Batched fused compression: many fields, one persistent launch.  CTAs take
+// (field, chunk) units from a global counter in the order `unit_order`
+// lists the fields; every unit runs the same chunk body as the single-field
+// kernel, so each field's bytes equal its own fzb_lq_bs_rze_compress output.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 3) lq_batch_kernel(BatchArgs b) {
+    extern __shared__ float4 Q[];
+    __shared__ uint32_t s_ws[16];
+    __shared__ uint32_t s_obase;
+    __shared__ uint32_t s_unit;
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = atomicAdd(b.counter, 1u);
+        __syncthreads();
+        const uint32_t u = s_unit;
+        __syncthreads();  // s_unit is rewritten on the next iteration
+        if (u >= b.total_units) break;
+        // field = last slot whose unit_begin <= u (fields in unit_order)
+        uint32_t lo = 0, hi = b.nfields;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (b.unit_begin[mid] <= u) lo = mid;
+            else hi = mid;
+        }
+        const BatchField& f = b.fields[b.unit_order[lo]];
+        const uint32_t c = u - b.unit_begin[lo];
+        switch (f.kind) {
+            case 0: lq_chunk_body<1, true, true>(f.a, c, Q, s_ws, s_obase); break;
+            case 1: lq_chunk_body<2, true, true>(f.a, c, Q, s_ws, s_obase); break;
+            case 2: lq_chunk_body<2, true, false>(f.a, c, Q, s_ws, s_obase); break;
+            case 3: lq_chunk_body<3, true, true>(f.a, c, Q, s_ws, s_obase); break;
+            default: lq_chunk_body<3, true, false>(f.a, c, Q, s_ws, s_obase); break;
+        }
+        __syncthreads();  // shared memory is reused by the next unit
+    }
+}
+
+// REL/NOA value bases of every field in one launch: blockIdx.y = field,
+// blockIdx.x < parts(field) take part; the last block of a field resolves it.
+__global__ void __launch_bounds__(256) batch_minmax_kernel(BatchArgs b) {
+    const BatchField& f = b.fields[blockIdx.y];
+    if (blockIdx.x >= f.mm_parts) return;
+    if (f.mm_parts == 1 && f.scan == 0) {  // ABS, or a caller-provided value base
+        if (threadIdx.x == 0) resolve_eb_store(0.f, 0.f, f.mode, f.user_eb, f.vb_given, false, f.eb_state);
+        return;
+    }
+    minmax_body(f.in, f.n, f.pmin, f.pmax, f.mm_done, f.mode, f.user_eb, f.eb_state, blockIdx.x, f.mm_parts);
+}
+
+__global__ void __launch_bounds__(1024) batch_assemble_scan_kernel(BatchArgs b) {
+    assemble_scan_body(b.fields[blockIdx.x].m);
+}
+
+__global__ void __launch_bounds__(256) batch_assemble_copy_kernel(BatchArgs b) {
+    const uint32_t u = blockIdx.x;
+    uint32_t lo = 0, hi = b.nfields;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (b.unit_begin[mid] <= u) lo = mid;
+        else hi = mid;
+    }
+    assemble_copy_body(b.fields[b.unit_order[lo]].m, u - b.unit_begin[lo]);
+}
+
+// Per launch: the unit dispenser, every field's error word and outlier
+// staging counter start at zero.
+__global__ void batch_reset_kernel(BatchArgs b) {
+    const BatchField& f = b.fields[blockIdx.x];
+    if (threadIdx.x == 0) {
+        *f.a.ostage_ctr = 0;
+        *f.a.err = 0;
+        if (blockIdx.x == 0) *b.counter = 0;
+    }
+}
+
+int launch_batch(const BatchArgs& b, uint32_t mm_grid_x, unsigned lq_grid, size_t smem, cudaStream_t s) {
+    batch_reset_kernel<<<b.nfields, 32, 0, s>>>(b);
+    batch_minmax_kernel<<<dim3(mm_grid_x, b.nfields), 256, 0, s>>>(b);
+    cudaError_t e = cudaFuncSetAttribute(lq_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    lq_batch_kernel<<<lq_grid, kThreads, smem, s>>>(b);
+    batch_assemble_scan_kernel<<<b.nfields, 1024, 0, s>>>(b);
+    batch_assemble_copy_kernel<<<b.total_units, 256, 0, s>>>(b);
+    return (int)cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -137,6 +137,36 @@ int launch_bitpack_encode(const void* in, uint64_t n, int elem, int nbits, uint8
                           unsigned int* done, cudaStream_t s);
 int launch_bitpack_decode(const uint8_t* in, uint64_t n, int elem, int nbits, void* out, cudaStream_t s);
 
+// Batched fused compression (fzb_forward.cu): one field's arguments.
+struct BatchField {
+    FwdArgs a;               // chunk kernel arguments (slots, staging, ...)
+    AsmArgs m;               // assembly arguments
+    const float* in;         // value-base scan
+    uint64_t n;
+    float* pmin;
+    float* pmax;
+    unsigned int* mm_done;
+    float* eb_state;
+    int mode;
+    float user_eb;
+    float vb_given;
+    uint32_t mm_parts;       // blocks of the scan (1 when no scan)
+    uint32_t scan;           // 1: REL/NOA scan, 0: resolve only
+    uint32_t kind;           // 0 1-D, 1 2-D rows %32, 2 2-D, 3 3-D rows %32, 4 3-D
+    uint32_t n_chunks;
+};
+
+struct BatchArgs {
+    const BatchField* fields;
+    uint32_t nfields;
+    const uint32_t* unit_order;  // field index per slot
+    const uint32_t* unit_begin;  // first unit of each slot
+    uint32_t total_units;
+    uint32_t* counter;           // unit dispenser
+};
+
+int launch_batch(const BatchArgs& b, uint32_t mm_grid_x, unsigned lq_grid, size_t smem, cudaStream_t s);
+
 // Per-kernel CUDA-event timing (fzb_trace.cu): a TraceScope around a launch
 // records an event pair on the launching stream while tracing is enabled.
 extern bool g_trace_on;

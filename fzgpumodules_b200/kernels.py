@@ -328,3 +328,88 @@ class Trace:
             check(lib().fzb_trace_get(i, name, 96, C.byref(launches), C.byref(ms)), "fzb_trace_get")
             out[name.value.decode()] = (int(launches.value), float(ms.value))
         return out
+
+
+# ------------------------------------------------------------------ batches
+
+class _BatchField(C.Structure):
+    _fields_ = [("d_in", C.c_void_p), ("n_total", C.c_uint64), ("dims", C.c_uint32 * 3), ("eb", C.c_float),
+                ("eb_mode", C.c_int), ("value_base", C.c_float), ("radius", C.c_uint32), ("zigzag", C.c_int),
+                ("d_err", C.c_void_p), ("d_idx", C.c_void_p), ("cap", C.c_uint64), ("d_count", C.c_void_p),
+                ("d_rze", C.c_void_p), ("d_rze_size", C.c_void_p), ("d_eb_state", C.c_void_p)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("ctas_per_sm", C.c_int), ("order", C.c_int)]
+
+    def __repr__(self):
+        return f"BatchTuning(ctas_per_sm={self.ctas_per_sm}, order={self.order})"
+
+
+class Batch:
+    """Batched LorenzoQuant -> Bitshuffle -> RZE over many fields
+    (fzb_batch_*).  ``fields``: dicts with x (device float tensor), dims,
+    eb, mode, radius, zigzag and optionally outlier_capacity / value_base.
+    Outputs per field live in ``self.outputs`` (the same dict layout as
+    lq_bs_rze_compress); launch() re-runs the batch into them."""
+
+    def __init__(self, fields: list, tuning: BatchTuning | None = None):
+        self.device = fields[0]["x"].device
+        self.fields, self.outputs = fields, []
+        arr = (_BatchField * len(fields))()
+        for i, f in enumerate(fields):
+            x = f["x"]
+            n = x.numel()
+            cap = max_outliers(n, f.get("outlier_capacity", 0.2))
+            o = dict(rze=torch.empty(int(lib().fzb_rze_max_bytes(2 * n)), dtype=torch.uint8, device=self.device),
+                     rze_size=torch.zeros(1, dtype=torch.int64, device=self.device),
+                     err=torch.empty(max(cap, 1), dtype=torch.float32, device=self.device),
+                     idx=torch.empty(max(cap, 1), dtype=torch.int32, device=self.device),
+                     count=torch.zeros(1, dtype=torch.int32, device=self.device),
+                     eb_state=torch.zeros(4, dtype=torch.float32, device=self.device), cap=cap)
+            self.outputs.append(o)
+            d = f["dims"]
+            arr[i] = _BatchField(x.data_ptr(), n, (C.c_uint32 * 3)(*d), f["eb"], f.get("mode", ABS),
+                                 f.get("value_base", 0.0), f.get("radius", 32768), int(f.get("zigzag", False)),
+                                 o["err"].data_ptr(), o["idx"].data_ptr(), cap, o["count"].data_ptr(),
+                                 o["rze"].data_ptr(), o["rze_size"].data_ptr(), o["eb_state"].data_ptr())
+        self._arr = arr
+        need = int(lib().fzb_batch_workspace_bytes(arr, len(fields)))
+        self.work = torch.empty(need, dtype=torch.uint8, device=self.device)
+        self._h = None
+        self.retune(tuning)
+
+    def retune(self, tuning: BatchTuning | None):
+        if self._h:
+            lib().fzb_batch_destroy(self._h)
+        st = C.c_int(0)
+        with torch.cuda.device(self.device):
+            h = lib().fzb_batch_create(self._arr, len(self.fields), C.byref(tuning) if tuning else None,
+                                       _ptr(self.work), self.work.numel(), C.byref(st))
+        if not h:
+            check(st.value or -1, "fzb_batch_create")
+        self._h = h
+        self.tuning = tuning
+
+    def autotune(self) -> tuple:
+        best, ms = BatchTuning(), C.c_float(0)
+        with torch.cuda.device(self.device):
+            check(lib().fzb_batch_autotune(self._arr, len(self.fields), _ptr(self.work), self.work.numel(),
+                                           _stream(self.device), C.byref(best), C.byref(ms)), "fzb_batch_autotune")
+        self.retune(best)
+        return best, ms.value
+
+    def launch(self, stream: torch.cuda.Stream | None = None):
+        s = C.c_void_p(stream.cuda_stream) if stream is not None else _stream(self.device)
+        check(lib().fzb_batch_launch(self._h, s), "fzb_batch_launch")
+
+    def close(self):
+        if self._h:
+            lib().fzb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

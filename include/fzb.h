@@ -220,6 +220,53 @@ uint64_t fzb_concat_bytes(const uint64_t* sizes, int n);
 int fzb_concat(const void* const* d_srcs, const uint64_t* sizes, int n, void* d_out, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Batched compression of many fields (no reference counterpart: it runs the
+ * chain of fzb_lq_bs_rze_compress for every field in five launches --
+ * reset, one value-base scan over all fields, one persistent chunk kernel
+ * over every (field, chunk) unit, two assembly kernels -- so a batch is one
+ * CUDA graph node group regardless of its size).  Each field's outputs are
+ * byte-identical to its own fzb_lq_bs_rze_compress call.
+ *
+ * fzb_batch_create validates the fields, writes the descriptors into
+ * d_work (synchronous copy) and returns a handle; fzb_batch_launch only
+ * enqueues (capturable; the buffers named at create time are reused on
+ * every launch).  Tuning: CTAs per SM of the persistent kernel, and the
+ * order fields are dispensed in (0 as given, 1 largest first); neither
+ * changes any output byte.  fzb_batch_autotune times the candidates on the
+ * given fields and returns the fastest.
+ * ------------------------------------------------------------------------ */
+typedef struct fzb_batch_field {
+    const float* d_in;
+    uint64_t n_total;
+    uint32_t dims[3];
+    float eb;
+    int eb_mode;
+    float value_base;
+    uint32_t radius;
+    int zigzag;
+    float* d_err;
+    uint32_t* d_idx;
+    uint64_t cap;
+    uint32_t* d_count;
+    void* d_rze;
+    uint64_t* d_rze_size;
+    float* d_eb_state;
+} fzb_batch_field;
+
+typedef struct fzb_batch_tuning {
+    int ctas_per_sm;
+    int order;
+} fzb_batch_tuning;
+
+size_t fzb_batch_workspace_bytes(const fzb_batch_field* fields, int nfields);
+void* fzb_batch_create(const fzb_batch_field* fields, int nfields, const fzb_batch_tuning* tuning, void* d_work,
+                       size_t work_bytes, int* status);
+int fzb_batch_launch(void* batch, void* stream);
+void fzb_batch_destroy(void* batch);
+int fzb_batch_autotune(const fzb_batch_field* fields, int nfields, void* d_work, size_t work_bytes, void* stream,
+                       fzb_batch_tuning* best, float* best_ms);
+
+/* ------------------------------------------------------------------------
  * Pipelines: C view of fz::Pipeline (include/fz/pipeline.h), the reference's
  * Pipeline API (include/pipeline/compressor.h:34-386) for bindings without
  * C++ interop.  A pipeline is an opaque handle; stages are the indices the
