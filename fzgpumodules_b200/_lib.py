@@ -84,6 +84,19 @@ def lib():
         L.fzb_batch_destroy.restype = None
         L.fzb_batch_destroy.argtypes = [p]
         L.fzb_batch_autotune.argtypes = [p, i32, p, sz, p, p, p]
+        L.fzb_sel_chunks.restype = u64
+        L.fzb_sel_chunks.argtypes = [u64]
+        L.fzb_sel_workspace_bytes.restype = sz
+        L.fzb_sel_workspace_bytes.argtypes = [u64]
+        L.fzb_sel_max_bytes.restype = u64
+        L.fzb_sel_max_bytes.argtypes = [u64]
+        L.fzb_sel_features.argtypes = [p, u64, p, p]
+        L.fzb_sel_trial.argtypes = [p, u64, p, p, sz, p]
+        L.fzb_sel_encode.argtypes = [p, u64, i32, p, p, p, p, p, sz, p]
+        L.fzb_sel_decode.argtypes = [p, u64, p, u64, p, sz, p]
+        L.fzb_mlp_forward.argtypes = [p, p, p, u32, p]
+        L.fzb_mlp_grad.argtypes = [p, p, p, u32, i32, p, p, p]
+        L.fzb_mlp_adam.argtypes = [p, p, p, p, f32, i32, p]
         L.fzb_last_error.restype = C.c_char_p
         L.fzb_last_error.argtypes = []
         L.fzb_pipeline_create.restype = p

@@ -167,6 +167,45 @@ struct BatchArgs {
 
 int launch_batch(const BatchArgs& b, uint32_t mm_grid_x, unsigned lq_grid, size_t smem, cudaStream_t s);
 
+// Per-chunk coding with a learned selector (fzb_select.cu).
+constexpr int kSelCodes = 32768;            // codes per 64 KiB chunk
+constexpr int kSelBytes = 65536;
+constexpr int kSelCoders = 4;               // Bitshuffle+RZE, RLE, Bitpack, Huffman
+constexpr uint32_t kSelSlot = 65536 + 256;  // per (chunk, coder) output slot
+constexpr uint32_t kSelNoFit = 0xffffffffu; // coder output larger than the chunk / not applicable
+constexpr int kSelFeat = 16;
+constexpr int kSelBk = 1024;                // Huffman book length
+constexpr int kSelParts = (kSelCodes + 767) / 768;
+constexpr int kMlpParams = 16 * 64 + 64 + 64 * 64 + 64 + 64 * 4 + 4;
+constexpr float kMlpTau = 0.02f;            // soft-label temperature on log2 regrets
+
+struct SelArgs {
+    const uint16_t* codes;
+    uint64_t n;
+    const uint32_t* list;    // chunk ids (null: blockIdx)
+    const uint8_t* want;     // per chunk: bit k = run coder k (null: all)
+    uint8_t* slots;          // nchunks * 4 * kSelSlot
+    uint32_t* sizes;         // nchunks * 4 (kSelNoFit = no output)
+    uint8_t* params;         // nchunks * 4
+    uint8_t* scratch;        // nchunks * 4 * 16 KiB (RZE blocks)
+    uint32_t* subsizes;      // nchunks * 4
+    uint32_t* hf_freq;       // nchunks * kSelBk
+    uint32_t* hf_book;       // nchunks * kSelBk
+    uint8_t* tags;           // nchunks
+};
+
+int launch_sel_features(const uint16_t* codes, uint64_t n, float* feats, cudaStream_t s);
+int launch_sel_coders(const SelArgs& a, uint32_t nchunks, unsigned coder_mask, cudaStream_t s);
+int launch_sel_choose(const SelArgs& a, uint32_t nchunks, int mode, const float* pred, cudaStream_t s);
+int launch_sel_fallback_mask(const SelArgs& a, uint32_t nchunks, uint8_t* want, cudaStream_t s);
+int launch_sel_tag_mask(const SelArgs& a, uint32_t nchunks, uint8_t* want, cudaStream_t s);
+int launch_sel_container(const SelArgs& a, uint32_t nchunks, uint8_t* out, unsigned long long* out_size,
+                         unsigned long long* offs, cudaStream_t s);
+int launch_mlp_forward(const float* P, const float* X, float* Y, uint32_t batch, cudaStream_t s);
+int launch_mlp_backward(const float* P, const float* X, const float* T, uint32_t batch, float* G, float* loss,
+                        int kind, cudaStream_t s);
+int launch_mlp_adam(float* P, const float* G, float* M, float* V, float lr, int step, cudaStream_t s);
+
 // Per-kernel CUDA-event timing (fzb_trace.cu): a TraceScope around a launch
 // records an event pair on the launching stream while tracing is enabled.
 extern bool g_trace_on;

@@ -1,0 +1,1047 @@
+// fzb_select.cu -- per-chunk lossless coding of quantization codes with a
+// learned coder selector.
+//
+// The code array is cut into 64 KiB chunks (32768 u16 codes; the last may
+// be shorter).  Each chunk is coded on its own by one of four coders, each
+// producing exactly the bytes its reference stage would produce on that
+// chunk alone:
+//   0  Bitshuffle(16 KiB, ew 2) -> RZE(16 KiB, 4 levels)   (RZE stream)
+//   1  RLE<uint16_t>                                        (RLE stream)
+//   2  Bitpack<uint16_t>, nbits detected                    (packed bytes)
+//   3  Huffman<uint16_t>, bklen 1024, coarse                (PHF blob)
+// A coder whose output would exceed 64 KiB, or Huffman with a symbol >= 1024,
+// is never chosen (Bitpack always fits).  Choice: exhaustive trial (smallest
+// size, lowest coder index on ties) or a 16 -> 64 -> 64 -> 4 FP32 MLP on 16
+// per-chunk statistics that predicts each coder's log2 size.
+//
+// Container: [u32 'FZSC'][u32 nchunks][u32 n_codes][u32 32768]
+//            [u8 tag x nchunks, padded to 4][u8 param x nchunks, padded to 4]
+//            [u32 size x nchunks][payload_i padded to 4 bytes] ...
+// (param = Bitpack nbits, 0 otherwise).
+#include "fzb_kernels.cuh"
+
+namespace fzb {
+
+namespace {
+
+__device__ __forceinline__ void sel_raw_to_packed(const uint32_t (&rw)[16], uint32_t (&x)[16]) {
+#pragma unroll
+    for (int l = 0; l < 8; l++) {
+        x[2 * l] = __byte_perm(rw[l], rw[l + 8], 0x5410);
+        x[2 * l + 1] = __byte_perm(rw[l], rw[l + 8], 0x7632);
+    }
+}
+
+__device__ __forceinline__ uint32_t chunk_count(uint64_t n, uint32_t c) {
+    const uint64_t b = (uint64_t)c * kSelCodes;
+    return (uint32_t)(n - b < (uint64_t)kSelCodes ? n - b : (uint64_t)kSelCodes);
+}
+
+// chunk id of this block, or -1 when coder k is not wanted for it
+__device__ __forceinline__ int sel_chunk(const SelArgs& s, int k) {
+    const uint32_t c = s.list ? s.list[blockIdx.x] : blockIdx.x;
+    if (s.want && !((s.want[c] >> k) & 1u)) return -1;
+    return (int)c;
+}
+
+__device__ __forceinline__ float bin_entropy(float p) {
+    if (p <= 0.0f || p >= 1.0f) return 0.0f;
+    return -(p * __log2f(p) + (1.0f - p) * __log2f(1.0f - p));
+}
+
+// Block-wide float sum (256 threads), fixed reduction order.
+__device__ __forceinline__ float block_sum(float v, float* red) {
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float s = 0.0f;
+#pragma unroll
+    for (int w = 0; w < 8; w++) s += red[w];
+    __syncthreads();
+    return s;
+}
+
+__device__ __forceinline__ uint32_t block_max_u32(uint32_t v, uint32_t* red) {
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, d));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint32_t m = 0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) m = max(m, red[w]);
+    __syncthreads();
+    return m;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Features: 16 statistics per chunk (CTA per chunk, 128 codes per thread).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) sel_features_kernel(const uint16_t* __restrict__ codes, uint64_t n,
+                                                           float* __restrict__ feats) {
+    __shared__ uint32_t h1024[1024];
+    __shared__ uint32_t hlo[256], hhi[256];
+    __shared__ float red[8];
+    __shared__ uint32_t ured[8];
+    const uint32_t c = blockIdx.x, t = threadIdx.x;
+    const uint32_t cnt = chunk_count(n, c);
+    const uint16_t* src = codes + (uint64_t)c * kSelCodes;
+    for (uint32_t i = t; i < 1024; i += 256) h1024[i] = 0;
+    hlo[t] = 0;
+    hhi[t] = 0;
+    __syncthreads();
+    float s1 = 0, s2 = 0, sd = 0, zero = 0, zbyte = 0, same = 0, nzb = 0, big = 0;
+    uint32_t bits[16] = {0}, vmax = 0, gor = 0;
+    const uint32_t b0 = 128 * t;
+    uint32_t prev = (b0 > 0 && b0 - 1 < cnt) ? src[b0 - 1] : 0xffffffffu;
+    for (uint32_t k = 0; k < 128; k++) {
+        const uint32_t i = b0 + k;
+        if (i >= cnt) break;
+        const uint32_t u = src[i];
+        const float lg = __log2f(1.0f + (float)u);
+        s1 += lg;
+        s2 += lg * lg;
+        zero += (u == 0);
+        zbyte += ((u & 0xff) == 0) + ((u >> 8) == 0);
+        // bit-plane bytes of 8 consecutive codes (the Bitshuffle layout):
+        // nonzero iff any of the 8 codes has that bit set
+        gor |= u;
+        if ((k & 7) == 7 || i + 1 == cnt) {
+            nzb += (float)__popc(gor);
+            gor = 0;
+        }
+        big += (u >= 1024);
+        vmax = max(vmax, u);
+        if (prev != 0xffffffffu) {
+            same += (u == prev);
+            const uint32_t d = u > prev ? u - prev : prev - u;
+            sd += __log2f(1.0f + (float)d);
+        }
+        prev = u;
+#pragma unroll
+        for (int b = 0; b < 16; b++) bits[b] += (u >> b) & 1u;
+        atomicAdd(&h1024[min(u, 1023u)], 1u);
+        atomicAdd(&hlo[u & 0xff], 1u);
+        atomicAdd(&hhi[u >> 8], 1u);
+    }
+    const float fn = (float)max(cnt, 1u);
+    const float m1 = block_sum(s1, red) / fn;
+    const float m2 = block_sum(s2, red) / fn;
+    float f[16];
+    f[0] = m1 / 16.0f;
+    f[1] = sqrtf(fmaxf(m2 - m1 * m1, 0.0f)) / 8.0f;
+    f[2] = block_sum(zero, red) / fn;
+    f[3] = 1.0f - block_sum(same, red) / fn;  // runs per code
+    f[4] = block_sum(zbyte, red) / (2.0f * fn);
+    f[5] = block_sum(sd, red) / fn / 16.0f;
+    float hb[4] = {0, 0, 0, 0};
+    for (int b = 0; b < 16; b++) hb[b >> 2] += bin_entropy(block_sum((float)bits[b], red) / fn) * 0.25f;
+    f[6] = hb[0];
+    f[7] = hb[1];
+    f[8] = hb[2];
+    f[9] = hb[3];
+    f[10] = __log2f(1.0f + (float)block_max_u32(vmax, ured)) / 16.0f;
+    __syncthreads();
+    // histogram entropies
+    const float plo = hlo[t] / fn, phi = hhi[t] / fn;
+    f[11] = block_sum(plo > 0 ? -plo * __log2f(plo) : 0.0f, red) / 8.0f;
+    f[12] = block_sum(phi > 0 ? -phi * __log2f(phi) : 0.0f, red) / 8.0f;
+    f[13] = block_sum(big, red) > 0.0f ? 1.0f : 0.0f;  // Huffman (bklen 1024) not applicable
+    f[14] = block_sum(nzb, red) / (2.0f * fn);
+    float e = 0;
+    for (uint32_t i = t; i < 1024; i += 256) {
+        const float p = h1024[i] / fn;
+        if (p > 0) e -= p * __log2f(p);
+    }
+    f[15] = block_sum(e, red) / 10.0f;
+    if (t < 16) {
+        float v = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            if (k == (int)t) v = f[k];
+        feats[(uint64_t)c * kSelFeat + t] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coder 0: Bitshuffle + RZE.  Sub-chunk kernel (grid nlist x 4) encodes one
+// 16 KiB block into scratch; the assembly kernel writes the chunk's RZE
+// stream ([u32 orig][u32 nsub][u32 size x nsub][payloads], padded to 4).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) sel_rze_sub_kernel(SelArgs s) {
+    extern __shared__ uint4 sm4[];
+    __shared__ uint32_t s_ws[16];
+    const int ci = sel_chunk(s, 0);
+    if (ci < 0) return;
+    const uint32_t c = (uint32_t)ci;
+    const uint32_t j = blockIdx.y, t = threadIdx.x;
+    const uint32_t cnt = chunk_count(s.n, c);
+    const uint32_t sb = j * (uint32_t)kChunkCodes;  // first code of the block within the chunk
+    if (sb >= cnt) return;
+    const uint32_t bc = min((uint32_t)kChunkCodes, cnt - sb);
+    uint8_t* base = reinterpret_cast<uint8_t*>(sm4);
+    RzeSmem sm;
+    sm.S = reinterpret_cast<uint32_t*>(base);
+    sm.O = base + kChunkBytes;
+    sm.bm1 = reinterpret_cast<uint32_t*>(base + 2 * kChunkBytes + 16);
+    sm.bm2 = base + 2 * kChunkBytes + 16 + 2048;
+    sm.bm3 = reinterpret_cast<uint32_t*>(base + 2 * kChunkBytes + 16 + 2048 + 256);
+    sm.ws = s_ws;
+    const uint16_t* src = s.codes + (uint64_t)c * kSelCodes + sb;
+    uint32_t rw[16];
+    if (bc == (uint32_t)kChunkCodes && (reinterpret_cast<uintptr_t>(s.codes) & 15) == 0) {
+        const uint4* s4 = reinterpret_cast<const uint4*>(src) + 4 * t;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const uint4 q = __ldg(s4 + v);
+            rw[4 * v] = q.x;
+            rw[4 * v + 1] = q.y;
+            rw[4 * v + 2] = q.z;
+            rw[4 * v + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int l = 0; l < 16; l++) {
+            const uint32_t e = 32 * t + 2 * l;
+            const uint32_t lo = e < bc ? src[e] : 0u, hi = e + 1 < bc ? src[e + 1] : 0u;
+            rw[l] = lo | (hi << 16);
+        }
+    }
+    if (bc == (uint32_t)kChunkCodes) {
+        uint32_t x[16];
+        sel_raw_to_packed(rw, x);
+        transpose16x2(x);
+#pragma unroll
+        for (int b = 0; b < 16; b++) sm.S[(15 - b) * 256 + t] = x[b];
+    } else {  // the block shorter than 16 KiB is copied unchanged
+#pragma unroll
+        for (int l = 0; l < 16; l++) sm.S[16 * t + l] = rw[l];
+    }
+    __syncthreads();
+    const uint32_t sw = rze_encode_chunk(sm, (int)(2 * bc));
+    const uint32_t clean = sw & 0x7fffffffu;
+    const uint8_t* payload = (sw >> 31) ? reinterpret_cast<const uint8_t*>(sm.S) : sm.O;
+    uint4* d4 = reinterpret_cast<uint4*>(s.scratch + ((size_t)c * 4 + j) * kChunkBytes);
+    const uint4* p4 = reinterpret_cast<const uint4*>(payload);
+    for (uint32_t i = t; i < (clean + 15) / 16; i += kThreads) d4[i] = p4[i];
+    if (t == 0) s.subsizes[(size_t)c * 4 + j] = sw;
+}
+
+__global__ void __launch_bounds__(256) sel_rze_assemble_kernel(SelArgs s) {
+    const int ci = sel_chunk(s, 0);
+    if (ci < 0) return;
+    const uint32_t c = (uint32_t)ci;
+    const uint32_t cnt = chunk_count(s.n, c);
+    const uint32_t nsub = (2 * cnt + kChunkBytes - 1) / kChunkBytes;
+    uint32_t sw[4], off[4], tot = 8 + 4 * nsub;
+    for (uint32_t j = 0; j < 4; j++) {
+        sw[j] = j < nsub ? s.subsizes[(size_t)c * 4 + j] : 0u;
+        off[j] = tot;
+        tot += sw[j] & 0x7fffffffu;
+    }
+    const uint32_t padded = (tot + 3) & ~3u;
+    if (padded > (uint32_t)kSelBytes) {
+        if (threadIdx.x == 0) s.sizes[(size_t)c * kSelCoders + 0] = kSelNoFit;
+        return;
+    }
+    uint8_t* dst = s.slots + ((size_t)c * kSelCoders + 0) * kSelSlot;
+    if (threadIdx.x == 0) {
+        uint32_t* h = reinterpret_cast<uint32_t*>(dst);
+        h[0] = 2 * cnt;
+        h[1] = nsub;
+        for (uint32_t j = 0; j < nsub; j++) h[2 + j] = sw[j];
+        for (uint32_t i = tot; i < padded; i++) dst[i] = 0;
+        s.sizes[(size_t)c * kSelCoders + 0] = padded;
+    }
+    for (uint32_t j = 0; j < nsub; j++) {
+        const uint8_t* src = s.scratch + ((size_t)c * 4 + j) * kChunkBytes;
+        const uint32_t len = sw[j] & 0x7fffffffu;
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) dst[off[j] + i] = src[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coder 1: RLE  [u32 runs][u16 values, padded to 4][u32 lengths]
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) sel_rle_kernel(SelArgs s) {
+    __shared__ uint32_t ws[16];
+    __shared__ uint32_t first_start[256];
+    const int ci = sel_chunk(s, 1);
+    if (ci < 0) return;
+    const uint32_t c = (uint32_t)ci;
+    const uint32_t cnt = chunk_count(s.n, c), t = threadIdx.x;
+    const uint16_t* src = s.codes + (uint64_t)c * kSelCodes;
+    const uint32_t b0 = 128 * t;
+    uint32_t nstart = 0, fs = 0xffffffffu;
+    for (uint32_t k = 0; k < 128; k++) {
+        const uint32_t i = b0 + k;
+        if (i >= cnt) break;
+        if (i == 0 || src[i] != src[i - 1]) {
+            nstart++;
+            if (fs == 0xffffffffu) fs = i;
+        }
+    }
+    uint32_t runs;
+    const uint32_t r0 = block_excl_scan(nstart, ws, &runs);
+    first_start[t] = fs;
+    __syncthreads();
+    const uint32_t vbytes = (2 * runs + 3) & ~3u;
+    const uint32_t total = 4 + vbytes + 4 * runs;
+    if (total > (uint32_t)kSelBytes) {
+        if (t == 0) s.sizes[(size_t)c * kSelCoders + 1] = kSelNoFit;
+        return;
+    }
+    // next run start after this thread's range
+    uint32_t next = cnt;
+    for (uint32_t u = t + 1; u < 256; u++)
+        if (first_start[u] != 0xffffffffu) {
+            next = first_start[u];
+            break;
+        }
+    uint8_t* dst = s.slots + ((size_t)c * kSelCoders + 1) * kSelSlot;
+    uint16_t* vals = reinterpret_cast<uint16_t*>(dst + 4);
+    uint32_t* lens = reinterpret_cast<uint32_t*>(dst + 4 + vbytes);
+    uint32_t r = r0, last = 0xffffffffu;
+    for (uint32_t k = 0; k < 128; k++) {
+        const uint32_t i = b0 + k;
+        if (i >= cnt) break;
+        if (i == 0 || src[i] != src[i - 1]) {
+            if (last != 0xffffffffu) lens[r - 1] = i - last;
+            vals[r] = src[i];
+            last = i;
+            r++;
+        }
+    }
+    if (last != 0xffffffffu) lens[r - 1] = next - last;
+    if (t == 0) {
+        *reinterpret_cast<uint32_t*>(dst) = runs;
+        if (runs & 1) vals[runs] = 0;  // pad the values to 4 bytes
+        s.sizes[(size_t)c * kSelCoders + 1] = total;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coder 2: Bitpack with detected nbits (smallest power of two whose range
+// holds the maximum), LSB-first below 8 bits.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) sel_bitpack_kernel(SelArgs s) {
+    __shared__ uint32_t red[8];
+    const int ci = sel_chunk(s, 2);
+    if (ci < 0) return;
+    const uint32_t c = (uint32_t)ci;
+    const uint32_t cnt = chunk_count(s.n, c), t = threadIdx.x;
+    const uint16_t* src = s.codes + (uint64_t)c * kSelCodes;
+    uint32_t m = 0;
+    for (uint32_t i = t; i < cnt; i += 256) m = max(m, (uint32_t)src[i]);
+    m = block_max_u32(m, red);
+    uint32_t nb = 16;
+    for (uint32_t b = 1; b < 16; b *= 2)
+        if (m < (1u << b)) {
+            nb = b;
+            break;
+        }
+    const uint32_t out_bytes = (cnt * nb + 7) / 8;
+    uint8_t* dst = s.slots + ((size_t)c * kSelCoders + 2) * kSelSlot;
+    if (nb >= 8) {
+        const uint32_t per = nb / 8;
+        for (uint32_t i = t; i < cnt; i += 256) {
+            const uint32_t v = src[i];
+            for (uint32_t b = 0; b < per; b++) dst[i * per + b] = (uint8_t)(v >> (8 * b));
+        }
+    } else {
+        const uint32_t per = 8 / nb, mask = (1u << nb) - 1u;
+        for (uint32_t o = t; o < out_bytes; o += 256) {
+            uint32_t packed = 0;
+            for (uint32_t k = 0; k < per; k++) {
+                const uint32_t e = o * per + k;
+                if (e < cnt) packed |= ((uint32_t)src[e] & mask) << (k * nb);
+            }
+            dst[o] = (uint8_t)packed;
+        }
+    }
+    if (t == 0) {
+        s.sizes[(size_t)c * kSelCoders + 2] = out_bytes;
+        s.params[c * kSelCoders + 2] = (uint8_t)nb;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coder 3: Huffman (bklen 1024).  Histogram (CTA per chunk), canonical
+// codebook (one warp per chunk; lane 0 runs the reference's heap
+// construction, the warp canonizes), coarse encode into the PHF blob.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) sel_hf_hist_kernel(SelArgs s) {
+    __shared__ uint32_t h[kSelBk];
+    __shared__ uint32_t bad;
+    const int ci = sel_chunk(s, 3);
+    if (ci < 0) return;
+    const uint32_t c = (uint32_t)ci;
+    const uint32_t cnt = chunk_count(s.n, c), t = threadIdx.x;
+    const uint16_t* src = s.codes + (uint64_t)c * kSelCodes;
+    for (uint32_t i = t; i < kSelBk; i += 256) h[i] = 0;
+    if (t == 0) bad = 0;
+    __syncthreads();
+    for (uint32_t i = t; i < cnt; i += 256) {
+        const uint32_t u = src[i];
+        if (u < (uint32_t)kSelBk) atomicAdd(&h[u], 1u);
+        else bad = 1;
+    }
+    __syncthreads();
+    uint32_t* f = s.hf_freq + (size_t)c * kSelBk;
+    for (uint32_t i = t; i < kSelBk; i += 256) f[i] = h[i];
+    if (t == 0 && bad) s.sizes[(size_t)c * kSelCoders + 3] = kSelNoFit;
+    else if (t == 0) s.sizes[(size_t)c * kSelCoders + 3] = 0;
+}
+
+// Book for one chunk (warp).  Shared memory (dynamic): node arrays for up to
+// 2*1024 nodes, the heap, the walk stack, code lengths and codes.
+__global__ void __launch_bounds__(32) sel_hf_book_kernel(SelArgs s) {
+    extern __shared__ uint32_t smb[];
+    const int ci = sel_chunk(s, 3);
+    if (ci < 0) return;
+    const uint32_t c = (uint32_t)ci;
+    if (s.sizes[(size_t)c * kSelCoders + 3] == kSelNoFit) return;
+    constexpr int NN = 2 * kSelBk;
+    uint32_t* F = smb;                                          // NN freq
+    int16_t* L = reinterpret_cast<int16_t*>(F + NN);            // NN left
+    int16_t* R = L + NN;                                        // NN right
+    uint16_t* S = reinterpret_cast<uint16_t*>(R + NN);          // NN symbol
+    uint32_t* heap = reinterpret_cast<uint32_t*>(S + NN);       // kSelBk + 2 keys (1-indexed)
+    uint8_t* len = reinterpret_cast<uint8_t*>(heap + kSelBk + 2);  // kSelBk
+    uint32_t* code = reinterpret_cast<uint32_t*>(len + kSelBk);    // kSelBk
+    int* meta = reinterpret_cast<int*>(code + kSelBk);          // numl[32], entry[32], first[32], next[32]
+    int* numl = meta;
+    int* entry = meta + 32;
+    int* first = meta + 64;
+    int* nxt = meta + 96;
+    int* stk_node = meta + 128;                                 // 64
+    uint32_t* stk_code = reinterpret_cast<uint32_t*>(stk_node + 64);  // 64 (low 27 bits kept)
+    uint8_t* stk_len = reinterpret_cast<uint8_t*>(stk_code + 64);     // 64
+    int* shared_ok = reinterpret_cast<int*>(stk_len + 64);
+    const uint32_t* freq = s.hf_freq + (size_t)c * kSelBk;
+    const int lane = threadIdx.x;
+    for (int i = lane; i < kSelBk; i += 32) len[i] = 0xff;
+    if (lane < 32) {
+        numl[lane] = 0;
+        entry[lane] = 0;
+        first[lane] = 0;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        int nn = 0;
+        for (int sym = 0; sym < kSelBk; sym++) {
+            const uint32_t fq = freq[sym];
+            if (fq) {
+                F[nn] = fq;
+                L[nn] = -1;
+                R[nn] = -1;
+                S[nn] = (uint16_t)sym;
+                nn++;
+            }
+        }
+        // binary min-heap, 1-indexed, of keys freq << 11 | node id (freq <=
+        // 32768, ids < 2048; comparisons look at the frequency only):
+        // insertion stops at a parent whose frequency is <= the new node's;
+        // removal sinks the moved node, taking the right child only when
+        // strictly smaller and swapping only when strictly larger
+        uint32_t* hk = heap;
+        int hs = 0;
+        auto push = [&](int id) {
+            const uint32_t key = (F[id] << 11) | (uint32_t)id, kf = F[id];
+            int i = ++hs;
+            while (i > 1) {
+                const int p = i >> 1;
+                const uint32_t kp = hk[p];
+                if ((kp >> 11) <= kf) break;
+                hk[i] = kp;
+                i = p;
+            }
+            hk[i] = key;
+        };
+        auto pop = [&]() -> int {
+            const uint32_t top = hk[1];
+            const uint32_t moved = hk[hs];
+            hs--;
+            const uint32_t mf = moved >> 11;
+            int i = 1;
+            while (2 * i <= hs) {
+                int ch = 2 * i;
+                uint32_t kc = hk[ch];
+                if (ch + 1 <= hs) {
+                    const uint32_t k2 = hk[ch + 1];
+                    if ((k2 >> 11) < (kc >> 11)) {
+                        ch++;
+                        kc = k2;
+                    }
+                }
+                if (mf > (kc >> 11)) {
+                    hk[i] = kc;
+                    i = ch;
+                } else {
+                    break;
+                }
+            }
+            hk[i] = moved;
+            return (int)(top & 0x7ffu);
+        };
+        const int leaves = nn;
+        for (int i = 0; i < leaves; i++) push(i);
+        while (hs > 1) {  // the first popped node becomes the right child
+            const int right = pop();
+            const int left = pop();
+            F[nn] = F[left] + F[right];
+            L[nn] = (int16_t)left;
+            R[nn] = (int16_t)right;
+            S[nn] = 0;
+            push(nn);
+            nn++;
+        }
+        int ok = 1;
+        if (hs == 1) {  // in-order walk, left = 0, right = 1, depth limit 58
+            int sp = 0;
+            int p = pop();
+            uint32_t cd = 0, ln = 0;
+            while (true) {
+                if (L[p] >= 0 || R[p] >= 0) {
+                    if (sp + 1 > 58 || ln + 1 > 58) {
+                        ok = 0;
+                        break;
+                    }
+                    stk_node[sp] = p;
+                    stk_code[sp] = cd;
+                    stk_len[sp] = (uint8_t)ln;
+                    sp++;
+                    p = L[p];
+                    cd <<= 1;
+                    ln++;
+                } else {
+                    // lengths above 27 become the cutoff length 28 with code 0
+                    len[S[p]] = (uint8_t)(ln > 27 ? 28 : ln);
+                    code[S[p]] = ln > 27 ? 0u : (cd & 0x7ffffffu);
+                    if (sp == 0) break;
+                    sp--;
+                    p = R[stk_node[sp]];
+                    cd = (stk_code[sp] << 1) | 1u;
+                    ln = stk_len[sp] + 1u;
+                    if (ln > 58) {
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        *shared_ok = ok;
+        // canonical form
+        int max_l = 0;
+        for (int sym = 0; sym < kSelBk; sym++)
+            if (len[sym] != 0xff) {
+                numl[len[sym]]++;
+                if (len[sym] > max_l) max_l = len[sym];
+            }
+        for (int i = 1; i < 32; i++) entry[i] = entry[i - 1] + numl[i - 1];
+        for (int i = 0; i < 32; i++) nxt[i] = entry[i];
+        first[max_l] = 0;
+        for (int l = max_l - 1; l >= 1; l--) first[l] = (first[l + 1] + numl[l + 1] + 1) >> 1;
+        first[0] = 0xff;
+    }
+    __syncwarp();
+    if (!*shared_ok) {
+        if (lane == 0) s.sizes[(size_t)c * kSelCoders + 3] = kSelNoFit;
+        return;
+    }
+    // keys / canonical codes (lane 0: slot order is symbol order per length)
+    uint32_t* bk4 = s.hf_book + (size_t)c * kSelBk;
+    uint8_t* blob = s.slots + ((size_t)c * kSelCoders + 3) * kSelSlot;
+    int* rb_first = reinterpret_cast<int*>(blob + 128);
+    uint16_t* keys = reinterpret_cast<uint16_t*>(blob + 128 + 256);
+    for (int i = lane; i < kSelBk; i += 32) {
+        bk4[i] = 0xffffffffu;
+        keys[i] = 0;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        for (int sym = 0; sym < kSelBk; sym++) {
+            if (len[sym] == 0xff) continue;
+            const uint32_t l = len[sym];
+            const int slot = nxt[l]++;
+            bk4[sym] = ((uint32_t)(first[l] + slot - entry[l]) & 0x7ffffffu) | (l << 27);
+            keys[slot] = (uint16_t)sym;
+        }
+    }
+    __syncwarp();
+    rb_first[lane] = first[lane];
+    rb_first[32 + lane] = entry[lane];
+}
+
+__global__ void __launch_bounds__(256) sel_hf_encode_kernel(SelArgs s) {
+    __shared__ uint32_t book[kSelBk];
+    __shared__ uint32_t cells[kHfSublen];
+    __shared__ uint32_t pnbit[kSelParts], pent[kSelParts + 1];
+    __shared__ uint32_t ws[16];
+    const int ci = sel_chunk(s, 3);
+    if (ci < 0) return;
+    const uint32_t c = (uint32_t)ci;
+    if (s.sizes[(size_t)c * kSelCoders + 3] == kSelNoFit) return;
+    const uint32_t cnt = chunk_count(s.n, c), t = threadIdx.x;
+    const uint16_t* src = s.codes + (uint64_t)c * kSelCodes;
+    const uint32_t* bk4 = s.hf_book + (size_t)c * kSelBk;
+    for (uint32_t i = t; i < (uint32_t)kSelBk; i += 256) book[i] = bk4[i];
+    __syncthreads();
+    const uint32_t pardeg = (cnt + kHfSublen - 1) / kHfSublen;
+    // pass 1: bits per partition
+    for (uint32_t p = 0; p < pardeg; p++) {
+        uint32_t bits = 0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const uint32_t i = p * kHfSublen + 3 * t + k;
+            if (i < cnt) bits += book[src[i]] >> 27;
+        }
+        uint32_t tot;
+        block_excl_scan(bits, ws, &tot);
+        if (t == 0) pnbit[p] = tot;
+        __syncthreads();
+    }
+    if (t == 0) {
+        uint32_t e = 0;
+        for (uint32_t p = 0; p < pardeg; p++) {
+            pent[p] = e;
+            e += (pnbit[p] + 31) / 32;
+        }
+        pent[pardeg] = e;
+    }
+    __syncthreads();
+    const uint32_t ncell = pent[pardeg];
+    const uint32_t rb = 256 + 2 * kSelBk;
+    const uint32_t e1 = 128, e2 = e1 + rb, e3 = e2 + 4 * pardeg, e4 = e3 + 4 * pardeg, e5 = e4 + 4 * ncell;
+    if (e5 > (uint32_t)kSelBytes) {
+        if (t == 0) s.sizes[(size_t)c * kSelCoders + 3] = kSelNoFit;
+        return;
+    }
+    uint8_t* blob = s.slots + ((size_t)c * kSelCoders + 3) * kSelSlot;
+    uint32_t* bitstream = reinterpret_cast<uint32_t*>(blob + e4);
+    // pass 2: partitions into their cells
+    for (uint32_t p = 0; p < pardeg; p++) {
+        for (uint32_t i = t; i < (uint32_t)kHfSublen; i += 256) cells[i] = 0;
+        __syncthreads();
+        uint32_t w[3], bits = 0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const uint32_t i = p * kHfSublen + 3 * t + k;
+            w[k] = i < cnt ? book[src[i]] : 0u;
+            bits += w[k] >> 27;
+        }
+        uint32_t tot;
+        uint32_t off = block_excl_scan(bits, ws, &tot);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const uint32_t ln = w[k] >> 27, cd = w[k] & 0x7ffffffu;
+            if (ln) {
+                const uint32_t cell = off >> 5, pos = off & 31;
+                if (pos + ln <= 32) {
+                    atomicOr(&cells[cell], cd << (32 - pos - ln));
+                } else {
+                    const uint32_t spill = pos + ln - 32;
+                    atomicOr(&cells[cell], cd >> spill);
+                    atomicOr(&cells[cell + 1], cd << (32 - spill));
+                }
+            }
+            off += ln;
+        }
+        __syncthreads();
+        const uint32_t nc = (tot + 31) / 32;
+        for (uint32_t i = t; i < nc; i += 256) bitstream[pent[p] + i] = cells[i];
+        __syncthreads();
+    }
+    uint32_t* h32 = reinterpret_cast<uint32_t*>(blob);
+    if (t < 32) h32[t] = 0;
+    __syncthreads();
+    for (uint32_t p = t; p < pardeg; p += 256) {  // per-partition tables
+        reinterpret_cast<uint32_t*>(blob + e2)[p] = pnbit[p];
+        reinterpret_cast<uint32_t*>(blob + e3)[p] = pent[p];
+    }
+    if (t == 0) {
+        uint64_t nbit = 0;
+        for (uint32_t p = 0; p < pardeg; p++) nbit += pnbit[p];
+        h32[0] = kSelBk;
+        h32[1] = kHfSublen;
+        h32[2] = pardeg;
+        h32[4] = cnt;
+        h32[5] = 0;
+        h32[6] = (uint32_t)nbit;
+        h32[7] = (uint32_t)(nbit >> 32);
+        h32[8] = ncell;
+        h32[9] = 0;
+        h32[10] = 0;
+        h32[11] = e1;
+        h32[12] = e2;
+        h32[13] = e3;
+        h32[14] = e4;
+        h32[15] = e5;
+        s.sizes[(size_t)c * kSelCoders + 3] = e5;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Choice and container.
+// ---------------------------------------------------------------------------
+// mode 0: smallest size; mode 1: smallest predicted log-size (pred[c][4]);
+// mode 2 + k: coder k when it fits, else the smallest.
+__global__ void sel_choose_kernel(SelArgs s, uint32_t nchunks, int mode, const float* __restrict__ pred) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchunks) return;
+    const uint32_t* sz = s.sizes + (size_t)c * kSelCoders;
+    int best = -1;
+    if (mode == 1) {
+        float bp = INFINITY;
+        for (int k = 0; k < kSelCoders; k++) {
+            const float v = pred[(size_t)c * kSelCoders + k];
+            if (v < bp) {
+                bp = v;
+                best = k;
+            }
+        }
+    } else if (mode >= 2) {
+        best = mode - 2;
+    }
+    if (best < 0 || sz[best] == kSelNoFit) {  // exhaustive, or the predicted coder does not fit
+        uint32_t bs = kSelNoFit;
+        for (int k = 0; k < kSelCoders; k++)
+            if (sz[k] < bs) {
+                bs = sz[k];
+                best = k;
+            }
+    }
+    s.tags[c] = (uint8_t)best;
+}
+
+// want[c] = the chosen coder only.
+__global__ void sel_tag_mask_kernel(SelArgs s, uint32_t nchunks, uint8_t* __restrict__ want) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nchunks) want[c] = (uint8_t)(1u << s.tags[c]);
+}
+
+// Learned choices whose coder did not fit get the other coders tried.
+__global__ void sel_fallback_kernel(SelArgs s, uint32_t nchunks, uint8_t* __restrict__ want) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchunks) return;
+    const uint32_t k = s.tags[c];
+    want[c] = s.sizes[(size_t)c * kSelCoders + k] == kSelNoFit ? (uint8_t)(0xFu & ~(1u << k)) : (uint8_t)0;
+}
+
+__global__ void sel_header_kernel(SelArgs s, uint32_t nchunks, uint8_t* __restrict__ out,
+                                  unsigned long long* __restrict__ out_size, unsigned long long* __restrict__ offs) {
+    // offs: exclusive scan of padded chosen sizes (one CTA, 1024 threads)
+    __shared__ unsigned long long part[1024];
+    const uint32_t t = threadIdx.x, per = (nchunks + 1023) / 1024;
+    const uint32_t b = t * per, e = min(nchunks, b + per);
+    auto chosen = [&](uint32_t c) {
+        const uint32_t k = s.tags[c];
+        return (s.sizes[(size_t)c * kSelCoders + k] + 3u) & ~3u;
+    };
+    unsigned long long sum = 0;
+    for (uint32_t c = b; c < e; c++) sum += chosen(c);
+    part[t] = sum;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+        const unsigned long long v = t >= (unsigned)d ? part[t - d] : 0ull;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    const uint32_t hdr = 16 + 2 * ((nchunks + 3) & ~3u) + 4 * nchunks;
+    unsigned long long run = hdr + part[t] - sum;
+    uint32_t* h32 = reinterpret_cast<uint32_t*>(out);
+    uint8_t* tags = out + 16;
+    uint8_t* params = tags + ((nchunks + 3) & ~3u);
+    uint32_t* sizes = reinterpret_cast<uint32_t*>(params + ((nchunks + 3) & ~3u));
+    for (uint32_t c = b; c < e; c++) {
+        const uint32_t k = s.tags[c];
+        offs[c] = run;
+        run += chosen(c);
+        tags[c] = (uint8_t)k;
+        params[c] = s.params[c * kSelCoders + k];
+        sizes[c] = s.sizes[(size_t)c * kSelCoders + k];
+    }
+    for (uint32_t c = nchunks + t; c < ((nchunks + 3) & ~3u); c += 1024) {
+        tags[c] = 0;
+        params[c] = 0;
+    }
+    if (t == 1023) {
+        h32[0] = 0x43535A46u;  // "FZSC"
+        h32[1] = nchunks;
+        h32[2] = (uint32_t)s.n;
+        h32[3] = kSelCodes;
+        *out_size = hdr + part[1023];
+    }
+}
+
+__global__ void __launch_bounds__(256) sel_copy_kernel(SelArgs s, uint8_t* __restrict__ out,
+                                                       const unsigned long long* __restrict__ offs) {
+    const uint32_t c = blockIdx.x;
+    const uint32_t k = s.tags[c];
+    const uint32_t len = s.sizes[(size_t)c * kSelCoders + k], plen = (len + 3u) & ~3u;
+    const uint8_t* src = s.slots + ((size_t)c * kSelCoders + k) * kSelSlot;
+    uint8_t* dst = out + offs[c];
+    for (uint32_t i = threadIdx.x; i < plen; i += blockDim.x) dst[i] = i < len ? src[i] : 0;
+}
+
+// ---------------------------------------------------------------------------
+// MLP 16 -> 64 -> 64 -> 4, FP32, ReLU.  Parameters packed as
+// W1[16][64] b1[64] W2[64][64] b2[64] W3[64][4] b3[4] (row = input).
+// One thread per sample; the parameters sit in shared memory.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) mlp_forward_kernel(const float* __restrict__ P, const float* __restrict__ X,
+                                                          float* __restrict__ Y, uint32_t batch) {
+    __shared__ float w[kMlpParams];
+    for (uint32_t i = threadIdx.x; i < (uint32_t)kMlpParams; i += blockDim.x) w[i] = P[i];
+    __syncthreads();
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    const float* W1 = w;
+    const float* B1 = W1 + 16 * 64;
+    const float* W2 = B1 + 64;
+    const float* B2 = W2 + 64 * 64;
+    const float* W3 = B2 + 64;
+    const float* B3 = W3 + 64 * 4;
+    float x[16], h1[64], h2[64];
+#pragma unroll
+    for (int i = 0; i < 16; i++) x[i] = X[(size_t)b * 16 + i];
+    for (int j = 0; j < 64; j++) {
+        float a = B1[j];
+#pragma unroll
+        for (int i = 0; i < 16; i++) a = __fadd_rn(a, __fmul_rn(x[i], W1[i * 64 + j]));
+        h1[j] = fmaxf(a, 0.0f);
+    }
+    for (int j = 0; j < 64; j++) {
+        float a = B2[j];
+        for (int i = 0; i < 64; i++) a = __fadd_rn(a, __fmul_rn(h1[i], W2[i * 64 + j]));
+        h2[j] = fmaxf(a, 0.0f);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        float a = B3[j];
+        for (int i = 0; i < 64; i++) a = __fadd_rn(a, __fmul_rn(h2[i], W3[i * 4 + j]));
+        Y[(size_t)b * 4 + j] = a;
+    }
+}
+
+// Gradients of the mean squared error 1/(4B) sum (Y - T)^2 over the batch,
+// accumulated into G (same packing as P, zeroed by the caller); *loss +=
+// the batch's loss.  Per-sample gradients are summed in shared memory, then
+// added to G once per block.
+__global__ void __launch_bounds__(128) mlp_backward_kernel(const float* __restrict__ P, const float* __restrict__ X,
+                                                           const float* __restrict__ T, uint32_t batch,
+                                                           float* __restrict__ G, float* __restrict__ loss,
+                                                           const int kind) {
+    __shared__ float w[kMlpParams];
+    __shared__ float g[kMlpParams];
+    __shared__ float sl[4];
+    for (uint32_t i = threadIdx.x; i < (uint32_t)kMlpParams; i += blockDim.x) {
+        w[i] = P[i];
+        g[i] = 0.0f;
+    }
+    __syncthreads();
+    const float* W1 = w;
+    const float* B1 = W1 + 16 * 64;
+    const float* W2 = B1 + 64;
+    const float* B2 = W2 + 64 * 64;
+    const float* W3 = B2 + 64;
+    const float* B3 = W3 + 64 * 4;
+    float* gW1 = g;
+    float* gB1 = gW1 + 16 * 64;
+    float* gW2 = gB1 + 64;
+    float* gB2 = gW2 + 64 * 64;
+    float* gW3 = gB2 + 64;
+    float* gB3 = gW3 + 64 * 4;
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (b < batch) {
+        float x[16], h1[64], h2[64], dy[4];
+#pragma unroll
+        for (int i = 0; i < 16; i++) x[i] = X[(size_t)b * 16 + i];
+        for (int j = 0; j < 64; j++) {
+            float a = B1[j];
+#pragma unroll
+            for (int i = 0; i < 16; i++) a = __fadd_rn(a, __fmul_rn(x[i], W1[i * 64 + j]));
+            h1[j] = fmaxf(a, 0.0f);
+        }
+        for (int j = 0; j < 64; j++) {
+            float a = B2[j];
+            for (int i = 0; i < 64; i++) a = __fadd_rn(a, __fmul_rn(h1[i], W2[i * 64 + j]));
+            h2[j] = fmaxf(a, 0.0f);
+        }
+        float y[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float a = B3[j];
+            for (int i = 0; i < 64; i++) a = __fadd_rn(a, __fmul_rn(h2[i], W3[i * 4 + j]));
+            y[j] = a;
+        }
+        if (kind == 0) {  // mean squared error against T
+            const float scale = 2.0f / (4.0f * (float)batch);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float d = y[j] - T[(size_t)b * 4 + j];
+                l += d * d / 4.0f;
+                dy[j] = scale * d;
+            }
+        } else {  // cross-entropy of p = softmax(-y) against q = softmax(-T / tau), T = regrets
+            const float m = fminf(fminf(y[0], y[1]), fminf(y[2], y[3]));
+            float tr[4], e[4], qv[4], z = 0.0f, zq = 0.0f, tmin = INFINITY;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                tr[j] = T[(size_t)b * 4 + j];
+                tmin = fminf(tmin, tr[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                e[j] = __expf(m - y[j]);
+                z += e[j];
+                qv[j] = __expf((tmin - tr[j]) * (1.0f / kMlpTau));
+                zq += qv[j];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float p = e[j] / z, q = qv[j] / zq;
+                l -= q * (__logf(e[j]) - __logf(z));
+                dy[j] = (q - p) / (float)batch;
+            }
+        }
+        // layer 3
+        float dh2[64];
+        for (int i = 0; i < 64; i++) {
+            float a = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                atomicAdd(&gW3[i * 4 + j], h2[i] * dy[j]);
+                a += W3[i * 4 + j] * dy[j];
+            }
+            dh2[i] = h2[i] > 0.0f ? a : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) atomicAdd(&gB3[j], dy[j]);
+        // layer 2 (dh1 reuses h1's storage after its use)
+        float dh1[64];
+        for (int i = 0; i < 64; i++) dh1[i] = 0.0f;
+        for (int j = 0; j < 64; j++) {
+            const float d = dh2[j];
+            if (d == 0.0f) continue;
+            atomicAdd(&gB2[j], d);
+            for (int i = 0; i < 64; i++) {
+                atomicAdd(&gW2[i * 64 + j], h1[i] * d);
+                dh1[i] += W2[i * 64 + j] * d;
+            }
+        }
+        for (int j = 0; j < 64; j++) {
+            const float d = h1[j] > 0.0f ? dh1[j] : 0.0f;
+            if (d == 0.0f) continue;
+            atomicAdd(&gB1[j], d);
+#pragma unroll
+            for (int i = 0; i < 16; i++) atomicAdd(&gW1[i * 64 + j], x[i] * d);
+        }
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) l += __shfl_xor_sync(0xffffffffu, l, d);
+    if ((threadIdx.x & 31) == 0) sl[threadIdx.x >> 5] = l;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < (uint32_t)kMlpParams; i += blockDim.x)
+        if (g[i] != 0.0f) atomicAdd(&G[i], g[i]);
+    if (threadIdx.x == 0) atomicAdd(loss, (sl[0] + sl[1] + sl[2] + sl[3]) / (float)batch);
+}
+
+// Adam (beta1 0.9, beta2 0.999, eps 1e-8); step counts from 1.
+__global__ void mlp_adam_kernel(float* __restrict__ P, const float* __restrict__ G, float* __restrict__ M,
+                                float* __restrict__ V, float lr, int step) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint32_t)kMlpParams) return;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float g = G[i];
+    const float m = b1 * M[i] + (1.0f - b1) * g;
+    const float v = b2 * V[i] + (1.0f - b2) * g * g;
+    M[i] = m;
+    V[i] = v;
+    const float mh = m / (1.0f - powf(b1, (float)step));
+    const float vh = v / (1.0f - powf(b2, (float)step));
+    P[i] -= lr * mh / (sqrtf(vh) + 1e-8f);
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+int launch_sel_features(const uint16_t* codes, uint64_t n, float* feats, cudaStream_t s) {
+    const uint32_t nch = (uint32_t)((n + kSelCodes - 1) / kSelCodes);
+    sel_features_kernel<<<nch, 256, 0, s>>>(codes, n, feats);
+    return (int)cudaGetLastError();
+}
+
+// F[NN] L[NN] R[NN] S[NN] heap[kSelBk+2] len[kSelBk] code[kSelBk] meta[192]
+// stk_code[64] stk_len[64] ok
+size_t sel_book_smem() {
+    constexpr size_t NN = 2 * kSelBk;
+    return NN * 4 + NN * 2 * 3 + (kSelBk + 2) * 4 + kSelBk + kSelBk * 4 + 4 * (128 + 64) + 64 * 4 + 64 + 16;
+}
+
+int launch_sel_tag_mask(const SelArgs& a, uint32_t nchunks, uint8_t* want, cudaStream_t s) {
+    sel_tag_mask_kernel<<<(nchunks + 255) / 256, 256, 0, s>>>(a, nchunks, want);
+    return (int)cudaGetLastError();
+}
+
+int launch_sel_fallback_mask(const SelArgs& a, uint32_t nchunks, uint8_t* want, cudaStream_t s) {
+    sel_fallback_kernel<<<(nchunks + 255) / 256, 256, 0, s>>>(a, nchunks, want);
+    return (int)cudaGetLastError();
+}
+
+int launch_sel_coders(const SelArgs& a, uint32_t nlist, unsigned coder_mask, cudaStream_t s) {
+    if (nlist == 0) return 0;
+    cudaError_t e;
+    if (coder_mask & 1u) {
+        const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
+        e = cudaFuncSetAttribute(sel_rze_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return (int)e;
+        sel_rze_sub_kernel<<<dim3(nlist, 4), kThreads, smem, s>>>(a);
+        sel_rze_assemble_kernel<<<nlist, 256, 0, s>>>(a);
+    }
+    if (coder_mask & 2u) sel_rle_kernel<<<nlist, 256, 0, s>>>(a);
+    if (coder_mask & 4u) sel_bitpack_kernel<<<nlist, 256, 0, s>>>(a);
+    if (coder_mask & 8u) {
+        sel_hf_hist_kernel<<<nlist, 256, 0, s>>>(a);
+        const int smem = (int)sel_book_smem();
+        e = cudaFuncSetAttribute(sel_hf_book_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return (int)e;
+        sel_hf_book_kernel<<<nlist, 32, smem, s>>>(a);
+        sel_hf_encode_kernel<<<nlist, 256, 0, s>>>(a);
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_sel_choose(const SelArgs& a, uint32_t nchunks, int mode, const float* pred, cudaStream_t s) {
+    sel_choose_kernel<<<(nchunks + 255) / 256, 256, 0, s>>>(a, nchunks, mode, pred);
+    return (int)cudaGetLastError();
+}
+
+int launch_sel_container(const SelArgs& a, uint32_t nchunks, uint8_t* out, unsigned long long* out_size,
+                         unsigned long long* offs, cudaStream_t s) {
+    sel_header_kernel<<<1, 1024, 0, s>>>(a, nchunks, out, out_size, offs);
+    sel_copy_kernel<<<nchunks, 256, 0, s>>>(a, out, offs);
+    return (int)cudaGetLastError();
+}
+
+int launch_mlp_forward(const float* P, const float* X, float* Y, uint32_t batch, cudaStream_t s) {
+    mlp_forward_kernel<<<(batch + 127) / 128, 128, 0, s>>>(P, X, Y, batch);
+    return (int)cudaGetLastError();
+}
+
+int launch_mlp_backward(const float* P, const float* X, const float* T, uint32_t batch, float* G, float* loss,
+                        int kind, cudaStream_t s) {
+    mlp_backward_kernel<<<(batch + 127) / 128, 128, 0, s>>>(P, X, T, batch, G, loss, kind);
+    return (int)cudaGetLastError();
+}
+
+int launch_mlp_adam(float* P, const float* G, float* M, float* V, float lr, int step, cudaStream_t s) {
+    mlp_adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, s>>>(P, G, M, V, lr, step);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace fzb

@@ -97,3 +97,44 @@ def fractal2d(n: int, seed: int, octaves: int = 6, persistence: float = 0.5,
     out = out / total
     out = (out - out.min()) / (out.max() - out.min()) * 100.0 - 50.0
     return out.contiguous()
+
+
+def piecewise(n: int, seed: int, min_run: int = 10, max_run: int = 1000, device="cpu") -> torch.Tensor:
+    """Piecewise-constant values: runs of 10-1000 cells, each run N(0, 1)."""
+    g = _gen(seed, device)
+    runs = torch.randint(min_run, max_run + 1, (n // min_run + 2,), generator=g, device=device)
+    ends = torch.cumsum(runs, 0)
+    k = int(torch.searchsorted(ends, torch.tensor([n], device=device)).item()) + 1
+    vals = torch.randn(k, generator=g, device=device)
+    rid = torch.searchsorted(ends[:k], torch.arange(n, device=device), right=True)
+    return vals[rid.clamp(max=k - 1)].to(torch.float32).contiguous()
+
+
+def noise(n: int, seed: int, device="cpu") -> torch.Tensor:
+    """White noise N(0, 1)."""
+    return torch.randn(n, generator=_gen(seed, device), device=device, dtype=torch.float32)
+
+
+def sparse(n: int, seed: int, density: float = 0.05, device="cpu") -> torch.Tensor:
+    """95 % zeros, the rest N(0, 1)."""
+    g = _gen(seed, device)
+    v = torch.randn(n, generator=g, device=device, dtype=torch.float32)
+    keep = torch.rand(n, generator=g, device=device) < density
+    return torch.where(keep, v, torch.zeros_like(v)).contiguous()
+
+
+def mixed_field(kind: str, shape, seed: int, device="cpu") -> torch.Tensor:
+    """One field of the learned-selector workload: 'smooth' (GRF k^-3),
+    'piecewise', 'noise' or 'sparse'; shape (nz, ny, nx)."""
+    n = 1
+    for s in shape:
+        n *= int(s)
+    if kind == "smooth":
+        return grf(shape, seed=seed, device=device).reshape(-1)
+    if kind == "piecewise":
+        return piecewise(n, seed, device=device)
+    if kind == "noise":
+        return noise(n, seed, device=device)
+    if kind == "sparse":
+        return sparse(n, seed, device=device)
+    raise ValueError(kind)

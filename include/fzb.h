@@ -267,6 +267,57 @@ int fzb_batch_autotune(const fzb_batch_field* fields, int nfields, void* d_work,
                        fzb_batch_tuning* best, float* best_ms);
 
 /* ------------------------------------------------------------------------
+ * Per-chunk lossless coding with a learned coder selector (no reference
+ * counterpart; every coder's bytes are its stage's bytes on that chunk).
+ * Codes are cut into 64 KiB chunks (FZB_SEL_CHUNK_CODES); each chunk is
+ * coded by one of: 0 Bitshuffle(16 KiB, ew 2) -> RZE, 1 RLE<u16>,
+ * 2 Bitpack<u16> (detected nbits), 3 Huffman<u16> (bklen 1024, coarse).
+ * Container: [u32 "FZSC"][u32 nchunks][u32 n][u32 chunk codes]
+ *            [u8 tag x nchunks, pad 4][u8 param x nchunks, pad 4]
+ *            [u32 size x nchunks][payloads, each padded to 4].
+ * Modes: exhaustive trial (smallest output; also the labeller), learned
+ * (features -> MLP -> predicted smallest; a pick that does not fit falls
+ * back to trying the other coders), or one fixed coder.
+ * MLP: 16 -> 64 -> 64 -> 4 FP32 with ReLU, FZB_MLP_PARAMS floats packed as
+ * W1[16][64] b1[64] W2[64][64] b2[64] W3[64][4] b3[4]; it regresses the
+ * four coders' costs; a chunk is coded with the coder of the smallest
+ * output.  fzb_mlp_grad computes the batch gradient and loss of either the
+ * mean squared error against targets T (FZB_MLP_MSE, T = log2(size/65536))
+ * or the cross-entropy of softmax(-y) against the soft labels
+ * softmax(-T / 0.02) (FZB_MLP_REGRET, T_k = log2(size_k / smallest size));
+ * fzb_mlp_adam applies one Adam step.
+ * ------------------------------------------------------------------------ */
+#define FZB_SEL_CHUNK_CODES 32768
+#define FZB_SEL_FEATURES 16
+#define FZB_SEL_CODERS 4
+#define FZB_MLP_PARAMS 5508
+#define FZB_SEL_EXHAUSTIVE 0
+#define FZB_SEL_LEARNED 1
+#define FZB_SEL_FIXED(k) (2 + (k))
+uint64_t fzb_sel_chunks(uint64_t n);
+size_t fzb_sel_workspace_bytes(uint64_t n);
+uint64_t fzb_sel_max_bytes(uint64_t n);
+/* d_feats[nchunks][16] */
+int fzb_sel_features(const uint16_t* d_codes, uint64_t n, float* d_feats, void* stream);
+/* every coder's output size per chunk (d_sizes[nchunks][4], 0xFFFFFFFF =
+ * does not fit / not applicable): the exhaustive-trial labels */
+int fzb_sel_trial(const uint16_t* d_codes, uint64_t n, uint32_t* d_sizes, void* d_work, size_t work_bytes,
+                  void* stream);
+/* container into d_out (fzb_sel_max_bytes), size to *d_out_size (device
+ * u64), chosen coder per chunk to d_tags (optional); d_params for LEARNED */
+int fzb_sel_encode(const uint16_t* d_codes, uint64_t n, int mode, const float* d_params, void* d_out,
+                   uint64_t* d_out_size, uint8_t* d_tags, void* d_work, size_t work_bytes, void* stream);
+/* synchronous; work_bytes >= fzb_workspace_bytes(32768, 0) + 131328 */
+int fzb_sel_decode(const void* d_in, uint64_t in_bytes, uint16_t* d_codes, uint64_t n, void* d_work,
+                   size_t work_bytes, void* stream);
+int fzb_mlp_forward(const float* d_params, const float* d_x, float* d_y, uint32_t batch, void* stream);
+#define FZB_MLP_MSE 0
+#define FZB_MLP_REGRET 1
+int fzb_mlp_grad(const float* d_params, const float* d_x, const float* d_t, uint32_t batch, int loss_kind,
+                 float* d_grad, float* d_loss, void* stream);
+int fzb_mlp_adam(float* d_params, const float* d_grad, float* d_m, float* d_v, float lr, int step, void* stream);
+
+/* ------------------------------------------------------------------------
  * Pipelines: C view of fz::Pipeline (include/fz/pipeline.h), the reference's
  * Pipeline API (include/pipeline/compressor.h:34-386) for bindings without
  * C++ interop.  A pipeline is an opaque handle; stages are the indices the
