@@ -10,6 +10,8 @@ end-to-end (host buffers, copies inside the timed region) figures, the CPU
 baseline and clock samples sit beside it in the same JSON line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --workload c1|c3|batch|selector   (secondary workloads,
+      one JSON line each; fzgpumodules_b200/benchmarks.py)
 
 Under torchrun each rank compresses its own field (no data exchange: the
 path shards by field); timings are maxed over ranks.
@@ -361,7 +363,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--dims", type=int, nargs=3, default=list(DEFAULT_DIMS), metavar=("NX", "NY", "NZ"),
                     help="field extents (x fastest); the default is the 512^3 workload")
+    ap.add_argument("--workload", default="chain", choices=["chain", "c1", "c3", "batch", "selector"],
+                    help="chain: the headline LQ3D->BS->RZE line; others: secondary workloads (1 GPU)")
     args = ap.parse_args()
+    if args.workload != "chain":
+        import torch
+
+        from fzgpumodules_b200 import benchmarks
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(benchmarks.WORKLOADS[args.workload](args, torch.device("cuda", 0)), flush=True)
+        return
     world, rank, local = dist_setup() if args.impl == "ours" else (
         int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
     if args.impl == "reference":

@@ -1,0 +1,220 @@
+"""Secondary benchmark workloads (``bench.py --workload ...``), each printed
+as one JSON line with the same keys as the headline line:
+
+* ``c1``        LorenzoQuant 2-D (ABS 1e-4) -> RLE on the 1800 x 3600 sinusoid
+                field, through fz::Pipeline (the Quick Start chain);
+* ``c3``        LorenzoQuant 2-D (ABS 1e-3, radius 512, zigzag) -> Huffman
+                (bklen 1024) on an 8192^2 fractal field, with and without
+                the host codebook in the timed region;
+* ``batch``     64 fields (log-uniform 1 MB - 256 MB, mixed ranks, REL eb in
+                {1e-2, 1e-3, 1e-4}) through the batched chain replayed from one
+                CUDA graph, against 64 plain per-field calls;
+* ``selector``  2 GiB of mixed fields -> LorenzoQuant (REL 1e-3) codes in 64 KiB
+                chunks, coded by exhaustive trial and by the trained MLP selector.
+
+Timing: CUDA events on the launching stream after warm-up; inputs larger than
+L2 or an L2 flush between timed iterations.
+"""
+from __future__ import annotations
+
+import json
+import time
+
+import numpy as np
+import torch
+
+from . import fields as F
+from . import kernels as K
+
+
+def _events():
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _time(fn, steps: int, warmup: int, flush: torch.Tensor | None = None) -> float:
+    """Mean device milliseconds of fn() over `steps` timed calls."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(steps):
+        if flush is not None:
+            flush.zero_()
+        a, b = _events()
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    return tot / steps
+
+
+def _line(workload: str, value: float, unit: str, args, extra: dict) -> str:
+    d = {"metric": "comp/decomp GB/s and % HBM roofline at fixed eb; ratio, learned vs exhaustive",
+         "workload": workload, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+         "warmup": args.warmup, "higher_is_better": True, "dtype": "f32", "data": "synthetic"}
+    d.update(extra)
+    return json.dumps(d)
+
+
+def run_c1(args, dev):
+    from .pipeline import LorenzoQuantStage, Pipeline, RLEStage, ABS, PREALLOCATE
+    x = F.sinusoids2d(1800, 3600, seed=1001, device=dev).reshape(-1)
+    n = x.numel()
+    pl = Pipeline(n * 4, PREALLOCATE)
+    pl.setDims(3600, 1800, 1)
+    lq = pl.addStage(LorenzoQuantStage(1e-4, 32768, 0.2, ABS, False))
+    rle = pl.addStage(RLEStage(2))
+    pl.connect(rle, lq, "codes")
+    pl.finalize()
+    comp = pl.compress(x).clone()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    tc = _time(lambda: pl.compress(x), args.steps, args.warmup, flush)
+    td = _time(lambda: pl.decompress(comp), args.steps, args.warmup, flush)
+    y = pl.decompress(comp)[:n]
+    err = float((y - x).abs().max())
+    pl.close()
+    return _line("c1: LorenzoQuant2D(ABS 1e-4)->RLE, 1800x3600 sinusoids, fz::Pipeline", 4 * n / tc / 1e6,
+                 "GB/s", args, {"compress_ms": tc, "decompress_ms": td, "decompress_gbs": 4 * n / td / 1e6,
+                                "ratio": 4 * n / comp.numel(), "max_abs_err": err,
+                                "note": "Pipeline calls include their host synchronisation, as the reference's do"})
+
+
+def run_c3(args, dev):
+    x = F.fractal2d(8192, seed=1003, device=dev).reshape(-1)
+    n = x.numel()
+    dims = (8192, 8192, 1)
+    ws = K.Workspace()
+    out = K.lq_forward(x, dims, 1e-3, K.ABS, 512, True, 0.2, ws=ws)
+    codes = out["codes"]
+    hws = K.Workspace()
+    blob, size = K.huff_compress(codes, 1024, ws=hws)
+    freq = K.huff_histogram(codes, 1024)
+    bk4, rb = K.huff_book(freq, 1024)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    t_lq = _time(lambda: K.lq_forward(x, dims, 1e-3, K.ABS, 512, True, 0.2, ws=ws), args.steps, args.warmup, flush)
+    t_hist = _time(lambda: K.huff_histogram(codes, 1024), args.steps, args.warmup, flush)
+    t_enc = _time(lambda: K.huff_encode(codes, bk4, rb, 1024, ws=hws, trim=False), args.steps, args.warmup, flush)
+    t_full = _time(lambda: K.huff_compress(codes, 1024, ws=hws, trim=False), args.steps, args.warmup, flush)
+    dec = torch.empty(n, dtype=torch.uint16, device=dev)
+    t_dec = _time(lambda: K.huff_decode(blob, n, 1024, ws=hws, out=dec), args.steps, args.warmup, flush)
+    t0 = time.perf_counter()
+    for _ in range(10):
+        K.huff_book(freq, 1024)
+    t_book = (time.perf_counter() - t0) / 10 * 1e3
+    assert torch.equal(K.huff_decode(blob, n, 1024), codes)
+    comp_bytes = blob.numel() + 8 * min(int(out["count"].item()), out["cap"]) + 4
+    return _line("c3: LorenzoQuant2D(ABS 1e-3, r512, zigzag)->Huffman(1024), 8192^2 fractal", 4 * n / (t_lq + t_full) / 1e6,
+                 "GB/s", args, {"lq_ms": t_lq, "huffman_histogram_ms": t_hist, "huffman_book_host_ms": t_book,
+                                "huffman_encode_ms": t_enc, "huffman_compress_ms_with_book": t_full,
+                                "huffman_decode_ms": t_dec, "compress_gbs_without_book": 4 * n / (t_lq + t_hist + t_enc) / 1e6,
+                                "decode_gbs_codes": 2 * n / t_dec / 1e6, "ratio": 4 * n / comp_bytes,
+                                "bits_per_code": 8 * blob.numel() / n})
+
+
+def batch_fields(dev, count=64, seed=1004, max_mb=256):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        nbytes = int(np.exp(rng.uniform(np.log(1 << 20), np.log(max_mb << 20))))
+        n = max(nbytes // 4, 1024)
+        rank = int(rng.integers(1, 4))
+        if rank == 1:
+            dims = (n, 1, 1)
+        elif rank == 2:
+            nx = int(rng.choice([256, 512, 1000, 1024, 2048, 3000]))
+            dims = (nx, max(n // nx, 2), 1)
+        else:
+            nx = int(rng.choice([64, 128, 200, 256, 512]))
+            ny = int(rng.choice([64, 128, 256]))
+            dims = (nx, ny, max(n // (nx * ny), 2))
+        shape = tuple(d for d in reversed(dims) if d > 1) or (dims[0],)
+        x = F.grf(shape, seed=seed + i, spike_frac=1e-3, device=dev).reshape(-1).contiguous()
+        out.append(dict(x=x, dims=dims, eb=float(rng.choice([1e-2, 1e-3, 1e-4])), mode=K.REL, radius=32768,
+                        zigzag=True, outlier_capacity=0.1))
+    return out
+
+
+def run_batch(args, dev):
+    fields = batch_fields(dev)
+    total = sum(f["x"].numel() * 4 for f in fields)
+    b = K.Batch(fields)
+    best, tune_ms = b.autotune()
+    s = torch.cuda.Stream(device=dev)
+    b.launch(s)
+    s.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        b.launch(s)
+    torch.cuda.synchronize()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    t_batch = _time(lambda: g.replay(), args.steps, args.warmup, flush)
+    ws = K.Workspace()
+    plain_out = [None] * len(fields)
+
+    def plain():
+        for i, f in enumerate(fields):
+            plain_out[i] = K.lq_bs_rze_compress(f["x"], f["dims"], f["eb"], f["mode"], f["radius"], f["zigzag"],
+                                                f["outlier_capacity"], ws=ws, out=plain_out[i])
+    t_plain = _time(plain, args.steps, args.warmup, flush)
+    torch.cuda.synchronize()
+    same = all(int(o["rze_size"].item()) == int(p["rze_size"].item()) and
+               torch.equal(o["rze"][: int(o["rze_size"].item())], p["rze"][: int(p["rze_size"].item())])
+               for o, p in zip(b.outputs, plain_out))
+    comp = sum(int(o["rze_size"].item()) + 8 * min(int(o["count"].item()), o["cap"]) + 4 for o in b.outputs)
+    del g
+    b.close()
+    return _line("batch: 64 fields 1-256 MB, mixed rank, REL {1e-2,1e-3,1e-4}, LQ->BS->RZE", total / t_batch / 1e6,
+                 "GB/s", args, {"batched_ms": t_batch, "plain_ms": t_plain, "plain_gbs": total / t_plain / 1e6,
+                                "speedup_vs_plain": t_plain / t_batch, "bytes_identical": same,
+                                "tuning": {"ctas_per_sm": best.ctas_per_sm, "order": best.order},
+                                "autotune_best_ms": tune_ms, "total_bytes": total, "ratio": total / comp,
+                                "launches_per_batch": 5})
+
+
+def run_selector(args, dev):
+    from . import selector as S
+    kinds = ("smooth", "piecewise", "noise", "sparse")
+    # 2 GiB: 32 fields of 64 MiB (256 x 256 x 256), eight per kind
+    codes = []
+    for i in range(32):
+        x = F.mixed_field(kinds[i % 4], (256, 256, 256), 1005 + i, device=dev)
+        codes.append(K.lq_forward(x, (256, 256, 256), 1e-3, K.REL, 32768, True, 0.2)["codes"])
+        del x
+    codes = torch.cat(codes)
+    # training set: method-generated chunks (other seeds and shape), labelled
+    # by exhaustive trial; trained with the library's own MLP kernels
+    t0 = time.perf_counter()
+    tr = S.method_codes(192, seed=500, device=dev)
+    X = S.features(tr)
+    T = S.regrets_from_sizes(S.trial_sizes(tr))
+    del tr
+    sel = S.CoderSelector(seed=0, device=dev)
+    losses = sel.train(X, T, epochs=60, batch=256, lr=3e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    t_ex = _time(lambda: S.encode(codes, S.EXHAUSTIVE, trim=False), args.steps, args.warmup, flush)
+    t_le = _time(lambda: S.encode(codes, S.LEARNED, sel, trim=False), args.steps, args.warmup, flush)
+    with K.Trace():
+        S.encode(codes, S.LEARNED, sel, trim=False)
+        torch.cuda.synchronize()
+        learned_kernels = {k: round(v[1], 3) for k, v in K.Trace.kernels().items()}
+    pre = codes[: 1 << 22]  # decode runs a host loop per chunk: check a 128-chunk prefix
+    blob, _ = S.encode(pre, S.LEARNED, sel)
+    ok = bool(torch.equal(S.decode(blob, pre.numel()), pre))
+    r = S.compare(codes, sel)
+    nbytes = codes.numel() * 2
+    return _line("selector: 2 GiB mixed fields -> LQ(REL 1e-3) codes, 64 KiB chunks, MLP 16-64-64-4",
+                 nbytes / t_le / 1e6, "GB/s", args,
+                 {"learned_ms": t_le, "exhaustive_ms": t_ex, "exhaustive_gbs": nbytes / t_ex / 1e6,
+                  "speedup_vs_exhaustive": t_ex / t_le, "ratio_learned": r["ratio_learned"],
+                  "ratio_exhaustive": r["ratio_exhaustive"], "ratio_best_fixed": r["ratio_best_fixed"],
+                  "learned_over_exhaustive": r["ratio_learned"] / r["ratio_exhaustive"],
+                  "choice_agreement": r["agreement"], "train_chunks": int(X.shape[0]), "train_seconds": t_train,
+                  "final_loss": losses[-1], "chunks": int(S.nchunks(codes.numel())),
+                  "learned_kernel_ms": learned_kernels, "decode_prefix_identical": ok,
+                  "bytes_unit": "GB/s of 16-bit codes (2 B per value)"})
+
+
+WORKLOADS = {"c1": run_c1, "c3": run_c3, "batch": run_batch, "selector": run_selector}

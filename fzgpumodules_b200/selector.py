@@ -99,8 +99,10 @@ def regrets_from_sizes(sizes: torch.Tensor) -> torch.Tensor:
     return r.to(torch.float32)
 
 
-def encode(codes: torch.Tensor, mode: int, selector: "CoderSelector | None" = None):
-    """Container bytes (trimmed), and the chosen coder per chunk."""
+def encode(codes: torch.Tensor, mode: int, selector: "CoderSelector | None" = None, trim: bool = True):
+    """Container bytes (trimmed), and the chosen coder per chunk.  With
+    trim=False nothing synchronises: returns (buffer at capacity, tags,
+    device size)."""
     c = codes.reshape(-1)
     dev = c.device
     nch = nchunks(c.numel())
@@ -111,6 +113,8 @@ def encode(codes: torch.Tensor, mode: int, selector: "CoderSelector | None" = No
     params = _p(selector.params) if selector is not None else None
     check(lib().fzb_sel_encode(_p(c), c.numel(), mode, params, _p(out), _p(size), _p(tags), wp, wn, _s(dev)),
           "fzb_sel_encode")
+    if not trim:
+        return out, tags, size
     return out[: int(size.item())], tags
 
 
