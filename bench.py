@@ -260,7 +260,7 @@ def run_ours(args, world, rank, local):
         launches, ms = per_kernel.get(name, (0, 0.0))
         return launches, max_over_ranks(ms / launches / 1e3 if launches else 0.0, world)
 
-    slab_name = "lq3d_slab_bs_rze" if "lq3d_slab_bs_rze" in per_kernel else "lq_chunk_bs_rze"
+    slab_name = next((k for k in ("lq3d_tma_bs_rze", "lq3d_slab_bs_rze") if k in per_kernel), "lq_chunk_bs_rze")
     inv_name = "fused_inverse_3d" if "fused_inverse_3d" in per_kernel else "lq_inverse"
     n_slab, t_slab = kern(slab_name)
     n_inv, t_inv = kern(inv_name)

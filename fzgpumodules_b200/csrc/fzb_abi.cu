@@ -83,10 +83,12 @@ Work carve(void* base, uint64_t n_total, uint64_t cap) {
 inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 
 // FZB_DISABLE_SLAB=1 routes 3-D fused compression through the per-chunk
-// kernel (both produce identical bytes; tests exercise each).
+// kernel, FZB_DISABLE_SLAB=2 through the cp.async slab kernel instead of the
+// TMA one (all produce identical bytes; tests exercise each).
 inline unsigned flags_env() {
     const char* v = getenv("FZB_DISABLE_SLAB");
-    return (v && v[0] == '1') ? 1u : 0u;
+    if (!v) return 0u;
+    return v[0] == '1' ? 1u : (v[0] == '2' ? 2u : 0u);
 }
 
 #define CK(call)                                          \
@@ -236,8 +238,13 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        TraceScope ts(s, "lq3d_slab_bs_rze");
-        rc = launch_lq3d_slab(a, (unsigned)(2 * sms), s) == 0 ? FZB_OK : FZB_E_CUDA;
+        if (lq3d_tma_supported(a) && !(flags_env() & 2)) {
+            TraceScope ts(s, "lq3d_tma_bs_rze");
+            rc = launch_lq3d_tma(a, (unsigned)(2 * sms), s) == 0 ? FZB_OK : FZB_E_CUDA;
+        } else {
+            TraceScope ts(s, "lq3d_slab_bs_rze");
+            rc = launch_lq3d_slab(a, (unsigned)(2 * sms), s) == 0 ? FZB_OK : FZB_E_CUDA;
+        }
     } else {
         TraceScope ts(s, fused ? "lq_chunk_bs_rze" : "lq_chunk");
         rc = launch_lq(g, fused, a, lq_smem_bytes(g, fused), (uint32_t)nch, s);
@@ -303,7 +310,7 @@ int read_status(const Work& w, cudaStream_t s, uint32_t* bits) {
 
 int status_of(uint32_t bits) {
     if (bits & kErrMalformed) return FZB_E_MALFORMED;
-    if (bits & kErrLookbackTimeout) return FZB_E_TIMEOUT;
+    if (bits & (kErrLookbackTimeout | kErrTmaTimeout)) return FZB_E_TIMEOUT;
     return FZB_OK;
 }
 

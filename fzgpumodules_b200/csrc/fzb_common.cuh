@@ -20,6 +20,7 @@ constexpr uint32_t kErrLookbackTimeout = 1u;
 constexpr uint32_t kErrMalformed = 2u;
 constexpr uint32_t kErrInexact = 4u;      // fused inverse left the exact-integer regime
 constexpr uint32_t kErrUnsorted = 8u;     // outlier indices not ascending
+constexpr uint32_t kErrTmaTimeout = 16u;  // a TMA copy did not complete within its bound
 
 // Round half away from zero (the float overload of `round` that the
 // reference applies to x * ebx2_r).  v - trunc(v) is exact in FP32.

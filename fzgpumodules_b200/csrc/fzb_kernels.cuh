@@ -95,6 +95,10 @@ int launch_lq_chunk(int ndim, bool fused, bool rowal, const FwdArgs& a, size_t s
                     unsigned grid, cudaStream_t s);
 // Slab-column fused 3-D kernel (see fzb_forward.cu); `grid` persistent CTAs.
 int launch_lq3d_slab(const FwdArgs& a, unsigned grid, cudaStream_t s);
+// TMA-fed slab kernel (fzb_slab.cu): same applicability and bytes, plus a
+// 16-byte aligned input and radius <= 2^21.
+bool lq3d_tma_supported(const FwdArgs& a);
+int launch_lq3d_tma(const FwdArgs& a, unsigned grid, cudaStream_t s);
 __global__ void bitshuffle2_kernel(const uint8_t* in, uint8_t* out, int inverse);
 __global__ void bitshuffle_ballot_kernel(const uint8_t* in, uint8_t* out, uint32_t block, int ew,
                                          int inverse);

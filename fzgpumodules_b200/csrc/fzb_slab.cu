@@ -1,0 +1,694 @@
+// fzb_slab.cu -- TMA-fed slab kernel for the fused 3-D chain
+// LorenzoQuant(3-D) -> Bitshuffle(16 KiB, element width 2) -> RZE(16 KiB).
+//
+// Applies to 3-D fields whose 8192-element chunks are R = 8192/nx whole rows
+// (nx a power of two in [32, 1024], ny % R == 0, no padding).  A work unit is
+// one R-row slab across one 8-plane z tile; the unit's chunks are produced
+// plane by plane by one persistent CTA of 256 threads.
+//
+// Data flow per chunk (= one slab plane):
+//   * one thread issues a 2-D TMA copy of the 32 KiB plane into a 128-byte
+//     swizzled shared buffer, two planes ahead of use (double buffer,
+//     mbarrier completion, bounded waits);
+//   * thread t owns chunk elements 32t..32t+31 (one 32-wide x segment of one
+//     row).  It quantizes them (packed f32x2 arithmetic), forms the z
+//     difference against the previous plane's q held in registers and the x
+//     difference in registers, writes B = (z, x)-differenced values back over
+//     its own bytes of the buffer, and after one barrier reads the row above
+//     for the y difference (lorenzo_quant_nd.cu:236-246 order);
+//   * codes come from the exact integer-valued deltas through the float
+//     magic-number conversion (c + 1.5*2^23 holds c in its low mantissa
+//     bits), zigzag works on packed code pairs, outliers are found per
+//     4-element granule with a NaN-propagating max;
+//   * the 32 codes are bit-transposed in registers (the Bitshuffle ballot
+//     layout, bitshuffle_stage.cu:299-323) and RZE level 1 is built straight
+//     from the registers: per-plane nonzero-byte counts are scanned per warp
+//     (8-bit fields), warp 0 turns the warp totals into byte offsets, and each
+//     thread compacts the nonzero bytes of each of its plane words (byte
+//     permute) into zeroed shared memory with two shared atomics; the level-1
+//     bitmap is formed by an 8-lane byte transpose.  Levels 2-4 follow
+//     (rze_stage.cu:324-445), levels 3-4 in warp 0 alone;
+//   * the encoded chunk goes to its 16 KiB slot; assemble_scan/assemble_copy
+//     (fzb_forward.cu) place slots and staged outliers exactly as for the
+//     other chunk kernels.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "fzb_kernels.cuh"
+
+namespace fzb {
+namespace {
+
+constexpr int kStageBytes = kChunkCodes * 4;  // one slab plane of f32
+constexpr int kOBytes = kChunkBytes + 128;    // level payload (+ slack for the second atomic word)
+constexpr int kSmemAlign = 1024;              // 128-byte swizzle atom
+constexpr size_t kSlabSmem = kSmemAlign + 2 * kStageBytes + kOBytes + 2048 + 256;
+constexpr uint32_t kWaitLimit = 1u << 26;     // mbarrier polls before giving up (with a 2 s clock bound)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// 2-D tiled TMA load (no multicast) of box {32 floats, 256 rows} at row `y`.
+__device__ __forceinline__ void tma_load_rows(void* dst, const CUtensorMap* map, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Orders this thread's earlier generic shared-memory accesses before later
+// async-proxy (TMA) writes to the same bytes.
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// max that returns NaN when either input is NaN (an outlier by the
+// reference's fabsf(delta) < radius test).
+__device__ __forceinline__ float max_nan(float a, float b) {
+    float d;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// a - b for both lanes, one rounding each (fma(b, -1, a) == a - b exactly).
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+
+// Round half away from zero of y: trunc(y + copysign(0.49999997, y)) with the
+// add rounded to nearest equals round(y) for every float (for |y| >= 2^23 y is
+// already integral and the add returns y).  `sv` supplies the sign (of v, the
+// same as y's since the scale is positive).
+__device__ __forceinline__ uint32_t half_bits(float sv) {
+    return (__float_as_uint(sv) & 0x80000000u) | 0x3effffffu;
+}
+
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: c + kMagic holds integer c in its low bits
+
+// Byte offset in a 128-byte-swizzled buffer of 16-byte granule g of row `row`
+// (the TMA SWIZZLE_128B layout: granule index XOR row % 8).
+__device__ __forceinline__ uint32_t swz_off(uint32_t row, uint32_t g) {
+    return row * 128u + 16u * (g ^ (row & 7u));
+}
+
+}  // namespace
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Codes of one thread's 32 elements from B (z- and x-differenced) and the
+// row above (read from the swizzled exchange buffer when ty != 0).
+// x[k] = code[k] | code[k + 16] << 16; om8 bit g = granule g (elements
+// 4g..4g+3) may hold an outlier.  Outlier codes are not zeroed here.
+// ---------------------------------------------------------------------------
+template <bool ZZ>
+__device__ __forceinline__ void make_codes(const float (&B)[32], const uint8_t* stg, uint32_t tu, bool ty,
+                                           float R, uint32_t (&x)[16], uint32_t& om8) {
+    om8 = 0;
+#pragma unroll
+    for (int g = 0; g < 4; g++) {
+        float c[8];  // elements 4g..4g+3 and 16+4g..16+4g+3
+        float4 u0 = make_float4(0.f, 0.f, 0.f, 0.f), u1 = u0;
+        if (ty) {
+            u0 = *reinterpret_cast<const float4*>(stg + swz_off(tu, g));
+            u1 = *reinterpret_cast<const float4*>(stg + swz_off(tu, g + 4));
+        }
+        float2 d;
+        if (ty) {
+            d = sub2(f2(B[4 * g], B[4 * g + 1]), f2(u0.x, u0.y));  c[0] = d.x; c[1] = d.y;
+            d = sub2(f2(B[4 * g + 2], B[4 * g + 3]), f2(u0.z, u0.w));  c[2] = d.x; c[3] = d.y;
+            d = sub2(f2(B[16 + 4 * g], B[17 + 4 * g]), f2(u1.x, u1.y));  c[4] = d.x; c[5] = d.y;
+            d = sub2(f2(B[18 + 4 * g], B[19 + 4 * g]), f2(u1.z, u1.w));  c[6] = d.x; c[7] = d.y;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                c[k] = B[4 * g + k];
+                c[4 + k] = B[16 + 4 * g + k];
+            }
+        }
+        const float m0 = max_nan(max_nan(fabsf(c[0]), fabsf(c[1])), max_nan(fabsf(c[2]), fabsf(c[3])));
+        const float m1 = max_nan(max_nan(fabsf(c[4]), fabsf(c[5])), max_nan(fabsf(c[6]), fabsf(c[7])));
+        if (!(m0 < R)) om8 |= 1u << g;
+        if (!(m1 < R)) om8 |= 1u << (g + 4);
+        const float2 M2 = make_float2(kMagic, kMagic);
+        float cm[8];
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+            d = __fadd2_rn(f2(c[k], c[k + 1]), M2);
+            cm[k] = d.x;
+            cm[k + 1] = d.y;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            uint32_t p = __byte_perm(__float_as_uint(cm[k]), __float_as_uint(cm[4 + k]), 0x5410);
+            if (ZZ) {
+                uint32_t s;
+                asm("prmt.b32 %0, %1, %1, 0xBB99;" : "=r"(s) : "r"(p));  // per-half sign mask
+                p = ((p << 1) & 0xfffefffeu) ^ s;
+            }
+            x[4 * g + k] = p;
+        }
+    }
+}
+
+// Exact outlier mask (bit e = element e) for the granules flagged in om8,
+// recomputed from the exchange buffer (the thread's own B and the row above).
+__device__ __forceinline__ uint32_t outlier_mask(const uint8_t* stg, uint32_t t, uint32_t tu, bool ty, float R,
+                                                 uint32_t om8) {
+    uint32_t om = 0;
+    while (om8) {
+        const uint32_t g = __ffs(om8) - 1;
+        om8 &= om8 - 1;
+        const float4 b = *reinterpret_cast<const float4*>(stg + swz_off(t, g));
+        float c[4] = {b.x, b.y, b.z, b.w};
+        if (ty) {
+            const float4 u = *reinterpret_cast<const float4*>(stg + swz_off(tu, g));
+            c[0] = __fsub_rn(c[0], u.x);
+            c[1] = __fsub_rn(c[1], u.y);
+            c[2] = __fsub_rn(c[2], u.z);
+            c[3] = __fsub_rn(c[3], u.w);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (!(fabsf(c[k]) < R)) om |= 1u << (4 * g + k);
+    }
+    return om;
+}
+
+// Delta of element e (the value an outlier record stores).
+__device__ __forceinline__ float delta_at(const uint8_t* stg, uint32_t t, uint32_t tu, bool ty, uint32_t e) {
+    const float* p = reinterpret_cast<const float*>(stg + swz_off(t, e >> 2)) + (e & 3);
+    float c = *p;
+    if (ty) c = __fsub_rn(c, *(reinterpret_cast<const float*>(stg + swz_off(tu, e >> 2)) + (e & 3)));
+    return c;
+}
+
+// Level-1 bitmap words of this lane's 8-lane group: lane j (= lane & 7) gets
+// the words of planes 2j (first) and 2j+1 (second); nibble i of each word is
+// the nonzero-byte nibble of lane i of the group.  nib64 byte u holds the
+// nibbles of planes 2u (low) and 2u+1 (high).  Three butterfly stages
+// transpose the 8x8 byte matrix across the group.
+__device__ __forceinline__ uint2 bm1_words(uint64_t nib64, uint32_t lane) {
+    uint32_t lo = (uint32_t)nib64, hi = (uint32_t)(nib64 >> 32);
+    const uint32_t full = 0xffffffffu;
+    // stage 1 (partner lane ^ 4): word s2 <- bytes of source lane with bit 2 = s2
+    uint32_t w0, w1;
+    {
+        const bool b2 = lane & 4;
+        const uint32_t r = __shfl_xor_sync(full, b2 ? lo : hi, 4);
+        w0 = b2 ? r : lo;
+        w1 = b2 ? hi : r;
+    }
+    // stage 2 (^ 2): half s1 of word s2 <- source lane (s2, s1)
+    {
+        const bool b1 = lane & 2;
+        const uint32_t send = b1 ? __byte_perm(w0, w1, 0x5410) : __byte_perm(w0, w1, 0x7632);
+        const uint32_t r = __shfl_xor_sync(full, send, 2);
+        const uint32_t n0 = b1 ? __byte_perm(r, w0, 0x7610) : __byte_perm(w0, r, 0x5410);
+        const uint32_t n1 = b1 ? __byte_perm(r, w1, 0x7632) : __byte_perm(w1, r, 0x7610);
+        w0 = n0;
+        w1 = n1;
+    }
+    // stage 3 (^ 1): lo <- source lanes 0,2,4,6, hi <- 1,3,5,7
+    {
+        const bool b0 = lane & 1;
+        const uint32_t even = __byte_perm(w0, w1, 0x6420), odd = __byte_perm(w0, w1, 0x7531);
+        const uint32_t r = __shfl_xor_sync(full, b0 ? even : odd, 1);
+        lo = b0 ? r : even;
+        hi = b0 ? odd : r;
+    }
+    // byte k of lo = source 2k, of hi = source 2k+1: nibble i of the word = source i
+    uint2 out;
+    out.x = (lo & 0x0f0f0f0fu) | ((hi << 4) & 0xf0f0f0f0u);
+    out.y = ((lo >> 4) & 0x0f0f0f0fu) | (hi & 0xf0f0f0f0u);
+    return out;
+}
+
+// Compaction selectors: __byte_perm(w, 0, kSel[m]) moves the bytes of w
+// flagged in the 4-bit mask m to the low end, in order, zero-filled.
+__constant__ uint32_t kSelInit[16] = {
+    0x4444, 0x4440, 0x4441, 0x4410, 0x4442, 0x4420, 0x4421, 0x4210,
+    0x4443, 0x4430, 0x4431, 0x4310, 0x4432, 0x4320, 0x4321, 0x3210};
+
+}  // namespace
+
+namespace {
+
+// Bounded mbarrier wait on the global timer (2 s): false when it ran out.
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t v;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+    return v;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 0; i < kWaitLimit; i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > 2000000000ull) break;
+    }
+    return false;
+}
+
+template <bool ZZ>
+__global__ void __launch_bounds__(kThreads, 2)
+    lq3d_tma_kernel(const FwdArgs a, const __grid_constant__ CUtensorMap map, uint32_t slabs, uint32_t units) {
+    extern __shared__ uint8_t dsm[];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_sel[16];
+    __shared__ uint32_t s_tot[8][4];     // per warp: inclusive plane counts, 8-bit fields
+    __shared__ uint32_t s_base[8][16];   // per warp, per plane: level-1 byte offset
+    __shared__ uint32_t s_wout[8];       // per warp: outlier count
+    __shared__ uint32_t s_l2[8];         // per warp: level-2 byte count
+    __shared__ uint32_t s_misc[4];       // 0 level-1 total, 1 outlier staging base, 2 size word
+
+    uint8_t* base = dsm + ((kSmemAlign - (smem_u32(dsm) & (kSmemAlign - 1))) & (kSmemAlign - 1));
+    uint8_t* O = base + 2 * kStageBytes;
+    uint32_t* Ow = reinterpret_cast<uint32_t*>(O);
+    uint32_t* bm1 = reinterpret_cast<uint32_t*>(O + kOBytes);
+    uint8_t* bm2 = O + kOBytes + 2048;
+
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t full = 0xffffffffu;
+    const uint32_t nx = a.nx, R = kChunkCodes / nx, S = nx / 32;
+    const bool ty = ((t / S) & 7u) != 0;   // slab origins have y % 8 == 0
+    const uint32_t tu = ty ? t - S : t;    // thread holding the row above
+    const float r = *a.ebx2_r;
+    const float rad = a.radius;
+    const uint32_t G = gridDim.x;
+
+    if (t < 16) s_sel[t] = kSelInit[t];
+    for (uint32_t i = t; i < (uint32_t)kOBytes / 16; i += kThreads)
+        reinterpret_cast<uint4*>(O)[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (t == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // plane sequence of this CTA: units blockIdx.x, +G, ... (last to first),
+    // each from its tile's first plane; thread 0 keeps the issue cursor
+    auto unit_z0 = [&](uint32_t uu) { return ((units - 1 - uu) / slabs) * 8u; };
+    uint32_t iu = blockIdx.x, iz = iu < units ? unit_z0(iu) : 0u;
+    auto issue_next = [&](uint32_t seq) {
+        if (iu >= units) return;
+        const uint32_t s = (units - 1 - iu) % slabs;
+        const int row = (int)((((size_t)iz * a.ny + (size_t)s * R) * nx) >> 5);
+        uint64_t* bar = &s_bar[seq & 1];
+        mbar_expect_tx(bar, kStageBytes);
+        tma_load_rows(base + (seq & 1) * kStageBytes, &map, row, bar);
+        if (++iz >= min(unit_z0(iu) + 8u, a.nz)) {
+            iu += G;
+            if (iu < units) iz = unit_z0(iu);
+        }
+    };
+    if (t == 0) {
+        issue_next(0);
+        issue_next(1);
+    }
+
+    uint32_t k = 0;  // plane sequence number
+    for (uint32_t uu = blockIdx.x; uu < units; uu += G) {
+        const uint32_t u = units - 1 - uu, s = u % slabs;
+        const uint32_t z0 = (u / slabs) * 8u, z1 = min(z0 + 8u, a.nz);
+        float qp[32];
+        for (uint32_t z = z0; z < z1; z++, k++) {
+            const uint32_t c = z * slabs + s;
+            const bool tz = z != z0;
+            uint8_t* stg = base + (k & 1) * kStageBytes;
+            const bool bad = !mbar_wait_bounded(&s_bar[k & 1], (k >> 1) & 1u);
+
+            // q, z difference, x difference; B over the thread's own bytes
+            float B[32];
+            float alast = 0.0f;
+#pragma unroll
+            for (int g = 0; g < 8; g++) {
+                const float4 v = *reinterpret_cast<const float4*>(stg + swz_off(t, g));
+                const float2 rr = f2(r, r);
+                const float2 y0 = __fmul2_rn(f2(v.x, v.y), rr), y1 = __fmul2_rn(f2(v.z, v.w), rr);
+                const float2 s0 = __fadd2_rn(y0, f2(__uint_as_float(half_bits(v.x)), __uint_as_float(half_bits(v.y))));
+                const float2 s1 = __fadd2_rn(y1, f2(__uint_as_float(half_bits(v.z)), __uint_as_float(half_bits(v.w))));
+                const float2 q0 = f2(truncf(s0.x), truncf(s0.y)), q1 = f2(truncf(s1.x), truncf(s1.y));
+                float2 A0 = q0, A1 = q1;
+                if (tz) {
+                    A0 = sub2(q0, f2(qp[4 * g], qp[4 * g + 1]));
+                    A1 = sub2(q1, f2(qp[4 * g + 2], qp[4 * g + 3]));
+                }
+                qp[4 * g] = q0.x;
+                qp[4 * g + 1] = q0.y;
+                qp[4 * g + 2] = q1.x;
+                qp[4 * g + 3] = q1.y;
+                const float b0 = (g & 1) ? __fsub_rn(A0.x, alast) : A0.x;  // x % 8 == 0 starts a tile
+                const float b1 = __fsub_rn(A0.y, A0.x);
+                const float b2 = __fsub_rn(A1.x, A0.y);
+                const float b3 = __fsub_rn(A1.y, A1.x);
+                alast = A1.y;
+                B[4 * g] = b0;
+                B[4 * g + 1] = b1;
+                B[4 * g + 2] = b2;
+                B[4 * g + 3] = b3;
+                *reinterpret_cast<float4*>(stg + swz_off(t, g)) = make_float4(b0, b1, b2, b3);
+            }
+            if (__syncthreads_or(bad)) {  // B1 (a copy did not arrive: give up)
+                if (t == 0) {
+                    atomicOr(a.err, kErrTmaTimeout);
+                    // bounded drain of the copies still in flight
+                    mbar_wait_bounded(&s_bar[k & 1], (k >> 1) & 1u);
+                    if (k == 0) mbar_wait_bounded(&s_bar[1], 0u);
+                }
+                __syncthreads();
+                return;
+            }
+            if (t == 0 && k >= 1) issue_next(k + 1);
+
+            // codes, outliers, bit transpose
+            uint32_t x[16], om8;
+            make_codes<ZZ>(B, stg, tu, ty, rad, x, om8);
+            const uint32_t om = om8 ? outlier_mask(stg, t, tu, ty, rad, om8) : 0u;
+            uint32_t pm;
+            {
+                uint32_t o = 0;
+#pragma unroll
+                for (int i = 0; i < 16; i++) o |= x[i];
+                pm = __reduce_or_sync(full, (o | (o >> 16)) & 0xffffu);  // planes nonzero in the warp
+            }
+            transpose16x2(x);
+            if (__any_sync(full, om != 0u)) {
+#pragma unroll
+                for (int b = 0; b < 16; b++) x[b] &= ~om;  // outlier codes are 0
+            }
+            const uint32_t nout = __popc(om);
+            uint32_t oex = 0;
+            if (__any_sync(full, nout != 0u)) {
+                const uint32_t inc = warp_incl_scan(nout);
+                oex = inc - nout;
+                if (lane == 31) s_wout[warp] = inc;
+            } else if (lane == 0) {
+                s_wout[warp] = 0;
+            }
+
+            // level 1: nonzero bytes per plane word, warp scans of the counts
+            uint32_t K[4] = {0u, 0u, 0u, 0u};
+            uint64_t nib64 = 0;
+#pragma unroll
+            for (int b = 0; b < 16; b++) {
+                if ((pm >> b) & 1u) {
+                    const uint32_t w = x[b];
+                    const uint32_t hb = (((w & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w) & 0x80808080u;
+                    K[b >> 2] += (uint32_t)__popc(hb) << (8 * (b & 3));
+                    nib64 |= (uint64_t)((hb * 0x00204081u) >> 28) << (4 * b);
+                }
+            }
+            uint32_t KX[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                KX[j] = 0;
+                if ((pm >> (4 * j)) & 15u) {
+                    const uint32_t inc = warp_incl_scan(K[j]);
+                    KX[j] = inc - K[j];
+                    if (lane == 31) s_tot[warp][j] = inc;
+                } else if (lane == 31) {
+                    s_tot[warp][j] = 0;
+                }
+            }
+            __syncthreads();  // B2
+
+            // staging for this chunk's outliers; level-1 byte offsets per (warp, plane)
+            if (t == 0) {
+                uint32_t tot = 0;
+#pragma unroll
+                for (int w = 0; w < 8; w++) tot += s_wout[w];
+                const uint32_t ob = tot ? atomicAdd(a.ostage_ctr, tot) : 0u;
+                a.obase[c] = ob;
+                a.ocnt[c] = tot;
+                s_misc[1] = ob;
+            }
+            if (warp == 0) {
+                const uint32_t b = lane & 15u, h = lane >> 4;
+                uint32_t cnt[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) cnt[i] = (s_tot[4 * h + i][b >> 2] >> (8 * (b & 3u))) & 0xffu;
+                const uint32_t gs = cnt[0] + cnt[1] + cnt[2] + cnt[3];
+                const uint32_t other = __shfl_xor_sync(full, gs, 16);
+                const uint32_t T = gs + other;  // plane b, all warps
+                uint32_t suf = T;               // planes >= b come first (plane 15 leads)
+#pragma unroll
+                for (uint32_t d = 1; d < 16; d <<= 1) {
+                    const uint32_t n = __shfl_down_sync(full, suf, d, 16);
+                    if (b + d < 16) suf += n;
+                }
+                uint32_t off = suf - T + (h ? other : 0u);
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    s_base[4 * h + i][b] = off;
+                    off += cnt[i];
+                }
+                if (lane == 0) s_misc[0] = suf;
+            }
+            __syncthreads();  // B3
+            const uint32_t nzT = s_misc[0];
+
+            if (om) {  // outlier records, ascending index within the chunk
+                uint32_t pos = s_misc[1] + oex;
+                for (uint32_t w = 0; w < warp; w++) pos += s_wout[w];
+                const uint32_t kb = c * (uint32_t)kChunkCodes + 32u * t;
+                uint32_t m = om;
+                while (m) {
+                    const uint32_t e = __ffs(m) - 1;
+                    m &= m - 1;
+                    if (pos < a.ostage_cap) {
+                        a.ostage_err[pos] = delta_at(stg, t, tu, ty, e);
+                        a.ostage_idx[pos] = kb + e;
+                    }
+                    pos++;
+                }
+            }
+
+            // 0: encode, 1: all-zero chunk, 2: stored raw (rze_stage.cu:365-372)
+            int mode = nzT == 0 ? 1 : ((nzT >= (uint32_t)kRzeAvail || nzT > (uint32_t)(kRzeAvail - 2048)) ? 2 : 0);
+            if (mode == 0) {
+#pragma unroll
+                for (int b = 0; b < 16; b++) {
+                    if ((pm >> b) & 1u) {
+                        const uint32_t nib = (uint32_t)(nib64 >> (4 * b)) & 15u;
+                        if (nib) {
+                            const uint32_t pos = s_base[warp][b] + ((KX[b >> 2] >> (8 * (b & 3))) & 0xffu);
+                            const uint32_t packed = __byte_perm(x[b], 0u, s_sel[nib]);
+                            const uint32_t sh = (pos & 3u) * 8u;
+                            atomicOr(&Ow[pos >> 2], packed << sh);
+                            atomicOr(&Ow[(pos >> 2) + 1], __funnelshift_l(packed, 0u, sh));
+                        }
+                    }
+                }
+                const uint2 bw = bm1_words(nib64, lane);
+                const uint32_t j = lane & 7u;
+                bm1[(15 - 2 * j) * 32 + (t >> 3)] = bw.x;
+                bm1[(14 - 2 * j) * 32 + (t >> 3)] = bw.y;
+            }
+            __syncthreads();  // B4
+
+            // level 2: the bm1 bytes that differ from their predecessor
+            uint64_t M = 0;
+            uint32_t m2 = 0, ex2 = 0;
+            if (mode == 0) {
+                const uint2 mw = reinterpret_cast<const uint2*>(bm1)[t];
+                M = ((uint64_t)mw.y << 32) | mw.x;
+                uint32_t prev = __shfl_up_sync(full, mw.y, 1) >> 24;
+                if (lane == 0) prev = t ? (uint32_t)reinterpret_cast<const uint8_t*>(bm1)[8 * t - 1] : 0u;
+                m2 = nz_byte_mask64(M ^ ((M << 8) | prev));
+                const uint32_t n2 = __popc(m2);
+                const uint32_t inc = warp_incl_scan(n2);
+                ex2 = inc - n2;
+                if (lane == 31) s_l2[warp] = inc;
+                bm2[t] = (uint8_t)m2;
+            }
+            __syncthreads();  // B5
+            uint32_t wpos = 0;
+            if (mode == 0) {
+                uint32_t n2T = 0;
+#pragma unroll
+                for (int w = 0; w < 8; w++) {
+                    const uint32_t v = s_l2[w];
+                    if ((uint32_t)w < warp) ex2 += v;
+                    n2T += v;
+                }
+                wpos = nzT + n2T;
+                if (wpos >= (uint32_t)kRzeAvail || wpos > (uint32_t)(kRzeAvail - 256)) {
+                    mode = 2;
+                } else {
+                    uint32_t p = nzT + ex2, m = m2;
+                    while (m) {
+                        const uint32_t b = __ffs(m) - 1;
+                        m &= m - 1;
+                        O[p++] = (uint8_t)(M >> (8 * b));
+                    }
+                }
+            }
+            __syncthreads();  // B6
+
+            // levels 3 and 4 (warp 0), header
+            if (mode == 0 && warp == 0) {
+                const uint2 mw = reinterpret_cast<const uint2*>(bm2)[lane];
+                const uint64_t M3 = ((uint64_t)mw.y << 32) | mw.x;
+                uint32_t prev = __shfl_up_sync(full, mw.y, 1) >> 24;
+                if (lane == 0) prev = 0;
+                const uint32_t m3 = nz_byte_mask64(M3 ^ ((M3 << 8) | prev));  // bm3 byte `lane`
+                const uint32_t n3 = __popc(m3), inc = warp_incl_scan(n3);
+                const uint32_t n3T = __shfl_sync(full, inc, 31);
+                {
+                    uint32_t p = wpos + inc - n3, m = m3;
+                    while (m) {
+                        const uint32_t b = __ffs(m) - 1;
+                        m &= m - 1;
+                        O[p++] = (uint8_t)(M3 >> (8 * b));
+                    }
+                }
+                uint32_t pb = __shfl_up_sync(full, m3, 1);
+                if (lane == 0) pb = 0;
+                const bool nr4 = m3 != pb;
+                const uint32_t bm4 = __ballot_sync(full, nr4);
+                uint32_t wp = wpos + n3T;
+                uint32_t sw = 0x80000000u | (uint32_t)kChunkBytes;
+                if (!(wp >= (uint32_t)kRzeAvail || wp >= (uint32_t)(kRzeAvail - 4) ||
+                      wp > (uint32_t)(kRzeAvail - 4 - 32))) {
+                    if (nr4) O[wp + __popc(bm4 & ((1u << lane) - 1u))] = (uint8_t)m3;
+                    wp += __popc(bm4);
+                    if (wp < (uint32_t)(kRzeAvail - 4)) {
+                        if (lane == 0) {
+                            O[wp + 0] = (uint8_t)bm4;
+                            O[wp + 1] = (uint8_t)(bm4 >> 8);
+                            O[wp + 2] = (uint8_t)(bm4 >> 16);
+                            O[wp + 3] = (uint8_t)(bm4 >> 24);
+                            O[wp + 4] = (uint8_t)(kChunkBytes & 0xff);
+                            O[wp + 5] = (uint8_t)(kChunkBytes >> 8);
+                        }
+                        sw = wp + 6;
+                    }
+                }
+                if (lane == 0) s_misc[2] = sw;
+            }
+            if (t == 0) {
+                if (mode == 1) {
+                    O[0] = (uint8_t)(kChunkBytes & 0xff);
+                    O[1] = (uint8_t)(kChunkBytes >> 8);
+                    s_misc[2] = 2u;
+                } else if (mode == 2) {
+                    s_misc[2] = 0x80000000u | (uint32_t)kChunkBytes;
+                }
+            }
+            __syncthreads();  // B7
+
+            const uint32_t sw = s_misc[2];
+            uint8_t* slot = a.slots + (size_t)c * kChunkBytes;
+            if (sw >> 31) {
+                // stored raw: the shuffled chunk, recomputed from the exchange buffer
+                float Bs[32];
+#pragma unroll
+                for (int g = 0; g < 8; g++) {
+                    const float4 v = *reinterpret_cast<const float4*>(stg + swz_off(t, g));
+                    Bs[4 * g] = v.x;
+                    Bs[4 * g + 1] = v.y;
+                    Bs[4 * g + 2] = v.z;
+                    Bs[4 * g + 3] = v.w;
+                }
+                uint32_t xr[16], o8;
+                make_codes<ZZ>(Bs, stg, tu, ty, rad, xr, o8);
+                transpose16x2(xr);
+                uint32_t* sl = reinterpret_cast<uint32_t*>(slot);
+#pragma unroll
+                for (int b = 0; b < 16; b++) sl[(15 - b) * 256 + t] = xr[b] & ~om;
+                for (uint32_t i = t; i < (uint32_t)kOBytes / 16; i += kThreads)
+                    reinterpret_cast<uint4*>(O)[i] = make_uint4(0u, 0u, 0u, 0u);
+            } else {
+                uint4* d4 = reinterpret_cast<uint4*>(slot);
+                uint4* o4 = reinterpret_cast<uint4*>(O);
+                for (uint32_t i = t; i < (sw + 15) / 16; i += kThreads) {
+                    d4[i] = o4[i];
+                    o4[i] = make_uint4(0u, 0u, 0u, 0u);
+                }
+            }
+            if (t == 0) a.sizes[c] = sw;
+            fence_proxy_async();  // this plane's generic accesses before the buffer's next TMA fill
+        }
+    }
+}
+
+}  // namespace
+
+// Host: a 2-D view of the field as rows of 32 floats, box = one slab plane.
+namespace {
+using EncodeTiled = PFN_cuTensorMapEncodeTiled_v12000;
+
+EncodeTiled encode_tiled() {
+    static EncodeTiled fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiled) nullptr;
+        return reinterpret_cast<EncodeTiled>(p);
+    }();
+    return fn;
+}
+}  // namespace
+
+bool lq3d_tma_supported(const FwdArgs& a) {
+    return encode_tiled() != nullptr && (reinterpret_cast<uintptr_t>(a.in) & 15u) == 0 &&
+           a.radius <= 2097152.0f && a.nfield % 8192u == 0;
+}
+
+int launch_lq3d_tma(const FwdArgs& a, unsigned grid, cudaStream_t s) {
+    EncodeTiled enc = encode_tiled();
+    if (!enc) return (int)cudaErrorNotSupported;
+    CUtensorMap map;
+    const cuuint64_t gdim[2] = {32, (cuuint64_t)(a.nfield / 32)};
+    const cuuint64_t gstride[1] = {128};
+    const cuuint32_t box[2] = {32, 256};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(a.in), gdim, gstride, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return (int)cudaErrorInvalidValue;
+    const uint32_t slabs = a.ny / (kChunkCodes / a.nx), units = slabs * ((a.nz + 7) / 8);
+    grid = grid < units ? grid : units;
+    cudaError_t e;
+    if (a.zigzag) {
+        e = cudaFuncSetAttribute(lq3d_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem);
+        if (e != cudaSuccess) return (int)e;
+        lq3d_tma_kernel<true><<<grid, kThreads, kSlabSmem, s>>>(a, map, slabs, units);
+    } else {
+        e = cudaFuncSetAttribute(lq3d_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem);
+        if (e != cudaSuccess) return (int)e;
+        lq3d_tma_kernel<false><<<grid, kThreads, kSlabSmem, s>>>(a, map, slabs, units);
+    }
+    return (int)cudaGetLastError();
+}
+
+}  // namespace fzb

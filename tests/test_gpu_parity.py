@@ -36,6 +36,15 @@ def _field(n, seed, kind="smooth"):
         pos = rng.choice(n, max(1, n // 500), replace=False)
         x[pos] = rng.choice([-1e3, 1e3], pos.size)
         return x.astype(np.float32)
+    if kind == "blocks":  # zero stretches (all-zero chunks) and constant runs
+        x = np.repeat(rng.normal(size=n // 4096 + 1), 4096)[:n].astype(np.float32)
+        x[(np.arange(n) // 8192) % 3 == 0] = 0.0
+        return x
+    if kind == "special":  # NaN / +-inf / huge values among a smooth field
+        x = np.cumsum(rng.normal(size=n) * 0.01).astype(np.float32)
+        pos = rng.choice(n, max(4, n // 300), replace=False)
+        x[pos] = rng.choice(np.array([np.nan, np.inf, -np.inf, 3e30, -2e25, 1e9], np.float32), pos.size)
+        return x
     raise ValueError(kind)
 
 
@@ -177,20 +186,29 @@ def test_fused_compress_matches_oracle_chain(cuda, dims, mode, zz, radius, kind)
         assert np.array_equal(_h(dec).view(np.uint32), y.view(np.uint32)), f"flags={flags}"
 
 
-@pytest.mark.parametrize("dims", [(512, 32, 16), (64, 256, 10)])
-def test_fused_compress_slab_and_chunk_kernels_agree(cuda, dims, monkeypatch):
-    # the slab-column kernel and the per-chunk kernel must emit identical bytes
+@pytest.mark.parametrize("dims", [(512, 32, 16), (64, 256, 10), (32, 256, 9), (1024, 16, 17), (128, 64, 3)])
+@pytest.mark.parametrize("kind,eb,radius,zz", [("spiky", 1e-3, 512, True), ("noise", 1e-3, 32768, False),
+                                               ("blocks", 1e-3, 32768, True), ("special", 1e-3, 64, True)])
+def test_fused_compress_slab_and_chunk_kernels_agree(cuda, dims, kind, eb, radius, zz, monkeypatch):
+    # the TMA slab kernel, the cp.async slab kernel and the per-chunk kernel
+    # must emit identical bytes (raw, all-zero and outlier-heavy chunks included)
     n = int(np.prod(dims))
-    x = _g(_field(n, 18, "spiky"), cuda)
-    a = kern().lq_bs_rze_compress(x, dims, 1e-3, O.ABS, 512, True, 0.2)
-    monkeypatch.setenv("FZB_DISABLE_SLAB", "1")
-    b = kern().lq_bs_rze_compress(x, dims, 1e-3, O.ABS, 512, True, 0.2)
-    sa, sb = int(_h(a["rze_size"])[0]), int(_h(b["rze_size"])[0])
-    assert sa == sb and np.array_equal(_h(a["rze"])[:sa], _h(b["rze"])[:sb])
+    x = _g(_field(n, 18, kind), cuda)
+    outs = []
+    for flag in ("0", "2", "1"):
+        monkeypatch.setenv("FZB_DISABLE_SLAB", flag)
+        outs.append(kern().lq_bs_rze_compress(x, dims, eb, O.ABS, radius, zz, 1.0))
+    a = outs[0]
+    sa = int(_h(a["rze_size"])[0])
     k = int(_h(a["count"])[0])
-    assert k == int(_h(b["count"])[0]) and k > 0
-    assert np.array_equal(_h(a["idx"])[:k], _h(b["idx"])[:k])
-    assert np.array_equal(_h(a["err"])[:k].view(np.uint32), _h(b["err"])[:k].view(np.uint32))
+    if kind in ("spiky", "special"):
+        assert k > 0
+    for b in outs[1:]:
+        sb = int(_h(b["rze_size"])[0])
+        assert sa == sb and np.array_equal(_h(a["rze"])[:sa], _h(b["rze"])[:sb])
+        assert k == int(_h(b["count"])[0])
+        assert np.array_equal(_h(a["idx"])[:k], _h(b["idx"])[:k])
+        assert np.array_equal(_h(a["err"])[:k].view(np.uint32), _h(b["err"])[:k].view(np.uint32))
 
 
 def test_fused_decompress_exactness_fallback(cuda):
