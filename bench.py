@@ -261,7 +261,7 @@ def run_ours(args, world, rank, local):
         return launches, max_over_ranks(ms / launches / 1e3 if launches else 0.0, world)
 
     slab_name = next((k for k in ("lq3d_tma_bs_rze", "lq3d_slab_bs_rze") if k in per_kernel), "lq_chunk_bs_rze")
-    inv_name = "fused_inverse_3d" if "fused_inverse_3d" in per_kernel else "lq_inverse"
+    inv_name = next((k for k in ("lq3d_inv_slab", "fused_inverse_3d") if k in per_kernel), "lq_inverse")
     n_slab, t_slab = kern(slab_name)
     n_inv, t_inv = kern(inv_name)
     launches = sum(v[0] for v in per_kernel.values())

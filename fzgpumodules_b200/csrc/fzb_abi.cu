@@ -82,13 +82,14 @@ Work carve(void* base, uint64_t n_total, uint64_t cap) {
 
 inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 
-// FZB_DISABLE_SLAB=1 routes 3-D fused compression through the per-chunk
-// kernel, FZB_DISABLE_SLAB=2 through the cp.async slab kernel instead of the
-// TMA one (all produce identical bytes; tests exercise each).
+// FZB_DISABLE_SLAB is a bit mask selecting the alternative kernels (all
+// produce identical results; tests exercise each): 1 = 3-D fused compression
+// through the per-chunk kernel, 2 = the cp.async slab kernel instead of the
+// TMA one, 4 = the per-(slab, tile) fused inverse instead of the persistent
+// slab inverse.
 inline unsigned flags_env() {
     const char* v = getenv("FZB_DISABLE_SLAB");
-    if (!v) return 0u;
-    return v[0] == '1' ? 1u : (v[0] == '2' ? 2u : 0u);
+    return v ? (unsigned)strtoul(v, nullptr, 10) & 7u : 0u;
 }
 
 #define CK(call)                                          \
@@ -529,8 +530,14 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
         const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32 + 4 * kChunkCodes;
         CK(cudaFuncSetAttribute(fused_inverse_3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem));
-        dim3 grid(g.ny / R, (g.nz + 7) / 8, 1);
-        {
+        if (nx >= 32 && !(flags_env() & 4)) {
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            TraceScope ts(s, "lq3d_inv_slab");
+            if (launch_lq3d_inv_slab(a, (unsigned)(2 * sms), s) != 0) return FZB_E_CUDA;
+        } else {
+            dim3 grid(g.ny / R, (g.nz + 7) / 8, 1);
             TraceScope ts(s, "fused_inverse_3d");
             fused_inverse_3d_kernel<<<grid, kThreads, smem, s>>>(a);
         }

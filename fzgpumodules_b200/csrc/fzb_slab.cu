@@ -31,74 +31,13 @@
 //   * the encoded chunk goes to its 16 KiB slot; assemble_scan/assemble_copy
 //     (fzb_forward.cu) place slots and staged outliers exactly as for the
 //     other chunk kernels.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
-#include "fzb_kernels.cuh"
+#include "fzb_slab.cuh"
 
 namespace fzb {
 namespace {
 
-constexpr int kStageBytes = kChunkCodes * 4;  // one slab plane of f32
 constexpr int kOBytes = kChunkBytes + 128;    // level payload (+ slack for the second atomic word)
-constexpr int kSmemAlign = 1024;              // 128-byte swizzle atom
 constexpr size_t kSlabSmem = kSmemAlign + 2 * kStageBytes + kOBytes + 2048 + 256;
-constexpr uint32_t kWaitLimit = 1u << 26;     // mbarrier polls before giving up (with a 2 s clock bound)
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// 2-D tiled TMA load (no multicast) of box {32 floats, 256 rows} at row `y`.
-__device__ __forceinline__ void tma_load_rows(void* dst, const CUtensorMap* map, int y, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// Orders this thread's earlier generic shared-memory accesses before later
-// async-proxy (TMA) writes to the same bytes.
-__device__ __forceinline__ void fence_proxy_async() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// max that returns NaN when either input is NaN (an outlier by the
-// reference's fabsf(delta) < radius test).
-__device__ __forceinline__ float max_nan(float a, float b) {
-    float d;
-    asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
-    return d;
-}
-
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-
-// a - b for both lanes, one rounding each (fma(b, -1, a) == a - b exactly).
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
-    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
-}
 
 // Round half away from zero of y: trunc(y + copysign(0.49999997, y)) with the
 // add rounded to nearest equals round(y) for every float (for |y| >= 2^23 y is
@@ -106,14 +45,6 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) {
 // same as y's since the scale is positive).
 __device__ __forceinline__ uint32_t half_bits(float sv) {
     return (__float_as_uint(sv) & 0x80000000u) | 0x3effffffu;
-}
-
-constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: c + kMagic holds integer c in its low bits
-
-// Byte offset in a 128-byte-swizzled buffer of 16-byte granule g of row `row`
-// (the TMA SWIZZLE_128B layout: granule index XOR row % 8).
-__device__ __forceinline__ uint32_t swz_off(uint32_t row, uint32_t g) {
-    return row * 128u + 16u * (g ^ (row & 7u));
 }
 
 }  // namespace
@@ -208,47 +139,6 @@ __device__ __forceinline__ float delta_at(const uint8_t* stg, uint32_t t, uint32
     return c;
 }
 
-// Level-1 bitmap words of this lane's 8-lane group: lane j (= lane & 7) gets
-// the words of planes 2j (first) and 2j+1 (second); nibble i of each word is
-// the nonzero-byte nibble of lane i of the group.  nib64 byte u holds the
-// nibbles of planes 2u (low) and 2u+1 (high).  Three butterfly stages
-// transpose the 8x8 byte matrix across the group.
-__device__ __forceinline__ uint2 bm1_words(uint64_t nib64, uint32_t lane) {
-    uint32_t lo = (uint32_t)nib64, hi = (uint32_t)(nib64 >> 32);
-    const uint32_t full = 0xffffffffu;
-    // stage 1 (partner lane ^ 4): word s2 <- bytes of source lane with bit 2 = s2
-    uint32_t w0, w1;
-    {
-        const bool b2 = lane & 4;
-        const uint32_t r = __shfl_xor_sync(full, b2 ? lo : hi, 4);
-        w0 = b2 ? r : lo;
-        w1 = b2 ? hi : r;
-    }
-    // stage 2 (^ 2): half s1 of word s2 <- source lane (s2, s1)
-    {
-        const bool b1 = lane & 2;
-        const uint32_t send = b1 ? __byte_perm(w0, w1, 0x5410) : __byte_perm(w0, w1, 0x7632);
-        const uint32_t r = __shfl_xor_sync(full, send, 2);
-        const uint32_t n0 = b1 ? __byte_perm(r, w0, 0x7610) : __byte_perm(w0, r, 0x5410);
-        const uint32_t n1 = b1 ? __byte_perm(r, w1, 0x7632) : __byte_perm(w1, r, 0x7610);
-        w0 = n0;
-        w1 = n1;
-    }
-    // stage 3 (^ 1): lo <- source lanes 0,2,4,6, hi <- 1,3,5,7
-    {
-        const bool b0 = lane & 1;
-        const uint32_t even = __byte_perm(w0, w1, 0x6420), odd = __byte_perm(w0, w1, 0x7531);
-        const uint32_t r = __shfl_xor_sync(full, b0 ? even : odd, 1);
-        lo = b0 ? r : even;
-        hi = b0 ? odd : r;
-    }
-    // byte k of lo = source 2k, of hi = source 2k+1: nibble i of the word = source i
-    uint2 out;
-    out.x = (lo & 0x0f0f0f0fu) | ((hi << 4) & 0xf0f0f0f0u);
-    out.y = ((lo >> 4) & 0x0f0f0f0fu) | (hi & 0xf0f0f0f0u);
-    return out;
-}
-
 // Compaction selectors: __byte_perm(w, 0, kSel[m]) moves the bytes of w
 // flagged in the 4-bit mask m to the low end, in order, zero-filled.
 __constant__ uint32_t kSelInit[16] = {
@@ -258,23 +148,6 @@ __constant__ uint32_t kSelInit[16] = {
 }  // namespace
 
 namespace {
-
-// Bounded mbarrier wait on the global timer (2 s): false when it ran out.
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t v;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
-    return v;
-}
-
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    for (uint32_t i = 0; i < kWaitLimit; i++) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > 2000000000ull) break;
-    }
-    return false;
-}
 
 template <bool ZZ>
 __global__ void __launch_bounds__(kThreads, 2)
@@ -416,28 +289,29 @@ __global__ void __launch_bounds__(kThreads, 2)
 
             // level 1: nonzero bytes per plane word, warp scans of the counts
             uint32_t K[4] = {0u, 0u, 0u, 0u};
-            uint64_t nib64 = 0;
+            uint32_t nlo = 0, nhi = 0;  // plane nibbles (planes 0-7, 8-15)
 #pragma unroll
             for (int b = 0; b < 16; b++) {
                 if ((pm >> b) & 1u) {
                     const uint32_t w = x[b];
                     const uint32_t hb = (((w & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w) & 0x80808080u;
                     K[b >> 2] += (uint32_t)__popc(hb) << (8 * (b & 3));
-                    nib64 |= (uint64_t)((hb * 0x00204081u) >> 28) << (4 * b);
+                    const uint32_t nb = ((hb * 0x00204081u) >> (28 - 4 * (b & 7))) & (15u << (4 * (b & 7)));
+                    if (b < 8) nlo |= nb;
+                    else nhi |= nb;
                 }
             }
-            uint32_t KX[4];
+            const uint64_t nib64 = ((uint64_t)nhi << 32) | nlo;
+            uint32_t KX[4], act = 0;
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                KX[j] = 0;
-                if ((pm >> (4 * j)) & 15u) {
-                    const uint32_t inc = warp_incl_scan(K[j]);
-                    KX[j] = inc - K[j];
-                    if (lane == 31) s_tot[warp][j] = inc;
-                } else if (lane == 31) {
-                    s_tot[warp][j] = 0;
-                }
+            for (int j = 0; j < 4; j++) act |= (((pm >> (4 * j)) & 15u) ? 1u : 0u) << j;
+            warp_scan4(K, act, KX);
+            if (lane == 31) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) s_tot[warp][j] = ((act >> j) & 1u) ? KX[j] : 0u;
             }
+#pragma unroll
+            for (int j = 0; j < 4; j++) KX[j] = ((act >> j) & 1u) ? KX[j] - K[j] : 0u;
             __syncthreads();  // B2
 
             // staging for this chunk's outliers; level-1 byte offsets per (warp, plane)

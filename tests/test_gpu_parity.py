@@ -209,6 +209,14 @@ def test_fused_compress_slab_and_chunk_kernels_agree(cuda, dims, kind, eb, radiu
         assert k == int(_h(b["count"])[0])
         assert np.array_equal(_h(a["idx"])[:k], _h(b["idx"])[:k])
         assert np.array_equal(_h(a["err"])[:k].view(np.uint32), _h(b["err"])[:k].view(np.uint32))
+    # inverse: persistent slab kernel, per-tile fused kernel and the exact path agree bit for bit
+    abs_eb = float(_h(a["eb_state"])[1])
+    decs = []
+    for flag, flags in (("0", 0), ("4", 0), ("0", kern().FORCE_EXACT)):
+        monkeypatch.setenv("FZB_DISABLE_SLAB", flag)
+        decs.append(_h(kern().lq_bs_rze_decompress(a["rze"], sa, a["err"], a["idx"], a["count"], a["cap"], n,
+                                                   dims, abs_eb, zz, flags=flags)).view(np.uint32))
+    assert np.array_equal(decs[0], decs[2]) and np.array_equal(decs[1], decs[2])
 
 
 def test_fused_decompress_exactness_fallback(cuda):
