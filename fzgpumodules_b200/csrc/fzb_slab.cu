@@ -37,7 +37,7 @@ namespace fzb {
 namespace {
 
 constexpr int kOBytes = kChunkBytes + 128;    // level payload (+ slack for the second atomic word)
-constexpr size_t kSlabSmem = kSmemAlign + 2 * kStageBytes + kOBytes + 2048 + 256;
+constexpr size_t kSlabSmem = kSmemAlign + 2 * kStageBytes + kOBytes + kChunkBytes + 256;
 
 // Round half away from zero of y: trunc(y + copysign(0.49999997, y)) with the
 // add rounded to nearest equals round(y) for every float (for |y| >= 2^23 y is
@@ -155,17 +155,15 @@ __global__ void __launch_bounds__(kThreads, 2)
     extern __shared__ uint8_t dsm[];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ uint32_t s_sel[16];
-    __shared__ uint32_t s_tot[8][4];     // per warp: inclusive plane counts, 8-bit fields
-    __shared__ uint32_t s_base[8][16];   // per warp, per plane: level-1 byte offset
     __shared__ uint32_t s_wout[8];       // per warp: outlier count
-    __shared__ uint32_t s_l2[8];         // per warp: level-2 byte count
-    __shared__ uint32_t s_misc[4];       // 0 level-1 total, 1 outlier staging base, 2 size word
+    __shared__ uint32_t s_l1[8];         // per warp: level-1 | level-2 << 16 byte counts
+    __shared__ uint32_t s_misc[4];       // 1 outlier staging base, 2 size word
 
     uint8_t* base = dsm + ((kSmemAlign - (smem_u32(dsm) & (kSmemAlign - 1))) & (kSmemAlign - 1));
     uint8_t* O = base + 2 * kStageBytes;
     uint32_t* Ow = reinterpret_cast<uint32_t*>(O);
-    uint32_t* bm1 = reinterpret_cast<uint32_t*>(O + kOBytes);
-    uint8_t* bm2 = O + kOBytes + 2048;
+    uint8_t* Sbuf = O + kOBytes;            // the shuffled chunk (16 KiB)
+    uint8_t* bm2 = Sbuf + kChunkBytes;
 
     const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t full = 0xffffffffu;
@@ -265,13 +263,6 @@ __global__ void __launch_bounds__(kThreads, 2)
             uint32_t x[16], om8;
             make_codes<ZZ>(B, stg, tu, ty, rad, x, om8);
             const uint32_t om = om8 ? outlier_mask(stg, t, tu, ty, rad, om8) : 0u;
-            uint32_t pm;
-            {
-                uint32_t o = 0;
-#pragma unroll
-                for (int i = 0; i < 16; i++) o |= x[i];
-                pm = __reduce_or_sync(full, (o | (o >> 16)) & 0xffffu);  // planes nonzero in the warp
-            }
             transpose16x2(x);
             if (__any_sync(full, om != 0u)) {
 #pragma unroll
@@ -287,35 +278,15 @@ __global__ void __launch_bounds__(kThreads, 2)
                 s_wout[warp] = 0;
             }
 
-            // level 1: nonzero bytes per plane word, warp scans of the counts
-            uint32_t K[4] = {0u, 0u, 0u, 0u};
-            uint32_t nlo = 0, nhi = 0;  // plane nibbles (planes 0-7, 8-15)
+            // RZE levels 1 and 2 from the shuffled chunk S (plane word b of
+            // segment t at word (15-b)*256 + t): thread t then takes S words
+            // 16t..16t+15 (bytes 64t..64t+63, one plane region), whose
+            // nonzero-byte nibbles are bm1 bytes 8t..8t+7
+            uint32_t* Sw = reinterpret_cast<uint32_t*>(Sbuf);
 #pragma unroll
-            for (int b = 0; b < 16; b++) {
-                if ((pm >> b) & 1u) {
-                    const uint32_t w = x[b];
-                    const uint32_t hb = (((w & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w) & 0x80808080u;
-                    K[b >> 2] += (uint32_t)__popc(hb) << (8 * (b & 3));
-                    const uint32_t nb = ((hb * 0x00204081u) >> (28 - 4 * (b & 7))) & (15u << (4 * (b & 7)));
-                    if (b < 8) nlo |= nb;
-                    else nhi |= nb;
-                }
-            }
-            const uint64_t nib64 = ((uint64_t)nhi << 32) | nlo;
-            uint32_t KX[4], act = 0;
-#pragma unroll
-            for (int j = 0; j < 4; j++) act |= (((pm >> (4 * j)) & 15u) ? 1u : 0u) << j;
-            warp_scan4(K, act, KX);
-            if (lane == 31) {
-#pragma unroll
-                for (int j = 0; j < 4; j++) s_tot[warp][j] = ((act >> j) & 1u) ? KX[j] : 0u;
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) KX[j] = ((act >> j) & 1u) ? KX[j] - K[j] : 0u;
+            for (int b = 0; b < 16; b++) Sw[(15 - b) * 256 + t] = x[b];
             __syncthreads();  // B2
-
-            // staging for this chunk's outliers; level-1 byte offsets per (warp, plane)
-            if (t == 0) {
+            if (t == 0) {  // staging for this chunk's outliers
                 uint32_t tot = 0;
 #pragma unroll
                 for (int w = 0; w < 8; w++) tot += s_wout[w];
@@ -324,34 +295,52 @@ __global__ void __launch_bounds__(kThreads, 2)
                 a.ocnt[c] = tot;
                 s_misc[1] = ob;
             }
-            if (warp == 0) {
-                const uint32_t b = lane & 15u, h = lane >> 4;
-                uint32_t cnt[4];
+            uint32_t w[16];
 #pragma unroll
-                for (int i = 0; i < 4; i++) cnt[i] = (s_tot[4 * h + i][b >> 2] >> (8 * (b & 3u))) & 0xffu;
-                const uint32_t gs = cnt[0] + cnt[1] + cnt[2] + cnt[3];
-                const uint32_t other = __shfl_xor_sync(full, gs, 16);
-                const uint32_t T = gs + other;  // plane b, all warps
-                uint32_t suf = T;               // planes >= b come first (plane 15 leads)
-#pragma unroll
-                for (uint32_t d = 1; d < 16; d <<= 1) {
-                    const uint32_t n = __shfl_down_sync(full, suf, d, 16);
-                    if (b + d < 16) suf += n;
-                }
-                uint32_t off = suf - T + (h ? other : 0u);
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    s_base[4 * h + i][b] = off;
-                    off += cnt[i];
-                }
-                if (lane == 0) s_misc[0] = suf;
+            for (int i = 0; i < 4; i++) {
+                const uint4 q = reinterpret_cast<const uint4*>(Sw)[4 * t + i];
+                w[4 * i] = q.x;
+                w[4 * i + 1] = q.y;
+                w[4 * i + 2] = q.z;
+                w[4 * i + 3] = q.w;
             }
+            uint32_t nlo = 0, nhi = 0;
+            {
+                uint32_t o = 0;
+#pragma unroll
+                for (int i = 0; i < 16; i++) o |= w[i];
+                if (__any_sync(full, o != 0u)) {  // warps over empty plane regions skip
+#pragma unroll
+                    for (int i = 0; i < 16; i++) {
+                        const uint32_t hb = (((w[i] & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w[i]) & 0x80808080u;
+                        const uint32_t nb = ((hb * 0x00204081u) >> (28 - 4 * (i & 7))) & (15u << (4 * (i & 7)));
+                        if (i < 8) nlo |= nb;
+                        else nhi |= nb;
+                    }
+                }
+            }
+            // level 2: bm1 bytes that differ from their predecessor
+            uint32_t prev = __shfl_up_sync(full, nhi, 1) >> 24;
+            if (lane == 0) prev = t ? (nz_nibble(Sw[16 * t - 2]) | (nz_nibble(Sw[16 * t - 1]) << 4)) : 0u;
+            const uint64_t M = ((uint64_t)nhi << 32) | nlo;
+            const uint32_t m2 = nz_byte_mask64(M ^ ((M << 8) | prev));
+            const uint32_t v12 = (uint32_t)(__popc(nlo) + __popc(nhi)) | ((uint32_t)__popc(m2) << 16);
+            const uint32_t inc12 = warp_incl_scan(v12);
+            if (lane == 31) s_l1[warp] = inc12;
+            bm2[t] = (uint8_t)m2;
             __syncthreads();  // B3
-            const uint32_t nzT = s_misc[0];
+            uint32_t tot12 = 0, pre12 = inc12 - v12;
+#pragma unroll
+            for (int w8 = 0; w8 < 8; w8++) {
+                const uint32_t v = s_l1[w8];
+                tot12 += v;
+                if ((uint32_t)w8 < warp) pre12 += v;
+            }
+            const uint32_t nzT = tot12 & 0xffffu, n2T = tot12 >> 16;
 
             if (om) {  // outlier records, ascending index within the chunk
                 uint32_t pos = s_misc[1] + oex;
-                for (uint32_t w = 0; w < warp; w++) pos += s_wout[w];
+                for (uint32_t w8 = 0; w8 < warp; w8++) pos += s_wout[w8];
                 const uint32_t kb = c * (uint32_t)kChunkCodes + 32u * t;
                 uint32_t m = om;
                 while (m) {
@@ -365,67 +354,39 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
             }
 
-            // 0: encode, 1: all-zero chunk, 2: stored raw (rze_stage.cu:365-372)
+            // 0: encode, 1: all-zero chunk, 2: stored raw (rze_stage.cu:365-389)
             int mode = nzT == 0 ? 1 : ((nzT >= (uint32_t)kRzeAvail || nzT > (uint32_t)(kRzeAvail - 2048)) ? 2 : 0);
+            const uint32_t wpos = nzT + n2T;
+            if (mode == 0 && (wpos >= (uint32_t)kRzeAvail || wpos > (uint32_t)(kRzeAvail - 256))) mode = 2;
             if (mode == 0) {
+                // level-1 payload: the nonzero bytes of the 16 words, compacted
+                uint32_t pos = pre12 & 0xffffu;
 #pragma unroll
-                for (int b = 0; b < 16; b++) {
-                    if ((pm >> b) & 1u) {
-                        const uint32_t nib = (uint32_t)(nib64 >> (4 * b)) & 15u;
-                        if (nib) {
-                            const uint32_t pos = s_base[warp][b] + ((KX[b >> 2] >> (8 * (b & 3))) & 0xffu);
-                            const uint32_t packed = __byte_perm(x[b], 0u, s_sel[nib]);
-                            const uint32_t sh = (pos & 3u) * 8u;
-                            atomicOr(&Ow[pos >> 2], packed << sh);
-                            atomicOr(&Ow[(pos >> 2) + 1], __funnelshift_l(packed, 0u, sh));
-                        }
+                for (int i = 0; i < 16; i++) {
+                    const uint32_t nb = ((i < 8 ? nlo : nhi) >> (4 * (i & 7))) & 15u;
+                    if (nb) {
+                        const uint32_t packed = __byte_perm(w[i], 0u, s_sel[nb]);
+                        const uint32_t sh = (pos & 3u) * 8u;
+                        atomicOr(&Ow[pos >> 2], packed << sh);
+                        atomicOr(&Ow[(pos >> 2) + 1], __funnelshift_l(packed, 0u, sh));
                     }
+                    pos += __popc(nb);
                 }
-                const uint2 bw = bm1_words(nib64, lane);
-                const uint32_t j = lane & 7u;
-                bm1[(15 - 2 * j) * 32 + (t >> 3)] = bw.x;
-                bm1[(14 - 2 * j) * 32 + (t >> 3)] = bw.y;
+                // level-2 payload: the non-repeated bm1 bytes
+                uint32_t q = nzT + (pre12 >> 16);
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const uint32_t mb = (m2 >> (4 * h)) & 15u;
+                    if (mb) {
+                        const uint32_t packed = __byte_perm(h ? nhi : nlo, 0u, s_sel[mb]);
+                        const uint32_t sh = (q & 3u) * 8u;
+                        atomicOr(&Ow[q >> 2], packed << sh);
+                        atomicOr(&Ow[(q >> 2) + 1], __funnelshift_l(packed, 0u, sh));
+                    }
+                    q += __popc(mb);
+                }
             }
             __syncthreads();  // B4
-
-            // level 2: the bm1 bytes that differ from their predecessor
-            uint64_t M = 0;
-            uint32_t m2 = 0, ex2 = 0;
-            if (mode == 0) {
-                const uint2 mw = reinterpret_cast<const uint2*>(bm1)[t];
-                M = ((uint64_t)mw.y << 32) | mw.x;
-                uint32_t prev = __shfl_up_sync(full, mw.y, 1) >> 24;
-                if (lane == 0) prev = t ? (uint32_t)reinterpret_cast<const uint8_t*>(bm1)[8 * t - 1] : 0u;
-                m2 = nz_byte_mask64(M ^ ((M << 8) | prev));
-                const uint32_t n2 = __popc(m2);
-                const uint32_t inc = warp_incl_scan(n2);
-                ex2 = inc - n2;
-                if (lane == 31) s_l2[warp] = inc;
-                bm2[t] = (uint8_t)m2;
-            }
-            __syncthreads();  // B5
-            uint32_t wpos = 0;
-            if (mode == 0) {
-                uint32_t n2T = 0;
-#pragma unroll
-                for (int w = 0; w < 8; w++) {
-                    const uint32_t v = s_l2[w];
-                    if ((uint32_t)w < warp) ex2 += v;
-                    n2T += v;
-                }
-                wpos = nzT + n2T;
-                if (wpos >= (uint32_t)kRzeAvail || wpos > (uint32_t)(kRzeAvail - 256)) {
-                    mode = 2;
-                } else {
-                    uint32_t p = nzT + ex2, m = m2;
-                    while (m) {
-                        const uint32_t b = __ffs(m) - 1;
-                        m &= m - 1;
-                        O[p++] = (uint8_t)(M >> (8 * b));
-                    }
-                }
-            }
-            __syncthreads();  // B6
 
             // levels 3 and 4 (warp 0), header
             if (mode == 0 && warp == 0) {
@@ -477,7 +438,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     s_misc[2] = 0x80000000u | (uint32_t)kChunkBytes;
                 }
             }
-            __syncthreads();  // B7
+            __syncthreads();  // B5
 
             const uint32_t sw = s_misc[2];
             uint8_t* slot = a.slots + (size_t)c * kChunkBytes;
