@@ -259,7 +259,7 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
     CK(cudaGetLastError());
     {
         TraceScope ts(s, "assemble_copy");
-        assemble_copy_kernel<<<(unsigned)nch, 256, 0, s>>>(m);
+        assemble_copy_kernel<<<copy_grid(nch), 256, 0, s>>>(m);
     }
     CK(cudaGetLastError());
     return FZB_OK;
@@ -448,7 +448,7 @@ int fzb_rze_encode(const void* d_in, uint64_t bytes, void* d_out, uint64_t* d_ou
     m.pay_off = w.in_off;
     assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
     CK(cudaGetLastError());
-    assemble_copy_kernel<<<(unsigned)nch, 256, 0, s>>>(m);
+    assemble_copy_kernel<<<copy_grid(nch), 256, 0, s>>>(m);
     CK(cudaGetLastError());
     return FZB_OK;
 }

@@ -324,59 +324,106 @@ __device__ __forceinline__ void write_slot(uint8_t* __restrict__ slots, uint32_t
 // Exclusive scans over chunks (one CTA of 1024 threads): payload offsets,
 // outlier offsets, RZE header, total sizes.
 __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a) {
-    __shared__ unsigned long long sp[1024];
-    __shared__ unsigned int so[1024];
-    const uint32_t n = a.n_chunks, t = threadIdx.x;
-    const uint32_t per = (n + 1023) / 1024;
-    const uint32_t b = t * per, e = min(n, b + per);
+    // Tiles of 4096 chunks: coalesced loads into shared memory, 4 chunks per
+    // thread, a warp-shuffle block scan, coalesced writes, carry to the next tile.
+    constexpr uint32_t kTile = 4096, kPer = kTile / 1024;
+    __shared__ uint32_t sp[kTile], so[kTile];
+    __shared__ uint32_t wp[32], wo[32], s_tile[2];
+    const uint32_t n = a.n_chunks, t = threadIdx.x, lane = t & 31, warp = t >> 5;
     // outliers that found room in staging (an overflowing run keeps those,
     // the count still reports every outlier found)
     auto staged = [&](uint32_t i) -> uint32_t {
         const uint32_t b0 = a.obase[i], n0 = a.ocnt[i];
         return b0 >= a.ostage_cap ? 0u : min(n0, a.ostage_cap - b0);
     };
-    unsigned long long ps = 0;
-    unsigned int os = 0, ot = 0;
-    for (uint32_t i = b; i < e; i++) {
-        if (a.sizes) ps += a.sizes[i] & 0x7fffffffu;
-        if (a.ocnt) {
-            os += staged(i);
-            ot += a.ocnt[i];
+    uint32_t* hdr = reinterpret_cast<uint32_t*>(a.out);
+    unsigned long long carry_p = 0;
+    uint32_t carry_o = 0, ot = 0;
+    for (uint32_t t0 = 0; t0 < n; t0 += kTile) {
+        const uint32_t cnt = min(kTile, n - t0);
+        for (uint32_t i = t; i < kTile; i += 1024) {
+            uint32_t vp = 0, vo = 0;
+            if (i < cnt) {
+                if (a.sizes) vp = a.sizes[t0 + i] & 0x7fffffffu;
+                if (a.ocnt) {
+                    vo = staged(t0 + i);
+                    ot += a.ocnt[t0 + i];
+                }
+            }
+            sp[i] = vp;
+            so[i] = vo;
         }
+        __syncthreads();
+        uint32_t lp = 0, lo = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j++) {
+            lp += sp[kPer * t + j];
+            lo += so[kPer * t + j];
+        }
+        uint32_t ip = lp, io = lo;  // inclusive warp scans
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t np = __shfl_up_sync(0xffffffffu, ip, d), no = __shfl_up_sync(0xffffffffu, io, d);
+            if (lane >= (uint32_t)d) {
+                ip += np;
+                io += no;
+            }
+        }
+        if (lane == 31) {
+            wp[warp] = ip;
+            wo[warp] = io;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t vp = wp[lane], vo = wo[lane];
+            uint32_t xp = vp, xo = vo;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t np = __shfl_up_sync(0xffffffffu, xp, d), no = __shfl_up_sync(0xffffffffu, xo, d);
+                if (lane >= (uint32_t)d) {
+                    xp += np;
+                    xo += no;
+                }
+            }
+            wp[lane] = xp - vp;  // exclusive warp offsets
+            wo[lane] = xo - vo;
+        }
+        __syncthreads();
+        uint32_t rp = wp[warp] + ip - lp, ro = wo[warp] + io - lo;
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j++) {  // exclusive prefixes in place
+            const uint32_t vp = sp[kPer * t + j], vo = so[kPer * t + j];
+            sp[kPer * t + j] = rp;
+            so[kPer * t + j] = ro;
+            rp += vp;
+            ro += vo;
+        }
+        if (t == 1023) {
+            s_tile[0] = rp;
+            s_tile[1] = ro;
+        }
+        __syncthreads();
+        for (uint32_t i = t; i < cnt; i += 1024) {
+            if (a.sizes) {
+                a.pay_off[t0 + i] = carry_p + sp[i];
+                hdr[2 + t0 + i] = a.sizes[t0 + i];
+            }
+            if (a.ocnt) a.ofin[t0 + i] = carry_o + so[i];
+        }
+        carry_p += s_tile[0];
+        carry_o += s_tile[1];
+        __syncthreads();  // the next tile reuses the arrays
     }
-    sp[t] = ps;
-    so[t] = os;
     __shared__ unsigned int s_tot;
     if (t == 0) s_tot = 0;
     __syncthreads();
-    if (a.ocnt) atomicAdd(&s_tot, ot);
-    for (int d = 1; d < 1024; d <<= 1) {
-        unsigned long long vp = (t >= (unsigned)d) ? sp[t - d] : 0ull;
-        unsigned int vo = (t >= (unsigned)d) ? so[t - d] : 0u;
-        __syncthreads();
-        sp[t] += vp;
-        so[t] += vo;
-        __syncthreads();
-    }
-    unsigned long long rp = sp[t] - ps;
-    unsigned int ro = so[t] - os;
-    uint32_t* hdr = reinterpret_cast<uint32_t*>(a.out);
-    for (uint32_t i = b; i < e; i++) {
-        if (a.sizes) {
-            a.pay_off[i] = rp;
-            rp += a.sizes[i] & 0x7fffffffu;
-            hdr[2 + i] = a.sizes[i];
-        }
-        if (a.ocnt) {
-            a.ofin[i] = ro;
-            ro += staged(i);
-        }
-    }
+    if (a.ocnt && ot) atomicAdd(&s_tot, ot);
+    __syncthreads();
     if (t == 1023) {
         if (a.sizes) {
             hdr[0] = a.orig_bytes;
             hdr[1] = n;
-            const unsigned long long total = 8ull + 4ull * n + sp[1023];
+            const unsigned long long total = 8ull + 4ull * n + carry_p;
             const unsigned long long padded = (total + 3) & ~3ull;
             for (unsigned long long i = total; i < padded; i++) a.out[i] = 0;
             *a.out_size = padded;
@@ -387,10 +434,12 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a) {
 
 __global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) { assemble_scan_body(a); }
 
-// One CTA per chunk: payload from its slot to the final stream position
+// One chunk per group of `nth` threads (thread `tid` of the group): payload
+// from its slot to the final stream position
 // (any byte alignment), and its outliers from staging to their sorted
 // position (chunks are index ranges and each chunk's block is sorted).
-__device__ __forceinline__ void assemble_copy_body(const AsmArgs& a, const uint32_t c) {
+__device__ __forceinline__ void assemble_copy_body(const AsmArgs& a, const uint32_t c, const uint32_t tid,
+                                                   const uint32_t nth) {
     if (a.sizes) {
         const uint32_t len = a.sizes[c] & 0x7fffffffu;
         uint8_t* dst = a.out + 8ull + 4ull * a.n_chunks + a.pay_off[c];
@@ -399,14 +448,14 @@ __device__ __forceinline__ void assemble_copy_body(const AsmArgs& a, const uint3
         const uintptr_t d0 = reinterpret_cast<uintptr_t>(dst), d1 = d0 + len;
         const uintptr_t a0 = (d0 + 3) & ~(uintptr_t)3, a1 = d1 & ~(uintptr_t)3;
         if (a0 >= a1) {
-            for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) dst[i] = src[i];
+            for (uint32_t i = tid; i < len; i += nth) dst[i] = src[i];
         } else {
             const uint32_t head = (uint32_t)(a0 - d0), tail = (uint32_t)(d1 - a1);
-            if (threadIdx.x < head) dst[threadIdx.x] = src[threadIdx.x];
-            if (threadIdx.x < tail) dst[(a1 - d0) + threadIdx.x] = src[(a1 - d0) + threadIdx.x];
+            if (tid < head) dst[tid] = src[tid];
+            if (tid < tail) dst[(a1 - d0) + tid] = src[(a1 - d0) + tid];
             uint32_t* dw = reinterpret_cast<uint32_t*>(a0);
             const uint32_t nw = (uint32_t)((a1 - a0) >> 2), r = head & 3;
-            for (uint32_t i = threadIdx.x; i < nw; i += blockDim.x) {
+            for (uint32_t i = tid; i < nw; i += nth) {
                 const uint32_t w0 = (head + 4 * i) >> 2;  // source word of destination word i
                 const uint32_t lo = __ldg(s32 + w0);
                 const uint32_t hi = r ? __ldg(s32 + w0 + 1) : 0u;
@@ -417,7 +466,7 @@ __device__ __forceinline__ void assemble_copy_body(const AsmArgs& a, const uint3
     if (a.ocnt) {
         const uint32_t b = a.obase[c], f = a.ofin[c];
         const uint32_t n = b >= a.ostage_cap ? 0u : min(a.ocnt[c], a.ostage_cap - b);
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        for (uint32_t i = tid; i < n; i += nth) {
             const uint32_t s = b + i, d = f + i;
             if (d < a.cap) {
                 a.out_err[d] = a.ostage_err[s];
@@ -427,7 +476,13 @@ __device__ __forceinline__ void assemble_copy_body(const AsmArgs& a, const uint3
     }
 }
 
-__global__ void __launch_bounds__(256) assemble_copy_kernel(AsmArgs a) { assemble_copy_body(a, blockIdx.x); }
+// One warp per chunk, grid-stride over the chunks.
+__global__ void __launch_bounds__(256) assemble_copy_kernel(AsmArgs a) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < a.n_chunks; c += nw)
+        assemble_copy_body(a, c, lane, 32);
+}
 
 // Row-vector path: one thread, 32 consecutive elements of one row, all
 // operands staged in shared memory.  TZ/TY say whether the z / y predecessor
@@ -743,7 +798,7 @@ __global__ void __launch_bounds__(256) batch_assemble_copy_kernel(BatchArgs b) {
         if (b.unit_begin[mid] <= u) lo = mid;
         else hi = mid;
     }
-    assemble_copy_body(b.fields[b.unit_order[lo]].m, u - b.unit_begin[lo]);
+    assemble_copy_body(b.fields[b.unit_order[lo]].m, u - b.unit_begin[lo], threadIdx.x, blockDim.x);
 }
 
 // Per launch: the unit dispenser, every field's error word and outlier

@@ -104,7 +104,11 @@ __global__ void bitshuffle_ballot_kernel(const uint8_t* in, uint8_t* out, uint32
                                          int inverse);
 __global__ void rze_encode_kernel(RzeEncArgs a);
 __global__ void assemble_scan_kernel(AsmArgs a);
-__global__ void assemble_copy_kernel(AsmArgs a);
+__global__ void assemble_copy_kernel(AsmArgs a);  // one warp per chunk, grid-stride
+inline unsigned copy_grid(uint64_t n_chunks) {
+    const uint64_t g = (n_chunks + 7) / 8;
+    return (unsigned)(g < 1184 ? (g ? g : 1) : 1184);
+}
 
 __global__ void rze_prepass_kernel(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect,
                                    uint32_t orig_expect, unsigned long long* in_off, uint32_t* err);

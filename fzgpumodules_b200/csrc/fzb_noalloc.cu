@@ -97,7 +97,7 @@ extern "C" int fzb_rze_encode_noalloc(const void* d_in, uint64_t bytes, void* d_
     m.pay_off = reinterpret_cast<unsigned long long*>(scratch + kPayOff);
     assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
     if (cudaGetLastError() != cudaSuccess) return FZB_E_CUDA;
-    assemble_copy_kernel<<<nch, 256, 0, s>>>(m);
+    assemble_copy_kernel<<<copy_grid(nch), 256, 0, s>>>(m);
     if (cudaGetLastError() != cudaSuccess) return FZB_E_CUDA;
     return FZB_OK;
 }

@@ -51,46 +51,51 @@ __device__ __forceinline__ uint32_t half_bits(float sv) {
 
 namespace {
 
+constexpr int kTT = 512;  // threads of a slab-compressor CTA: 16 chunk elements each
+
+// Byte offset of 16-byte granule g (0..3) of thread t's elements 16t..16t+15
+// in a swizzled plane buffer (two threads per 128-byte row).
+__device__ __forceinline__ uint32_t thr_off(uint32_t t, uint32_t g) {
+    return swz_off(t >> 1, 4u * (t & 1u) + g);
+}
+
 // ---------------------------------------------------------------------------
-// Codes of one thread's 32 elements from B (z- and x-differenced) and the
+// Codes of one thread's 16 elements from B (z- and x-differenced) and the
 // row above (read from the swizzled exchange buffer when ty != 0).
-// x[k] = code[k] | code[k + 16] << 16; om8 bit g = granule g (elements
+// x[k] = code[k] | code[k + 8] << 16; om4 bit g = granule g (elements
 // 4g..4g+3) may hold an outlier.  Outlier codes are not zeroed here.
 // ---------------------------------------------------------------------------
 template <bool ZZ>
-__device__ __forceinline__ void make_codes(const float (&B)[32], const uint8_t* stg, uint32_t tu, bool ty,
-                                           float R, uint32_t (&x)[16], uint32_t& om8) {
-    om8 = 0;
+__device__ __forceinline__ void make_codes16(const float (&B)[16], const uint8_t* stg, uint32_t tu, bool ty,
+                                             float R, uint32_t (&x)[8], uint32_t& om4) {
+    om4 = 0;
 #pragma unroll
-    for (int g = 0; g < 4; g++) {
-        float c[8];  // elements 4g..4g+3 and 16+4g..16+4g+3
-        float4 u0 = make_float4(0.f, 0.f, 0.f, 0.f), u1 = u0;
+    for (int g = 0; g < 2; g++) {
+        float c[8];  // elements 4g..4g+3 and 8+4g..8+4g+3
         if (ty) {
-            u0 = *reinterpret_cast<const float4*>(stg + swz_off(tu, g));
-            u1 = *reinterpret_cast<const float4*>(stg + swz_off(tu, g + 4));
-        }
-        float2 d;
-        if (ty) {
+            const float4 u0 = *reinterpret_cast<const float4*>(stg + thr_off(tu, g));
+            const float4 u1 = *reinterpret_cast<const float4*>(stg + thr_off(tu, g + 2));
+            float2 d;
             d = sub2(f2(B[4 * g], B[4 * g + 1]), f2(u0.x, u0.y));  c[0] = d.x; c[1] = d.y;
             d = sub2(f2(B[4 * g + 2], B[4 * g + 3]), f2(u0.z, u0.w));  c[2] = d.x; c[3] = d.y;
-            d = sub2(f2(B[16 + 4 * g], B[17 + 4 * g]), f2(u1.x, u1.y));  c[4] = d.x; c[5] = d.y;
-            d = sub2(f2(B[18 + 4 * g], B[19 + 4 * g]), f2(u1.z, u1.w));  c[6] = d.x; c[7] = d.y;
+            d = sub2(f2(B[8 + 4 * g], B[9 + 4 * g]), f2(u1.x, u1.y));  c[4] = d.x; c[5] = d.y;
+            d = sub2(f2(B[10 + 4 * g], B[11 + 4 * g]), f2(u1.z, u1.w));  c[6] = d.x; c[7] = d.y;
         } else {
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 c[k] = B[4 * g + k];
-                c[4 + k] = B[16 + 4 * g + k];
+                c[4 + k] = B[8 + 4 * g + k];
             }
         }
         const float m0 = max_nan(max_nan(fabsf(c[0]), fabsf(c[1])), max_nan(fabsf(c[2]), fabsf(c[3])));
         const float m1 = max_nan(max_nan(fabsf(c[4]), fabsf(c[5])), max_nan(fabsf(c[6]), fabsf(c[7])));
-        if (!(m0 < R)) om8 |= 1u << g;
-        if (!(m1 < R)) om8 |= 1u << (g + 4);
+        if (!(m0 < R)) om4 |= 1u << g;
+        if (!(m1 < R)) om4 |= 1u << (g + 2);
         const float2 M2 = make_float2(kMagic, kMagic);
         float cm[8];
 #pragma unroll
         for (int k = 0; k < 8; k += 2) {
-            d = __fadd2_rn(f2(c[k], c[k + 1]), M2);
+            const float2 d = __fadd2_rn(f2(c[k], c[k + 1]), M2);
             cm[k] = d.x;
             cm[k + 1] = d.y;
         }
@@ -107,18 +112,18 @@ __device__ __forceinline__ void make_codes(const float (&B)[32], const uint8_t* 
     }
 }
 
-// Exact outlier mask (bit e = element e) for the granules flagged in om8,
+// Exact outlier mask (bit e = element e) for the granules flagged in om4,
 // recomputed from the exchange buffer (the thread's own B and the row above).
-__device__ __forceinline__ uint32_t outlier_mask(const uint8_t* stg, uint32_t t, uint32_t tu, bool ty, float R,
-                                                 uint32_t om8) {
+__device__ __forceinline__ uint32_t outlier_mask16(const uint8_t* stg, uint32_t t, uint32_t tu, bool ty, float R,
+                                                   uint32_t om4) {
     uint32_t om = 0;
-    while (om8) {
-        const uint32_t g = __ffs(om8) - 1;
-        om8 &= om8 - 1;
-        const float4 b = *reinterpret_cast<const float4*>(stg + swz_off(t, g));
+    while (om4) {
+        const uint32_t g = __ffs(om4) - 1;
+        om4 &= om4 - 1;
+        const float4 b = *reinterpret_cast<const float4*>(stg + thr_off(t, g));
         float c[4] = {b.x, b.y, b.z, b.w};
         if (ty) {
-            const float4 u = *reinterpret_cast<const float4*>(stg + swz_off(tu, g));
+            const float4 u = *reinterpret_cast<const float4*>(stg + thr_off(tu, g));
             c[0] = __fsub_rn(c[0], u.x);
             c[1] = __fsub_rn(c[1], u.y);
             c[2] = __fsub_rn(c[2], u.z);
@@ -132,51 +137,81 @@ __device__ __forceinline__ uint32_t outlier_mask(const uint8_t* stg, uint32_t t,
 }
 
 // Delta of element e (the value an outlier record stores).
-__device__ __forceinline__ float delta_at(const uint8_t* stg, uint32_t t, uint32_t tu, bool ty, uint32_t e) {
-    const float* p = reinterpret_cast<const float*>(stg + swz_off(t, e >> 2)) + (e & 3);
-    float c = *p;
-    if (ty) c = __fsub_rn(c, *(reinterpret_cast<const float*>(stg + swz_off(tu, e >> 2)) + (e & 3)));
+__device__ __forceinline__ float delta_at16(const uint8_t* stg, uint32_t t, uint32_t tu, bool ty, uint32_t e) {
+    float c = *(reinterpret_cast<const float*>(stg + thr_off(t, e >> 2)) + (e & 3));
+    if (ty) c = __fsub_rn(c, *(reinterpret_cast<const float*>(stg + thr_off(tu, e >> 2)) + (e & 3)));
     return c;
 }
 
-// Compaction selectors: __byte_perm(w, 0, kSel[m]) moves the bytes of w
+// In-place transpose of a 16x16 bit matrix held as x[k] = row k | row (k+8)
+// << 16: afterwards x[m] = column m | column (m+8) << 16, bit i of a column
+// = bit of row i.  With rows = codes this yields the bit planes of the 16
+// codes (the Bitshuffle ballot layout, bitshuffle_stage.cu:299-323, for half
+// of a 32-code group).  The 8x8 off-diagonal blocks swap by a byte permute,
+// then each byte lane transposes its 8x8 block in three stages.
+__device__ __forceinline__ void transpose16(uint32_t (&x)[8]) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = __byte_perm(x[k], 0u, 0x3120);
+#pragma unroll
+    for (int s = 4; s >= 1; s >>= 1) {
+        const uint32_t m = (s == 4) ? 0x0f0f0f0fu : (s == 2) ? 0x33333333u : 0x55555555u;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            if (i & s) continue;
+            const uint32_t d = ((x[i] >> s) ^ x[i + s]) & m;
+            x[i + s] ^= d;
+            x[i] ^= d << s;
+        }
+    }
+}
+
+// Compaction selectors: __byte_perm(w, 0, kSelInit[m]) moves the bytes of w
 // flagged in the 4-bit mask m to the low end, in order, zero-filled.
 __constant__ uint32_t kSelInit[16] = {
     0x4444, 0x4440, 0x4441, 0x4410, 0x4442, 0x4420, 0x4421, 0x4210,
     0x4443, 0x4430, 0x4431, 0x4310, 0x4432, 0x4320, 0x4321, 0x3210};
+
+// ORs the 4 bytes of `packed` (the low popc bytes meaningful) into the
+// zeroed byte stream O at byte offset pos.
+__device__ __forceinline__ void or_bytes_at(uint32_t* Ow, uint32_t pos, uint32_t packed) {
+    const uint32_t sh = (pos & 3u) * 8u;
+    atomicOr(&Ow[pos >> 2], packed << sh);
+    atomicOr(&Ow[(pos >> 2) + 1], __funnelshift_l(packed, 0u, sh));
+}
 
 }  // namespace
 
 namespace {
 
 template <bool ZZ>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kTT, 2)
     lq3d_tma_kernel(const FwdArgs a, const __grid_constant__ CUtensorMap map, uint32_t slabs, uint32_t units) {
     extern __shared__ uint8_t dsm[];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ uint32_t s_sel[16];
-    __shared__ uint32_t s_wout[8];       // per warp: outlier count
-    __shared__ uint32_t s_l1[8];         // per warp: level-1 | level-2 << 16 byte counts
-    __shared__ uint32_t s_misc[4];       // 1 outlier staging base, 2 size word
+    __shared__ uint32_t s_wout[kTT / 32];  // per warp: outlier count
+    __shared__ uint32_t s_l1[kTT / 32];    // per warp: level-1 | level-2 << 16 byte counts
+    __shared__ uint32_t s_misc[4];         // 1 outlier staging base, 2 size word
 
     uint8_t* base = dsm + ((kSmemAlign - (smem_u32(dsm) & (kSmemAlign - 1))) & (kSmemAlign - 1));
     uint8_t* O = base + 2 * kStageBytes;
     uint32_t* Ow = reinterpret_cast<uint32_t*>(O);
-    uint8_t* Sbuf = O + kOBytes;            // the shuffled chunk (16 KiB)
+    uint8_t* Sbuf = O + kOBytes;  // the shuffled chunk (16 KiB)
+    uint32_t* Sw = reinterpret_cast<uint32_t*>(Sbuf);
+    uint16_t* Sh = reinterpret_cast<uint16_t*>(Sbuf);
     uint8_t* bm2 = Sbuf + kChunkBytes;
 
     const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t full = 0xffffffffu;
-    const uint32_t nx = a.nx, R = kChunkCodes / nx, S = nx / 32;
-    const bool ty = ((t / S) & 7u) != 0;   // slab origins have y % 8 == 0
-    const uint32_t tu = ty ? t - S : t;    // thread holding the row above
+    const uint32_t nx = a.nx, R = kChunkCodes / nx, S16 = nx / 16;  // threads per row
+    const bool ty = ((t / S16) & 7u) != 0;  // slab origins have y % 8 == 0
+    const uint32_t tu = ty ? t - S16 : t;   // thread holding the row above
     const float r = *a.ebx2_r;
     const float rad = a.radius;
     const uint32_t G = gridDim.x;
 
     if (t < 16) s_sel[t] = kSelInit[t];
-    for (uint32_t i = t; i < (uint32_t)kOBytes / 16; i += kThreads)
-        reinterpret_cast<uint4*>(O)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (uint32_t i = t; i < (uint32_t)kOBytes / 16; i += kTT) reinterpret_cast<uint4*>(O)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (t == 0) {
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
@@ -209,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     for (uint32_t uu = blockIdx.x; uu < units; uu += G) {
         const uint32_t u = units - 1 - uu, s = u % slabs;
         const uint32_t z0 = (u / slabs) * 8u, z1 = min(z0 + 8u, a.nz);
-        float qp[32];
+        float qp[16];
         for (uint32_t z = z0; z < z1; z++, k++) {
             const uint32_t c = z * slabs + s;
             const bool tz = z != z0;
@@ -217,11 +252,11 @@ __global__ void __launch_bounds__(kThreads, 2)
             const bool bad = !mbar_wait_bounded(&s_bar[k & 1], (k >> 1) & 1u);
 
             // q, z difference, x difference; B over the thread's own bytes
-            float B[32];
+            float B[16];
             float alast = 0.0f;
 #pragma unroll
-            for (int g = 0; g < 8; g++) {
-                const float4 v = *reinterpret_cast<const float4*>(stg + swz_off(t, g));
+            for (int g = 0; g < 4; g++) {
+                const float4 v = *reinterpret_cast<const float4*>(stg + thr_off(t, g));
                 const float2 rr = f2(r, r);
                 const float2 y0 = __fmul2_rn(f2(v.x, v.y), rr), y1 = __fmul2_rn(f2(v.z, v.w), rr);
                 const float2 s0 = __fadd2_rn(y0, f2(__uint_as_float(half_bits(v.x)), __uint_as_float(half_bits(v.y))));
@@ -236,16 +271,13 @@ __global__ void __launch_bounds__(kThreads, 2)
                 qp[4 * g + 1] = q0.y;
                 qp[4 * g + 2] = q1.x;
                 qp[4 * g + 3] = q1.y;
-                const float b0 = (g & 1) ? __fsub_rn(A0.x, alast) : A0.x;  // x % 8 == 0 starts a tile
-                const float b1 = __fsub_rn(A0.y, A0.x);
-                const float b2 = __fsub_rn(A1.x, A0.y);
-                const float b3 = __fsub_rn(A1.y, A1.x);
+                // x % 8 == 0 starts a tile: elements 0 and 8 of the thread
+                B[4 * g] = (g & 1) ? __fsub_rn(A0.x, alast) : A0.x;
+                B[4 * g + 1] = __fsub_rn(A0.y, A0.x);
+                B[4 * g + 2] = __fsub_rn(A1.x, A0.y);
+                B[4 * g + 3] = __fsub_rn(A1.y, A1.x);
                 alast = A1.y;
-                B[4 * g] = b0;
-                B[4 * g + 1] = b1;
-                B[4 * g + 2] = b2;
-                B[4 * g + 3] = b3;
-                *reinterpret_cast<float4*>(stg + swz_off(t, g)) = make_float4(b0, b1, b2, b3);
+                *reinterpret_cast<float4*>(stg + thr_off(t, g)) = make_float4(B[4 * g], B[4 * g + 1], B[4 * g + 2], B[4 * g + 3]);
             }
             if (__syncthreads_or(bad)) {  // B1 (a copy did not arrive: give up)
                 if (t == 0) {
@@ -259,14 +291,15 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
             if (t == 0 && k >= 1) issue_next(k + 1);
 
-            // codes, outliers, bit transpose
-            uint32_t x[16], om8;
-            make_codes<ZZ>(B, stg, tu, ty, rad, x, om8);
-            const uint32_t om = om8 ? outlier_mask(stg, t, tu, ty, rad, om8) : 0u;
-            transpose16x2(x);
+            // codes, outliers, bit planes
+            uint32_t x[8], om4;
+            make_codes16<ZZ>(B, stg, tu, ty, rad, x, om4);
+            const uint32_t om = om4 ? outlier_mask16(stg, t, tu, ty, rad, om4) : 0u;
+            transpose16(x);
             if (__any_sync(full, om != 0u)) {
+                const uint32_t keep = ~(om | (om << 16));  // outlier codes are 0
 #pragma unroll
-                for (int b = 0; b < 16; b++) x[b] &= ~om;  // outlier codes are 0
+                for (int b = 0; b < 8; b++) x[b] &= keep;
             }
             const uint32_t nout = __popc(om);
             uint32_t oex = 0;
@@ -277,77 +310,76 @@ __global__ void __launch_bounds__(kThreads, 2)
             } else if (lane == 0) {
                 s_wout[warp] = 0;
             }
-
-            // RZE levels 1 and 2 from the shuffled chunk S (plane word b of
-            // segment t at word (15-b)*256 + t): thread t then takes S words
-            // 16t..16t+15 (bytes 64t..64t+63, one plane region), whose
-            // nonzero-byte nibbles are bm1 bytes 8t..8t+7
-            uint32_t* Sw = reinterpret_cast<uint32_t*>(Sbuf);
+            // the shuffled chunk S: plane b of the 32-code group j is word
+            // (15-b)*256 + j, its low half from thread 2j, high half from 2j+1
 #pragma unroll
-            for (int b = 0; b < 16; b++) Sw[(15 - b) * 256 + t] = x[b];
+            for (int b = 0; b < 8; b++) {
+                Sh[(15 - b) * 512 + t] = (uint16_t)x[b];
+                Sh[(7 - b) * 512 + t] = (uint16_t)(x[b] >> 16);
+            }
             __syncthreads();  // B2
             if (t == 0) {  // staging for this chunk's outliers
                 uint32_t tot = 0;
 #pragma unroll
-                for (int w = 0; w < 8; w++) tot += s_wout[w];
+                for (int w = 0; w < kTT / 32; w++) tot += s_wout[w];
                 const uint32_t ob = tot ? atomicAdd(a.ostage_ctr, tot) : 0u;
                 a.obase[c] = ob;
                 a.ocnt[c] = tot;
                 s_misc[1] = ob;
             }
-            uint32_t w[16];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const uint4 q = reinterpret_cast<const uint4*>(Sw)[4 * t + i];
-                w[4 * i] = q.x;
-                w[4 * i + 1] = q.y;
-                w[4 * i + 2] = q.z;
-                w[4 * i + 3] = q.w;
-            }
-            uint32_t nlo = 0, nhi = 0;
+
+            // RZE levels 1 and 2: thread t takes S words 8t..8t+7 (warp w =
+            // plane region w); their nonzero-byte nibbles are bm1 word t
+            uint32_t w[8];
             {
-                uint32_t o = 0;
+                const uint4 q0 = reinterpret_cast<const uint4*>(Sw)[2 * t], q1 = reinterpret_cast<const uint4*>(Sw)[2 * t + 1];
+                w[0] = q0.x; w[1] = q0.y; w[2] = q0.z; w[3] = q0.w;
+                w[4] = q1.x; w[5] = q1.y; w[6] = q1.z; w[7] = q1.w;
+            }
+            uint32_t nb1 = 0;
+            if (__any_sync(full, (w[0] | w[1] | w[2] | w[3] | w[4] | w[5] | w[6] | w[7]) != 0u)) {
 #pragma unroll
-                for (int i = 0; i < 16; i++) o |= w[i];
-                if (__any_sync(full, o != 0u)) {  // warps over empty plane regions skip
-#pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        const uint32_t hb = (((w[i] & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w[i]) & 0x80808080u;
-                        const uint32_t nb = ((hb * 0x00204081u) >> (28 - 4 * (i & 7))) & (15u << (4 * (i & 7)));
-                        if (i < 8) nlo |= nb;
-                        else nhi |= nb;
-                    }
+                for (int i = 0; i < 8; i++) {
+                    const uint32_t hb = (((w[i] & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w[i]) & 0x80808080u;
+                    nb1 |= ((hb * 0x00204081u) >> (28 - 4 * i)) & (15u << (4 * i));
                 }
             }
             // level 2: bm1 bytes that differ from their predecessor
-            uint32_t prev = __shfl_up_sync(full, nhi, 1) >> 24;
-            if (lane == 0) prev = t ? (nz_nibble(Sw[16 * t - 2]) | (nz_nibble(Sw[16 * t - 1]) << 4)) : 0u;
-            const uint64_t M = ((uint64_t)nhi << 32) | nlo;
-            const uint32_t m2 = nz_byte_mask64(M ^ ((M << 8) | prev));
-            const uint32_t v12 = (uint32_t)(__popc(nlo) + __popc(nhi)) | ((uint32_t)__popc(m2) << 16);
+            uint32_t prev = __shfl_up_sync(full, nb1, 1) >> 24;
+            if (lane == 0) prev = t ? (nz_nibble(Sw[8 * t - 2]) | (nz_nibble(Sw[8 * t - 1]) << 4)) : 0u;
+            const uint32_t m2 = nz_nibble(nb1 ^ ((nb1 << 8) | prev));
+            const uint32_t v12 = (uint32_t)__popc(nb1) | ((uint32_t)__popc(m2) << 16);
             const uint32_t inc12 = warp_incl_scan(v12);
             if (lane == 31) s_l1[warp] = inc12;
-            bm2[t] = (uint8_t)m2;
+            {   // bm2 byte t/2 = bm2 bits of bm1 bytes 8(t/2)..: two lanes per byte
+                const uint32_t pair = m2 | (__shfl_down_sync(full, m2, 1) << 4);
+                if (!(lane & 1u)) bm2[t >> 1] = (uint8_t)pair;
+            }
             __syncthreads();  // B3
-            uint32_t tot12 = 0, pre12 = inc12 - v12;
+            uint32_t tot12, pre12 = inc12 - v12;
+            {   // warp totals: lane l scans warps 0..l
+                const uint32_t v = lane < kTT / 32 ? s_l1[lane] : 0u;
+                uint32_t iv = v;
 #pragma unroll
-            for (int w8 = 0; w8 < 8; w8++) {
-                const uint32_t v = s_l1[w8];
-                tot12 += v;
-                if ((uint32_t)w8 < warp) pre12 += v;
+                for (int d = 1; d < kTT / 32; d <<= 1) {
+                    const uint32_t n = __shfl_up_sync(full, iv, d);
+                    if (lane >= (uint32_t)d) iv += n;
+                }
+                pre12 += __shfl_sync(full, iv - v, warp);
+                tot12 = __shfl_sync(full, iv, kTT / 32 - 1);
             }
             const uint32_t nzT = tot12 & 0xffffu, n2T = tot12 >> 16;
 
             if (om) {  // outlier records, ascending index within the chunk
                 uint32_t pos = s_misc[1] + oex;
                 for (uint32_t w8 = 0; w8 < warp; w8++) pos += s_wout[w8];
-                const uint32_t kb = c * (uint32_t)kChunkCodes + 32u * t;
+                const uint32_t kb = c * (uint32_t)kChunkCodes + 16u * t;
                 uint32_t m = om;
                 while (m) {
                     const uint32_t e = __ffs(m) - 1;
                     m &= m - 1;
                     if (pos < a.ostage_cap) {
-                        a.ostage_err[pos] = delta_at(stg, t, tu, ty, e);
+                        a.ostage_err[pos] = delta_at16(stg, t, tu, ty, e);
                         a.ostage_idx[pos] = kb + e;
                     }
                     pos++;
@@ -359,32 +391,16 @@ __global__ void __launch_bounds__(kThreads, 2)
             const uint32_t wpos = nzT + n2T;
             if (mode == 0 && (wpos >= (uint32_t)kRzeAvail || wpos > (uint32_t)(kRzeAvail - 256))) mode = 2;
             if (mode == 0) {
-                // level-1 payload: the nonzero bytes of the 16 words, compacted
+                // level-1 payload: the nonzero bytes of the 8 words, compacted
                 uint32_t pos = pre12 & 0xffffu;
 #pragma unroll
-                for (int i = 0; i < 16; i++) {
-                    const uint32_t nb = ((i < 8 ? nlo : nhi) >> (4 * (i & 7))) & 15u;
-                    if (nb) {
-                        const uint32_t packed = __byte_perm(w[i], 0u, s_sel[nb]);
-                        const uint32_t sh = (pos & 3u) * 8u;
-                        atomicOr(&Ow[pos >> 2], packed << sh);
-                        atomicOr(&Ow[(pos >> 2) + 1], __funnelshift_l(packed, 0u, sh));
-                    }
+                for (int i = 0; i < 8; i++) {
+                    const uint32_t nb = (nb1 >> (4 * i)) & 15u;
+                    if (nb) or_bytes_at(Ow, pos, __byte_perm(w[i], 0u, s_sel[nb]));
                     pos += __popc(nb);
                 }
                 // level-2 payload: the non-repeated bm1 bytes
-                uint32_t q = nzT + (pre12 >> 16);
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const uint32_t mb = (m2 >> (4 * h)) & 15u;
-                    if (mb) {
-                        const uint32_t packed = __byte_perm(h ? nhi : nlo, 0u, s_sel[mb]);
-                        const uint32_t sh = (q & 3u) * 8u;
-                        atomicOr(&Ow[q >> 2], packed << sh);
-                        atomicOr(&Ow[(q >> 2) + 1], __funnelshift_l(packed, 0u, sh));
-                    }
-                    q += __popc(mb);
-                }
+                if (m2) or_bytes_at(Ow, nzT + (pre12 >> 16), __byte_perm(nb1, 0u, s_sel[m2]));
             }
             __syncthreads();  // B4
 
@@ -392,9 +408,9 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (mode == 0 && warp == 0) {
                 const uint2 mw = reinterpret_cast<const uint2*>(bm2)[lane];
                 const uint64_t M3 = ((uint64_t)mw.y << 32) | mw.x;
-                uint32_t prev = __shfl_up_sync(full, mw.y, 1) >> 24;
-                if (lane == 0) prev = 0;
-                const uint32_t m3 = nz_byte_mask64(M3 ^ ((M3 << 8) | prev));  // bm3 byte `lane`
+                uint32_t p3 = __shfl_up_sync(full, mw.y, 1) >> 24;
+                if (lane == 0) p3 = 0;
+                const uint32_t m3 = nz_byte_mask64(M3 ^ ((M3 << 8) | p3));  // bm3 byte `lane`
                 const uint32_t n3 = __popc(m3), inc = warp_incl_scan(n3);
                 const uint32_t n3T = __shfl_sync(full, inc, 31);
                 {
@@ -441,30 +457,14 @@ __global__ void __launch_bounds__(kThreads, 2)
             __syncthreads();  // B5
 
             const uint32_t sw = s_misc[2];
-            uint8_t* slot = a.slots + (size_t)c * kChunkBytes;
-            if (sw >> 31) {
-                // stored raw: the shuffled chunk, recomputed from the exchange buffer
-                float Bs[32];
-#pragma unroll
-                for (int g = 0; g < 8; g++) {
-                    const float4 v = *reinterpret_cast<const float4*>(stg + swz_off(t, g));
-                    Bs[4 * g] = v.x;
-                    Bs[4 * g + 1] = v.y;
-                    Bs[4 * g + 2] = v.z;
-                    Bs[4 * g + 3] = v.w;
-                }
-                uint32_t xr[16], o8;
-                make_codes<ZZ>(Bs, stg, tu, ty, rad, xr, o8);
-                transpose16x2(xr);
-                uint32_t* sl = reinterpret_cast<uint32_t*>(slot);
-#pragma unroll
-                for (int b = 0; b < 16; b++) sl[(15 - b) * 256 + t] = xr[b] & ~om;
-                for (uint32_t i = t; i < (uint32_t)kOBytes / 16; i += kThreads)
-                    reinterpret_cast<uint4*>(O)[i] = make_uint4(0u, 0u, 0u, 0u);
+            uint4* d4 = reinterpret_cast<uint4*>(a.slots + (size_t)c * kChunkBytes);
+            uint4* o4 = reinterpret_cast<uint4*>(O);
+            if (sw >> 31) {  // stored raw: the shuffled chunk itself
+                const uint4* s4 = reinterpret_cast<const uint4*>(Sbuf);
+                for (uint32_t i = t; i < (uint32_t)kChunkBytes / 16; i += kTT) d4[i] = s4[i];
+                for (uint32_t i = t; i < (uint32_t)kOBytes / 16; i += kTT) o4[i] = make_uint4(0u, 0u, 0u, 0u);
             } else {
-                uint4* d4 = reinterpret_cast<uint4*>(slot);
-                uint4* o4 = reinterpret_cast<uint4*>(O);
-                for (uint32_t i = t; i < (sw + 15) / 16; i += kThreads) {
+                for (uint32_t i = t; i < (sw + 15) / 16; i += kTT) {
                     d4[i] = o4[i];
                     o4[i] = make_uint4(0u, 0u, 0u, 0u);
                 }
@@ -517,11 +517,11 @@ int launch_lq3d_tma(const FwdArgs& a, unsigned grid, cudaStream_t s) {
     if (a.zigzag) {
         e = cudaFuncSetAttribute(lq3d_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem);
         if (e != cudaSuccess) return (int)e;
-        lq3d_tma_kernel<true><<<grid, kThreads, kSlabSmem, s>>>(a, map, slabs, units);
+        lq3d_tma_kernel<true><<<grid, kTT, kSlabSmem, s>>>(a, map, slabs, units);
     } else {
         e = cudaFuncSetAttribute(lq3d_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem);
         if (e != cudaSuccess) return (int)e;
-        lq3d_tma_kernel<false><<<grid, kThreads, kSlabSmem, s>>>(a, map, slabs, units);
+        lq3d_tma_kernel<false><<<grid, kTT, kSlabSmem, s>>>(a, map, slabs, units);
     }
     return (int)cudaGetLastError();
 }
