@@ -50,17 +50,6 @@ __device__ __forceinline__ float bin_entropy(float p) {
 }
 
 // Block-wide float sum (256 threads), fixed reduction order.
-__device__ __forceinline__ float block_sum(float v, float* red) {
-#pragma unroll
-    for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    float s = 0.0f;
-#pragma unroll
-    for (int w = 0; w < 8; w++) s += red[w];
-    __syncthreads();
-    return s;
-}
 
 __device__ __forceinline__ uint32_t block_max_u32(uint32_t v, uint32_t* red) {
 #pragma unroll
@@ -77,90 +66,215 @@ __device__ __forceinline__ uint32_t block_max_u32(uint32_t v, uint32_t* red) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Features: 16 statistics per chunk (CTA per chunk, 128 codes per thread).
+// Features: 16 statistics per chunk (CTA per chunk).  Thread t takes the
+// 8-code groups t, t+256, ... with 16-byte loads; counts are exact integers
+// (packed zero / zero-byte tests, nibble-field bit-plane counters); one
+// 1024-bin histogram (lane-private bins for codes < 16, where nearly all
+// codes fall, shared bins above) gives the low- and high-byte histograms
+// with two side tables for the rare codes >= 256 and >= 1024.
 // ---------------------------------------------------------------------------
+// Block-wide sums of K values per thread (256 threads, K <= 24), in place;
+// two barriers for all K.
+template <int K>
+__device__ __forceinline__ void block_sum_n(float (&v)[K], float* red) {
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], d);
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < K; k++) red[(threadIdx.x >> 5) * 24 + k] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        float s = 0.0f;
+#pragma unroll
+        for (int w = 0; w < 8; w++) s += red[w * 24 + k];
+        v[k] = s;
+    }
+    __syncthreads();
+}
+
+struct FeatAcc {
+    float s1 = 0, s2 = 0, sd = 0;
+    uint32_t zero = 0, nzbytes = 0, same = 0, nzb = 0, vmax = 0;
+    uint32_t bE[4] = {0, 0, 0, 0}, bO[4] = {0, 0, 0, 0};  // bit-plane counts in byte fields
+};
+
+__device__ __forceinline__ void feat_hist(uint32_t u, uint32_t* h1024, uint32_t* priv, uint32_t* hlo_x,
+                                          uint32_t* hhi_x) {
+    atomicAdd(u < 16 ? priv + 32 * u : h1024 + min(u, 1023u), 1u);
+    if (u >= 256) atomicAdd(hlo_x + (u & 0xffu), 1u);
+    if (u >= 1024) atomicAdd(hhi_x + (u >> 8), 1u);
+}
+
+// One code u with predecessor pv (has_prev: i > 0), scalar path (partial groups).
+__device__ __forceinline__ void feat_code(FeatAcc& f, uint32_t u, uint32_t pv, bool has_prev) {
+    const float lg = __log2f(1.0f + (float)u);
+    f.s1 += lg;
+    f.s2 += lg * lg;
+    f.zero += (u == 0);
+    f.nzbytes += ((u & 0xffu) != 0) + ((u >> 8) != 0);
+    f.vmax = max(f.vmax, u);
+    if (has_prev) {
+        f.same += (u == pv);
+        f.sd += __log2f(1.0f + (float)(u > pv ? u - pv : pv - u));
+    }
+}
+
 __global__ void __launch_bounds__(256) sel_features_kernel(const uint16_t* __restrict__ codes, uint64_t n,
                                                            float* __restrict__ feats) {
     __shared__ uint32_t h1024[1024];
-    __shared__ uint32_t hlo[256], hhi[256];
-    __shared__ float red[8];
+    __shared__ uint32_t hlo_x[256], hhi_x[256];
+    __shared__ uint32_t priv[8 * 16 * 32];  // [warp][bin][lane]
+    __shared__ float redn[8 * 24];
     __shared__ uint32_t ured[8];
-    const uint32_t c = blockIdx.x, t = threadIdx.x;
+    const uint32_t c = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t cnt = chunk_count(n, c);
     const uint16_t* src = codes + (uint64_t)c * kSelCodes;
     for (uint32_t i = t; i < 1024; i += 256) h1024[i] = 0;
-    hlo[t] = 0;
-    hhi[t] = 0;
-    __syncthreads();
-    float s1 = 0, s2 = 0, sd = 0, zero = 0, zbyte = 0, same = 0, nzb = 0, big = 0;
-    uint32_t bits[16] = {0}, vmax = 0, gor = 0;
-    const uint32_t b0 = 128 * t;
-    uint32_t prev = (b0 > 0 && b0 - 1 < cnt) ? src[b0 - 1] : 0xffffffffu;
-    for (uint32_t k = 0; k < 128; k++) {
-        const uint32_t i = b0 + k;
-        if (i >= cnt) break;
-        const uint32_t u = src[i];
-        const float lg = __log2f(1.0f + (float)u);
-        s1 += lg;
-        s2 += lg * lg;
-        zero += (u == 0);
-        zbyte += ((u & 0xff) == 0) + ((u >> 8) == 0);
-        // bit-plane bytes of 8 consecutive codes (the Bitshuffle layout):
-        // nonzero iff any of the 8 codes has that bit set
-        gor |= u;
-        if ((k & 7) == 7 || i + 1 == cnt) {
-            nzb += (float)__popc(gor);
-            gor = 0;
-        }
-        big += (u >= 1024);
-        vmax = max(vmax, u);
-        if (prev != 0xffffffffu) {
-            same += (u == prev);
-            const uint32_t d = u > prev ? u - prev : prev - u;
-            sd += __log2f(1.0f + (float)d);
-        }
-        prev = u;
+    hlo_x[t] = 0;
+    hhi_x[t] = 0;
+    uint32_t* mypriv = priv + warp * 512 + lane;
 #pragma unroll
-        for (int b = 0; b < 16; b++) bits[b] += (u >> b) & 1u;
-        atomicAdd(&h1024[min(u, 1023u)], 1u);
-        atomicAdd(&hlo[u & 0xff], 1u);
-        atomicAdd(&hhi[u >> 8], 1u);
+    for (int b = 0; b < 16; b++) mypriv[32 * b] = 0;
+    __syncthreads();
+    FeatAcc f;
+    const bool vec = (reinterpret_cast<uintptr_t>(src) & 15u) == 0;
+    for (uint32_t g = t; 8 * g < cnt; g += 256) {
+        const uint32_t i0 = 8 * g;
+        uint32_t pv = i0 ? src[i0 - 1] : 0u;
+        if (vec && i0 + 8 <= cnt) {
+            const uint4 q = *reinterpret_cast<const uint4*>(src + i0);
+            const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+            uint32_t acc[4] = {0, 0, 0, 0}, o = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t x = w[k];
+                o |= x;
+                const uint32_t nzh = (((x & 0x7fff7fffu) + 0x7fff7fffu) | x) & 0x80008000u;  // nonzero halves
+                f.zero += 2 - __popc(nzh);
+                f.nzbytes += __popc((((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x) & 0x80808080u);
+                f.vmax = max(f.vmax, max(x & 0xffffu, x >> 16));
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[j] += (x >> j) & 0x11111111u;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const uint32_t u = h ? x >> 16 : x & 0xffffu;
+                    const float lg = __log2f(1.0f + (float)u);
+                    f.s1 += lg;
+                    f.s2 += lg * lg;
+                    if (i0 + 2 * k + h > 0) {
+                        f.same += (u == pv);
+                        f.sd += __log2f(1.0f + (float)(u > pv ? u - pv : pv - u));
+                    }
+                    pv = u;
+                    feat_hist(u, h1024, mypriv, hlo_x, hhi_x);
+                }
+            }
+            f.nzb += __popc((o | (o >> 16)) & 0xffffu);  // nonzero bit-plane bytes of the 8 codes
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                f.bE[j] += acc[j] & 0x0f0f0f0fu;
+                f.bO[j] += (acc[j] >> 4) & 0x0f0f0f0fu;
+            }
+        } else {  // partial group (or unaligned codes): code by code
+            uint32_t o = 0;
+            for (uint32_t k = 0; k < 8 && i0 + k < cnt; k++) {
+                const uint32_t u = src[i0 + k];
+                feat_code(f, u, pv, i0 + k > 0);
+                pv = u;
+                o |= u;
+                feat_hist(u, h1024, mypriv, hlo_x, hhi_x);
+                const uint32_t x = u << (16 * (k & 1));  // counts by the packed-word layout below
+                uint32_t acc[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[j] = (x >> j) & 0x11111111u;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    f.bE[j] += acc[j] & 0x0f0f0f0fu;
+                    f.bO[j] += (acc[j] >> 4) & 0x0f0f0f0fu;
+                }
+            }
+            f.nzb += __popc(o & 0xffffu);
+        }
+    }
+    // lane-private bins -> h1024[0..15]
+#pragma unroll
+    for (int b = 0; b < 16; b++) {
+        const uint32_t v = __reduce_add_sync(0xffffffffu, mypriv[32 * b]);
+        if (lane == 0 && v) atomicAdd(h1024 + b, v);
     }
     const float fn = (float)max(cnt, 1u);
-    const float m1 = block_sum(s1, red) / fn;
-    const float m2 = block_sum(s2, red) / fn;
-    float f[16];
-    f[0] = m1 / 16.0f;
-    f[1] = sqrtf(fmaxf(m2 - m1 * m1, 0.0f)) / 8.0f;
-    f[2] = block_sum(zero, red) / fn;
-    f[3] = 1.0f - block_sum(same, red) / fn;  // runs per code
-    f[4] = block_sum(zbyte, red) / (2.0f * fn);
-    f[5] = block_sum(sd, red) / fn / 16.0f;
-    float hb[4] = {0, 0, 0, 0};
-    for (int b = 0; b < 16; b++) hb[b >> 2] += bin_entropy(block_sum((float)bits[b], red) / fn) * 0.25f;
-    f[6] = hb[0];
-    f[7] = hb[1];
-    f[8] = hb[2];
-    f[9] = hb[3];
-    f[10] = __log2f(1.0f + (float)block_max_u32(vmax, ured)) / 16.0f;
-    __syncthreads();
-    // histogram entropies
-    const float plo = hlo[t] / fn, phi = hhi[t] / fn;
-    f[11] = block_sum(plo > 0 ? -plo * __log2f(plo) : 0.0f, red) / 8.0f;
-    f[12] = block_sum(phi > 0 ? -phi * __log2f(phi) : 0.0f, red) / 8.0f;
-    f[13] = block_sum(big, red) > 0.0f ? 1.0f : 0.0f;  // Huffman (bklen 1024) not applicable
-    f[14] = block_sum(nzb, red) / (2.0f * fn);
-    float e = 0;
-    for (uint32_t i = t; i < 1024; i += 256) {
-        const float p = h1024[i] / fn;
-        if (p > 0) e -= p * __log2f(p);
+    // round 1: per-thread statistics (the barrier also completes the histogram)
+    float r1[23];
+    r1[0] = f.s1;
+    r1[1] = f.s2;
+    r1[2] = (float)f.zero;
+    r1[3] = (float)f.same;
+    r1[4] = (float)f.nzbytes;
+    r1[5] = f.sd;
+    r1[6] = (float)f.nzb;
+#pragma unroll
+    for (int b = 0; b < 16; b++) {  // bit b = 4q + j: nibble q (low code of a word) or q + 4 (high code) of acc[j]
+        const int q = b >> 2, j = b & 3;
+        auto nib = [&](int qq) { return (float)(((qq & 1 ? f.bO[j] : f.bE[j]) >> (8 * (qq >> 1))) & 0xffu); };
+        r1[7 + b] = nib(q) + nib(q + 4);
     }
-    f[15] = block_sum(e, red) / 10.0f;
+    block_sum_n(r1, redn);
+    const uint32_t vmax = block_max_u32(f.vmax, ured);
+    const float m1 = r1[0] / fn, m2 = r1[1] / fn;
+    float out[16];
+    out[0] = m1 / 16.0f;
+    out[1] = sqrtf(fmaxf(m2 - m1 * m1, 0.0f)) / 8.0f;
+    out[2] = r1[2] / fn;
+    out[3] = 1.0f - r1[3] / fn;  // runs per code
+    out[4] = (2.0f * fn - r1[4]) / (2.0f * fn);
+    out[5] = r1[5] / fn / 16.0f;
+    float hb[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int b = 0; b < 16; b++) hb[b >> 2] += bin_entropy(r1[7 + b] / fn) * 0.25f;
+    out[6] = hb[0];
+    out[7] = hb[1];
+    out[8] = hb[2];
+    out[9] = hb[3];
+    out[10] = __log2f(1.0f + (float)vmax) / 16.0f;
+    out[13] = vmax >= 1024 ? 1.0f : 0.0f;  // Huffman (bklen 1024) not applicable
+    out[14] = r1[6] / (2.0f * fn);
+    // round 2: low-byte entropy (h1024[b] + rare codes' low bytes), 1024-bin
+    // entropy, the count of codes >= 1024 and the quarter sums of h1024
+    float r2[7];
+    {
+        const float pl = (h1024[t] + hlo_x[t]) / fn;
+        r2[0] = pl > 0 ? -pl * __log2f(pl) : 0.0f;
+        float e = 0;
+        for (uint32_t i = t; i < 1024; i += 256) {
+            const float p = h1024[i] / fn;
+            if (p > 0) e -= p * __log2f(p);
+        }
+        r2[1] = e;
+        r2[2] = (float)hhi_x[t];
+#pragma unroll
+        for (int qq = 0; qq < 4; qq++) r2[3 + qq] = (float)h1024[256 * qq + t];
+    }
+    block_sum_n(r2, redn);
+    out[11] = r2[0] / 8.0f;
+    out[15] = r2[1] / 10.0f;
+    // round 3: high-byte entropy; bins 0..3 = quarters of h1024 less the codes
+    // >= 1024 folded into its last bin
+    float r3[1];
+    {
+        const float qv = t == 0 ? r2[3] : t == 1 ? r2[4] : t == 2 ? r2[5] : r2[6] - r2[2];
+        const float ph = (t < 4 ? qv : (float)hhi_x[t]) / fn;
+        r3[0] = ph > 0 ? -ph * __log2f(ph) : 0.0f;
+    }
+    block_sum_n(r3, redn);
+    out[12] = r3[0] / 8.0f;
     if (t < 16) {
         float v = 0;
 #pragma unroll
         for (int k = 0; k < 16; k++)
-            if (k == (int)t) v = f[k];
+            if (k == (int)t) v = out[k];
         feats[(uint64_t)c * kSelFeat + t] = v;
     }
 }

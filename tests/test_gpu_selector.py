@@ -89,6 +89,16 @@ def test_features_match_oracle(cuda):
     np.testing.assert_allclose(f, S.features(c), rtol=1e-4, atol=2e-5)
 
 
+def test_features_ragged_and_unaligned(cuda):
+    # a length that is not a multiple of 8 codes, and a view 2 bytes off the
+    # 16-byte boundary (the scalar path of the features kernel)
+    c = _codes()
+    dev = torch.from_numpy(c).to(cuda)
+    for lo, hi in ((0, 32768 + 13), (1, 1 + 2 * 32768 + 5)):
+        f = Sel().features(dev[lo:hi]).cpu().numpy()
+        np.testing.assert_allclose(f, S.features(c[lo:hi]), rtol=1e-4, atol=2e-5)
+
+
 def test_mlp_forward_and_gradient_match_oracle(cuda):
     rng = np.random.default_rng(4)
     sel = Sel().CoderSelector(seed=3, device=cuda)
