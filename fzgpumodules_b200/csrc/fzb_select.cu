@@ -66,14 +66,16 @@ __device__ __forceinline__ uint32_t block_max_u32(uint32_t v, uint32_t* red) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Features: 16 statistics per chunk (CTA per chunk).  Thread t takes the
-// 8-code groups t, t+256, ... with 16-byte loads; counts are exact integers
-// (packed zero / zero-byte tests, nibble-field bit-plane counters); one
-// 1024-bin histogram (lane-private bins for codes < 16, where nearly all
-// codes fall, shared bins above) gives the low- and high-byte histograms
-// with two side tables for the rare codes >= 256 and >= 1024.
+// Features: 16 statistics per chunk (CTA per chunk).  Per code the kernel only
+// histograms the code (1024 bins of min(code, 1023): lane-private bins for
+// codes < 16, where nearly all codes fall, shared bins above), compares it
+// with its predecessor and ORs it into its 8-code group; everything that is a
+// function of the code alone (log moments, zero codes, zero bytes, bit-plane
+// counts, the maximum, both byte histograms) is then summed over the bins,
+// with the rare codes >= 1023 handled one by one.  Thread t takes the 8-code
+// groups t, t+256, ... with 16-byte loads.
 // ---------------------------------------------------------------------------
-// Block-wide sums of K values per thread (256 threads, K <= 24), in place;
+// Block-wide sums of K values per thread (256 threads, K <= 32), in place;
 // two barriers for all K.
 template <int K>
 __device__ __forceinline__ void block_sum_n(float (&v)[K], float* red) {
@@ -83,51 +85,52 @@ __device__ __forceinline__ void block_sum_n(float (&v)[K], float* red) {
         for (int d = 16; d >= 1; d >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], d);
     if ((threadIdx.x & 31) == 0)
 #pragma unroll
-        for (int k = 0; k < K; k++) red[(threadIdx.x >> 5) * 24 + k] = v[k];
+        for (int k = 0; k < K; k++) red[(threadIdx.x >> 5) * 32 + k] = v[k];
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < K; k++) {
         float s = 0.0f;
 #pragma unroll
-        for (int w = 0; w < 8; w++) s += red[w * 24 + k];
+        for (int w = 0; w < 8; w++) s += red[w * 32 + k];
         v[k] = s;
     }
     __syncthreads();
 }
 
 struct FeatAcc {
-    float s1 = 0, s2 = 0, sd = 0;
-    uint32_t zero = 0, nzbytes = 0, same = 0, nzb = 0, vmax = 0;
-    uint32_t bE[4] = {0, 0, 0, 0}, bO[4] = {0, 0, 0, 0};  // bit-plane counts in byte fields
+    float sd = 0;                      // sum of log2(1 + |delta|)
+    uint32_t same = 0, nzb = 0;        // equal neighbours, nonzero bit-plane bytes
+    float s1 = 0, s2 = 0;              // codes >= 1023: log moments
+    uint32_t vmax = 0, bits[16] = {};  // codes >= 1023: maximum, bit counts
 };
 
-__device__ __forceinline__ void feat_hist(uint32_t u, uint32_t* h1024, uint32_t* priv, uint32_t* hlo_x,
-                                          uint32_t* hhi_x) {
+__device__ __forceinline__ void feat_code(FeatAcc& f, uint32_t u, uint32_t pv, bool has_prev, uint32_t* h1024,
+                                          uint32_t* priv, uint32_t* hlo_x, uint32_t* hhi_x) {
     atomicAdd(u < 16 ? priv + 32 * u : h1024 + min(u, 1023u), 1u);
-    if (u >= 256) atomicAdd(hlo_x + (u & 0xffu), 1u);
-    if (u >= 1024) atomicAdd(hhi_x + (u >> 8), 1u);
-}
-
-// One code u with predecessor pv (has_prev: i > 0), scalar path (partial groups).
-__device__ __forceinline__ void feat_code(FeatAcc& f, uint32_t u, uint32_t pv, bool has_prev) {
-    const float lg = __log2f(1.0f + (float)u);
-    f.s1 += lg;
-    f.s2 += lg * lg;
-    f.zero += (u == 0);
-    f.nzbytes += ((u & 0xffu) != 0) + ((u >> 8) != 0);
-    f.vmax = max(f.vmax, u);
     if (has_prev) {
         f.same += (u == pv);
         f.sd += __log2f(1.0f + (float)(u > pv ? u - pv : pv - u));
+    }
+    if (u >= 1023) {  // rare: the bin holds every code >= 1023
+        const float lg = __log2f(1.0f + (float)u);
+        f.s1 += lg;
+        f.s2 += lg * lg;
+        f.vmax = max(f.vmax, u);
+#pragma unroll
+        for (int b = 0; b < 16; b++) f.bits[b] += (u >> b) & 1u;
+        atomicAdd(hlo_x + (u & 0xffu), 1u);
+        if (u >= 1024) atomicAdd(hhi_x + (u >> 8), 1u);
+    } else if (u >= 256) {
+        atomicAdd(hlo_x + (u & 0xffu), 1u);
     }
 }
 
 __global__ void __launch_bounds__(256) sel_features_kernel(const uint16_t* __restrict__ codes, uint64_t n,
                                                            float* __restrict__ feats) {
     __shared__ uint32_t h1024[1024];
-    __shared__ uint32_t hlo_x[256], hhi_x[256];
-    __shared__ uint32_t priv[8 * 16 * 32];  // [warp][bin][lane]
-    __shared__ float redn[8 * 24];
+    __shared__ uint32_t hlo_x[256], hhi_x[256];  // low bytes of codes >= 256, high bytes of codes >= 1024
+    __shared__ uint32_t priv[8 * 16 * 32];     // [warp][bin][lane]
+    __shared__ float redn[8 * 32];
     __shared__ uint32_t ured[8];
     const uint32_t c = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t cnt = chunk_count(n, c);
@@ -144,60 +147,30 @@ __global__ void __launch_bounds__(256) sel_features_kernel(const uint16_t* __res
     for (uint32_t g = t; 8 * g < cnt; g += 256) {
         const uint32_t i0 = 8 * g;
         uint32_t pv = i0 ? src[i0 - 1] : 0u;
+        uint32_t o = 0;
         if (vec && i0 + 8 <= cnt) {
             const uint4 q = *reinterpret_cast<const uint4*>(src + i0);
             const uint32_t w[4] = {q.x, q.y, q.z, q.w};
-            uint32_t acc[4] = {0, 0, 0, 0}, o = 0;
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                const uint32_t x = w[k];
-                o |= x;
-                const uint32_t nzh = (((x & 0x7fff7fffu) + 0x7fff7fffu) | x) & 0x80008000u;  // nonzero halves
-                f.zero += 2 - __popc(nzh);
-                f.nzbytes += __popc((((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x) & 0x80808080u);
-                f.vmax = max(f.vmax, max(x & 0xffffu, x >> 16));
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[j] += (x >> j) & 0x11111111u;
+                o |= w[k];
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
-                    const uint32_t u = h ? x >> 16 : x & 0xffffu;
-                    const float lg = __log2f(1.0f + (float)u);
-                    f.s1 += lg;
-                    f.s2 += lg * lg;
-                    if (i0 + 2 * k + h > 0) {
-                        f.same += (u == pv);
-                        f.sd += __log2f(1.0f + (float)(u > pv ? u - pv : pv - u));
-                    }
+                    const uint32_t u = h ? w[k] >> 16 : w[k] & 0xffffu;
+                    feat_code(f, u, pv, i0 + 2 * k + h > 0, h1024, mypriv, hlo_x, hhi_x);
                     pv = u;
-                    feat_hist(u, h1024, mypriv, hlo_x, hhi_x);
                 }
             }
-            f.nzb += __popc((o | (o >> 16)) & 0xffffu);  // nonzero bit-plane bytes of the 8 codes
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                f.bE[j] += acc[j] & 0x0f0f0f0fu;
-                f.bO[j] += (acc[j] >> 4) & 0x0f0f0f0fu;
-            }
+            o |= o >> 16;
         } else {  // partial group (or unaligned codes): code by code
-            uint32_t o = 0;
             for (uint32_t k = 0; k < 8 && i0 + k < cnt; k++) {
                 const uint32_t u = src[i0 + k];
-                feat_code(f, u, pv, i0 + k > 0);
+                feat_code(f, u, pv, i0 + k > 0, h1024, mypriv, hlo_x, hhi_x);
                 pv = u;
                 o |= u;
-                feat_hist(u, h1024, mypriv, hlo_x, hhi_x);
-                const uint32_t x = u << (16 * (k & 1));  // counts by the packed-word layout below
-                uint32_t acc[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[j] = (x >> j) & 0x11111111u;
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    f.bE[j] += acc[j] & 0x0f0f0f0fu;
-                    f.bO[j] += (acc[j] >> 4) & 0x0f0f0f0fu;
-                }
             }
-            f.nzb += __popc(o & 0xffffu);
         }
+        f.nzb += __popc(o & 0xffffu);  // nonzero bit-plane bytes of the 8 codes
     }
     // lane-private bins -> h1024[0..15]
 #pragma unroll
@@ -205,66 +178,70 @@ __global__ void __launch_bounds__(256) sel_features_kernel(const uint16_t* __res
         const uint32_t v = __reduce_add_sync(0xffffffffu, mypriv[32 * b]);
         if (lane == 0 && v) atomicAdd(h1024 + b, v);
     }
+    __syncthreads();  // the histogram is complete
     const float fn = (float)max(cnt, 1u);
-    // round 1: per-thread statistics (the barrier also completes the histogram)
-    float r1[23];
+    // per-code sums plus the bins of this thread (t, t+256, t+512, t+768; bin
+    // 1023 holds every code >= 1023 and was summed code by code)
+    float r1[29];
     r1[0] = f.s1;
     r1[1] = f.s2;
-    r1[2] = (float)f.zero;
-    r1[3] = (float)f.same;
-    r1[4] = (float)f.nzbytes;
-    r1[5] = f.sd;
-    r1[6] = (float)f.nzb;
+    r1[2] = (float)f.same;
+    r1[3] = f.sd;
+    r1[4] = (float)f.nzb;
 #pragma unroll
-    for (int b = 0; b < 16; b++) {  // bit b = 4q + j: nibble q (low code of a word) or q + 4 (high code) of acc[j]
-        const int q = b >> 2, j = b & 3;
-        auto nib = [&](int qq) { return (float)(((qq & 1 ? f.bO[j] : f.bE[j]) >> (8 * (qq >> 1))) & 0xffu); };
-        r1[7 + b] = nib(q) + nib(q + 4);
+    for (int b = 0; b < 16; b++) r1[5 + b] = (float)f.bits[b];
+    uint32_t vmax = f.vmax;
+    float e1024 = 0;
+#pragma unroll
+    for (int qq = 0; qq < 4; qq++) {
+        const uint32_t bin = t + 256u * qq;
+        const uint32_t h = h1024[bin];
+        const float p = h / fn;
+        if (p > 0) e1024 -= p * __log2f(p);
+        r1[25 + qq] = (float)h;  // quarter sums of the histogram
+        if (h && bin < 1023) {
+            const float lg = __log2f(1.0f + (float)bin), fh = (float)h;
+            r1[0] += fh * lg;
+            r1[1] += fh * lg * lg;
+            vmax = max(vmax, bin);
+#pragma unroll
+            for (int b = 0; b < 10; b++)
+                if ((bin >> b) & 1u) r1[5 + b] += fh;
+        }
     }
+    const float pl = (h1024[t] + hlo_x[t]) / fn;  // low byte b: codes equal to b plus codes >= 256
+    r1[21] = pl > 0 ? -pl * __log2f(pl) : 0.0f;
+    r1[22] = e1024;
+    r1[23] = (float)hhi_x[t];                     // codes >= 1024
+    r1[24] = (float)hlo_x[0] * (t == 0);          // codes >= 256 with a zero low byte
     block_sum_n(r1, redn);
-    const uint32_t vmax = block_max_u32(f.vmax, ured);
+    vmax = block_max_u32(vmax, ured);
     const float m1 = r1[0] / fn, m2 = r1[1] / fn;
     float out[16];
     out[0] = m1 / 16.0f;
     out[1] = sqrtf(fmaxf(m2 - m1 * m1, 0.0f)) / 8.0f;
-    out[2] = r1[2] / fn;
-    out[3] = 1.0f - r1[3] / fn;  // runs per code
-    out[4] = (2.0f * fn - r1[4]) / (2.0f * fn);
-    out[5] = r1[5] / fn / 16.0f;
+    out[2] = (float)h1024[0] / fn;
+    out[3] = 1.0f - r1[2] / fn;  // runs per code
+    // zero low bytes: codes 0 and codes >= 256 with a zero low byte; zero high bytes: codes < 256
+    out[4] = ((float)h1024[0] + r1[24] + r1[25]) / (2.0f * fn);
+    out[5] = r1[3] / fn / 16.0f;
     float hb[4] = {0, 0, 0, 0};
 #pragma unroll
-    for (int b = 0; b < 16; b++) hb[b >> 2] += bin_entropy(r1[7 + b] / fn) * 0.25f;
+    for (int b = 0; b < 16; b++) hb[b >> 2] += bin_entropy(r1[5 + b] / fn) * 0.25f;
     out[6] = hb[0];
     out[7] = hb[1];
     out[8] = hb[2];
     out[9] = hb[3];
     out[10] = __log2f(1.0f + (float)vmax) / 16.0f;
+    out[11] = r1[21] / 8.0f;
     out[13] = vmax >= 1024 ? 1.0f : 0.0f;  // Huffman (bklen 1024) not applicable
-    out[14] = r1[6] / (2.0f * fn);
-    // round 2: low-byte entropy (h1024[b] + rare codes' low bytes), 1024-bin
-    // entropy, the count of codes >= 1024 and the quarter sums of h1024
-    float r2[7];
-    {
-        const float pl = (h1024[t] + hlo_x[t]) / fn;
-        r2[0] = pl > 0 ? -pl * __log2f(pl) : 0.0f;
-        float e = 0;
-        for (uint32_t i = t; i < 1024; i += 256) {
-            const float p = h1024[i] / fn;
-            if (p > 0) e -= p * __log2f(p);
-        }
-        r2[1] = e;
-        r2[2] = (float)hhi_x[t];
-#pragma unroll
-        for (int qq = 0; qq < 4; qq++) r2[3 + qq] = (float)h1024[256 * qq + t];
-    }
-    block_sum_n(r2, redn);
-    out[11] = r2[0] / 8.0f;
-    out[15] = r2[1] / 10.0f;
-    // round 3: high-byte entropy; bins 0..3 = quarters of h1024 less the codes
-    // >= 1024 folded into its last bin
+    out[14] = r1[4] / (2.0f * fn);
+    out[15] = r1[22] / 10.0f;
+    // high-byte entropy: bins 0..3 = quarters of h1024 less the codes >= 1024
+    // folded into its last bin, bins >= 4 from the rare codes
     float r3[1];
     {
-        const float qv = t == 0 ? r2[3] : t == 1 ? r2[4] : t == 2 ? r2[5] : r2[6] - r2[2];
+        const float qv = t == 0 ? r1[25] : t == 1 ? r1[26] : t == 2 ? r1[27] : r1[28] - r1[23];
         const float ph = (t < 4 ? qv : (float)hhi_x[t]) / fn;
         r3[0] = ph > 0 ? -ph * __log2f(ph) : 0.0f;
     }
