@@ -9,12 +9,17 @@
 // its header size word carries bit 31.
 //
 // Work split: thread t owns input bytes [64t, 64t+64) (bm1 bytes 8t..8t+7 =
-// bm2 byte t); level 3 is one ballot per warp, level 4 one ballot in warp 0.
+// bm2 byte t); levels 3 and 4 run in warp 0.
 #pragma once
 
 #include "fzb_common.cuh"
 
 namespace fzb {
+
+// Compaction selectors: __byte_perm(w, 0, kRzeSel[m]) moves the bytes of w
+// flagged in the 4-bit mask m to the low end, in order, zero-filled.
+__constant__ static uint32_t kRzeSel[16] = {0x4444, 0x4440, 0x4441, 0x4410, 0x4442, 0x4420, 0x4421, 0x4210,
+                                            0x4443, 0x4430, 0x4431, 0x4310, 0x4432, 0x4320, 0x4321, 0x3210};
 
 struct RzeSmem {
     uint32_t* S;    // 4096 words: chunk bytes (zero past in_size)
@@ -28,20 +33,71 @@ struct RzeSmem {
 // Encodes the chunk held in sm.S (in_size bytes, rest zero).  Returns the
 // header size word (bit 31 = stored raw; then the payload is S itself).
 // Uniform across the block; ends with a barrier.
+//
+// Thread t takes S words 16t..16t+15 (bytes 64t..64t+63): their nonzero-byte
+// nibbles are bm1 bytes 8t..8t+7, so levels 1 and 2 need one packed warp scan
+// of both byte counts and one barrier for the per-warp totals.  Nonzero bytes
+// are compacted per word by a byte permute and OR-ed into the zeroed output
+// with two shared atomics (an output word can straddle two threads).  Levels
+// 3 and 4 run in warp 0.  Same bytes and raw decisions as rze_stage.cu:324-445.
 __device__ static uint32_t rze_encode_chunk(const RzeSmem& sm, int in_size) {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t full = 0xffffffffu;
     const uint32_t raw_word = 0x80000000u | (uint32_t)in_size;
-
+    const int b1 = (in_size + 7) >> 3, b2 = (b1 + 7) >> 3, b3 = (b2 + 7) >> 3;
+    uint32_t* Ow = reinterpret_cast<uint32_t*>(sm.O);
+    const uint32_t sel_tbl = kRzeSel[lane & 15];  // lane l holds selector l (read with a shuffle)
+    // output zeroed for the atomics: payloads stay below kRzeAvail, so the
+    // second word of an atomic pair stays below kChunkBytes + 4
+    for (int i = t; i < (kChunkBytes + 16) / 16; i += kThreads)
+        reinterpret_cast<uint4*>(sm.O)[i] = make_uint4(0u, 0u, 0u, 0u);
     uint32_t w[16];
-    uint64_t M = 0;
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        w[i] = sm.S[16 * t + i];
-        M |= (uint64_t)nz_nibble(w[i]) << (4 * i);
+    for (int i = 0; i < 4; i++) {
+        const uint4 q = reinterpret_cast<const uint4*>(sm.S)[4 * t + i];
+        w[4 * i] = q.x;
+        w[4 * i + 1] = q.y;
+        w[4 * i + 2] = q.z;
+        w[4 * i + 3] = q.w;
     }
-    uint32_t nzT;
-    uint32_t off1 = block_excl_scan((uint32_t)__popcll(M), sm.ws, &nzT);
-    if (nzT == 0) {
+    uint32_t nlo = 0, nhi = 0;
+    {
+        uint32_t o = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) o |= w[i];
+        if (__any_sync(full, o != 0u)) {
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const uint32_t hb = (((w[i] & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w[i]) & 0x80808080u;
+                const uint32_t nb = ((hb * 0x00204081u) >> (28 - 4 * (i & 7))) & (15u << (4 * (i & 7)));
+                if (i < 8) nlo |= nb;
+                else nhi |= nb;
+            }
+        }
+    }
+    // level 2: the bm1 bytes (< b1) that differ from their predecessor
+    uint32_t prev = __shfl_up_sync(full, nhi, 1) >> 24;
+    if (lane == 0) prev = t ? (nz_nibble(sm.S[16 * t - 2]) | (nz_nibble(sm.S[16 * t - 1]) << 4)) : 0u;
+    const uint64_t M = ((uint64_t)nhi << 32) | nlo;
+    uint32_t m2 = nz_byte_mask64(M ^ ((M << 8) | prev));
+    {
+        const int valid = b1 - 8 * t;
+        m2 &= (valid >= 8) ? 0xffu : (valid <= 0 ? 0u : ((1u << valid) - 1u));
+    }
+    const uint32_t v12 = (uint32_t)(__popc(nlo) + __popc(nhi)) | ((uint32_t)__popc(m2) << 16);
+    const uint32_t inc12 = warp_incl_scan(v12);
+    if (lane == 31) sm.ws[warp] = inc12;
+    sm.bm2[t] = (uint8_t)m2;
+    __syncthreads();
+    uint32_t tot12 = 0, pre12 = inc12 - v12;
+#pragma unroll
+    for (int w8 = 0; w8 < kThreads / 32; w8++) {
+        const uint32_t v = sm.ws[w8];
+        tot12 += v;
+        if (w8 < warp) pre12 += v;
+    }
+    const uint32_t nzT = tot12 & 0xffffu, n2T = tot12 >> 16;
+    if (nzT == 0) {  // all-zero chunk: the 2-byte size tag alone
         if (t == 0) {
             sm.O[0] = (uint8_t)(in_size & 0xff);
             sm.O[1] = (uint8_t)((in_size >> 8) & 0xff);
@@ -49,89 +105,87 @@ __device__ static uint32_t rze_encode_chunk(const RzeSmem& sm, int in_size) {
         __syncthreads();
         return 2u;
     }
-    const int b1 = (in_size + 7) >> 3;
-    if ((int)nzT >= kRzeAvail || (int)nzT > kRzeAvail - b1) return raw_word;
-
-    {   // level 1 payload: nonzero bytes in byte order
-        uint32_t pos = off1;
+    const uint32_t wpos = nzT + n2T;
+    if ((int)nzT >= kRzeAvail || (int)nzT > kRzeAvail - b1 || (int)wpos >= kRzeAvail ||
+        (int)wpos > kRzeAvail - b2) {
+        __syncthreads();
+        return raw_word;
+    }
+    {   // level-1 payload: nonzero bytes in byte order; level-2: non-repeated bm1 bytes
+        uint32_t pos = pre12 & 0xffffu;
 #pragma unroll
         for (int i = 0; i < 16; i++) {
-            uint32_t nib = (uint32_t)(M >> (4 * i)) & 15u;
-            const uint32_t wv = w[i];
-            while (nib) {
-                int b = __ffs(nib) - 1;
-                nib &= nib - 1;
-                sm.O[pos++] = (uint8_t)(wv >> (8 * b));
+            const uint32_t nb = ((i < 8 ? nlo : nhi) >> (4 * (i & 7))) & 15u;
+            const uint32_t sel = __shfl_sync(full, sel_tbl, nb);
+            if (nb) {
+                const uint32_t packed = __byte_perm(w[i], 0u, sel);
+                const uint32_t sh = (pos & 3u) * 8u;
+                atomicOr(&Ow[pos >> 2], packed << sh);
+                atomicOr(&Ow[(pos >> 2) + 1], __funnelshift_l(packed, 0u, sh));
+            }
+            pos += __popc(nb);
+        }
+        uint32_t q = nzT + (pre12 >> 16);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint32_t mb = (m2 >> (4 * h)) & 15u;
+            const uint32_t sel = __shfl_sync(full, sel_tbl, mb);
+            if (mb) {
+                const uint32_t packed = __byte_perm(h ? nhi : nlo, 0u, sel);
+                const uint32_t sh = (q & 3u) * 8u;
+                atomicOr(&Ow[q >> 2], packed << sh);
+                atomicOr(&Ow[(q >> 2) + 1], __funnelshift_l(packed, 0u, sh));
+            }
+            q += __popc(mb);
+        }
+    }
+    __syncthreads();
+    // levels 3 and 4 (warp 0), header
+    if (warp == 0) {
+        const uint2 mw = reinterpret_cast<const uint2*>(sm.bm2)[lane];
+        const uint64_t M3 = ((uint64_t)mw.y << 32) | mw.x;
+        uint32_t p3 = __shfl_up_sync(full, mw.y, 1) >> 24;
+        if (lane == 0) p3 = 0;
+        uint32_t m3 = nz_byte_mask64(M3 ^ ((M3 << 8) | p3));  // bm3 byte `lane`
+        {
+            const int valid = b2 - 8 * lane;
+            m3 &= (valid >= 8) ? 0xffu : (valid <= 0 ? 0u : ((1u << valid) - 1u));
+        }
+        const uint32_t n3 = __popc(m3), inc = warp_incl_scan(n3);
+        const uint32_t n3T = __shfl_sync(full, inc, 31);
+        {
+            uint32_t p = wpos + inc - n3, m = m3;
+            while (m) {
+                const uint32_t b = __ffs(m) - 1;
+                m &= m - 1;
+                sm.O[p++] = (uint8_t)(M3 >> (8 * b));
             }
         }
-    }
-    sm.bm1[2 * t] = (uint32_t)M;
-    sm.bm1[2 * t + 1] = (uint32_t)(M >> 32);
-    __syncthreads();
-
-    // level 2: RE of bm1 (b1 bytes); this thread's bytes are M
-    uint32_t m2;
-    {
-        uint32_t prev = (t > 0) ? (uint32_t)reinterpret_cast<const uint8_t*>(sm.bm1)[8 * t - 1] : 0u;
-        uint64_t diff = M ^ ((M << 8) | (uint64_t)prev);
-        m2 = nz_byte_mask64(diff);
-        int valid = b1 - 8 * t;
-        m2 &= (valid >= 8) ? 0xffu : (valid <= 0 ? 0u : ((1u << valid) - 1u));
-    }
-    uint32_t n2T;
-    uint32_t off2 = block_excl_scan((uint32_t)__popc(m2), sm.ws, &n2T);
-    int wpos = (int)(nzT + n2T);
-    if (wpos >= kRzeAvail) return raw_word;
-    {
-        uint32_t m = m2, pos = nzT + off2;
-        while (m) {
-            int b = __ffs(m) - 1;
-            m &= m - 1;
-            sm.O[pos++] = (uint8_t)(M >> (8 * b));
+        uint32_t pb = __shfl_up_sync(full, m3, 1);
+        if (lane == 0) pb = 0;
+        const bool nr4 = (lane < b3) && (m3 != pb);
+        const uint32_t bm4 = __ballot_sync(full, nr4);
+        uint32_t wp = wpos + n3T;
+        uint32_t sw = raw_word;
+        if (!((int)wp >= kRzeAvail || (int)wp >= kRzeAvail - 4 || (int)wp > (kRzeAvail - 4) - b3)) {
+            if (nr4) sm.O[wp + __popc(bm4 & ((1u << lane) - 1u))] = (uint8_t)m3;
+            wp += __popc(bm4);
+            if ((int)wp < kRzeAvail - 4) {
+                if (lane == 0) {
+                    sm.O[wp + 0] = (uint8_t)(bm4);
+                    sm.O[wp + 1] = (uint8_t)(bm4 >> 8);
+                    sm.O[wp + 2] = (uint8_t)(bm4 >> 16);
+                    sm.O[wp + 3] = (uint8_t)(bm4 >> 24);
+                    sm.O[wp + 4] = (uint8_t)(in_size & 0xff);
+                    sm.O[wp + 5] = (uint8_t)((in_size >> 8) & 0xff);
+                }
+                sw = wp + 6;
+            }
         }
-    }
-    sm.bm2[t] = (uint8_t)m2;
-    __syncthreads();
-
-    // level 3: RE of bm2 (b2 bytes); bm2 byte t is m2
-    const int b2 = (b1 + 7) >> 3;
-    if (wpos >= kRzeAvail || wpos > kRzeAvail - b2) return raw_word;
-    uint32_t p3 = (t > 0) ? (uint32_t)sm.bm2[t - 1] : 0u;
-    bool nr3 = (t < b2) && (m2 != p3);
-    uint32_t bal = __ballot_sync(0xffffffffu, nr3);
-    if (lane == 0) sm.bm3[warp] = bal;
-    uint32_t n3T;
-    uint32_t off3 = block_excl_scan(nr3 ? 1u : 0u, sm.ws, &n3T);  // has barriers
-    if (nr3) sm.O[wpos + off3] = (uint8_t)m2;
-    wpos += (int)n3T;
-    if (wpos >= kRzeAvail) return raw_word;
-
-    // level 4: RE of bm3 (b3 <= 32 bytes), bm4 stored raw
-    const int b3 = (b2 + 7) >> 3;
-    if (wpos >= kRzeAvail - 4 || wpos > (kRzeAvail - 4) - b3) return raw_word;
-    if (warp == 0) {
-        const uint8_t* b3p = reinterpret_cast<const uint8_t*>(sm.bm3);
-        uint32_t byte = b3p[lane];
-        uint32_t pb = lane ? (uint32_t)b3p[lane - 1] : 0u;
-        bool nr4 = (lane < b3) && (byte != pb);
-        uint32_t bm4 = __ballot_sync(0xffffffffu, nr4);
-        if (nr4) sm.O[wpos + __popc(bm4 & ((1u << lane) - 1u))] = (uint8_t)byte;
-        if (lane == 0) sm.ws[12] = bm4;
+        if (lane == 0) sm.ws[12] = sw;
     }
     __syncthreads();
-    const uint32_t bm4 = sm.ws[12];
-    wpos += __popc(bm4);
-    if (wpos >= kRzeAvail - 4) return raw_word;
-    if (t == 0) {
-        sm.O[wpos + 0] = (uint8_t)(bm4);
-        sm.O[wpos + 1] = (uint8_t)(bm4 >> 8);
-        sm.O[wpos + 2] = (uint8_t)(bm4 >> 16);
-        sm.O[wpos + 3] = (uint8_t)(bm4 >> 24);
-        sm.O[wpos + 4] = (uint8_t)(in_size & 0xff);
-        sm.O[wpos + 5] = (uint8_t)((in_size >> 8) & 0xff);
-    }
-    __syncthreads();
-    return (uint32_t)(wpos + 6);
+    return sm.ws[12];
 }
 
 // Copies `len` bytes from shared memory `src` to global `dst` (any byte

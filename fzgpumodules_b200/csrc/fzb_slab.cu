@@ -11,7 +11,7 @@
 //     swizzled shared buffer, two planes ahead of use (double buffer,
 //     mbarrier completion, bounded waits);
 //   * thread t owns chunk elements 32t..32t+31 (one 32-wide x segment of one
-//     row).  It quantizes them (packed f32x2 arithmetic), forms the z
+//     row).  It quantizes them (f32x2 adds, scalar products), forms the z
 //     difference against the previous plane's q held in registers and the x
 //     difference in registers, writes B = (z, x)-differenced values back over
 //     its own bytes of the buffer, and after one barrier reads the row above
@@ -257,8 +257,11 @@ __global__ void __launch_bounds__(kTT, 2)
 #pragma unroll
             for (int g = 0; g < 4; g++) {
                 const float4 v = *reinterpret_cast<const float4*>(stg + thr_off(t, g));
-                const float2 rr = f2(r, r);
-                const float2 y0 = __fmul2_rn(f2(v.x, v.y), rr), y1 = __fmul2_rn(f2(v.z, v.w), rr);
+                // scalar products: a packed multiply followed by the packed add
+                // below can be contracted into one fused multiply-add, which
+                // rounds differently when v*r lies next to a rounding midpoint
+                const float2 y0 = f2(__fmul_rn(v.x, r), __fmul_rn(v.y, r));
+                const float2 y1 = f2(__fmul_rn(v.z, r), __fmul_rn(v.w, r));
                 const float2 s0 = __fadd2_rn(y0, f2(__uint_as_float(half_bits(v.x)), __uint_as_float(half_bits(v.y))));
                 const float2 s1 = __fadd2_rn(y1, f2(__uint_as_float(half_bits(v.z)), __uint_as_float(half_bits(v.w))));
                 const float2 q0 = f2(truncf(s0.x), truncf(s0.y)), q1 = f2(truncf(s1.x), truncf(s1.y));

@@ -48,6 +48,25 @@ def _field(n, seed, kind="smooth"):
     raise ValueError(kind)
 
 
+def _midpoint_field(n, seed, eb):
+    """Values whose float product with ebx2_r = 1/(2 eb) lands exactly on k + 0.5
+    while the exact product does not: a fused multiply-add would round them
+    to the other integer."""
+    r = np.float32(1.0) / (np.float32(2.0) * np.float32(eb))
+    rng = np.random.default_rng(seed)
+    found = []
+    for k in rng.integers(-3000, 3000, 4000):
+        t = float(k) + 0.5
+        v0 = np.array([t / float(r)], np.float32).view(np.int32)[0]
+        for j in range(-3, 4):
+            v = np.array([v0 + j], np.int32).view(np.float32)
+            if float(v[0] * r) == t and float(v[0]) * float(r) != t:
+                found.append(v[0])
+    found = np.array(found, np.float32)
+    assert found.size > 100
+    return found[rng.integers(0, found.size, n)]
+
+
 def _g(a, dev):
     return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
 
@@ -217,6 +236,25 @@ def test_fused_compress_slab_and_chunk_kernels_agree(cuda, dims, kind, eb, radiu
         decs.append(_h(kern().lq_bs_rze_decompress(a["rze"], sa, a["err"], a["idx"], a["count"], a["cap"], n,
                                                    dims, abs_eb, zz, flags=flags)).view(np.uint32))
     assert np.array_equal(decs[0], decs[2]) and np.array_equal(decs[1], decs[2])
+
+
+@pytest.mark.parametrize("dims", [(256, 64, 9), (512, 16, 8), (96, 40, 9)])
+def test_rounding_midpoints_match_oracle(cuda, dims, monkeypatch):
+    # every element sits next to a rounding midpoint of x * ebx2_r: codes must
+    # come from the rounded product, with no fused multiply-add
+    n = int(np.prod(dims))
+    eb = 1e-3
+    x = _midpoint_field(n, 31, eb)
+    cap = n
+    codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, eb, O.ABS, 32768, True, cap)
+    stream = O.rze_encode(O.bitshuffle(codes, 16384, 2))
+    for flag in ("0", "1"):  # slab kernel where it applies, and the per-chunk kernel
+        monkeypatch.setenv("FZB_DISABLE_SLAB", flag)
+        out = kern().lq_bs_rze_compress(_g(x, cuda), dims, eb, O.ABS, 32768, True, 1.0)
+        size = int(_h(out["rze_size"])[0])
+        assert size == stream.size and np.array_equal(_h(out["rze"])[:size], stream), flag
+    got = kern().lq_forward(_g(x, cuda), dims, eb, O.ABS, 32768, True, 1.0)
+    assert np.array_equal(_h(got["codes"]), codes)
 
 
 def test_fused_decompress_exactness_fallback(cuda):
