@@ -162,6 +162,68 @@ def cpu_baseline(steps: int = 1):
             "ratio": nbytes / size}
 
 
+def _cpu_2d(x2d, chain: str, eb: float, mode: int, radius: int, zigzag: bool):
+    """The oracle on one 2-D field (host cores): compress and decompress GB/s,
+    median of three runs."""
+    import numpy as np
+
+    from oracle import oracle as O
+    O.lib()
+    x = np.ascontiguousarray(x2d.reshape(-1).numpy())
+    ny, nx = x2d.shape
+    dims = (nx, ny, 1)
+    cap = int(np.ceil(x.size * 0.2))
+    tc, td = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        vb = O.value_base(x, mode) if mode else 0.0
+        abs_eb, r, e2 = O.resolve_eb(eb, mode, vb)
+        codes, err, idx, cnt = O.lq_fwd(x, dims, r, radius, zigzag, cap=cap)
+        if chain == "rle":
+            s = O.rle_encode(codes)
+        elif chain == "bsrze":
+            s = O.rze_encode(O.bitshuffle(codes, 16384, 2))
+        else:
+            freq, _ = O.histogram(codes, 1024)
+            bk4, rb = O.huff_book(freq, 1024)
+            s = O.huff_encode(codes, 1024, bk4, rb)
+        t1 = time.perf_counter()
+        if chain == "rle":
+            c2 = O.rle_decode(s, x.size)
+        elif chain == "bsrze":
+            c2 = O.bitshuffle(O.rze_decode(s), 16384, 2, inverse=True).view(np.uint16)
+        else:
+            c2 = O.huff_decode(s, x.size)
+        O.lq_inv(c2, err, idx, dims, e2, zigzag)
+        t2 = time.perf_counter()
+        tc.append(t1 - t0)
+        td.append(t2 - t1)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": x.size * 4 / np.median(tc) / 1e9, "unit": "GB/s", "cores": cores, "kind": "port",
+            "decompress_gbs": x.size * 4 / np.median(td) / 1e9, "sample": f"the whole {ny}x{nx} field, oracle chain"}
+
+
+def _cpu_c1():
+    from fzgpumodules_b200 import fields
+    from oracle import oracle as O
+    return _cpu_2d(fields.sinusoids2d(1800, 3600, seed=1001), "rle", 1e-4, O.ABS, 32768, False)
+
+
+def _cpu_cli():
+    from fzgpumodules_b200 import fields
+    from oracle import oracle as O
+    return _cpu_2d(fields.sinusoids2d(1800, 3600, seed=1001), "bsrze", 1e-3, O.REL, 32768, True)
+
+
+def _cpu_c3():
+    from fzgpumodules_b200 import fields
+    from oracle import oracle as O
+    return _cpu_2d(fields.fractal2d(8192, seed=1003), "huff", 1e-3, O.ABS, 512, True)
+
+
+CPU_WORKLOADS = {"c1": _cpu_c1, "cli": _cpu_cli, "c3": _cpu_c3}
+
+
 def run_reference(args, world, rank):
     """The reference arm: the reference's stage math on the host cores (the
     reference ships no CPU implementation of this path, so the oracle port)."""
@@ -363,7 +425,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--dims", type=int, nargs=3, default=list(DEFAULT_DIMS), metavar=("NX", "NY", "NZ"),
                     help="field extents (x fastest); the default is the 512^3 workload")
-    ap.add_argument("--workload", default="chain", choices=["chain", "c1", "c3", "batch", "selector"],
+    ap.add_argument("--workload", default="chain", choices=["chain", "c1", "cli", "c3", "batch", "selector"],
                     help="chain: the headline LQ3D->BS->RZE line; others: secondary workloads (1 GPU)")
     args = ap.parse_args()
     if args.workload != "chain":
@@ -371,7 +433,10 @@ def main():
 
         from fzgpumodules_b200 import benchmarks
         if int(os.environ.get("RANK", "0")) == 0:
-            print(benchmarks.WORKLOADS[args.workload](args, torch.device("cuda", 0)), flush=True)
+            line = json.loads(benchmarks.WORKLOADS[args.workload](args, torch.device("cuda", 0)))
+            if not args.no_cpu and args.workload in CPU_WORKLOADS:
+                line["cpu_baseline"] = CPU_WORKLOADS[args.workload]()
+            print(json.dumps(line), flush=True)
         return
     world, rank, local = dist_setup() if args.impl == "ours" else (
         int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)

@@ -145,7 +145,7 @@ int resolve_eb(const float* d_in, uint64_t n_total, float eb, int mode, float va
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         uint64_t want = (n_total / 4 + 255) / 256;
-        int parts = (int)(want < (uint64_t)(4 * sms) ? want : (uint64_t)(4 * sms));
+        int parts = (int)(want < (uint64_t)(7 * sms) ? want : (uint64_t)(7 * sms));
         if (parts < 1) parts = 1;
         if (parts > kMaxParts) parts = kMaxParts;
         TraceScope ts(s, "minmax_resolve_eb");

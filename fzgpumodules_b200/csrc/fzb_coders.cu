@@ -193,36 +193,45 @@ __global__ void __launch_bounds__(256) rle_expand_kernel(const uint8_t* __restri
                                                          uint32_t* err) {
     __shared__ uint32_t s_off[kScanTile + 2];
     __shared__ T s_val[kScanTile + 2];
-    __shared__ uint32_t s_r0, s_nr;
+    __shared__ uint32_t s_nr;
     const uint32_t R = min(*reinterpret_cast<const uint32_t*>(in), n);
     const T* values = reinterpret_cast<const T*>(in + 4);
     const uint32_t t0 = blockIdx.x * kScanTile, t1 = min(n, t0 + kScanTile);
     if (t0 >= n) return;
-    if (threadIdx.x == 0) {
-        // last run whose start <= t0
-        uint32_t lo = 0, hi = R;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (offs[mid] <= t0) lo = mid;
-            else hi = mid;
-        }
-        uint32_t r1 = lo;
-        while (r1 < R && offs[r1] < t1 && r1 - lo < (uint32_t)kScanTile + 1) r1++;
-        s_r0 = lo;
-        s_nr = r1 - lo;
-        if (R == 0) atomicOr(err, kErrMalformed);
+    if (R == 0) {
+        if (threadIdx.x == 0) atomicOr(err, kErrMalformed);
+        for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) out[i] = T(0);
+        return;
     }
+    // last run whose start <= t0: every round all threads probe evenly spaced
+    // starts and the count of starts <= t0 narrows the range about blockDim-fold
+    uint32_t lo = 0, hi = R;
+    while (hi - lo > 1) {
+        const uint32_t step = (hi - lo + blockDim.x - 1) / blockDim.x;
+        const uint32_t p = lo + threadIdx.x * step;
+        const int c = __syncthreads_count(p < hi && offs[p] <= t0);
+        const uint32_t nlo = lo + (uint32_t)(c > 0 ? c - 1 : 0) * step;
+        hi = min(hi, lo + (uint32_t)(c > 0 ? c : 1) * step);
+        lo = nlo;
+    }
+    // the runs overlapping the tile: at most kScanTile + 1 from r0
+    const uint32_t r0 = lo, win = min(R - r0, (uint32_t)kScanTile + 1);
+    if (threadIdx.x == 0) s_nr = 0;
     __syncthreads();
-    const uint32_t r0 = s_r0, nr = s_nr;
+    uint32_t mine = 0;
+    for (uint32_t i = threadIdx.x; i < win; i += blockDim.x) {
+        const uint32_t o = offs[r0 + i];
+        s_off[i] = o;
+        s_val[i] = values[r0 + i];
+        mine += o < t1;
+    }
+    if (mine) atomicAdd(&s_nr, mine);
+    __syncthreads();
+    const uint32_t nr = s_nr;
     if (nr == 0) {
         for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) out[i] = T(0);
         return;
     }
-    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
-        s_off[i] = offs[r0 + i];
-        s_val[i] = values[r0 + i];
-    }
-    __syncthreads();
     for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) {
         uint32_t lo = 0, hi = nr;
         while (hi - lo > 1) {

@@ -16,7 +16,7 @@ namespace fzb {
 // device, so REL/NOA need no host round trip.
 // ---------------------------------------------------------------------------
 
-// Grid-stride min/max with four independent 16-byte loads in flight per
+// Grid-stride min/max with eight independent 16-byte loads in flight per
 // thread; the last block to finish reduces the partials and resolves
 // abs_eb / ebx2_r into st (lorenzo_quant.cu:612-644).  st layout:
 // [0] value_base, [1] abs_eb, [2] ebx2_r, [3] ebx2.
@@ -52,12 +52,12 @@ __device__ __forceinline__ void minmax_body(const float* __restrict__ x, uint64_
     const float4* x4 = reinterpret_cast<const float4*>(x);
     const uint64_t stride = (uint64_t)nblk * blockDim.x;
     uint64_t i = (uint64_t)blk * blockDim.x + threadIdx.x;
-    for (; i + 3 * stride < nv; i += 4 * stride) {
-        float4 v[4];
+    for (; i + 7 * stride < nv; i += 8 * stride) {
+        float4 v[8];
 #pragma unroll
-        for (int k = 0; k < 4; k++) v[k] = __ldg(x4 + i + k * stride);
+        for (int k = 0; k < 8; k++) v[k] = __ldg(x4 + i + k * stride);
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < 8; k++) {
             lo = fminf(lo, fminf(fminf(v[k].x, v[k].y), fminf(v[k].z, v[k].w)));
             hi = fmaxf(hi, fmaxf(fmaxf(v[k].x, v[k].y), fmaxf(v[k].z, v[k].w)));
         }

@@ -15,36 +15,63 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
                                                            uint32_t orig_expect,
                                                            unsigned long long* __restrict__ in_off,
                                                            uint32_t* err) {
-    __shared__ unsigned long long s[1024];
+    // Tiles of 4096 size words: coalesced loads into shared memory, 4 per
+    // thread, a warp-shuffle block scan, coalesced writes, carry between tiles.
+    constexpr uint32_t kTile = 4096, kPer = kTile / 1024;
+    __shared__ uint32_t sz[kTile];
+    __shared__ uint32_t wsum[32], s_tile;
     const uint32_t* h = reinterpret_cast<const uint32_t*>(rze);
-    const uint32_t n = n_expect;
+    const uint32_t n = n_expect, t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint64_t hdr = 8ull + 4ull * n;
     if (h[0] != orig_expect || h[1] != n_expect || hdr > rze_bytes) {
         // inconsistent header: flag it and point every chunk at the header end
-        if (threadIdx.x == 0) atomicOr(err, kErrMalformed);
-        for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) in_off[i] = rze_bytes + 1;
+        if (t == 0) atomicOr(err, kErrMalformed);
+        for (uint32_t i = t; i <= n; i += blockDim.x) in_off[i] = rze_bytes + 1;
         return;
     }
-    const uint32_t per = (n + 1023) / 1024;
-    const uint32_t b = threadIdx.x * per, e = min(n, b + per);
-    unsigned long long sum = 0;
-    for (uint32_t i = b; i < e; i++) sum += h[2 + i] & 0x7fffffffu;
-    s[threadIdx.x] = sum;
-    __syncthreads();
-    for (int d = 1; d < 1024; d <<= 1) {
-        unsigned long long v = (threadIdx.x >= (unsigned)d) ? s[threadIdx.x - d] : 0ull;
+    unsigned long long carry = hdr;
+    for (uint32_t t0 = 0; t0 < n; t0 += kTile) {
+        const uint32_t cnt = min(kTile, n - t0);
+        for (uint32_t i = t; i < kTile; i += 1024) sz[i] = i < cnt ? (h[2 + t0 + i] & 0x7fffffffu) : 0u;
         __syncthreads();
-        s[threadIdx.x] += v;
+        uint32_t l = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j++) l += sz[kPer * t + j];
+        uint32_t inc = l;  // tile sums fit 32 bits: 4096 chunks of at most 16 KiB
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= (uint32_t)d) inc += v;
+        }
+        if (lane == 31) wsum[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t v = wsum[lane];
+            uint32_t x = v;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t u = __shfl_up_sync(0xffffffffu, x, d);
+                if (lane >= (uint32_t)d) x += u;
+            }
+            wsum[lane] = x - v;
+        }
+        __syncthreads();
+        uint32_t r = wsum[warp] + inc - l;
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j++) {
+            const uint32_t v = sz[kPer * t + j];
+            sz[kPer * t + j] = r;
+            r += v;
+        }
+        if (t == 1023) s_tile = r;
+        __syncthreads();
+        for (uint32_t i = t; i < cnt; i += 1024) in_off[t0 + i] = carry + sz[i];
+        carry += s_tile;
         __syncthreads();
     }
-    unsigned long long run = hdr + s[threadIdx.x] - sum;
-    for (uint32_t i = b; i < e; i++) {
-        in_off[i] = run;
-        run += h[2 + i] & 0x7fffffffu;
-    }
-    if (threadIdx.x == 1023) {
-        in_off[n] = hdr + s[1023];
-        if (hdr + s[1023] > rze_bytes) atomicOr(err, kErrMalformed);
+    if (t == 0) {
+        in_off[n] = carry;
+        if (carry > rze_bytes) atomicOr(err, kErrMalformed);
     }
 }
 
