@@ -821,61 +821,98 @@ __global__ void sel_fallback_kernel(SelArgs s, uint32_t nchunks, uint8_t* __rest
     want[c] = s.sizes[(size_t)c * kSelCoders + k] == kSelNoFit ? (uint8_t)(0xFu & ~(1u << k)) : (uint8_t)0;
 }
 
-__global__ void sel_header_kernel(SelArgs s, uint32_t nchunks, uint8_t* __restrict__ out,
-                                  unsigned long long* __restrict__ out_size, unsigned long long* __restrict__ offs) {
-    // offs: exclusive scan of padded chosen sizes (one CTA, 1024 threads)
-    __shared__ unsigned long long part[1024];
-    const uint32_t t = threadIdx.x, per = (nchunks + 1023) / 1024;
-    const uint32_t b = t * per, e = min(nchunks, b + per);
-    auto chosen = [&](uint32_t c) {
-        const uint32_t k = s.tags[c];
-        return (s.sizes[(size_t)c * kSelCoders + k] + 3u) & ~3u;
-    };
-    unsigned long long sum = 0;
-    for (uint32_t c = b; c < e; c++) sum += chosen(c);
-    part[t] = sum;
-    __syncthreads();
-    for (int d = 1; d < 1024; d <<= 1) {
-        const unsigned long long v = t >= (unsigned)d ? part[t - d] : 0ull;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
-    }
+__global__ void __launch_bounds__(1024) sel_header_kernel(SelArgs s, uint32_t nchunks, uint8_t* __restrict__ out,
+                                                          unsigned long long* __restrict__ out_size,
+                                                          unsigned long long* __restrict__ offs) {
+    // offs: exclusive scan of the padded chosen sizes.  Tiles of 4096 chunks:
+    // coalesced loads (and header writes), a warp-shuffle block scan, carry.
+    constexpr uint32_t kTile = 4096, kPer = kTile / 1024;
+    __shared__ uint32_t sz[kTile];
+    __shared__ uint32_t wsum[32], s_tile;
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t hdr = 16 + 2 * ((nchunks + 3) & ~3u) + 4 * nchunks;
-    unsigned long long run = hdr + part[t] - sum;
     uint32_t* h32 = reinterpret_cast<uint32_t*>(out);
     uint8_t* tags = out + 16;
     uint8_t* params = tags + ((nchunks + 3) & ~3u);
     uint32_t* sizes = reinterpret_cast<uint32_t*>(params + ((nchunks + 3) & ~3u));
-    for (uint32_t c = b; c < e; c++) {
-        const uint32_t k = s.tags[c];
-        offs[c] = run;
-        run += chosen(c);
-        tags[c] = (uint8_t)k;
-        params[c] = s.params[c * kSelCoders + k];
-        sizes[c] = s.sizes[(size_t)c * kSelCoders + k];
+    unsigned long long carry = hdr;
+    for (uint32_t t0 = 0; t0 < nchunks; t0 += kTile) {
+        const uint32_t cnt = min(kTile, nchunks - t0);
+        for (uint32_t i = t; i < kTile; i += 1024) {
+            uint32_t v = 0;
+            if (i < cnt) {
+                const uint32_t c = t0 + i, k = s.tags[c];
+                const uint32_t len = s.sizes[(size_t)c * kSelCoders + k];
+                v = (len + 3u) & ~3u;
+                tags[c] = (uint8_t)k;
+                params[c] = s.params[c * kSelCoders + k];
+                sizes[c] = len;
+            }
+            sz[i] = v;
+        }
+        __syncthreads();
+        uint32_t l = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j++) l += sz[kPer * t + j];
+        uint32_t inc = l;  // a tile's padded sizes fit 32 bits (4096 x 64 KiB)
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= (uint32_t)d) inc += v;
+        }
+        if (lane == 31) wsum[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t v = wsum[lane];
+            uint32_t x = v;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t u = __shfl_up_sync(0xffffffffu, x, d);
+                if (lane >= (uint32_t)d) x += u;
+            }
+            wsum[lane] = x - v;
+        }
+        __syncthreads();
+        uint32_t r = wsum[warp] + inc - l;
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; j++) {
+            const uint32_t v = sz[kPer * t + j];
+            sz[kPer * t + j] = r;
+            r += v;
+        }
+        if (t == 1023) s_tile = r;
+        __syncthreads();
+        for (uint32_t i = t; i < cnt; i += 1024) offs[t0 + i] = carry + sz[i];
+        carry += s_tile;
+        __syncthreads();
     }
     for (uint32_t c = nchunks + t; c < ((nchunks + 3) & ~3u); c += 1024) {
         tags[c] = 0;
         params[c] = 0;
     }
-    if (t == 1023) {
+    if (t == 0) {
         h32[0] = 0x43535A46u;  // "FZSC"
         h32[1] = nchunks;
         h32[2] = (uint32_t)s.n;
         h32[3] = kSelCodes;
-        *out_size = hdr + part[1023];
+        *out_size = carry;
     }
 }
 
 __global__ void __launch_bounds__(256) sel_copy_kernel(SelArgs s, uint8_t* __restrict__ out,
                                                        const unsigned long long* __restrict__ offs) {
+    // payload words: offsets are multiples of 4 and slots 16-byte aligned; the
+    // bytes past len in the last word are zero padding
     const uint32_t c = blockIdx.x;
     const uint32_t k = s.tags[c];
-    const uint32_t len = s.sizes[(size_t)c * kSelCoders + k], plen = (len + 3u) & ~3u;
-    const uint8_t* src = s.slots + ((size_t)c * kSelCoders + k) * kSelSlot;
-    uint8_t* dst = out + offs[c];
-    for (uint32_t i = threadIdx.x; i < plen; i += blockDim.x) dst[i] = i < len ? src[i] : 0;
+    const uint32_t len = s.sizes[(size_t)c * kSelCoders + k], nw = (len + 3u) >> 2;
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(s.slots + ((size_t)c * kSelCoders + k) * kSelSlot);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(out + offs[c]);
+    for (uint32_t i = threadIdx.x; i < nw; i += blockDim.x) {
+        uint32_t v = src[i];
+        if (4 * i + 4 > len) v &= 0xffffffffu >> (8 * (4 * i + 4 - len));
+        dst[i] = v;
+    }
 }
 
 // ---------------------------------------------------------------------------
