@@ -233,6 +233,10 @@ def run_selector(args, dev):
         S.encode(codes, S.LEARNED, sel, trim=False)
         torch.cuda.synchronize()
         learned_kernels = {k: round(v[1], 3) for k, v in K.Trace.kernels().items()}
+    with K.Trace():
+        S.encode(codes, S.EXHAUSTIVE, trim=False)
+        torch.cuda.synchronize()
+        exhaustive_kernels = {k: round(v[1], 3) for k, v in K.Trace.kernels().items()}
     pre = codes[: 1 << 22]  # decode runs a host loop per chunk: check a 128-chunk prefix
     blob, _ = S.encode(pre, S.LEARNED, sel)
     ok = bool(torch.equal(S.decode(blob, pre.numel()), pre))
@@ -246,7 +250,8 @@ def run_selector(args, dev):
                   "learned_over_exhaustive": r["ratio_learned"] / r["ratio_exhaustive"],
                   "choice_agreement": r["agreement"], "train_chunks": int(X.shape[0]), "train_seconds": t_train,
                   "final_loss": losses[-1], "chunks": int(S.nchunks(codes.numel())),
-                  "learned_kernel_ms": learned_kernels, "decode_prefix_identical": ok,
+                  "learned_kernel_ms": learned_kernels, "exhaustive_kernel_ms": exhaustive_kernels,
+                  "decode_prefix_identical": ok,
                   "bytes_unit": "GB/s of 16-bit codes (2 B per value)"})
 
 

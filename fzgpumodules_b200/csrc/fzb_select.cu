@@ -460,8 +460,9 @@ __global__ void __launch_bounds__(256) sel_bitpack_kernel(SelArgs s) {
 
 // ---------------------------------------------------------------------------
 // Coder 3: Huffman (bklen 1024).  Histogram (CTA per chunk), canonical
-// codebook (one warp per chunk; lane 0 runs the reference's heap
-// construction, the warp canonizes), coarse encode into the PHF blob.
+// codebook (one warp per chunk; lane 0 replays the reference's heap
+// construction, the warp gathers leaves and canonizes), coarse encode into
+// the PHF blob.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) sel_hf_hist_kernel(SelArgs s) {
     __shared__ uint32_t h[kSelBk];
@@ -486,61 +487,66 @@ __global__ void __launch_bounds__(256) sel_hf_hist_kernel(SelArgs s) {
     else if (t == 0) s.sizes[(size_t)c * kSelCoders + 3] = 0;
 }
 
-// Book for one chunk (warp).  Shared memory (dynamic): node arrays for up to
-// 2*1024 nodes, the heap, the walk stack, code lengths and codes.
+// Book for one chunk (one warp).  Lane 0 replays the reference's heap
+// construction exactly (same keys, same sift rules, the first popped node
+// becomes the right child); each merge records the parent of the two merged
+// nodes, and one pass from the root down turns the parents into depths (the
+// code lengths of the reference's tree walk).  The leaf gather and the
+// canonical codebook are warp-parallel.  Dynamic shared memory (8 KB, so
+// about 25 chunks run per SM): the heap (later the per-symbol lengths), then
+// the parent/depth array.
 __global__ void __launch_bounds__(32) sel_hf_book_kernel(SelArgs s) {
     extern __shared__ uint32_t smb[];
+    __shared__ int numl[32], entry[32], first[32], nxt[32];
+    __shared__ uint32_t nzmask[32], leafbase[32];
+    __shared__ int s_ok, s_nsym;
     const int ci = sel_chunk(s, 3);
     if (ci < 0) return;
     const uint32_t c = (uint32_t)ci;
     if (s.sizes[(size_t)c * kSelCoders + 3] == kSelNoFit) return;
-    constexpr int NN = 2 * kSelBk;
-    uint32_t* F = smb;                                          // NN freq
-    int16_t* L = reinterpret_cast<int16_t*>(F + NN);            // NN left
-    int16_t* R = L + NN;                                        // NN right
-    uint16_t* S = reinterpret_cast<uint16_t*>(R + NN);          // NN symbol
-    uint32_t* heap = reinterpret_cast<uint32_t*>(S + NN);       // kSelBk + 2 keys (1-indexed)
-    uint8_t* len = reinterpret_cast<uint8_t*>(heap + kSelBk + 2);  // kSelBk
-    uint32_t* code = reinterpret_cast<uint32_t*>(len + kSelBk);    // kSelBk
-    int* meta = reinterpret_cast<int*>(code + kSelBk);          // numl[32], entry[32], first[32], next[32]
-    int* numl = meta;
-    int* entry = meta + 32;
-    int* first = meta + 64;
-    int* nxt = meta + 96;
-    int* stk_node = meta + 128;                                 // 64
-    uint32_t* stk_code = reinterpret_cast<uint32_t*>(stk_node + 64);  // 64 (low 27 bits kept)
-    uint8_t* stk_len = reinterpret_cast<uint8_t*>(stk_code + 64);     // 64
-    int* shared_ok = reinterpret_cast<int*>(stk_len + 64);
+    uint32_t* hk = smb;                                                      // kSelBk + 2 keys, 1-indexed
+    uint16_t* par = reinterpret_cast<uint16_t*>(smb + kSelBk + 2);           // 2 * kSelBk: parent, then depth
+    uint8_t* len = reinterpret_cast<uint8_t*>(smb);                          // kSelBk, over the dead heap
     const uint32_t* freq = s.hf_freq + (size_t)c * kSelBk;
-    const int lane = threadIdx.x;
-    for (int i = lane; i < kSelBk; i += 32) len[i] = 0xff;
-    if (lane < 32) {
-        numl[lane] = 0;
-        entry[lane] = 0;
-        first[lane] = 0;
+    const uint32_t lane = threadIdx.x, full = 0xffffffffu, lt = (1u << lane) - 1u;
+
+    // leaves in symbol order: leaf id = rank of the symbol among the present
+    // ones; par[leaf] holds its frequency until the heap is built
+    uint32_t fq[kSelBk / 32];
+#pragma unroll
+    for (int g = 0; g < kSelBk / 32; g++) fq[g] = freq[g * 32 + lane];
+    uint32_t mine = 0;  // lane g: present-symbol mask of group g
+#pragma unroll
+    for (int g = 0; g < kSelBk / 32; g++) {
+        const uint32_t b = __ballot_sync(full, fq[g] != 0);
+        if (lane == (uint32_t)g) mine = b;
     }
+    const uint32_t pc = __popc(mine);
+    uint32_t inc = pc;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(full, inc, d);
+        if (lane >= (uint32_t)d) inc += v;
+    }
+    nzmask[lane] = mine;
+    leafbase[lane] = inc - pc;
+    numl[lane] = 0;
+    const int leaves = (int)__shfl_sync(full, inc, 31);
     __syncwarp();
+#pragma unroll
+    for (int g = 0; g < kSelBk / 32; g++)
+        if (fq[g]) par[leafbase[g] + __popc(nzmask[g] & lt)] = (uint16_t)fq[g];
+    __syncwarp();
+
     if (lane == 0) {
-        int nn = 0;
-        for (int sym = 0; sym < kSelBk; sym++) {
-            const uint32_t fq = freq[sym];
-            if (fq) {
-                F[nn] = fq;
-                L[nn] = -1;
-                R[nn] = -1;
-                S[nn] = (uint16_t)sym;
-                nn++;
-            }
-        }
         // binary min-heap, 1-indexed, of keys freq << 11 | node id (freq <=
         // 32768, ids < 2048; comparisons look at the frequency only):
         // insertion stops at a parent whose frequency is <= the new node's;
         // removal sinks the moved node, taking the right child only when
         // strictly smaller and swapping only when strictly larger
-        uint32_t* hk = heap;
         int hs = 0;
-        auto push = [&](int id) {
-            const uint32_t key = (F[id] << 11) | (uint32_t)id, kf = F[id];
+        auto push = [&](uint32_t key) {
+            const uint32_t kf = key >> 11;
             int i = ++hs;
             while (i > 1) {
                 const int p = i >> 1;
@@ -551,21 +557,19 @@ __global__ void __launch_bounds__(32) sel_hf_book_kernel(SelArgs s) {
             }
             hk[i] = key;
         };
-        auto pop = [&]() -> int {
+        auto pop = [&]() -> uint32_t {
             const uint32_t top = hk[1];
             const uint32_t moved = hk[hs];
             hs--;
             const uint32_t mf = moved >> 11;
             int i = 1;
             while (2 * i <= hs) {
+                const uint2 kk = *reinterpret_cast<const uint2*>(hk + 2 * i);  // both children
                 int ch = 2 * i;
-                uint32_t kc = hk[ch];
-                if (ch + 1 <= hs) {
-                    const uint32_t k2 = hk[ch + 1];
-                    if ((k2 >> 11) < (kc >> 11)) {
-                        ch++;
-                        kc = k2;
-                    }
+                uint32_t kc = kk.x;
+                if (ch + 1 <= hs && (kk.y >> 11) < (kc >> 11)) {
+                    ch++;
+                    kc = kk.y;
                 }
                 if (mf > (kc >> 11)) {
                     hk[i] = kc;
@@ -575,93 +579,94 @@ __global__ void __launch_bounds__(32) sel_hf_book_kernel(SelArgs s) {
                 }
             }
             hk[i] = moved;
-            return (int)(top & 0x7ffu);
+            return top;
         };
-        const int leaves = nn;
-        for (int i = 0; i < leaves; i++) push(i);
+        for (int i = 0; i < leaves; i++) push(((uint32_t)par[i] << 11) | (uint32_t)i);
+        int nn = leaves;
         while (hs > 1) {  // the first popped node becomes the right child
-            const int right = pop();
-            const int left = pop();
-            F[nn] = F[left] + F[right];
-            L[nn] = (int16_t)left;
-            R[nn] = (int16_t)right;
-            S[nn] = 0;
-            push(nn);
+            const uint32_t kr = pop();
+            const uint32_t kl = pop();
+            par[kr & 0x7ffu] = (uint16_t)nn;
+            par[kl & 0x7ffu] = (uint16_t)nn;
+            push((((kr >> 11) + (kl >> 11)) << 11) | (uint32_t)nn);
             nn++;
         }
-        int ok = 1;
-        if (hs == 1) {  // in-order walk, left = 0, right = 1, depth limit 58
-            int sp = 0;
-            int p = pop();
-            uint32_t cd = 0, ln = 0;
-            while (true) {
-                if (L[p] >= 0 || R[p] >= 0) {
-                    if (sp + 1 > 58 || ln + 1 > 58) {
-                        ok = 0;
-                        break;
-                    }
-                    stk_node[sp] = p;
-                    stk_code[sp] = cd;
-                    stk_len[sp] = (uint8_t)ln;
-                    sp++;
-                    p = L[p];
-                    cd <<= 1;
-                    ln++;
-                } else {
-                    // lengths above 27 become the cutoff length 28 with code 0
-                    len[S[p]] = (uint8_t)(ln > 27 ? 28 : ln);
-                    code[S[p]] = ln > 27 ? 0u : (cd & 0x7ffffffu);
-                    if (sp == 0) break;
-                    sp--;
-                    p = R[stk_node[sp]];
-                    cd = (stk_code[sp] << 1) | 1u;
-                    ln = stk_len[sp] + 1u;
-                    if (ln > 58) {
-                        ok = 0;
-                        break;
-                    }
-                }
+        // depths: every parent id is above its children's, so one pass from
+        // the root down, in place; the walk's 58-level stack limit fails the
+        // book when any node lies deeper
+        int maxd = 0;
+        if (nn > 0) {
+            par[nn - 1] = 0;
+            for (int id = nn - 2; id >= 0; id--) {
+                const int d = par[par[id]] + 1;
+                par[id] = (uint16_t)d;
+                maxd = max(maxd, d);
             }
         }
-        *shared_ok = ok;
-        // canonical form
-        int max_l = 0;
-        for (int sym = 0; sym < kSelBk; sym++)
-            if (len[sym] != 0xff) {
-                numl[len[sym]]++;
-                if (len[sym] > max_l) max_l = len[sym];
-            }
-        for (int i = 1; i < 32; i++) entry[i] = entry[i - 1] + numl[i - 1];
-        for (int i = 0; i < 32; i++) nxt[i] = entry[i];
-        first[max_l] = 0;
-        for (int l = max_l - 1; l >= 1; l--) first[l] = (first[l + 1] + numl[l + 1] + 1) >> 1;
-        first[0] = 0xff;
+        s_ok = maxd <= 58;
+        s_nsym = leaves;
     }
     __syncwarp();
-    if (!*shared_ok) {
+    if (!s_ok) {
         if (lane == 0) s.sizes[(size_t)c * kSelCoders + 3] = kSelNoFit;
         return;
     }
-    // keys / canonical codes (lane 0: slot order is symbol order per length)
+    // lengths (above 27: the cutoff length 28) and their counts
+    for (int g = 0; g < kSelBk / 32; g++) {
+        uint32_t l = 0xffu;
+        const uint32_t m = nzmask[g];
+        if ((m >> lane) & 1u) {
+            const uint32_t d = par[leafbase[g] + __popc(m & lt)];
+            l = d > 27 ? 28u : d;
+        }
+        len[g * 32 + lane] = (uint8_t)l;
+        const uint32_t same = __match_any_sync(full, l);
+        if (l != 0xffu && (same >> lane) == 1u) numl[l] += __popc(same);  // highest lane of the group
+        __syncwarp();
+    }
+    // canonical form: entry = exclusive scan of the counts; first[l] from the
+    // longest length down
+    {
+        const int cnt_l = numl[lane];
+        int e = cnt_l;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(full, e, d);
+            if (lane >= (uint32_t)d) e += v;
+        }
+        entry[lane] = e - cnt_l;
+        const uint32_t used = __ballot_sync(full, cnt_l != 0);
+        const int max_l = used ? 31 - __clz(used) : 0;
+        if (lane == 0) {
+            for (int i = 0; i < 32; i++) first[i] = 0;
+            for (int l = max_l - 1; l >= 1; l--) first[l] = (first[l + 1] + numl[l + 1] + 1) >> 1;
+            first[0] = 0xff;
+        }
+    }
+    __syncwarp();
+    // slots in symbol order within each length: book words and keys
     uint32_t* bk4 = s.hf_book + (size_t)c * kSelBk;
     uint8_t* blob = s.slots + ((size_t)c * kSelCoders + 3) * kSelSlot;
     int* rb_first = reinterpret_cast<int*>(blob + 128);
     uint16_t* keys = reinterpret_cast<uint16_t*>(blob + 128 + 256);
-    for (int i = lane; i < kSelBk; i += 32) {
-        bk4[i] = 0xffffffffu;
-        keys[i] = 0;
-    }
+    nxt[lane] = entry[lane];
     __syncwarp();
-    if (lane == 0) {
-        for (int sym = 0; sym < kSelBk; sym++) {
-            if (len[sym] == 0xff) continue;
-            const uint32_t l = len[sym];
-            const int slot = nxt[l]++;
-            bk4[sym] = ((uint32_t)(first[l] + slot - entry[l]) & 0x7ffffffu) | (l << 27);
+    for (int g = 0; g < kSelBk / 32; g++) {
+        const uint32_t sym = g * 32 + lane;
+        const uint32_t l = len[sym];
+        const uint32_t same = __match_any_sync(full, l);
+        uint32_t w = 0xffffffffu;
+        if (l != 0xffu) {
+            const int slot = nxt[l] + __popc(same & lt);
+            w = ((uint32_t)(first[l] + slot - entry[l]) & 0x7ffffffu) | (l << 27);
             keys[slot] = (uint16_t)sym;
         }
+        bk4[sym] = w;
+        __syncwarp();
+        if (l != 0xffu && (same >> lane) == 1u) nxt[l] += __popc(same);
+        __syncwarp();
     }
-    __syncwarp();
+    for (int i = s_nsym + (int)lane; i < kSelBk; i += 32) keys[i] = 0;
     rb_first[lane] = first[lane];
     rb_first[32 + lane] = entry[lane];
 }
@@ -1107,8 +1112,7 @@ int launch_sel_features(const uint16_t* codes, uint64_t n, float* feats, cudaStr
 // F[NN] L[NN] R[NN] S[NN] heap[kSelBk+2] len[kSelBk] code[kSelBk] meta[192]
 // stk_code[64] stk_len[64] ok
 size_t sel_book_smem() {
-    constexpr size_t NN = 2 * kSelBk;
-    return NN * 4 + NN * 2 * 3 + (kSelBk + 2) * 4 + kSelBk + kSelBk * 4 + 4 * (128 + 64) + 64 * 4 + 64 + 16;
+    return (kSelBk + 2) * 4 + 2 * kSelBk * 2;  // heap (later the lengths), parent/depth array
 }
 
 int launch_sel_tag_mask(const SelArgs& a, uint32_t nchunks, uint8_t* want, cudaStream_t s) {
@@ -1125,20 +1129,34 @@ int launch_sel_coders(const SelArgs& a, uint32_t nlist, unsigned coder_mask, cud
     if (nlist == 0) return 0;
     cudaError_t e;
     if (coder_mask & 1u) {
+        TraceScope ts(s, "sel_rze");
         const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
         e = cudaFuncSetAttribute(sel_rze_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return (int)e;
         sel_rze_sub_kernel<<<dim3(nlist, 4), kThreads, smem, s>>>(a);
         sel_rze_assemble_kernel<<<nlist, 256, 0, s>>>(a);
     }
-    if (coder_mask & 2u) sel_rle_kernel<<<nlist, 256, 0, s>>>(a);
-    if (coder_mask & 4u) sel_bitpack_kernel<<<nlist, 256, 0, s>>>(a);
+    if (coder_mask & 2u) {
+        TraceScope ts(s, "sel_rle");
+        sel_rle_kernel<<<nlist, 256, 0, s>>>(a);
+    }
+    if (coder_mask & 4u) {
+        TraceScope ts(s, "sel_bitpack");
+        sel_bitpack_kernel<<<nlist, 256, 0, s>>>(a);
+    }
     if (coder_mask & 8u) {
-        sel_hf_hist_kernel<<<nlist, 256, 0, s>>>(a);
+        {
+            TraceScope ts(s, "sel_hf_hist");
+            sel_hf_hist_kernel<<<nlist, 256, 0, s>>>(a);
+        }
         const int smem = (int)sel_book_smem();
         e = cudaFuncSetAttribute(sel_hf_book_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return (int)e;
-        sel_hf_book_kernel<<<nlist, 32, smem, s>>>(a);
+        {
+            TraceScope ts(s, "sel_hf_book");
+            sel_hf_book_kernel<<<nlist, 32, smem, s>>>(a);
+        }
+        TraceScope ts(s, "sel_hf_encode");
         sel_hf_encode_kernel<<<nlist, 256, 0, s>>>(a);
     }
     return (int)cudaGetLastError();

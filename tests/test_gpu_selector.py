@@ -33,6 +33,9 @@ def _codes():
         rng.integers(0, 65536, 32768).astype(np.uint16),                                 # incompressible
         np.zeros(32768, np.uint16),                                                      # constant
         rng.integers(0, 3, 32768).astype(np.uint16),                                     # 2-bit noise
+        rng.permutation(np.repeat(np.arange(512), 64)).astype(np.uint16),                # all frequencies tie
+        rng.permutation(np.repeat(rng.permutation(1024),                                 # four frequency levels
+                                  np.repeat([48, 24, 12, 4], [512, 256, 128, 128]))).astype(np.uint16),
         rng.integers(0, 1200, 20000).astype(np.uint16),                                  # partial, >= 1024
     ]
     return np.concatenate(parts)
