@@ -4,33 +4,36 @@
 // Applies to 3-D fields whose 8192-element chunks are R = 8192/nx whole rows
 // (nx a power of two in [32, 1024], ny % R == 0, no padding).  A work unit is
 // one R-row slab across one 8-plane z tile; the unit's chunks are produced
-// plane by plane by one persistent CTA of 256 threads.
+// plane by plane by one persistent CTA of 512 threads (two CTAs per SM).
 //
-// Data flow per chunk (= one slab plane):
+// Data flow per chunk (= one slab plane), four CTA barriers:
 //   * one thread issues a 2-D TMA copy of the 32 KiB plane into a 128-byte
-//     swizzled shared buffer, two planes ahead of use (double buffer,
-//     mbarrier completion, bounded waits);
-//   * thread t owns chunk elements 32t..32t+31 (one 32-wide x segment of one
-//     row).  It quantizes them (f32x2 adds, scalar products), forms the z
-//     difference against the previous plane's q held in registers and the x
-//     difference in registers, writes B = (z, x)-differenced values back over
-//     its own bytes of the buffer, and after one barrier reads the row above
-//     for the y difference (lorenzo_quant_nd.cu:236-246 order);
+//     swizzled shared buffer one plane ahead of use (double buffer, mbarrier
+//     completion, bounded waits);
+//   * thread t owns chunk elements 16t..16t+15 (half of one 32-wide x
+//     segment of one row).  It quantizes them (f32x2 adds, scalar products),
+//     forms the z difference against the previous plane's q held in
+//     registers and the x difference in registers, writes B = (z, x)-
+//     differenced values back over its own bytes of the buffer, and after
+//     barrier B1 reads the row above for the y difference
+//     (lorenzo_quant_nd.cu:236-246 order);
 //   * codes come from the exact integer-valued deltas through the float
 //     magic-number conversion (c + 1.5*2^23 holds c in its low mantissa
 //     bits), zigzag works on packed code pairs, outliers are found per
 //     4-element granule with a NaN-propagating max;
-//   * the 32 codes are bit-transposed in registers (the Bitshuffle ballot
-//     layout, bitshuffle_stage.cu:299-323) and RZE level 1 is built straight
-//     from the registers: per-plane nonzero-byte counts are scanned per warp
-//     (8-bit fields), warp 0 turns the warp totals into byte offsets, and each
-//     thread compacts the nonzero bytes of each of its plane words (byte
-//     permute) into zeroed shared memory with two shared atomics; the level-1
-//     bitmap is formed by an 8-lane byte transpose.  Levels 2-4 follow
-//     (rze_stage.cu:324-445), levels 3-4 in warp 0 alone;
-//   * the encoded chunk goes to its 16 KiB slot; assemble_scan/assemble_copy
-//     (fzb_forward.cu) place slots and staged outliers exactly as for the
-//     other chunk kernels.
+//   * the 16 codes are bit-transposed in registers (the Bitshuffle ballot
+//     layout, bitshuffle_stage.cu:299-323) and stored as the shuffled chunk S
+//     in shared memory (B2);
+//   * RZE (rze_stage.cu:324-445): thread t reads S words 8t..8t+7, forms
+//     their nonzero-byte nibbles (level-1 bitmap word t) and the level-2 bits
+//     of its four bm1 bytes; one packed warp scan counts both levels, and
+//     after B3 the warp totals give every thread its payload offsets.  Each
+//     thread compacts the nonzero bytes of its word pairs (two byte permutes
+//     from a 256-entry selector table) into a zeroed payload buffer with
+//     shared atomics; meanwhile warp 0 codes levels 3 and 4 and the trailer;
+//   * after B4 the encoded chunk goes to its 16 KiB slot; assemble_scan /
+//     assemble_copy (fzb_forward.cu) place slots and staged outliers exactly
+//     as for the other chunk kernels.
 #include "fzb_slab.cuh"
 
 namespace fzb {
@@ -189,6 +192,7 @@ __global__ void __launch_bounds__(kTT, 2)
     extern __shared__ uint8_t dsm[];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ uint32_t s_sel[16];
+    __shared__ uint2 s_sel8[256];  // pair compaction selectors: set bytes first, then a zero byte
     __shared__ uint32_t s_wout[kTT / 32];  // per warp: outlier count
     __shared__ uint32_t s_l1[kTT / 32];    // per warp: level-1 | level-2 << 16 byte counts
     __shared__ uint32_t s_misc[4];         // 1 outlier staging base, 2 size word
@@ -211,6 +215,18 @@ __global__ void __launch_bounds__(kTT, 2)
     const uint32_t G = gridDim.x;
 
     if (t < 16) s_sel[t] = kSelInit[t];
+    if (t < 256) {  // mask t: the flagged bytes of a word pair in order, then a zero (unflagged) byte
+        uint32_t sel = 0, k = 0, zb = 0;
+        for (uint32_t b = 0; b < 8; b++)
+            if (!((t >> b) & 1u)) {
+                zb = b;
+                break;
+            }
+        for (uint32_t b = 0; b < 8; b++)
+            if ((t >> b) & 1u) sel |= b << (4 * k++);
+        for (; k < 8; k++) sel |= zb << (4 * k);
+        s_sel8[t] = make_uint2(sel & 0xffffu, sel >> 16);  // output bytes 0-3 and 4-7
+    }
     for (uint32_t i = t; i < (uint32_t)kOBytes / 16; i += kTT) reinterpret_cast<uint4*>(O)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (t == 0) {
         mbar_init(&s_bar[0], 1);
@@ -394,20 +410,33 @@ __global__ void __launch_bounds__(kTT, 2)
             const uint32_t wpos = nzT + n2T;
             if (mode == 0 && (wpos >= (uint32_t)kRzeAvail || wpos > (uint32_t)(kRzeAvail - 256))) mode = 2;
             if (mode == 0) {
-                // level-1 payload: the nonzero bytes of the 8 words, compacted
+                // level-1 payload: the nonzero bytes of each word pair, compacted
+                // by two byte permutes and ORed into the zeroed payload buffer
                 uint32_t pos = pre12 & 0xffffu;
+                if (nb1)  // threads of all-zero plane regions skip the loop
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const uint32_t nb = (nb1 >> (4 * i)) & 15u;
-                    if (nb) or_bytes_at(Ow, pos, __byte_perm(w[i], 0u, s_sel[nb]));
-                    pos += __popc(nb);
+                for (int i = 0; i < 4; i++) {
+                    const uint32_t m8 = (nb1 >> (8 * i)) & 0xffu;
+                    if (m8) {
+                        const uint2 sel = s_sel8[m8];
+                        const uint32_t lo = __byte_perm(w[2 * i], w[2 * i + 1], sel.x);
+                        const uint32_t hi = __byte_perm(w[2 * i], w[2 * i + 1], sel.y);
+                        const uint32_t sh = (pos & 3u) * 8u;
+                        uint32_t* dst = Ow + (pos >> 2);
+                        atomicOr(dst, lo << sh);
+                        atomicOr(dst + 1, __funnelshift_l(lo, hi, sh));
+                        atomicOr(dst + 2, __funnelshift_l(hi, 0u, sh));
+                    }
+                    pos += __popc(m8);
                 }
                 // level-2 payload: the non-repeated bm1 bytes
                 if (m2) or_bytes_at(Ow, nzT + (pre12 >> 16), __byte_perm(nb1, 0u, s_sel[m2]));
             }
-            __syncthreads();  // B4
 
-            // levels 3 and 4 (warp 0), header
+            // levels 3 and 4 and the chunk trailer (warp 0, while the other
+            // warps compact): bm2 and the payload end wpos are known since B3;
+            // bytes at and after wpos go in by atomics too, since the last
+            // level-2 payload word may be shared
             if (mode == 0 && warp == 0) {
                 const uint2 mw = reinterpret_cast<const uint2*>(bm2)[lane];
                 const uint64_t M3 = ((uint64_t)mw.y << 32) | mw.x;
@@ -421,7 +450,8 @@ __global__ void __launch_bounds__(kTT, 2)
                     while (m) {
                         const uint32_t b = __ffs(m) - 1;
                         m &= m - 1;
-                        O[p++] = (uint8_t)(M3 >> (8 * b));
+                        atomicOr(&Ow[p >> 2], (uint32_t)(uint8_t)(M3 >> (8 * b)) << (8 * (p & 3u)));
+                        p++;
                     }
                 }
                 uint32_t pb = __shfl_up_sync(full, m3, 1);
@@ -432,16 +462,18 @@ __global__ void __launch_bounds__(kTT, 2)
                 uint32_t sw = 0x80000000u | (uint32_t)kChunkBytes;
                 if (!(wp >= (uint32_t)kRzeAvail || wp >= (uint32_t)(kRzeAvail - 4) ||
                       wp > (uint32_t)(kRzeAvail - 4 - 32))) {
-                    if (nr4) O[wp + __popc(bm4 & ((1u << lane) - 1u))] = (uint8_t)m3;
+                    if (nr4) {
+                        const uint32_t q = wp + __popc(bm4 & ((1u << lane) - 1u));
+                        atomicOr(&Ow[q >> 2], (m3 & 0xffu) << (8 * (q & 3u)));
+                    }
                     wp += __popc(bm4);
                     if (wp < (uint32_t)(kRzeAvail - 4)) {
-                        if (lane == 0) {
-                            O[wp + 0] = (uint8_t)bm4;
-                            O[wp + 1] = (uint8_t)(bm4 >> 8);
-                            O[wp + 2] = (uint8_t)(bm4 >> 16);
-                            O[wp + 3] = (uint8_t)(bm4 >> 24);
-                            O[wp + 4] = (uint8_t)(kChunkBytes & 0xff);
-                            O[wp + 5] = (uint8_t)(kChunkBytes >> 8);
+                        if (lane == 0) {  // bm4 word and the original size, 6 bytes from wp
+                            const uint32_t sh = 8 * (wp & 3u);
+                            const uint32_t lo = bm4, hi = (uint32_t)kChunkBytes;
+                            atomicOr(&Ow[wp >> 2], lo << sh);
+                            atomicOr(&Ow[(wp >> 2) + 1], __funnelshift_l(lo, hi, sh));
+                            atomicOr(&Ow[(wp >> 2) + 2], __funnelshift_l(hi, 0u, sh));
                         }
                         sw = wp + 6;
                     }
@@ -457,7 +489,7 @@ __global__ void __launch_bounds__(kTT, 2)
                     s_misc[2] = 0x80000000u | (uint32_t)kChunkBytes;
                 }
             }
-            __syncthreads();  // B5
+            __syncthreads();  // B4
 
             const uint32_t sw = s_misc[2];
             uint4* d4 = reinterpret_cast<uint4*>(a.slots + (size_t)c * kChunkBytes);
