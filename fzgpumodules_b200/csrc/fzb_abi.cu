@@ -535,7 +535,7 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             TraceScope ts(s, "lq3d_inv_slab");
-            if (launch_lq3d_inv_slab(a, (unsigned)(2 * sms), s) != 0) return FZB_E_CUDA;
+            if (launch_lq3d_inv_slab(a, (unsigned)sms, s) != 0) return FZB_E_CUDA;
         } else {
             dim3 grid(g.ny / R, (g.nz + 7) / 8, 1);
             TraceScope ts(s, "fused_inverse_3d");

@@ -122,7 +122,7 @@ __global__ void lq_inverse_2d_kernel(InvArgs a);
 __global__ void lq_inverse_3d_kernel(InvArgs a);
 __global__ void fused_inverse_3d_kernel(InvArgs a);
 // Persistent slab inverse (fzb_slab_inv.cu) for nx >= 32; same results.
-int launch_lq3d_inv_slab(const InvArgs& a, unsigned grid, cudaStream_t s);
+int launch_lq3d_inv_slab(const InvArgs& a, unsigned sms, cudaStream_t s);  // persistent grid: 3 CTAs per SM
 
 // Exclusive scan of u32 values (fzb_coders.cu).  The source is a plain
 // array (count given, or read from *cptr on the device) or the run-length

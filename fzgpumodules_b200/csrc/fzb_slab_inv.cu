@@ -15,10 +15,13 @@
 //     re-expanded with a byte permute; the words are bit-transposed back to
 //     32 codes (bitshuffle_stage.cu:299-323 layout);
 //   * codes -> deltas through the float magic-number conversion, outliers of
-//     the segment are added, the x prefix runs in registers; after one barrier
-//     each thread takes a 4-wide, 8-row column strip for the y prefix, the
-//     running z sum (registers, across the unit's planes) and the 16-byte
-//     output stores (value * 2 * eb).
+//     the segment are added, the x prefix runs in registers; after the next
+//     chunk's first barrier (so that this pass overlaps warp 0's level
+//     decoding of that chunk) each thread takes a 4-wide, 8-row column strip
+//     for the y prefix, the running z sum (registers, across the unit's
+//     planes) and the 16-byte output stores (value * 2 * eb).
+//
+// Three CTAs of 256 threads run per SM (80 registers a thread).
 //
 // The reference scans x, y and z with Hillis-Steele add trees
 // (lorenzo_quant_nd.cu inverse); this kernel sums sequentially.  Every
@@ -35,6 +38,7 @@ namespace {
 constexpr int kCBytes = kChunkBytes + 64;  // one staged chunk (+ lead bytes and a slack word)
 constexpr size_t kInvSmem = kSmemAlign + kStageBytes + 2 * kCBytes + 2048 + 256 + 1024;
 constexpr float kExact = 2097152.0f;       // 2^21
+constexpr int kInvCtasPerSm = 3;           // 80 registers a thread, 3 x 73 KB of shared memory an SM
 
 // Expansion selectors: __byte_perm(v, 0, kExpandInit[m]) moves the low
 // popc(m) bytes of v to the byte positions flagged in the 4-bit mask m.
@@ -102,7 +106,7 @@ __device__ __forceinline__ uint32_t biased_pair(uint32_t x) {
 namespace {
 
 template <bool ZZ>
-__global__ void __launch_bounds__(kThreads, 2) lq3d_inv_slab_kernel(InvArgs a, uint32_t slabs, uint32_t units) {
+__global__ void __launch_bounds__(kThreads, kInvCtasPerSm) lq3d_inv_slab_kernel(InvArgs a, uint32_t slabs, uint32_t units) {
     extern __shared__ uint8_t dsm[];
     __shared__ uint32_t s_exp[16];
     __shared__ uint32_t s_tot[8][4];    // per warp: inclusive plane counts, 8-bit fields
@@ -138,18 +142,51 @@ __global__ void __launch_bounds__(kThreads, 2) lq3d_inv_slab_kernel(InvArgs a, u
         stage_chunk(a, unit_z0(blockIdx.x) * slabs + u % slabs, Cbuf, ce, clead, cok);
     }
 
+    // Output pass of one decoded plane (x-prefixed rows in X): the thread's
+    // column strip gets its y prefix, the running z sum and 16-byte stores.
+    float acc[32];
+#pragma unroll
+    for (int i = 0; i < 32; i++) acc[i] = 0.0f;
+    auto strip = [&](uint32_t sz, uint32_t ss, bool chk) {
+        float2 y0 = f2(0.0f, 0.0f), y1 = y0;
+        float mx = 0.0f;
+        const float2 e2 = f2(ebx2, ebx2);
+        float* orow = a.out + ((size_t)sz * a.ny + (size_t)ss * R + band * 8u) * nx + 4u * x4;
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const uint32_t own = (band * 8u + r) * S + (x4 >> 3);
+            const float4 v = *reinterpret_cast<const float4*>(X + swz_off(own, x4 & 7u));
+            if (r == 0) {
+                y0 = f2(v.x, v.y);
+                y1 = f2(v.z, v.w);
+            } else {
+                y0 = __fadd2_rn(y0, f2(v.x, v.y));
+                y1 = __fadd2_rn(y1, f2(v.z, v.w));
+            }
+            if (chk) mx = max_nan(max_nan(mx, fmaxf(fabsf(y0.x), fabsf(y0.y))), fmaxf(fabsf(y1.x), fabsf(y1.y)));
+            const float2 a0 = __fadd2_rn(f2(acc[4 * r], acc[4 * r + 1]), y0);
+            const float2 a1 = __fadd2_rn(f2(acc[4 * r + 2], acc[4 * r + 3]), y1);
+            acc[4 * r] = a0.x;
+            acc[4 * r + 1] = a0.y;
+            acc[4 * r + 2] = a1.x;
+            acc[4 * r + 3] = a1.y;
+            const float2 o0v = __fmul2_rn(a0, e2), o1v = __fmul2_rn(a1, e2);
+            *reinterpret_cast<float4*>(orow + (size_t)r * nx) = make_float4(o0v.x, o0v.y, o1v.x, o1v.y);
+        }
+        if (chk && !(mx < kExact)) inexact = true;
+    };
+    bool pend = false, pchk = false;
+    uint32_t pz = 0, ps = 0;
+
     uint32_t k = 0;
     for (uint32_t uu = blockIdx.x; uu < units; uu += G) {
         const uint32_t u = units - 1 - uu, s = u % slabs;
         const uint32_t z0 = (u / slabs) * 8u, z1 = min(z0 + 8u, a.nz);
-        float acc[32];
-#pragma unroll
-        for (int i = 0; i < 32; i++) acc[i] = 0.0f;
         for (uint32_t z = z0; z < z1; z++, k++) {
             const uint32_t c = z * slabs + s;
             const uint32_t* Cw = Cbuf + (k & 1) * (kCBytes / 4);
             cp_async_wait_all();
-            __syncthreads();  // B0: chunk c staged; the previous plane is done with every buffer
+            __syncthreads();  // B0: chunk c staged; the previous plane's X rows are complete
             const uint32_t e = ce, lead = clead;
             const bool ok = cok;
             {   // stage the next plane's chunk into the other buffer
@@ -161,6 +198,11 @@ __global__ void __launch_bounds__(kThreads, 2) lq3d_inv_slab_kernel(InvArgs a, u
                 if (nu < units)
                     stage_chunk(a, nz * slabs + (units - 1 - nu) % slabs, Cbuf + ((k + 1) & 1) * (kCBytes / 4), ce,
                                 clead, cok);
+            }
+            if (pend) strip(pz, ps, pchk);  // the previous plane (X is complete since B0)
+            if (z == z0) {
+#pragma unroll
+                for (int i = 0; i < 32; i++) acc[i] = 0.0f;
             }
 
             // 0: RZE levels, 1: zeros, 2: stored raw (rze_stage.cu:904-930 cases)
@@ -377,38 +419,16 @@ __global__ void __launch_bounds__(kThreads, 2) lq3d_inv_slab_kernel(InvArgs a, u
 #pragma unroll
             for (int g = 0; g < 8; g++)
                 *reinterpret_cast<float4*>(X + swz_off(t, g)) = make_float4(d[4 * g], d[4 * g + 1], d[4 * g + 2], d[4 * g + 3]);
-            __syncthreads();  // B5
-
-            // column strip: y prefix, running z sum, output rows
-            {
-                float2 y0 = f2(0.0f, 0.0f), y1 = y0;
-                float mx = 0.0f;
-                const float2 e2 = f2(ebx2, ebx2);
-                float* orow = a.out + ((size_t)z * a.ny + (size_t)s * R + band * 8u) * nx + 4u * x4;
-#pragma unroll
-                for (int r = 0; r < 8; r++) {
-                    const uint32_t own = (band * 8u + r) * S + (x4 >> 3);
-                    const float4 v = *reinterpret_cast<const float4*>(X + swz_off(own, x4 & 7u));
-                    if (r == 0) {
-                        y0 = f2(v.x, v.y);
-                        y1 = f2(v.z, v.w);
-                    } else {
-                        y0 = __fadd2_rn(y0, f2(v.x, v.y));
-                        y1 = __fadd2_rn(y1, f2(v.z, v.w));
-                    }
-                    if (checked) mx = max_nan(max_nan(mx, fmaxf(fabsf(y0.x), fabsf(y0.y))), fmaxf(fabsf(y1.x), fabsf(y1.y)));
-                    const float2 a0 = __fadd2_rn(f2(acc[4 * r], acc[4 * r + 1]), y0);
-                    const float2 a1 = __fadd2_rn(f2(acc[4 * r + 2], acc[4 * r + 3]), y1);
-                    acc[4 * r] = a0.x;
-                    acc[4 * r + 1] = a0.y;
-                    acc[4 * r + 2] = a1.x;
-                    acc[4 * r + 3] = a1.y;
-                    const float2 o0v = __fmul2_rn(a0, e2), o1v = __fmul2_rn(a1, e2);
-                    *reinterpret_cast<float4*>(orow + (size_t)r * nx) = make_float4(o0v.x, o0v.y, o1v.x, o1v.y);
-                }
-                if (checked && !(mx < kExact)) inexact = true;
-            }
+            // this plane's output pass runs after the next B0
+            pend = true;
+            pz = z;
+            ps = s;
+            pchk = checked;
         }
+    }
+    if (pend) {  // the last plane
+        __syncthreads();
+        strip(pz, ps, pchk);
     }
     cp_async_wait_all();
     if (__any_sync(full, inexact) && lane == 0) atomicOr(a.err, kErrInexact);
@@ -417,8 +437,9 @@ __global__ void __launch_bounds__(kThreads, 2) lq3d_inv_slab_kernel(InvArgs a, u
 
 }  // namespace
 
-int launch_lq3d_inv_slab(const InvArgs& a, unsigned grid, cudaStream_t s) {
+int launch_lq3d_inv_slab(const InvArgs& a, unsigned sms, cudaStream_t s) {
     const uint32_t slabs = a.ny / (kChunkCodes / a.nx), units = slabs * ((a.nz + 7) / 8);
+    unsigned grid = sms * kInvCtasPerSm;
     grid = grid < units ? grid : units;
     cudaError_t e;
     if (a.zigzag) {
