@@ -109,6 +109,7 @@ def lib():
         L.fzb_pipeline_add_rze.argtypes = [p, u32, i32]
         L.fzb_pipeline_add_rle.argtypes = [p, i32]
         L.fzb_pipeline_add_huffman.argtypes = [p, u32]
+        L.fzb_pipeline_add_huffman_mode.argtypes = [p, u32, i32]
         L.fzb_pipeline_add_bitpack.argtypes = [p, i32, i32]
         L.fzb_pipeline_connect.argtypes = [p, i32, i32, C.c_char_p]
         L.fzb_pipeline_set_fusion.argtypes = [p, i32]
@@ -144,6 +145,10 @@ def lib():
         L.fzb_huff_encode.argtypes = [p, u64, u32, p, p, p, p, p, sz, p]
         L.fzb_huff_compress.restype = i32
         L.fzb_huff_compress.argtypes = [p, u64, u32, p, p, p, sz, p]
+        L.fzb_huff_encode_fine.restype = i32
+        L.fzb_huff_encode_fine.argtypes = [p, u64, u32, p, p, p, p, p, sz, p]
+        L.fzb_huff_compress_fine.restype = i32
+        L.fzb_huff_compress_fine.argtypes = [p, u64, u32, p, p, p, sz, p]
         L.fzb_huff_decode.restype = i32
         L.fzb_huff_decode.argtypes = [p, u64, u64, u32, p, p, sz, p]
         L.fzb_rze_encode_noalloc.restype = i32

@@ -664,7 +664,9 @@ HfWork carve_hf(void* base, uint64_t n, uint32_t bklen) {
     w.par_ncell = reinterpret_cast<uint32_t*>(take(4 * pd));
     w.par_entry = reinterpret_cast<uint32_t*>(take(4 * pd));
     w.tiles = reinterpret_cast<uint32_t*>(take(4 * (pd / 4096 + 64)));
-    w.slots = reinterpret_cast<uint32_t*>(take(4 * pd * kHfSublen));
+    // partition slots for either partition length
+    const uint64_t pd_fine = (n - 1) / kHfSublenFine + 1;
+    w.slots = reinterpret_cast<uint32_t*>(take(4 * std::max(pd * kHfSublen, pd_fine * kHfSublenFine)));
     w.need = off;
     return w;
 }
@@ -707,8 +709,12 @@ int fzb_huff_book(const uint32_t* h_freq, uint32_t bklen, uint32_t* h_bk4, uint8
     return build_huffman_book(h_freq, bklen, h_bk4, h_revbook) == 0 ? FZB_OK : FZB_E_INVALID;
 }
 
-int fzb_huff_encode(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint32_t* d_bk4,
-                    const uint8_t* d_revbook, void* d_out, uint64_t* d_out_size, void* d_work,
+}  // extern "C"
+
+namespace {
+
+int huff_encode_sub(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint32_t* d_bk4,
+                    const uint8_t* d_revbook, uint32_t sublen, void* d_out, uint64_t* d_out_size, void* d_work,
                     size_t work_bytes, void* stream) {
     if (!d_in || !d_bk4 || !d_revbook || !d_out || !d_out_size || !hf_args_ok(n, bklen))
         return FZB_E_INVALID;
@@ -717,13 +723,13 @@ int fzb_huff_encode(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint
     if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
     cudaStream_t s = S(stream);
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
-    return launch_hf_encode(d_in, n, d_bk4, bklen, d_revbook, static_cast<uint8_t*>(d_out),
+    return launch_hf_encode(d_in, n, d_bk4, bklen, sublen, d_revbook, static_cast<uint8_t*>(d_out),
                             reinterpret_cast<unsigned long long*>(d_out_size), w.slots, w.par_nbit,
                             w.par_ncell, w.par_entry, w.tiles, w.ncell_total, sm_count(), s) == 0
                ? FZB_OK : FZB_E_CUDA;
 }
 
-int fzb_huff_compress(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_out,
+int huff_compress_sub(const uint16_t* d_in, uint64_t n, uint32_t bklen, uint32_t sublen, void* d_out,
                       uint64_t* d_out_size, void* d_work, size_t work_bytes, void* stream) {
     if (!d_in || !d_out || !d_out_size || !hf_args_ok(n, bklen)) return FZB_E_INVALID;
     if (reinterpret_cast<uintptr_t>(d_out) & 3) return FZB_E_INVALID;
@@ -743,8 +749,36 @@ int fzb_huff_compress(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_
     // pageable sources: each copy has read its host buffer when the call returns
     CK(cudaMemcpyAsync(w.bk4, bk4.data(), 4 * (size_t)bklen, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(w.revbook, revbook.data(), revbook.size(), cudaMemcpyHostToDevice, s));
-    return fzb_huff_encode(d_in, n, bklen, w.bk4, w.revbook, d_out, d_out_size, d_work, work_bytes,
+    return huff_encode_sub(d_in, n, bklen, w.bk4, w.revbook, sublen, d_out, d_out_size, d_work, work_bytes,
                            stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fzb_huff_encode(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint32_t* d_bk4,
+                    const uint8_t* d_revbook, void* d_out, uint64_t* d_out_size, void* d_work,
+                    size_t work_bytes, void* stream) {
+    return huff_encode_sub(d_in, n, bklen, d_bk4, d_revbook, kHfSublen, d_out, d_out_size, d_work, work_bytes,
+                           stream);
+}
+
+int fzb_huff_encode_fine(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint32_t* d_bk4,
+                         const uint8_t* d_revbook, void* d_out, uint64_t* d_out_size, void* d_work,
+                         size_t work_bytes, void* stream) {
+    return huff_encode_sub(d_in, n, bklen, d_bk4, d_revbook, kHfSublenFine, d_out, d_out_size, d_work,
+                           work_bytes, stream);
+}
+
+int fzb_huff_compress(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_out,
+                      uint64_t* d_out_size, void* d_work, size_t work_bytes, void* stream) {
+    return huff_compress_sub(d_in, n, bklen, kHfSublen, d_out, d_out_size, d_work, work_bytes, stream);
+}
+
+int fzb_huff_compress_fine(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_out,
+                           uint64_t* d_out_size, void* d_work, size_t work_bytes, void* stream) {
+    return huff_compress_sub(d_in, n, bklen, kHfSublenFine, d_out, d_out_size, d_work, work_bytes, stream);
 }
 
 int fzb_huff_decode(const void* d_in, uint64_t in_bytes, uint64_t n, uint32_t bklen, uint16_t* d_out,

@@ -232,10 +232,11 @@ private:
 };
 
 // PHF Huffman, coarse mode (fzb_huffman.cu, codebook in fzb_hfbook.cpp).
-constexpr int kHfSublen = 768;
+constexpr int kHfSublen = 768;       // coarse mode partition (hf_bk.cc:28-37)
+constexpr int kHfSublenFine = 1024;  // fine mode partition (hf_buf.cc:46-49)
 int launch_hf_histogram(const uint16_t* in, uint64_t n, uint32_t bklen, uint32_t* freq, int sms,
                         cudaStream_t s);
-int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32_t bklen,
+int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32_t bklen, uint32_t sublen,
                      const uint8_t* d_revbook, uint8_t* out, unsigned long long* out_size,
                      uint32_t* slots, uint32_t* par_nbit, uint32_t* par_ncell, uint32_t* par_entry,
                      uint32_t* tiles, uint32_t* ncell_total, int sms, cudaStream_t s);

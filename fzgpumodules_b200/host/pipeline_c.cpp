@@ -133,6 +133,16 @@ int fzb_pipeline_add_huffman(void* p, uint32_t bklen) {
     });
 }
 
+int fzb_pipeline_add_huffman_mode(void* p, uint32_t bklen, int encode_mode) {
+    if (!p || bklen < 1 || bklen > 65535 || encode_mode < 0 || encode_mode > 1) return FZB_E_INVALID;
+    return guarded([&] {
+        auto* s = H(p)->p->addStage<fz::HuffmanStage<uint16_t>>();
+        s->setBklen(bklen);
+        s->setEncodeMode(encode_mode ? fz::HuffmanEncodeMode::Fine : fz::HuffmanEncodeMode::Coarse);
+        return add(p, s);
+    });
+}
+
 int fzb_pipeline_add_bitpack(void* p, int elem, int nbits) {
     if (!p || (elem != 1 && elem != 2 && elem != 4)) return FZB_E_INVALID;
     return guarded([&] {

@@ -488,8 +488,9 @@ void HuffmanStage<T>::execute(cudaStream_t stream, MemoryPool* pool, const std::
     if (need == 0) throw std::runtime_error("HuffmanStage: unsupported bklen " + std::to_string(bklen_));
     uint8_t* w = static_cast<uint8_t*>(ws_.ensure(align256(need) + kTail, pool, stream));
     uint64_t* d_size = reinterpret_cast<uint64_t*>(w + align256(need));
-    const int rc = fzb_huff_compress(static_cast<const uint16_t*>(inputs[0]), n, bklen_, outputs[0], d_size, w,
-                                     align256(need), stream);
+    const auto compress = encode_mode_ == HuffmanEncodeMode::Fine ? fzb_huff_compress_fine : fzb_huff_compress;
+    const int rc = compress(static_cast<const uint16_t*>(inputs[0]), n, bklen_, outputs[0], d_size, w,
+                            align256(need), stream);
     if (rc == FZB_E_RANGE)
         throw std::runtime_error("HuffmanStage: input contains symbols >= bklen (" + std::to_string(bklen_) +
                                  "). Increase bklen or use setZigzagCodes(true) with LorenzoQuantStage.");

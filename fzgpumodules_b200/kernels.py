@@ -252,9 +252,10 @@ def huff_book(freq, bklen: int = 1024):
 
 
 def huff_encode(codes: torch.Tensor, bk4, revbook, bklen: int = 1024, ws: Workspace | None = None,
-                trim: bool = True):
-    """GPU_coarse_encode + blob assembly with a given codebook.  Returns
-    (blob, size_tensor)."""
+                trim: bool = True, fine: bool = False):
+    """GPU_coarse_encode (or, fine=True, GPU_fine_encode with 1024-symbol
+    partitions) + blob assembly with a given codebook.  Returns (blob,
+    size_tensor)."""
     import numpy as np
     ws = ws or _default_ws
     src = codes.reshape(-1)
@@ -264,25 +265,26 @@ def huff_encode(codes: torch.Tensor, bk4, revbook, bklen: int = 1024, ws: Worksp
     out = torch.empty(int(lib().fzb_huff_max_bytes(n, bklen)), dtype=torch.uint8, device=dev)
     size = torch.zeros(1, dtype=torch.int64, device=dev)
     wp, wn = ws.get_bytes(lib().fzb_huff_workspace_bytes(n, bklen), dev)
-    check(lib().fzb_huff_encode(_ptr(src), n, bklen, _ptr(d_bk4), _ptr(d_rb), _ptr(out), _ptr(size),
-                                wp, wn, _stream(dev)), "fzb_huff_encode")
+    fn = lib().fzb_huff_encode_fine if fine else lib().fzb_huff_encode
+    check(fn(_ptr(src), n, bklen, _ptr(d_bk4), _ptr(d_rb), _ptr(out), _ptr(size), wp, wn, _stream(dev)),
+          "fzb_huff_encode")
     if trim:
         return out[: int(size.item())], size
     return out, size
 
 
 def huff_compress(codes: torch.Tensor, bklen: int = 1024, ws: Workspace | None = None,
-                  trim: bool = True):
-    """HuffmanStage<uint16_t>::execute forward (huffman_stage.cu:111-186).
-    Returns (blob, size_tensor)."""
+                  trim: bool = True, fine: bool = False):
+    """HuffmanStage<uint16_t>::execute forward (huffman_stage.cu:111-186);
+    fine=True is setEncodeMode(Fine).  Returns (blob, size_tensor)."""
     ws = ws or _default_ws
     src = codes.reshape(-1)
     n, dev = src.numel(), src.device
     out = torch.empty(int(lib().fzb_huff_max_bytes(n, bklen)), dtype=torch.uint8, device=dev)
     size = torch.zeros(1, dtype=torch.int64, device=dev)
     wp, wn = ws.get_bytes(lib().fzb_huff_workspace_bytes(n, bklen), dev)
-    check(lib().fzb_huff_compress(_ptr(src), n, bklen, _ptr(out), _ptr(size), wp, wn, _stream(dev)),
-          "fzb_huff_compress")
+    fn = lib().fzb_huff_compress_fine if fine else lib().fzb_huff_compress
+    check(fn(_ptr(src), n, bklen, _ptr(out), _ptr(size), wp, wn, _stream(dev)), "fzb_huff_compress")
     if trim:
         return out[: int(size.item())], size
     return out, size

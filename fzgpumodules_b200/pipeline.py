@@ -128,16 +128,25 @@ class RLEStage(Stage):
         return lib().fzb_pipeline_add_rle(h, self.elem)
 
 
+class HuffmanEncodeMode:
+    """HuffmanEncodeMode (coders/huffman/huffman_stage.h)."""
+    Coarse = 0
+    Fine = 1
+
+
 class HuffmanStage(Stage):
-    """HuffmanStage<uint16_t> (coders/huffman/huffman_stage.h), coarse mode."""
+    """HuffmanStage<uint16_t> (coders/huffman/huffman_stage.h), coarse or fine mode."""
 
     def __init__(self, bklen: int = 1024):
         self.bklen = bklen
+        self.encode_mode = HuffmanEncodeMode.Coarse
 
     def setBklen(self, v): self.bklen = v
 
+    def setEncodeMode(self, mode): self.encode_mode = int(mode)
+
     def _add(self, h):
-        return lib().fzb_pipeline_add_huffman(h, self.bklen)
+        return lib().fzb_pipeline_add_huffman_mode(h, self.bklen, self.encode_mode)
 
 
 class BitpackStage(Stage):

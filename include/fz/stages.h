@@ -347,7 +347,7 @@ private:
 };
 
 // ---------------------------------------------------------------------------
-// PHF Huffman (coarse mode) over 16-bit symbols.
+// PHF Huffman (coarse or fine mode) over 16-bit symbols.
 // ---------------------------------------------------------------------------
 enum class HuffmanEncodeMode { Coarse, Fine };
 
@@ -359,7 +359,8 @@ public:
     HuffmanStage() = default;
     void setBklen(uint32_t bklen) { bklen_ = bklen; }
     uint32_t getBklen() const { return bklen_; }
-    // Fine mode is not built; setting it keeps the coarse format.
+    // Fine mode (huffman_stage.cu:41, hf_buf.cc:46-49): partitions of 1024
+    // symbols instead of 768; the decoder reads the length from the blob.
     void setEncodeMode(HuffmanEncodeMode mode) { encode_mode_ = mode; }
     HuffmanEncodeMode getEncodeMode() const { return encode_mode_; }
     void setInverse(bool inv) override { is_inverse_ = inv; }

@@ -168,7 +168,7 @@ int fzb_bitpack_encode(const void* d_in, uint64_t n, int elem, int nbits, void* 
                        void* stream);
 int fzb_bitpack_decode(const void* d_in, uint64_t n, int elem, int nbits, void* d_out, void* stream);
 
-/* PHF Huffman, HuffmanStage<uint16_t> in coarse mode
+/* PHF Huffman, HuffmanStage<uint16_t> (coarse mode; fine mode below)
  * (modules/coders/huffman/huffman_stage.cu:111-205, phf/hf_hl.cc:25-160).
  * Blob layout (phf/hf.h:38-44): [128-byte header slot][revbook = int first[32],
  * int entry[32], u16 keys[bklen]][u32 par_nbit x pardeg][u32 par_entry x
@@ -203,8 +203,23 @@ int fzb_huff_encode(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint
 int fzb_huff_compress(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_out,
                       uint64_t* d_out_size, void* d_work, size_t work_bytes, void* stream);
 
+/* HuffmanStage<uint16_t> in fine mode (setEncodeMode(Fine)): Buf with use_HFR
+ * (phf/hf_buf.cc:46-58) partitions 1024 symbols; GPU_fine_encode
+ * (phf/hf_kernels.cu:145-250, 486-514) when the longest code is at most 8
+ * bits, else GPU_coarse_encode at sublen 1024 (phf/hf_hl.cc:69-103).  Same
+ * blob layout as coarse mode with sublen 1024 and pardeg = ceil(n / 1024);
+ * the bits after par_nbit in a partition's last cell are zero (the
+ * reference's ReVISIT-lite kernel leaves stale shared memory there for a
+ * partial last partition).  Same workspace and output bounds as coarse mode;
+ * fzb_huff_decode reads the partition length from the blob. */
+int fzb_huff_encode_fine(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint32_t* d_bk4,
+                         const uint8_t* d_revbook, void* d_out, uint64_t* d_out_size, void* d_work,
+                         size_t work_bytes, void* stream);
+int fzb_huff_compress_fine(const uint16_t* d_in, uint64_t n, uint32_t bklen, void* d_out,
+                           uint64_t* d_out_size, void* d_work, size_t work_bytes, void* stream);
+
 /* HuffmanStage<uint16_t> inverse (phf/hf_kernels.cu:267-298): decodes the blob
- * (4-byte aligned) into n symbols.  A header that disagrees with n / bklen or a
+ * (4-byte aligned, coarse or fine: sublen 768 or 1024) into n symbols.  A header that disagrees with n / bklen or a
  * bitstream that does not decode to exactly n symbols is reported as
  * FZB_E_MALFORMED by fzb_workspace_status(); work_bytes >= 256. */
 int fzb_huff_decode(const void* d_in, uint64_t in_bytes, uint64_t n, uint32_t bklen, uint16_t* d_out,
@@ -340,6 +355,8 @@ int fzb_pipeline_add_bitshuffle(void* pipeline, uint32_t block_size, int element
 int fzb_pipeline_add_rze(void* pipeline, uint32_t chunk_size, int levels);
 int fzb_pipeline_add_rle(void* pipeline, int elem);
 int fzb_pipeline_add_huffman(void* pipeline, uint32_t bklen);
+/* HuffmanStage with setEncodeMode: 0 Coarse, 1 Fine (huffman_stage.h). */
+int fzb_pipeline_add_huffman_mode(void* pipeline, uint32_t bklen, int encode_mode);
 int fzb_pipeline_add_bitpack(void* pipeline, int elem, int nbits);   /* nbits 0 = setAutoDetect */
 /* connect(dependent, producer, output_name); returns the buffer id. */
 int fzb_pipeline_connect(void* pipeline, int dependent, int producer, const char* output_name);

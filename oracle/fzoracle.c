@@ -805,9 +805,20 @@ size_t orc_huff_max_bytes(size_t n, uint32_t bklen) {
 static inline uint32_t shl32(uint32_t x, uint32_t s) { return s >= 32 ? 0u : x << s; }
 static inline uint32_t shr32(uint32_t x, uint32_t s) { return s >= 32 ? 0u : x >> s; }
 
+/* Coarse mode partitions 768 symbols (hf_bk.cc:28-37).  Fine mode
+ * (encode_mode = Fine, hf_buf.cc:46-49) partitions 1024: its ReVISIT-lite
+ * kernel (hf_kernels.cu:145-250) packs each partition MSB-first into the same
+ * cells the coarse deflate below produces, and when the longest code is over
+ * 8 bits it runs this coarse deflate at sublen 1024 (hf_hl.cc:69-103). */
 size_t orc_huff_encode(const uint16_t* in, size_t n, uint32_t bklen, const uint32_t* bk4,
                        const uint8_t* revbook, uint8_t* out) {
-    const size_t pardeg = (n - 1) / HUFF_SUBLEN + 1;
+    return orc_huff_encode_sub(in, n, bklen, bk4, revbook, HUFF_SUBLEN, out);
+}
+
+size_t orc_huff_encode_sub(const uint16_t* in, size_t n, uint32_t bklen, const uint32_t* bk4,
+                           const uint8_t* revbook, uint32_t sublen_, uint8_t* out) {
+    const size_t SUB = sublen_;
+    const size_t pardeg = (n - 1) / SUB + 1;
     uint32_t* nbit = (uint32_t*)malloc(4 * pardeg);
     uint32_t* ncell = (uint32_t*)malloc(4 * pardeg);
     uint32_t* entry = (uint32_t*)malloc(4 * pardeg);
@@ -815,11 +826,11 @@ size_t orc_huff_encode(const uint16_t* in, size_t n, uint32_t bklen, const uint3
     /* phase 1 fill + phase 2 deflate per partition (hf_kernels.cu:59-122) */
 #pragma omp parallel for schedule(static)
     for (size_t p = 0; p < pardeg; p++) {
-        uint32_t* ptr = cells + p * HUFF_SUBLEN;
+        uint32_t* ptr = cells + p * SUB;
         int residue = 32, total = 0;
         uint32_t bufr = 0;
-        size_t did = p * HUFF_SUBLEN;
-        for (int i = 0; i < HUFF_SUBLEN && did < n; i++, did++) {
+        size_t did = p * SUB;
+        for (size_t i = 0; i < SUB && did < n; i++, did++) {
             uint32_t word = bk4[in[did]];
             uint32_t w = word >> 27;
             uint32_t code = word & 0x7ffffffu;
@@ -860,7 +871,7 @@ size_t orc_huff_encode(const uint16_t* in, size_t n, uint32_t bklen, const uint3
     ent[4] = ent[3] + 4 * (uint32_t)pardeg;
     ent[5] = ent[4] + 4 * (uint32_t)total_ncell;
     memset(out, 0, 128);
-    int32_t bkl = (int32_t)(bklen & 0xffff), sublen = HUFF_SUBLEN, pd = (int32_t)pardeg;
+    int32_t bkl = (int32_t)(bklen & 0xffff), sublen = (int32_t)SUB, pd = (int32_t)pardeg;
     uint64_t olen = n;
     memcpy(out + 0, &bkl, 4);
     memcpy(out + 4, &sublen, 4);
@@ -873,7 +884,7 @@ size_t orc_huff_encode(const uint16_t* in, size_t n, uint32_t bklen, const uint3
     memcpy(out + ent[2], nbit, 4 * pardeg);
     memcpy(out + ent[3], entry, 4 * pardeg);
     for (size_t p = 0; p < pardeg; p++)
-        memcpy(out + ent[4] + 4 * (size_t)entry[p], cells + p * HUFF_SUBLEN, 4 * (size_t)ncell[p]);
+        memcpy(out + ent[4] + 4 * (size_t)entry[p], cells + p * SUB, 4 * (size_t)ncell[p]);
     free(nbit);
     free(ncell);
     free(entry);

@@ -118,6 +118,10 @@ size_t orc_huff_max_bytes(size_t n, uint32_t bklen);
 size_t orc_huff_encode(const uint16_t* in, size_t n, uint32_t bklen,
                        const uint32_t* bk4, const uint8_t* revbook,
                        uint8_t* out);
+/* Same blob with partitions of `sublen` symbols (1024: fine mode). */
+size_t orc_huff_encode_sub(const uint16_t* in, size_t n, uint32_t bklen,
+                           const uint32_t* bk4, const uint8_t* revbook,
+                           uint32_t sublen, uint8_t* out);
 /* Decode (phf/hf_kernels.cu:258-312).  Returns symbols written. */
 size_t orc_huff_decode(const uint8_t* blob, size_t blob_bytes, uint16_t* out,
                        size_t out_cap);

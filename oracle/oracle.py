@@ -73,6 +73,8 @@ def lib():
         L.orc_huff_max_bytes.argtypes = [sz, u32]
         L.orc_huff_encode.restype = sz
         L.orc_huff_encode.argtypes = [p, sz, u32, p, p, p]
+        L.orc_huff_encode_sub.restype = sz
+        L.orc_huff_encode_sub.argtypes = [p, sz, u32, p, p, u32, p]
         L.orc_huff_decode.restype = sz
         L.orc_huff_decode.argtypes = [p, sz, p, sz]
         L.orc_crc32.restype = u32
@@ -212,10 +214,11 @@ def huff_book(freq: np.ndarray, bklen: int = 1024):
     return bk4, rb
 
 
-def huff_encode(codes: np.ndarray, bklen: int, bk4: np.ndarray, revbook: np.ndarray):
+def huff_encode(codes: np.ndarray, bklen: int, bk4: np.ndarray, revbook: np.ndarray, sublen: int = 768):
+    """PHF blob; sublen 768 is coarse mode, 1024 fine mode (hf_buf.cc:46-49)."""
     c = np.ascontiguousarray(codes, dtype=np.uint16)
     out = np.zeros(lib().orc_huff_max_bytes(c.size, bklen), np.uint8)
-    n = lib().orc_huff_encode(_p(c), c.size, bklen, _p(bk4), _p(revbook), _p(out))
+    n = lib().orc_huff_encode_sub(_p(c), c.size, bklen, _p(bk4), _p(revbook), sublen, _p(out))
     return out[:n].copy()
 
 

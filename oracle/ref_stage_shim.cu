@@ -163,6 +163,30 @@ extern "C" int ref_bitpack_u16(const uint16_t* d_in, size_t n, int nbits, void* 
     return 0;
 }
 
+// Fine mode (setEncodeMode(Fine)).  Only whole 1024-symbol partitions are
+// passed here: for a partial last partition the reference's ReVISIT-lite
+// kernel reads symbols from shared memory it never filled.
+extern "C" int ref_huffman_u16_fine(const uint16_t* d_in, size_t n, int bklen, void* d_out,
+                                    size_t* out_bytes, uint16_t* d_dec) {
+    if (n == 0 || n % 1024 != 0) return -2;
+    GUARD_BEGIN
+    MemoryPool pool(MemoryPoolConfig(n * 2 + (size_t(1) << 22), 3.0f));
+    HuffmanStage<uint16_t> st;
+    st.setBklen((uint32_t)bklen);
+    st.setEncodeMode(HuffmanEncodeMode::Fine);
+    cudaStream_t s = 0;
+    st.execute(s, &pool, {const_cast<uint16_t*>(d_in)}, {d_out}, {n * 2});
+    if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("sync failed");
+    *out_bytes = st.getActualOutputSize(0);
+    if (d_dec) {
+        st.setInverse(true);
+        st.execute(s, &pool, {d_out}, {d_dec}, {*out_bytes});
+        if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("sync failed");
+    }
+    GUARD_END
+    return 0;
+}
+
 extern "C" int ref_huffman_u16(const uint16_t* d_in, size_t n, int bklen, void* d_out,
                                size_t* out_bytes, uint16_t* d_dec) {
     GUARD_BEGIN

@@ -177,3 +177,84 @@ def test_c3_chain_lq2d_huffman(cuda):
     assert np.array_equal(blob.cpu().numpy(), ref)
     dec = K().huff_decode(blob, codes.size, 1024)
     assert np.array_equal(dec.cpu().numpy(), codes)
+
+
+# ----------------------------------------------------------------- fine mode
+
+def _fine_cases():
+    rng = np.random.default_rng(43)
+    lap = np.clip(np.round(rng.laplace(0, 3.0, 100_000)), -511, 511).astype(np.int64)
+    return {
+        "n1": np.array([5], np.uint16),
+        "short_codes_ragged": rng.integers(0, 16, 1024 * 9 + 333).astype(np.uint16),   # longest code 4 bits
+        "short_codes_partial": rng.integers(0, 100, 1000).astype(np.uint16),           # under one partition
+        "two_symbols": (rng.integers(0, 2, 4096) * 700).astype(np.uint16),
+        "eight_bit_book": rng.integers(0, 200, 1024 * 20).astype(np.uint16),           # lengths 7-8
+        "laplace_zigzag": ((lap << 1) ^ (lap >> 63)).astype(np.uint16),                # longer codes
+        "uniform_1024_ragged": rng.integers(0, 1024, 50_001).astype(np.uint16),
+    }
+
+
+@pytest.mark.parametrize("case", list(_fine_cases()))
+def test_fine_mode_blob_decode(cuda, case):
+    """Fine mode (1024-symbol partitions): the blob equals the oracle's at
+    sublen 1024 whether the four-codes-per-word packing applies or not, and
+    decodes back."""
+    a = _fine_cases()[case]
+    bklen = 1024
+    d = torch.from_numpy(a).to(cuda)
+    freq = _hist(a, bklen)
+    bk4, rb = O.huff_book(freq, bklen)
+    ref = O.huff_encode(a, bklen, bk4, rb, sublen=1024)
+    assert ref[4:8].view(np.int32)[0] == 1024
+    blob, size = K().huff_compress(d, bklen, fine=True)
+    assert int(size.item()) == ref.size
+    assert np.array_equal(blob.cpu().numpy(), ref)
+    blob2, _ = K().huff_encode(d, bk4, rb, bklen, fine=True)
+    assert np.array_equal(blob2.cpu().numpy(), ref)
+    ws = K().Workspace()
+    dec = K().huff_decode(blob, a.size, bklen, ws=ws)
+    assert ws.status() == 0
+    assert np.array_equal(dec.cpu().numpy(), a)
+
+
+def test_fine_mode_header_disagreement_reported(cuda):
+    a = _fine_cases()["laplace_zigzag"]
+    blob, _ = K().huff_compress(torch.from_numpy(a).to(cuda), 1024, fine=True)
+    bad = blob.clone()
+    bad[4:8] = torch.tensor(np.array([1000], np.int32).view(np.uint8), device=cuda)  # neither 768 nor 1024
+    ws = K().Workspace()
+    K().huff_decode(bad, a.size, 1024, ws=ws)
+    assert ws.status() == -5
+
+
+# Whole 1024-symbol partitions only (see ref_huffman_u16_fine), and inputs
+# above the reference's small-input limit noted for coarse mode.
+@pytest.mark.parametrize("case", ["short", "eight_bit", "long_codes"])
+def test_fine_reference_stage_matches(cuda, case):
+    L = _ref()
+    if not hasattr(L, "ref_huffman_u16_fine"):
+        pytest.skip("reference stage build without the fine-mode entry")
+    rng = np.random.default_rng(44)
+    n = 1024 * 40
+    if case == "short":
+        a = rng.integers(0, 16, n).astype(np.uint16)
+    elif case == "eight_bit":
+        a = rng.integers(0, 200, n).astype(np.uint16)
+    else:
+        lap = np.clip(np.round(rng.laplace(0, 3.0, n)), -511, 511).astype(np.int64)
+        a = ((lap << 1) ^ (lap >> 63)).astype(np.uint16)
+    d = torch.from_numpy(a).to(cuda)
+    out = torch.zeros(int(O.lib().orc_huff_max_bytes(a.size, 1024)) + 4 * a.size + 4096,
+                      dtype=torch.uint8, device=cuda)
+    dec = torch.zeros(a.size, dtype=torch.uint16, device=cuda)
+    nb = C.c_size_t(0)
+    rc = L.ref_huffman_u16_fine(C.c_void_p(d.data_ptr()), C.c_size_t(a.size), 1024, C.c_void_p(out.data_ptr()),
+                                C.byref(nb), C.c_void_p(dec.data_ptr()))
+    assert rc == 0, L.ref_last_error()
+    ref = out.cpu().numpy()[: nb.value]
+    ours, _ = K().huff_compress(d, 1024, fine=True)
+    ours = ours.cpu().numpy()
+    assert ours.size == ref.size
+    assert np.array_equal(_masked(ours), _masked(ref))
+    assert np.array_equal(dec.cpu().numpy(), a)

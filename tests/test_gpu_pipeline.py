@@ -88,6 +88,8 @@ def build(chain: str, dims, eb, mode, radius, zigzag, cap=0.2, strategy=None, fu
         pl.connect(rz, bs)
     else:
         hf = pl.addStage(p.HuffmanStage(1024))
+        if chain == "huffman_fine":
+            hf.setEncodeMode(p.HuffmanEncodeMode.Fine)
         pl.connect(hf, lq, "codes")
     pl.setFusion(fusion)
     pl.finalize()
@@ -111,6 +113,7 @@ CASES = {
     "bs_rze_3d_rel": ("bs_rze", (128, 128, 64), 1e-3, 1, 32768, True, "grf"),
     "bs_rze_3d_abs_outliers": ("bs_rze", (256, 64, 32), 1e-3, 0, 512, True, "grf"),
     "huffman_2d": ("huffman", (1024, 1024, 1), 1e-3, 0, 512, True, "fractal"),
+    "huffman_fine_2d": ("huffman_fine", (1000, 1000, 1), 1e-3, 0, 512, True, "fractal"),
 }
 
 
@@ -145,7 +148,7 @@ def test_pipeline_roundtrip_and_segments(cuda, case):
         if chain == "rle":
             enc, _ = K().rle_encode(ref["codes"])
         else:
-            enc, _ = K().huff_compress(ref["codes"], 1024)
+            enc, _ = K().huff_compress(ref["codes"], 1024, fine=chain == "huffman_fine")
         assert np.array_equal(segs[3], enc.cpu().numpy())
     assert np.array_equal(segs[0].view(np.float32), ref["err"][:stored].cpu().numpy())
     assert np.array_equal(segs[1].view(np.uint32), ref["idx"][:stored].cpu().numpy().view(np.uint32))
@@ -173,7 +176,7 @@ def test_fused_equals_stage_by_stage(cuda, case):
     b.close()
 
 
-@pytest.mark.parametrize("case", ["c1_rle_2d", "bs_rze_3d_rel", "huffman_2d"])
+@pytest.mark.parametrize("case", ["c1_rle_2d", "bs_rze_3d_rel", "huffman_2d", "huffman_fine_2d"])
 def test_preallocate_equals_minimal(cuda, case):
     chain, dims, eb, mode, radius, zz, kind = CASES[case]
     x = make_field(kind, dims, cuda)

@@ -196,3 +196,63 @@ def test_histogram_skips_out_of_range():
 
 def test_crc32_known_answer():
     assert O.crc32(b"123456789") == 0xCBF43926
+
+
+def _revisit_lite_cells(sym, bk4):
+    """Cells of one full 1024-symbol partition the way the reference's fine
+    encoder builds them (phf/hf_kernels.cu:145-250): 256 shards of 4 codes,
+    each packed MSB-first into one word (reduce-merge), then 8 rounds of
+    pairwise merges in which the right group's words are shifted in behind the
+    left group's bits (shuffle-merge)."""
+    M = 0xFFFFFFFF
+    buf, cnt = [], []
+    for s in range(256):
+        acc, nb = 0, 0
+        for k in range(4):
+            w = int(bk4[sym[4 * s + k]])
+            ln, code = w >> 27, w & 0x7FFFFFF
+            if ln:
+                acc |= ((code << (32 - ln)) & M) >> nb
+            nb += ln
+        buf.append(acc)
+        cnt.append(nb)
+    stride = 1
+    for _ in range(8):
+        for left in range(0, 256, 2 * stride):
+            r = left + stride
+            units, bits = divmod(cnt[left], 32)
+            right = buf[r:r + stride]
+            buf[r:r + stride] = [0] * stride
+            for i, w in enumerate(right):
+                buf[left + units + i] |= w >> bits
+                if bits:
+                    buf[left + units + i + 1] |= (w << (32 - bits)) & M
+            cnt[left] += cnt[r]
+        stride *= 2
+    return np.array(buf[: (cnt[0] + 31) // 32], np.uint32), cnt[0]
+
+
+def test_huffman_fine_layout_equals_revisit_lite_merge():
+    """Fine mode's ReVISIT-lite shard/merge produces exactly the cells of an
+    MSB-first deflate at sublen 1024, which is what the oracle (and the GPU
+    coder) write for fine mode; checked on full partitions of books whose
+    longest code is at most 8 bits."""
+    rng = np.random.default_rng(7)
+    cases = [rng.integers(0, hi, 1024 * 3).astype(np.uint16) for hi in (2, 16, 60)]
+    cases.append(rng.permutation(np.repeat(np.arange(256), 12)).astype(np.uint16))  # every code 8 bits
+    for a in cases:
+        freq = np.bincount(a, minlength=1024).astype(np.uint32)
+        bk4, rb = O.huff_book(freq, 1024)
+        assert int((bk4[freq > 0] >> 27).max()) <= 8
+        blob = O.huff_encode(a, 1024, bk4, rb, sublen=1024)
+        ent = blob[40:64].view(np.uint32)
+        pd = int(blob[8:12].view(np.int32)[0])
+        assert pd == 3 and int(blob[4:8].view(np.int32)[0]) == 1024
+        nbit = blob[ent[2]:ent[3]].view(np.uint32)
+        pent = blob[ent[3]:ent[4]].view(np.uint32)
+        bits = blob[ent[4]:ent[5]].view(np.uint32)
+        for p in range(pd):
+            cells, nb = _revisit_lite_cells(a[1024 * p:1024 * (p + 1)], bk4)
+            assert nb == int(nbit[p])
+            assert np.array_equal(bits[int(pent[p]):int(pent[p]) + cells.size], cells)
+        assert np.array_equal(O.huff_decode(blob, a.size), a)
