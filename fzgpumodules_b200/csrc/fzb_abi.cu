@@ -392,7 +392,7 @@ int fzb_lq_inverse(const uint16_t* d_codes, const float* d_err, const uint32_t* 
 
 int fzb_bitshuffle(const void* d_in, uint64_t bytes, uint32_t block, int ew, int inverse,
                    void* d_out, void* stream) {
-    if (!d_in || !d_out || (ew != 1 && ew != 2)) return FZB_E_INVALID;
+    if (!d_in || !d_out || (ew != 1 && ew != 2 && ew != 4 && ew != 8)) return FZB_E_INVALID;
     if (block == 0 || block % (1024u * (uint32_t)ew) != 0) return FZB_E_INVALID;
     cudaStream_t s = S(stream);
     const uint64_t nfull = bytes / block;
@@ -402,6 +402,10 @@ int fzb_bitshuffle(const void* d_in, uint64_t bytes, uint32_t block, int ew, int
         if (ew == 2 && block == (uint32_t)kChunkBytes &&
             ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0) {
             bitshuffle2_kernel<<<(unsigned)nfull, kThreads, 0, s>>>(in, out, inverse);
+        } else if (ew == 4 || ew == 8) {
+            if (((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & (uintptr_t)(ew - 1)) != 0)
+                return FZB_E_INVALID;  // the reference reads and writes u32 / u64 words
+            if (launch_bitshuffle_wide(in, out, nfull, block, ew, inverse, s) != 0) return FZB_E_CUDA;
         } else {
             const uint32_t nchunk = block / (uint32_t)ew;
             bitshuffle_ballot_kernel<<<(unsigned)nfull, nchunk < 1024 ? nchunk : 1024, 0, s>>>(

@@ -1098,6 +1098,102 @@ __global__ void bitshuffle_ballot_kernel(const uint8_t* __restrict__ in, uint8_t
     }
 }
 
+// Element widths 4 and 8 (the reference's butterfly kernels,
+// bitshuffle_stage.cu:66-110 and :175-278): plane p holds bit W-1-p; a plane
+// word (u32 for width 4, u64 for width 8) covers a group of 32 / 64
+// elements with element e at the word's top bit minus e.  A warp handles one
+// group per step: lane l loads element l (width 8: also l + 32), a 5-stage
+// shuffle transpose (plus a register swap stage for 64 rows) gives lane j
+// column j, and the plane word of plane p is column W-1-p bit-reversed,
+// taken from lane 31-p.  The inverse runs the same steps backwards.
+template <int EW>
+__device__ __forceinline__ uint64_t bs_lo_mask(int s) {
+    const uint32_t m = s == 16 ? 0x0000ffffu : s == 8 ? 0x00ff00ffu : s == 4 ? 0x0f0f0f0fu : s == 2 ? 0x33333333u
+                                                                                                : 0x55555555u;
+    return EW == 4 ? (uint64_t)m : ((uint64_t)m << 32) | m;
+}
+
+// Transpose of the 32 x 32 bit matrix whose row l is lane l's word.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, uint32_t lane) {
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const uint32_t m = (uint32_t)bs_lo_mask<4>(s);
+        const uint32_t q = __shfl_xor_sync(0xffffffffu, x, s);
+        x = (lane & s) ? ((x & ~m) | ((q & ~m) >> s)) : ((x & m) | ((q & m) << s));
+    }
+    return x;
+}
+
+// Transpose of the 64 x 64 bit matrix whose rows l and l + 32 are lane l's
+// a0 and a1; afterwards a0 / a1 of lane j are columns j / j + 32.
+__device__ __forceinline__ void warp_transpose64(uint64_t& a0, uint64_t& a1, uint32_t lane) {
+    const uint64_t lo = 0x00000000ffffffffull;
+    const uint64_t n0 = (a0 & lo) | ((a1 & lo) << 32), n1 = (a1 & ~lo) | ((a0 & ~lo) >> 32);
+    a0 = n0;
+    a1 = n1;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const uint64_t m = bs_lo_mask<8>(s);
+        const uint64_t q0 = __shfl_xor_sync(0xffffffffu, a0, s), q1 = __shfl_xor_sync(0xffffffffu, a1, s);
+        if (lane & s) {
+            a0 = (a0 & ~m) | ((q0 & ~m) >> s);
+            a1 = (a1 & ~m) | ((q1 & ~m) >> s);
+        } else {
+            a0 = (a0 & m) | ((q0 & m) << s);
+            a1 = (a1 & m) | ((q1 & m) << s);
+        }
+    }
+}
+
+template <int EW>
+__global__ void __launch_bounds__(1024) bitshuffle_wide_kernel(const uint8_t* __restrict__ in,
+                                                               uint8_t* __restrict__ out, uint32_t block,
+                                                               int inverse) {
+    constexpr uint32_t GW = EW == 4 ? 32u : 64u;  // elements per plane word
+    const uint32_t n_chunk = block / EW, npp = n_chunk / GW, groups = n_chunk / GW;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t rl = 31 - lane;
+    if (EW == 4) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(in + (size_t)blockIdx.x * block);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(out + (size_t)blockIdx.x * block);
+        for (uint32_t g = warp; g < groups; g += nwarps) {
+            if (!inverse) {
+                const uint32_t t = warp_transpose32(__ldg(src + GW * g + lane), lane);
+                dst[(size_t)lane * npp + g] = __brev(__shfl_sync(0xffffffffu, t, rl));
+            } else {
+                const uint32_t t = __shfl_sync(0xffffffffu, __brev(__ldg(src + (size_t)lane * npp + g)), rl);
+                dst[GW * g + lane] = warp_transpose32(t, lane);
+            }
+        }
+    } else {
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(in + (size_t)blockIdx.x * block);
+        uint64_t* dst = reinterpret_cast<uint64_t*>(out + (size_t)blockIdx.x * block);
+        for (uint32_t g = warp; g < groups; g += nwarps) {
+            if (!inverse) {
+                uint64_t a0 = __ldg(src + GW * g + lane), a1 = __ldg(src + GW * g + 32 + lane);
+                warp_transpose64(a0, a1, lane);
+                const uint64_t r0 = __shfl_sync(0xffffffffu, a0, rl), r1 = __shfl_sync(0xffffffffu, a1, rl);
+                dst[(size_t)lane * npp + g] = __brevll(r1);          // plane lane: column 63 - lane
+                dst[(size_t)(lane + 32) * npp + g] = __brevll(r0);   // plane lane + 32: column 31 - lane
+            } else {
+                const uint64_t w0 = __ldg(src + (size_t)lane * npp + g), w1 = __ldg(src + (size_t)(lane + 32) * npp + g);
+                uint64_t a1 = __shfl_sync(0xffffffffu, __brevll(w0), rl);
+                uint64_t a0 = __shfl_sync(0xffffffffu, __brevll(w1), rl);
+                warp_transpose64(a0, a1, lane);
+                dst[GW * g + lane] = a0;
+                dst[GW * g + 32 + lane] = a1;
+            }
+        }
+    }
+}
+
+int launch_bitshuffle_wide(const uint8_t* in, uint8_t* out, uint64_t nfull, uint32_t block, int ew, int inverse,
+                           cudaStream_t s) {
+    if (ew == 4) bitshuffle_wide_kernel<4><<<(unsigned)nfull, 1024, 0, s>>>(in, out, block, inverse);
+    else bitshuffle_wide_kernel<8><<<(unsigned)nfull, 1024, 0, s>>>(in, out, block, inverse);
+    return (int)cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // Standalone RZE encode of a byte stream (rze_stage.cu:774-843 semantics,
 // one pass: chunk encode + look-back placement).

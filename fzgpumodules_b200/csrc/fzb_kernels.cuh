@@ -102,6 +102,9 @@ int launch_lq3d_tma(const FwdArgs& a, unsigned grid, cudaStream_t s);
 __global__ void bitshuffle2_kernel(const uint8_t* in, uint8_t* out, int inverse);
 __global__ void bitshuffle_ballot_kernel(const uint8_t* in, uint8_t* out, uint32_t block, int ew,
                                          int inverse);
+// Element widths 4 and 8: one CTA per block (fzb_forward.cu).
+int launch_bitshuffle_wide(const uint8_t* in, uint8_t* out, uint64_t nfull, uint32_t block, int ew, int inverse,
+                           cudaStream_t s);
 __global__ void rze_encode_kernel(RzeEncArgs a);
 __global__ void assemble_scan_kernel(AsmArgs a);
 __global__ void assemble_copy_kernel(AsmArgs a);  // one warp per chunk, grid-stride

@@ -279,11 +279,11 @@ void BitshuffleStage::execute(cudaStream_t stream, MemoryPool*, const std::vecto
                               const std::vector<void*>& outputs, const std::vector<size_t>& sizes) {
     if (inputs.empty() || outputs.empty() || sizes.empty())
         throw std::runtime_error("BitshuffleStage: invalid inputs/outputs");
-    if (element_width_ != 1 && element_width_ != 2)
-        throw std::runtime_error("BitshuffleStage: element width " + std::to_string(element_width_) +
-                                 " is not supported by the sm_100a kernels (1 or 2)");
+    // bitshuffle_stage.h:139-150
+    if (element_width_ != 1 && element_width_ != 2 && element_width_ != 4 && element_width_ != 8)
+        throw std::invalid_argument("BitshuffleStage: element_width must be 1, 2, 4, or 8");
     if (block_size_ == 0 || block_size_ % (1024u * element_width_) != 0)
-        throw std::runtime_error("BitshuffleStage: block size must be a multiple of 1024 * element width");
+        throw std::invalid_argument("BitshuffleStage: block_size must be a positive multiple of 1024 * element_width");
     actual_ = sizes[0];
     if (sizes[0] == 0) return;
     check(fzb_bitshuffle(inputs[0], sizes[0], block_size_, element_width_, is_inverse_ ? 1 : 0, outputs[0],

@@ -91,7 +91,9 @@ int fzb_lq_inverse(const uint16_t* d_codes, const float* d_err, const uint32_t* 
                    void* d_work, size_t work_bytes, void* stream);
 
 /* BitshuffleStage::execute (modules/shufflers/bitshuffle/bitshuffle_stage.cu
- * :355-475).  ew = 1 or 2; block a positive multiple of 1024*ew. */
+ * :355-475).  ew = 1, 2, 4 or 8; block a positive multiple of 1024*ew;
+ * for ew 4 / 8 the buffers are ew-byte aligned.  Widths 1-2 use the ballot
+ * layout (:299-349), widths 4-8 the butterfly layout (:66-278). */
 int fzb_bitshuffle(const void* d_in, uint64_t bytes, uint32_t block, int ew, int inverse,
                    void* d_out, void* stream);
 

@@ -303,33 +303,51 @@ void orc_lq_inv(const uint16_t* codes, size_t n_total, const float* out_err,
 /* Bitshuffle                                                          */
 /* ------------------------------------------------------------------ */
 
+/* Plane p holds bit W-1-p of every element of the block.  Element widths 1
+ * and 2 (bitshuffle_stage.cu:299-349, ballot kernels): plane words are u32,
+ * element 32g+e at bit e of word g.  Widths 4 and 8 (the butterfly kernels,
+ * :66-110 and :175-278): plane words are u32 / u64 and element e of a group
+ * sits at the word's bit W'-1-e (W' = 32 / 64), i.e. the group order is
+ * reversed inside the word. */
+static inline size_t bs_slot(uint32_t ew, uint32_t W, uint32_t nchunk, uint32_t i, uint32_t bit, int* pos) {
+    if (ew <= 2) {
+        *pos = (int)(i % 32);
+        return (size_t)(W - 1 - bit) * (nchunk / 32) * 4 + (size_t)(i / 32) * 4;  /* byte offset of the u32 word */
+    }
+    const uint32_t gw = ew == 4 ? 32u : 64u;  /* elements per plane word */
+    *pos = (int)(gw - 1 - i % gw);
+    return (size_t)(W - 1 - bit) * (nchunk / gw) * (gw / 8) + (size_t)(i / gw) * (gw / 8);
+}
+
 void orc_bitshuffle(const uint8_t* in, size_t bytes, uint32_t block, int ew,
                     int inverse, uint8_t* out) {
     const size_t nfull = bytes / block;
     const uint32_t W = (uint32_t)ew * 8u;
     const uint32_t nchunk = block / (uint32_t)ew; /* elements per block */
-    const uint32_t npp = nchunk / 32u;             /* words per plane */
 #pragma omp parallel for schedule(static)
     for (size_t b = 0; b < nfull; b++) {
         const uint8_t* src = in + b * block;
         uint8_t* dst = out + b * block;
         if (!inverse) {
-            uint32_t* o = (uint32_t*)dst;
-            memset(o, 0, block);
+            memset(dst, 0, block);
             for (uint32_t i = 0; i < nchunk; i++) {
                 uint64_t val = 0;
                 memcpy(&val, src + (size_t)i * ew, (size_t)ew);
                 for (uint32_t bit = 0; bit < W; bit++)
-                    if ((val >> bit) & 1u)
-                        o[(W - 1 - bit) * npp + i / 32] |= 1u << (i % 32);
+                    if ((val >> bit) & 1u) {
+                        int pos;
+                        const size_t off = bs_slot((uint32_t)ew, W, nchunk, i, bit, &pos);
+                        dst[off + (size_t)(pos / 8)] |= (uint8_t)(1u << (pos % 8));
+                    }
             }
         } else {
-            const uint32_t* w = (const uint32_t*)src;
             for (uint32_t i = 0; i < nchunk; i++) {
                 uint64_t val = 0;
-                for (uint32_t bit = 0; bit < W; bit++)
-                    if ((w[(W - 1 - bit) * npp + i / 32] >> (i % 32)) & 1u)
-                        val |= (uint64_t)1 << bit;
+                for (uint32_t bit = 0; bit < W; bit++) {
+                    int pos;
+                    const size_t off = bs_slot((uint32_t)ew, W, nchunk, i, bit, &pos);
+                    if ((src[off + (size_t)(pos / 8)] >> (pos % 8)) & 1u) val |= (uint64_t)1 << bit;
+                }
                 memcpy(dst + (size_t)i * ew, &val, (size_t)ew);
             }
         }

@@ -138,7 +138,7 @@ def test_lq_inverse_matches_oracle(cuda, dims):
     assert np.max(np.abs(y - x)) <= 1e-3 * 1.01
 
 
-@pytest.mark.parametrize("ew", [1, 2])
+@pytest.mark.parametrize("ew", [1, 2, 4, 8])
 def test_bitshuffle_matches_oracle(cuda, ew):
     rng = np.random.default_rng(13)
     d = rng.integers(0, 256, 16384 * 5 + 300, dtype=np.uint8)
@@ -149,6 +149,30 @@ def test_bitshuffle_matches_oracle(cuda, ew):
     assert np.array_equal(_h(back), d)
     s2 = kern().bitshuffle(_g(d[: 8192 * 3], cuda), 8192, ew)  # non-default block
     assert np.array_equal(_h(s2), O.bitshuffle(d[: 8192 * 3], 8192, ew))
+    s3 = kern().bitshuffle(_g(d, cuda), 65536, ew)  # larger block, ragged tail
+    assert np.array_equal(_h(s3), O.bitshuffle(d, 65536, ew))
+    assert np.array_equal(_h(kern().bitshuffle(s3, 65536, ew, inverse=True)), d)
+
+
+@pytest.mark.parametrize("ew", [1, 2, 4, 8])
+def test_reference_bitshuffle_widths(cuda, ew):
+    """The reference's own BitshuffleStage (ballot kernels for widths 1-2,
+    butterfly kernels for 4-8) equals the oracle and ours, both ways."""
+    L = _ref()
+    rng = np.random.default_rng(15 + ew)
+    d = rng.integers(0, 256, 16384 * 4, dtype=np.uint8)
+    d[:16384] &= 0x11
+    din = _g(d, cuda)
+    for block in (16384, 8192 * ew):
+        ref = torch.empty_like(din)
+        assert L.ref_bitshuffle(_vp(din), C.c_size_t(d.size), block, ew, 0, _vp(ref)) == 0, L.ref_last_error()
+        want = O.bitshuffle(d, block, ew)
+        assert np.array_equal(_h(ref), want)
+        ours = kern().bitshuffle(din, block, ew)
+        assert np.array_equal(_h(ours), want)
+        back = torch.empty_like(din)
+        assert L.ref_bitshuffle(_vp(ref), C.c_size_t(d.size), block, ew, 1, _vp(back)) == 0, L.ref_last_error()
+        assert np.array_equal(_h(back), d)
 
 
 def _byte_cases():

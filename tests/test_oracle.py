@@ -78,9 +78,37 @@ def test_bitshuffle_msb_plane_known_answer():
     b = np.full(16384, 0x80, np.uint8)
     s = O.bitshuffle(b, 16384, 1).view(np.uint32)
     assert np.all(s[:512] == 0xFFFFFFFF) and np.all(s[512:] == 0)
+    # width 4, the reference's own case (test_bitshuffle_stage.cpp:336-374):
+    # 1024 elements with only bit 31 set -> plane 0 (32 words) all ones
+    c = np.full(1024, 0x80000000, np.uint32)
+    s = O.bitshuffle(c.view(np.uint8), 4096, 4).view(np.uint32)
+    assert np.all(s[:32] == 0xFFFFFFFF) and np.all(s[32:] == 0)
+    e = np.full(1024, 1 << 63, np.uint64)
+    s = O.bitshuffle(e.view(np.uint8), 8192, 8).view(np.uint64)
+    assert np.all(s[:16] == np.uint64(0xFFFFFFFFFFFFFFFF)) and np.all(s[16:] == 0)
 
 
-@pytest.mark.parametrize("ew", [1, 2])
+def test_bitshuffle_wide_word_order():
+    """Widths 4 and 8 (the reference's butterfly kernels): element e of a
+    32- / 64-element group sits at the plane word's bit 31-e / 63-e, the
+    reverse of the ballot kernels' order for widths 1 and 2."""
+    c = np.zeros(1024, np.uint32)
+    c[0] = 1          # element 0, bit 0 -> plane 31, word 0, bit 31
+    c[33] = 1 << 5    # element 33 (group 1, e = 1), bit 5 -> plane 26, word 1, bit 30
+    s = O.bitshuffle(c.view(np.uint8), 4096, 4).view(np.uint32).reshape(32, 32)
+    assert s[31, 0] == 1 << 31 and s[26, 1] == 1 << 30
+    assert np.count_nonzero(s) == 2
+    e = np.zeros(1024, np.uint64)
+    e[65] = 1 << 40   # group 1, e = 1, bit 40 -> plane 23, word 1, bit 62
+    s = O.bitshuffle(e.view(np.uint8), 8192, 8).view(np.uint64).reshape(64, 16)
+    assert s[23, 1] == np.uint64(1 << 62) and np.count_nonzero(s) == 1
+    a = np.zeros(8192, np.uint16)
+    a[1] = 1          # width 2: element 1, bit 0 -> plane 15, word 0, bit 1
+    s = O.bitshuffle(a, 16384, 2).view(np.uint32).reshape(16, 256)
+    assert s[15, 0] == 2 and np.count_nonzero(s) == 1
+
+
+@pytest.mark.parametrize("ew", [1, 2, 4, 8])
 def test_bitshuffle_invariants_and_roundtrip(ew):
     rng = np.random.default_rng(4)
     for fill in (0x00, 0xFF):  # zeros -> zeros, 0xFF -> 0xFF (:235-292)
