@@ -254,7 +254,7 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
     const AsmArgs m = asm_args(w, a, fused, d_rze, d_rze_size, d_err, d_idx, d_count);
     {
         TraceScope ts(s, "assemble_scan");
-        assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
+        if (launch_assemble_scan(m, s) != 0) return FZB_E_CUDA;
     }
     CK(cudaGetLastError());
     {
@@ -450,7 +450,7 @@ int fzb_rze_encode(const void* d_in, uint64_t bytes, void* d_out, uint64_t* d_ou
     m.out = static_cast<uint8_t*>(d_out);
     m.out_size = reinterpret_cast<unsigned long long*>(d_out_size);
     m.pay_off = w.in_off;
-    assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
+    if (launch_assemble_scan(m, s) != 0) return FZB_E_CUDA;
     CK(cudaGetLastError());
     assemble_copy_kernel<<<copy_grid(nch), 256, 0, s>>>(m);
     CK(cudaGetLastError());
@@ -467,8 +467,9 @@ int fzb_rze_decode(const void* d_in, uint64_t in_bytes, uint64_t orig_bytes, voi
     if (!d_work || work_bytes < w.need) return FZB_E_WORKSPACE;
     cudaStream_t s = S(stream);
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
-    rze_prepass_kernel<<<1, 1024, 0, s>>>(static_cast<const uint8_t*>(d_in), in_bytes, (uint32_t)nch,
-                                          (uint32_t)orig_bytes, w.in_off, w.err);
+    if (launch_rze_prepass(static_cast<const uint8_t*>(d_in), in_bytes, (uint32_t)nch, (uint32_t)orig_bytes,
+                           w.in_off, w.err, s) != 0)
+        return FZB_E_CUDA;
     CK(cudaGetLastError());
     InvArgs a{};
     a.rze = static_cast<const uint8_t*>(d_in);
@@ -502,8 +503,9 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
     {
         TraceScope ts(s, "rze_prepass");
-        rze_prepass_kernel<<<1, 1024, 0, s>>>(static_cast<const uint8_t*>(d_rze), rze_bytes,
-                                              (uint32_t)nch, (uint32_t)(2 * n_total), w.in_off, w.err);
+        if (launch_rze_prepass(static_cast<const uint8_t*>(d_rze), rze_bytes, (uint32_t)nch,
+                               (uint32_t)(2 * n_total), w.in_off, w.err, s) != 0)
+            return FZB_E_CUDA;
     }
     CK(cudaGetLastError());
     InvArgs a = inv_args(w, g, n_total);

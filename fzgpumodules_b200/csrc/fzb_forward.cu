@@ -323,17 +323,17 @@ __device__ __forceinline__ void write_slot(uint8_t* __restrict__ slots, uint32_t
 
 // Exclusive scans over chunks (one CTA of 1024 threads): payload offsets,
 // outlier offsets, RZE header, total sizes.
-__device__ __forceinline__ void assemble_scan_body(const AsmArgs& a) {
-    // Tiles of 4096 chunks: coalesced loads into shared memory, 4 chunks per
-    // thread, a warp-shuffle block scan, coalesced writes, carry to the next tile.
-    constexpr uint32_t kTile = 4096, kPer = kTile / 1024;
-    __shared__ uint32_t sp[kTile], so[kTile];
+template <uint32_t kTile>
+__device__ __forceinline__ void assemble_scan_body(const AsmArgs& a, uint32_t* sp, uint32_t* so) {
+    // Tiles of kTile chunks: loads issued in batches of eight per thread (all
+    // in flight at once) into shared memory, kTile/1024 chunks per thread, a
+    // warp-shuffle block scan, coalesced writes, carry to the next tile.
+    constexpr uint32_t kPer = kTile / 1024;
     __shared__ uint32_t wp[32], wo[32], s_tile[2];
     const uint32_t n = a.n_chunks, t = threadIdx.x, lane = t & 31, warp = t >> 5;
     // outliers that found room in staging (an overflowing run keeps those,
     // the count still reports every outlier found)
-    auto staged = [&](uint32_t i) -> uint32_t {
-        const uint32_t b0 = a.obase[i], n0 = a.ocnt[i];
+    auto staged = [&](uint32_t b0, uint32_t n0) -> uint32_t {
         return b0 >= a.ostage_cap ? 0u : min(n0, a.ostage_cap - b0);
     };
     uint32_t* hdr = reinterpret_cast<uint32_t*>(a.out);
@@ -341,17 +341,25 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a) {
     uint32_t carry_o = 0, ot = 0;
     for (uint32_t t0 = 0; t0 < n; t0 += kTile) {
         const uint32_t cnt = min(kTile, n - t0);
-        for (uint32_t i = t; i < kTile; i += 1024) {
-            uint32_t vp = 0, vo = 0;
-            if (i < cnt) {
-                if (a.sizes) vp = a.sizes[t0 + i] & 0x7fffffffu;
-                if (a.ocnt) {
-                    vo = staged(t0 + i);
-                    ot += a.ocnt[t0 + i];
-                }
+        for (uint32_t j0 = 0; j0 < kPer; j0 += (kPer < 8 ? kPer : 8)) {
+            constexpr uint32_t kB = kPer < 8 ? kPer : 8;
+            uint32_t vs[kB], vb[kB], vc[kB];
+#pragma unroll
+            for (uint32_t j = 0; j < kB; j++) {
+                const uint32_t i = t + 1024u * (j0 + j);
+                const bool in = i < cnt;
+                vs[j] = (in && a.sizes) ? a.sizes[t0 + i] : 0u;
+                vb[j] = (in && a.ocnt) ? a.obase[t0 + i] : 0u;
+                vc[j] = (in && a.ocnt) ? a.ocnt[t0 + i] : 0u;
             }
-            sp[i] = vp;
-            so[i] = vo;
+#pragma unroll
+            for (uint32_t j = 0; j < kB; j++) {
+                const uint32_t i = t + 1024u * (j0 + j);
+                sp[i] = vs[j] & 0x7fffffffu;
+                so[i] = a.ocnt ? staged(vb[j], vc[j]) : 0u;
+                ot += vc[j];
+                if (a.sizes && i < cnt) hdr[2 + t0 + i] = vs[j];  // the stream's size table
+            }
         }
         __syncthreads();
         uint32_t lp = 0, lo = 0;
@@ -404,10 +412,7 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a) {
         }
         __syncthreads();
         for (uint32_t i = t; i < cnt; i += 1024) {
-            if (a.sizes) {
-                a.pay_off[t0 + i] = carry_p + sp[i];
-                hdr[2 + t0 + i] = a.sizes[t0 + i];
-            }
+            if (a.sizes) a.pay_off[t0 + i] = carry_p + sp[i];
             if (a.ocnt) a.ofin[t0 + i] = carry_o + so[i];
         }
         carry_p += s_tile[0];
@@ -432,7 +437,19 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a) {
     }
 }
 
-__global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) { assemble_scan_body(a); }
+__global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) {
+    extern __shared__ uint32_t asm_dyn[];
+    assemble_scan_body<kAsmTile>(a, asm_dyn, asm_dyn + kAsmTile);
+}
+
+int launch_assemble_scan(const AsmArgs& a, cudaStream_t s) {
+    const int smem = (int)(2 * kAsmTile * sizeof(uint32_t));
+    static SmemAttr attr;
+    const cudaError_t e = ensure_dyn_smem(attr, (const void*)assemble_scan_kernel, smem);
+    if (e != cudaSuccess) return (int)e;
+    assemble_scan_kernel<<<1, 1024, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
 
 // One chunk per group of `nth` threads (thread `tid` of the group): payload
 // from its slot to the final stream position
@@ -455,11 +472,20 @@ __device__ __forceinline__ void assemble_copy_body(const AsmArgs& a, const uint3
             if (tid < tail) dst[(a1 - d0) + tid] = src[(a1 - d0) + tid];
             uint32_t* dw = reinterpret_cast<uint32_t*>(a0);
             const uint32_t nw = (uint32_t)((a1 - a0) >> 2), r = head & 3;
-            for (uint32_t i = tid; i < nw; i += nth) {
-                const uint32_t w0 = (head + 4 * i) >> 2;  // source word of destination word i
-                const uint32_t lo = __ldg(s32 + w0);
-                const uint32_t hi = r ? __ldg(s32 + w0 + 1) : 0u;
-                dw[i] = r ? __funnelshift_r(lo, hi, 8 * r) : lo;
+            for (uint32_t i0 = tid; i0 < nw; i0 += 4 * nth) {  // four words per thread in flight
+                uint32_t lo[4], hi[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const uint32_t i = i0 + k * nth;
+                    const uint32_t w0 = (head + 4 * i) >> 2;  // source word of destination word i
+                    lo[k] = i < nw ? __ldg(s32 + w0) : 0u;
+                    hi[k] = (i < nw && r) ? __ldg(s32 + w0 + 1) : 0u;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const uint32_t i = i0 + k * nth;
+                    if (i < nw) dw[i] = r ? __funnelshift_r(lo[k], hi[k], 8 * r) : lo[k];
+                }
             }
         }
     }
@@ -787,7 +813,8 @@ __global__ void __launch_bounds__(256) batch_minmax_kernel(BatchArgs b) {
 }
 
 __global__ void __launch_bounds__(1024) batch_assemble_scan_kernel(BatchArgs b) {
-    assemble_scan_body(b.fields[blockIdx.x].m);
+    __shared__ uint32_t sp[4096], so[4096];
+    assemble_scan_body<4096>(b.fields[blockIdx.x].m, sp, so);
 }
 
 __global__ void __launch_bounds__(256) batch_assemble_copy_kernel(BatchArgs b) {

@@ -15,10 +15,11 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
                                                            uint32_t orig_expect,
                                                            unsigned long long* __restrict__ in_off,
                                                            uint32_t* err) {
-    // Tiles of 4096 size words: coalesced loads into shared memory, 4 per
-    // thread, a warp-shuffle block scan, coalesced writes, carry between tiles.
-    constexpr uint32_t kTile = 4096, kPer = kTile / 1024;
-    __shared__ uint32_t sz[kTile];
+    // Tiles of kAsmTile size words: loads issued in batches of eight per
+    // thread (all in flight at once) into shared memory, 16 per thread, a
+    // warp-shuffle block scan, coalesced writes, carry between tiles.
+    constexpr uint32_t kTile = kAsmTile, kPer = kTile / 1024;
+    extern __shared__ uint32_t sz[];
     __shared__ uint32_t wsum[32], s_tile;
     const uint32_t* h = reinterpret_cast<const uint32_t*>(rze);
     const uint32_t n = n_expect, t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -32,7 +33,16 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
     unsigned long long carry = hdr;
     for (uint32_t t0 = 0; t0 < n; t0 += kTile) {
         const uint32_t cnt = min(kTile, n - t0);
-        for (uint32_t i = t; i < kTile; i += 1024) sz[i] = i < cnt ? (h[2 + t0 + i] & 0x7fffffffu) : 0u;
+        for (uint32_t j0 = 0; j0 < kPer; j0 += 8) {
+            uint32_t v[8];
+#pragma unroll
+            for (uint32_t j = 0; j < 8; j++) {
+                const uint32_t i = t + 1024u * (j0 + j);
+                v[j] = i < cnt ? h[2 + t0 + i] : 0u;
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < 8; j++) sz[t + 1024u * (j0 + j)] = v[j] & 0x7fffffffu;
+        }
         __syncthreads();
         uint32_t l = 0;
 #pragma unroll
@@ -73,6 +83,16 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
         in_off[n] = carry;
         if (carry > rze_bytes) atomicOr(err, kErrMalformed);
     }
+}
+
+int launch_rze_prepass(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect, uint32_t orig_expect,
+                       unsigned long long* in_off, uint32_t* err, cudaStream_t s) {
+    const int smem = (int)(kAsmTile * sizeof(uint32_t));
+    static SmemAttr attr;
+    const cudaError_t e = ensure_dyn_smem(attr, (const void*)rze_prepass_kernel, smem);
+    if (e != cudaSuccess) return (int)e;
+    rze_prepass_kernel<<<1, 1024, smem, s>>>(rze, rze_bytes, n_expect, orig_expect, in_off, err);
+    return (int)cudaGetLastError();
 }
 
 // Per-chunk start of the (index-sorted) outlier list, and a sortedness check.

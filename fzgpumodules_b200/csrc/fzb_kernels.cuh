@@ -4,7 +4,25 @@
 
 #include "fzb_rze.cuh"
 
+#include <atomic>
+
 namespace fzb {
+
+// Raises a kernel's dynamic shared memory limit once per device: the
+// attribute outlasts the call, so later launches skip the driver call.  One
+// SmemAttr per kernel (a static at the launch site); devices past the eighth
+// set it on every call.
+struct SmemAttr {
+    std::atomic<int> bytes[8] = {};
+};
+inline cudaError_t ensure_dyn_smem(SmemAttr& st, const void* func, int bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    if (dev >= 0 && dev < 8 && st.bytes[dev].load(std::memory_order_relaxed) >= bytes) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && dev >= 0 && dev < 8) st.bytes[dev].store(bytes, std::memory_order_relaxed);
+    return e;
+}
 
 struct FwdArgs {
     const float* in;
@@ -107,6 +125,8 @@ int launch_bitshuffle_wide(const uint8_t* in, uint8_t* out, uint64_t nfull, uint
                            cudaStream_t s);
 __global__ void rze_encode_kernel(RzeEncArgs a);
 __global__ void assemble_scan_kernel(AsmArgs a);
+constexpr uint32_t kAsmTile = 16384;  // chunks per tile of the single-CTA assembly scan (shared memory: 2 words each)
+int launch_assemble_scan(const AsmArgs& a, cudaStream_t s);
 __global__ void assemble_copy_kernel(AsmArgs a);  // one warp per chunk, grid-stride
 inline unsigned copy_grid(uint64_t n_chunks) {
     const uint64_t g = (n_chunks + 7) / 8;
@@ -115,6 +135,8 @@ inline unsigned copy_grid(uint64_t n_chunks) {
 
 __global__ void rze_prepass_kernel(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect,
                                    uint32_t orig_expect, unsigned long long* in_off, uint32_t* err);
+int launch_rze_prepass(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect, uint32_t orig_expect,
+                       unsigned long long* in_off, uint32_t* err, cudaStream_t s);
 __global__ void outlier_ranges_kernel(const uint32_t* idx, const uint32_t* count, uint32_t cap,
                                       uint32_t n_chunks, uint32_t* ostart, uint32_t* err);
 __global__ void rze_decode_kernel(InvArgs a);

@@ -95,7 +95,7 @@ extern "C" int fzb_rze_encode_noalloc(const void* d_in, uint64_t bytes, void* d_
     m.out = static_cast<uint8_t*>(d_out);
     m.out_size = reinterpret_cast<unsigned long long*>(d_out_size);
     m.pay_off = reinterpret_cast<unsigned long long*>(scratch + kPayOff);
-    assemble_scan_kernel<<<1, 1024, 0, s>>>(m);
+    if (launch_assemble_scan(m, s) != 0) return FZB_E_CUDA;
     if (cudaGetLastError() != cudaSuccess) return FZB_E_CUDA;
     assemble_copy_kernel<<<copy_grid(nch), 256, 0, s>>>(m);
     if (cudaGetLastError() != cudaSuccess) return FZB_E_CUDA;

@@ -550,11 +550,13 @@ int launch_lq3d_tma(const FwdArgs& a, unsigned grid, cudaStream_t s) {
     grid = grid < units ? grid : units;
     cudaError_t e;
     if (a.zigzag) {
-        e = cudaFuncSetAttribute(lq3d_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem);
+        static SmemAttr attr;
+        e = ensure_dyn_smem(attr, (const void*)lq3d_tma_kernel<true>, (int)kSlabSmem);
         if (e != cudaSuccess) return (int)e;
         lq3d_tma_kernel<true><<<grid, kTT, kSlabSmem, s>>>(a, map, slabs, units);
     } else {
-        e = cudaFuncSetAttribute(lq3d_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem);
+        static SmemAttr attr;
+        e = ensure_dyn_smem(attr, (const void*)lq3d_tma_kernel<false>, (int)kSlabSmem);
         if (e != cudaSuccess) return (int)e;
         lq3d_tma_kernel<false><<<grid, kTT, kSlabSmem, s>>>(a, map, slabs, units);
     }

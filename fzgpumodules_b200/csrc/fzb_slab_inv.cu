@@ -443,11 +443,13 @@ int launch_lq3d_inv_slab(const InvArgs& a, unsigned sms, cudaStream_t s) {
     grid = grid < units ? grid : units;
     cudaError_t e;
     if (a.zigzag) {
-        e = cudaFuncSetAttribute(lq3d_inv_slab_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem);
+        static SmemAttr attr;
+        e = ensure_dyn_smem(attr, (const void*)lq3d_inv_slab_kernel<true>, (int)kInvSmem);
         if (e != cudaSuccess) return (int)e;
         lq3d_inv_slab_kernel<true><<<grid, kThreads, kInvSmem, s>>>(a, slabs, units);
     } else {
-        e = cudaFuncSetAttribute(lq3d_inv_slab_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem);
+        static SmemAttr attr;
+        e = ensure_dyn_smem(attr, (const void*)lq3d_inv_slab_kernel<false>, (int)kInvSmem);
         if (e != cudaSuccess) return (int)e;
         lq3d_inv_slab_kernel<false><<<grid, kThreads, kInvSmem, s>>>(a, slabs, units);
     }
