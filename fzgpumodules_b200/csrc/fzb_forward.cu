@@ -52,12 +52,18 @@ __device__ __forceinline__ void minmax_body(const float* __restrict__ x, uint64_
     const float4* x4 = reinterpret_cast<const float4*>(x);
     const uint64_t stride = (uint64_t)nblk * blockDim.x;
     uint64_t i = (uint64_t)blk * blockDim.x + threadIdx.x;
-    for (; i + 7 * stride < nv; i += 8 * stride) {
-        float4 v[8];
+    // sixteen 16-byte loads in flight per thread, streamed past L1 with a
+    // 256-byte L2 fetch (a read-once scan)
+    for (; i + 15 * stride < nv; i += 16 * stride) {
+        float4 v[16];
 #pragma unroll
-        for (int k = 0; k < 8; k++) v[k] = __ldg(x4 + i + k * stride);
+        for (int k = 0; k < 16; k++) {
+            const float4* q = x4 + i + k * stride;
+            asm volatile("ld.global.nc.L1::no_allocate.L2::256B.v4.f32 {%0,%1,%2,%3}, [%4];"
+                         : "=f"(v[k].x), "=f"(v[k].y), "=f"(v[k].z), "=f"(v[k].w) : "l"(q));
+        }
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
+        for (int k = 0; k < 16; k++) {
             lo = fminf(lo, fminf(fminf(v[k].x, v[k].y), fminf(v[k].z, v[k].w)));
             hi = fmaxf(hi, fmaxf(fmaxf(v[k].x, v[k].y), fmaxf(v[k].z, v[k].w)));
         }
@@ -328,6 +334,7 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a, uint32_t* s
     // Tiles of kTile chunks: loads issued in batches of eight per thread (all
     // in flight at once) into shared memory, kTile/1024 chunks per thread, a
     // warp-shuffle block scan, coalesced writes, carry to the next tile.
+    // sp / so hold pad32-indexed entries (kTile + kTile / 32 words each).
     constexpr uint32_t kPer = kTile / 1024;
     __shared__ uint32_t wp[32], wo[32], s_tile[2];
     const uint32_t n = a.n_chunks, t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -355,8 +362,8 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a, uint32_t* s
 #pragma unroll
             for (uint32_t j = 0; j < kB; j++) {
                 const uint32_t i = t + 1024u * (j0 + j);
-                sp[i] = vs[j] & 0x7fffffffu;
-                so[i] = a.ocnt ? staged(vb[j], vc[j]) : 0u;
+                sp[pad32(i)] = vs[j] & 0x7fffffffu;
+                so[pad32(i)] = a.ocnt ? staged(vb[j], vc[j]) : 0u;
                 ot += vc[j];
                 if (a.sizes && i < cnt) hdr[2 + t0 + i] = vs[j];  // the stream's size table
             }
@@ -365,8 +372,8 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a, uint32_t* s
         uint32_t lp = 0, lo = 0;
 #pragma unroll
         for (uint32_t j = 0; j < kPer; j++) {
-            lp += sp[kPer * t + j];
-            lo += so[kPer * t + j];
+            lp += sp[pad32(kPer * t + j)];
+            lo += so[pad32(kPer * t + j)];
         }
         uint32_t ip = lp, io = lo;  // inclusive warp scans
 #pragma unroll
@@ -400,9 +407,10 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a, uint32_t* s
         uint32_t rp = wp[warp] + ip - lp, ro = wo[warp] + io - lo;
 #pragma unroll
         for (uint32_t j = 0; j < kPer; j++) {  // exclusive prefixes in place
-            const uint32_t vp = sp[kPer * t + j], vo = so[kPer * t + j];
-            sp[kPer * t + j] = rp;
-            so[kPer * t + j] = ro;
+            const uint32_t k = pad32(kPer * t + j);
+            const uint32_t vp = sp[k], vo = so[k];
+            sp[k] = rp;
+            so[k] = ro;
             rp += vp;
             ro += vo;
         }
@@ -412,8 +420,8 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a, uint32_t* s
         }
         __syncthreads();
         for (uint32_t i = t; i < cnt; i += 1024) {
-            if (a.sizes) a.pay_off[t0 + i] = carry_p + sp[i];
-            if (a.ocnt) a.ofin[t0 + i] = carry_o + so[i];
+            if (a.sizes) a.pay_off[t0 + i] = carry_p + sp[pad32(i)];
+            if (a.ocnt) a.ofin[t0 + i] = carry_o + so[pad32(i)];
         }
         carry_p += s_tile[0];
         carry_o += s_tile[1];
@@ -439,11 +447,11 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a, uint32_t* s
 
 __global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) {
     extern __shared__ uint32_t asm_dyn[];
-    assemble_scan_body<kAsmTile>(a, asm_dyn, asm_dyn + kAsmTile);
+    assemble_scan_body<kAsmTile>(a, asm_dyn, asm_dyn + kAsmTile + kAsmTile / 32);
 }
 
 int launch_assemble_scan(const AsmArgs& a, cudaStream_t s) {
-    const int smem = (int)(2 * kAsmTile * sizeof(uint32_t));
+    const int smem = (int)(2 * (kAsmTile + kAsmTile / 32) * sizeof(uint32_t));
     static SmemAttr attr;
     const cudaError_t e = ensure_dyn_smem(attr, (const void*)assemble_scan_kernel, smem);
     if (e != cudaSuccess) return (int)e;
@@ -813,7 +821,7 @@ __global__ void __launch_bounds__(256) batch_minmax_kernel(BatchArgs b) {
 }
 
 __global__ void __launch_bounds__(1024) batch_assemble_scan_kernel(BatchArgs b) {
-    __shared__ uint32_t sp[4096], so[4096];
+    __shared__ uint32_t sp[4096 + 128], so[4096 + 128];
     assemble_scan_body<4096>(b.fields[blockIdx.x].m, sp, so);
 }
 

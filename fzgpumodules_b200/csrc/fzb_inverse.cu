@@ -19,7 +19,7 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
     // thread (all in flight at once) into shared memory, 16 per thread, a
     // warp-shuffle block scan, coalesced writes, carry between tiles.
     constexpr uint32_t kTile = kAsmTile, kPer = kTile / 1024;
-    extern __shared__ uint32_t sz[];
+    extern __shared__ uint32_t sz[];  // pad32-indexed
     __shared__ uint32_t wsum[32], s_tile;
     const uint32_t* h = reinterpret_cast<const uint32_t*>(rze);
     const uint32_t n = n_expect, t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -41,12 +41,12 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
                 v[j] = i < cnt ? h[2 + t0 + i] : 0u;
             }
 #pragma unroll
-            for (uint32_t j = 0; j < 8; j++) sz[t + 1024u * (j0 + j)] = v[j] & 0x7fffffffu;
+            for (uint32_t j = 0; j < 8; j++) sz[pad32(t + 1024u * (j0 + j))] = v[j] & 0x7fffffffu;
         }
         __syncthreads();
         uint32_t l = 0;
 #pragma unroll
-        for (uint32_t j = 0; j < kPer; j++) l += sz[kPer * t + j];
+        for (uint32_t j = 0; j < kPer; j++) l += sz[pad32(kPer * t + j)];
         uint32_t inc = l;  // tile sums fit 32 bits: 4096 chunks of at most 16 KiB
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -69,13 +69,13 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
         uint32_t r = wsum[warp] + inc - l;
 #pragma unroll
         for (uint32_t j = 0; j < kPer; j++) {
-            const uint32_t v = sz[kPer * t + j];
-            sz[kPer * t + j] = r;
+            const uint32_t v = sz[pad32(kPer * t + j)];
+            sz[pad32(kPer * t + j)] = r;
             r += v;
         }
         if (t == 1023) s_tile = r;
         __syncthreads();
-        for (uint32_t i = t; i < cnt; i += 1024) in_off[t0 + i] = carry + sz[i];
+        for (uint32_t i = t; i < cnt; i += 1024) in_off[t0 + i] = carry + sz[pad32(i)];
         carry += s_tile;
         __syncthreads();
     }
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
 
 int launch_rze_prepass(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect, uint32_t orig_expect,
                        unsigned long long* in_off, uint32_t* err, cudaStream_t s) {
-    const int smem = (int)(kAsmTile * sizeof(uint32_t));
+    const int smem = (int)((kAsmTile + kAsmTile / 32) * sizeof(uint32_t));
     static SmemAttr attr;
     const cudaError_t e = ensure_dyn_smem(attr, (const void*)rze_prepass_kernel, smem);
     if (e != cudaSuccess) return (int)e;

@@ -125,6 +125,9 @@ int launch_bitshuffle_wide(const uint8_t* in, uint8_t* out, uint64_t nfull, uint
                            cudaStream_t s);
 __global__ void rze_encode_kernel(RzeEncArgs a);
 __global__ void assemble_scan_kernel(AsmArgs a);
+// Shared-memory index with one pad word per 32 entries: thread t touching
+// entries k*t + j (k a power of two up to 32) stays free of bank conflicts.
+__device__ __forceinline__ uint32_t pad32(uint32_t i) { return i + (i >> 5); }
 constexpr uint32_t kAsmTile = 16384;  // chunks per tile of the single-CTA assembly scan (shared memory: 2 words each)
 int launch_assemble_scan(const AsmArgs& a, cudaStream_t s);
 __global__ void assemble_copy_kernel(AsmArgs a);  // one warp per chunk, grid-stride
