@@ -145,6 +145,10 @@ def lib():
         L.fzb_huff_encode.argtypes = [p, u64, u32, p, p, p, p, p, sz, p]
         L.fzb_huff_compress.restype = i32
         L.fzb_huff_compress.argtypes = [p, u64, u32, p, p, p, sz, p]
+        L.fzb_crc32_workspace_bytes.restype = sz
+        L.fzb_crc32_workspace_bytes.argtypes = [u64]
+        L.fzb_crc32.restype = i32
+        L.fzb_crc32.argtypes = [p, u64, p, p, sz, p]
         L.fzb_huff_encode_fine.restype = i32
         L.fzb_huff_encode_fine.argtypes = [p, u64, u32, p, p, p, p, p, sz, p]
         L.fzb_huff_compress_fine.restype = i32

@@ -306,6 +306,22 @@ Pipeline::FZMFileHeader Pipeline::buildHeader() const {
 
 namespace {
 
+// CRC-32 of `bytes` bytes of device memory, computed on the device
+// (fzb_crc32) with its small workspace from `pool`; one 4-byte read-back.
+uint32_t device_crc32(const void* d_data, size_t bytes, MemoryPool* pool, cudaStream_t stream) {
+    const size_t need = fzb_crc32_workspace_bytes(bytes) + 256;
+    uint8_t* w = static_cast<uint8_t*>(pool->allocate(need, stream, "crc32_workspace", false));
+    if (!w) throw std::runtime_error("allocation for the CRC-32 workspace failed");
+    uint32_t* d_crc = reinterpret_cast<uint32_t*>(w + need - 256);
+    const int rc = fzb_crc32(d_data, bytes, d_crc, w, need - 256, stream);
+    uint32_t crc = 0;
+    if (rc == 0) cuda_check(cudaMemcpyAsync(&crc, d_crc, 4, cudaMemcpyDeviceToHost, stream), "CRC-32 read-back");
+    cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize failed");
+    pool->free(w, stream);
+    if (rc) throw std::runtime_error(std::string("fzb_crc32: ") + fzb_status_string(rc));
+    return crc;
+}
+
 uint32_t header_checksum(const Pipeline::FZMFileHeader& fh) {
     FZMHeaderCore c = fh.core;
     c.header_checksum = 0;
@@ -322,16 +338,32 @@ void Pipeline::writeToFile(const std::string& filename, cudaStream_t stream) {
     if (!compressed_) throw std::runtime_error("compress() must be called before writeToFile()");
     FZMFileHeader fh = buildHeader();
     std::vector<uint8_t> payload(fh.core.compressed_size);
+    // the payload is the outputs back to back: gather them on the device, take
+    // the checksum there, and read the payload back in one copy
+    uint8_t* d_payload = nullptr;
+    if (!payload.empty()) {
+        d_payload = static_cast<uint8_t*>(pool_->allocate(payload.size(), stream, "fzm_payload", false));
+        if (!d_payload) throw std::runtime_error("allocation for the FZM payload failed");
+    }
     size_t off = 0;
     for (const auto& m : meta_) {
         if (m.actual_size)
-            cuda_check(cudaMemcpyAsync(payload.data() + off, dag_->getBuffer(m.buffer_id), m.actual_size,
-                                       cudaMemcpyDeviceToHost, stream),
+            cuda_check(cudaMemcpyAsync(d_payload + off, dag_->getBuffer(m.buffer_id), m.actual_size,
+                                       cudaMemcpyDeviceToDevice, stream),
                        "cudaMemcpyAsync failed");
         off += m.actual_size;
     }
-    cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize failed");
-    fh.core.data_checksum = crc32(payload.data(), payload.size());
+    try {
+        fh.core.data_checksum = device_crc32(d_payload, payload.size(), pool_.get(), stream);
+        if (!payload.empty())
+            cuda_check(cudaMemcpyAsync(payload.data(), d_payload, payload.size(), cudaMemcpyDeviceToHost, stream),
+                       "cudaMemcpyAsync failed");
+        cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize failed");
+    } catch (...) {
+        if (d_payload) pool_->free(d_payload, stream);
+        throw;
+    }
+    if (d_payload) pool_->free(d_payload, stream);
     fh.core.flags |= FZM_FLAG_HAS_DATA_CHECKSUM | FZM_FLAG_HAS_HEADER_CHECKSUM;
     fh.core.header_checksum = header_checksum(fh);
     std::ofstream f(filename, std::ios::binary);
@@ -399,13 +431,6 @@ void Pipeline::decompressFromFile(const std::string& filename, void** d_output, 
         if (!payload.empty()) f.read(reinterpret_cast<char*>(payload.data()), payload.size());
         if (!f) throw std::runtime_error("Failed to read compressed data from file: " + filename);
     }
-    if (fh.core.flags & FZM_FLAG_HAS_DATA_CHECKSUM) {
-        const uint32_t got = crc32(payload.data(), payload.size());
-        if (got != fh.core.data_checksum)
-            throw std::runtime_error("FZM data checksum mismatch in '" + filename + "': expected 0x" +
-                                     hex8(fh.core.data_checksum) + ", computed 0x" + hex8(got) +
-                                     " — compressed data may be corrupted");
-    }
     for (const auto& e : fh.buffers)
         if (e.byte_offset + e.data_size > fh.core.compressed_size)
             throw std::runtime_error("FZM buffer '" + std::string(e.name, strnlen(e.name, FZM_MAX_NAME_LEN)) +
@@ -423,6 +448,21 @@ void Pipeline::decompressFromFile(const std::string& filename, void** d_output, 
         cuda_check(cudaMemcpyAsync(d_payload, payload.data(), payload.size(), cudaMemcpyHostToDevice, stream),
                    "cudaMemcpyAsync failed");
         cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize failed");
+    }
+    if (fh.core.flags & FZM_FLAG_HAS_DATA_CHECKSUM) {  // checked on the device copy
+        uint32_t got = 0;
+        try {
+            got = device_crc32(d_payload, payload.size(), &pool, stream);
+        } catch (...) {
+            if (d_payload) pool.free(d_payload, stream);
+            throw;
+        }
+        if (got != fh.core.data_checksum) {
+            if (d_payload) pool.free(d_payload, stream);
+            throw std::runtime_error("FZM data checksum mismatch in '" + filename + "': expected 0x" +
+                                     hex8(fh.core.data_checksum) + ", computed 0x" + hex8(got) +
+                                     " — compressed data may be corrupted");
+        }
     }
     std::vector<std::unique_ptr<Stage>> owned;
     std::vector<FwdDesc> fwd;

@@ -231,6 +231,18 @@ def bitpack_decode(packed: torch.Tensor, n: int, nbits: int, dtype=torch.uint16)
 
 # ------------------------------------------------------------------ Huffman
 
+def crc32(data: torch.Tensor, ws: Workspace | None = None) -> torch.Tensor:
+    """CRC-32 of a device tensor's bytes (the FZM data checksum,
+    compressor_io.cpp:25-52).  Returns a 1-element int64 device tensor."""
+    ws = ws or _default_ws
+    src = data.reshape(-1).view(torch.uint8) if data.numel() else data.reshape(-1)
+    out = torch.zeros(1, dtype=torch.int32, device=data.device)
+    wp, wn = ws.get_bytes(lib().fzb_crc32_workspace_bytes(src.numel() * src.element_size()), data.device)
+    check(lib().fzb_crc32(_ptr(src) if src.numel() else None, src.numel() * src.element_size(), _ptr(out), wp, wn,
+                          _stream(data.device)), "fzb_crc32")
+    return out.to(torch.int64) & 0xFFFFFFFF
+
+
 def huff_histogram(codes: torch.Tensor, bklen: int = 1024) -> torch.Tensor:
     """GPU_histogram_generic (util/histogram/histogram.cu): u32 counts."""
     src = codes.reshape(-1)

@@ -227,6 +227,15 @@ int fzb_huff_compress_fine(const uint16_t* d_in, uint64_t n, uint32_t bklen, voi
 int fzb_huff_decode(const void* d_in, uint64_t in_bytes, uint64_t n, uint32_t bklen, uint16_t* d_out,
                     void* d_work, size_t work_bytes, void* stream);
 
+/* CRC-32 of device memory: the FZM data checksum (IEEE polynomial
+ * 0xEDB88320, initial register and final inversion 0xFFFFFFFF;
+ * src/pipeline/compressor_io.cpp:25-52, computed on the host there at
+ * :218-228).  Writes the checksum to *d_crc (device u32); enqueue only.
+ * Any byte alignment; up to 128 GiB. */
+size_t fzb_crc32_workspace_bytes(uint64_t bytes);
+int fzb_crc32(const void* d_data, uint64_t bytes, uint32_t* d_crc, void* d_work, size_t work_bytes,
+              void* stream);
+
 /* Pipeline output concatenation (the reference's Pipeline::concatOutputs,
  * src/pipeline/compressor.cpp:760-875; layout pipeline_utils.h:35-46):
  * [u32 n][u64 size_i x n] padded to 16 bytes, then segment i padded to 16
