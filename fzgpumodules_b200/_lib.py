@@ -149,6 +149,22 @@ def lib():
         L.fzb_crc32_workspace_bytes.argtypes = [u64]
         L.fzb_crc32.restype = i32
         L.fzb_crc32.argtypes = [p, u64, p, p, sz, p]
+        for name in ("fzb_zigzag", "fzb_negabinary"):
+            getattr(L, name).restype = i32
+            getattr(L, name).argtypes = [p, u64, i32, i32, p, p]
+        L.fzb_scan_workspace_bytes.restype = sz
+        L.fzb_scan_workspace_bytes.argtypes = [u64, i32]
+        L.fzb_diff.restype = i32
+        L.fzb_diff.argtypes = [p, u64, i32, u64, i32, i32, p, p, sz, p]
+        L.fzb_lorenzo_int.restype = i32
+        L.fzb_lorenzo_int.argtypes = [p, p, u64, i32, i32, p, p, sz, p]
+        L.fzb_quantizer_workspace_bytes.restype = sz
+        L.fzb_quantizer_workspace_bytes.argtypes = [u64]
+        L.fzb_quantizer_forward.restype = i32
+        L.fzb_quantizer_forward.argtypes = [p, u64, i32, f32, i32, f32, u32, i32, f32, i32, p, p, p, p, u64, p, p,
+                                            sz, p]
+        L.fzb_quantizer_inverse.restype = i32
+        L.fzb_quantizer_inverse.argtypes = [p, u64, i32, f32, i32, f32, u32, i32, i32, p, p, p, u64, p, p]
         L.fzb_huff_encode_fine.restype = i32
         L.fzb_huff_encode_fine.argtypes = [p, u64, u32, p, p, p, p, p, sz, p]
         L.fzb_huff_compress_fine.restype = i32

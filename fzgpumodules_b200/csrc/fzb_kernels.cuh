@@ -24,6 +24,23 @@ inline cudaError_t ensure_dyn_smem(SmemAttr& st, const void* func, int bytes) {
     return e;
 }
 
+// Multiprocessor count of the current device, queried once per device (the
+// first eight devices; later ones query on every call).
+inline int device_sms() {
+    static std::atomic<int> cache[8] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    if (dev >= 0 && dev < 8) {
+        const int v = cache[dev].load(std::memory_order_relaxed);
+        if (v > 0) return v;
+    }
+    int sms = 0;
+    if (dev < 0 || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        return 1;
+    if (dev < 8) cache[dev].store(sms, std::memory_order_relaxed);
+    return sms;
+}
+
 struct FwdArgs {
     const float* in;
     uint32_t n_total;  // elements in the code domain (>= nfield when padded)

@@ -231,6 +231,98 @@ def bitpack_decode(packed: torch.Tensor, n: int, nbits: int, dtype=torch.uint16)
 
 # ------------------------------------------------------------------ Huffman
 
+# ------------------------------------------------------- stages around the codes
+
+def _flat(data: torch.Tensor) -> torch.Tensor:
+    return data.reshape(-1).contiguous()
+
+
+def zigzag(data: torch.Tensor, inverse: bool = False, out: torch.Tensor | None = None) -> torch.Tensor:
+    """ZigzagStage (transforms/zigzag/zigzag_stage.cu) on the element bit
+    patterns of `data` (1/2/4/8-byte elements); same dtype out."""
+    src = _flat(data)
+    dst = torch.empty_like(src) if out is None else out
+    check(lib().fzb_zigzag(_ptr(src), src.numel(), src.element_size(), int(inverse), _ptr(dst), _stream(src.device)),
+          "fzb_zigzag")
+    return dst
+
+
+def negabinary(data: torch.Tensor, inverse: bool = False, out: torch.Tensor | None = None) -> torch.Tensor:
+    """NegabinaryStage (transforms/negabinary/negabinary_stage.cu)."""
+    src = _flat(data)
+    dst = torch.empty_like(src) if out is None else out
+    check(lib().fzb_negabinary(_ptr(src), src.numel(), src.element_size(), int(inverse), _ptr(dst),
+                               _stream(src.device)), "fzb_negabinary")
+    return dst
+
+
+def diff(data: torch.Tensor, chunk_bytes: int = 0, negabinary: bool = False, inverse: bool = False,
+         ws: Workspace | None = None) -> torch.Tensor:
+    """DifferenceStage<T> / <T, TOut> for integer T (predictors/diff/diff.cu);
+    chunk_bytes as setChunkSize (0 = one chunk)."""
+    ws = ws or _default_ws
+    src = _flat(data)
+    e = src.element_size()
+    dst = torch.empty_like(src)
+    wp, wn = ws.get_bytes(lib().fzb_scan_workspace_bytes(src.numel(), e), src.device)
+    check(lib().fzb_diff(_ptr(src), src.numel(), e, chunk_bytes // e, int(negabinary), int(inverse), _ptr(dst), wp,
+                         wn, _stream(src.device)), "fzb_diff")
+    return dst
+
+
+def lorenzo_int(data: torch.Tensor, dims, inverse: bool = False, ws: Workspace | None = None) -> torch.Tensor:
+    """LorenzoStage<T> (predictors/lorenzo/lorenzo_stage.cu); dims = (x, y, z)."""
+    ws = ws or _default_ws
+    src = _flat(data)
+    e = src.element_size()
+    dst = torch.empty_like(src)
+    d = (C.c_uint64 * 3)(*[int(v) for v in dims])
+    wp, wn = ws.get_bytes(lib().fzb_scan_workspace_bytes(src.numel(), e), src.device)
+    check(lib().fzb_lorenzo_int(_ptr(src), d, src.numel(), e, int(inverse), _ptr(dst), wp, wn, _stream(src.device)),
+          "fzb_lorenzo_int")
+    return dst
+
+
+def quantizer_forward(x: torch.Tensor, eb: float, mode: int = ABS, radius: int = 32768, code_bytes: int = 2,
+                      zigzag: bool = False, outlier_capacity: float = 0.05, threshold: float = float("inf"),
+                      inplace: bool = False, value_base: float = 0.0, ws: Workspace | None = None) -> dict:
+    """QuantizerStage<float, TCode> forward (quantizers/quantizer/quantizer.cu).
+    Returns codes, index-ordered outlier lists, capped count, cap and the
+    device-resolved bound (value_base, abs_eb, 1/(2 abs_eb), 2 abs_eb)."""
+    ws = ws or _default_ws
+    src = _flat(x)
+    n, dev = src.numel(), src.device
+    cap = 0 if (inplace and mode != REL) else max_outliers(n, outlier_capacity)
+    ctype = torch.int16 if code_bytes == 2 else torch.int32
+    out = dict(codes=torch.empty(n, dtype=ctype, device=dev),
+               vals=torch.empty(max(cap, 1), dtype=torch.float32, device=dev),
+               idx=torch.empty(max(cap, 1), dtype=torch.int32, device=dev),
+               count=torch.zeros(1, dtype=torch.int32, device=dev),
+               eb_state=torch.zeros(4, dtype=torch.float32, device=dev), cap=cap)
+    wp, wn = ws.get_bytes(lib().fzb_quantizer_workspace_bytes(n), dev)
+    check(lib().fzb_quantizer_forward(_ptr(src), n, code_bytes, eb, mode, value_base, radius, int(zigzag), threshold,
+                                      int(inplace), _ptr(out["codes"]), _ptr(out["vals"]), _ptr(out["idx"]),
+                                      _ptr(out["count"]), cap, _ptr(out["eb_state"]), wp, wn, _stream(dev)),
+          "fzb_quantizer_forward")
+    st = lib().fzb_workspace_status(wp, _stream(dev))
+    if st != 0:
+        raise FzbError(st, "fzb_quantizer_forward")
+    return out
+
+
+def quantizer_inverse(codes: torch.Tensor, eb: float, mode: int, abs_eb: float, radius: int = 32768,
+                      zigzag: bool = False, inplace: bool = False, vals=None, idx=None, count=None,
+                      cap: int = 0) -> torch.Tensor:
+    """QuantizerStage inverse: dequantise, then scatter the outliers."""
+    src = _flat(codes)
+    n, dev = src.numel(), src.device
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    check(lib().fzb_quantizer_inverse(_ptr(src), n, src.element_size(), eb, mode, abs_eb, radius, int(zigzag),
+                                      int(inplace), _ptr(vals), _ptr(idx), _ptr(count), cap, _ptr(out),
+                                      _stream(dev)), "fzb_quantizer_inverse")
+    return out
+
+
 def crc32(data: torch.Tensor, ws: Workspace | None = None) -> torch.Tensor:
     """CRC-32 of a device tensor's bytes (the FZM data checksum,
     compressor_io.cpp:25-52).  Returns a 1-element int64 device tensor."""

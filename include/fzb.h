@@ -236,6 +236,53 @@ size_t fzb_crc32_workspace_bytes(uint64_t bytes);
 int fzb_crc32(const void* d_data, uint64_t bytes, uint32_t* d_crc, void* d_work, size_t work_bytes,
               void* stream);
 
+/* ---- Stages around the codes (enqueue only; elem_bytes 1, 2, 4 or 8;
+ * arithmetic on the element bit pattern modulo 2^(8*elem_bytes)). */
+
+/* ZigzagStage<S, U> (modules/transforms/zigzag/zigzag_stage.cu:19-96, codec
+ * zigzag.h:33-57): encode signed -> unsigned, inverse decodes.  d_in may
+ * equal d_out. */
+int fzb_zigzag(const void* d_in, uint64_t n, int elem_bytes, int inverse, void* d_out, void* stream);
+/* NegabinaryStage<S, U> (modules/transforms/negabinary/negabinary_stage.cu,
+ * codec negabinary.h:30-56).  d_in may equal d_out. */
+int fzb_negabinary(const void* d_in, uint64_t n, int elem_bytes, int inverse, void* d_out, void* stream);
+/* Workspace of fzb_diff / fzb_lorenzo_int inverses for n elements. */
+size_t fzb_scan_workspace_bytes(uint64_t n, int elem_bytes);
+/* DifferenceStage<T> / DifferenceStage<S, U> (modules/predictors/diff/
+ * diff.cu:26-220) for integer T: forward first differences restarting at
+ * multiples of chunk_elems (a power of two; 0 = one chunk), negabinary-coded
+ * when `negabinary`; inverse = the chunked prefix sum.  The forward needs
+ * d_in != d_out and no workspace. */
+int fzb_diff(const void* d_in, uint64_t n, int elem_bytes, uint64_t chunk_elems, int negabinary, int inverse,
+             void* d_out, void* d_work, size_t work_bytes, void* stream);
+/* LorenzoStage<T> (modules/predictors/lorenzo/lorenzo_stage.cu:18-400):
+ * lossless integer Lorenzo.  dims {x, y, z} (0 -> x = n, y = z = 1); 1-D
+ * works on all n elements in 256-element blocks, 2-D / 3-D on the
+ * x*y*z field (elements past it are copied).  Forward needs d_in != d_out;
+ * the 2-D / 3-D inverse needs fzb_scan_workspace_bytes(n) of workspace. */
+int fzb_lorenzo_int(const void* d_in, const uint64_t dims[3], uint64_t n, int elem_bytes, int inverse, void* d_out,
+                    void* d_work, size_t work_bytes, void* stream);
+
+/* QuantizerStage<float, TCode> forward (modules/quantizers/quantizer/
+ * quantizer.cu:388-649), code_bytes 2 (u16) or 4 (u32); eb_mode FZB_ABS /
+ * FZB_REL / FZB_NOA; value_base > 0 skips the NOA data scan
+ * (setValueBase); threshold = setOutlierThreshold (INFINITY: off); inplace =
+ * setInplaceOutliers (ABS/NOA, u32 codes, zigzag required: no outlier
+ * lists).  Outliers are listed in ascending index order; *d_count receives
+ * min(outliers, cap).  d_eb_state (4 floats): value_base, abs_eb,
+ * 1/(2 abs_eb), 2 abs_eb as resolved on the device.  Device status
+ * (look-back timeout) through fzb_workspace_status(d_work). */
+size_t fzb_quantizer_workspace_bytes(uint64_t n);
+int fzb_quantizer_forward(const float* d_in, uint64_t n, int code_bytes, float eb, int eb_mode, float value_base,
+                          uint32_t radius, int zigzag, float threshold, int inplace, void* d_codes, float* d_ovals,
+                          uint32_t* d_oidx, uint32_t* d_count, uint64_t cap, float* d_eb_state, void* d_work,
+                          size_t work_bytes, void* stream);
+/* Inverse (quantizer.cu:398-484): abs_eb as the header stores it (ignored
+ * for REL); scatters min(*d_count, cap) outliers. */
+int fzb_quantizer_inverse(const void* d_codes, uint64_t n, int code_bytes, float eb, int eb_mode, float abs_eb,
+                          uint32_t radius, int zigzag, int inplace, const float* d_ovals, const uint32_t* d_oidx,
+                          const uint32_t* d_count, uint64_t cap, float* d_out, void* stream);
+
 /* Pipeline output concatenation (the reference's Pipeline::concatOutputs,
  * src/pipeline/compressor.cpp:760-875; layout pipeline_utils.h:35-46):
  * [u32 n][u64 size_i x n] padded to 16 bytes, then segment i padded to 16

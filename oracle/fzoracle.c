@@ -981,3 +981,205 @@ uint32_t orc_crc32(const void* data, size_t len) {
     for (size_t i = 0; i < len; i++) crc = table[(crc ^ p[i]) & 0xFFu] ^ (crc >> 8);
     return crc ^ 0xFFFFFFFFu;
 }
+
+/* ------------------------------------------------------------------ */
+/* Stages around the codes: Zigzag, Negabinary, Difference, integer    */
+/* Lorenzo, the direct Quantizer (ABS / NOA)                           */
+/* ------------------------------------------------------------------ */
+
+static uint64_t ew_mask(int ew) { return ew == 8 ? ~0ull : ((1ull << (8 * ew)) - 1ull); }
+
+static uint64_t ld_w(const void* p, size_t i, int ew) {
+    switch (ew) {
+        case 1: return ((const uint8_t*)p)[i];
+        case 2: return ((const uint16_t*)p)[i];
+        case 4: return ((const uint32_t*)p)[i];
+        default: return ((const uint64_t*)p)[i];
+    }
+}
+
+static void st_w(void* p, size_t i, int ew, uint64_t v) {
+    switch (ew) {
+        case 1: ((uint8_t*)p)[i] = (uint8_t)v; break;
+        case 2: ((uint16_t*)p)[i] = (uint16_t)v; break;
+        case 4: ((uint32_t*)p)[i] = (uint32_t)v; break;
+        default: ((uint64_t*)p)[i] = v; break;
+    }
+}
+
+/* zigzag.h:41-48: (x << 1) ^ (x >> (W-1)); decode (u >> 1) ^ -(u & 1). */
+static uint64_t zz_enc(uint64_t u, int ew) {
+    const uint64_t m = ew_mask(ew);
+    const int sign = (int)((u >> (8 * ew - 1)) & 1u);
+    return ((u << 1) ^ (sign ? m : 0)) & m;
+}
+static uint64_t zz_dec(uint64_t u, int ew) {
+    const uint64_t m = ew_mask(ew);
+    return ((u >> 1) ^ ((u & 1u) ? m : 0)) & m;
+}
+/* negabinary.h:43-52: (n + M) ^ M, decode (u ^ M) - M, M = 0xAA..AA. */
+static uint64_t nb_enc(uint64_t u, int ew) {
+    const uint64_t m = ew_mask(ew), M = 0xAAAAAAAAAAAAAAAAull & m;
+    return ((u + M) & m) ^ M;
+}
+static uint64_t nb_dec(uint64_t u, int ew) {
+    const uint64_t m = ew_mask(ew), M = 0xAAAAAAAAAAAAAAAAull & m;
+    return ((u ^ M) - M) & m;
+}
+
+void orc_zigzag(const void* in, size_t n, int ew, int inverse, void* out) {
+    for (size_t i = 0; i < n; i++) {
+        const uint64_t u = ld_w(in, i, ew);
+        st_w(out, i, ew, inverse ? zz_dec(u, ew) : zz_enc(u, ew));
+    }
+}
+
+void orc_negabinary(const void* in, size_t n, int ew, int inverse, void* out) {
+    for (size_t i = 0; i < n; i++) {
+        const uint64_t u = ld_w(in, i, ew);
+        st_w(out, i, ew, inverse ? nb_dec(u, ew) : nb_enc(u, ew));
+    }
+}
+
+/* diff.cu:26-48 (forward) and :83-104 + :166-205 (chunked prefix sum). */
+void orc_diff(const void* in, size_t n, int ew, size_t chunk, int nb, int inverse, void* out) {
+    const uint64_t m = ew_mask(ew);
+    uint64_t acc = 0;
+    for (size_t i = 0; i < n; i++) {
+        const int start = (i == 0) || (chunk && i % chunk == 0);
+        const uint64_t x = ld_w(in, i, ew);
+        if (!inverse) {
+            const uint64_t d = start ? x : ((x - ld_w(in, i - 1, ew)) & m);
+            st_w(out, i, ew, nb ? nb_enc(d, ew) : d);
+        } else {
+            const uint64_t v = nb ? nb_dec(x, ew) : x;
+            acc = start ? v : ((acc + v) & m);
+            st_w(out, i, ew, acc);
+        }
+    }
+}
+
+/* lorenzo_stage.cu: 1-D deltas inside 256-element blocks (:18-33) and their
+ * block prefix sums (:38-58); 2-D / 3-D inclusion-exclusion over the field
+ * (:100-118, :215-243) and prefix sums along x, y, z (:120-200, :245-375).
+ * Elements past the 2-D / 3-D field are copied. */
+void orc_lorenzo_int(const void* in, size_t n, size_t nx, size_t ny, size_t nz, int ew, int inverse, void* out) {
+    const uint64_t m = ew_mask(ew);
+    if (ny <= 1 && nz <= 1) {
+        uint64_t acc = 0;
+        for (size_t i = 0; i < n; i++) {
+            const uint64_t x = ld_w(in, i, ew);
+            if (!inverse) {
+                st_w(out, i, ew, (i & 255) ? ((x - ld_w(in, i - 1, ew)) & m) : x);
+            } else {
+                acc = (i & 255) ? ((acc + x) & m) : x;
+                st_w(out, i, ew, acc);
+            }
+        }
+        return;
+    }
+    const size_t nf = nx * ny * nz, sy = nx, sz = nx * ny;
+    for (size_t i = nf; i < n; i++) st_w(out, i, ew, ld_w(in, i, ew));
+    if (!inverse) {
+        for (size_t z = 0; z < nz; z++)
+            for (size_t y = 0; y < ny; y++)
+                for (size_t x = 0; x < nx; x++) {
+                    const size_t i = z * sz + y * sy + x;
+                    uint64_t v = ld_w(in, i, ew);
+                    if (x) v -= ld_w(in, i - 1, ew);
+                    if (y) v -= ld_w(in, i - sy, ew);
+                    if (x && y) v += ld_w(in, i - sy - 1, ew);
+                    if (z) {
+                        v -= ld_w(in, i - sz, ew);
+                        if (x) v += ld_w(in, i - sz - 1, ew);
+                        if (y) v += ld_w(in, i - sz - sy, ew);
+                        if (x && y) v -= ld_w(in, i - sz - sy - 1, ew);
+                    }
+                    st_w(out, i, ew, v & m);
+                }
+        return;
+    }
+    for (size_t i = 0; i < nf; i++) st_w(out, i, ew, ld_w(in, i, ew));
+    for (size_t i = 0; i < nf; i++)
+        if (i % nx) st_w(out, i, ew, (ld_w(out, i, ew) + ld_w(out, i - 1, ew)) & m);
+    for (size_t i = 0; i < nf; i++)
+        if ((i / nx) % ny) st_w(out, i, ew, (ld_w(out, i, ew) + ld_w(out, i - sy, ew)) & m);
+    for (size_t i = sz; i < nf; i++) st_w(out, i, ew, (ld_w(out, i, ew) + ld_w(out, i - sz, ew)) & m);
+}
+
+/* __float2int_rn: round half to even, saturating, NaN -> 0. */
+static int f2i_rn(float v) {
+    if (isnan(v)) return 0;
+    const float r = nearbyintf(v);
+    if (r >= 2147483648.0f) return 2147483647;
+    if (r < -2147483648.0f) return (-2147483647 - 1);
+    return (int)r;
+}
+
+/* quantizer.cu:30-70 (forward ABS/NOA) with the outliers listed in index
+ * order; returns the outlier total (only cap stored). */
+size_t orc_quantizer_abs(const float* in, size_t n, int code_bytes, float ebx2_r, float threshold, uint32_t radius,
+                         int zigzag, void* codes, float* ovals, uint32_t* oidx, size_t cap) {
+    const int R = (int)(code_bytes == 2 ? (uint32_t)(uint16_t)radius : radius);
+    size_t k = 0;
+    for (size_t i = 0; i < n; i++) {
+        const float x = in[i];
+        const float p = x * ebx2_r;
+        const int q = f2i_rn(p);
+        uint64_t c = 0;
+        if (q > -R && q < R && fabsf(x) < threshold) {
+            const uint64_t u = (uint64_t)(int64_t)q & ew_mask(code_bytes);
+            c = zigzag ? zz_enc(u, code_bytes) : u;
+        } else {
+            if (k < cap) {
+                ovals[k] = x;
+                oidx[k] = (uint32_t)i;
+            }
+            k++;
+        }
+        st_w(codes, i, code_bytes, c);
+    }
+    return k;
+}
+
+/* quantizer.cu:117-138 (inverse ABS/NOA) and the scatter
+ * (predictor_utils.cuh:149-160). */
+void orc_quantizer_abs_inv(const void* codes, size_t n, int code_bytes, float ebx2, int zigzag, const float* ovals,
+                           const uint32_t* oidx, size_t nout, float* out) {
+    for (size_t i = 0; i < n; i++) {
+        uint64_t u = ld_w(codes, i, code_bytes);
+        if (zigzag) u = zz_dec(u, code_bytes);
+        const int q = code_bytes == 2 ? (int)(int16_t)(uint16_t)u : (int)(int32_t)(uint32_t)u;
+        out[i] = (float)q * ebx2;
+    }
+    for (size_t k = 0; k < nout; k++)
+        if (oidx[k] < n) out[oidx[k]] = ovals[k];
+}
+
+/* quantizer.cu:83-107 / :147-167: in-place outliers, u32 codes. */
+void orc_quantizer_inplace(const float* in, size_t n, float ebx2_r, float threshold, uint32_t radius,
+                           uint32_t* codes) {
+    const int R = (int)radius;
+    for (size_t i = 0; i < n; i++) {
+        const float x = in[i];
+        const int q = f2i_rn(x * ebx2_r);
+        if (q > -R && q < R && fabsf(x) < threshold) {
+            codes[i] = ((uint32_t)q << 1) ^ (uint32_t)(q >> 31);
+        } else {
+            memcpy(&codes[i], &x, 4);
+        }
+    }
+}
+
+void orc_quantizer_inplace_inv(const uint32_t* codes, size_t n, float ebx2, uint32_t radius, float* out) {
+    for (size_t i = 0; i < n; i++) {
+        const uint32_t c = codes[i];
+        if ((c >> 1) >= radius) {
+            memcpy(&out[i], &c, 4);
+        } else {
+            const int32_t ci = (int32_t)c;
+            const int q = (ci & 1) ? -((ci + 1) >> 1) : (ci >> 1);
+            out[i] = (float)q * ebx2;
+        }
+    }
+}

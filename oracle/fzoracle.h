@@ -129,6 +129,28 @@ size_t orc_huff_decode(const uint8_t* blob, size_t blob_bytes, uint16_t* out,
 /* CRC32 IEEE (src/pipeline/compressor_io.cpp:25-52). */
 uint32_t orc_crc32(const void* data, size_t len);
 
+/* Stages around the codes; ew = element bytes 1/2/4/8, arithmetic on the
+ * bit pattern modulo 2^(8*ew).
+ *   Zigzag (transforms/zigzag/zigzag.h:33-57), Negabinary
+ *   (transforms/negabinary/negabinary.h:30-56), Difference
+ *   (predictors/diff/diff.cu:26-205; chunk = elements, 0 = one chunk),
+ *   integer Lorenzo (predictors/lorenzo/lorenzo_stage.cu:18-375). */
+void orc_zigzag(const void* in, size_t n, int ew, int inverse, void* out);
+void orc_negabinary(const void* in, size_t n, int ew, int inverse, void* out);
+void orc_diff(const void* in, size_t n, int ew, size_t chunk, int nb, int inverse, void* out);
+void orc_lorenzo_int(const void* in, size_t n, size_t nx, size_t ny, size_t nz, int ew, int inverse, void* out);
+/* Direct quantizer ABS/NOA (quantizers/quantizer/quantizer.cu:30-167);
+ * code_bytes 2 or 4; returns the outlier total, the first cap by index
+ * stored.  The REL path calls CUDA's __log2f / exp2f and is checked against
+ * the reference's own kernels instead. */
+size_t orc_quantizer_abs(const float* in, size_t n, int code_bytes, float ebx2_r, float threshold, uint32_t radius,
+                         int zigzag, void* codes, float* ovals, uint32_t* oidx, size_t cap);
+void orc_quantizer_abs_inv(const void* codes, size_t n, int code_bytes, float ebx2, int zigzag, const float* ovals,
+                           const uint32_t* oidx, size_t nout, float* out);
+void orc_quantizer_inplace(const float* in, size_t n, float ebx2_r, float threshold, uint32_t radius,
+                           uint32_t* codes);
+void orc_quantizer_inplace_inv(const uint32_t* codes, size_t n, float ebx2, uint32_t radius, float* out);
+
 #ifdef __cplusplus
 }
 #endif

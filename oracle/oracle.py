@@ -79,6 +79,15 @@ def lib():
         L.orc_huff_decode.argtypes = [p, sz, p, sz]
         L.orc_crc32.restype = u32
         L.orc_crc32.argtypes = [p, sz]
+        L.orc_zigzag.argtypes = [p, sz, i32, i32, p]
+        L.orc_negabinary.argtypes = [p, sz, i32, i32, p]
+        L.orc_diff.argtypes = [p, sz, i32, sz, i32, i32, p]
+        L.orc_lorenzo_int.argtypes = [p, sz, sz, sz, sz, i32, i32, p]
+        L.orc_quantizer_abs.restype = sz
+        L.orc_quantizer_abs.argtypes = [p, sz, i32, f32, f32, u32, i32, p, p, p, sz]
+        L.orc_quantizer_abs_inv.argtypes = [p, sz, i32, f32, i32, p, p, sz, p]
+        L.orc_quantizer_inplace.argtypes = [p, sz, f32, f32, u32, p]
+        L.orc_quantizer_inplace_inv.argtypes = [p, sz, f32, u32, p]
         _lib = L
     return _lib
 
@@ -232,6 +241,79 @@ def huff_decode(blob: np.ndarray, n: int) -> np.ndarray:
 def crc32(data) -> int:
     b = np.ascontiguousarray(np.frombuffer(bytes(data), np.uint8) if isinstance(data, (bytes, bytearray)) else data).view(np.uint8).reshape(-1)
     return int(lib().orc_crc32(_p(b), b.size))
+
+
+def _uview(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a).reshape(-1)
+    return a.view({1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[a.itemsize])
+
+
+def zigzag(a: np.ndarray, inverse: bool = False) -> np.ndarray:
+    """Zigzag on the element bit patterns; returns the unsigned view."""
+    u = _uview(a)
+    out = np.empty_like(u)
+    lib().orc_zigzag(_p(u), u.size, u.itemsize, int(inverse), _p(out))
+    return out
+
+
+def negabinary(a: np.ndarray, inverse: bool = False) -> np.ndarray:
+    u = _uview(a)
+    out = np.empty_like(u)
+    lib().orc_negabinary(_p(u), u.size, u.itemsize, int(inverse), _p(out))
+    return out
+
+
+def diff(a: np.ndarray, chunk_elems: int = 0, negabinary: bool = False, inverse: bool = False) -> np.ndarray:
+    u = _uview(a)
+    out = np.empty_like(u)
+    lib().orc_diff(_p(u), u.size, u.itemsize, chunk_elems, int(negabinary), int(inverse), _p(out))
+    return out
+
+
+def lorenzo_int(a: np.ndarray, dims, inverse: bool = False) -> np.ndarray:
+    """dims = (x, y, z); 1-D when y = z = 1 (blocks of 256 over all n)."""
+    u = _uview(a)
+    out = np.empty_like(u)
+    nx, ny, nz = (int(v) for v in dims)
+    lib().orc_lorenzo_int(_p(u), u.size, nx, ny, nz, u.itemsize, int(inverse), _p(out))
+    return out
+
+
+def quantizer_abs(x: np.ndarray, code_bytes: int, ebx2_r, radius: int, zigzag: bool, cap: int,
+                  threshold: float = float("inf")):
+    """Returns (codes, outlier values, outlier indices, total outliers)."""
+    xs = np.ascontiguousarray(x, dtype=np.float32).reshape(-1)
+    codes = np.empty(xs.size, np.uint16 if code_bytes == 2 else np.uint32)
+    vals = np.zeros(max(cap, 1), np.float32)
+    idx = np.zeros(max(cap, 1), np.uint32)
+    k = lib().orc_quantizer_abs(_p(xs), xs.size, code_bytes, np.float32(ebx2_r), np.float32(threshold), radius,
+                                int(zigzag), _p(codes), _p(vals), _p(idx), cap)
+    m = min(k, cap)
+    return codes, vals[:m].copy(), idx[:m].copy(), int(k)
+
+
+def quantizer_abs_inv(codes: np.ndarray, ebx2, zigzag: bool, vals: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    c = np.ascontiguousarray(codes).reshape(-1)
+    v = np.ascontiguousarray(vals, dtype=np.float32)
+    ix = np.ascontiguousarray(idx, dtype=np.uint32)
+    out = np.empty(c.size, np.float32)
+    lib().orc_quantizer_abs_inv(_p(c), c.size, c.itemsize, np.float32(ebx2), int(zigzag), _p(v), _p(ix), v.size,
+                                _p(out))
+    return out
+
+
+def quantizer_inplace(x: np.ndarray, ebx2_r, radius: int, threshold: float = float("inf")) -> np.ndarray:
+    xs = np.ascontiguousarray(x, dtype=np.float32).reshape(-1)
+    codes = np.empty(xs.size, np.uint32)
+    lib().orc_quantizer_inplace(_p(xs), xs.size, np.float32(ebx2_r), np.float32(threshold), radius, _p(codes))
+    return codes
+
+
+def quantizer_inplace_inv(codes: np.ndarray, ebx2, radius: int) -> np.ndarray:
+    c = np.ascontiguousarray(codes, dtype=np.uint32).reshape(-1)
+    out = np.empty(c.size, np.float32)
+    lib().orc_quantizer_inplace_inv(_p(c), c.size, np.float32(ebx2), radius, _p(out))
+    return out
 
 
 # ---------------------------------------------------------------- reference builds

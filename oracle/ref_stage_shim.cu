@@ -17,7 +17,12 @@
 #include "coders/rze/rze_stage.h"
 #include "fused/lorenzo_quant/lorenzo_quant.h"
 #include "mem/mempool.h"
+#include "predictors/diff/diff.h"
+#include "predictors/lorenzo/lorenzo_stage.h"
+#include "quantizers/quantizer/quantizer.h"
 #include "shufflers/bitshuffle/bitshuffle_stage.h"
+#include "transforms/negabinary/negabinary_stage.h"
+#include "transforms/zigzag/zigzag_stage.h"
 
 using namespace fz;
 
@@ -202,6 +207,116 @@ extern "C" int ref_huffman_u16(const uint16_t* d_in, size_t n, int bklen, void* 
         st.execute(s, &pool, {d_out}, {d_dec}, {*out_bytes});
         if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("sync failed");
     }
+    GUARD_END
+    return 0;
+}
+
+// DifferenceStage<int32_t> / <int32_t, uint32_t> (predictors/diff/diff.cu).
+extern "C" int ref_diff_i32(const void* d_in, size_t n, size_t chunk_bytes, int negabinary, int inverse,
+                            void* d_out) {
+    GUARD_BEGIN
+    MemoryPool pool(MemoryPoolConfig(n * 8 + (size_t(1) << 22), 2.0f));
+    cudaStream_t s = 0;
+    if (negabinary) {
+        DifferenceStage<int32_t, uint32_t> st;
+        st.setChunkSize(chunk_bytes);
+        st.setInverse(inverse != 0);
+        st.execute(s, &pool, {const_cast<void*>(d_in)}, {d_out}, {n * 4});
+    } else {
+        DifferenceStage<int32_t> st;
+        st.setChunkSize(chunk_bytes);
+        st.setInverse(inverse != 0);
+        st.execute(s, &pool, {const_cast<void*>(d_in)}, {d_out}, {n * 4});
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("sync failed");
+    GUARD_END
+    return 0;
+}
+
+// LorenzoStage<int32_t> (predictors/lorenzo/lorenzo_stage.cu).
+extern "C" int ref_lorenzo_i32(const void* d_in, size_t n, size_t nx, size_t ny, size_t nz, int inverse,
+                               void* d_out) {
+    GUARD_BEGIN
+    MemoryPool pool(MemoryPoolConfig(n * 8 + (size_t(1) << 22), 2.0f));
+    LorenzoStage<int32_t> st;
+    st.setDims(nx, ny, nz);
+    st.setInverse(inverse != 0);
+    cudaStream_t s = 0;
+    st.execute(s, &pool, {const_cast<void*>(d_in)}, {d_out}, {n * 4});
+    if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("sync failed");
+    GUARD_END
+    return 0;
+}
+
+// ZigzagStage<int32_t, uint32_t> / NegabinaryStage<int32_t, uint32_t>.
+extern "C" int ref_transform_i32(int negabinary, const void* d_in, size_t n, int inverse, void* d_out) {
+    GUARD_BEGIN
+    cudaStream_t s = 0;
+    if (negabinary) {
+        NegabinaryStage<int32_t, uint32_t> st;
+        st.setInverse(inverse != 0);
+        st.execute(s, nullptr, {const_cast<void*>(d_in)}, {d_out}, {n * 4});
+    } else {
+        ZigzagStage<int32_t, uint32_t> st;
+        st.setInverse(inverse != 0);
+        st.execute(s, nullptr, {const_cast<void*>(d_in)}, {d_out}, {n * 4});
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("sync failed");
+    GUARD_END
+    return 0;
+}
+
+// QuantizerStage<float, uint16_t / uint32_t> forward, then its inverse from
+// the serialized header (quantizers/quantizer/quantizer.cu).  mode: 0 ABS,
+// 1 REL, 2 NOA.  hdr receives the 36-byte QuantizerConfig; d_recon may be
+// null (forward only).
+template <typename TC>
+static void ref_quant_run(const float* d_in, size_t n, float eb, int mode, int radius, int zigzag, int inplace,
+                          float threshold, float cap_frac, void* d_codes, float* d_vals, uint32_t* d_idx,
+                          uint32_t* d_count, float* d_recon, uint8_t* hdr) {
+    MemoryPool pool(MemoryPoolConfig(n * 16 + (size_t(1) << 22), 2.0f));
+    typename QuantizerStage<float, TC>::Config cfg;
+    cfg.error_bound = eb;
+    cfg.eb_mode = mode == 0 ? ErrorBoundMode::ABS : (mode == 1 ? ErrorBoundMode::REL : ErrorBoundMode::NOA);
+    cfg.quant_radius = radius;
+    cfg.outlier_capacity = cap_frac;
+    cfg.zigzag_codes = zigzag != 0;
+    cfg.inplace_outliers = inplace != 0;
+    cfg.outlier_threshold = threshold;
+    QuantizerStage<float, TC> st(cfg);
+    cudaStream_t s = 0;
+    const bool inpl = inplace && mode != 1;
+    if (inpl) st.execute(s, &pool, {const_cast<float*>(d_in)}, {d_codes}, {n * 4});
+    else st.execute(s, &pool, {const_cast<float*>(d_in)}, {d_codes, d_vals, d_idx, d_count}, {n * 4});
+    if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("sync failed");
+    st.postStreamSync(s);
+    const size_t hn = st.serializeHeader(0, hdr, 128);
+    if (d_recon) {
+        QuantizerStage<float, TC> inv;
+        inv.deserializeHeader(hdr, hn);
+        inv.setInverse(true);
+        if (inpl) {
+            inv.execute(s, &pool, {d_codes}, {d_recon}, {n * sizeof(TC)});
+        } else {
+            QuantizerConfig qc;
+            std::memcpy(&qc, hdr, sizeof(qc));
+            const size_t k = qc.outlier_count;
+            inv.execute(s, &pool, {d_codes, d_vals, d_idx, d_count}, {d_recon}, {n * sizeof(TC), k * 4, k * 4, 4});
+        }
+        if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("sync failed");
+    }
+}
+
+extern "C" int ref_quantizer_f32(const float* d_in, size_t n, int code_bytes, float eb, int mode, int radius,
+                                 int zigzag, int inplace, float threshold, float cap_frac, void* d_codes,
+                                 float* d_vals, uint32_t* d_idx, uint32_t* d_count, float* d_recon, uint8_t* hdr) {
+    GUARD_BEGIN
+    if (code_bytes == 2)
+        ref_quant_run<uint16_t>(d_in, n, eb, mode, radius, zigzag, inplace, threshold, cap_frac, d_codes, d_vals,
+                                d_idx, d_count, d_recon, hdr);
+    else
+        ref_quant_run<uint32_t>(d_in, n, eb, mode, radius, zigzag, inplace, threshold, cap_frac, d_codes, d_vals,
+                                d_idx, d_count, d_recon, hdr);
     GUARD_END
     return 0;
 }
