@@ -111,6 +111,11 @@ def lib():
         L.fzb_pipeline_add_huffman.argtypes = [p, u32]
         L.fzb_pipeline_add_huffman_mode.argtypes = [p, u32, i32]
         L.fzb_pipeline_add_bitpack.argtypes = [p, i32, i32]
+        L.fzb_pipeline_add_quantizer.argtypes = [p, i32, f32, i32, i32, f32, i32, i32, f32, f32]
+        L.fzb_pipeline_add_difference.argtypes = [p, i32, i32, u32]
+        L.fzb_pipeline_add_lorenzo.argtypes = [p, i32]
+        L.fzb_pipeline_add_zigzag.argtypes = [p, i32]
+        L.fzb_pipeline_add_negabinary.argtypes = [p, i32]
         L.fzb_pipeline_connect.argtypes = [p, i32, i32, C.c_char_p]
         L.fzb_pipeline_set_fusion.argtypes = [p, i32]
         L.fzb_pipeline_enable_graph_mode.argtypes = [p, i32]

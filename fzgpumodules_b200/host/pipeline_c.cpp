@@ -94,6 +94,98 @@ int fzb_pipeline_add_lorenzo_quant(void* p, float eb, int eb_mode, int radius, f
     });
 }
 
+int fzb_pipeline_add_quantizer(void* p, int code_bytes, float eb, int eb_mode, int radius, float outlier_capacity,
+                               int zigzag, int inplace, float threshold, float value_base) {
+    if (!p || eb_mode < FZB_ABS || eb_mode > FZB_NOA || (code_bytes != 2 && code_bytes != 4) || radius <= 0)
+        return FZB_E_INVALID;
+    return guarded([&] {
+        auto fill = [&](auto& c) {
+            c.error_bound = eb;
+            c.quant_radius = radius;
+            c.outlier_capacity = outlier_capacity;
+            c.eb_mode = (fz::ErrorBoundMode)eb_mode;
+            c.precomputed_value_base = value_base;
+            c.zigzag_codes = zigzag != 0;
+            c.inplace_outliers = inplace != 0;
+            c.outlier_threshold = threshold;
+        };
+        if (code_bytes == 2) {
+            fz::QuantizerStage<float, uint16_t>::Config c;
+            fill(c);
+            return add(p, H(p)->p->addStage<fz::QuantizerStage<float, uint16_t>>(c));
+        }
+        fz::QuantizerStage<float, uint32_t>::Config c;
+        fill(c);
+        return add(p, H(p)->p->addStage<fz::QuantizerStage<float, uint32_t>>(c));
+    });
+}
+
+int fzb_pipeline_add_difference(void* p, int in_type, int out_type, uint32_t chunk_size) {
+    if (!p) return FZB_E_INVALID;
+    return guarded([&] {
+        using DT = fz::DataType;
+        const DT a = (DT)in_type, b = (DT)out_type;
+        fz::Stage* s = nullptr;
+        auto mk = [&](auto* st) {
+            st->setChunkSize(chunk_size);
+            s = st;
+        };
+        auto& P = *H(p)->p;
+        if (a == DT::INT8 && b == DT::UINT8) mk(P.addStage<fz::DifferenceStage<int8_t, uint8_t>>());
+        else if (a == DT::INT16 && b == DT::UINT16) mk(P.addStage<fz::DifferenceStage<int16_t, uint16_t>>());
+        else if (a == DT::INT32 && b == DT::UINT32) mk(P.addStage<fz::DifferenceStage<int32_t, uint32_t>>());
+        else if (a == DT::INT64 && b == DT::UINT64) mk(P.addStage<fz::DifferenceStage<int64_t, uint64_t>>());
+        else if (a == b && a == DT::UINT8) mk(P.addStage<fz::DifferenceStage<uint8_t>>());
+        else if (a == b && a == DT::UINT16) mk(P.addStage<fz::DifferenceStage<uint16_t>>());
+        else if (a == b && a == DT::UINT32) mk(P.addStage<fz::DifferenceStage<uint32_t>>());
+        else if (a == b && a == DT::INT32) mk(P.addStage<fz::DifferenceStage<int32_t>>());
+        else if (a == b && a == DT::INT64) mk(P.addStage<fz::DifferenceStage<int64_t>>());
+        else throw std::invalid_argument("unsupported Difference type combination");
+        return add(p, s);
+    });
+}
+
+int fzb_pipeline_add_lorenzo(void* p, int data_type) {
+    if (!p) return FZB_E_INVALID;
+    return guarded([&] {
+        using DT = fz::DataType;
+        auto& P = *H(p)->p;
+        switch ((DT)data_type) {
+            case DT::INT8: return add(p, P.addStage<fz::LorenzoStage<int8_t>>());
+            case DT::INT16: return add(p, P.addStage<fz::LorenzoStage<int16_t>>());
+            case DT::INT32: return add(p, P.addStage<fz::LorenzoStage<int32_t>>());
+            case DT::INT64: return add(p, P.addStage<fz::LorenzoStage<int64_t>>());
+            default: throw std::invalid_argument("unsupported Lorenzo data_type");
+        }
+    });
+}
+
+static int add_sign_coding(void* p, int in_type, bool nb) {
+    if (!p) return FZB_E_INVALID;
+    return guarded([&] {
+        using DT = fz::DataType;
+        auto& P = *H(p)->p;
+        switch ((DT)in_type) {
+            case DT::INT8:
+                return add(p, nb ? (fz::Stage*)P.addStage<fz::NegabinaryStage<int8_t, uint8_t>>()
+                                 : P.addStage<fz::ZigzagStage<int8_t, uint8_t>>());
+            case DT::INT16:
+                return add(p, nb ? (fz::Stage*)P.addStage<fz::NegabinaryStage<int16_t, uint16_t>>()
+                                 : P.addStage<fz::ZigzagStage<int16_t, uint16_t>>());
+            case DT::INT32:
+                return add(p, nb ? (fz::Stage*)P.addStage<fz::NegabinaryStage<int32_t, uint32_t>>()
+                                 : P.addStage<fz::ZigzagStage<int32_t, uint32_t>>());
+            case DT::INT64:
+                return add(p, nb ? (fz::Stage*)P.addStage<fz::NegabinaryStage<int64_t, uint64_t>>()
+                                 : P.addStage<fz::ZigzagStage<int64_t, uint64_t>>());
+            default: throw std::invalid_argument("unsupported input_type (a signed integer type is required)");
+        }
+    });
+}
+
+int fzb_pipeline_add_zigzag(void* p, int in_type) { return add_sign_coding(p, in_type, false); }
+int fzb_pipeline_add_negabinary(void* p, int in_type) { return add_sign_coding(p, in_type, true); }
+
 int fzb_pipeline_add_bitshuffle(void* p, uint32_t block_size, int element_width) {
     if (!p) return FZB_E_INVALID;
     return guarded([&] {

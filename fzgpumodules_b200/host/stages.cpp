@@ -638,8 +638,10 @@ Stage* createStage(StageType type, const uint8_t* config, size_t config_size) {
             break;
         }
         default:
-            throw std::runtime_error("Unsupported stage type " + std::to_string((int)type) + " (" +
-                                     stageTypeToString(type) + ")");
+            s = createCodeStage(type, config, config_size);
+            if (!s)
+                throw std::runtime_error("Unsupported stage type " + std::to_string((int)type) + " (" +
+                                         stageTypeToString(type) + ")");
     }
     if (config_size) s->deserializeHeader(config, config_size);
     return s;

@@ -86,6 +86,86 @@ class LorenzoQuantStage(Stage):
                                                     self.outlier_capacity, int(self.zigzag_codes), self.value_base)
 
 
+# FZM DataType codes (include/fzm_format.h)
+UINT8, UINT16, UINT32, UINT64, INT8, INT16, INT32, INT64, FLOAT32, FLOAT64 = range(10)
+
+
+class QuantizerStage(Stage):
+    """QuantizerStage<float, uint16_t | uint32_t> (quantizers/quantizer/quantizer.h);
+    code_bytes = sizeof(TCode).  Outputs: codes, outlier_vals, outlier_idxs,
+    outlier_count (codes only with in-place outliers)."""
+
+    def __init__(self, error_bound: float = 1e-4, eb_mode: int = ABS, quant_radius: int = 32768,
+                 outlier_capacity: float = 0.05, code_bytes: int = 2, zigzag_codes: bool = False,
+                 inplace_outliers: bool = False, outlier_threshold: float = float("inf"), value_base: float = 0.0):
+        self.error_bound, self.eb_mode, self.quant_radius = error_bound, eb_mode, quant_radius
+        self.outlier_capacity, self.code_bytes, self.zigzag_codes = outlier_capacity, code_bytes, zigzag_codes
+        self.inplace_outliers, self.outlier_threshold, self.value_base = inplace_outliers, outlier_threshold, value_base
+
+    def getName(self):
+        return "Quantizer"
+
+    def setErrorBound(self, v): self.error_bound = v
+    def setQuantRadius(self, v): self.quant_radius = v
+    def setOutlierCapacity(self, v): self.outlier_capacity = v
+    def setErrorBoundMode(self, v): self.eb_mode = v
+    def setValueBase(self, v): self.value_base = v
+    def setZigzagCodes(self, v): self.zigzag_codes = bool(v)
+    def setOutlierThreshold(self, v): self.outlier_threshold = v
+    def setInplaceOutliers(self, v): self.inplace_outliers = bool(v)
+
+    def _add(self, h):
+        return lib().fzb_pipeline_add_quantizer(h, self.code_bytes, self.error_bound, self.eb_mode, self.quant_radius,
+                                                self.outlier_capacity, int(self.zigzag_codes),
+                                                int(self.inplace_outliers), self.outlier_threshold, self.value_base)
+
+
+class DifferenceStage(Stage):
+    """DifferenceStage<T, TOut> (predictors/diff/diff.h) for integer T; TOut the
+    unsigned type of a signed T fuses negabinary coding."""
+
+    def __init__(self, input_type: int = INT32, output_type: int | None = None, chunk_size: int = 0):
+        self.input_type = input_type
+        self.output_type = input_type if output_type is None else output_type
+        self.chunk_size = chunk_size
+
+    def setChunkSize(self, v): self.chunk_size = v
+
+    def _add(self, h):
+        return lib().fzb_pipeline_add_difference(h, self.input_type, self.output_type, self.chunk_size)
+
+
+class LorenzoStage(Stage):
+    """LorenzoStage<T> (predictors/lorenzo/lorenzo_stage.h), lossless integer
+    Lorenzo over the pipeline's dims; T signed."""
+
+    def __init__(self, data_type: int = INT32):
+        self.data_type = data_type
+
+    def _add(self, h):
+        return lib().fzb_pipeline_add_lorenzo(h, self.data_type)
+
+
+class ZigzagStage(Stage):
+    """ZigzagStage<S, U> (transforms/zigzag/zigzag_stage.h); input_type signed."""
+
+    def __init__(self, input_type: int = INT32):
+        self.input_type = input_type
+
+    def _add(self, h):
+        return lib().fzb_pipeline_add_zigzag(h, self.input_type)
+
+
+class NegabinaryStage(Stage):
+    """NegabinaryStage<S, U> (transforms/negabinary/negabinary_stage.h)."""
+
+    def __init__(self, input_type: int = INT32):
+        self.input_type = input_type
+
+    def _add(self, h):
+        return lib().fzb_pipeline_add_negabinary(h, self.input_type)
+
+
 class BitshuffleStage(Stage):
     """BitshuffleStage (shufflers/bitshuffle/bitshuffle_stage.h); defaults 16 KiB blocks, element width 4."""
 

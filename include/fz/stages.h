@@ -2,7 +2,10 @@
 // the reference's class names, setters, output names and container headers
 // (modules/fused/lorenzo_quant/lorenzo_quant.h, shufflers/bitshuffle/
 // bitshuffle_stage.h, coders/rze/rze_stage.h, coders/rle/rle.h,
-// coders/huffman/huffman_stage.h, coders/bitpack/bitpack_stage.h).  Every
+// coders/huffman/huffman_stage.h, coders/bitpack/bitpack_stage.h,
+// quantizers/quantizer/quantizer.h, predictors/diff/diff.h,
+// predictors/lorenzo/lorenzo_stage.h, transforms/zigzag/zigzag_stage.h,
+// transforms/negabinary/negabinary_stage.h).  Every
 // stage runs the sm_100a kernels of libfzb through the C ABI in fzb.h; errors
 // are thrown as std::runtime_error, as the reference does.
 #pragma once
@@ -468,8 +471,318 @@ private:
     StageWorkspace ws_;
 };
 
+// ---------------------------------------------------------------------------
+// Quantizer: prediction-free quantisation (quantizers/quantizer/quantizer.h).
+// Outputs codes, outlier_vals, outlier_idxs, outlier_count (codes only with
+// in-place outliers).
+// ---------------------------------------------------------------------------
+// 36-byte container record (quantizer.h:25-47).
+struct QuantizerConfig {
+    float abs_error_bound;   // 0 for REL
+    float user_error_bound;
+    float value_base;        // NOA value range; 0 for ABS / REL
+    uint32_t quant_radius;
+    uint32_t num_elements;
+    uint32_t outlier_count;
+    DataType input_type;
+    DataType code_type;
+    uint8_t eb_mode;
+    uint8_t zigzag_codes;
+    float outlier_threshold;
+    uint8_t inplace_outliers;
+    uint8_t pad[3];
+    QuantizerConfig()
+        : abs_error_bound(0.0f), user_error_bound(0.0f), value_base(0.0f), quant_radius(0), num_elements(0),
+          outlier_count(0), input_type(DataType::FLOAT32), code_type(DataType::UINT16), eb_mode(0), zigzag_codes(0),
+          outlier_threshold(__builtin_inff()), inplace_outliers(0), pad{0, 0, 0} {}
+};
+static_assert(sizeof(QuantizerConfig) == 36, "QuantizerConfig is 36 bytes");
+
+template <typename TInput = float, typename TCode = uint16_t>
+class QuantizerStage : public Stage {
+    static_assert(std::is_same<TInput, float>::value &&
+                      (std::is_same<TCode, uint16_t>::value || std::is_same<TCode, uint32_t>::value),
+                  "the sm_100a kernels implement QuantizerStage<float, uint16_t / uint32_t>");
+
+public:
+    struct Config {
+        float error_bound = 1e-4f;
+        int quant_radius = 32768;
+        float outlier_capacity = 0.05f;
+        ErrorBoundMode eb_mode = ErrorBoundMode::ABS;
+        float precomputed_value_base = 0.0f;       // > 0 skips the NOA scan
+        float outlier_threshold = __builtin_inff();  // |x| >= threshold -> outlier
+        bool zigzag_codes = false;
+        bool inplace_outliers = false;             // ABS / NOA, uint32 codes, zigzag
+        Config() = default;
+        Config(TInput eb, ErrorBoundMode mode = ErrorBoundMode::ABS, int radius = 32768, float outlier_cap = 0.05f)
+            : error_bound(eb), quant_radius(radius), outlier_capacity(outlier_cap), eb_mode(mode) {}
+    };
+
+    explicit QuantizerStage(const Config& config = Config());
+
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    void postStreamSync(cudaStream_t stream) override;
+    void onGraphReplay(cudaStream_t) override { pending_ = !is_inverse_ && d_eb_state_ != nullptr && ran_; }
+
+    std::string getName() const override { return "Quantizer"; }
+    size_t getNumInputs() const override { return is_inverse_ ? (isInplaceMode() ? 1 : 4) : 1; }
+    size_t getNumOutputs() const override { return is_inverse_ ? 1 : (isInplaceMode() ? 1 : 4); }
+    std::vector<std::string> getOutputNames() const override {
+        if (is_inverse_) return {"reconstructed"};
+        if (isInplaceMode()) return {"codes"};
+        return {"codes", "outlier_vals", "outlier_idxs", "outlier_count"};
+    }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& input_sizes) const override;
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override;
+    size_t getActualOutputSize(int index) const override {
+        return (index >= 0 && index < (int)actual_.size()) ? actual_[index] : 0;
+    }
+    size_t getExecuteTimeOutputSize(int index) const override {
+        if (is_inverse_) return getActualOutputSize(index);
+        return (index >= 0 && index < (int)at_execute_.size()) ? at_execute_[index] : 0;
+    }
+    void setInverse(bool inverse) override { is_inverse_ = inverse; }
+    bool isInverse() const override { return is_inverse_; }
+    uint16_t getStageTypeId() const override { return (uint16_t)StageType::QUANTIZER; }
+    uint8_t getOutputDataType(size_t i) const override;
+    uint8_t getInputDataType(size_t) const override {
+        return (uint8_t)(is_inverse_ ? codeType() : DataType::FLOAT32);
+    }
+    size_t serializeHeader(size_t output_index, uint8_t* buf, size_t max_size) const override;
+    void deserializeHeader(const uint8_t* buf, size_t size) override;
+    size_t getMaxHeaderSize(size_t) const override { return sizeof(QuantizerConfig); }
+    void saveState() override { saved_ = {config_, num_elements_, actual_outlier_count_, computed_abs_eb_,
+                                          computed_value_base_, actual_}; }
+    void restoreState() override {
+        config_ = saved_.config;
+        num_elements_ = saved_.n;
+        actual_outlier_count_ = saved_.count;
+        computed_abs_eb_ = saved_.abs_eb;
+        computed_value_base_ = saved_.vb;
+        actual_ = saved_.actual;
+    }
+
+    void setErrorBound(TInput eb) { config_.error_bound = eb; }
+    void setQuantRadius(int r) { config_.quant_radius = r; }
+    void setOutlierCapacity(float c) { config_.outlier_capacity = c; }
+    void setErrorBoundMode(ErrorBoundMode m) { config_.eb_mode = m; }
+    void setValueBase(float vb) { config_.precomputed_value_base = vb; }
+    void setZigzagCodes(bool enable) { config_.zigzag_codes = enable; }
+    void setOutlierThreshold(float t) { config_.outlier_threshold = t; }
+    void setInplaceOutliers(bool enable) { config_.inplace_outliers = enable; }
+    TInput getErrorBound() const { return config_.error_bound; }
+    int getQuantRadius() const { return config_.quant_radius; }
+    ErrorBoundMode getErrorBoundMode() const { return config_.eb_mode; }
+    float getValueBase() const { return config_.precomputed_value_base; }
+    float getOutlierCapacity() const { return config_.outlier_capacity; }
+    bool getZigzagCodes() const { return config_.zigzag_codes; }
+    float getOutlierThreshold() const { return config_.outlier_threshold; }
+    bool getInplaceOutliers() const { return config_.inplace_outliers; }
+    // ceil(n * outlier_capacity) in single precision (quantizer.h:262-264).
+    size_t getMaxOutlierCount(size_t n) const;
+    float computedAbsErrorBound() const { return computed_abs_eb_; }
+
+private:
+    bool isInplaceMode() const { return config_.inplace_outliers && config_.eb_mode != ErrorBoundMode::REL; }
+    static DataType codeType() { return sizeof(TCode) == 2 ? DataType::UINT16 : DataType::UINT32; }
+    struct Saved {
+        Config config;
+        size_t n = 0;
+        uint32_t count = 0;
+        float abs_eb = 0.0f, vb = 0.0f;
+        std::vector<size_t> actual;
+    };
+    Config config_;
+    bool is_inverse_ = false;
+    bool ran_ = false;
+    bool pending_ = false;
+    std::vector<size_t> actual_, at_execute_;
+    size_t num_elements_ = 0;
+    uint32_t actual_outlier_count_ = 0;
+    float computed_abs_eb_ = 0.0f;
+    float computed_value_base_ = 0.0f;
+    const void* d_count_ = nullptr;
+    float* d_eb_state_ = nullptr;  // inside the workspace
+    Saved saved_;
+    StageWorkspace ws_;
+};
+
+// ---------------------------------------------------------------------------
+// Difference (predictors/diff/diff.h): first differences in power-of-two
+// chunks; TOut the unsigned type of T's width fuses negabinary coding.
+// ---------------------------------------------------------------------------
+template <typename T, typename TOut = T>
+class DifferenceStage : public Stage {
+    static_assert(std::is_integral<T>::value && sizeof(T) == sizeof(TOut) &&
+                      (std::is_same<T, TOut>::value || (std::is_signed<T>::value && std::is_unsigned<TOut>::value)),
+                  "the sm_100a kernels implement integer DifferenceStage<T> and <signed, unsigned> pairs");
+
+public:
+    DifferenceStage() = default;
+    void setInverse(bool inverse) override { is_inverse_ = inverse; }
+    bool isInverse() const override { return is_inverse_; }
+    void setChunkSize(size_t bytes) { chunk_size_ = bytes; }
+    size_t getChunkSize() const { return chunk_size_; }
+    size_t getRequiredInputAlignment() const override { return chunk_size_ > 0 ? chunk_size_ : 1; }
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    std::string getName() const override { return "Difference"; }
+    size_t getNumInputs() const override { return 1; }
+    size_t getNumOutputs() const override { return 1; }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& s) const override { return {s[0]}; }
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override {
+        return {{"output", actual_}};
+    }
+    size_t getActualOutputSize(int index) const override { return index == 0 ? actual_ : 0; }
+    uint16_t getStageTypeId() const override { return (uint16_t)StageType::DIFFERENCE; }
+    uint8_t getOutputDataType(size_t) const override;
+    uint8_t getInputDataType(size_t) const override;
+    // diff.h:120-140: [u8 T type][u8 TOut type][u32 chunk_size]
+    size_t serializeHeader(size_t, uint8_t* buf, size_t max_size) const override;
+    void deserializeHeader(const uint8_t* buf, size_t size) override;
+    size_t getMaxHeaderSize(size_t) const override { return 6; }
+    void saveState() override { saved_ = {chunk_size_, actual_}; }
+    void restoreState() override {
+        chunk_size_ = saved_[0];
+        actual_ = saved_[1];
+    }
+
+private:
+    bool is_inverse_ = false;
+    size_t chunk_size_ = 0;
+    size_t actual_ = 0;
+    std::array<size_t, 2> saved_ = {0, 0};
+    StageWorkspace ws_;
+};
+
+// ---------------------------------------------------------------------------
+// Lorenzo (predictors/lorenzo/lorenzo_stage.h): lossless integer Lorenzo.
+// ---------------------------------------------------------------------------
+// 16-byte container record (lorenzo_stage.h:24-38).
+struct LorenzoConfig {
+    DataType data_type;
+    uint8_t ndim;
+    uint8_t reserved[2];
+    uint32_t dim_x;
+    uint32_t dim_y;
+    uint32_t dim_z;
+    LorenzoConfig() : data_type(DataType::INT32), ndim(1), reserved{0, 0}, dim_x(0), dim_y(1), dim_z(1) {}
+};
+static_assert(sizeof(LorenzoConfig) == 16, "LorenzoConfig is 16 bytes");
+
+template <typename T>
+class LorenzoStage : public Stage {
+    static_assert(std::is_integral<T>::value && std::is_signed<T>::value, "LorenzoStage requires a signed integer type");
+
+public:
+    LorenzoStage() = default;
+    void setInverse(bool inv) override { is_inverse_ = inv; }
+    bool isInverse() const override { return is_inverse_; }
+    void setDims(const std::array<size_t, 3>& dims) override { dims_ = dims; }
+    void setDims(size_t x, size_t y = 1, size_t z = 1) { dims_ = {x, y, z}; }
+    std::array<size_t, 3> getDims() const { return dims_; }
+    int ndim() const { return dims_[2] > 1 ? 3 : (dims_[1] > 1 ? 2 : 1); }
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    std::string getName() const override { return "Lorenzo"; }
+    size_t getNumInputs() const override { return 1; }
+    size_t getNumOutputs() const override { return 1; }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& s) const override {
+        return {s.empty() ? 0 : s[0]};
+    }
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override {
+        return {{"output", actual_}};
+    }
+    size_t getActualOutputSize(int index) const override { return index == 0 ? actual_ : 0; }
+    uint16_t getStageTypeId() const override { return (uint16_t)StageType::LORENZO; }
+    uint8_t getOutputDataType(size_t) const override { return (uint8_t)elemType(); }
+    uint8_t getInputDataType(size_t) const override { return (uint8_t)elemType(); }
+    size_t serializeHeader(size_t, uint8_t* buf, size_t max_size) const override;
+    void deserializeHeader(const uint8_t* buf, size_t size) override;
+    size_t getMaxHeaderSize(size_t) const override { return sizeof(LorenzoConfig); }
+
+private:
+    static DataType elemType() {
+        return sizeof(T) == 1 ? DataType::INT8
+               : sizeof(T) == 2 ? DataType::INT16
+               : sizeof(T) == 4 ? DataType::INT32
+                                : DataType::INT64;
+    }
+    bool is_inverse_ = false;
+    size_t actual_ = 0;
+    std::array<size_t, 3> dims_ = {0, 1, 1};
+    StageWorkspace ws_;
+};
+
+// ---------------------------------------------------------------------------
+// Zigzag / Negabinary (transforms/zigzag/zigzag_stage.h,
+// transforms/negabinary/negabinary_stage.h): signed <-> unsigned of the same
+// width, header [u8 TIn type][u8 TOut type].
+// ---------------------------------------------------------------------------
+template <typename TIn, typename TOut, bool NEGABINARY>
+class SignCodingStage : public Stage {
+    static_assert(std::is_integral<TIn>::value && std::is_signed<TIn>::value && std::is_unsigned<TOut>::value &&
+                      sizeof(TIn) == sizeof(TOut),
+                  "TIn signed, TOut its unsigned counterpart");
+
+public:
+    void setInverse(bool inv) override { is_inverse_ = inv; }
+    bool isInverse() const override { return is_inverse_; }
+    void execute(cudaStream_t stream, MemoryPool* pool, const std::vector<void*>& inputs,
+                 const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
+    std::string getName() const override { return NEGABINARY ? "Negabinary" : "Zigzag"; }
+    size_t getNumInputs() const override { return 1; }
+    size_t getNumOutputs() const override { return 1; }
+    std::vector<size_t> estimateOutputSizes(const std::vector<size_t>& s) const override {
+        return {s.empty() ? 0 : s[0]};
+    }
+    std::unordered_map<std::string, size_t> getActualOutputSizesByName() const override {
+        return {{"output", actual_}};
+    }
+    size_t getActualOutputSize(int index) const override { return index == 0 ? actual_ : 0; }
+    uint16_t getStageTypeId() const override {
+        return (uint16_t)(NEGABINARY ? StageType::NEGABINARY : StageType::ZIGZAG);
+    }
+    uint8_t getOutputDataType(size_t) const override { return (uint8_t)(is_inverse_ ? inType() : outType()); }
+    uint8_t getInputDataType(size_t) const override { return (uint8_t)(is_inverse_ ? outType() : inType()); }
+    size_t serializeHeader(size_t, uint8_t* buf, size_t max_size) const override {
+        if (max_size < 2) return 0;
+        buf[0] = (uint8_t)inType();
+        buf[1] = (uint8_t)outType();
+        return 2;
+    }
+    void deserializeHeader(const uint8_t*, size_t) override {}
+    size_t getMaxHeaderSize(size_t) const override { return 2; }
+
+private:
+    static DataType inType() {
+        return sizeof(TIn) == 1 ? DataType::INT8
+               : sizeof(TIn) == 2 ? DataType::INT16
+               : sizeof(TIn) == 4 ? DataType::INT32
+                                  : DataType::INT64;
+    }
+    static DataType outType() {
+        return sizeof(TIn) == 1 ? DataType::UINT8
+               : sizeof(TIn) == 2 ? DataType::UINT16
+               : sizeof(TIn) == 4 ? DataType::UINT32
+                                  : DataType::UINT64;
+    }
+    bool is_inverse_ = false;
+    size_t actual_ = 0;
+};
+
+template <typename TIn, typename TOut>
+using ZigzagStage = SignCodingStage<TIn, TOut, false>;
+template <typename TIn, typename TOut>
+using NegabinaryStage = SignCodingStage<TIn, TOut, true>;
+
 // Rebuilds a stage from its container record (stage_factory.h:36-...).  The
 // stage types of this library's path are supported; others throw.
 Stage* createStage(StageType type, const uint8_t* config, size_t config_size);
+// The Quantizer / Difference / Lorenzo / Zigzag / Negabinary cases of it;
+// nullptr for other types.
+Stage* createCodeStage(StageType type, const uint8_t* config, size_t config_size);
 
 }  // namespace fz

@@ -416,6 +416,22 @@ int fzb_pipeline_add_huffman(void* pipeline, uint32_t bklen);
 /* HuffmanStage with setEncodeMode: 0 Coarse, 1 Fine (huffman_stage.h). */
 int fzb_pipeline_add_huffman_mode(void* pipeline, uint32_t bklen, int encode_mode);
 int fzb_pipeline_add_bitpack(void* pipeline, int elem, int nbits);   /* nbits 0 = setAutoDetect */
+/* addStage<QuantizerStage<float, u16|u32>> with Config fields
+ * (modules/quantizers/quantizer/quantizer.h:96-118); threshold INFINITY = off. */
+int fzb_pipeline_add_quantizer(void* pipeline, int code_bytes, float eb, int eb_mode, int radius,
+                               float outlier_capacity, int zigzag, int inplace, float threshold, float value_base);
+/* addStage<DifferenceStage<T, TOut>> (modules/predictors/diff/diff.h); types
+ * are FZM DataType codes (0 u8, 1 u16, 2 u32, 3 u64, 4 i8, 5 i16, 6 i32,
+ * 7 i64): out_type == in_type, or the unsigned type of a signed in_type
+ * (negabinary-fused).  chunk_size in bytes (setChunkSize; 0 = one chunk). */
+int fzb_pipeline_add_difference(void* pipeline, int in_type, int out_type, uint32_t chunk_size);
+/* addStage<LorenzoStage<T>> (modules/predictors/lorenzo/lorenzo_stage.h), T
+ * signed (DataType code 4..7); dims come from fzb_pipeline_set_dims. */
+int fzb_pipeline_add_lorenzo(void* pipeline, int data_type);
+/* addStage<ZigzagStage<S, U>> / <NegabinaryStage<S, U>> (modules/transforms/
+ * zigzag/zigzag_stage.h, negabinary/negabinary_stage.h), S signed (4..7). */
+int fzb_pipeline_add_zigzag(void* pipeline, int in_type);
+int fzb_pipeline_add_negabinary(void* pipeline, int in_type);
 /* connect(dependent, producer, output_name); returns the buffer id. */
 int fzb_pipeline_connect(void* pipeline, int dependent, int producer, const char* output_name);
 /* Fusion of LorenzoQuant -> Bitshuffle -> RZE into one pass (default on). */

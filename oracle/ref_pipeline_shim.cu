@@ -14,6 +14,11 @@
 #include <string>
 
 #include "pipeline/compressor.h"
+#include "predictors/diff/diff.h"
+#include "predictors/lorenzo/lorenzo_stage.h"
+#include "quantizers/quantizer/quantizer.h"
+#include "transforms/negabinary/negabinary_stage.h"
+#include "transforms/zigzag/zigzag_stage.h"
 
 using namespace fz;
 
@@ -62,6 +67,87 @@ extern "C" int ref_pipeline_fzm(int chain, const float* d_in, size_t n, size_t x
         *decomp_bytes = dsz;
         if (d_decomp && dec) cudaMemcpy(d_decomp, dec, dsz, cudaMemcpyDeviceToDevice);
         if (dec) cudaFree(dec);
+        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device sync failed");
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    } catch (...) {
+        g_err = "unknown exception";
+        return -1;
+    }
+    return 0;
+}
+
+// Pipelines around the direct Quantizer (the shipped presets
+// examples/presets/pfpl.toml, speed.toml, quantizer_lorenzo_bitpack.toml and
+// two more codings of the codes):
+// chain 3: Quantizer<float,u32>(REL, zigzag) -> Difference<int32,uint32>(16 KiB)
+//          -> Bitshuffle(16384, ew 2) -> RZE
+// chain 4: Quantizer<float,u32>(REL, zigzag) -> Bitshuffle(16384, ew 4) -> RZE
+// chain 5: Quantizer<float,u32>(NOA, radius 512) -> Lorenzo<int32> -> Bitpack<u32>(16)
+// chain 6: Quantizer<float,u16>(ABS) -> Negabinary<int16,uint16> -> Bitshuffle(ew 2) -> RZE
+// chain 7: Quantizer<float,u32>(ABS, zigzag, in-place outliers) -> Zigzag<int32,uint32>
+//          -> Bitshuffle(ew 4) -> RZE
+// The reference's stage factory has no Quantizer case, so the file cannot be
+// read back by decompressFromFile; decompression runs on the live pipeline.
+extern "C" int ref_pipeline_codes(int chain, const float* d_in, size_t n, size_t x, size_t y, size_t z, float eb,
+                                  int mode, int radius, float outlier_cap, const char* path, float* d_decomp,
+                                  size_t* decomp_bytes, size_t* comp_bytes) {
+    try {
+        Pipeline p(n * sizeof(float), MemoryStrategy::PREALLOCATE, 3.0f);
+        p.setDims(x, y, z);
+        auto bs_rze = [&](Stage* from, const char* port, int ew) {
+            auto* bs = p.addStage<BitshuffleStage>();
+            bs->setBlockSize(16384);
+            bs->setElementWidth(ew);
+            auto* rze = p.addStage<RZEStage>();
+            rze->setLevels(4);
+            p.connect(bs, from, port);
+            p.connect(rze, bs);
+        };
+        if (chain == 6) {
+            QuantizerStage<float, uint16_t>::Config c(eb, static_cast<ErrorBoundMode>(mode), radius, outlier_cap);
+            auto* q = p.addStage<QuantizerStage<float, uint16_t>>(c);
+            auto* nb = p.addStage<NegabinaryStage<int16_t, uint16_t>>();
+            p.connect(nb, q, "codes");
+            bs_rze(nb, "output", 2);
+        } else {
+            QuantizerStage<float, uint32_t>::Config c(eb, static_cast<ErrorBoundMode>(mode), radius, outlier_cap);
+            c.zigzag_codes = chain == 3 || chain == 4 || chain == 7;
+            c.inplace_outliers = chain == 7;
+            auto* q = p.addStage<QuantizerStage<float, uint32_t>>(c);
+            if (chain == 3) {
+                auto* d = p.addStage<DifferenceStage<int32_t, uint32_t>>();
+                d->setChunkSize(16384);
+                p.connect(d, q, "codes");
+                bs_rze(d, "output", 2);
+            } else if (chain == 4) {
+                bs_rze(q, "codes", 4);
+            } else if (chain == 5) {
+                auto* l = p.addStage<LorenzoStage<int32_t>>();
+                auto* bp = p.addStage<BitpackStage<uint32_t>>();
+                bp->setNBits(16);
+                p.connect(l, q, "codes");
+                p.connect(bp, l);
+            } else {
+                auto* zz = p.addStage<ZigzagStage<int32_t, uint32_t>>();
+                p.connect(zz, q, "codes");
+                bs_rze(zz, "output", 4);
+            }
+        }
+        p.finalize();
+        void* out = nullptr;
+        size_t sz = 0;
+        p.compress(d_in, n * sizeof(float), &out, &sz, 0);
+        if (cudaStreamSynchronize(0) != cudaSuccess) throw std::runtime_error("sync failed");
+        *comp_bytes = sz;
+        p.writeToFile(path, 0);
+        void* dec = nullptr;
+        size_t dsz = 0;
+        p.decompress(nullptr, 0, &dec, &dsz, 0);
+        if (cudaStreamSynchronize(0) != cudaSuccess) throw std::runtime_error("sync failed");
+        *decomp_bytes = dsz;
+        if (d_decomp && dec) cudaMemcpy(d_decomp, dec, dsz, cudaMemcpyDeviceToDevice);
         if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device sync failed");
     } catch (const std::exception& e) {
         g_err = e.what();
