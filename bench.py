@@ -10,8 +10,9 @@ end-to-end (host buffers, copies inside the timed region) figures, the CPU
 baseline and clock samples sit beside it in the same JSON line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-  python bench.py --workload c1|c3|batch|selector   (secondary workloads,
-      one JSON line each; fzgpumodules_b200/benchmarks.py)
+  python bench.py --workload c1|cli|c3|batch|selector|pfpl   (secondary
+      workloads, one JSON line each; fzgpumodules_b200/benchmarks.py;
+      --impl reference --workload pfpl times the reference's own pipeline)
 
 Under torchrun each rank compresses its own field (no data exchange: the
 path shards by field); timings are maxed over ranks.
@@ -420,6 +421,41 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_pfpl(args):
+    """Reference arm of the pfpl workload: the reference's own fz::Pipeline
+    (built from its sources into oracle/_ref) compressing and decompressing
+    the same 512^3 field on this GPU, each call timed with CUDA events."""
+    import ctypes as C
+
+    import torch
+
+    from fzgpumodules_b200 import benchmarks
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "_ref", "libfzref_pipe.so")
+    base = {"impl": "reference", "workload": "pfpl"}
+    if not os.path.exists(path):
+        return dict(base, unavailable="the reference pipeline build (oracle/_ref/libfzref_pipe.so) is absent")
+    dev = torch.device("cuda", 0)
+    x = benchmarks.pfpl_field(dev)
+    n = x.numel()
+    L = C.CDLL(path)
+    L.ref_pipe_last_error.restype = C.c_char_p
+    cm, dm, cb = C.c_float(0), C.c_float(0), C.c_size_t(0)
+    rc = L.ref_pipeline_time_pfpl(C.c_void_p(x.data_ptr()), C.c_size_t(n), C.c_float(1e-3), C.c_float(0.1),
+                                  args.steps, args.warmup, C.byref(cm), C.byref(dm), C.byref(cb))
+    if rc != 0:
+        return dict(base, unavailable="reference pipeline failed: " + L.ref_pipe_last_error().decode())
+    v = 4 * n / cm.value / 1e6
+    return dict(base, metric="compress GB/s of the pfpl preset pipeline", value=v, unit="GB/s", n_gpus=1,
+                steps=args.steps, warmup=args.warmup, higher_is_better=True, dtype="f32", data="synthetic",
+                config={"workload": "pfpl: Quantizer(REL 1e-3)->Difference->Bitshuffle->RZE, 512^3 GRF",
+                        "flush": "256 MiB written between calls"},
+                compress_ms=cm.value, decompress_ms=dm.value, decompress_gbs=4 * n / dm.value / 1e6,
+                compressed_bytes=cb.value, e2e={"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                                                "d2h_bytes_per_step": 0},
+                note="the reference's GPU pipeline through its public API (Pipeline::compress / decompress, "
+                     "host synchronisation included)")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -430,9 +466,13 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--dims", type=int, nargs=3, default=list(DEFAULT_DIMS), metavar=("NX", "NY", "NZ"),
                     help="field extents (x fastest); the default is the 512^3 workload")
-    ap.add_argument("--workload", default="chain", choices=["chain", "c1", "cli", "c3", "batch", "selector"],
+    ap.add_argument("--workload", default="chain", choices=["chain", "c1", "cli", "c3", "batch", "selector", "pfpl"],
                     help="chain: the headline LQ3D->BS->RZE line; others: secondary workloads (1 GPU)")
     args = ap.parse_args()
+    if args.workload == "pfpl" and args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(run_reference_pfpl(args)), flush=True)
+        return
     if args.workload != "chain":
         import torch
 

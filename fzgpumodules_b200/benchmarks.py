@@ -13,7 +13,9 @@ as one JSON line with the same keys as the headline line:
                 {1e-2, 1e-3, 1e-4}) through the batched chain replayed from one
                 CUDA graph, against 64 plain per-field calls;
 * ``selector``  2 GiB of mixed fields -> LorenzoQuant (REL 1e-3) codes in 64 KiB
-                chunks, coded by exhaustive trial and by the trained MLP selector.
+                chunks, coded by exhaustive trial and by the trained MLP selector;
+* ``pfpl``      the pfpl preset, Quantizer (REL 1e-3) -> Difference -> Bitshuffle
+                -> RZE, on a 512^3 field, as kernels and through fz::Pipeline.
 
 Timing: CUDA events on the launching stream after warm-up; inputs larger than
 L2 or an L2 flush between timed iterations.
@@ -255,4 +257,87 @@ def run_selector(args, dev):
                   "bytes_unit": "GB/s of 16-bit codes (2 B per value)"})
 
 
-WORKLOADS = {"c1": run_c1, "cli": run_cli, "c3": run_c3, "batch": run_batch, "selector": run_selector}
+PFPL_DIMS = (512, 512, 512)
+
+
+def pfpl_field(dev):
+    """The pfpl workload's input: a 512^3 Gaussian random field with 0.1 % spikes."""
+    return F.grf(PFPL_DIMS[::-1], seed=1006, spike_frac=1e-3, device=dev).reshape(-1)
+
+
+def run_pfpl(args, dev):
+    """The pfpl preset (examples/presets/pfpl.toml): Quantizer(REL 1e-3, u32
+    codes, zigzag, outlier capacity 0.1) -> Difference(int32 -> uint32,
+    16 KiB chunks) -> Bitshuffle(16384, ew 2) -> RZE(16384, 4), as the stage
+    kernels run back to back on device-resident data and through fz::Pipeline."""
+    from .pipeline import (BitshuffleStage, DifferenceStage, Pipeline, QuantizerStage, RZEStage, INT32, PREALLOCATE,
+                           REL, UINT32)
+    x = pfpl_field(dev)
+    n = x.numel()
+    wq, wd, wr = K.Workspace(), K.Workspace(), K.Workspace()
+    q = K.quantizer_forward(x, 1e-3, K.REL, 32768, 4, True, 0.1, ws=wq)
+    rze, size = K.rze_encode(K.bitshuffle(K.diff(q["codes"], 16384, True, ws=wd), 16384, 2), ws=wr)
+    comp_bytes = rze.numel() + 8 * int(q["count"].item()) + 4
+
+    def comp():
+        K.quantizer_forward(x, 1e-3, K.REL, 32768, 4, True, 0.1, ws=wq, out=q, check_status=False)
+        d = K.diff(q["codes"], 16384, True, ws=wd)
+        K.rze_encode(K.bitshuffle(d, 16384, 2), ws=wr, trim=False)
+
+    def decomp():
+        b = K.bitshuffle(K.rze_decode(rze, 4 * n, ws=wr), 16384, 2, inverse=True)
+        c = K.diff(b.view(torch.int32), 16384, True, inverse=True, ws=wd)
+        return K.quantizer_inverse(c, 1e-3, K.REL, 0.0, 32768, True, vals=q["vals"], idx=q["idx"],
+                                   count=q["count"], cap=q["cap"])
+
+    y = decomp()
+    rel_ok = bool(((y.double() - x.double()).abs() <= x.double().abs() * 1e-3 * 1.01).all())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    tc = _time(comp, args.steps, args.warmup, flush)
+    td = _time(decomp, args.steps, args.warmup, flush)
+    assert wq.status() == 0 and wr.status() == 0
+    per_kernel = {}
+    for fn in (comp, decomp):
+        with K.Trace():
+            for _ in range(args.steps):
+                flush.zero_()
+                fn()
+            torch.cuda.synchronize()
+            for k, (launches, ms) in K.Trace.kernels().items():
+                per_kernel[k] = round(ms / launches, 4)
+    # through fz::Pipeline (each call includes the pipeline's host synchronisation)
+    pl = Pipeline(n * 4, PREALLOCATE)
+    qs = pl.addStage(QuantizerStage(1e-3, REL, 32768, 0.1, code_bytes=4, zigzag_codes=True))
+    ds = pl.addStage(DifferenceStage(INT32, UINT32, 16384))
+    bs = pl.addStage(BitshuffleStage(16384, 2))
+    rz = pl.addStage(RZEStage(16384, 4))
+    pl.connect(ds, qs, "codes")
+    pl.connect(bs, ds)
+    pl.connect(rz, bs)
+    pl.finalize()
+    cp = pl.compress(x).clone()
+    tpc = _time(lambda: pl.compress(x), args.steps, args.warmup, flush)
+    tpd = _time(lambda: pl.decompress(), args.steps, args.warmup, flush)
+    pl.close()
+    peak = None
+    try:
+        import json as _j
+        import os as _o
+        with open(_o.path.join(_o.path.dirname(_o.path.dirname(_o.path.abspath(__file__))), "MEASURED_PEAKS.json")) as f:
+            peak = float(_j.load(f)["hbm_gbs"])
+    except Exception:
+        peak = None
+    qf = per_kernel.get("quantizer_fwd")
+    q_gbs = 8 * n / qf / 1e6 if qf else None  # 4 B read + 4 B code written per value
+    return _line("pfpl: Quantizer(REL 1e-3, u32, zigzag)->Difference(i32->u32, 16 KiB)->Bitshuffle(16384, ew2)->RZE, "
+                 "512^3 GRF", 4 * n / tc / 1e6, "GB/s", args,
+                 {"compress_ms": tc, "decompress_ms": td, "decompress_gbs": 4 * n / td / 1e6,
+                  "pipeline_compress_gbs": 4 * n / tpc / 1e6, "pipeline_decompress_gbs": 4 * n / tpd / 1e6,
+                  "pipeline_compressed_bytes": cp.numel(), "ratio": 4 * n / comp_bytes,
+                  "outliers": int(q["count"].item()), "rel_bound_held": rel_ok, "kernel_ms": per_kernel,
+                  "quantizer_fwd_gbs": q_gbs, "quantizer_fwd_frac_of_measured_hbm": (q_gbs / peak) if (q_gbs and peak) else None,
+                  "note": "kernel chain on device-resident data (value); pipeline_* through fz::Pipeline with its host syncs"})
+
+
+WORKLOADS = {"c1": run_c1, "cli": run_cli, "c3": run_c3, "batch": run_batch, "selector": run_selector,
+             "pfpl": run_pfpl}

@@ -550,6 +550,7 @@ extern "C" {
 int fzb_zigzag(const void* d_in, uint64_t n, int elem_bytes, int inverse, void* d_out, void* stream) {
     if ((!d_in || !d_out) && n) return FZB_E_INVALID;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    TraceScope ts(s, "zigzag");
     return inverse ? xform_dispatch<kZzDec>(d_in, n, elem_bytes, d_out, s)
                    : xform_dispatch<kZzEnc>(d_in, n, elem_bytes, d_out, s);
 }
@@ -557,6 +558,7 @@ int fzb_zigzag(const void* d_in, uint64_t n, int elem_bytes, int inverse, void* 
 int fzb_negabinary(const void* d_in, uint64_t n, int elem_bytes, int inverse, void* d_out, void* stream) {
     if ((!d_in || !d_out) && n) return FZB_E_INVALID;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    TraceScope ts(s, "negabinary");
     return inverse ? xform_dispatch<kNbDec>(d_in, n, elem_bytes, d_out, s)
                    : xform_dispatch<kNbEnc>(d_in, n, elem_bytes, d_out, s);
 }
@@ -575,6 +577,7 @@ int fzb_diff(const void* d_in, uint64_t n, int elem_bytes, uint64_t chunk_elems,
     const ScanWork w = carve_scan(d_work, n);
     if (inverse && (!d_work || work_bytes < w.need)) return FZB_E_WORKSPACE;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    TraceScope ts(s, inverse ? "diff_inv" : "diff_fwd");
     switch (elem_bytes) {
         case 1: return diff_typed<uint8_t>(d_in, n, chunk_elems, negabinary, inverse, d_out, w, s);
         case 2: return diff_typed<uint16_t>(d_in, n, chunk_elems, negabinary, inverse, d_out, w, s);
@@ -595,6 +598,7 @@ int fzb_lorenzo_int(const void* d_in, const uint64_t dims[3], uint64_t n, int el
     const ScanWork w = carve_scan(d_work, n);
     if (inverse && nd && (!d_work || work_bytes < w.need)) return FZB_E_WORKSPACE;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    TraceScope ts(s, inverse ? "lorenzo_int_inv" : "lorenzo_int_fwd");
     switch (elem_bytes) {
         case 1: return lorenzo_typed<uint8_t>(d_in, d, n, inverse, d_out, w, s);
         case 2: return lorenzo_typed<uint16_t>(d_in, d, n, inverse, d_out, w, s);

@@ -285,28 +285,33 @@ def lorenzo_int(data: torch.Tensor, dims, inverse: bool = False, ws: Workspace |
 
 def quantizer_forward(x: torch.Tensor, eb: float, mode: int = ABS, radius: int = 32768, code_bytes: int = 2,
                       zigzag: bool = False, outlier_capacity: float = 0.05, threshold: float = float("inf"),
-                      inplace: bool = False, value_base: float = 0.0, ws: Workspace | None = None) -> dict:
+                      inplace: bool = False, value_base: float = 0.0, ws: Workspace | None = None,
+                      out: dict | None = None, check_status: bool = True) -> dict:
     """QuantizerStage<float, TCode> forward (quantizers/quantizer/quantizer.cu).
     Returns codes, index-ordered outlier lists, capped count, cap and the
-    device-resolved bound (value_base, abs_eb, 1/(2 abs_eb), 2 abs_eb)."""
+    device-resolved bound (value_base, abs_eb, 1/(2 abs_eb), 2 abs_eb).
+    check_status=False skips the synchronising read of the device status
+    (read it later with ws.status()); `out` reuses a previous result's buffers."""
     ws = ws or _default_ws
     src = _flat(x)
     n, dev = src.numel(), src.device
     cap = 0 if (inplace and mode != REL) else max_outliers(n, outlier_capacity)
     ctype = torch.int16 if code_bytes == 2 else torch.int32
-    out = dict(codes=torch.empty(n, dtype=ctype, device=dev),
-               vals=torch.empty(max(cap, 1), dtype=torch.float32, device=dev),
-               idx=torch.empty(max(cap, 1), dtype=torch.int32, device=dev),
-               count=torch.zeros(1, dtype=torch.int32, device=dev),
-               eb_state=torch.zeros(4, dtype=torch.float32, device=dev), cap=cap)
+    if out is None:
+        out = dict(codes=torch.empty(n, dtype=ctype, device=dev),
+                   vals=torch.empty(max(cap, 1), dtype=torch.float32, device=dev),
+                   idx=torch.empty(max(cap, 1), dtype=torch.int32, device=dev),
+                   count=torch.zeros(1, dtype=torch.int32, device=dev),
+                   eb_state=torch.zeros(4, dtype=torch.float32, device=dev), cap=cap)
     wp, wn = ws.get_bytes(lib().fzb_quantizer_workspace_bytes(n), dev)
     check(lib().fzb_quantizer_forward(_ptr(src), n, code_bytes, eb, mode, value_base, radius, int(zigzag), threshold,
                                       int(inplace), _ptr(out["codes"]), _ptr(out["vals"]), _ptr(out["idx"]),
                                       _ptr(out["count"]), cap, _ptr(out["eb_state"]), wp, wn, _stream(dev)),
           "fzb_quantizer_forward")
-    st = lib().fzb_workspace_status(wp, _stream(dev))
-    if st != 0:
-        raise FzbError(st, "fzb_quantizer_forward")
+    if check_status:
+        st = lib().fzb_workspace_status(wp, _stream(dev))
+        if st != 0:
+            raise FzbError(st, "fzb_quantizer_forward")
     return out
 
 

@@ -158,3 +158,72 @@ extern "C" int ref_pipeline_codes(int chain, const float* d_in, size_t n, size_t
     }
     return 0;
 }
+
+// Times the reference's pfpl chain (chain 3 above: Quantizer REL -> Difference
+// -> Bitshuffle -> RZE) through its own Pipeline::compress / decompress on
+// the default stream: `warmup` untimed calls, then the mean of `steps` calls
+// each bracketed by CUDA events.  Every call includes the reference's own
+// host synchronisation.  A 256 MiB buffer is rewritten between calls to
+// evict L2.
+extern "C" int ref_pipeline_time_pfpl(const float* d_in, size_t n, float eb, float outlier_cap, int steps, int warmup,
+                                      float* comp_ms, float* decomp_ms, size_t* comp_bytes) {
+    try {
+        Pipeline p(n * sizeof(float), MemoryStrategy::PREALLOCATE, 3.0f);
+        p.setDims(n, 1, 1);
+        QuantizerStage<float, uint32_t>::Config c(eb, ErrorBoundMode::REL, 32768, outlier_cap);
+        c.zigzag_codes = true;
+        auto* q = p.addStage<QuantizerStage<float, uint32_t>>(c);
+        auto* d = p.addStage<DifferenceStage<int32_t, uint32_t>>();
+        d->setChunkSize(16384);
+        auto* bs = p.addStage<BitshuffleStage>();
+        bs->setBlockSize(16384);
+        bs->setElementWidth(2);
+        auto* rze = p.addStage<RZEStage>();
+        rze->setLevels(4);
+        p.connect(d, q, "codes");
+        p.connect(bs, d);
+        p.connect(rze, bs);
+        p.finalize();
+        void* flush = nullptr;
+        if (cudaMalloc(&flush, 256u << 20) != cudaSuccess) throw std::runtime_error("flush alloc failed");
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        double tc = 0, td = 0;
+        void* out = nullptr;
+        size_t sz = 0;
+        for (int i = 0; i < warmup + steps; i++) {
+            cudaMemsetAsync(flush, i & 0xff, 256u << 20, 0);
+            cudaEventRecord(a, 0);
+            p.compress(d_in, n * sizeof(float), &out, &sz, 0);
+            cudaEventRecord(b, 0);
+            cudaEventSynchronize(b);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            if (i >= warmup) tc += ms;
+            cudaMemsetAsync(flush, i & 0xff, 256u << 20, 0);
+            void* dec = nullptr;
+            size_t dsz = 0;
+            cudaEventRecord(a, 0);
+            p.decompress(nullptr, 0, &dec, &dsz, 0);
+            cudaEventRecord(b, 0);
+            cudaEventSynchronize(b);
+            cudaEventElapsedTime(&ms, a, b);
+            if (i >= warmup) td += ms;
+        }
+        *comp_ms = (float)(tc / steps);
+        *decomp_ms = (float)(td / steps);
+        *comp_bytes = sz;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaFree(flush);
+        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device sync failed");
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    } catch (...) {
+        g_err = "unknown exception";
+        return -1;
+    }
+    return 0;
+}
