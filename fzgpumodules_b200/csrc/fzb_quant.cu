@@ -23,10 +23,15 @@
 // like the reference's kernels: its REL path calls __log2f and exp2f, and the
 // codes must come out bit-identical.
 //
-// Forward kernel: tiles of 2048 elements (256 threads x 8, element k*256 + t
-// of the tile in thread t) taken in ticket order; codes are written
-// coalesced; outlier slots come from per-(k, warp) ballot counts ordered by
-// index and a decoupled look-back over the tiles' outlier counts.
+// Forward: two kernels and no inter-CTA waits.  quantizer_codes_kernel
+// streams tiles of 4096 values (256 threads x four 16-byte loads; element
+// k*1024 + 4t + j in thread t), writes the codes with vector stores and
+// records each tile's outlier count, summed per group of 256 tiles.
+// quantizer_outliers_kernel then revisits only the tiles that hold outliers
+// (the first kernel appends them to a list):
+// it takes the tile's offset from the group and tile counts before it,
+// recomputes the outlier flags from the input and writes (value, index)
+// pairs in index order; its block 0 stores min(total, cap) as the count.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -40,8 +45,8 @@
 namespace fzb {
 namespace {
 
-constexpr int kQPer = 8;
-constexpr uint32_t kQTile = (uint32_t)kThreads * kQPer;  // 2048
+constexpr uint32_t kQTile = 4096;   // values per tile: 256 threads x 4 granules of 4
+constexpr uint32_t kQGroup = 256;   // tiles per group count
 constexpr int kQWarps = kThreads / 32;
 constexpr int kQMaxParts = 1024;
 
@@ -58,10 +63,12 @@ struct QArgs {
     uint32_t* oidx;
     uint32_t* count;
     uint64_t cap;
-    unsigned long long* status;
-    uint32_t* ticket;
-    uint32_t* err;
-    uint32_t ntiles;
+    uint32_t* tile_cnt;   // outliers per tile
+    uint32_t* group_cnt;  // outliers per group of kQGroup tiles (zeroed per launch)
+    uint32_t* list;       // tiles holding outliers, in completion order
+    uint32_t* list_len;   // zeroed per launch
+    uint32_t ntiles, ngroups;
+    int vec;              // input 16-byte aligned, codes aligned for 4-code stores
 };
 
 template <typename TC>
@@ -107,69 +114,165 @@ __device__ __forceinline__ TC quantize_one(const QArgs& a, float x, float ebx2_r
     return (TC)0;
 }
 
+// Four consecutive values of granule k of this thread's tile (zero past n).
+__device__ __forceinline__ float4 load_granule(const QArgs& a, uint64_t i0, bool full) {
+    if (full) return __ldcs(reinterpret_cast<const float4*>(a.in + i0));
+    float4 v;
+    v.x = i0 < a.n ? a.in[i0] : 0.0f;
+    v.y = i0 + 1 < a.n ? a.in[i0 + 1] : 0.0f;
+    v.z = i0 + 2 < a.n ? a.in[i0 + 2] : 0.0f;
+    v.w = i0 + 3 < a.n ? a.in[i0 + 3] : 0.0f;
+    return v;
+}
+
+// Quantises granule k; returns the 4-bit outlier mask of its valid values.
 template <typename TC, bool REL>
-__global__ void __launch_bounds__(kThreads) quantizer_fwd_kernel(QArgs a) {
-    __shared__ uint32_t s_tile, s_total;
-    __shared__ uint32_t s_off[kQPer * kQWarps];  // (k, warp) counts, then exclusive offsets
-    __shared__ unsigned long long s_red[2 * kQWarps + 2];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    if (t == 0) s_tile = atomicAdd(a.ticket, 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    const uint64_t base = (uint64_t)tile * kQTile;
-    const float ebx2_r = REL ? 0.0f : a.st[2];
-    TC* codes = static_cast<TC*>(a.codes);
-    float xv[kQPer];
+__device__ __forceinline__ uint32_t quantize_granule(const QArgs& a, const float4& v, uint64_t i0, float r,
+                                                     TC (&c)[4]) {
+    const float x[4] = {v.x, v.y, v.z, v.w};
+    uint32_t m = 0;
 #pragma unroll
-    for (int k = 0; k < kQPer; k++) {
-        const uint64_t i = base + (uint64_t)k * kThreads + t;
-        xv[k] = i < a.n ? __ldcs(a.in + i) : 0.0f;
+    for (int j = 0; j < 4; j++) {
+        bool o;
+        c[j] = quantize_one<TC, REL>(a, x[j], r, o);
+        if (o && i0 + j < a.n) m |= 1u << j;
     }
-    uint32_t om = 0;
+    return m;
+}
+
+template <typename TC, bool REL>
+__global__ void __launch_bounds__(kThreads) quantizer_codes_kernel(QArgs a) {
+    __shared__ uint32_t s_w[kQWarps];
+    const int t = threadIdx.x;
+    const uint64_t base = (uint64_t)blockIdx.x * kQTile;
+    const bool full = a.vec && base + kQTile <= a.n;
+    const float r = REL ? 0.0f : a.st[2];
+    TC* codes = static_cast<TC*>(a.codes);
+    float4 v[4];
 #pragma unroll
-    for (int k = 0; k < kQPer; k++) {
-        const uint64_t i = base + (uint64_t)k * kThreads + t;
-        if (i < a.n) {
-            bool o;
-            codes[i] = quantize_one<TC, REL>(a, xv[k], ebx2_r, o);
-            om |= (o ? 1u : 0u) << k;
+    for (int k = 0; k < 4; k++) v[k] = load_granule(a, base + (uint64_t)k * 1024 + 4 * t, full);
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint64_t i0 = base + (uint64_t)k * 1024 + 4 * t;
+        TC c[4];
+        cnt += __popc(quantize_granule<TC, REL>(a, v[k], i0, r, c));
+        if (full) {
+            if (sizeof(TC) == 4) {
+                *reinterpret_cast<uint4*>(codes + i0) = make_uint4(c[0], c[1], c[2], c[3]);
+            } else {
+                *reinterpret_cast<uint2*>(codes + i0) =
+                    make_uint2((uint32_t)c[0] | ((uint32_t)c[1] << 16), (uint32_t)c[2] | ((uint32_t)c[3] << 16));
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (i0 + j < a.n) codes[i0 + j] = c[j];
         }
     }
 #pragma unroll
-    for (int k = 0; k < kQPer; k++) {
-        const uint32_t b = __ballot_sync(0xffffffffu, (om >> k) & 1u);
-        if (lane == 0) s_off[k * kQWarps + warp] = __popc(b);
-    }
+    for (int d = 16; d >= 1; d >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
+    if ((t & 31) == 0) s_w[t >> 5] = cnt;
     __syncthreads();
-    if (warp == 0) {  // 64 (k, warp) entries in index order, two per lane
-        const uint32_t c0 = s_off[2 * lane], c1 = s_off[2 * lane + 1];
-        const uint32_t inc = warp_incl_scan(c0 + c1);
-        const uint32_t ex = inc - c0 - c1;
-        s_off[2 * lane] = ex;
-        s_off[2 * lane + 1] = ex + c0;
-        if (lane == 31) s_total = inc;
-    }
-    __syncthreads();
-    const uint32_t total = s_total;
-    const uint64_t prefix = lookback(a.status, tile, total, a.err, s_red);
-    if (total) {
-        const uint32_t below = (1u << lane) - 1u;
+    if (t == 0) {
+        uint32_t total = 0;
 #pragma unroll
-        for (int k = 0; k < kQPer; k++) {
-            const uint32_t b = __ballot_sync(0xffffffffu, (om >> k) & 1u);
-            if ((om >> k) & 1u) {
-                const uint64_t slot = prefix + s_off[k * kQWarps + warp] + __popc(b & below);
+        for (int w = 0; w < kQWarps; w++) total += s_w[w];
+        a.tile_cnt[blockIdx.x] = total;
+        if (total) {
+            atomicAdd(a.group_cnt + blockIdx.x / kQGroup, total);
+            a.list[atomicAdd(a.list_len, 1u)] = blockIdx.x;
+        }
+    }
+}
+
+// Block-wide sum of one value per thread (result in every thread).
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* s_w) {
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint32_t t = 0;
+#pragma unroll
+    for (int w = 0; w < kQWarps; w++) t += s_w[w];
+    return t;
+}
+
+template <typename TC, bool REL>
+__device__ __forceinline__ void write_tile_outliers(const QArgs& a, uint32_t tile, uint32_t* s_w,
+                                                    unsigned long long* s_wx) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    // offset: every outlier in earlier groups and in earlier tiles of this group
+    const uint32_t g = tile / kQGroup;
+    uint32_t part = 0;
+    for (uint32_t i = t; i < g; i += kThreads) part += a.group_cnt[i];
+    for (uint32_t i = g * kQGroup + t; i < tile; i += kThreads) part += a.tile_cnt[i];
+    const uint64_t prefix = block_sum(part, s_w);
+    if (prefix >= a.cap) return;
+    const uint64_t base = (uint64_t)tile * kQTile;
+    const bool full = a.vec && base + kQTile <= a.n;
+    const float r = REL ? 0.0f : a.st[2];
+    float4 v[4];
+    uint32_t m[4];
+    unsigned long long packed = 0;  // 16-bit outlier count of granule k in bits 16k..16k+15
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        v[k] = load_granule(a, base + (uint64_t)k * 1024 + 4 * t, full);
+        TC c[4];
+        m[k] = quantize_granule<TC, REL>(a, v[k], base + (uint64_t)k * 1024 + 4 * t, r, c);
+        packed |= (unsigned long long)__popc(m[k]) << (16 * k);
+    }
+    // exclusive block scan of the packed counts: four independent 16-bit lanes
+    unsigned long long inc = packed;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long o = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc += o;
+    }
+    __syncthreads();
+    if (lane == 31) s_wx[warp] = inc;
+    __syncthreads();
+    unsigned long long before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < kQWarps; w++) {
+        if (w < warp) before += s_wx[w];
+        all += s_wx[w];
+    }
+    const unsigned long long excl = before + inc - packed;
+    uint64_t kbase = prefix;  // outliers of granules < k across the tile come first
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        uint64_t slot = kbase + ((excl >> (16 * k)) & 0xffffu);
+        const float x[4] = {v[k].x, v[k].y, v[k].z, v[k].w};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if ((m[k] >> j) & 1u) {
                 if (slot < a.cap) {
-                    a.ovals[slot] = xv[k];
-                    a.oidx[slot] = (uint32_t)(base + (uint64_t)k * kThreads + t);
+                    a.ovals[slot] = x[j];
+                    a.oidx[slot] = (uint32_t)(base + (uint64_t)k * 1024 + 4 * t + j);
                 }
+                slot++;
             }
         }
+        kbase += (all >> (16 * k)) & 0xffffu;
     }
-    if (tile == a.ntiles - 1 && t == 0) {
-        const uint64_t all = prefix + total;
-        *a.count = (uint32_t)(all < a.cap ? all : a.cap);
+}
+
+// The grid walks the list of tiles that hold outliers.  A tile's slots
+// depend only on the counts before it, so the list order does not matter.
+template <typename TC, bool REL>
+__global__ void __launch_bounds__(kThreads) quantizer_outliers_kernel(QArgs a) {
+    __shared__ uint32_t s_w[kQWarps];
+    __shared__ unsigned long long s_wx[kQWarps];
+    if (blockIdx.x == 0) {  // the stored count: min(total, cap)
+        uint32_t part = 0;
+        for (uint32_t g = threadIdx.x; g < a.ngroups; g += kThreads) part += a.group_cnt[g];
+        const uint32_t total = block_sum(part, s_w);
+        if (threadIdx.x == 0) *a.count = (uint32_t)((uint64_t)total < a.cap ? total : a.cap);
     }
+    const uint32_t len = *a.list_len;
+    for (uint32_t i = blockIdx.x; i < len; i += gridDim.x) write_tile_outliers<TC, REL>(a, a.list[i], s_w, s_wx);
 }
 
 __global__ void __launch_bounds__(256) quantizer_fwd_inplace_kernel(const float* __restrict__ in, uint64_t n,
@@ -187,42 +290,76 @@ __global__ void __launch_bounds__(256) quantizer_fwd_inplace_kernel(const float*
 }
 
 template <typename TC, bool REL>
-__global__ void __launch_bounds__(256) quantizer_inv_kernel(const TC* __restrict__ codes, uint64_t n, float ebx2,
-                                                            float log2eb, int zigzag, float* __restrict__ out) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const TC c = codes[i];
-        float v;
-        if (!REL) {
-            using S = typename std::make_signed<TC>::type;
-            const int q = zigzag ? unzigzag_code<TC>(c) : (int)(S)c;
-            v = (float)q * ebx2;
-        } else if (c == 0) {
-            v = 0.0f;
-        } else {
-            const uint32_t cv = (uint32_t)c - 1u;
-            const int alb = (int)(cv >> 2);
-            const int lb = ((cv >> 1) & 1u) ? -alb : alb;
-            const float ar = exp2f((float)lb * log2eb);
-            v = (cv & 1u) ? -ar : ar;
-        }
-        out[i] = v;
+__device__ __forceinline__ float dequant_one(TC c, float ebx2, float log2eb, int zigzag) {
+    if (!REL) {
+        using S = typename std::make_signed<TC>::type;
+        const int q = zigzag ? unzigzag_code<TC>(c) : (int)(S)c;
+        return (float)q * ebx2;
     }
+    if (c == 0) return 0.0f;
+    const uint32_t cv = (uint32_t)c - 1u;
+    const int alb = (int)(cv >> 2);
+    const int lb = ((cv >> 1) & 1u) ? -alb : alb;
+    const float ar = exp2f((float)lb * log2eb);
+    return (cv & 1u) ? -ar : ar;
 }
 
-__global__ void __launch_bounds__(256) quantizer_inv_inplace_kernel(const uint32_t* __restrict__ codes, uint64_t n,
-                                                                    float ebx2, uint32_t radius,
-                                                                    float* __restrict__ out) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t c = codes[i];
-        if ((c >> 1) >= radius) {
-            out[i] = __uint_as_float(c);
+__device__ __forceinline__ float dequant_inplace(uint32_t c, float ebx2, uint32_t radius) {
+    if ((c >> 1) >= radius) return __uint_as_float(c);
+    const int32_t ci = (int32_t)c;
+    const int q = (ci & 1) ? -((ci + 1) >> 1) : (ci >> 1);
+    return (float)q * ebx2;
+}
+
+// Four codes of granule i0 (zero past n).
+template <typename TC>
+__device__ __forceinline__ void load_codes(const TC* __restrict__ codes, uint64_t i0, uint64_t n, bool full,
+                                           TC (&c)[4]) {
+    if (full) {
+        if (sizeof(TC) == 4) {
+            const uint4 u = __ldcs(reinterpret_cast<const uint4*>(codes + i0));
+            c[0] = (TC)u.x, c[1] = (TC)u.y, c[2] = (TC)u.z, c[3] = (TC)u.w;
         } else {
-            const int32_t ci = (int32_t)c;
-            const int q = (ci & 1) ? -((ci + 1) >> 1) : (ci >> 1);
-            out[i] = (float)q * ebx2;
+            const uint2 u = __ldcs(reinterpret_cast<const uint2*>(codes + i0));
+            c[0] = (TC)(u.x & 0xffffu), c[1] = (TC)(u.x >> 16), c[2] = (TC)(u.y & 0xffffu), c[3] = (TC)(u.y >> 16);
         }
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) c[j] = i0 + j < n ? codes[i0 + j] : (TC)0;
+}
+
+__device__ __forceinline__ void store_values(float* __restrict__ out, uint64_t i0, uint64_t n, bool full,
+                                             const float (&y)[4]) {
+    if (full) {
+        __stcs(reinterpret_cast<float4*>(out + i0), make_float4(y[0], y[1], y[2], y[3]));
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (i0 + j < n) out[i0 + j] = y[j];
+}
+
+// One block per tile of 4096 codes (granule k*1024 + 4t in thread t); all
+// loads are issued before any value is computed.  MODE 0 ABS/NOA, 1 REL,
+// 2 in-place outliers.
+template <typename TC, int MODE>
+__global__ void __launch_bounds__(256) quantizer_inv_kernel(const TC* __restrict__ codes, uint64_t n, float ebx2,
+                                                            float log2eb, int zigzag, uint32_t radius, int vec,
+                                                            float* __restrict__ out) {
+    const uint64_t base = (uint64_t)blockIdx.x * kQTile;
+    const bool full = vec && base + kQTile <= n;
+    TC c[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) load_codes(codes, base + (uint64_t)k * 1024 + 4 * threadIdx.x, n, full, c[k]);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float y[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            y[j] = MODE == 2 ? dequant_inplace((uint32_t)c[k][j], ebx2, radius)
+                             : dequant_one<TC, MODE == 1>(c[k][j], ebx2, log2eb, zigzag);
+        store_values(out, base + (uint64_t)k * 1024 + 4 * threadIdx.x, n, full, y);
     }
 }
 
@@ -239,30 +376,42 @@ __global__ void __launch_bounds__(256) scatter_assign_kernel(const float* __rest
     }
 }
 
+// Workspace: [256 B control: word 0 device status (fzb_workspace_status),
+// word 2 the value-range scan's completion counter, word 3 the outlier tile
+// list length][group counts][min / max partials][tile counts][tile list].  The control block and the group counts are
+// cleared by one memset per call.
 struct QWork {
-    uint32_t* err;     // word 0: device status bits (read by fzb_workspace_status)
-    uint32_t* ticket;  // word 1
-    uint32_t* mm_done; // word 2
+    uint32_t* err;
+    uint32_t* mm_done;
+    uint32_t* list_len;
+    uint32_t* group_cnt;
     float* pmin;
     float* pmax;
-    unsigned long long* status;
+    uint32_t* tile_cnt;
+    uint32_t* list;
+    size_t head;  // bytes cleared per call
     size_t need;
 };
 
 QWork carve_q(void* base, uint64_t n) {
     uint8_t* p = static_cast<uint8_t*>(base);
-    const uint64_t ntiles = (n + kQTile - 1) / kQTile;
+    const uint64_t ntiles = (n + kQTile - 1) / kQTile, ngroups = (ntiles + kQGroup - 1) / kQGroup;
     QWork w{};
     w.err = reinterpret_cast<uint32_t*>(p);
-    w.ticket = w.err ? w.err + 1 : nullptr;
     w.mm_done = w.err ? w.err + 2 : nullptr;
+    w.list_len = w.err ? w.err + 3 : nullptr;
     size_t off = 256;
+    w.group_cnt = p ? reinterpret_cast<uint32_t*>(p + off) : nullptr;
+    off += (ngroups * 4 + 255) / 256 * 256;
+    w.head = off;
     w.pmin = p ? reinterpret_cast<float*>(p + off) : nullptr;
     off += kQMaxParts * 4;
     w.pmax = p ? reinterpret_cast<float*>(p + off) : nullptr;
     off += kQMaxParts * 4;
-    w.status = p ? reinterpret_cast<unsigned long long*>(p + off) : nullptr;
-    off += ((ntiles + 1) * 8 + 255) / 256 * 256;
+    w.tile_cnt = p ? reinterpret_cast<uint32_t*>(p + off) : nullptr;
+    off += (ntiles * 4 + 255) / 256 * 256;
+    w.list = p ? reinterpret_cast<uint32_t*>(p + off) : nullptr;
+    off += (ntiles * 4 + 255) / 256 * 256;
     w.need = off;
     return w;
 }
@@ -307,9 +456,8 @@ int fzb_quantizer_forward(const float* d_in, uint64_t n, int code_bytes, float e
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // the stored radius is the TCode conversion of quant_radius
     const uint32_t R = code_bytes == 2 ? (uint32_t)(uint16_t)radius : radius;
-    if (cudaMemsetAsync(d_work, 0, 256, s) != cudaSuccess) return FZB_E_CUDA;
-    if (!inpl && cudaMemsetAsync(d_count, 0, 4, s) != cudaSuccess) return FZB_E_CUDA;
-    if (n == 0) return FZB_OK;
+    if (cudaMemsetAsync(d_work, 0, w.head, s) != cudaSuccess) return FZB_E_CUDA;
+    if (n == 0) return (inpl || cudaMemsetAsync(d_count, 0, 4, s) == cudaSuccess) ? FZB_OK : FZB_E_CUDA;
     {
         TraceScope ts(s, "quantizer_resolve_eb");
         if (eb_mode == FZB_NOA && !(value_base > 0.0f)) {
@@ -342,18 +490,33 @@ int fzb_quantizer_forward(const float* d_in, uint64_t n, int code_bytes, float e
     a.oidx = d_oidx;
     a.count = d_count;
     a.cap = cap;
-    a.status = w.status;
-    a.ticket = w.ticket;
-    a.err = w.err;
+    a.tile_cnt = w.tile_cnt;
+    a.group_cnt = w.group_cnt;
+    a.list = w.list;
+    a.list_len = w.list_len;
     a.ntiles = (uint32_t)((n + kQTile - 1) / kQTile);
-    if (cudaMemsetAsync(w.status, 0, (size_t)a.ntiles * 8, s) != cudaSuccess) return FZB_E_CUDA;
-    TraceScope ts(s, "quantizer_fwd");
+    a.ngroups = (a.ntiles + kQGroup - 1) / kQGroup;
+    a.vec = ((reinterpret_cast<uintptr_t>(d_in) & 15) == 0) &&
+            ((reinterpret_cast<uintptr_t>(d_codes) & (uintptr_t)(4 * code_bytes - 1)) == 0);
+    {
+        TraceScope ts(s, "quantizer_fwd");
+        if (code_bytes == 2) {
+            if (rel) quantizer_codes_kernel<uint16_t, true><<<a.ntiles, kThreads, 0, s>>>(a);
+            else quantizer_codes_kernel<uint16_t, false><<<a.ntiles, kThreads, 0, s>>>(a);
+        } else {
+            if (rel) quantizer_codes_kernel<uint32_t, true><<<a.ntiles, kThreads, 0, s>>>(a);
+            else quantizer_codes_kernel<uint32_t, false><<<a.ntiles, kThreads, 0, s>>>(a);
+        }
+        if (cudaGetLastError() != cudaSuccess) return FZB_E_CUDA;
+    }
+    TraceScope ts(s, "quantizer_outliers");
+    const unsigned og = a.ntiles < (uint32_t)device_sms() * 8 ? a.ntiles : (unsigned)device_sms() * 8;
     if (code_bytes == 2) {
-        if (rel) quantizer_fwd_kernel<uint16_t, true><<<a.ntiles, kThreads, 0, s>>>(a);
-        else quantizer_fwd_kernel<uint16_t, false><<<a.ntiles, kThreads, 0, s>>>(a);
+        if (rel) quantizer_outliers_kernel<uint16_t, true><<<og, kThreads, 0, s>>>(a);
+        else quantizer_outliers_kernel<uint16_t, false><<<og, kThreads, 0, s>>>(a);
     } else {
-        if (rel) quantizer_fwd_kernel<uint32_t, true><<<a.ntiles, kThreads, 0, s>>>(a);
-        else quantizer_fwd_kernel<uint32_t, false><<<a.ntiles, kThreads, 0, s>>>(a);
+        if (rel) quantizer_outliers_kernel<uint32_t, true><<<og, kThreads, 0, s>>>(a);
+        else quantizer_outliers_kernel<uint32_t, false><<<og, kThreads, 0, s>>>(a);
     }
     return cudaGetLastError() == cudaSuccess ? FZB_OK : FZB_E_CUDA;
 }
@@ -374,20 +537,25 @@ int fzb_quantizer_inverse(const void* d_codes, uint64_t n, int code_bytes, float
     const uint32_t R = code_bytes == 2 ? (uint32_t)(uint16_t)radius : radius;
     float log2eb = 0.0f, r_, o_, oo_;
     rel_params(eb, &log2eb, &r_, &o_, &oo_);
-    const unsigned g = elem_grid(n);
+    const uint64_t ntiles = (n + kQTile - 1) / kQTile;
+    if (ntiles > 0x7fffffffull) return FZB_E_INVALID;
+    const unsigned g = (unsigned)ntiles;
+    const int vec = ((reinterpret_cast<uintptr_t>(d_out) & 15) == 0) &&
+                    ((reinterpret_cast<uintptr_t>(d_codes) & (uintptr_t)(4 * code_bytes - 1)) == 0);
     TraceScope ts(s, "quantizer_inv");
     if (inpl) {
-        quantizer_inv_inplace_kernel<<<g, 256, 0, s>>>(static_cast<const uint32_t*>(d_codes), n, ebx2, R, d_out);
+        quantizer_inv_kernel<uint32_t, 2><<<g, 256, 0, s>>>(static_cast<const uint32_t*>(d_codes), n, ebx2, log2eb,
+                                                             zigzag, R, vec, d_out);
         return cudaGetLastError() == cudaSuccess ? FZB_OK : FZB_E_CUDA;
     }
     if (code_bytes == 2) {
         const uint16_t* c = static_cast<const uint16_t*>(d_codes);
-        if (rel) quantizer_inv_kernel<uint16_t, true><<<g, 256, 0, s>>>(c, n, ebx2, log2eb, zigzag, d_out);
-        else quantizer_inv_kernel<uint16_t, false><<<g, 256, 0, s>>>(c, n, ebx2, log2eb, zigzag, d_out);
+        if (rel) quantizer_inv_kernel<uint16_t, 1><<<g, 256, 0, s>>>(c, n, ebx2, log2eb, zigzag, R, vec, d_out);
+        else quantizer_inv_kernel<uint16_t, 0><<<g, 256, 0, s>>>(c, n, ebx2, log2eb, zigzag, R, vec, d_out);
     } else {
         const uint32_t* c = static_cast<const uint32_t*>(d_codes);
-        if (rel) quantizer_inv_kernel<uint32_t, true><<<g, 256, 0, s>>>(c, n, ebx2, log2eb, zigzag, d_out);
-        else quantizer_inv_kernel<uint32_t, false><<<g, 256, 0, s>>>(c, n, ebx2, log2eb, zigzag, d_out);
+        if (rel) quantizer_inv_kernel<uint32_t, 1><<<g, 256, 0, s>>>(c, n, ebx2, log2eb, zigzag, R, vec, d_out);
+        else quantizer_inv_kernel<uint32_t, 0><<<g, 256, 0, s>>>(c, n, ebx2, log2eb, zigzag, R, vec, d_out);
     }
     if (cudaGetLastError() != cudaSuccess) return FZB_E_CUDA;
     if (cap) {
