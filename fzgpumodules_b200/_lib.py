@@ -111,6 +111,14 @@ def lib():
         L.fzb_pipeline_add_huffman.argtypes = [p, u32]
         L.fzb_pipeline_add_huffman_mode.argtypes = [p, u32, i32]
         L.fzb_pipeline_add_bitpack.argtypes = [p, i32, i32]
+        L.fzb_pfpl_workspace_bytes.restype = sz
+        L.fzb_pfpl_workspace_bytes.argtypes = [u64, u64]
+        L.fzb_pfpl_compress.restype = i32
+        L.fzb_pfpl_compress.argtypes = [p, u64, f32, i32, f32, u32, i32, f32, p, p, u64, p, p, p, p, p, sz, p]
+        L.fzb_pfpl_decompress_workspace_bytes.restype = sz
+        L.fzb_pfpl_decompress_workspace_bytes.argtypes = [u64]
+        L.fzb_pfpl_decompress.restype = i32
+        L.fzb_pfpl_decompress.argtypes = [p, u64, p, p, p, u64, u64, f32, i32, f32, i32, p, p, sz, p]
         L.fzb_pipeline_add_quantizer.argtypes = [p, i32, f32, i32, i32, f32, i32, i32, f32, f32]
         L.fzb_pipeline_add_difference.argtypes = [p, i32, i32, u32]
         L.fzb_pipeline_add_lorenzo.argtypes = [p, i32]

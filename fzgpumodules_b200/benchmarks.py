@@ -296,8 +296,26 @@ def run_pfpl(args, dev):
     tc = _time(comp, args.steps, args.warmup, flush)
     td = _time(decomp, args.steps, args.warmup, flush)
     assert wq.status() == 0 and wr.status() == 0
+    # the one-pass chain (fzb_pfpl_compress / fzb_pfpl_decompress)
+    wf, wf2 = K.Workspace(), K.Workspace()
+    f = K.pfpl_compress(x, 1e-3, K.REL, 32768, True, 0.1, ws=wf)
+    fsize = int(f["rze_size"].item())
+    same = fsize == rze.numel() and bool(torch.equal(f["rze"][:fsize], rze))
+    yf = torch.empty_like(x)
+
+    def fcomp():
+        K.pfpl_compress(x, 1e-3, K.REL, 32768, True, 0.1, ws=wf, out=f)
+
+    def fdecomp():
+        K.pfpl_decompress(f["rze"], fsize, f["vals"], f["idx"], f["count"], f["cap"], n, ws=wf2, out=yf)
+
+    fdecomp()
+    fused_equal = bool(torch.equal(yf.view(torch.int32), y.view(torch.int32)))
+    tfc = _time(fcomp, args.steps, args.warmup, flush)
+    tfd = _time(fdecomp, args.steps, args.warmup, flush)
+    assert wf2.status() == 0
     per_kernel = {}
-    for fn in (comp, decomp):
+    for fn in (comp, decomp, fcomp, fdecomp):
         with K.Trace():
             for _ in range(args.steps):
                 flush.zero_()
@@ -329,14 +347,24 @@ def run_pfpl(args, dev):
         peak = None
     qf = per_kernel.get("quantizer_fwd")
     q_gbs = 8 * n / qf / 1e6 if qf else None  # 4 B read + 4 B code written per value
+    ck, dk = per_kernel.get("pfpl_chunk"), per_kernel.get("pfpl_decode")
+    # algorithmic bytes: the field read (written) plus the compressed stream written (read)
+    ck_gbs = (4 * n + comp_bytes) / ck / 1e6 if ck else None
+    dk_gbs = (4 * n + comp_bytes) / dk / 1e6 if dk else None
     return _line("pfpl: Quantizer(REL 1e-3, u32, zigzag)->Difference(i32->u32, 16 KiB)->Bitshuffle(16384, ew2)->RZE, "
-                 "512^3 GRF", 4 * n / tc / 1e6, "GB/s", args,
-                 {"compress_ms": tc, "decompress_ms": td, "decompress_gbs": 4 * n / td / 1e6,
+                 "512^3 GRF", 4 * n / tfc / 1e6, "GB/s", args,
+                 {"fused_compress_ms": tfc, "fused_decompress_ms": tfd, "fused_decompress_gbs": 4 * n / tfd / 1e6,
+                  "fused_bytes_equal_staged": same, "fused_values_equal_staged": fused_equal,
+                  "pfpl_chunk_gbs": ck_gbs, "pfpl_chunk_frac_of_measured_hbm": (ck_gbs / peak) if (ck_gbs and peak) else None,
+                  "pfpl_decode_gbs": dk_gbs, "pfpl_decode_frac_of_measured_hbm": (dk_gbs / peak) if (dk_gbs and peak) else None,
+                  "staged_compress_ms": tc, "staged_decompress_ms": td, "staged_compress_gbs": 4 * n / tc / 1e6,
+                  "staged_decompress_gbs": 4 * n / td / 1e6,
                   "pipeline_compress_gbs": 4 * n / tpc / 1e6, "pipeline_decompress_gbs": 4 * n / tpd / 1e6,
                   "pipeline_compressed_bytes": cp.numel(), "ratio": 4 * n / comp_bytes,
                   "outliers": int(q["count"].item()), "rel_bound_held": rel_ok, "kernel_ms": per_kernel,
                   "quantizer_fwd_gbs": q_gbs, "quantizer_fwd_frac_of_measured_hbm": (q_gbs / peak) if (q_gbs and peak) else None,
-                  "note": "kernel chain on device-resident data (value); pipeline_* through fz::Pipeline with its host syncs"})
+                  "note": "value: the one-pass chain on device-resident data; staged_*: the four stage kernels back to "
+                          "back; pipeline_* through fz::Pipeline (staged, host syncs included)"})
 
 
 WORKLOADS = {"c1": run_c1, "cli": run_cli, "c3": run_c3, "batch": run_batch, "selector": run_selector,

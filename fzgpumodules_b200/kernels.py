@@ -328,6 +328,43 @@ def quantizer_inverse(codes: torch.Tensor, eb: float, mode: int, abs_eb: float, 
     return out
 
 
+def pfpl_compress(x: torch.Tensor, eb: float = 1e-3, mode: int = REL, radius: int = 32768, zigzag: bool = True,
+                  outlier_capacity: float = 0.1, threshold: float = float("inf"), value_base: float = 0.0,
+                  ws: Workspace | None = None, out: dict | None = None) -> dict:
+    """The pfpl preset's Quantizer(u32) -> Difference(16 KiB) -> Bitshuffle(ew 2)
+    -> RZE chain in one pass.  Returns the RZE stream (max size), its device
+    size, the outlier lists, the capped count, cap and eb_state."""
+    ws = ws or _default_ws
+    src = _flat(x)
+    n, dev = src.numel(), src.device
+    cap = max_outliers(n, outlier_capacity)
+    if out is None:
+        out = dict(rze=torch.empty(int(lib().fzb_rze_max_bytes(4 * n)), dtype=torch.uint8, device=dev),
+                   rze_size=torch.zeros(1, dtype=torch.int64, device=dev),
+                   vals=torch.empty(max(cap, 1), dtype=torch.float32, device=dev),
+                   idx=torch.empty(max(cap, 1), dtype=torch.int32, device=dev),
+                   count=torch.zeros(1, dtype=torch.int32, device=dev),
+                   eb_state=torch.zeros(4, dtype=torch.float32, device=dev), cap=cap)
+    wp, wn = ws.get_bytes(lib().fzb_pfpl_workspace_bytes(n, cap), dev)
+    check(lib().fzb_pfpl_compress(_ptr(src), n, eb, mode, value_base, radius, int(zigzag), threshold,
+                                  _ptr(out["vals"]), _ptr(out["idx"]), cap, _ptr(out["count"]), _ptr(out["rze"]),
+                                  _ptr(out["rze_size"]), _ptr(out["eb_state"]), wp, wn, _stream(dev)),
+          "fzb_pfpl_compress")
+    return out
+
+
+def pfpl_decompress(rze: torch.Tensor, rze_bytes: int, vals, idx, count, cap: int, n: int, eb: float = 1e-3,
+                    mode: int = REL, abs_eb: float = 0.0, zigzag: bool = True, ws: Workspace | None = None,
+                    out: torch.Tensor | None = None) -> torch.Tensor:
+    ws = ws or _default_ws
+    dev = rze.device
+    y = torch.empty(n, dtype=torch.float32, device=dev) if out is None else out
+    wp, wn = ws.get_bytes(lib().fzb_pfpl_decompress_workspace_bytes(n), dev)
+    check(lib().fzb_pfpl_decompress(_ptr(rze), rze_bytes, _ptr(vals), _ptr(idx), _ptr(count), cap, n, eb, mode,
+                                    abs_eb, int(zigzag), _ptr(y), wp, wn, _stream(dev)), "fzb_pfpl_decompress")
+    return y
+
+
 def crc32(data: torch.Tensor, ws: Workspace | None = None) -> torch.Tensor:
     """CRC-32 of a device tensor's bytes (the FZM data checksum,
     compressor_io.cpp:25-52).  Returns a 1-element int64 device tensor."""

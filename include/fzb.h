@@ -283,6 +283,28 @@ int fzb_quantizer_inverse(const void* d_codes, uint64_t n, int code_bytes, float
                           uint32_t radius, int zigzag, int inplace, const float* d_ovals, const uint32_t* d_oidx,
                           const uint32_t* d_count, uint64_t cap, float* d_out, void* stream);
 
+/* The pfpl preset's chain in one pass (examples/presets/pfpl.toml):
+ * QuantizerStage<float, uint32_t> -> DifferenceStage<int32_t, uint32_t>
+ * (16 KiB chunks) -> Bitshuffle(16384, ew 2) -> RZE(16384, 4), the chain of
+ * quantizer.cu:388-649, diff.cu:26-220, bitshuffle_stage.cu:355-475 and
+ * rze_stage.cu:774-843.  The RZE stream and the outliers equal those of
+ * the four stages run one after another (outliers in index order unless
+ * more than cap occur; then which ones are kept depends on execution
+ * order); *d_count receives min(outliers, cap).  n < 2^30. */
+size_t fzb_pfpl_workspace_bytes(uint64_t n, uint64_t cap);
+int fzb_pfpl_compress(const float* d_in, uint64_t n, float eb, int eb_mode, float value_base, uint32_t radius,
+                      int zigzag, float threshold, float* d_ovals, uint32_t* d_oidx, uint64_t cap,
+                      uint32_t* d_count, void* d_rze, uint64_t* d_rze_size, float* d_eb_state, void* d_work,
+                      size_t work_bytes, void* stream);
+/* Its inverse: RZE decode, Bitshuffle inverse, the chunks' prefix sums and
+ * dequantisation in one kernel, then the outlier scatter.  abs_eb as the
+ * Quantizer header stores it (ignored for REL).  Malformed streams are
+ * reported by fzb_workspace_status(d_work). */
+size_t fzb_pfpl_decompress_workspace_bytes(uint64_t n);
+int fzb_pfpl_decompress(const void* d_rze, uint64_t rze_bytes, const float* d_ovals, const uint32_t* d_oidx,
+                        const uint32_t* d_count, uint64_t cap, uint64_t n, float eb, int eb_mode, float abs_eb,
+                        int zigzag, float* d_out, void* d_work, size_t work_bytes, void* stream);
+
 /* Pipeline output concatenation (the reference's Pipeline::concatOutputs,
  * src/pipeline/compressor.cpp:760-875; layout pipeline_utils.h:35-46):
  * [u32 n][u64 size_i x n] padded to 16 bytes, then segment i padded to 16

@@ -1,0 +1,75 @@
+"""The one-pass pfpl chain (fzb_pfpl_compress / fzb_pfpl_decompress) against
+the same four stages run one after another through the C ABI -- Quantizer
+(u32 codes) -> Difference (int32 -> uint32, 16 KiB chunks) -> Bitshuffle
+(16384, ew 2) -> RZE -- whose parity with the reference's kernels and
+pipeline is established in test_gpu_transforms.py and
+test_gpu_pipeline_codes.py: identical RZE bytes, outlier lists and counts,
+and bit-identical decompressed values, on whole and partial chunks, in every
+error-bound mode, and at full size."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+ABS, REL, NOA = 0, 1, 2
+
+
+def K():
+    from fzgpumodules_b200 import kernels
+    return kernels
+
+
+def _field(n, seed, dev):
+    g = torch.Generator(device=dev).manual_seed(seed)
+    x = torch.cumsum(torch.randn(n, device=dev, generator=g), 0) * 0.05 + 3.0
+    idx = torch.randint(0, n, (max(n // 500, 1),), device=dev, generator=g)
+    x[idx] = torch.randn(idx.numel(), device=dev, generator=g) * 1e5
+    x[idx[: max(idx.numel() // 4, 1)]] = 0.0
+    return x.float()
+
+
+def _staged(x, eb, mode, radius, zz, capf, thr):
+    q = K().quantizer_forward(x, eb, mode, radius, 4, zz, capf, thr)
+    d = K().diff(q["codes"], 16384, True)
+    rze, size = K().rze_encode(K().bitshuffle(d, 16384, 2))
+    return q, rze, size
+
+
+@pytest.mark.parametrize("n", [1, 4095, 4096, 4097, 100_003, 4096 * 37, 700_001])
+@pytest.mark.parametrize("mode,radius,zz,thr", [(REL, 32768, True, float("inf")), (ABS, 32768, True, float("inf")),
+                                                (NOA, 512, False, float("inf")), (ABS, 1 << 20, False, 50.0)])
+def test_pfpl_fused_equals_stages(cuda, n, mode, radius, zz, thr):
+    x = _field(n, n % 997 + mode, cuda)
+    eb, capf = 1e-3, 0.1
+    q, rze, size = _staged(x, eb, mode, radius, zz, capf, thr)
+    f = K().pfpl_compress(x, eb, mode, radius, zz, capf, thr)
+    fsize = int(f["rze_size"].item())
+    assert fsize == int(size.item())
+    assert torch.equal(f["rze"][:fsize], rze[:fsize])
+    cnt = int(f["count"].item())
+    assert cnt == int(q["count"].item())
+    assert torch.equal(f["idx"][:cnt], q["idx"][:cnt]) and torch.equal(f["vals"][:cnt], q["vals"][:cnt])
+    assert torch.equal(f["eb_state"][:3], q["eb_state"][:3])
+    abs_eb = 0.0 if mode == REL else float(q["eb_state"][1].item())
+    y = K().pfpl_decompress(f["rze"], fsize, f["vals"], f["idx"], f["count"], f["cap"], n, eb, mode, abs_eb, zz)
+    b = K().bitshuffle(K().rze_decode(rze[:fsize], 4 * n), 16384, 2, inverse=True)
+    c = K().diff(b.view(torch.int32), 16384, True, inverse=True)
+    want = K().quantizer_inverse(c, eb, mode, abs_eb, radius, zz, vals=q["vals"], idx=q["idx"], count=q["count"],
+                                 cap=q["cap"])
+    assert torch.equal(y.view(torch.int32), want.view(torch.int32))
+
+
+def test_pfpl_fused_full_size(cuda):
+    n = 64 << 20  # 256 MiB of values, above L2
+    x = _field(n, 7, cuda)
+    q, rze, size = _staged(x, 1e-3, REL, 32768, True, 0.1, float("inf"))
+    f = K().pfpl_compress(x, 1e-3, REL, 32768, True, 0.1)
+    fsize = int(f["rze_size"].item())
+    assert fsize == int(size.item()) and torch.equal(f["rze"][:fsize], rze[:fsize])
+    cnt = int(f["count"].item())
+    assert torch.equal(f["idx"][:cnt], q["idx"][:cnt])
+    y = K().pfpl_decompress(f["rze"], fsize, f["vals"], f["idx"], f["count"], f["cap"], n)
+    xd, yd = x.double(), y.double()
+    assert bool(((yd - xd).abs() <= xd.abs() * 1e-3 * 1.01).all())
+    assert K()._default_ws.status() == 0
