@@ -364,7 +364,7 @@ def run_pfpl(args, dev):
                   "outliers": int(q["count"].item()), "rel_bound_held": rel_ok, "kernel_ms": per_kernel,
                   "quantizer_fwd_gbs": q_gbs, "quantizer_fwd_frac_of_measured_hbm": (q_gbs / peak) if (q_gbs and peak) else None,
                   "note": "value: the one-pass chain on device-resident data; staged_*: the four stage kernels back to "
-                          "back; pipeline_* through fz::Pipeline (staged, host syncs included)"})
+                          "back; pipeline_* through fz::Pipeline (which runs the one-pass chain; host syncs included)"})
 
 
 WORKLOADS = {"c1": run_c1, "cli": run_cli, "c3": run_c3, "batch": run_batch, "selector": run_selector,

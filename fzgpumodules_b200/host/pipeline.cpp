@@ -411,13 +411,22 @@ void Pipeline::finalize() {
 
 void Pipeline::detectFusion() {
     fused_ = false;
+    fused_pfpl_ = false;
     if (!fusion_enabled_) return;
     auto* lq = dynamic_cast<LorenzoQuantStage<float, uint16_t>*>(input_node_->stage);
-    if (!lq) return;
+    auto* qs = dynamic_cast<QuantizerStage<float, uint32_t>*>(input_node_->stage);
+    if (!lq && !(qs && !qs->isInplace())) return;
     const int codes = input_node_->output_index_to_buffer_id.at(0);
     const BufferInfo& cb = dag_->getBufferInfo(codes);
     if (cb.consumer_stage_ids.size() != 1) return;
     DAGNode* bsn = dag_->getNodes()[cb.consumer_stage_ids[0]];
+    if (qs) {  // Quantizer -> Difference(int32 -> uint32, 16 KiB) -> ...
+        auto* df = dynamic_cast<DifferenceStage<int32_t, uint32_t>*>(bsn->stage);
+        if (!df || df->getChunkSize() != 16384 || bsn->input_buffer_ids.size() != 1) return;
+        const BufferInfo& db = dag_->getBufferInfo(bsn->output_buffer_ids[0]);
+        if (db.consumer_stage_ids.size() != 1) return;
+        bsn = dag_->getNodes()[db.consumer_stage_ids[0]];
+    }
     auto* bs = dynamic_cast<BitshuffleStage*>(bsn->stage);
     if (!bs || bs->getBlockSize() != 16384 || bs->getElementWidth() != 2 || bsn->input_buffer_ids.size() != 1) return;
     const BufferInfo& bb = dag_->getBufferInfo(bsn->output_buffer_ids[0]);
@@ -426,6 +435,7 @@ void Pipeline::detectFusion() {
     auto* rz = dynamic_cast<RZEStage*>(rzn->stage);
     if (!rz || rz->getChunkSize() != 16384 || rz->getLevels() != 4 || rzn->input_buffer_ids.size() != 1) return;
     fused_ = true;
+    fused_pfpl_ = qs != nullptr;
 }
 
 void Pipeline::propagateBufferSizes(size_t source_bytes) {
@@ -492,10 +502,15 @@ void Pipeline::runForward(cudaStream_t stream) {
     for (auto* n : dag_->getNodes())
         for (int id : n->input_buffer_ids) remaining[id]++;
     std::vector<bool> skip(dag_->getNodes().size(), false);
-    DAGNode *bsn = nullptr, *rzn = nullptr;
+    DAGNode *dfn = nullptr, *bsn = nullptr, *rzn = nullptr;
     if (fused_) {
         const BufferInfo& cb = dag_->getBufferInfo(input_node_->output_index_to_buffer_id.at(0));
         bsn = dag_->getNodes()[cb.consumer_stage_ids[0]];
+        if (fused_pfpl_) {
+            dfn = bsn;
+            bsn = dag_->getNodes()[dag_->getBufferInfo(dfn->output_buffer_ids[0]).consumer_stage_ids[0]];
+            skip[dfn->id] = true;
+        }
         rzn = dag_->getNodes()[dag_->getBufferInfo(bsn->output_buffer_ids[0]).consumer_stage_ids[0]];
         skip[bsn->id] = skip[rzn->id] = true;
     }
@@ -515,18 +530,30 @@ void Pipeline::runForward(cudaStream_t stream) {
                 cudaEventRecord(n->start_event, stream);
             }
             if (fused_ && n == input_node_) {
-                auto* lq = static_cast<LorenzoQuantStage<float, uint16_t>*>(n->stage);
                 for (int i = 1; i < 4; i++) dag_->allocate(n->output_buffer_ids[i], stream);
                 const int rz_out = rzn->output_buffer_ids[0];
                 dag_->allocate(rz_out, stream);
-                lq->fusedForward(stream, pool_.get(), in[0], sizes[0], dag_->getBuffer(n->output_buffer_ids[1]),
-                                 dag_->getBuffer(n->output_buffer_ids[2]), dag_->getBuffer(n->output_buffer_ids[3]),
-                                 dag_->getBuffer(rz_out), d_fused_size_);
-                const size_t code_bytes = sizes[0] / sizeof(float) * sizeof(uint16_t);
+                size_t code_bytes;
+                if (fused_pfpl_) {
+                    auto* qs = static_cast<QuantizerStage<float, uint32_t>*>(n->stage);
+                    qs->fusedForward(stream, pool_.get(), in[0], sizes[0], dag_->getBuffer(n->output_buffer_ids[1]),
+                                     dag_->getBuffer(n->output_buffer_ids[2]),
+                                     dag_->getBuffer(n->output_buffer_ids[3]), dag_->getBuffer(rz_out),
+                                     d_fused_size_);
+                    code_bytes = sizes[0];  // one uint32 code per float
+                    static_cast<DifferenceStage<int32_t, uint32_t>*>(dfn->stage)->markFused(code_bytes);
+                } else {
+                    auto* lq = static_cast<LorenzoQuantStage<float, uint16_t>*>(n->stage);
+                    lq->fusedForward(stream, pool_.get(), in[0], sizes[0], dag_->getBuffer(n->output_buffer_ids[1]),
+                                     dag_->getBuffer(n->output_buffer_ids[2]),
+                                     dag_->getBuffer(n->output_buffer_ids[3]), dag_->getBuffer(rz_out),
+                                     d_fused_size_);
+                    code_bytes = sizes[0] / sizeof(float) * sizeof(uint16_t);
+                }
                 static_cast<BitshuffleStage*>(bsn->stage)->markFused(code_bytes);
                 static_cast<RZEStage*>(rzn->stage)->markFused(code_bytes, d_fused_size_, stream);
                 for (int i = 1; i < 4; i++) {
-                    const size_t s = lq->getExecuteTimeOutputSize(i);
+                    const size_t s = n->stage->getExecuteTimeOutputSize(i);
                     if (s) dag_->buffer(n->output_buffer_ids[i]).size = s;
                 }
                 if (profiling_enabled_) cudaEventRecord(n->end_event, stream);

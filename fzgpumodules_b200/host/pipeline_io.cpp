@@ -37,12 +37,90 @@ std::string hex8(uint32_t v) {
 // The fused inverse applies when the source stage is LorenzoQuant whose codes
 // go through Bitshuffle(16 KiB, ew 2) into RZE(16 KiB, 4 levels) and nothing
 // else reads the intermediates.
+// The pfpl chain, Quantizer<float, uint32_t> -> Difference<int32_t,
+// uint32_t>(16 KiB) -> Bitshuffle(16 KiB, ew 2) -> RZE(16 KiB, 4 levels), is
+// inverted in one pass the same way.
+bool fused_inverse_pfpl(const std::vector<FwdDesc>& fwd, const Avail& avail, const FwdDesc* q,
+                        MemoryPool* pool, void* d_result, size_t capacity, size_t* result_size,
+                        cudaStream_t stream) {
+    auto* qs = dynamic_cast<QuantizerStage<float, uint32_t>*>(q->stage);
+    if (!qs || q->out_ids.size() != 4) return false;
+    auto only = [&](int buf) -> const FwdDesc* {
+        const FwdDesc* r = nullptr;
+        int k = 0;
+        for (const auto& d : fwd)
+            for (int i : d.in_ids)
+                if (i == buf) r = &d, k++;
+        return (k == 1 && r->out_ids.size() == 1 && r->in_ids.size() == 1) ? r : nullptr;
+    };
+    const FwdDesc* df = only(q->out_ids[0]);
+    if (!df) return false;
+    auto* dfs = dynamic_cast<DifferenceStage<int32_t, uint32_t>*>(df->stage);
+    if (!dfs || dfs->getChunkSize() != 16384) return false;
+    const FwdDesc* bs = only(df->out_ids[0]);
+    if (!bs) return false;
+    auto* bss = dynamic_cast<BitshuffleStage*>(bs->stage);
+    if (!bss || bss->getBlockSize() != 16384 || bss->getElementWidth() != 2) return false;
+    const FwdDesc* rz = only(bs->out_ids[0]);
+    if (!rz) return false;
+    auto* rzs = dynamic_cast<RZEStage*>(rz->stage);
+    if (!rzs || rzs->getChunkSize() != 16384 || rzs->getLevels() != 4) return false;
+    for (int i = 1; i < 4; i++)
+        if (!avail.count(q->out_ids[i])) return false;
+    if (!avail.count(rz->out_ids[0])) return false;
+    const auto& rze = avail.at(rz->out_ids[0]);
+    const auto& val = avail.at(q->out_ids[1]);
+    const auto& idx = avail.at(q->out_ids[2]);
+    const auto& cnt = avail.at(q->out_ids[3]);
+    const size_t n = rzs->getCachedOrigBytes() / sizeof(uint32_t);
+    *result_size = n * sizeof(float);
+    if (n == 0) return true;
+    if (*result_size > capacity) throw std::runtime_error("decompress: output buffer too small");
+    // the outlier lists and the stream are read with word loads: realign
+    std::vector<void*> temps;
+    auto aligned = [&](const std::pair<void*, size_t>& b) -> const void* {
+        if (!(reinterpret_cast<uintptr_t>(b.first) & 15) || !b.second) return b.first;
+        void* t = pool->allocate(b.second, stream, "inverse_realign", false);
+        if (!t) throw std::runtime_error("decompress: allocation failed");
+        temps.push_back(t);
+        cuda_check(cudaMemcpyAsync(t, b.first, b.second, cudaMemcpyDeviceToDevice, stream), "decompress realign");
+        return t;
+    };
+    const size_t need = fzb_pfpl_decompress_workspace_bytes(n);
+    void* w = pool->allocate(need, stream, "inverse_workspace", false);
+    if (!w) throw std::runtime_error("decompress: workspace allocation failed");
+    int rc = FZB_OK;
+    try {
+        const void* r = aligned(rze);
+        const void* v = aligned(val);
+        const void* ix = aligned(idx);
+        const void* ct = aligned(cnt);
+        rc = fzb_pfpl_decompress(r, rze.second, static_cast<const float*>(v), static_cast<const uint32_t*>(ix),
+                                 static_cast<const uint32_t*>(ct), val.second / sizeof(float), n,
+                                 qs->getErrorBound(), (int)qs->getErrorBoundMode(), qs->computedAbsErrorBound(),
+                                 qs->getZigzagCodes() ? 1 : 0, static_cast<float*>(d_result), w, need, stream);
+        if (rc == FZB_OK) rc = fzb_workspace_status(w, stream);
+    } catch (...) {
+        cudaStreamSynchronize(stream);
+        for (void* t : temps) pool->free(t, stream);
+        pool->free(w, stream);
+        throw;
+    }
+    cudaStreamSynchronize(stream);
+    for (void* t : temps) pool->free(t, stream);
+    pool->free(w, stream);
+    if (rc) throw std::runtime_error(std::string("Quantizer<-Difference<-Bitshuffle<-RZE decompress: ") +
+                                     fzb_status_string(rc));
+    return true;
+}
+
 bool fused_inverse(const std::vector<FwdDesc>& fwd, const Avail& avail, int source_buf, MemoryPool* pool,
                    void* d_result, size_t capacity, size_t* result_size, cudaStream_t stream) {
     const FwdDesc* lq = nullptr;
     for (const auto& d : fwd)
         if (d.in_ids.size() == 1 && d.in_ids[0] == source_buf) lq = &d;
     if (!lq || lq->out_ids.size() != 4) return false;
+    if (fused_inverse_pfpl(fwd, avail, lq, pool, d_result, capacity, result_size, stream)) return true;
     auto* lqs = dynamic_cast<LorenzoQuantStage<float, uint16_t>*>(lq->stage);
     if (!lqs) return false;
     auto consumers = [&](int buf) {

@@ -149,6 +149,37 @@ void QuantizerStage<TInput, TCode>::execute(cudaStream_t stream, MemoryPool* poo
 }
 
 template <typename TInput, typename TCode>
+void QuantizerStage<TInput, TCode>::fusedForward(cudaStream_t stream, MemoryPool* pool, const void* d_in,
+                                                 size_t in_bytes, void* d_vals, void* d_idx, void* d_count,
+                                                 void* d_rze, uint64_t* d_rze_size) {
+    if (sizeof(TCode) != 4 || isInplaceMode())
+        throw std::runtime_error("QuantizerStage: the one-pass chain needs uint32 codes and outlier lists");
+    const size_t n = in_bytes / sizeof(TInput);
+    num_elements_ = n;
+    actual_outlier_count_ = 0;
+    pending_ = ran_ = false;
+    computed_abs_eb_ = config_.eb_mode == ErrorBoundMode::ABS ? config_.error_bound : 0.0f;
+    computed_value_base_ = 0.0f;
+    at_execute_.assign(4, 0);
+    actual_ = at_execute_;
+    if (n == 0) return;
+    const size_t cap = getMaxOutlierCount(n);
+    const size_t need = align256(fzb_pfpl_workspace_bytes(n, cap));
+    uint8_t* base = static_cast<uint8_t*>(ws_.ensure(need + kTail, pool, stream));
+    d_eb_state_ = reinterpret_cast<float*>(base + need);
+    check(fzb_pfpl_compress(static_cast<const float*>(d_in), n, config_.error_bound, (int)config_.eb_mode,
+                            config_.precomputed_value_base, (uint32_t)config_.quant_radius,
+                            config_.zigzag_codes ? 1 : 0, config_.outlier_threshold, static_cast<float*>(d_vals),
+                            static_cast<uint32_t*>(d_idx), cap, static_cast<uint32_t*>(d_count), d_rze, d_rze_size,
+                            d_eb_state_, base, need, stream),
+          "Quantizer->Difference->Bitshuffle->RZE");
+    d_count_ = d_count;
+    pending_ = ran_ = true;
+    at_execute_ = {n * sizeof(TCode), cap * sizeof(TInput), cap * sizeof(uint32_t), sizeof(uint32_t)};
+    actual_ = at_execute_;
+}
+
+template <typename TInput, typename TCode>
 void QuantizerStage<TInput, TCode>::postStreamSync(cudaStream_t stream) {
     if (is_inverse_ || !pending_) return;
     pending_ = false;

@@ -9,10 +9,12 @@
 // index); the reference orders them by hash-map iteration, so its segment
 // order can differ while every segment's bytes agree.
 //
-// A LorenzoQuant -> Bitshuffle(16 KiB, ew 2) -> RZE(16 KiB, 4 levels) chain
-// whose intermediate buffers feed nothing else runs as one fused kernel pass
-// (the intermediates are never materialised); setFusion(false) runs the
-// stages one by one.  Both produce identical bytes.
+// A LorenzoQuant -> Bitshuffle(16 KiB, ew 2) -> RZE(16 KiB, 4 levels) chain,
+// or the pfpl chain Quantizer(uint32 codes) -> Difference(int32 -> uint32,
+// 16 KiB) -> Bitshuffle(16 KiB, ew 2) -> RZE(16 KiB, 4 levels), whose
+// intermediate buffers feed nothing else runs as one fused kernel pass in
+// each direction (the intermediates are never materialised);
+// setFusion(false) runs the stages one by one.  Both produce identical bytes.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -242,6 +244,7 @@ private:
     bool finalized_ = false, compressed_ = false, warmup_on_finalize_ = false;
     bool pool_managed_decomp_ = true, profiling_enabled_ = false;
     bool fusion_enabled_ = true, fused_ = false;
+    bool fused_pfpl_ = false;  // the fused chain starts at a Quantizer (pfpl) rather than LorenzoQuant
     bool graph_mode_ = false;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;

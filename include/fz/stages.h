@@ -583,6 +583,13 @@ public:
     // ceil(n * outlier_capacity) in single precision (quantizer.h:262-264).
     size_t getMaxOutlierCount(size_t n) const;
     float computedAbsErrorBound() const { return computed_abs_eb_; }
+    bool isInplace() const { return isInplaceMode(); }
+
+    // The one-pass Quantizer -> Difference(16 KiB) -> Bitshuffle(ew 2) -> RZE
+    // path (uint32 codes) runs this stage's work itself; it records what
+    // execute() would.
+    void fusedForward(cudaStream_t stream, MemoryPool* pool, const void* d_in, size_t in_bytes, void* d_vals,
+                      void* d_idx, void* d_count, void* d_rze, uint64_t* d_rze_size);
 
 private:
     bool isInplaceMode() const { return config_.inplace_outliers && config_.eb_mode != ErrorBoundMode::REL; }
@@ -636,6 +643,7 @@ public:
         return {{"output", actual_}};
     }
     size_t getActualOutputSize(int index) const override { return index == 0 ? actual_ : 0; }
+    void markFused(size_t bytes) { actual_ = bytes; }
     uint16_t getStageTypeId() const override { return (uint16_t)StageType::DIFFERENCE; }
     uint8_t getOutputDataType(size_t) const override;
     uint8_t getInputDataType(size_t) const override;

@@ -73,3 +73,35 @@ def test_pfpl_fused_full_size(cuda):
     xd, yd = x.double(), y.double()
     assert bool(((yd - xd).abs() <= xd.abs() * 1e-3 * 1.01).all())
     assert K()._default_ws.status() == 0
+
+
+@pytest.mark.parametrize("dims", [(128, 128, 64), (3600, 1800, 1)])
+def test_pfpl_pipeline_fused_equals_staged(cuda, dims, tmp_path):
+    from fzgpumodules_b200 import pipeline as p
+    n = dims[0] * dims[1] * dims[2]
+    x = _field(n, 11, cuda)
+    outs = []
+    for fusion in (True, False):
+        pl = p.Pipeline(n * 4, p.PREALLOCATE)
+        pl.setDims(*dims)
+        q = pl.addStage(p.QuantizerStage(1e-3, p.REL, 32768, 0.1, code_bytes=4, zigzag_codes=True))
+        d = pl.addStage(p.DifferenceStage(p.INT32, p.UINT32, 16384))
+        bs = pl.addStage(p.BitshuffleStage(16384, 2))
+        rz = pl.addStage(p.RZEStage(16384, 4))
+        pl.connect(d, q, "codes")
+        pl.connect(bs, d)
+        pl.connect(rz, bs)
+        pl.setFusion(fusion)
+        pl.finalize()
+        assert pl.isFused() == fusion
+        comp = pl.compress(x).clone()
+        y = pl.decompress().clone()
+        path = str(tmp_path / f"f{int(fusion)}.fzm")
+        pl.writeToFile(path)
+        yf = p.Pipeline.decompressFromFile(path)[:n]
+        outs.append((comp, y, yf))
+        pl.close()
+    (ca, ya, fa), (cb, yb, fb) = outs
+    assert torch.equal(ca, cb)
+    assert torch.equal(ya.view(torch.int32), yb.view(torch.int32))
+    assert torch.equal(fa.view(torch.int32), ya.view(torch.int32)) and torch.equal(fb.view(torch.int32), ya.view(torch.int32))
