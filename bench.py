@@ -435,7 +435,7 @@ def run_reference_pfpl(args):
     if not os.path.exists(path):
         return dict(base, unavailable="the reference pipeline build (oracle/_ref/libfzref_pipe.so) is absent")
     dev = torch.device("cuda", 0)
-    x = benchmarks.pfpl_field(dev)
+    x = benchmarks.pfpl_field(dev, tuple(args.dims))
     n = x.numel()
     L = C.CDLL(path)
     L.ref_pipe_last_error.restype = C.c_char_p

@@ -260,9 +260,10 @@ def run_selector(args, dev):
 PFPL_DIMS = (512, 512, 512)
 
 
-def pfpl_field(dev):
-    """The pfpl workload's input: a 512^3 Gaussian random field with 0.1 % spikes."""
-    return F.grf(PFPL_DIMS[::-1], seed=1006, spike_frac=1e-3, device=dev).reshape(-1)
+def pfpl_field(dev, dims=PFPL_DIMS):
+    """The pfpl workload's input: a Gaussian random field (512^3 by default)
+    with 0.1 % spikes; dims are (x, y, z)."""
+    return F.grf(tuple(dims)[::-1], seed=1006, spike_frac=1e-3, device=dev).reshape(-1)
 
 
 def run_pfpl(args, dev):
@@ -272,7 +273,8 @@ def run_pfpl(args, dev):
     kernels run back to back on device-resident data and through fz::Pipeline."""
     from .pipeline import (BitshuffleStage, DifferenceStage, Pipeline, QuantizerStage, RZEStage, INT32, PREALLOCATE,
                            REL, UINT32)
-    x = pfpl_field(dev)
+    dims = tuple(getattr(args, "dims", PFPL_DIMS))
+    x = pfpl_field(dev, dims)
     n = x.numel()
     wq, wd, wr = K.Workspace(), K.Workspace(), K.Workspace()
     q = K.quantizer_forward(x, 1e-3, K.REL, 32768, 4, True, 0.1, ws=wq)
@@ -352,7 +354,7 @@ def run_pfpl(args, dev):
     ck_gbs = (4 * n + comp_bytes) / ck / 1e6 if ck else None
     dk_gbs = (4 * n + comp_bytes) / dk / 1e6 if dk else None
     return _line("pfpl: Quantizer(REL 1e-3, u32, zigzag)->Difference(i32->u32, 16 KiB)->Bitshuffle(16384, ew2)->RZE, "
-                 "512^3 GRF", 4 * n / tfc / 1e6, "GB/s", args,
+                 + "x".join(map(str, dims)) + " GRF", 4 * n / tfc / 1e6, "GB/s", args,
                  {"fused_compress_ms": tfc, "fused_decompress_ms": tfd, "fused_decompress_gbs": 4 * n / tfd / 1e6,
                   "fused_bytes_equal_staged": same, "fused_values_equal_staged": fused_equal,
                   "pfpl_chunk_gbs": ck_gbs, "pfpl_chunk_frac_of_measured_hbm": (ck_gbs / peak) if (ck_gbs and peak) else None,
