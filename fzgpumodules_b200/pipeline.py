@@ -259,6 +259,42 @@ class Pipeline:
         self._last_in = 0
 
     # builder ---------------------------------------------------------------
+    def loadConfig(self, path: str):
+        """Pipeline::loadConfig (src/pipeline/config.cpp:534-640): the
+        [pipeline] settings and [[stage]] tables of a TOML file, connected by
+        their ``inputs`` and finalized."""
+        from . import config
+        if self._h is not None:
+            raise PipelineError("loadConfig: pipeline is already finalized")
+        with open(path) as f:
+            cfg = config.parse_config(f.read())
+        pl = cfg["pipeline"]
+        if "input_size" in pl:
+            self._hint = int(pl["input_size"])
+        if "dims" in pl:
+            d = [int(v) for v in pl["dims"]][:3] + [0, 1, 1][len(pl["dims"][:3]):]
+            self.setDims(*d)
+        if "memory_strategy" in pl:
+            self._strategy = config.STRATEGIES.get(pl["memory_strategy"], MINIMAL)
+        if "pool_multiplier" in pl:
+            self._mult = float(pl["pool_multiplier"])
+        for _, st in cfg["stages"]:
+            self.addStage(st)
+        for dep, prod, port in cfg["connections"]:
+            self.connect(dep, prod, port)
+        self.finalize()
+
+    def saveConfig(self, path: str):
+        """Pipeline::saveConfig (config.cpp:645-...): the finalized pipeline as TOML."""
+        from . import config
+        if self._h is None:
+            raise PipelineError("saveConfig: pipeline must be finalized first")
+        params = {"input_size": self._hint,
+                  "memory_strategy": "PREALLOCATE" if self._strategy == PREALLOCATE else "MINIMAL",
+                  "pool_multiplier": self._mult, "num_streams": 1, "dims": list(self._dims)}
+        with open(path, "w") as f:
+            f.write(config.dump_config(params, self._stages, self._conns))
+
     def setDims(self, x: int, y: int = 1, z: int = 1):
         self._dims = (int(x), int(y), int(z))
 

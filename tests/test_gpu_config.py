@@ -1,0 +1,86 @@
+"""TOML configurations and the command-line front end on the GPU: a
+pipeline loaded with Pipeline.loadConfig writes the same bytes as the same
+pipeline built by hand, saveConfig -> loadConfig keeps them, and the CLI's
+compress (-z) / decompress (-x) / benchmark (-b) modes round-trip a field
+within its error bound."""
+import numpy as np
+import pytest
+import torch
+
+from test_config_cpu import PFPL_LIKE
+
+pytestmark = pytest.mark.gpu
+
+
+def P():
+    from fzgpumodules_b200 import pipeline
+    return pipeline
+
+
+def _field(n, dev):
+    g = torch.Generator(device=dev).manual_seed(21)
+    return (torch.cumsum(torch.randn(n, device=dev, generator=g), 0) * 0.01 + 5.0).float()
+
+
+def test_load_and_save_config(cuda, tmp_path):
+    p = P()
+    cfg = tmp_path / "pfpl.toml"
+    cfg.write_text(PFPL_LIKE)
+    n = 512 * 512 * 64
+    x = _field(n, cuda)
+    a = p.Pipeline(n * 4)
+    a.loadConfig(str(cfg))
+    ca = a.compress(x).clone()
+    assert a.isFused()
+    b = p.Pipeline(n * 4, p.PREALLOCATE)
+    b.setDims(512, 512, 64)
+    q = b.addStage(p.QuantizerStage(1e-3, p.REL, 32768, 0.1, code_bytes=4, zigzag_codes=True))
+    d = b.addStage(p.DifferenceStage(p.INT32, p.UINT32, 16384))
+    bs = b.addStage(p.BitshuffleStage(16384, 2))
+    rz = b.addStage(p.RZEStage(16384, 4))
+    b.connect(d, q, "codes")
+    b.connect(bs, d)
+    b.connect(rz, bs)
+    b.finalize()
+    assert torch.equal(ca, b.compress(x))
+    saved = tmp_path / "saved.toml"
+    a.saveConfig(str(saved))
+    c = p.Pipeline(n * 4)
+    c.loadConfig(str(saved))
+    assert torch.equal(ca, c.compress(x))
+    for pl in (a, b, c):
+        pl.close()
+
+
+@pytest.mark.parametrize("stages,mode", [("lorenzo->bitshuffle->rze", "rel"), ("quantizer->diff->bitshuffle->rze", "rel"),
+                                         ("lorenzo->rle", "abs"), ("lorenzo->huffman", "abs")])
+def test_cli_round_trip(cuda, tmp_path, stages, mode, capsys):
+    from fzgpumodules_b200 import cli
+    x = _field(700 * 1000, cuda).cpu().numpy()
+    raw = tmp_path / "f.f32"
+    x.tofile(raw)
+    radius = ["-r", "512"] if "huffman" in stages else []  # codes must stay below the 1024-entry codebook
+    assert cli.main(["-z", "-i", str(raw), "-l", "1000x700", "--stages", stages, "-m", mode, "-e", "1e-3",
+                     "--report"] + radius) == 0
+    fzm = str(raw) + ".fzm"
+    out = tmp_path / "f.out"
+    assert cli.main(["-x", "-i", fzm, "-o", str(out), "--compare", str(raw), "--report"]) == 0
+    y = np.fromfile(out, dtype=np.float32)
+    assert y.size == x.size
+    err = np.abs(y.astype(np.float64) - x.astype(np.float64))
+    bound = np.abs(x.astype(np.float64)) * 1e-3 * 1.01 if (mode == "rel" and stages.startswith("quantizer")) else \
+        (1e-3 * 1.01 * (np.abs(x).max() if mode == "rel" else 1.0))
+    assert np.all(err <= bound)
+    text = capsys.readouterr().out
+    assert "ratio:" in text and "PSNR" in text
+
+
+def test_cli_benchmark_with_config(cuda, tmp_path, capsys):
+    from fzgpumodules_b200 import cli
+    cfg = tmp_path / "pfpl.toml"
+    cfg.write_text(PFPL_LIKE)
+    x = _field(512 * 512 * 64, cuda).cpu().numpy()
+    raw = tmp_path / "g.f32"
+    x.tofile(raw)
+    assert cli.main(["-b", "-c", str(cfg), "-i", str(raw), "-l", "512x512x64", "--runs", "2", "--report"]) == 0
+    assert "throughput:" in capsys.readouterr().out
