@@ -105,3 +105,42 @@ def test_pfpl_pipeline_fused_equals_staged(cuda, dims, tmp_path):
     assert torch.equal(ca, cb)
     assert torch.equal(ya.view(torch.int32), yb.view(torch.int32))
     assert torch.equal(fa.view(torch.int32), ya.view(torch.int32)) and torch.equal(fb.view(torch.int32), ya.view(torch.int32))
+
+
+def _pfpl_pipeline(p, n, dims, graph=False, fusion=True):
+    pl = p.Pipeline(n * 4, p.PREALLOCATE)
+    pl.setDims(*dims)
+    q = pl.addStage(p.QuantizerStage(1e-3, p.REL, 32768, 0.1, code_bytes=4, zigzag_codes=True))
+    d = pl.addStage(p.DifferenceStage(p.INT32, p.UINT32, 16384))
+    bs = pl.addStage(p.BitshuffleStage(16384, 2))
+    rz = pl.addStage(p.RZEStage(16384, 4))
+    pl.connect(d, q, "codes")
+    pl.connect(bs, d)
+    pl.connect(rz, bs)
+    pl.enableGraphMode(graph)
+    pl.setFusion(fusion)
+    pl.finalize()
+    return pl
+
+
+def test_pfpl_pipeline_graph_replay(cuda):
+    # one compress captured into a CUDA graph and replayed on new inputs
+    # gives the eager pipeline's bytes, outlier counts included
+    from fzgpumodules_b200 import pipeline as p
+    dims = (256, 256, 32)
+    n = dims[0] * dims[1] * dims[2]
+    x1 = _field(n, 3, cuda)
+    x2 = (x1 * 0.5 + 0.25).contiguous()
+    x3 = _field(n, 4, cuda)
+    pl = _pfpl_pipeline(p, n, dims, graph=True)
+    s = torch.cuda.Stream(device=cuda)
+    pl.captureGraph(s)
+    eager = _pfpl_pipeline(p, n, dims)
+    for x in (x1, x2, x3, x1):
+        with torch.cuda.stream(s):
+            cg = pl.compress(x).clone()
+        s.synchronize()
+        ce = eager.compress(x).clone()
+        assert torch.equal(cg.cpu(), ce.cpu())
+    pl.close()
+    eager.close()
