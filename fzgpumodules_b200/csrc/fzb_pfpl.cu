@@ -99,7 +99,7 @@ __device__ __forceinline__ void store_slot(uint8_t* __restrict__ slots, uint32_t
 }
 
 template <bool REL>
-__global__ void __launch_bounds__(kThreads, 4) pfpl_chunk_kernel(PArgs a) {
+__global__ void __launch_bounds__(kThreads, 5) pfpl_chunk_kernel(PArgs a) {
     extern __shared__ float4 smraw[];
     __shared__ uint32_t s_ws[16];
     __shared__ uint32_t s_last[kThreads / 32];
