@@ -125,6 +125,8 @@ def lib():
         L.fzb_pipeline_add_zigzag.argtypes = [p, i32]
         L.fzb_pipeline_add_negabinary.argtypes = [p, i32]
         L.fzb_pipeline_connect.argtypes = [p, i32, i32, C.c_char_p]
+        L.fzb_pipeline_load_config.argtypes = [p, C.c_char_p]
+        L.fzb_pipeline_save_config.argtypes = [p, C.c_char_p]
         L.fzb_pipeline_set_fusion.argtypes = [p, i32]
         L.fzb_pipeline_enable_graph_mode.argtypes = [p, i32]
         L.fzb_pipeline_enable_profiling.argtypes = [p, i32]

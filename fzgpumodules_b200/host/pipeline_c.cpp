@@ -186,6 +186,22 @@ static int add_sign_coding(void* p, int in_type, bool nb) {
 int fzb_pipeline_add_zigzag(void* p, int in_type) { return add_sign_coding(p, in_type, false); }
 int fzb_pipeline_add_negabinary(void* p, int in_type) { return add_sign_coding(p, in_type, true); }
 
+int fzb_pipeline_load_config(void* p, const char* path) {
+    if (!p || !path) return FZB_E_INVALID;
+    return guarded([&] {
+        H(p)->p->loadConfig(path);
+        return FZB_OK;
+    });
+}
+
+int fzb_pipeline_save_config(void* p, const char* path) {
+    if (!p || !path) return FZB_E_INVALID;
+    return guarded([&] {
+        H(p)->p->saveConfig(path);
+        return FZB_OK;
+    });
+}
+
 int fzb_pipeline_add_bitshuffle(void* p, uint32_t block_size, int element_width) {
     if (!p) return FZB_E_INVALID;
     return guarded([&] {

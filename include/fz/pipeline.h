@@ -142,6 +142,11 @@ public:
         addRawStage(s);
         return s;
     }
+    // TOML configurations (src/pipeline/config.cpp): loadConfig adds, connects
+    // and finalizes the stages a file describes; saveConfig writes a
+    // finalized pipeline in the same format.
+    void loadConfig(const std::string& path);
+    void saveConfig(const std::string& path) const;
     int connect(Stage* dependent, Stage* producer, const std::string& output_name = "output");
     int connect(Stage* dependent, const std::vector<Stage*>& producers);
     void finalize();

@@ -454,6 +454,11 @@ int fzb_pipeline_add_lorenzo(void* pipeline, int data_type);
  * zigzag/zigzag_stage.h, negabinary/negabinary_stage.h), S signed (4..7). */
 int fzb_pipeline_add_zigzag(void* pipeline, int in_type);
 int fzb_pipeline_add_negabinary(void* pipeline, int in_type);
+/* Pipeline::loadConfig / saveConfig (src/pipeline/config.cpp:515-640): a
+ * TOML file's [pipeline] settings and [[stage]] tables, connected by their
+ * `inputs` and finalized; saveConfig writes a finalized pipeline. */
+int fzb_pipeline_load_config(void* pipeline, const char* path);
+int fzb_pipeline_save_config(void* pipeline, const char* path);
 /* connect(dependent, producer, output_name); returns the buffer id. */
 int fzb_pipeline_connect(void* pipeline, int dependent, int producer, const char* output_name);
 /* Fusion of LorenzoQuant -> Bitshuffle -> RZE into one pass (default on). */

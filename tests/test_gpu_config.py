@@ -84,3 +84,47 @@ def test_cli_benchmark_with_config(cuda, tmp_path, capsys):
     x.tofile(raw)
     assert cli.main(["-b", "-c", str(cfg), "-i", str(raw), "-l", "512x512x64", "--runs", "2", "--report"]) == 0
     assert "throughput:" in capsys.readouterr().out
+
+
+def test_cxx_load_and_save_config(cuda, tmp_path):
+    # the C++ Pipeline::loadConfig / saveConfig through the C ABI
+    import ctypes as C
+
+    from fzgpumodules_b200 import config as CF
+    from fzgpumodules_b200._lib import lib
+    from fzgpumodules_b200.pipeline import _view
+    p = P()
+    L = lib()
+    cfg = tmp_path / "pfpl.toml"
+    cfg.write_text(PFPL_LIKE)
+    n = 512 * 512 * 64
+    x = _field(n, cuda)
+    h = L.fzb_pipeline_create(n * 4, 0, 3.0)
+    try:
+        assert L.fzb_pipeline_load_config(h, str(cfg).encode()) == 0, L.fzb_last_error()
+        assert L.fzb_pipeline_is_fused(h) == 1
+        out, sz = C.c_void_p(), C.c_uint64()
+        st = C.c_void_p(torch.cuda.current_stream(cuda).cuda_stream)
+        assert L.fzb_pipeline_compress(h, C.c_void_p(x.data_ptr()), n * 4, C.byref(out), C.byref(sz), st) == 0
+        torch.cuda.synchronize()
+        got = _view(out.value, sz.value, cuda).clone()
+        a = p.Pipeline(n * 4)
+        a.loadConfig(str(cfg))
+        assert torch.equal(got, a.compress(x))
+        a.close()
+        saved = tmp_path / "cxx.toml"
+        assert L.fzb_pipeline_save_config(h, str(saved).encode()) == 0, L.fzb_last_error()
+        f32 = lambda t: {k: (np.float32(v) if isinstance(v, float) else v) for k, v in t.items()}
+        mine, ref = CF.parse_config(saved.read_text()), CF.parse_config(PFPL_LIKE)
+        assert [f32(CF._stage_table(s)) for _, s in mine["stages"]] == [f32(CF._stage_table(s)) for _, s in ref["stages"]]
+        assert len(mine["connections"]) == 3
+    finally:
+        L.fzb_pipeline_destroy(h)
+    bad = tmp_path / "bad.toml"
+    bad.write_text('[[stage]]\nname = "a"\ntype = "Fancy"\n')
+    h = L.fzb_pipeline_create(0, 0, 3.0)
+    try:
+        assert L.fzb_pipeline_load_config(h, str(bad).encode()) == -8
+        assert b"unknown stage type" in L.fzb_last_error()
+    finally:
+        L.fzb_pipeline_destroy(h)
