@@ -274,7 +274,7 @@ __device__ __forceinline__ void block_seg_scan(A v, uint32_t f, A& ev, uint32_t&
 // PHASE 0: one-pass scan (every tile starts a segment) or apply with the
 // tile carries; PHASE 1: tile aggregates only.
 template <typename U, bool NB, int PHASE>
-__global__ void __launch_bounds__(kScanThreads) segscan_kernel(SegScan a) {
+__global__ void __launch_bounds__(kScanThreads, 4) segscan_kernel(SegScan a) {
     using A = Acc<U>;
     __shared__ A sv[kScanThreads / 32];
     __shared__ uint32_t sf[kScanThreads / 32];
