@@ -441,9 +441,15 @@ def run_reference_pfpl(args):
     L.ref_pipe_last_error.restype = C.c_char_p
     cm, dm, cb = C.c_float(0), C.c_float(0), C.c_size_t(0)
     rc = L.ref_pipeline_time_pfpl(C.c_void_p(x.data_ptr()), C.c_size_t(n), C.c_float(1e-3), C.c_float(0.1),
-                                  args.steps, args.warmup, C.byref(cm), C.byref(dm), C.byref(cb))
+                                  args.steps, args.warmup, C.byref(cm), C.byref(dm), C.byref(cb), 0)
     if rc != 0:
         return dict(base, unavailable="reference pipeline failed: " + L.ref_pipe_last_error().decode())
+    sm, sdm, scb = C.c_float(0), C.c_float(0), C.c_size_t(0)
+    rc = L.ref_pipeline_time_pfpl(C.c_void_p(x.data_ptr()), C.c_size_t(n), C.c_float(1e-3), C.c_float(0.05),
+                                  args.steps, args.warmup, C.byref(sm), C.byref(sdm), C.byref(scb), 1)
+    speed = ({"speed_compress_gbs": 4 * n / sm.value / 1e6, "speed_decompress_gbs": 4 * n / sdm.value / 1e6,
+              "speed_compressed_bytes": scb.value} if rc == 0 else
+             {"speed_unavailable": L.ref_pipe_last_error().decode()})
     v = 4 * n / cm.value / 1e6
     return dict(base, metric="compress GB/s of the pfpl preset pipeline", value=v, unit="GB/s", n_gpus=1,
                 steps=args.steps, warmup=args.warmup, higher_is_better=True, dtype="f32", data="synthetic",
@@ -452,6 +458,7 @@ def run_reference_pfpl(args):
                 compress_ms=cm.value, decompress_ms=dm.value, decompress_gbs=4 * n / dm.value / 1e6,
                 compressed_bytes=cb.value, e2e={"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0,
                                                 "d2h_bytes_per_step": 0},
+                **speed,
                 note="the reference's GPU pipeline through its public API (Pipeline::compress / decompress, "
                      "host synchronisation included)")
 

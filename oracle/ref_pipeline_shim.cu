@@ -160,28 +160,40 @@ extern "C" int ref_pipeline_codes(int chain, const float* d_in, size_t n, size_t
 }
 
 // Times the reference's pfpl chain (chain 3 above: Quantizer REL -> Difference
-// -> Bitshuffle -> RZE) through its own Pipeline::compress / decompress on
+// -> Bitshuffle -> RZE), or the speed chain, through its own
+// Pipeline::compress / decompress on
 // the default stream: `warmup` untimed calls, then the mean of `steps` calls
 // each bracketed by CUDA events.  Every call includes the reference's own
 // host synchronisation.  A 256 MiB buffer is rewritten between calls to
 // evict L2.
+// `speed` = 1 times the speed preset's chain instead (Quantizer REL ->
+// Bitshuffle(16384, ew 4) -> RZE, examples/presets/speed.toml).
 extern "C" int ref_pipeline_time_pfpl(const float* d_in, size_t n, float eb, float outlier_cap, int steps, int warmup,
-                                      float* comp_ms, float* decomp_ms, size_t* comp_bytes) {
+                                      float* comp_ms, float* decomp_ms, size_t* comp_bytes, int speed) {
     try {
         Pipeline p(n * sizeof(float), MemoryStrategy::PREALLOCATE, 3.0f);
         p.setDims(n, 1, 1);
         QuantizerStage<float, uint32_t>::Config c(eb, ErrorBoundMode::REL, 32768, outlier_cap);
         c.zigzag_codes = true;
+        // stages in topological order: the reference propagates buffer sizes
+        // in addStage order
         auto* q = p.addStage<QuantizerStage<float, uint32_t>>(c);
-        auto* d = p.addStage<DifferenceStage<int32_t, uint32_t>>();
-        d->setChunkSize(16384);
+        DifferenceStage<int32_t, uint32_t>* d = nullptr;
+        if (!speed) {
+            d = p.addStage<DifferenceStage<int32_t, uint32_t>>();
+            d->setChunkSize(16384);
+        }
         auto* bs = p.addStage<BitshuffleStage>();
         bs->setBlockSize(16384);
-        bs->setElementWidth(2);
+        bs->setElementWidth(speed ? 4 : 2);
         auto* rze = p.addStage<RZEStage>();
         rze->setLevels(4);
-        p.connect(d, q, "codes");
-        p.connect(bs, d);
+        if (d) {
+            p.connect(d, q, "codes");
+            p.connect(bs, d);
+        } else {
+            p.connect(bs, q, "codes");
+        }
         p.connect(rze, bs);
         p.finalize();
         void* flush = nullptr;
