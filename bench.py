@@ -242,7 +242,36 @@ def run_reference(args, world, rank):
             "cpu_baseline": {"value": comp, "unit": "GB/s", "cores": res[0]["cores"], "kind": "port",
                              "sample": res[0]["sample"]},
             "e2e": {"value": comp, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["reference_gpu_pipeline"] = _reference_gpu_lq(args)
     print(json.dumps(line), flush=True)
+
+
+def _reference_gpu_lq(args):
+    """For comparison beside the CPU arm: the reference's own GPU pipeline
+    (built from its sources into oracle/_ref) on the full 512^3 workload,
+    each Pipeline::compress / decompress call timed with CUDA events."""
+    import ctypes as C
+    path = os.path.join(ROOT, "oracle", "_ref", "libfzref_pipe.so")
+    try:
+        import torch
+        if not torch.cuda.is_available() or not os.path.exists(path):
+            return {"unavailable": "no GPU or no reference pipeline build"}
+        from fzgpumodules_b200 import fields
+        nx, ny, nz = DEFAULT_DIMS
+        x = fields.grf((nz, ny, nx), seed=SEED, spike_frac=1e-3, device=torch.device("cuda", 0)).reshape(-1)
+        L = C.CDLL(path)
+        L.ref_pipe_last_error.restype = C.c_char_p
+        cm, dm, cb = C.c_float(0), C.c_float(0), C.c_size_t(0)
+        steps = max(1, min(args.steps, 10))
+        if L.ref_pipeline_time_lq(C.c_void_p(x.data_ptr()), C.c_size_t(nx), C.c_size_t(ny), C.c_size_t(nz),
+                                  C.c_float(EB), steps, 3, C.byref(cm), C.byref(dm), C.byref(cb)) != 0:
+            return {"unavailable": L.ref_pipe_last_error().decode()}
+        nbytes = 4 * x.numel()
+        return {"compress_gbs": nbytes / cm.value / 1e6, "decompress_gbs": nbytes / dm.value / 1e6,
+                "compress_ms": cm.value, "decompress_ms": dm.value, "compressed_bytes": cb.value, "steps": steps,
+                "note": "Pipeline::compress / decompress calls, host synchronisation included"}
+    except Exception as e:  # the CPU arm's line stands on its own
+        return {"unavailable": str(e)[:200]}
 
 
 # ---------------------------------------------------------------- GPU side

@@ -239,3 +239,71 @@ extern "C" int ref_pipeline_time_pfpl(const float* d_in, size_t n, float eb, flo
     }
     return 0;
 }
+
+// Times the reference's own pipeline for the LorenzoQuant chain (chain 1
+// above: LorenzoQuant(REL, zigzag, capacity 0.1) -> Bitshuffle(16384, ew 2)
+// -> RZE(16384, 4)) on an x*y*z field, as ref_pipeline_time_pfpl does.
+extern "C" int ref_pipeline_time_lq(const float* d_in, size_t x, size_t y, size_t z, float eb, int steps, int warmup,
+                                    float* comp_ms, float* decomp_ms, size_t* comp_bytes) {
+    try {
+        const size_t n = x * y * z;
+        Pipeline p(n * sizeof(float), MemoryStrategy::PREALLOCATE, 3.0f);
+        p.setDims(x, y, z);
+        LorenzoQuantStage<float, uint16_t>::Config cfg;
+        cfg.error_bound = eb;
+        cfg.quant_radius = 32768;
+        cfg.outlier_capacity = 0.1f;
+        cfg.eb_mode = ErrorBoundMode::REL;
+        cfg.zigzag_codes = true;
+        auto* lq = p.addStage<LorenzoQuantStage<float, uint16_t>>(cfg);
+        auto* bs = p.addStage<BitshuffleStage>();
+        bs->setBlockSize(16384);
+        bs->setElementWidth(2);
+        auto* rze = p.addStage<RZEStage>();
+        rze->setLevels(4);
+        p.connect(bs, lq, "codes");
+        p.connect(rze, bs);
+        p.finalize();
+        void* flush = nullptr;
+        if (cudaMalloc(&flush, 256u << 20) != cudaSuccess) throw std::runtime_error("flush alloc failed");
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        double tc = 0, td = 0;
+        void* out = nullptr;
+        size_t sz = 0;
+        for (int i = 0; i < warmup + steps; i++) {
+            float ms = 0;
+            cudaMemsetAsync(flush, i & 0xff, 256u << 20, 0);
+            cudaEventRecord(a, 0);
+            p.compress(d_in, n * sizeof(float), &out, &sz, 0);
+            cudaEventRecord(b, 0);
+            cudaEventSynchronize(b);
+            cudaEventElapsedTime(&ms, a, b);
+            if (i >= warmup) tc += ms;
+            cudaMemsetAsync(flush, i & 0xff, 256u << 20, 0);
+            void* dec = nullptr;
+            size_t dsz = 0;
+            cudaEventRecord(a, 0);
+            p.decompress(nullptr, 0, &dec, &dsz, 0);
+            cudaEventRecord(b, 0);
+            cudaEventSynchronize(b);
+            cudaEventElapsedTime(&ms, a, b);
+            if (i >= warmup) td += ms;
+        }
+        *comp_ms = (float)(tc / steps);
+        *decomp_ms = (float)(td / steps);
+        *comp_bytes = sz;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaFree(flush);
+        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device sync failed");
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    } catch (...) {
+        g_err = "unknown exception";
+        return -1;
+    }
+    return 0;
+}
