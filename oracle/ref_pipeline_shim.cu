@@ -19,12 +19,23 @@
 #include "quantizers/quantizer/quantizer.h"
 #include "transforms/negabinary/negabinary_stage.h"
 #include "transforms/zigzag/zigzag_stage.h"
+#include "ref_scrub.cuh"
 
 using namespace fz;
 
 static std::string g_err;
+// byte written over every SM's shared memory before each reference compress
+// (ref_scrub.cuh); -1 leaves shared memory as it is
+static int g_fill = 0;
 
 extern "C" const char* ref_pipe_last_error() { return g_err.c_str(); }
+
+extern "C" void ref_pipe_set_shared_fill(int byte) { g_fill = byte; }
+
+static void fill_shared() {
+    if (g_fill >= 0 && ref_scrub::fill_shared((uint8_t)g_fill, 0) != cudaSuccess)
+        throw std::runtime_error("shared-memory fill failed");
+}
 
 extern "C" int ref_pipeline_fzm(int chain, const float* d_in, size_t n, size_t x, size_t y, size_t z, float eb,
                                 int mode, int radius, float outlier_cap, int zigzag, int preallocate,
@@ -57,6 +68,7 @@ extern "C" int ref_pipeline_fzm(int chain, const float* d_in, size_t n, size_t x
         p.finalize();
         void* out = nullptr;
         size_t sz = 0;
+        fill_shared();
         p.compress(d_in, n * sizeof(float), &out, &sz, 0);
         if (cudaStreamSynchronize(0) != cudaSuccess) throw std::runtime_error("sync failed");
         *comp_bytes = sz;
@@ -138,6 +150,7 @@ extern "C" int ref_pipeline_codes(int chain, const float* d_in, size_t n, size_t
         p.finalize();
         void* out = nullptr;
         size_t sz = 0;
+        fill_shared();
         p.compress(d_in, n * sizeof(float), &out, &sz, 0);
         if (cudaStreamSynchronize(0) != cudaSuccess) throw std::runtime_error("sync failed");
         *comp_bytes = sz;
@@ -274,6 +287,7 @@ extern "C" int ref_pipeline_time_lq(const float* d_in, size_t x, size_t y, size_
         size_t sz = 0;
         for (int i = 0; i < warmup + steps; i++) {
             float ms = 0;
+            fill_shared();
             cudaMemsetAsync(flush, i & 0xff, 256u << 20, 0);
             cudaEventRecord(a, 0);
             p.compress(d_in, n * sizeof(float), &out, &sz, 0);
@@ -297,6 +311,36 @@ extern "C" int ref_pipeline_time_lq(const float* d_in, size_t x, size_t y, size_
         cudaEventDestroy(a);
         cudaEventDestroy(b);
         cudaFree(flush);
+        if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device sync failed");
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    } catch (...) {
+        g_err = "unknown exception";
+        return -1;
+    }
+    return 0;
+}
+
+// Loads a TOML configuration with the reference's own Pipeline::loadConfig
+// (src/pipeline/config.cpp:534-640), compresses n floats with it, writes the
+// FZM file and saves the configuration back with Pipeline::saveConfig.
+// `x, y, z` set the dimensions before loading, as a caller of the reference
+// does when its file has no `dims` key.
+extern "C" int ref_pipeline_config(const char* config_path, size_t x, size_t y, size_t z, const float* d_in,
+                                   size_t n, const char* fzm_path, const char* saved_path, size_t* comp_bytes) {
+    try {
+        Pipeline p;
+        if (x) p.setDims(x, y, z);
+        p.loadConfig(config_path);
+        fill_shared();
+        void* out = nullptr;
+        size_t sz = 0;
+        p.compress(d_in, n * sizeof(float), &out, &sz, 0);
+        if (cudaStreamSynchronize(0) != cudaSuccess) throw std::runtime_error("sync failed");
+        *comp_bytes = sz;
+        p.writeToFile(fzm_path, 0);
+        p.saveConfig(saved_path);
         if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device sync failed");
     } catch (const std::exception& e) {
         g_err = e.what();

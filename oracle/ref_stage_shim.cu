@@ -23,12 +23,22 @@
 #include "shufflers/bitshuffle/bitshuffle_stage.h"
 #include "transforms/negabinary/negabinary_stage.h"
 #include "transforms/zigzag/zigzag_stage.h"
+#include "ref_scrub.cuh"
 
 using namespace fz;
 
 static std::string g_err;
+// byte written over every SM's shared memory before the reference's
+// LorenzoQuant runs (ref_scrub.cuh); -1 leaves shared memory as it is
+static int g_fill = 0;
 
 extern "C" const char* ref_last_error() { return g_err.c_str(); }
+
+extern "C" void ref_set_shared_fill(int byte) { g_fill = byte; }
+
+extern "C" int ref_fill_shared(int byte) {
+    return ref_scrub::fill_shared((uint8_t)byte, 0) == cudaSuccess ? 0 : -1;
+}
 
 #define GUARD_BEGIN try {
 #define GUARD_END                                   \
@@ -51,6 +61,8 @@ extern "C" int ref_lq_fwd(const float* d_in, size_t n, size_t nx, size_t ny, siz
                           uint16_t* d_codes, float* d_err, uint32_t* d_idx,
                           uint32_t* d_count, uint8_t* hdr44) {
     GUARD_BEGIN
+    if (g_fill >= 0 && ref_scrub::fill_shared((uint8_t)g_fill, 0) != cudaSuccess)
+        throw std::runtime_error("shared-memory fill failed");
     MemoryPool pool(MemoryPoolConfig(n * sizeof(float), 3.0f));
     LorenzoQuantStage<float, uint16_t>::Config cfg;
     cfg.error_bound = eb;
