@@ -30,6 +30,24 @@ class ConfigError(RuntimeError):
     """A configuration the reference's loadConfig would reject."""
 
 
+def _eb_mode(s: str) -> int:
+    if s not in EB_MODES:
+        raise ConfigError(f"loadConfig: unknown error_bound_mode \"{s}\"")
+    return EB_MODES[s]
+
+
+def strategy(s: str) -> int:
+    if s not in STRATEGIES:
+        raise ConfigError(f"loadConfig: unknown memory_strategy \"{s}\"")
+    return STRATEGIES[s]
+
+
+def _huffman_mode(s: str):
+    if s not in ("Fine", "Coarse"):
+        raise ConfigError(f"loadConfig: unknown Huffman encode_mode \"{s}\"")
+    return P.HuffmanEncodeMode.Fine if s == "Fine" else P.HuffmanEncodeMode.Coarse
+
+
 def _dtype(s: str, what: str) -> int:
     if s not in DTYPES:
         raise ConfigError(f"loadConfig: unknown data type \"{s}\" ({what})")
@@ -45,14 +63,14 @@ def _stage_from_table(t: dict) -> P.Stage:
             raise ConfigError("loadConfig: unsupported Lorenzo type combination input_type=\""
                               f"{g('input_type', 'float32')}\" code_type=\"{g('code_type', 'uint16')}\"")
         return P.LorenzoQuantStage(float(g("error_bound", 1e-3)), int(g("quant_radius", 32768)),
-                                   float(g("outlier_capacity", 0.2)), EB_MODES[g("error_bound_mode", "ABS")],
+                                   float(g("outlier_capacity", 0.2)), _eb_mode(g("error_bound_mode", "ABS")),
                                    bool(g("zigzag_codes", False)))
     if typ == "Quantizer":
         code = g("code_type", "uint32")
         if g("input_type", "float32") != "float32" or code not in ("uint16", "uint32"):
             raise ConfigError("loadConfig: unsupported Quantizer type combination input_type=\""
                               f"{g('input_type', 'float32')}\" code_type=\"{code}\"")
-        return P.QuantizerStage(float(g("error_bound", 1e-3)), EB_MODES[g("error_bound_mode", "REL")],
+        return P.QuantizerStage(float(g("error_bound", 1e-3)), _eb_mode(g("error_bound_mode", "REL")),
                                 int(g("quant_radius", 32768)), float(g("outlier_capacity", 0.05)),
                                 code_bytes=2 if code == "uint16" else 4, zigzag_codes=bool(g("zigzag_codes", True)),
                                 inplace_outliers=bool(g("inplace_outliers", False)),
@@ -88,9 +106,9 @@ def _stage_from_table(t: dict) -> P.Stage:
                               f"got {nb}")
         return P.BitpackStage(DTYPE_BYTES[dt], nb)
     if typ == "Huffman":
+        mode = _huffman_mode(g("encode_mode", "Coarse"))
         s = P.HuffmanStage(int(g("bklen", 1024)))
-        s.setEncodeMode(P.HuffmanEncodeMode.Fine if g("encode_mode", "Coarse") == "Fine"
-                        else P.HuffmanEncodeMode.Coarse)
+        s.setEncodeMode(mode)
         return s
     raise ConfigError(f"loadConfig: unknown stage type \"{typ}\"")
 
@@ -100,6 +118,8 @@ def parse_config(text: str) -> dict:
     [(name, stage)], "connections": [(dependent, producer, port)]}."""
     doc = tomllib.loads(text)
     pl = dict(doc.get("pipeline", {}))
+    if "memory_strategy" in pl:
+        strategy(pl["memory_strategy"])
     arr = doc.get("stage")
     if not arr:
         raise ConfigError("loadConfig: no [[stage]] entries found")
@@ -128,27 +148,45 @@ def parse_config(text: str) -> dict:
 
 
 def _fmt(v) -> str:
+    """Numbers as the reference's writer prints them: integers plainly,
+    floating point with 17 significant digits (std::setprecision(
+    max_digits10) on a std::ostream)."""
     if isinstance(v, bool):
         return "true" if v else "false"
     if isinstance(v, float):
-        return "inf" if math.isinf(v) else repr(v)
+        if math.isinf(v):
+            return "inf" if v > 0 else "-inf"
+        t = f"{v:.17g}"
+        return t
     if isinstance(v, str):
         return f"\"{v}\""
     return str(v)
 
 
+def _f32(v: float) -> float:
+    """The float the stage stores, widened to double as the writer does."""
+    import struct
+    return struct.unpack("<f", struct.pack("<f", float(v)))[0]
+
+
 def _stage_table(s: P.Stage) -> dict:
-    """The keys config.cpp's save*Stage functions write for a stage."""
+    """The keys config.cpp's save*Stage functions write for a stage, in their
+    order; optional keys only when they differ from the loader's defaults."""
     if isinstance(s, P.LorenzoQuantStage):
-        return {"type": "LorenzoQuant", "input_type": "float32", "code_type": "uint16", "error_bound": float(s.error_bound),
-                "error_bound_mode": EB_NAMES[s.eb_mode], "quant_radius": int(s.quant_radius),
-                "outlier_capacity": float(s.outlier_capacity), "zigzag_codes": bool(s.zigzag_codes)}
+        return {"type": "LorenzoQuant", "input_type": "float32", "code_type": "uint16",
+                "error_bound": _f32(s.error_bound), "error_bound_mode": EB_NAMES[s.eb_mode],
+                "quant_radius": int(s.quant_radius), "outlier_capacity": _f32(s.outlier_capacity),
+                "zigzag_codes": bool(s.zigzag_codes)}
     if isinstance(s, P.QuantizerStage):
-        return {"type": "Quantizer", "input_type": "float32", "code_type": "uint16" if s.code_bytes == 2 else "uint32",
-                "error_bound": float(s.error_bound), "error_bound_mode": EB_NAMES[s.eb_mode],
-                "quant_radius": int(s.quant_radius), "outlier_capacity": float(s.outlier_capacity),
-                "zigzag_codes": bool(s.zigzag_codes), "inplace_outliers": bool(s.inplace_outliers),
-                "outlier_threshold": float(s.outlier_threshold)}
+        d = {"type": "Quantizer", "input_type": "float32", "code_type": "uint16" if s.code_bytes == 2 else "uint32",
+             "error_bound": _f32(s.error_bound), "error_bound_mode": EB_NAMES[s.eb_mode],
+             "quant_radius": int(s.quant_radius), "outlier_capacity": _f32(s.outlier_capacity),
+             "zigzag_codes": bool(s.zigzag_codes)}
+        if math.isfinite(s.outlier_threshold):
+            d["outlier_threshold"] = _f32(s.outlier_threshold)
+        if s.inplace_outliers:
+            d["inplace_outliers"] = True
+        return d
     if isinstance(s, P.LorenzoStage):
         return {"type": "Lorenzo", "data_type": DTYPE_NAMES[s.data_type]}
     if isinstance(s, P.BitshuffleStage):
@@ -169,31 +207,51 @@ def _stage_table(s: P.Stage) -> dict:
     if isinstance(s, P.BitpackStage):
         return {"type": "Bitpack", "input_type": {1: "uint8", 2: "uint16", 4: "uint32"}[s.elem], "nbits": int(s.nbits)}
     if isinstance(s, P.HuffmanStage):
-        return {"type": "Huffman", "input_type": "uint16", "bklen": int(s.bklen),
-                "encode_mode": "Fine" if s.encode_mode == P.HuffmanEncodeMode.Fine else "Coarse"}
+        d = {"type": "Huffman", "input_type": "uint16", "bklen": int(s.bklen)}
+        if s.encode_mode == P.HuffmanEncodeMode.Fine:
+            d["encode_mode"] = "Fine"
+        return d
     raise ConfigError(f"saveConfig: no TOML form for stage {s.getName()}")
 
 
+def _esc(v: str) -> str:
+    return v.replace("\\", "\\\\").replace('"', '\\"')
+
+
 def dump_config(pipeline_params: dict, stages: list, connections: list) -> str:
-    """TOML text of a pipeline (config.cpp saveConfig layout: [pipeline] then
-    one [[stage]] per stage with its inputs)."""
+    """TOML text of a pipeline in the layout of the reference's saveConfig
+    (config.cpp:645-720): two comment lines, [pipeline], then one [[stage]]
+    per stage with its inputs, each table followed by a blank line."""
     names, counts = {}, {}
     for s in stages:
         base = s.getName()
         k = counts.get(base, 0)
         counts[base] = k + 1
         names[id(s)] = base if k == 0 else f"{base}{k}"
-    out = ["# FZGPUModules pipeline config", "", "[pipeline]"]
+    out = ["# FZGPUModules pipeline config",
+           "# Generated by Pipeline::saveConfig(). Load with Pipeline::loadConfig().", "", "[pipeline]"]
     for key in ("input_size", "memory_strategy", "pool_multiplier", "num_streams", "dims"):
         if key in pipeline_params:
             v = pipeline_params[key]
-            out.append(f"{key} = [{', '.join(str(int(d)) for d in v)}]" if key == "dims" else f"{key} = {_fmt(v)}")
+            if key == "dims":
+                out.append(f"dims = [{', '.join(str(int(d)) for d in v)}]")
+            elif key == "pool_multiplier":
+                out.append(f"pool_multiplier = {_fmt(_f32(v))}")
+            else:
+                out.append(f"{key} = {_fmt(v)}")
+    out.append("")
     for s in stages:
-        out += ["", "[[stage]]", f"name = \"{names[id(s)]}\""]
+        out += ["[[stage]]", f"name = \"{_esc(names[id(s)])}\""]
         for k, v in _stage_table(s).items():
             out.append(f"{k} = {_fmt(v)}")
         ins = [(p, port) for (d, p, port) in connections if d is s]
         if ins:
-            out.append("inputs = [" + ", ".join(f"{{from = \"{names[id(p)]}\", port = \"{port}\"}}"
-                                                for p, port in ins) + "]")
+            parts = []
+            for p, port in ins:
+                e = f"{{ from = \"{_esc(names[id(p)])}\""
+                if port != "output":
+                    e += f", port = \"{_esc(port)}\""
+                parts.append(e + " }")
+            out.append("inputs = [" + ", ".join(parts) + "]")
+        out.append("")
     return "\n".join(out) + "\n"

@@ -134,10 +134,14 @@ struct Parser {
                                                           : (d[0] == '-' ? -1.0 : 1.0) * INFINITY;
             } else if (d.find_first_of(".eE") != std::string::npos) {
                 v.kind = TVal::Flt;
-                try { v.f = std::stod(d); } catch (...) { err("bad number \"" + w + "\""); }
+                size_t used = 0;
+                try { v.f = std::stod(d, &used); } catch (...) { used = 0; }
+                if (d.empty() || used != d.size()) err("bad number \"" + w + "\"");
             } else {
                 v.kind = TVal::Int;
-                try { v.i = std::stoll(d); } catch (...) { err("bad value \"" + w + "\""); }
+                size_t used = 0;
+                try { v.i = std::stoll(d, &used, 10); } catch (...) { used = 0; }
+                if (d.empty() || used != d.size()) err("bad value \"" + w + "\"");
             }
         }
         return v;
@@ -173,6 +177,8 @@ struct Parser {
             if (p >= t.size() || t[p] != '=') err("expected '='");
             p++;
             cur->tab[k] = value();
+            ws(false);  // a value ends its line (a comment may follow)
+            if (p < t.size() && t[p] != '\n') err("expected the end of the line after the value of '" + k + "'");
         }
         return root;
     }
@@ -223,9 +229,31 @@ const char* dtype_name(uint8_t d) {
 }
 
 ErrorBoundMode eb_mode_of(const std::string& s) {
+    if (s == "ABS") return ErrorBoundMode::ABS;
     if (s == "REL") return ErrorBoundMode::REL;
     if (s == "NOA") return ErrorBoundMode::NOA;
-    return ErrorBoundMode::ABS;
+    fail("loadConfig: unknown error_bound_mode \"" + s + "\"");
+}
+
+MemoryStrategy strategy_of(const std::string& s) {
+    if (s == "PREALLOCATE") return MemoryStrategy::PREALLOCATE;
+    if (s == "MINIMAL") return MemoryStrategy::MINIMAL;
+    fail("loadConfig: unknown memory_strategy \"" + s + "\"");
+}
+
+HuffmanEncodeMode huffman_mode_of(const std::string& s) {
+    if (s == "Fine") return HuffmanEncodeMode::Fine;
+    if (s == "Coarse") return HuffmanEncodeMode::Coarse;
+    fail("loadConfig: unknown Huffman encode_mode \"" + s + "\"");
+}
+
+std::string toml_escape(const std::string& s) {
+    std::string o;
+    for (char c : s) {
+        if (c == '\\' || c == '"') o += '\\';
+        o += c;
+    }
+    return o;
 }
 const char* eb_mode_name(ErrorBoundMode m) {
     return m == ErrorBoundMode::REL ? "REL" : m == ErrorBoundMode::NOA ? "NOA" : "ABS";
@@ -349,8 +377,7 @@ Stage* add_stage(Pipeline& p, const TVal& t, const std::string& type) {
     if (type == "Huffman") {
         auto* s = p.addStage<HuffmanStage<uint16_t>>();
         s->setBklen((uint32_t)opt_int(t, "bklen", 1024));
-        s->setEncodeMode(opt_str(t, "encode_mode", "Coarse") == "Fine" ? HuffmanEncodeMode::Fine
-                                                                        : HuffmanEncodeMode::Coarse);
+        s->setEncodeMode(huffman_mode_of(opt_str(t, "encode_mode", "Coarse")));
         return s;
     }
     fail("loadConfig: unknown stage type \"" + type + "\"");
@@ -360,81 +387,102 @@ template <typename S>
 bool save_quant(Stage* st, std::ostringstream& o, const char* code) {
     auto* s = dynamic_cast<S*>(st);
     if (!s) return false;
-    o << "type = \"Quantizer\"\ninput_type = \"float32\"\ncode_type = \"" << code << "\"\n"
+    o << "input_type = \"float32\"\ncode_type = \"" << code << "\"\n"
       << "error_bound = " << (double)s->getErrorBound() << "\nerror_bound_mode = \"" << eb_mode_name(s->getErrorBoundMode())
-      << "\"\nquant_radius = " << s->getQuantRadius() << "\noutlier_capacity = " << (double)s->getOutlierCapacity()
-      << "\nzigzag_codes = " << (s->getZigzagCodes() ? "true" : "false")
-      << "\ninplace_outliers = " << (s->getInplaceOutliers() ? "true" : "false") << "\n";
+      << "\"\nquant_radius = " << (int64_t)s->getQuantRadius() << "\noutlier_capacity = " << (double)s->getOutlierCapacity()
+      << "\nzigzag_codes = " << (s->getZigzagCodes() ? "true" : "false") << "\n";
     const float th = s->getOutlierThreshold();
-    o << "outlier_threshold = ";
-    if (std::isinf(th)) o << (th > 0 ? "inf" : "-inf");
-    else o << (double)th;
-    o << "\n";
+    if (std::isfinite(th)) o << "outlier_threshold = " << th << "\n";  // only a finite threshold is written
+    if (s->getInplaceOutliers()) o << "inplace_outliers = true\n";
     return true;
 }
 
-template <typename T>
-bool save_bitpack(Stage* st, std::ostringstream& o, const char* name) {
-    auto* s = dynamic_cast<BitpackStage<T>*>(st);
-    if (!s) return false;
-    o << "type = \"Bitpack\"\ninput_type = \"" << name << "\"\nnbits = " << (int)s->getNBits() << "\n";
-    return true;
-}
-
-void save_stage(Stage* st, std::ostringstream& o) {
-    if (auto* s = dynamic_cast<LorenzoQuantStage<float, uint16_t>*>(st)) {
-        o << "type = \"LorenzoQuant\"\ninput_type = \"float32\"\ncode_type = \"uint16\"\nerror_bound = "
-          << (double)s->getErrorBound() << "\nerror_bound_mode = \"" << eb_mode_name(s->getErrorBoundMode())
-          << "\"\nquant_radius = " << (int)s->getQuantRadius() << "\noutlier_capacity = " << (double)s->getOutlierCapacity()
-          << "\nzigzag_codes = " << (s->getZigzagCodes() ? "true" : "false") << "\n";
-        return;
-    }
-    if (save_quant<QuantizerStage<float, uint16_t>>(st, o, "uint16")) return;
-    if (save_quant<QuantizerStage<float, uint32_t>>(st, o, "uint32")) return;
-    if (auto* s = dynamic_cast<BitshuffleStage*>(st)) {
-        o << "type = \"Bitshuffle\"\nblock_size = " << s->getBlockSize() << "\nelement_width = " << s->getElementWidth()
-          << "\n";
-        return;
-    }
-    if (auto* s = dynamic_cast<RZEStage*>(st)) {
-        o << "type = \"RZE\"\nchunk_size = " << s->getChunkSize() << "\nlevels = " << s->getLevels() << "\n";
-        return;
-    }
-    if (save_bitpack<uint8_t>(st, o, "uint8") || save_bitpack<uint16_t>(st, o, "uint16") ||
-        save_bitpack<uint32_t>(st, o, "uint32"))
-        return;
-    if (auto* s = dynamic_cast<HuffmanStage<uint16_t>*>(st)) {
-        o << "type = \"Huffman\"\ninput_type = \"uint16\"\nbklen = " << s->getBklen() << "\nencode_mode = \""
-          << (s->getEncodeMode() == HuffmanEncodeMode::Fine ? "Fine" : "Coarse") << "\"\n";
-        return;
-    }
+// The fields of one [[stage]] table after its name and type, in the order and
+// number format of the reference's writers (src/pipeline/config.cpp:250-395):
+// types from the stage's own header or data types, optional keys only when
+// they differ from the loader's defaults.
+void save_stage_fields(Stage* st, std::ostringstream& o) {
     const auto type = (StageType)st->getStageTypeId();
-    const bool was_inverse = st->isInverse();
-    st->setInverse(false);  // the forward direction's types
-    const char* in = dtype_name(st->getInputDataType(0));
-    const char* out = dtype_name(st->getOutputDataType(0));
-    st->setInverse(was_inverse);
+    auto in_t = [&] { return dtype_name(st->getInputDataType(0)); };
+    auto out_t = [&] { return dtype_name(st->getOutputDataType(0)); };
     switch (type) {
-        case StageType::RLE: o << "type = \"RLE\"\ndata_type = \"" << in << "\"\n"; return;
-        case StageType::LORENZO: o << "type = \"Lorenzo\"\ndata_type = \"" << in << "\"\n"; return;
+        case StageType::LORENZO_QUANT: {
+            auto* s = dynamic_cast<LorenzoQuantStage<float, uint16_t>*>(st);
+            if (!s) fail("saveConfig: no TOML form for stage " + st->getName());
+            o << "input_type = \"float32\"\ncode_type = \"uint16\"\nerror_bound = " << (double)s->getErrorBound()
+              << "\nerror_bound_mode = \"" << eb_mode_name(s->getErrorBoundMode())
+              << "\"\nquant_radius = " << (int64_t)s->getQuantRadius() << "\noutlier_capacity = "
+              << (double)s->getOutlierCapacity() << "\nzigzag_codes = " << (s->getZigzagCodes() ? "true" : "false")
+              << "\n";
+            return;
+        }
+        case StageType::QUANTIZER:
+            if (save_quant<QuantizerStage<float, uint16_t>>(st, o, "uint16")) return;
+            if (save_quant<QuantizerStage<float, uint32_t>>(st, o, "uint32")) return;
+            fail("saveConfig: no TOML form for stage " + st->getName());
+        case StageType::BITSHUFFLE: {
+            auto* s = static_cast<BitshuffleStage*>(st);
+            o << "block_size = " << (int64_t)s->getBlockSize() << "\nelement_width = " << (int64_t)s->getElementWidth()
+              << "\n";
+            return;
+        }
+        case StageType::RZE: {
+            auto* s = static_cast<RZEStage*>(st);
+            o << "chunk_size = " << (int64_t)s->getChunkSize() << "\nlevels = " << (int64_t)s->getLevels() << "\n";
+            return;
+        }
+        case StageType::RLE: o << "data_type = \"" << out_t() << "\"\n"; return;
+        case StageType::LORENZO: o << "data_type = \"" << out_t() << "\"\n"; return;
         case StageType::ZIGZAG:
         case StageType::NEGABINARY:
-            o << "type = \"" << (type == StageType::ZIGZAG ? "Zigzag" : "Negabinary") << "\"\ninput_type = \"" << in
-              << "\"\noutput_type = \"" << out << "\"\n";
+            o << "input_type = \"" << in_t() << "\"\noutput_type = \"" << out_t() << "\"\n";
             return;
         case StageType::DIFFERENCE: {
-            size_t cs = 0;
+            o << "input_type = \"" << in_t() << "\"\noutput_type = \"" << out_t() << "\"\n";
             uint8_t hdr[8] = {};
             if (st->serializeHeader(0, hdr, sizeof(hdr)) >= 6) {
                 uint32_t v;
                 std::memcpy(&v, hdr + 2, 4);
-                cs = v;
+                o << "chunk_size = " << (int64_t)v << "\n";
             }
-            o << "type = \"Difference\"\ninput_type = \"" << in << "\"\noutput_type = \"" << out
-              << "\"\nchunk_size = " << cs << "\n";
+            return;
+        }
+        case StageType::BITPACK: {
+            uint8_t hdr[10] = {};
+            const size_t n = st->serializeHeader(0, hdr, sizeof(hdr));
+            o << "input_type = \"" << dtype_name(n >= 1 ? hdr[0] : (uint8_t)DataType::UINT16) << "\"\nnbits = "
+              << (int64_t)(n >= 2 ? hdr[1] : 16) << "\n";
+            return;
+        }
+        case StageType::HUFFMAN: {
+            uint8_t hdr[16] = {};
+            const size_t n = st->serializeHeader(0, hdr, sizeof(hdr));
+            uint16_t bklen = 1024;
+            if (n >= 3) std::memcpy(&bklen, hdr + 1, 2);
+            o << "input_type = \"" << dtype_name(n >= 1 ? hdr[0] : (uint8_t)DataType::UINT16) << "\"\nbklen = "
+              << (int64_t)bklen << "\n";
+            auto* s = dynamic_cast<HuffmanStage<uint16_t>*>(st);
+            if (s && s->getEncodeMode() == HuffmanEncodeMode::Fine) o << "encode_mode = \"Fine\"\n";
             return;
         }
         default: fail("saveConfig: no TOML form for stage " + st->getName());
+    }
+}
+
+const char* stage_type_name(StageType t) {
+    switch (t) {
+        case StageType::LORENZO: return "Lorenzo";
+        case StageType::LORENZO_QUANT: return "LorenzoQuant";
+        case StageType::QUANTIZER: return "Quantizer";
+        case StageType::BITSHUFFLE: return "Bitshuffle";
+        case StageType::RZE: return "RZE";
+        case StageType::RLE: return "RLE";
+        case StageType::DIFFERENCE: return "Difference";
+        case StageType::ZIGZAG: return "Zigzag";
+        case StageType::NEGABINARY: return "Negabinary";
+        case StageType::BITPACK: return "Bitpack";
+        case StageType::HUFFMAN: return "Huffman";
+        default: return "Unknown";
     }
 }
 
@@ -459,7 +507,10 @@ void Pipeline::loadConfig(const std::string& path) {
             setDims(d);
         }
         if (const TVal* v = pl->get("memory_strategy"); v && v->kind == TVal::Str)
-            setMemoryStrategy(v->s == "PREALLOCATE" ? MemoryStrategy::PREALLOCATE : MemoryStrategy::MINIMAL);
+            setMemoryStrategy(strategy_of(v->s));
+        if (const TVal* v = pl->get("pool_multiplier"); v && (v->kind == TVal::Flt || v->kind == TVal::Int))
+            pool_multiplier_ = v->kind == TVal::Flt ? (float)v->f : (float)v->i;
+        if (const TVal* v = pl->get("num_streams"); v && v->kind == TVal::Int) setNumStreams((int)v->i);
     }
     const TVal* arr = doc.get("stage");
     if (!arr || arr->kind != TVal::Arr || arr->arr.empty())
@@ -504,26 +555,32 @@ void Pipeline::saveConfig(const std::string& path) const {
         names[s.get()] = k == 0 ? base : base + std::to_string(k);
     }
     std::ostringstream o;
+    o << "# FZGPUModules pipeline config\n"
+      << "# Generated by Pipeline::saveConfig(). Load with Pipeline::loadConfig().\n\n";
+    o << "[pipeline]\ninput_size = " << (int64_t)input_size_hint_ << "\nmemory_strategy = \""
+      << (strategy_ == MemoryStrategy::PREALLOCATE ? "PREALLOCATE" : "MINIMAL") << "\"\n";
     o << std::setprecision(std::numeric_limits<double>::max_digits10);
-    o << "# FZGPUModules pipeline config\n\n[pipeline]\ninput_size = " << input_size_hint_
-      << "\nmemory_strategy = \"" << (strategy_ == MemoryStrategy::PREALLOCATE ? "PREALLOCATE" : "MINIMAL")
-      << "\"\nnum_streams = 1\ndims = [" << dims_[0] << ", " << dims_[1] << ", " << dims_[2] << "]\n";
+    o << "pool_multiplier = " << (double)pool_multiplier_ << "\nnum_streams = " << (int64_t)num_streams_
+      << "\ndims = [" << (int64_t)dims_[0] << ", " << (int64_t)dims_[1] << ", " << (int64_t)dims_[2] << "]\n\n";
     for (const auto& s : stages_) {
-        o << "\n[[stage]]\nname = \"" << names[s.get()] << "\"\n";
-        save_stage(s.get(), o);
-        std::vector<std::string> ins;
-        for (const auto& c : connections_)
-            if (c.dependent == s.get())
-                ins.push_back("{from = \"" + names[c.producer] + "\", port = \"" + c.output_name + "\"}");
-        if (!ins.empty()) {
-            o << "inputs = [";
-            for (size_t k = 0; k < ins.size(); k++) o << (k ? ", " : "") << ins[k];
-            o << "]\n";
+        o << "[[stage]]\nname = \"" << toml_escape(names[s.get()]) << "\"\ntype = \""
+          << stage_type_name((StageType)s->getStageTypeId()) << "\"\n";
+        save_stage_fields(s.get(), o);
+        bool any = false;
+        for (const auto& c : connections_) {
+            if (c.dependent != s.get()) continue;
+            o << (any ? ", " : "inputs = [") << "{ from = \"" << toml_escape(names[c.producer]) << "\"";
+            if (c.output_name != "output") o << ", port = \"" << toml_escape(c.output_name) << "\"";
+            o << " }";
+            any = true;
         }
+        if (any) o << "]\n";
+        o << "\n";
     }
     std::ofstream f(path);
-    if (!f) fail("saveConfig: cannot write \"" + path + "\"");
+    if (!f) fail("saveConfig: cannot open \"" + path + "\" for writing");
     f << o.str();
+    if (!f) fail("saveConfig: write error on \"" + path + "\"");
 }
 
 }  // namespace fz

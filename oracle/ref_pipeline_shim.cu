@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 #include <string>
 
 #include "pipeline/compressor.h"
@@ -27,6 +28,20 @@ static std::string g_err;
 // byte written over every SM's shared memory before each reference compress
 // (ref_scrub.cuh); -1 leaves shared memory as it is
 static int g_fill = 0;
+
+// The reference's Huffman coarse encoder starts its host scan of the
+// partition cell counts at h_par_entry[0] without writing it
+// (phf/hf_kernels.cu:419-420); that array is pinned memory from
+// MemoryPool::allocatePersistentPinned (src/mem/mempool.cpp:258), which a
+// recycled pinned allocation can hand over with stale bytes, shifting every
+// partition of the bitstream.  The parity build compiles mempool.cpp with
+// its cudaMallocHost call routed here (oracle/Makefile), so that the array
+// starts at zero as on a fresh allocation.
+extern "C" cudaError_t fzref_zeroed_malloc_host(void** ptr, size_t bytes) {
+    const cudaError_t e = cudaHostAlloc(ptr, bytes, cudaHostAllocDefault);
+    if (e == cudaSuccess && *ptr) std::memset(*ptr, 0, bytes);
+    return e;
+}
 
 extern "C" const char* ref_pipe_last_error() { return g_err.c_str(); }
 

@@ -1,7 +1,7 @@
 // Test infrastructure shared by the reference shims: set every SM's shared
 // memory to one byte value before a reference kernel runs.
 //
-// The reference's 3-D LorenzoQuant kernel (lorenzo_quant_nd.cu:214-247)
+// The reference's 3-D LorenzoQuant kernel (lorenzo_quant_nd.cu:214,246)
 // takes its y difference as `delta -= (threadIdx.y > 0) * s[threadIdx.y][tx]`.
 // Row 0 of `s` is a ghost row that is never written, so threads with
 // threadIdx.y == 0 multiply whatever an earlier kernel left in that shared

@@ -92,3 +92,60 @@ def test_dump_round_trip():
     for (_, a), (_, b) in zip(cfg["stages"], again["stages"]):
         assert type(a) is type(b) and CF._stage_table(a) == CF._stage_table(b)
     assert len(again["connections"]) == 3 and again["pipeline"]["input_size"] == 4096
+
+
+BAD_VALUES = [
+    ('[[stage]]\nname = "a"\ntype = "LorenzoQuant"\nerror_bound_mode = "rel"\n', 'unknown error_bound_mode "rel"'),
+    ('[[stage]]\nname = "a"\ntype = "Quantizer"\nerror_bound_mode = "Absolute"\n',
+     'unknown error_bound_mode "Absolute"'),
+    ('[pipeline]\nmemory_strategy = "prealloc"\n[[stage]]\nname = "a"\ntype = "RZE"\n',
+     'unknown memory_strategy "prealloc"'),
+    ('[[stage]]\nname = "a"\ntype = "Huffman"\nencode_mode = "fine"\n', 'unknown Huffman encode_mode "fine"'),
+]
+
+
+@pytest.mark.parametrize("text,msg", BAD_VALUES)
+def test_unknown_enum_names_are_rejected(text, msg):
+    # the reference throws on names it does not know (config.cpp:60-98)
+    # rather than falling back to a default mode
+    with pytest.raises(CF.ConfigError, match=msg):
+        CF.parse_config(text)
+
+
+@pytest.mark.parametrize("text,msg", BAD_VALUES + [
+    ('[[stage]]\nname = "a"\ntype = "RZE"\nlevels = 4abc\n', 'bad value "4abc"'),
+    ('[[stage]]\nname = "a"\ntype = "RZE"\nlevels = 0x4\n', 'bad value "0x4"'),
+    ('[[stage]]\nname = "a"\ntype = "LorenzoQuant"\nerror_bound = 1e-3x\n', 'bad number "1e-3x"'),
+    ('[[stage]]\nname = "a"\ntype = "RZE" levels = 4\n', "end of the line after the value of 'type'"),
+])
+def test_native_loader_rejects_what_the_reference_rejects(tmp_path, text, msg):
+    # the C++ loader parses and fails before anything touches the device
+    import ctypes as C
+
+    from fzgpumodules_b200._lib import lib
+    path = tmp_path / "bad.toml"
+    path.write_text(text)
+    h = lib().fzb_pipeline_create(0, 0, 3.0)
+    assert h
+    try:
+        rc = lib().fzb_pipeline_load_config(C.c_void_p(h), str(path).encode())
+        assert rc < 0
+        assert msg in lib().fzb_last_error().decode()
+    finally:
+        lib().fzb_pipeline_destroy(C.c_void_p(h))
+
+
+def test_dump_matches_the_reference_layout():
+    cfg = CF.parse_config(PFPL_LIKE)
+    stages = [s for _, s in cfg["stages"]]
+    text = CF.dump_config({"input_size": 4096, "memory_strategy": "PREALLOCATE", "pool_multiplier": 2.5,
+                           "num_streams": 1, "dims": [512, 512, 64]}, stages, cfg["connections"])
+    lines = text.split("\n")
+    assert lines[:9] == ["# FZGPUModules pipeline config",
+                         "# Generated by Pipeline::saveConfig(). Load with Pipeline::loadConfig().", "",
+                         "[pipeline]", "input_size = 4096", 'memory_strategy = "PREALLOCATE"', "pool_multiplier = 2.5",
+                         "num_streams = 1", "dims = [512, 512, 64]"]
+    q = text[text.index('name = "Quantizer"'):]
+    assert "error_bound = 0.0010000000474974513\n" in q and "outlier_threshold" not in q
+    assert 'inputs = [{ from = "Quantizer", port = "codes" }]' in text
+    assert 'inputs = [{ from = "Difference" }]' in text
