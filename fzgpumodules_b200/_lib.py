@@ -62,6 +62,12 @@ def lib():
         L.fzb_lq_bs_rze_compress.argtypes = [p, u64, p, f32, i32, f32, u32, i32, p, p, u64, p, p, p, p, p, sz, p]
         L.fzb_lq_bs_rze_decompress.restype = i32
         L.fzb_lq_bs_rze_decompress.argtypes = [p, u64, p, p, p, u64, u64, p, f32, i32, p, C.c_uint, p, sz, p]
+        L.fzb_lq_bs_rze_decompress_dev.restype = i32
+        L.fzb_lq_bs_rze_decompress_dev.argtypes = [p, u64, p, p, p, u64, u64, p, p, i32, p, p, sz, p]
+        L.fzb_lq_inverse_dev.restype = i32
+        L.fzb_lq_inverse_dev.argtypes = [p, p, p, p, u64, u64, p, p, i32, p, p, sz, p]
+        L.fzb_concat_split.restype = i32
+        L.fzb_concat_split.argtypes = [p, u64, p, p, i32, p, p]
         L.fzb_rle_max_bytes.restype = u64
         L.fzb_rle_max_bytes.argtypes = [u64, i32]
         L.fzb_rle_encode.restype = i32
@@ -129,6 +135,11 @@ def lib():
         L.fzb_pipeline_save_config.argtypes = [p, C.c_char_p]
         L.fzb_pipeline_set_fusion.argtypes = [p, i32]
         L.fzb_pipeline_enable_graph_mode.argtypes = [p, i32]
+        L.fzb_pipeline_set_num_streams.argtypes = [p, i32]
+        L.fzb_pipeline_decompress_graph_captured.argtypes = [p]
+        L.fzb_pipeline_check_decompress.argtypes = [p, p]
+        L.fzb_pipeline_num_streams.argtypes = [p]
+        L.fzb_pipeline_enable_bounds_check.argtypes = [p, i32]
         L.fzb_pipeline_enable_profiling.argtypes = [p, i32]
         L.fzb_pipeline_finalize.argtypes = [p]
         L.fzb_pipeline_is_fused.argtypes = [p]

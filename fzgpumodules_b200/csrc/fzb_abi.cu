@@ -279,25 +279,39 @@ InvArgs inv_args(const Work& w, const Geometry& g, uint64_t n_total) {
     return a;
 }
 
-// memset(out) + scatter + tile kernels (the exact path).
+int sm_count() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+// zero(out) + scatter + tile kernels (the exact path).  Every kernel walks
+// its tiles grid-stride: one tile per CTA normally; when the launch is gated
+// on the device status (a.gate) the grids are a few CTAs per SM, so a gate
+// that says "not needed" costs a few microseconds.
 int exact_inverse(const InvArgs& a, const Geometry& g, cudaStream_t s) {
-    CK(cudaMemsetAsync(a.out, 0, sizeof(float) * (size_t)a.n_total, s));
+    const uint32_t lim = a.gate ? 2u * (uint32_t)sm_count() : 0xffffffffu;
+    auto grid = [&](uint64_t tiles) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, lim)); };
+    if (a.gate) {
+        TraceScope ts(s, "zero_out");
+        zero_out_kernel<<<grid(((uint64_t)a.n_total + 1023) / 1024), 256, 0, s>>>(a);
+        CK(cudaGetLastError());
+    } else {
+        CK(cudaMemsetAsync(a.out, 0, sizeof(float) * (size_t)a.n_total, s));
+    }
     if (a.cap) {
-        uint32_t blocks = (uint32_t)((a.cap + 255) / 256);
-        if (blocks > 4096) blocks = 4096;
         TraceScope ts(s, "scatter_outliers");
-        scatter_outliers_kernel<<<blocks, 256, 0, s>>>(a);
+        scatter_outliers_kernel<<<std::min(grid((a.cap + 255) / 256), 4096u), 256, 0, s>>>(a);
         CK(cudaGetLastError());
     }
     TraceScope ts(s, "lq_inverse");
     if (g.ndim == 1) {
-        lq_inverse_1d_kernel<<<(g.nfield + 1023) / 1024, 256, 0, s>>>(a);
+        lq_inverse_1d_kernel<<<grid((g.nfield + 1023) / 1024), 256, 0, s>>>(a);
     } else if (g.ndim == 2) {
-        dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32, 1);
-        lq_inverse_2d_kernel<<<grid, 128, 0, s>>>(a);
+        lq_inverse_2d_kernel<<<grid((uint64_t)((g.nx + 31) / 32) * ((g.ny + 31) / 32)), 128, 0, s>>>(a);
     } else {
-        dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + 7) / 8);
-        lq_inverse_3d_kernel<<<grid, 256, 0, s>>>(a);
+        lq_inverse_3d_kernel<<<grid((uint64_t)((g.nx + 31) / 32) * ((g.ny + 7) / 8) * ((g.nz + 7) / 8)), 256, 0, s>>>(a);
     }
     CK(cudaGetLastError());
     return FZB_OK;
@@ -366,10 +380,10 @@ int fzb_lq_bs_rze_compress(const float* d_in, uint64_t n_total, const uint32_t d
                           d_work, work_bytes, stream);
 }
 
-int fzb_lq_inverse(const uint16_t* d_codes, const float* d_err, const uint32_t* d_idx,
-                   const uint32_t* d_count, uint64_t cap, uint64_t n_total, const uint32_t dims[3],
-                   float abs_eb, int zigzag, float* d_out, void* d_work, size_t work_bytes,
-                   void* stream) {
+namespace {
+int lq_inverse_common(const uint16_t* d_codes, const float* d_err, const uint32_t* d_idx, const uint32_t* d_count,
+                      uint64_t cap, uint64_t n_total, const uint32_t dims[3], float abs_eb, const float* d_abs_eb,
+                      int zigzag, float* d_out, void* d_work, size_t work_bytes, void* stream) {
     Geometry g;
     int rc = geometry(n_total, dims, &g);
     if (rc) return rc;
@@ -385,9 +399,28 @@ int fzb_lq_inverse(const uint16_t* d_codes, const float* d_err, const uint32_t* 
     a.out_count = d_count;
     a.cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
     a.ebx2 = 2.0f * abs_eb;
+    a.abs_eb_src = d_abs_eb;
     a.zigzag = zigzag;
     a.out = d_out;
     return exact_inverse(a, g, s);
+}
+}  // namespace
+
+int fzb_lq_inverse(const uint16_t* d_codes, const float* d_err, const uint32_t* d_idx,
+                   const uint32_t* d_count, uint64_t cap, uint64_t n_total, const uint32_t dims[3],
+                   float abs_eb, int zigzag, float* d_out, void* d_work, size_t work_bytes,
+                   void* stream) {
+    return lq_inverse_common(d_codes, d_err, d_idx, d_count, cap, n_total, dims, abs_eb, nullptr, zigzag, d_out,
+                             d_work, work_bytes, stream);
+}
+
+int fzb_lq_inverse_dev(const uint16_t* d_codes, const float* d_err, const uint32_t* d_idx,
+                       const uint32_t* d_count, uint64_t cap, uint64_t n_total, const uint32_t dims[3],
+                       const float* d_abs_eb, int zigzag, float* d_out, void* d_work, size_t work_bytes,
+                       void* stream) {
+    if (!d_abs_eb) return FZB_E_INVALID;
+    return lq_inverse_common(d_codes, d_err, d_idx, d_count, cap, n_total, dims, 0.0f, d_abs_eb, zigzag, d_out,
+                             d_work, work_bytes, stream);
 }
 
 int fzb_bitshuffle(const void* d_in, uint64_t bytes, uint32_t block, int ew, int inverse,
@@ -486,11 +519,12 @@ int fzb_rze_decode(const void* d_in, uint64_t in_bytes, uint64_t orig_bytes, voi
     return FZB_OK;
 }
 
-int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float* d_err,
-                             const uint32_t* d_idx, const uint32_t* d_count, uint64_t cap,
-                             uint64_t n_total, const uint32_t dims[3], float abs_eb, int zigzag,
-                             float* d_out, unsigned flags, void* d_work, size_t work_bytes,
-                             void* stream) {
+namespace {
+int lq_bs_rze_decompress_common(const void* d_rze, uint64_t rze_bytes, const float* d_err,
+                                const uint32_t* d_idx, const uint32_t* d_count, uint64_t cap,
+                                uint64_t n_total, const uint32_t dims[3], float abs_eb, const float* d_abs_eb,
+                                int zigzag, float* d_out, unsigned flags, void* d_work, size_t work_bytes,
+                                void* stream) {
     Geometry g;
     int rc = geometry(n_total, dims, &g);
     if (rc) return rc;
@@ -518,9 +552,11 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
     a.out_count = d_count;
     a.cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
     a.ebx2 = 2.0f * abs_eb;
+    a.abs_eb_src = d_abs_eb;
     a.zigzag = zigzag;
     a.shuffled = 1;
     a.out = d_out;
+    const bool dev_fallback = (flags & FZB_DEVICE_FALLBACK) != 0;
 
     const uint32_t nx = g.nx;
     const bool pow2 = nx >= 8 && nx <= 1024 && (nx & (nx - 1)) == 0;
@@ -550,13 +586,19 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
         CK(cudaGetLastError());
         if (n_total > g.nfield)
             CK(cudaMemsetAsync(d_out + g.nfield, 0, sizeof(float) * (n_total - g.nfield), s));
-        if (flags & FZB_NO_SYNC) return FZB_OK;
+        if (dev_fallback) {
+            // the exact kernels follow, gated on the flags the fused kernel set
+            a.gate = w.err;
+            a.gate_mask = kErrInexact | kErrUnsorted;
+        } else {
+            if (flags & FZB_NO_SYNC) return FZB_OK;
         uint32_t bits = 0;
         rc = read_status(w, s, &bits);
         if (rc) return rc;
         if (bits & (kErrMalformed | kErrLookbackTimeout)) return status_of(bits);
-        if (!(bits & (kErrInexact | kErrUnsorted))) return FZB_OK;
-        CK(cudaMemsetAsync(w.err, 0, 4, s));  // rerun exactly below
+            if (!(bits & (kErrInexact | kErrUnsorted))) return FZB_OK;
+            CK(cudaMemsetAsync(w.err, 0, 4, s));  // rerun exactly below
+        }
     }
     a.codes = w.codes;
     const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
@@ -564,14 +606,35 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
                             smem));
     {
         TraceScope ts(s, "rze_decode_bitunshuffle");
-        rze_decode_codes_kernel<<<(unsigned)nch, kThreads, smem, s>>>(a);
+        const uint64_t lim = a.gate ? 4ull * (uint64_t)sm_count() : nch;
+        rze_decode_codes_kernel<<<(unsigned)std::min<uint64_t>(nch, lim), kThreads, smem, s>>>(a);
     }
     CK(cudaGetLastError());
     rc = exact_inverse(a, g, s);
-    if (rc || (flags & FZB_NO_SYNC)) return rc;
+    if (rc || (flags & (FZB_NO_SYNC | FZB_DEVICE_FALLBACK))) return rc;
     uint32_t bits = 0;
     rc = read_status(w, s, &bits);
     return rc ? rc : status_of(bits);
+}
+
+}  // namespace
+
+int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float* d_err,
+                             const uint32_t* d_idx, const uint32_t* d_count, uint64_t cap,
+                             uint64_t n_total, const uint32_t dims[3], float abs_eb, int zigzag,
+                             float* d_out, unsigned flags, void* d_work, size_t work_bytes,
+                             void* stream) {
+    return lq_bs_rze_decompress_common(d_rze, rze_bytes, d_err, d_idx, d_count, cap, n_total, dims, abs_eb,
+                                       nullptr, zigzag, d_out, flags, d_work, work_bytes, stream);
+}
+
+int fzb_lq_bs_rze_decompress_dev(const void* d_rze, uint64_t rze_capacity, const float* d_err,
+                                 const uint32_t* d_idx, const uint32_t* d_count, uint64_t cap,
+                                 uint64_t n_total, const uint32_t dims[3], const float* d_abs_eb, int zigzag,
+                                 float* d_out, void* d_work, size_t work_bytes, void* stream) {
+    if (!d_abs_eb) return FZB_E_INVALID;
+    return lq_bs_rze_decompress_common(d_rze, rze_capacity, d_err, d_idx, d_count, cap, n_total, dims, 0.0f,
+                                       d_abs_eb, zigzag, d_out, FZB_DEVICE_FALLBACK, d_work, work_bytes, stream);
 }
 
 uint64_t fzb_rle_max_bytes(uint64_t n, int elem) {
@@ -680,13 +743,6 @@ HfWork carve_hf(void* base, uint64_t n, uint32_t bklen) {
 // bklen even keeps every u32 table of the blob 4-byte aligned
 inline bool hf_args_ok(uint64_t n, uint32_t bklen) {
     return n > 0 && n < (1ull << 31) && bklen >= 2 && bklen <= 65534 && (bklen & 1) == 0;
-}
-
-inline int sm_count() {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms;
 }
 
 }  // namespace

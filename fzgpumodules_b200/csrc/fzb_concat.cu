@@ -87,3 +87,81 @@ extern "C" int fzb_concat(const void* const* d_srcs, const uint64_t* sizes, int 
     concat_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(p, static_cast<uint8_t*>(d_out));
     return cudaGetLastError() == cudaSuccess ? FZB_OK : FZB_E_CUDA;
 }
+
+// ---------------------------------------------------------------------------
+// The inverse: a container whose segment sizes only the device knows is cut
+// back into per-segment buffers.  Every CTA parses the header itself (n and
+// the u64 sizes), checks it against the expected count, the destination
+// capacities and the container capacity, and copies its share of every
+// segment with 16-byte words (segments start on 16-byte boundaries).  A bad
+// header sets FZB's malformed bit in *err and copies nothing.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SplitParams {
+    int n;
+    uint8_t* dst[kMaxSeg];
+    uint64_t cap[kMaxSeg];
+    uint64_t in_cap;
+};
+
+constexpr uint32_t kSplitMalformed = 2u;  // the status bit fzb_workspace_status reports as malformed
+
+__global__ void split_kernel(const uint8_t* __restrict__ in, SplitParams p, uint32_t* err) {
+    __shared__ uint64_t s_off[kMaxSeg + 1], s_len[kMaxSeg];
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        const uint32_t n = *reinterpret_cast<const uint32_t*>(in);
+        bool ok = n == (uint32_t)p.n && pad16(4 + 8ull * n) <= p.in_cap;
+        uint64_t off = pad16(4 + 8ull * (uint64_t)p.n);
+        for (int k = 0; ok && k < p.n; k++) {
+            uint64_t len;
+            memcpy(&len, in + 4 + 8 * k, 8);
+            ok = len <= p.cap[k] && off + pad16(len) <= p.in_cap;
+            s_off[k] = off;
+            s_len[k] = len;
+            off += pad16(len);
+        }
+        s_ok = ok;
+        if (!ok && blockIdx.x == 0) atomicOr(err, kSplitMalformed);
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int k = 0; k < p.n; k++) {
+        const uint4* s4 = reinterpret_cast<const uint4*>(in + s_off[k]);
+        uint4* d4 = reinterpret_cast<uint4*>(p.dst[k]);
+        const uint64_t nv = pad16(s_len[k]) / 16;
+        for (uint64_t i = t0; i < nv; i += stride) d4[i] = s4[i];
+    }
+}
+
+}  // namespace
+
+extern "C" int fzb_concat_split(const void* d_in, uint64_t in_capacity, void* const* d_dsts,
+                                const uint64_t* capacities, int n, uint32_t* d_err, void* stream) {
+    if (!d_in || !d_dsts || !capacities || !d_err || n <= 0 || n > kMaxSeg) return FZB_E_INVALID;
+    if (reinterpret_cast<uintptr_t>(d_in) & 15) return FZB_E_INVALID;
+    SplitParams p{};
+    p.n = n;
+    p.in_cap = in_capacity;
+    uint64_t maxcap = 0;
+    for (int i = 0; i < n; i++) {
+        // whole 16-byte words are copied: capacities are multiples of 16
+        if (!d_dsts[i] || (reinterpret_cast<uintptr_t>(d_dsts[i]) & 15) || (capacities[i] & 15))
+            return FZB_E_INVALID;
+        p.dst[i] = static_cast<uint8_t*>(d_dsts[i]);
+        p.cap[i] = capacities[i];
+        if (capacities[i] > maxcap) maxcap = capacities[i];
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    uint64_t blocks = (maxcap / 16 + 255) / 256;
+    if (blocks < 1) blocks = 1;
+    if (blocks > 4ull * (uint64_t)sms) blocks = 4ull * (uint64_t)sms;
+    split_kernel<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const uint8_t*>(d_in), p, d_err);
+    return cudaGetLastError() == cudaSuccess ? FZB_OK : FZB_E_CUDA;
+}

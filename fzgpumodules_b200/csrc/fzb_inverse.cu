@@ -162,51 +162,65 @@ __global__ void __launch_bounds__(kThreads) rze_decode_kernel(InvArgs a) {
     }
 }
 
-// RZE decode + Bitshuffle inverse: one CTA per chunk, codes to a.codes.
+// RZE decode + Bitshuffle inverse: one CTA per chunk (grid-stride over the
+// chunks when the grid is smaller), codes to a.codes.
 __global__ void __launch_bounds__(kThreads) rze_decode_codes_kernel(InvArgs a) {
     extern __shared__ float4 smraw[];
     __shared__ uint32_t s_ws[16];
-    const uint32_t c = blockIdx.x;
+    if (inv_gated_off(a)) return;
     const RzeDecSmem sm = dec_smem(reinterpret_cast<uint8_t*>(smraw), s_ws);
-    uint32_t e;
-    int osz;
-    const uint8_t* src;
-    if (!chunk_src(a, c, &e, &osz, &src)) {
-        if (threadIdx.x == 0) atomicOr(a.err, kErrMalformed);
-        e = 2;
-    }
-    rze_decode_chunk(src, e, osz, sm, a.err);
-    const int t = threadIdx.x;
-    if (osz == kChunkBytes) {
-        uint32_t x[16];
-        if (a.shuffled) {
-#pragma unroll
-            for (int b = 0; b < 16; b++) x[b] = sm.S[(15 - b) * 256 + t];
-            transpose16x2(x);
-            uint32_t rw[16];
-#pragma unroll
-            for (int l = 0; l < 8; l++) rw[l] = __byte_perm(x[2 * l], x[2 * l + 1], 0x5410);
-#pragma unroll
-            for (int l = 8; l < 16; l++) rw[l] = __byte_perm(x[2 * l - 16], x[2 * l - 15], 0x7632);
-#pragma unroll
-            for (int l = 0; l < 16; l++) x[l] = rw[l];
-        } else {
-#pragma unroll
-            for (int l = 0; l < 16; l++) x[l] = sm.S[16 * t + l];
+    for (uint32_t c = blockIdx.x; c < a.n_chunks; c += gridDim.x) {
+        uint32_t e;
+        int osz;
+        const uint8_t* src;
+        if (!chunk_src(a, c, &e, &osz, &src)) {
+            if (threadIdx.x == 0) atomicOr(a.err, kErrMalformed);
+            e = 2;
         }
-        uint4* d4 = reinterpret_cast<uint4*>(a.codes + (size_t)c * kChunkCodes + 32 * t);
+        rze_decode_chunk(src, e, osz, sm, a.err);
+        const int t = threadIdx.x;
+        if (osz == kChunkBytes) {
+            uint32_t x[16];
+            if (a.shuffled) {
 #pragma unroll
-        for (int v = 0; v < 4; v++) d4[v] = make_uint4(x[4 * v], x[4 * v + 1], x[4 * v + 2], x[4 * v + 3]);
-    } else {  // tail block: stored unshuffled
-        uint8_t* dst = reinterpret_cast<uint8_t*>(a.codes) + (size_t)c * kChunkBytes;
-        const uint8_t* Sb = reinterpret_cast<const uint8_t*>(sm.S);
-        for (int i = t; i < osz; i += kThreads) dst[i] = Sb[i];
+                for (int b = 0; b < 16; b++) x[b] = sm.S[(15 - b) * 256 + t];
+                transpose16x2(x);
+                uint32_t rw[16];
+#pragma unroll
+                for (int l = 0; l < 8; l++) rw[l] = __byte_perm(x[2 * l], x[2 * l + 1], 0x5410);
+#pragma unroll
+                for (int l = 8; l < 16; l++) rw[l] = __byte_perm(x[2 * l - 16], x[2 * l - 15], 0x7632);
+#pragma unroll
+                for (int l = 0; l < 16; l++) x[l] = rw[l];
+            } else {
+#pragma unroll
+                for (int l = 0; l < 16; l++) x[l] = sm.S[16 * t + l];
+            }
+            uint4* d4 = reinterpret_cast<uint4*>(a.codes + (size_t)c * kChunkCodes + 32 * t);
+#pragma unroll
+            for (int v = 0; v < 4; v++) d4[v] = make_uint4(x[4 * v], x[4 * v + 1], x[4 * v + 2], x[4 * v + 3]);
+        } else {  // tail block: stored unshuffled
+            uint8_t* dst = reinterpret_cast<uint8_t*>(a.codes) + (size_t)c * kChunkBytes;
+            const uint8_t* Sb = reinterpret_cast<const uint8_t*>(sm.S);
+            for (int i = t; i < osz; i += kThreads) dst[i] = Sb[i];
+        }
+        __syncthreads();  // the shared buffers are reused by the next chunk
     }
+}
+
+// Zeroes the n_total outputs (the exact path's first step; a kernel rather
+// than a memset so that it can be gated).
+__global__ void zero_out_kernel(InvArgs a) {
+    if (inv_gated_off(a)) return;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n_total;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        a.out[i] = 0.0f;
 }
 
 // out must be zeroed; writes each outlier's delta at its index
 // (lorenzo_quant_kernels.cuh:23-40).
 __global__ void scatter_outliers_kernel(InvArgs a) {
+    if (inv_gated_off(a)) return;
     const uint32_t n = min(*a.out_count, a.cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t k = a.out_idx[i];
@@ -223,49 +237,54 @@ __global__ void scatter_outliers_kernel(InvArgs a) {
 // (lorenzo_quant.cu:155-244).
 __global__ void __launch_bounds__(256) lq_inverse_1d_kernel(InvArgs a) {
     __shared__ float s_w[8];
+    if (inv_gated_off(a)) return;
     const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const uint64_t base = (uint64_t)blockIdx.x * 1024 + 4 * t;
-    const float ebx2 = a.ebx2;
+    const float ebx2 = inv_ebx2(a);
     const bool zz = a.zigzag != 0;
-    float v[4];
+    const uint32_t ntiles = (a.nfield + 1023) / 1024;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t base = (uint64_t)tile * 1024 + 4 * t;
+        float v[4];
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const uint64_t g = base + i;
-        v[i] = (g < a.nfield) ? __fadd_rn(a.out[g], decode_code(a.codes[g], zz)) : 0.0f;
-    }
+        for (int i = 0; i < 4; i++) {
+            const uint64_t g = base + i;
+            v[i] = (g < a.nfield) ? __fadd_rn(a.out[g], decode_code(a.codes[g], zz)) : 0.0f;
+        }
 #pragma unroll
-    for (int i = 1; i < 4; i++) v[i] = __fadd_rn(v[i], v[i - 1]);
-    float ts = v[3];
+        for (int i = 1; i < 4; i++) v[i] = __fadd_rn(v[i], v[i - 1]);
+        float ts = v[3];
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        float n = __shfl_up_sync(0xffffffffu, ts, d);
-        if ((int)lane >= d) ts = __fadd_rn(ts, n);
-    }
-    float pre = __shfl_up_sync(0xffffffffu, ts, 1);
-    if (lane > 0) {
+        for (int d = 1; d < 32; d <<= 1) {
+            float n = __shfl_up_sync(0xffffffffu, ts, d);
+            if ((int)lane >= d) ts = __fadd_rn(ts, n);
+        }
+        float pre = __shfl_up_sync(0xffffffffu, ts, 1);
+        if (lane > 0) {
 #pragma unroll
-        for (int i = 0; i < 4; i++) v[i] = __fadd_rn(v[i], pre);
-    }
-    if (lane == 31) s_w[warp] = v[3];
-    __syncthreads();
-    if (warp > 0) {
-        float w[8];
+            for (int i = 0; i < 4; i++) v[i] = __fadd_rn(v[i], pre);
+        }
+        if (lane == 31) s_w[warp] = v[3];
+        __syncthreads();
+        if (warp > 0) {
+            float w[8];
 #pragma unroll
-        for (int i = 0; i < 8; i++) w[i] = s_w[i];
-        // Hillis-Steele over the 8 warp totals, evaluated as a tree
+            for (int i = 0; i < 8; i++) w[i] = s_w[i];
+            // Hillis-Steele over the 8 warp totals, evaluated as a tree
 #pragma unroll
-        for (int d = 1; d < 8; d <<= 1)
+            for (int d = 1; d < 8; d <<= 1)
 #pragma unroll
-            for (int i = 7; i >= 1; i--)
-                if (i >= d) w[i] = __fadd_rn(w[i], w[i - d]);
-        const float add = w[warp - 1];
+                for (int i = 7; i >= 1; i--)
+                    if (i >= d) w[i] = __fadd_rn(w[i], w[i - d]);
+            const float add = w[warp - 1];
 #pragma unroll
-        for (int i = 0; i < 4; i++) v[i] = __fadd_rn(v[i], add);
-    }
+            for (int i = 0; i < 4; i++) v[i] = __fadd_rn(v[i], add);
+        }
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const uint64_t g = base + i;
-        if (g < a.nfield) a.out[g] = __fmul_rn(v[i], ebx2);
+        for (int i = 0; i < 4; i++) {
+            const uint64_t g = base + i;
+            if (g < a.nfield) a.out[g] = __fmul_rn(v[i], ebx2);
+        }
+        __syncthreads();  // s_w is rewritten by the next tile
     }
 }
 
@@ -273,43 +292,48 @@ __global__ void __launch_bounds__(256) lq_inverse_1d_kernel(InvArgs a) {
 // (lorenzo_quant_nd.cu:112-190).
 __global__ void __launch_bounds__(128) lq_inverse_2d_kernel(InvArgs a) {
     __shared__ float s_tot[4][32];
+    if (inv_gated_off(a)) return;
     const uint32_t lx = threadIdx.x & 31, wy = threadIdx.x >> 5;
-    const uint32_t gx = blockIdx.x * 32 + lx, gy0 = blockIdx.y * 32 + wy * 8;
-    const float ebx2 = a.ebx2;
+    const float ebx2 = inv_ebx2(a);
     const bool zz = a.zigzag != 0;
-    float v[8];
+    const uint32_t tx = (a.nx + 31) / 32, ntiles = tx * ((a.ny + 31) / 32);
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t gx = (tile % tx) * 32 + lx, gy0 = (tile / tx) * 32 + wy * 8;
+        float v[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        const uint32_t gy = gy0 + i;
-        v[i] = 0.0f;
-        if (gx < a.nx && gy < a.ny) {
-            const uint64_t g = (uint64_t)gy * a.nx + gx;
-            v[i] = __fadd_rn(a.out[g], decode_code(a.codes[g], zz));
+        for (int i = 0; i < 8; i++) {
+            const uint32_t gy = gy0 + i;
+            v[i] = 0.0f;
+            if (gx < a.nx && gy < a.ny) {
+                const uint64_t g = (uint64_t)gy * a.nx + gx;
+                v[i] = __fadd_rn(a.out[g], decode_code(a.codes[g], zz));
+            }
         }
-    }
 #pragma unroll
-    for (int i = 1; i < 8; i++) v[i] = __fadd_rn(v[i], v[i - 1]);
-    s_tot[wy][lx] = v[7];
-    __syncthreads();
-    if (wy > 0) {
-        const float t0 = s_tot[0][lx];
-        const float t1 = __fadd_rn(t0, s_tot[1][lx]);
-        const float add = (wy == 1) ? t0 : (wy == 2) ? t1 : __fadd_rn(t1, s_tot[2][lx]);
+        for (int i = 1; i < 8; i++) v[i] = __fadd_rn(v[i], v[i - 1]);
+        s_tot[wy][lx] = v[7];
+        __syncthreads();
+        if (wy > 0) {
+            const float t0 = s_tot[0][lx];
+            const float t1 = __fadd_rn(t0, s_tot[1][lx]);
+            const float add = (wy == 1) ? t0 : (wy == 2) ? t1 : __fadd_rn(t1, s_tot[2][lx]);
 #pragma unroll
-        for (int i = 0; i < 8; i++) v[i] = __fadd_rn(v[i], add);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            float n = __shfl_up_sync(0xffffffffu, v[i], d);
-            if ((int)lx >= d) v[i] = __fadd_rn(v[i], n);
+            for (int i = 0; i < 8; i++) v[i] = __fadd_rn(v[i], add);
         }
-    }
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        const uint32_t gy = gy0 + i;
-        if (gx < a.nx && gy < a.ny) a.out[(uint64_t)gy * a.nx + gx] = __fmul_rn(v[i], ebx2);
+        for (int i = 0; i < 8; i++) {
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                float n = __shfl_up_sync(0xffffffffu, v[i], d);
+                if ((int)lx >= d) v[i] = __fadd_rn(v[i], n);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const uint32_t gy = gy0 + i;
+            if (gx < a.nx && gy < a.ny) a.out[(uint64_t)gy * a.nx + gx] = __fmul_rn(v[i], ebx2);
+        }
+        __syncthreads();  // s_tot is rewritten by the next tile
     }
 }
 
@@ -318,48 +342,54 @@ __global__ void __launch_bounds__(128) lq_inverse_2d_kernel(InvArgs a) {
 // z Hillis-Steele tree in registers (lorenzo_quant_nd.cu:281-364).
 __global__ void __launch_bounds__(256) lq_inverse_3d_kernel(InvArgs a) {
     __shared__ float V[8][8][33];  // [z][y][x]
+    if (inv_gated_off(a)) return;
     const uint32_t lx = threadIdx.x & 31, lz = threadIdx.x >> 5;
-    const uint32_t gx = blockIdx.x * 32 + lx, gy0 = blockIdx.y * 8, gz = blockIdx.z * 8 + lz;
-    const float ebx2 = a.ebx2;
+    const float ebx2 = inv_ebx2(a);
     const bool zz = a.zigzag != 0;
-    float v[8];
+    const uint32_t tx = (a.nx + 31) / 32, ty = (a.ny + 7) / 8, ntiles = tx * ty * ((a.nz + 7) / 8);
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t bx = tile % tx, by = (tile / tx) % ty, bz = tile / (tx * ty);
+        const uint32_t gx = bx * 32 + lx, gy0 = by * 8, gz = bz * 8 + lz;
+        float v[8];
 #pragma unroll
-    for (int y = 0; y < 8; y++) {
-        v[y] = 0.0f;
-        const uint32_t gy = gy0 + y;
-        if (gx < a.nx && gy < a.ny && gz < a.nz) {
-            const uint64_t g = ((uint64_t)gz * a.ny + gy) * a.nx + gx;
-            v[y] = __fadd_rn(a.out[g], decode_code(a.codes[g], zz));
+        for (int y = 0; y < 8; y++) {
+            v[y] = 0.0f;
+            const uint32_t gy = gy0 + y;
+            if (gx < a.nx && gy < a.ny && gz < a.nz) {
+                const uint64_t g = ((uint64_t)gz * a.ny + gy) * a.nx + gx;
+                v[y] = __fadd_rn(a.out[g], decode_code(a.codes[g], zz));
+            }
         }
-    }
 #pragma unroll
-    for (int y = 1; y < 8; y++) v[y] = __fadd_rn(v[y], v[y - 1]);
-    const uint32_t tx = lx & 7;
+        for (int y = 1; y < 8; y++) v[y] = __fadd_rn(v[y], v[y - 1]);
+        const uint32_t sx = lx & 7;
 #pragma unroll
-    for (int y = 0; y < 8; y++) {
+        for (int y = 0; y < 8; y++) {
 #pragma unroll
-        for (int d = 1; d < 8; d <<= 1) {
-            float n = __shfl_up_sync(0xffffffffu, v[y], d, 8);
-            if ((int)tx >= d) v[y] = __fadd_rn(v[y], n);
+            for (int d = 1; d < 8; d <<= 1) {
+                float n = __shfl_up_sync(0xffffffffu, v[y], d, 8);
+                if ((int)sx >= d) v[y] = __fadd_rn(v[y], n);
+            }
+            V[lz][y][lx] = v[y];
         }
-        V[lz][y][lx] = v[y];
-    }
-    __syncthreads();
-    const uint32_t ly = lz;  // second phase: thread (x, y)
-    float w[8];
+        __syncthreads();
+        const uint32_t ly = lz;  // second phase: thread (x, y)
+        float w[8];
 #pragma unroll
-    for (int z = 0; z < 8; z++) w[z] = V[z][ly][lx];
+        for (int z = 0; z < 8; z++) w[z] = V[z][ly][lx];
 #pragma unroll
-    for (int d = 1; d < 8; d <<= 1)
+        for (int d = 1; d < 8; d <<= 1)
 #pragma unroll
-        for (int z = 7; z >= 1; z--)
-            if (z >= d) w[z] = __fadd_rn(w[z], w[z - d]);
-    const uint32_t gy = gy0 + ly;
+            for (int z = 7; z >= 1; z--)
+                if (z >= d) w[z] = __fadd_rn(w[z], w[z - d]);
+        const uint32_t gy = gy0 + ly;
 #pragma unroll
-    for (int z = 0; z < 8; z++) {
-        const uint32_t gzz = blockIdx.z * 8 + z;
-        if (gx < a.nx && gy < a.ny && gzz < a.nz)
-            a.out[((uint64_t)gzz * a.ny + gy) * a.nx + gx] = __fmul_rn(w[z], ebx2);
+        for (int z = 0; z < 8; z++) {
+            const uint32_t gzz = bz * 8 + z;
+            if (gx < a.nx && gy < a.ny && gzz < a.nz)
+                a.out[((uint64_t)gzz * a.ny + gy) * a.nx + gx] = __fmul_rn(w[z], ebx2);
+        }
+        __syncthreads();  // V is rewritten by the next brick
     }
 }
 
@@ -390,7 +420,7 @@ __global__ void __launch_bounds__(kThreads, 2) fused_inverse_3d_kernel(InvArgs a
     const uint32_t nx = a.nx, R = kChunkCodes / nx, slabs = a.ny / R;
     const uint32_t s = blockIdx.x, zt = blockIdx.y;
     const uint32_t lognx = 31 - __clz(nx);
-    const float ebx2 = a.ebx2;
+    const float ebx2 = inv_ebx2(a);
     const bool zz = a.zigzag != 0;
     const uint32_t nout = min(*a.out_count, a.cap);
 

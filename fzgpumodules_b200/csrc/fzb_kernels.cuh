@@ -119,7 +119,23 @@ struct InvArgs {
     int shuffled;                 // full chunks are bitshuffled (ew = 2)
     float* out;
     uint32_t* err;
+    // device-resident error bound: when set, kernels take 2 * *abs_eb_src
+    // (the compressor's eb state) instead of ebx2
+    const float* abs_eb_src;
+    // device-side fallback: when set, a kernel does its work only if
+    // *gate & gate_mask (the fused inverse flagged a case it leaves to the
+    // exact kernels), so the decision needs no host round trip
+    const uint32_t* gate;
+    uint32_t gate_mask;
 };
+
+__device__ __forceinline__ float inv_ebx2(const InvArgs& a) {
+    return a.abs_eb_src ? 2.0f * *a.abs_eb_src : a.ebx2;
+}
+
+__device__ __forceinline__ bool inv_gated_off(const InvArgs& a) {
+    return a.gate != nullptr && !(*reinterpret_cast<const volatile uint32_t*>(a.gate) & a.gate_mask);
+}
 
 __global__ void minmax_kernel(const float* x, uint64_t n, float* pmin, float* pmax,
                               unsigned int* done, int mode, float user_eb, float* st);
@@ -162,6 +178,7 @@ __global__ void outlier_ranges_kernel(const uint32_t* idx, const uint32_t* count
 __global__ void rze_decode_kernel(InvArgs a);
 __global__ void rze_decode_codes_kernel(InvArgs a);
 __global__ void scatter_outliers_kernel(InvArgs a);
+__global__ void zero_out_kernel(InvArgs a);
 __global__ void lq_inverse_1d_kernel(InvArgs a);
 __global__ void lq_inverse_2d_kernel(InvArgs a);
 __global__ void lq_inverse_3d_kernel(InvArgs a);

@@ -20,7 +20,10 @@
 //     them;
 //   * the first call on each device resolves the array's device address
 //     (cudaGetSymbolAddress with that device current) and caches it; make
-//     that first call before any stream capture begins.
+//     that first call before any stream capture begins;
+//   * the cached address belongs to the device's context: it does not
+//     survive cudaDeviceReset, after which this entry point must not be
+//     called again in the same process.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -82,9 +85,8 @@ extern "C" int fzb_rze_encode_noalloc(const void* d_in, uint64_t bytes, void* d_
     a.slots = scratch;
     a.sizes = reinterpret_cast<uint32_t*>(scratch + kSizesOff);
     const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32;
-    if (cudaFuncSetAttribute(rze_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-        cudaSuccess)
-        return FZB_E_CUDA;
+    static SmemAttr attr;  // the shared-memory attribute, set once per device
+    if (ensure_dyn_smem(attr, (const void*)rze_encode_kernel, smem) != cudaSuccess) return FZB_E_CUDA;
     rze_encode_kernel<<<nch, kThreads, smem, s>>>(a);
     if (cudaGetLastError() != cudaSuccess) return FZB_E_CUDA;
     AsmArgs m{};

@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(kThreads, kInvCtasPerSm) lq3d_inv_slab_kernel(
     const uint32_t full = 0xffffffffu;
     const uint32_t nx = a.nx, R = kChunkCodes / nx, S = nx / 32, G = gridDim.x;
     const uint32_t xq = nx / 4, band = t / xq, x4 = t % xq;  // column strip of this thread
-    const float ebx2 = a.ebx2;
+    const float ebx2 = inv_ebx2(a);
     const uint32_t nout = min(*a.out_count, a.cap);
     bool inexact = false, malformed = false;
 

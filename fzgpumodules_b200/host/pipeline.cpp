@@ -242,13 +242,17 @@ void CompressionDAG::preallocate(cudaStream_t stream) {
 // ================================================================== Pipeline
 
 Pipeline::Pipeline(size_t input_data_size, MemoryStrategy strategy, float pool_multiplier)
-    : strategy_(strategy), input_size_hint_(input_data_size) {
+    : strategy_(strategy), pool_multiplier_(pool_multiplier), input_size_hint_(input_data_size) {
     pool_.reset(new MemoryPool(MemoryPoolConfig(input_data_size, pool_multiplier)));
     dag_.reset(new CompressionDAG(pool_.get(), strategy));
 }
 
 Pipeline::~Pipeline() {
     cudaDeviceSynchronize();
+    releaseDecompressGraph();
+    for (cudaEvent_t e : fork_events_) cudaEventDestroy(e);
+    for (cudaEvent_t e : join_events_) cudaEventDestroy(e);
+    for (cudaStream_t st : side_streams_) cudaStreamDestroy(st);
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (graph_) cudaGraphDestroy(graph_);
     for (void* p : decomp_outputs_) pool_->free(p, 0);
@@ -279,6 +283,11 @@ void Pipeline::setMemoryStrategy(MemoryStrategy strategy) {
     }
     connections_.clear();
     for (const auto& c : conns) connect(c.dependent, c.producer, c.output_name);
+}
+
+void Pipeline::setNumStreams(int num_streams) {
+    if (finalized_) throw std::runtime_error("Cannot configure streams after finalization");
+    num_streams_ = num_streams;
 }
 
 void Pipeline::enableGraphMode(bool enable) {
@@ -391,6 +400,31 @@ void Pipeline::finalize() {
             const size_t inlen = n->input_buffer_ids.empty() ? 0 : dag_->getBufferSize(n->input_buffer_ids[0]);
             n->stage->onFinalize(inlen, pool_.get());
         }
+    {   // side streams for levels with several stages (dag.cpp:262-285, 343-369)
+        size_t widest = 1;
+        for (const auto& lv : dag_->getLevels()) widest = std::max(widest, lv.size());
+        const int ns = std::max<int>(num_streams_, (int)widest);
+        if (ns > 1 && widest > 1) {
+            for (int i = 0; i < ns; i++) {
+                cudaStream_t st = nullptr;
+                cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "Failed to create CUDA stream");
+                side_streams_.push_back(st);
+            }
+            for (size_t i = 0; i < dag_->getLevels().size(); i++) {
+                cudaEvent_t e = nullptr;
+                cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "level fork event");
+                fork_events_.push_back(e);
+            }
+            for (size_t i = 0; i < dag_->getNodes().size(); i++) {
+                cudaEvent_t e = nullptr;
+                cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "stage join event");
+                join_events_.push_back(e);
+            }
+        }
+        // the count the pipeline reports (and saveConfig writes) is the
+        // reference's: the requested count, or the widest level when larger
+        num_streams_ = ns > 1 ? ns : 1;
+    }
     d_fused_size_ = static_cast<uint64_t*>(pool_->allocate(256, 0, "fused_stream_size", true));
     if (strategy_ == MemoryStrategy::PREALLOCATE && input_size_hint_) dag_->preallocate(0);
     if (graph_mode_) {
@@ -494,89 +528,140 @@ const void* Pipeline::prepareInput(const void* d_input, size_t input_size, cudaS
     return d_input;
 }
 
-// Runs every node level by level on `stream`.  Input sizes come from the
-// producer's execute-time size (or the propagated estimate when that is 0),
-// as in the reference DAG (dag.cpp:382-510).
+// Runs every node level by level, as the reference DAG does
+// (dag.cpp:382-510).  Input sizes come from the producer's execute-time size
+// (or the propagated estimate when that is 0).  A level with several stages
+// forks from `stream` onto the side streams and joins back before the next
+// level; everything else runs on `stream`.
 void Pipeline::runForward(cudaStream_t stream) {
     std::unordered_map<int, int> remaining;
     for (auto* n : dag_->getNodes())
         for (int id : n->input_buffer_ids) remaining[id]++;
     std::vector<bool> skip(dag_->getNodes().size(), false);
-    DAGNode *dfn = nullptr, *bsn = nullptr, *rzn = nullptr;
     if (fused_) {
         const BufferInfo& cb = dag_->getBufferInfo(input_node_->output_index_to_buffer_id.at(0));
-        bsn = dag_->getNodes()[cb.consumer_stage_ids[0]];
+        DAGNode* bsn = dag_->getNodes()[cb.consumer_stage_ids[0]];
+        if (fused_pfpl_) {
+            skip[bsn->id] = true;
+            bsn = dag_->getNodes()[dag_->getBufferInfo(bsn->output_buffer_ids[0]).consumer_stage_ids[0]];
+        }
+        DAGNode* rzn = dag_->getNodes()[dag_->getBufferInfo(bsn->output_buffer_ids[0]).consumer_stage_ids[0]];
+        skip[bsn->id] = skip[rzn->id] = true;
+    }
+    const auto& levels = dag_->getLevels();
+    for (size_t lv = 0; lv < levels.size(); lv++) {
+        std::vector<DAGNode*> run;
+        for (auto* n : levels[lv])
+            if (!skip[n->id]) run.push_back(n);
+        if (run.size() > 1 && !side_streams_.empty()) {
+            // outputs are reserved on the caller's stream before the fork
+            for (auto* n : run)
+                for (int id : n->output_buffer_ids) dag_->allocate(id, stream);
+            cuda_check(cudaEventRecord(fork_events_[lv], stream), "level fork");
+            for (size_t k = 0; k < run.size(); k++) {
+                cudaStream_t s = side_streams_[k % side_streams_.size()];
+                cuda_check(cudaStreamWaitEvent(s, fork_events_[lv], 0), "level fork");
+                runNode(run[k], s);
+                cuda_check(cudaEventRecord(join_events_[run[k]->id], s), "level join");
+            }
+            for (auto* n : run) cuda_check(cudaStreamWaitEvent(stream, join_events_[n->id], 0), "level join");
+        } else {
+            for (auto* n : run) runNode(n, stream);
+        }
+        if (strategy_ == MemoryStrategy::MINIMAL)
+            for (auto* n : run)
+                for (int id : n->input_buffer_ids)
+                    if (--remaining[id] == 0 && !dag_->getBufferInfo(id).is_persistent) dag_->release(id, stream);
+    }
+}
+
+// One stage on `stream`: the fused chain when `n` starts it, else the
+// stage's own execute(); then the sizes its consumers see.
+void Pipeline::runNode(DAGNode* n, cudaStream_t stream) {
+    std::vector<void*> in, out;
+    std::vector<size_t> sizes;
+    for (int id : n->input_buffer_ids) {
+        const BufferInfo& b = dag_->getBufferInfo(id);
+        in.push_back(b.d_ptr);
+        sizes.push_back(b.size);
+    }
+    if (profiling_enabled_) {
+        if (!n->start_event) cudaEventCreate(&n->start_event);
+        if (!n->end_event) cudaEventCreate(&n->end_event);
+        cudaEventRecord(n->start_event, stream);
+    }
+    if (fused_ && n == input_node_) {
+        const BufferInfo& cb = dag_->getBufferInfo(n->output_index_to_buffer_id.at(0));
+        DAGNode* bsn = dag_->getNodes()[cb.consumer_stage_ids[0]];
+        DAGNode* dfn = nullptr;
         if (fused_pfpl_) {
             dfn = bsn;
             bsn = dag_->getNodes()[dag_->getBufferInfo(dfn->output_buffer_ids[0]).consumer_stage_ids[0]];
-            skip[dfn->id] = true;
         }
-        rzn = dag_->getNodes()[dag_->getBufferInfo(bsn->output_buffer_ids[0]).consumer_stage_ids[0]];
-        skip[bsn->id] = skip[rzn->id] = true;
+        DAGNode* rzn = dag_->getNodes()[dag_->getBufferInfo(bsn->output_buffer_ids[0]).consumer_stage_ids[0]];
+        for (int i = 1; i < 4; i++) dag_->allocate(n->output_buffer_ids[i], stream);
+        const int rz_out = rzn->output_buffer_ids[0];
+        dag_->allocate(rz_out, stream);
+        size_t code_bytes;
+        if (fused_pfpl_) {
+            auto* qs = static_cast<QuantizerStage<float, uint32_t>*>(n->stage);
+            qs->fusedForward(stream, pool_.get(), in[0], sizes[0], dag_->getBuffer(n->output_buffer_ids[1]),
+                             dag_->getBuffer(n->output_buffer_ids[2]), dag_->getBuffer(n->output_buffer_ids[3]),
+                             dag_->getBuffer(rz_out), d_fused_size_);
+            code_bytes = sizes[0];  // one uint32 code per float
+            static_cast<DifferenceStage<int32_t, uint32_t>*>(dfn->stage)->markFused(code_bytes);
+        } else {
+            auto* lq = static_cast<LorenzoQuantStage<float, uint16_t>*>(n->stage);
+            lq->fusedForward(stream, pool_.get(), in[0], sizes[0], dag_->getBuffer(n->output_buffer_ids[1]),
+                             dag_->getBuffer(n->output_buffer_ids[2]), dag_->getBuffer(n->output_buffer_ids[3]),
+                             dag_->getBuffer(rz_out), d_fused_size_);
+            code_bytes = sizes[0] / sizeof(float) * sizeof(uint16_t);
+        }
+        static_cast<BitshuffleStage*>(bsn->stage)->markFused(code_bytes);
+        static_cast<RZEStage*>(rzn->stage)->markFused(code_bytes, d_fused_size_, stream);
+        for (int i = 1; i < 4; i++) {
+            const size_t sz = n->stage->getExecuteTimeOutputSize(i);
+            if (sz) dag_->buffer(n->output_buffer_ids[i]).size = sz;
+        }
+        if (profiling_enabled_) cudaEventRecord(n->end_event, stream);
+        if (bounds_check_) {
+            checkBounds(n);
+            checkBounds(rzn);
+        }
+        return;
     }
-    for (const auto& lv : dag_->getLevels())
-        for (auto* n : lv) {
-            if (skip[n->id]) continue;
-            std::vector<void*> in, out;
-            std::vector<size_t> sizes;
-            for (int id : n->input_buffer_ids) {
-                const BufferInfo& b = dag_->getBufferInfo(id);
-                in.push_back(b.d_ptr);
-                sizes.push_back(b.size);
-            }
-            if (profiling_enabled_) {
-                if (!n->start_event) cudaEventCreate(&n->start_event);
-                if (!n->end_event) cudaEventCreate(&n->end_event);
-                cudaEventRecord(n->start_event, stream);
-            }
-            if (fused_ && n == input_node_) {
-                for (int i = 1; i < 4; i++) dag_->allocate(n->output_buffer_ids[i], stream);
-                const int rz_out = rzn->output_buffer_ids[0];
-                dag_->allocate(rz_out, stream);
-                size_t code_bytes;
-                if (fused_pfpl_) {
-                    auto* qs = static_cast<QuantizerStage<float, uint32_t>*>(n->stage);
-                    qs->fusedForward(stream, pool_.get(), in[0], sizes[0], dag_->getBuffer(n->output_buffer_ids[1]),
-                                     dag_->getBuffer(n->output_buffer_ids[2]),
-                                     dag_->getBuffer(n->output_buffer_ids[3]), dag_->getBuffer(rz_out),
-                                     d_fused_size_);
-                    code_bytes = sizes[0];  // one uint32 code per float
-                    static_cast<DifferenceStage<int32_t, uint32_t>*>(dfn->stage)->markFused(code_bytes);
-                } else {
-                    auto* lq = static_cast<LorenzoQuantStage<float, uint16_t>*>(n->stage);
-                    lq->fusedForward(stream, pool_.get(), in[0], sizes[0], dag_->getBuffer(n->output_buffer_ids[1]),
-                                     dag_->getBuffer(n->output_buffer_ids[2]),
-                                     dag_->getBuffer(n->output_buffer_ids[3]), dag_->getBuffer(rz_out),
-                                     d_fused_size_);
-                    code_bytes = sizes[0] / sizeof(float) * sizeof(uint16_t);
-                }
-                static_cast<BitshuffleStage*>(bsn->stage)->markFused(code_bytes);
-                static_cast<RZEStage*>(rzn->stage)->markFused(code_bytes, d_fused_size_, stream);
-                for (int i = 1; i < 4; i++) {
-                    const size_t s = n->stage->getExecuteTimeOutputSize(i);
-                    if (s) dag_->buffer(n->output_buffer_ids[i]).size = s;
-                }
-                if (profiling_enabled_) cudaEventRecord(n->end_event, stream);
-                continue;
-            }
-            for (int id : n->output_buffer_ids) {
-                dag_->allocate(id, stream);
-                out.push_back(dag_->getBuffer(id));
-            }
-            n->stage->execute(stream, pool_.get(), in, out, sizes);
-            if (profiling_enabled_) cudaEventRecord(n->end_event, stream);
-            // sizes downstream stages see; sinks are read after the sync
-            for (size_t k = 0; k < n->output_buffer_ids.size(); k++) {
-                BufferInfo& b = dag_->buffer(n->output_buffer_ids[k]);
-                if (b.consumer_stage_ids.empty()) continue;
-                const size_t s = n->stage->getExecuteTimeOutputSize((int)k);
-                if (s) b.size = s;
-            }
-            for (int id : n->input_buffer_ids)
-                if (--remaining[id] == 0 && !dag_->getBufferInfo(id).is_persistent &&
-                    strategy_ == MemoryStrategy::MINIMAL)
-                    dag_->release(id, stream);
-        }
+    for (int id : n->output_buffer_ids) {
+        dag_->allocate(id, stream);
+        out.push_back(dag_->getBuffer(id));
+    }
+    n->stage->execute(stream, pool_.get(), in, out, sizes);
+    if (profiling_enabled_) cudaEventRecord(n->end_event, stream);
+    // sizes downstream stages see; sinks are read after the sync
+    for (size_t k = 0; k < n->output_buffer_ids.size(); k++) {
+        BufferInfo& b = dag_->buffer(n->output_buffer_ids[k]);
+        if (b.consumer_stage_ids.empty()) continue;
+        const size_t sz = n->stage->getExecuteTimeOutputSize((int)k);
+        if (sz) b.size = sz;
+    }
+    if (bounds_check_) checkBounds(n);
+}
+
+// The bounds check of dag.cpp:438-462: each output's actual size (read back,
+// which synchronises) against the bytes reserved for it.  Skipped while the
+// stream is being captured into a graph.
+void Pipeline::checkBounds(DAGNode* n) {
+    if (capturing_) return;
+    const auto names = n->stage->getOutputNames();
+    for (size_t k = 0; k < n->output_buffer_ids.size(); k++) {
+        const BufferInfo& b = dag_->getBufferInfo(n->output_buffer_ids[k]);
+        if (b.allocated_size == 0) continue;
+        const size_t sz = n->stage->getActualOutputSize((int)k);
+        if (sz > b.allocated_size)
+            throw std::runtime_error("Buffer overwrite detected: stage '" + n->name + "' output '" +
+                                     (k < names.size() ? names[k] : std::to_string(k)) + "' wrote " +
+                                     std::to_string(sz) + " bytes into a " + std::to_string(b.allocated_size) +
+                                     "-byte buffer");
+    }
 }
 
 void Pipeline::collectMetadata() {
@@ -769,18 +854,22 @@ void Pipeline::captureGraph(cudaStream_t stream) {
     const bool prof = profiling_enabled_;
     profiling_enabled_ = false;
     cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    capturing_ = true;
     try {
         runForward(stream);
     } catch (...) {
+        capturing_ = false;
         cudaGraph_t g = nullptr;
         cudaStreamEndCapture(stream, &g);
         if (g) cudaGraphDestroy(g);
         profiling_enabled_ = prof;
         throw;
     }
+    capturing_ = false;
     profiling_enabled_ = prof;
     cuda_check(cudaStreamEndCapture(stream, &graph_), "end capture");
     cuda_check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
+    captureDecompress(stream);
 }
 
 std::vector<Pipeline::OutputBuffer> Pipeline::getOutputBuffers() const {

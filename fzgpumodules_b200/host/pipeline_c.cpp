@@ -280,6 +280,27 @@ int fzb_pipeline_set_fusion(void* p, int on) {
     });
 }
 
+int fzb_pipeline_set_num_streams(void* p, int num_streams) {
+    if (!p) return FZB_E_INVALID;
+    return guarded([&] {
+        H(p)->p->setNumStreams(num_streams);
+        return FZB_OK;
+    });
+}
+
+int fzb_pipeline_num_streams(void* p) {
+    if (!p) return FZB_E_INVALID;
+    return H(p)->p->getNumStreams();
+}
+
+int fzb_pipeline_enable_bounds_check(void* p, int on) {
+    if (!p) return FZB_E_INVALID;
+    return guarded([&] {
+        H(p)->p->enableBoundsCheck(on != 0);
+        return FZB_OK;
+    });
+}
+
 int fzb_pipeline_enable_graph_mode(void* p, int on) {
     if (!p) return FZB_E_INVALID;
     return guarded([&] {
@@ -310,6 +331,19 @@ int fzb_pipeline_capture_graph(void* p, void* stream) {
     if (!p) return FZB_E_INVALID;
     return guarded([&] {
         H(p)->p->captureGraph(static_cast<cudaStream_t>(stream));
+        return FZB_OK;
+    });
+}
+
+int fzb_pipeline_decompress_graph_captured(void* p) {
+    if (!p) return FZB_E_INVALID;
+    return H(p)->p->isDecompressGraphCaptured() ? 1 : 0;
+}
+
+int fzb_pipeline_check_decompress(void* p, void* stream) {
+    if (!p) return FZB_E_INVALID;
+    return guarded([&] {
+        H(p)->p->checkDecompressStatus(static_cast<cudaStream_t>(stream));
         return FZB_OK;
     });
 }

@@ -271,6 +271,38 @@ void Pipeline::decompress(const void* d_input, size_t input_size, void** d_outpu
         throw std::runtime_error("decompress(): input (" + std::to_string(input_size) +
                                  " bytes) is shorter than the compressed layout (" + std::to_string(off) + " bytes)");
     const size_t cap = input_size_;  // the source bytes (padded)
+    if (decomp_exec_) {  // replay the captured decompression: no host wait
+        const auto t0 = std::chrono::steady_clock::now();
+        const void* src = d_input;
+        size_t bytes = input_size;
+        if (!src) {
+            src = concat_buf_;
+            bytes = concatSize();
+        }
+        if (!src || bytes > decomp_in_bytes_)
+            throw std::runtime_error("decompress(): the container (" + std::to_string(bytes) +
+                                     " bytes) does not fit the decompression graph's slot (" +
+                                     std::to_string(decomp_in_bytes_) + " bytes)");
+        cuda_check(cudaMemcpyAsync(decomp_in_, src, bytes, cudaMemcpyDeviceToDevice, stream), "decompress input");
+        cuda_check(cudaGraphLaunch(decomp_exec_, stream), "decompress graph launch");
+        const size_t out = (original_input_size_ && original_input_size_ < cap) ? original_input_size_ : cap;
+        if (pool_managed_decomp_) {
+            *d_output = decomp_out_;
+        } else {
+            void* p = nullptr;
+            cuda_check(cudaMalloc(&p, out), "cudaMalloc for decompress output");
+            cuda_check(cudaMemcpyAsync(p, decomp_out_, out, cudaMemcpyDeviceToDevice, stream), "decompress copy-out");
+            *d_output = p;
+        }
+        *output_size = out;
+        last_perf_ = PipelinePerfResult();
+        last_perf_.is_compress = false;
+        last_perf_.input_bytes = bytes;
+        last_perf_.output_bytes = out;
+        last_perf_.host_elapsed_ms = last_perf_.dag_elapsed_ms =
+            std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return;
+    }
     void* d_final = nullptr;
     if (pool_managed_decomp_) {
         for (void* p : decomp_outputs_) pool_->free(p, stream);
@@ -310,7 +342,24 @@ void Pipeline::decompress(const void* d_input, size_t input_size, void* d_output
         }
         outs[m.buffer_id] = {p, m.actual_size};
     }
-    (void)input_size;
+    if (decomp_exec_) {
+        void* p = nullptr;
+        size_t sz = 0;
+        const bool managed = pool_managed_decomp_;
+        pool_managed_decomp_ = true;
+        try {
+            decompress(d_input, input_size, &p, &sz, stream);
+        } catch (...) {
+            pool_managed_decomp_ = managed;
+            throw;
+        }
+        pool_managed_decomp_ = managed;
+        if (sz > output_buf_capacity)
+            throw std::runtime_error("decompress(): output (" + std::to_string(sz) + " bytes) exceeds the buffer capacity");
+        cuda_check(cudaMemcpyAsync(d_output_buf, p, sz, cudaMemcpyDeviceToDevice, stream), "decompress copy-out");
+        *actual_output_size = sz;
+        return;
+    }
     if (output_buf_capacity >= input_size_) {
         runInverse(outs, d_output_buf, output_buf_capacity, actual_output_size, stream);
         return;
@@ -332,6 +381,215 @@ void Pipeline::decompress(const void* d_input, size_t input_size, void* d_output
     cuda_check(cudaMemcpyAsync(d_output_buf, tmp, sz, cudaMemcpyDeviceToDevice, stream), "decompress copy-out");
     pool_->free(tmp, stream);
     *actual_output_size = sz;
+}
+
+// --------------------------------------------------------- captured decompress
+
+namespace {
+
+// Stages whose inverse takes every size from the device or from values fixed
+// at capture time (element counts, capacities).
+bool inverse_on_device(Stage* s) {
+    switch ((StageType)s->getStageTypeId()) {
+        case StageType::LORENZO_QUANT:
+        case StageType::BITSHUFFLE:
+        case StageType::RZE:
+        case StageType::RLE:
+        case StageType::HUFFMAN:
+            return true;
+        case StageType::BITPACK:
+            return s->isGraphCompatible();  // a fixed bit width
+        default:
+            return false;
+    }
+}
+
+}  // namespace
+
+void Pipeline::releaseDecompressGraph() {
+    if (decomp_exec_) cudaGraphExecDestroy(decomp_exec_);
+    if (decomp_graph_) cudaGraphDestroy(decomp_graph_);
+    decomp_exec_ = nullptr;
+    decomp_graph_ = nullptr;
+    for (void* p : decomp_temps_) pool_->free(p, 0);
+    decomp_temps_.clear();
+    for (void** p : {&decomp_in_, &decomp_out_, &decomp_work_})
+        if (*p) {
+            pool_->free(*p, 0);
+            *p = nullptr;
+        }
+    decomp_in_bytes_ = decomp_work_bytes_ = 0;
+}
+
+// What the decompression graph runs: the container in decomp_in_ is split on
+// the device into the DAG's own output buffers, then the chain is inverted
+// into decomp_out_ -- the fused LorenzoQuant <- Bitshuffle <- RZE pass, or
+// stage by stage into intermediates kept from the first (uncaptured) pass.
+// Sizes passed to the stages are capacities; the kernels read the actual
+// sizes from the segments' own headers and counts.
+void Pipeline::enqueueGraphInverse(cudaStream_t stream) {
+    std::vector<void*> dsts;
+    std::vector<uint64_t> caps;
+    for (int id : output_buffer_ids_) {
+        const BufferInfo& b = dag_->getBufferInfo(id);
+        dsts.push_back(b.d_ptr);
+        caps.push_back(b.allocated_size);
+    }
+    uint32_t* status = static_cast<uint32_t*>(decomp_work_);
+    cuda_check(cudaMemsetAsync(status, 0, 256, stream), "decompress status");
+    int rc = fzb_concat_split(decomp_in_, decomp_in_bytes_, dsts.data(), caps.data(), (int)dsts.size(), status,
+                              stream);
+    if (rc) throw std::runtime_error(std::string("decompress container split: ") + fzb_status_string(rc));
+    auto consumer = [&](int buf) { return dag_->getNodes()[dag_->getBufferInfo(buf).consumer_stage_ids[0]]; };
+    if (decomp_fused_) {
+        auto* lq = static_cast<LorenzoQuantStage<float, uint16_t>*>(input_node_->stage);
+        DAGNode* bsn = consumer(input_node_->output_index_to_buffer_id.at(0));
+        DAGNode* rzn = consumer(bsn->output_buffer_ids[0]);
+        auto* rz = static_cast<RZEStage*>(rzn->stage);
+        const size_t n = rz->getCachedOrigBytes() / sizeof(uint16_t);
+        const BufferInfo& rb = dag_->getBufferInfo(rzn->output_buffer_ids[0]);
+        const BufferInfo& eb = dag_->getBufferInfo(input_node_->output_buffer_ids[1]);
+        const auto d = lq->getDims();
+        const uint32_t dims[3] = {(uint32_t)d[0], (uint32_t)d[1], (uint32_t)d[2]};
+        rc = fzb_lq_bs_rze_decompress_dev(
+            rb.d_ptr, rb.allocated_size, static_cast<const float*>(eb.d_ptr),
+            static_cast<const uint32_t*>(dag_->getBuffer(input_node_->output_buffer_ids[2])),
+            static_cast<const uint32_t*>(dag_->getBuffer(input_node_->output_buffer_ids[3])),
+            eb.estimate / sizeof(float), n, dims, lq->deviceEbState() + 1, lq->getZigzagCodes() ? 1 : 0,
+            static_cast<float*>(decomp_out_), static_cast<uint8_t*>(decomp_work_) + 256, decomp_work_bytes_ - 256,
+            stream);
+        if (rc) throw std::runtime_error(std::string("LorenzoQuant<-Bitshuffle<-RZE decompress: ") +
+                                         fzb_status_string(rc));
+        return;
+    }
+    std::unordered_map<int, std::pair<void*, size_t>> avail;
+    for (int id : output_buffer_ids_) avail[id] = {dag_->getBuffer(id), dag_->getBufferInfo(id).estimate};
+    std::vector<DAGNode*> order;
+    for (const auto& lv : dag_->getLevels())
+        for (auto* n : lv) order.push_back(n);
+    size_t k = 0;
+    for (auto it = order.rbegin(); it != order.rend(); ++it) {
+        DAGNode* n = *it;
+        std::vector<void*> in;
+        std::vector<size_t> sizes;
+        for (int id : n->output_buffer_ids) {
+            const auto& a = avail.at(id);
+            in.push_back(a.first);
+            sizes.push_back(a.second);
+        }
+        void* out = nullptr;
+        if (n->input_buffer_ids[0] == input_buffer_id_) {
+            out = decomp_out_;
+        } else {
+            if (k == decomp_temps_.size()) {  // the first pass reserves the intermediates
+                const size_t est = n->stage->estimateOutputSizes(sizes).at(0);
+                void* t = pool_->allocate(est ? est : 256, stream, "graph_decompress_intermediate", true);
+                if (!t) throw std::runtime_error("decompress: allocation failed");
+                decomp_temps_.push_back(t);
+            }
+            out = decomp_temps_[k++];
+        }
+        n->stage->execute(stream, pool_.get(), in, {out}, sizes);
+        avail[n->input_buffer_ids[0]] = {out, n->stage->getActualOutputSize(0)};
+    }
+}
+
+bool Pipeline::captureDecompress(cudaStream_t stream) {
+    releaseDecompressGraph();
+    const size_t nout = output_buffer_ids_.size();
+    if (nout < 2 || nout > FZB_CONCAT_MAX_SEGMENTS || fused_pfpl_) return false;
+    for (auto& s : stages_)
+        if (!inverse_on_device(s.get())) return false;
+    for (int id : output_buffer_ids_) {
+        const BufferInfo& b = dag_->getBufferInfo(id);
+        if (!b.d_ptr || (b.allocated_size & 15) || (reinterpret_cast<uintptr_t>(b.d_ptr) & 15)) return false;
+    }
+    auto* lq = dynamic_cast<LorenzoQuantStage<float, uint16_t>*>(input_node_->stage);
+    if (lq && !lq->deviceEbState()) return false;
+    decomp_fused_ = fused_ && lq != nullptr;
+    decomp_in_bytes_ = pad16(getMaxCompressedSize(graph_input_bytes_));
+    decomp_in_ = pool_->allocate(decomp_in_bytes_, stream, "graph_decompress_input", true);
+    decomp_out_ = pool_->allocate(graph_input_bytes_, stream, "graph_decompress_output", true);
+    decomp_work_bytes_ = 256;
+    if (decomp_fused_) {
+        DAGNode* bsn = dag_->getNodes()[dag_->getBufferInfo(input_node_->output_index_to_buffer_id.at(0))
+                                            .consumer_stage_ids[0]];
+        DAGNode* rzn = dag_->getNodes()[dag_->getBufferInfo(bsn->output_buffer_ids[0]).consumer_stage_ids[0]];
+        decomp_work_bytes_ += fzb_workspace_bytes(static_cast<RZEStage*>(rzn->stage)->getCachedOrigBytes() / 2, 0);
+    }
+    decomp_work_ = pool_->allocate(decomp_work_bytes_, stream, "graph_decompress_workspace", true);
+    if (!decomp_in_ || !decomp_out_ || !decomp_work_) {
+        releaseDecompressGraph();
+        throw std::runtime_error("Failed to allocate the decompression graph's buffers");
+    }
+    // a container of the warm pass's outputs: the uncaptured first pass sizes
+    // every stage workspace, so that nothing allocates inside the capture
+    const auto saved_meta = meta_;
+    collectMetadata();
+    size_t sz = 0;
+    concatOutputs(decomp_in_, decomp_in_bytes_, &sz, stream);
+    meta_ = saved_meta;
+    for (auto& s : stages_) s->saveState();
+    for (auto& s : stages_) s->setInverse(true);
+    if (lq) lq->setInverseDeviceErrorBound(true);
+    auto restore = [&] {
+        if (lq) lq->setInverseDeviceErrorBound(false);
+        for (auto& s : stages_) {
+            s->setInverse(false);
+            s->restoreState();
+        }
+    };
+    try {
+        enqueueGraphInverse(stream);
+        cuda_check(cudaStreamSynchronize(stream), "decompress graph warm pass");
+        for (auto& s : stages_) s->postStreamSync(stream);
+        const int st = fzb_workspace_status(decomp_work_, stream);
+        if (st) throw std::runtime_error(std::string("decompress graph warm pass: ") + fzb_status_string(st));
+        cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        capturing_ = true;
+        try {
+            enqueueGraphInverse(stream);
+        } catch (...) {
+            capturing_ = false;
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        capturing_ = false;
+        cuda_check(cudaStreamEndCapture(stream, &decomp_graph_), "end capture");
+        cuda_check(cudaGraphInstantiate(&decomp_exec_, decomp_graph_, 0), "graph instantiate");
+    } catch (...) {
+        restore();
+        releaseDecompressGraph();
+        throw;
+    }
+    restore();
+    return true;
+}
+
+void Pipeline::checkDecompressStatus(cudaStream_t stream) {
+    cuda_check(cudaStreamSynchronize(stream), "decompress");
+    if (!decomp_exec_) return;  // eager decompressions report a bad input when they run
+    int st = fzb_workspace_status(decomp_work_, stream);
+    if (st == FZB_OK && decomp_fused_) st = fzb_workspace_status(static_cast<uint8_t*>(decomp_work_) + 256, stream);
+    if (st != FZB_OK) throw std::runtime_error(std::string("decompress: ") + fzb_status_string(st));
+    if (decomp_fused_) return;
+    for (auto& s : stages_) s->saveState();
+    try {
+        for (auto& s : stages_) {
+            s->setInverse(true);
+            s->postStreamSync(stream);  // the inverse's workspace status
+            s->setInverse(false);
+        }
+    } catch (...) {
+        for (auto& s : stages_) {
+            s->setInverse(false);
+            s->restoreState();
+        }
+        throw;
+    }
+    for (auto& s : stages_) s->restoreState();
 }
 
 // ----------------------------------------------------------------------- FZM

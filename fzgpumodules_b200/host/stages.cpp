@@ -140,12 +140,19 @@ void LorenzoQuantStage<TInput, TCode>::execute(cudaStream_t stream, MemoryPool* 
         if (n == 0) return;
         const size_t cap = sizes[1] / sizeof(TInput);
         const size_t need = fzb_workspace_bytes(n, 0);
-        void* w = ws_.ensure(need, pool, stream);
-        check(fzb_lq_inverse(static_cast<const uint16_t*>(inputs[0]), static_cast<const float*>(inputs[1]),
-                             static_cast<const uint32_t*>(inputs[2]), static_cast<const uint32_t*>(inputs[3]),
-                             cap, n, dims, computed_abs_eb_, config_.zigzag_codes ? 1 : 0,
-                             static_cast<float*>(outputs[0]), w, ws_.size(), stream),
-              "LorenzoQuantStage (inverse)");
+        void* w = inv_ws_.ensure(need, pool, stream);
+        if (inv_dev_eb_ && d_eb_state_)
+            check(fzb_lq_inverse_dev(static_cast<const uint16_t*>(inputs[0]), static_cast<const float*>(inputs[1]),
+                                     static_cast<const uint32_t*>(inputs[2]), static_cast<const uint32_t*>(inputs[3]),
+                                     cap, n, dims, d_eb_state_ + 1, config_.zigzag_codes ? 1 : 0,
+                                     static_cast<float*>(outputs[0]), w, inv_ws_.size(), stream),
+                  "LorenzoQuantStage (inverse)");
+        else
+            check(fzb_lq_inverse(static_cast<const uint16_t*>(inputs[0]), static_cast<const float*>(inputs[1]),
+                                 static_cast<const uint32_t*>(inputs[2]), static_cast<const uint32_t*>(inputs[3]),
+                                 cap, n, dims, computed_abs_eb_, config_.zigzag_codes ? 1 : 0,
+                                 static_cast<float*>(outputs[0]), w, inv_ws_.size(), stream),
+                  "LorenzoQuantStage (inverse)");
         actual_[0] = n * sizeof(TInput);
         return;
     }
@@ -202,7 +209,7 @@ void LorenzoQuantStage<TInput, TCode>::fusedForward(cudaStream_t stream, MemoryP
 template <typename TInput, typename TCode>
 void LorenzoQuantStage<TInput, TCode>::postStreamSync(cudaStream_t stream) {
     if (is_inverse_) {
-        ws_.checkStatus(stream, "LorenzoQuantStage (inverse)");
+        inv_ws_.checkStatus(stream, "LorenzoQuantStage (inverse)");
         return;
     }
     if (!pending_) return;

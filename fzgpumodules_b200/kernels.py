@@ -175,6 +175,23 @@ def lq_bs_rze_decompress(rze: torch.Tensor, rze_bytes: int, err, idx, count, cap
     return out
 
 
+def lq_bs_rze_decompress_dev(rze: torch.Tensor, rze_capacity: int, err, idx, count, cap: int, n: int,
+                             dims, abs_eb: torch.Tensor, zigzag: bool = False, ws: Workspace | None = None,
+                             out=None):
+    """The fused inverse with no host wait: the error bound is read on the
+    device (abs_eb: a one-float device tensor) and the exact kernels follow
+    the fused pass, gated on its status.  Check ws.status() afterwards."""
+    ws = ws or _default_ws
+    dev = rze.device
+    if out is None:
+        out = torch.empty(n, dtype=torch.float32, device=dev)
+    wp, wn = ws.get(n, dev)
+    check(lib().fzb_lq_bs_rze_decompress_dev(
+        _ptr(rze), rze_capacity, _ptr(err), _ptr(idx), _ptr(count), cap, n, _dims(dims), _ptr(abs_eb),
+        int(zigzag), _ptr(out), wp, wn, _stream(dev)), "fzb_lq_bs_rze_decompress_dev")
+    return out
+
+
 def _elem(t: torch.Tensor) -> int:
     return t.element_size()
 

@@ -255,6 +255,7 @@ class Pipeline:
         self._conns: list[tuple[Stage, Stage, str]] = []
         self._dims = (0, 1, 1)
         self._fusion, self._graph, self._profiling = True, False, False
+        self._streams, self._bounds = 1, False
         self._h = None
         self._last_in = 0
 
@@ -275,9 +276,11 @@ class Pipeline:
             d = [int(v) for v in pl["dims"]][:3] + [0, 1, 1][len(pl["dims"][:3]):]
             self.setDims(*d)
         if "memory_strategy" in pl:
-            self._strategy = config.STRATEGIES.get(pl["memory_strategy"], MINIMAL)
+            self._strategy = config.strategy(pl["memory_strategy"])
         if "pool_multiplier" in pl:
             self._mult = float(pl["pool_multiplier"])
+        if "num_streams" in pl:
+            self.setNumStreams(int(pl["num_streams"]))
         for _, st in cfg["stages"]:
             self.addStage(st)
         for dep, prod, port in cfg["connections"]:
@@ -291,7 +294,7 @@ class Pipeline:
             raise PipelineError("saveConfig: pipeline must be finalized first")
         params = {"input_size": self._hint,
                   "memory_strategy": "PREALLOCATE" if self._strategy == PREALLOCATE else "MINIMAL",
-                  "pool_multiplier": self._mult, "num_streams": 1, "dims": list(self._dims)}
+                  "pool_multiplier": self._mult, "num_streams": self.getNumStreams(), "dims": list(self._dims)}
         with open(path, "w") as f:
             f.write(config.dump_config(params, self._stages, self._conns))
 
@@ -315,6 +318,21 @@ class Pipeline:
     def enableGraphMode(self, on: bool):
         self._graph = bool(on)
 
+    def setNumStreams(self, n: int):
+        """Side streams for DAG levels with several stages (before finalize)."""
+        if self._h is not None:
+            raise PipelineError("Cannot configure streams after finalization")
+        self._streams = int(n)
+
+    def getNumStreams(self) -> int:
+        return lib().fzb_pipeline_num_streams(self._h) if self._h is not None else self._streams
+
+    def enableBoundsCheck(self, on: bool):
+        """After each stage, compare its output sizes with the reserved bytes."""
+        self._bounds = bool(on)
+        if self._h is not None:
+            _check(lib().fzb_pipeline_enable_bounds_check(self._h, int(on)), "enableBoundsCheck")
+
     def enableProfiling(self, on: bool):
         self._profiling = bool(on)
         if self._h is not None:
@@ -336,6 +354,8 @@ class Pipeline:
                 _check(lib().fzb_pipeline_set_fusion(h, int(self._fusion)), "setFusion")
                 _check(lib().fzb_pipeline_enable_graph_mode(h, int(self._graph)), "enableGraphMode")
                 _check(lib().fzb_pipeline_enable_profiling(h, int(self._profiling)), "enableProfiling")
+                _check(lib().fzb_pipeline_set_num_streams(h, self._streams), "setNumStreams")
+                _check(lib().fzb_pipeline_enable_bounds_check(h, int(self._bounds)), "enableBoundsCheck")
                 _check(lib().fzb_pipeline_finalize(h), "finalize")
             except Exception:
                 lib().fzb_pipeline_destroy(h)
@@ -347,6 +367,15 @@ class Pipeline:
 
     def captureGraph(self, stream: torch.cuda.Stream):
         _check(lib().fzb_pipeline_capture_graph(self._h, C.c_void_p(stream.cuda_stream)), "captureGraph")
+
+    def isDecompressGraphCaptured(self) -> bool:
+        return bool(self._h and lib().fzb_pipeline_decompress_graph_captured(self._h) == 1)
+
+    def checkDecompressStatus(self):
+        """Waits for the last decompress and raises if the device found its
+        input malformed (graph-mode decompressions report it only here)."""
+        with torch.cuda.device(self.device):
+            _check(lib().fzb_pipeline_check_decompress(self._h, _stream(self.device)), "decompress")
 
     # execution -------------------------------------------------------------
     def compress(self, data: torch.Tensor) -> torch.Tensor:

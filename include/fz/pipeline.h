@@ -130,7 +130,19 @@ public:
     Pipeline& operator=(const Pipeline&) = delete;
 
     void setMemoryStrategy(MemoryStrategy strategy);
-    void setNumStreams(int) {}  // single stream: every stage runs stream-ordered
+    // Streams for sibling stages (include/pipeline/compressor.h:64).  At
+    // finalize() the pipeline keeps max(n, widest DAG level) side streams
+    // when that is above 1; a level with several stages forks from the
+    // caller's stream onto them (round-robin within the level, as
+    // dag.cpp:752-762) and joins back before the next level.  Levels of one
+    // stage, and every linear chain, run on the caller's stream.
+    void setNumStreams(int num_streams);
+    int getNumStreams() const { return num_streams_; }
+    // After each stage, read its actual output sizes (this synchronises) and
+    // throw when one exceeds the bytes reserved for it (dag.cpp:438-462).
+    void enableBoundsCheck(bool enable) { bounds_check_ = enable; }
+    bool isBoundsCheckEnabled() const { return bounds_check_; }
+    float getPoolMultiplier() const { return pool_multiplier_; }
     void setDims(size_t x, size_t y = 1, size_t z = 1) { dims_ = {x, y, z}; }
     void setDims(std::array<size_t, 3> dims) { dims_ = dims; }
     std::array<size_t, 3> getDims() const { return dims_; }
@@ -185,8 +197,21 @@ public:
     // stages, a non-default stream).
     void enableGraphMode(bool enable);
     bool isGraphModeEnabled() const { return graph_mode_; }
+    // Captures the compress DAG and, where every stage's inverse runs from
+    // device-resident sizes (LorenzoQuant, Bitshuffle, RZE, RLE, Bitpack,
+    // Huffman; two or more pipeline outputs), the decompression too.  A
+    // graph-mode decompress() then copies the container into a fixed slot
+    // and replays the graph: the container is split on the device (the
+    // segment sizes are read from its header there), the error bound comes
+    // from the compressor's device state, and nothing waits on the host.
+    // The reference's graph mode covers compression only
+    // (include/pipeline/compressor.h:321-341).
     void captureGraph(cudaStream_t stream);
     bool isGraphCaptured() const { return graph_exec_ != nullptr; }
+    bool isDecompressGraphCaptured() const { return decomp_exec_ != nullptr; }
+    // Waits for the last decompress() and throws if the device found its
+    // input malformed (graph-mode decompressions report it only here).
+    void checkDecompressStatus(cudaStream_t stream = 0);
 
     struct FZMFileHeader {
         FZMHeaderCore core;
@@ -224,6 +249,8 @@ private:
     void propagateBufferSizes(size_t source_bytes);
     void detectFusion();
     void runForward(cudaStream_t stream);
+    void runNode(DAGNode* n, cudaStream_t stream);
+    void checkBounds(DAGNode* n);
     const void* prepareInput(const void* d_input, size_t input_size, cudaStream_t stream, size_t* padded);
     void collectMetadata();
     void concatOutputs(void* d_out, size_t capacity, size_t* out_size, cudaStream_t stream);
@@ -251,8 +278,28 @@ private:
     bool fusion_enabled_ = true, fused_ = false;
     bool fused_pfpl_ = false;  // the fused chain starts at a Quantizer (pfpl) rather than LorenzoQuant
     bool graph_mode_ = false;
+    bool bounds_check_ = false, capturing_ = false;
+    float pool_multiplier_ = 3.0f;
+    int num_streams_ = 1;
+    std::vector<cudaStream_t> side_streams_;
+    std::vector<cudaEvent_t> fork_events_;   // one per DAG level
+    std::vector<cudaEvent_t> join_events_;   // one per stage
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
+    // captured decompression: container slot, reconstruction slot, split
+    // status word + fused-inverse workspace, stage-by-stage intermediates
+    cudaGraph_t decomp_graph_ = nullptr;
+    cudaGraphExec_t decomp_exec_ = nullptr;
+    void* decomp_in_ = nullptr;
+    size_t decomp_in_bytes_ = 0;
+    void* decomp_out_ = nullptr;
+    void* decomp_work_ = nullptr;
+    size_t decomp_work_bytes_ = 0;
+    bool decomp_fused_ = false;
+    std::vector<void*> decomp_temps_;
+    bool captureDecompress(cudaStream_t stream);
+    void enqueueGraphInverse(cudaStream_t stream);
+    void releaseDecompressGraph();
     void* graph_input_ = nullptr;
     size_t graph_input_bytes_ = 0;
     DAGNode* input_node_ = nullptr;

@@ -150,6 +150,11 @@ public:
     size_t getMaxOutlierCount(size_t num_elements) const;
     float computedAbsErrorBound() const { return computed_abs_eb_; }
     float computedValueBase() const { return computed_value_base_; }
+    // A captured decompression reads the error bound the compressor left on
+    // the device (the second float of deviceEbState()) instead of the host
+    // copy, which a graph-replayed compression does not refresh.
+    void setInverseDeviceErrorBound(bool on) { inv_dev_eb_ = on; }
+    const float* deviceEbState() const { return d_eb_state_; }
 
     // The fused LorenzoQuant -> Bitshuffle -> RZE path runs this stage's
     // forward kernel itself; it reports back what execute() would record.
@@ -168,7 +173,9 @@ private:
     const void* d_count_ = nullptr;  // pending read-back (forward)
     float* d_eb_state_ = nullptr;    // inside the workspace
     bool pending_ = false;
+    bool inv_dev_eb_ = false;
     StageWorkspace ws_;
+    StageWorkspace inv_ws_;  // the inverse's own, so the forward eb state survives it
 };
 
 // ---------------------------------------------------------------------------

@@ -38,6 +38,10 @@ extern "C" {
 /* fzb_*_decompress flags */
 #define FZB_NO_SYNC 1u        /* do not wait for / check the device status */
 #define FZB_FORCE_EXACT 2u    /* skip the fused inverse, run the exact kernels */
+#define FZB_DEVICE_FALLBACK 4u /* no host wait: the exact kernels follow the fused
+                                  pass and run only if it flagged a case it leaves
+                                  to them; the status is read later with
+                                  fzb_workspace_status() */
 
 int fzb_version(void);
 const char* fzb_status_string(int status);
@@ -89,6 +93,14 @@ int fzb_lq_inverse(const uint16_t* d_codes, const float* d_err, const uint32_t* 
                    const uint32_t* d_count, uint64_t cap, uint64_t n_total,
                    const uint32_t dims[3], float abs_eb, int zigzag, float* d_out,
                    void* d_work, size_t work_bytes, void* stream);
+/* The same with the error bound read on the device from d_abs_eb (the
+ * second float of the compressor's eb state), so that no host value from
+ * the compression is needed: what a captured decompression graph uses.  No
+ * counterpart in the reference, which reads the bound on the host. */
+int fzb_lq_inverse_dev(const uint16_t* d_codes, const float* d_err, const uint32_t* d_idx,
+                       const uint32_t* d_count, uint64_t cap, uint64_t n_total,
+                       const uint32_t dims[3], const float* d_abs_eb, int zigzag, float* d_out,
+                       void* d_work, size_t work_bytes, void* stream);
 
 /* BitshuffleStage::execute (modules/shufflers/bitshuffle/bitshuffle_stage.cu
  * :355-475).  ew = 1, 2, 4 or 8; block a positive multiple of 1024*ew;
@@ -114,7 +126,9 @@ int fzb_rze_encode(const void* d_in, uint64_t bytes, void* d_out, uint64_t* d_ou
  * rejected with FZB_E_CAPACITY.  All calls on a device share that array, so
  * calls whose GPU work overlaps race and must be serialised.  The first call
  * on each device resolves the array's address; make it before any stream
- * capture.  Allocates nothing; d_out must hold fzb_rze_max_bytes(bytes). */
+ * capture.  That address is kept for the process's life and does not
+ * survive cudaDeviceReset: do not call this again after a reset.  Allocates
+ * nothing; d_out must hold fzb_rze_max_bytes(bytes). */
 #define FZB_RZE_NOALLOC_MAX_BYTES (8ull << 20)
 int fzb_rze_encode_noalloc(const void* d_in, uint64_t bytes, void* d_out, uint64_t* d_out_size,
                            void* stream);
@@ -146,6 +160,17 @@ int fzb_lq_bs_rze_decompress(const void* d_rze, uint64_t rze_bytes, const float*
                              uint64_t n_total, const uint32_t dims[3], float abs_eb, int zigzag,
                              float* d_out, unsigned flags,
                              void* d_work, size_t work_bytes, void* stream);
+/* The same without any host wait (FZB_DEVICE_FALLBACK) and with the error
+ * bound read on the device from d_abs_eb; rze_capacity bounds the stream
+ * reads (the stream's own header gives its chunk sizes).  Used by the
+ * pipeline's captured decompression graph; no counterpart in the reference,
+ * whose RZE and LorenzoQuant inverses read sizes and the bound on the host
+ * (rze_stage.cu:853-989, lorenzo_quant.cu:494-581). */
+int fzb_lq_bs_rze_decompress_dev(const void* d_rze, uint64_t rze_capacity, const float* d_err,
+                                 const uint32_t* d_idx, const uint32_t* d_count, uint64_t cap,
+                                 uint64_t n_total, const uint32_t dims[3], const float* d_abs_eb,
+                                 int zigzag, float* d_out, void* d_work, size_t work_bytes,
+                                 void* stream);
 
 /* RLEStage<T>::execute forward (modules/coders/rle/rle.cu:261-384), element
  * width elem = 1, 2 or 4 bytes.  Wire format [u32 runs][values, padded to 4
@@ -313,6 +338,17 @@ int fzb_pfpl_decompress(const void* d_rze, uint64_t rze_bytes, const float* d_ov
 #define FZB_CONCAT_MAX_SEGMENTS 32
 uint64_t fzb_concat_bytes(const uint64_t* sizes, int n);
 int fzb_concat(const void* const* d_srcs, const uint64_t* sizes, int n, void* d_out, void* stream);
+/* The inverse of fzb_concat with the sizes read on the device: the n
+ * segments of the container at d_in (in_capacity readable bytes, 16-byte
+ * aligned) are copied, in whole 16-byte words, to d_dsts[i] (16-byte aligned,
+ * capacities[i] bytes, a multiple of 16).  A header whose count is not n,
+ * or a segment larger than its capacity or past in_capacity, sets the
+ * malformed bit in *d_err (a workspace status word) and copies nothing.
+ * No host wait; what the pipeline's decompression graph starts with.  The
+ * reference's decompress splits the container on the host
+ * (src/pipeline/compressor_exec.cpp:198-355). */
+int fzb_concat_split(const void* d_in, uint64_t in_capacity, void* const* d_dsts, const uint64_t* capacities,
+                     int n, uint32_t* d_err, void* stream);
 
 /* ------------------------------------------------------------------------
  * Batched compression of many fields (no reference counterpart: it runs the
@@ -464,10 +500,25 @@ int fzb_pipeline_connect(void* pipeline, int dependent, int producer, const char
 /* Fusion of LorenzoQuant -> Bitshuffle -> RZE into one pass (default on). */
 int fzb_pipeline_set_fusion(void* pipeline, int on);
 int fzb_pipeline_enable_graph_mode(void* pipeline, int on);
+/* Pipeline::setNumStreams (include/pipeline/compressor.h:64): side streams
+ * for DAG levels with several stages; before finalize.  fzb_pipeline_num_streams
+ * returns the count in use after finalize (1 = the caller's stream only). */
+int fzb_pipeline_set_num_streams(void* pipeline, int num_streams);
+int fzb_pipeline_num_streams(void* pipeline);
+/* Pipeline::enableBoundsCheck (include/pipeline/compressor.h:306): after each
+ * stage, compare its actual output sizes with the reserved bytes and fail
+ * with "Buffer overwrite detected" (dag.cpp:438-462). */
+int fzb_pipeline_enable_bounds_check(void* pipeline, int on);
 int fzb_pipeline_enable_profiling(void* pipeline, int on);
 int fzb_pipeline_finalize(void* pipeline);
 int fzb_pipeline_is_fused(void* pipeline);
 int fzb_pipeline_capture_graph(void* pipeline, void* stream);
+/* 1 when captureGraph also captured the decompression (then decompress
+ * replays it with no host wait), else 0. */
+int fzb_pipeline_decompress_graph_captured(void* pipeline);
+/* Waits for the last decompress and fails (-8, message in fzb_last_error)
+ * if the device found its input malformed. */
+int fzb_pipeline_check_decompress(void* pipeline, void* stream);
 /* compress (pool-owned output, valid until the next compress). */
 int fzb_pipeline_compress(void* pipeline, const void* d_in, uint64_t bytes, void** d_out, uint64_t* out_bytes,
                           void* stream);

@@ -53,13 +53,21 @@ def _compare_files(ours: str, ref: str):
         da = np.frombuffer(sa[key]["data"], np.uint8)
         db = np.frombuffer(sb[key]["data"], np.uint8)
         assert da.size == db.size, key
-        if key[1] in ("outlier_errors", "outlier_indices"):
-            continue
+        if key[1] in ("outlier_errors", "outlier_indices", "outlier_vals", "outlier_idxs"):
+            continue  # compared below as (index, value) sets: the reference appends them with atomics
         if key[0] == 6:  # Huffman blob: header scratch bytes
             da, db = da.copy(), db.copy()
             da[2:4] = db[2:4] = 0
             da[64:128] = db[64:128] = 0
         assert np.array_equal(da, db), key
+    for vals, idxs in (("outlier_errors", "outlier_indices"), ("outlier_vals", "outlier_idxs")):
+        for st in {k[0] for k in sa if k[1] == idxs}:
+            va = np.frombuffer(sa[(st, vals)]["data"], np.uint32)
+            vb = np.frombuffer(sb[(st, vals)]["data"], np.uint32)
+            ia = np.frombuffer(sa[(st, idxs)]["data"], np.uint32)
+            ib = np.frombuffer(sb[(st, idxs)]["data"], np.uint32)
+            oa, ob = np.argsort(ia, kind="stable"), np.argsort(ib, kind="stable")
+            assert np.array_equal(ia[oa], ib[ob]) and np.array_equal(va[oa], vb[ob]), (st, vals)
     if (1, "outlier_errors") not in sa:
         return 0, a["core"]["compressed"]
     ea = np.frombuffer(sa[(1, "outlier_errors")]["data"], np.float32)
@@ -121,7 +129,7 @@ def test_fullsize_matches_reference_pipeline(cuda, case, tmp_path):
 def test_reference_3d_ghost_row_reads_stale_shared_memory(cuda):
     """The reference's 3-D LorenzoQuant kernel takes its y difference as
     `delta -= (threadIdx.y > 0) * s[threadIdx.y][tx]` and never writes row 0
-    of `s` (lorenzo_quant_nd.cu:214-247), so its output depends on what an
+    of `s` (lorenzo_quant_nd.cu:214,246), so its output depends on what an
     earlier kernel left in shared memory.  With shared memory scrubbed to
     zero (what the parity shims do) it equals the oracle; with 0xFF bytes
     (NaN floats) left there, only cells with y % 8 == 0 change, each into an

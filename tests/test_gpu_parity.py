@@ -381,3 +381,34 @@ def test_reference_rze_and_bitshuffle_match(cuda, kind):
         bs = torch.empty_like(din)
         assert L.ref_bitshuffle(_vp(din), C.c_size_t(n), 16384, 2, 0, _vp(bs)) == 0
         assert np.array_equal(_h(bs), O.bitshuffle(d, 16384, 2))
+
+
+@pytest.mark.parametrize("case", ["in_regime", "inexact", "unsorted"])
+def test_device_fallback_decompress(cuda, case):
+    # the inverse with no host wait (fzb_lq_bs_rze_decompress_dev): the error
+    # bound is read on the device, and the exact kernels follow the fused pass
+    # gated on its status -- they take over for huge deltas (inexact) and for
+    # outlier lists not in index order (the reference's atomic order), and
+    # stay idle otherwise; every case equals the oracle bit for bit
+    dims = (64, 16, 16) if case != "in_regime" else (128, 64, 32)
+    n = int(np.prod(dims))
+    rng = np.random.default_rng(16)
+    if case == "inexact":
+        x = (rng.normal(size=n) * 1e4).astype(np.float32)
+    else:
+        x = _field(n, 29, "spiky")
+    cap = n
+    codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-4, O.ABS, 512, True, cap)
+    y = O.lq_inv(codes, err, idx, dims, e2, True)
+    out = kern().lq_bs_rze_compress(_g(x, cuda), dims, 1e-4, O.ABS, 512, True, 1.0)
+    k = int(_h(out["count"])[0])
+    assert k == cnt and k > 0
+    if case == "unsorted":
+        order = torch.arange(k - 1, -1, -1, device=cuda)
+        out["err"][:k] = out["err"][:k][order].clone()
+        out["idx"][:k] = out["idx"][:k][order].clone()
+    ws = kern().Workspace()
+    dec = kern().lq_bs_rze_decompress_dev(out["rze"], out["rze"].numel(), out["err"], out["idx"], out["count"],
+                                          out["cap"], n, dims, out["eb_state"][1:2], True, ws=ws)
+    assert ws.status() == 0
+    assert np.array_equal(_h(dec).view(np.uint32), y.view(np.uint32))

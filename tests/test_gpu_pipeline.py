@@ -348,3 +348,111 @@ def test_fzm_matches_reference_pipeline(cuda, case, tmp_path):
     assert dsz.value == n * 4
     assert torch.equal(y, dec)  # decompressed floats are bit-identical
     pl.close()
+
+
+def test_sibling_stages_on_side_streams(cuda):
+    """A DAG whose codes feed two coders (Bitshuffle -> RZE and RLE): the
+    coders share a level, so the pipeline keeps side streams and forks that
+    level onto them (Pipeline::setNumStreams, dag.cpp:343-369,752-762).  Each
+    branch's segment equals the one its linear pipeline writes, eagerly, with
+    the bounds check on, and from a replayed CUDA graph."""
+    p = P()
+    dims = (128, 64, 32)
+    x = make_field("grf", dims, cuda)
+    n4 = x.numel() * 4
+
+    def branched(streams, graph=False):
+        pl = p.Pipeline(n4, p.PREALLOCATE)
+        pl.setDims(*dims)
+        lq = pl.addStage(p.LorenzoQuantStage(1e-3, 32768, 0.2, p.REL, True))
+        bs = pl.addStage(p.BitshuffleStage(16384, 2))
+        rz = pl.addStage(p.RZEStage())
+        rl = pl.addStage(p.RLEStage(2))
+        pl.connect(bs, lq, "codes")
+        pl.connect(rz, bs)
+        pl.connect(rl, lq, "codes")
+        pl.setNumStreams(streams)
+        pl.enableBoundsCheck(True)
+        pl.enableGraphMode(graph)
+        pl.finalize()
+        return pl
+
+    lin_rze = build("bs_rze", dims, 1e-3, 1, 32768, True)
+    lin_rle = build("rle", dims, 1e-3, 1, 32768, True)
+    seg_rze = split_concat(lin_rze.compress(x).clone().cpu().numpy())[3]
+    seg_rle = split_concat(lin_rle.compress(x).clone().cpu().numpy())[3]
+    for streams in (1, 3):
+        pl = branched(streams)
+        assert pl.getNumStreams() == max(streams, 2)
+        comp = pl.compress(x).clone()
+        segs = split_concat(comp.cpu().numpy())
+        assert len(segs) == 5  # three outlier segments, the RZE stream, the RLE stream
+        assert np.array_equal(segs[3], seg_rze) and np.array_equal(segs[4], seg_rle)
+        y = pl.decompress(comp).clone()
+        assert torch.equal(y, lin_rze.decompress(None))
+        pl.close()
+    g = branched(2, graph=True)
+    s = torch.cuda.Stream(device=cuda)
+    g.captureGraph(s)
+    with torch.cuda.stream(s):
+        cg = g.compress(x).clone()
+    s.synchronize()
+    segs = split_concat(cg.cpu().numpy())
+    assert np.array_equal(segs[3], seg_rze) and np.array_equal(segs[4], seg_rle)
+    for pl in (g, lin_rze, lin_rle):
+        pl.close()
+
+
+@pytest.mark.parametrize("chain,fusion", [("bs_rze", True), ("bs_rze", False), ("rle", True)])
+def test_graph_decompress_on_new_inputs(cuda, chain, fusion):
+    """captureGraph also captures the decompression: the container is split on
+    the device, the error bound comes from the compressor's device state, and
+    decompress() returns without waiting on the host.  For each new field --
+    the second one with a different REL value base -- the replayed
+    decompression equals an eager pipeline's bit for bit, from the pipeline's
+    own outputs and from a copy of the container; a container with a bad
+    header is reported by checkDecompressStatus."""
+    p = P()
+    dims = (128, 128, 64)
+    mode = p.REL if chain == "bs_rze" else p.ABS
+    x1 = make_field("grf", dims, cuda)
+    xs = (x1, (x1 * 0.5 + 0.25).contiguous(), F().grf(dims[::-1], seed=9, spike_frac=1e-3, device=cuda).reshape(-1))
+    pl = p.Pipeline(x1.numel() * 4, p.PREALLOCATE)
+    pl.setDims(*dims)
+    lq = pl.addStage(p.LorenzoQuantStage(1e-3, 32768, 0.2, mode, True))
+    if chain == "bs_rze":
+        bs = pl.addStage(p.BitshuffleStage(16384, 2))
+        rz = pl.addStage(p.RZEStage())
+        pl.connect(bs, lq, "codes")
+        pl.connect(rz, bs)
+    else:
+        rl = pl.addStage(p.RLEStage(2))
+        pl.connect(rl, lq, "codes")
+    pl.enableGraphMode(True)
+    pl.setFusion(fusion)
+    pl.finalize()
+    s = torch.cuda.Stream(device=cuda)
+    pl.captureGraph(s)
+    assert pl.isDecompressGraphCaptured()
+    eager = build(chain, dims, 1e-3, mode, 32768, True, fusion=fusion)
+    for x in xs:
+        with torch.cuda.stream(s):
+            c = pl.compress(x).clone()
+            y = pl.decompress(None).clone()
+            y2 = pl.decompress(c).clone()
+            pl.checkDecompressStatus()
+        s.synchronize()
+        ce = eager.compress(x).clone()
+        ye = eager.decompress(ce).clone()
+        assert torch.equal(c, ce)
+        assert torch.equal(y.view(torch.int32), ye.view(torch.int32))
+        assert torch.equal(y2.view(torch.int32), ye.view(torch.int32))
+    bad = c.clone()
+    bad[0] = 99  # the header's segment count
+    with torch.cuda.stream(s):
+        pl.decompress(bad)
+        with pytest.raises(p.PipelineError, match="malformed"):
+            pl.checkDecompressStatus()
+    s.synchronize()
+    pl.close()
+    eager.close()
