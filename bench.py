@@ -5,9 +5,23 @@ Bitshuffle(16 KiB, element width 2) -> RZE(16 KiB, 4 levels) chain on a
 
 One step = one compression and one decompression of the field, inputs
 resident in HBM.  `value` is the compression throughput (uncompressed bytes /
-device time); the decompression throughput, both roofline fractions, the
-end-to-end (host buffers, copies inside the timed region) figures, the CPU
-baseline and clock samples sit beside it in the same JSON line.
+device time of the fused C-ABI call); beside it in the same JSON line:
+  decompress       the decompression throughput and its kernel roofline;
+  roofline         the compress kernel against the measured HBM peak;
+  pipeline         the same chain through this library's fz::Pipeline, each
+                   compress / decompress call timed with CUDA events around
+                   it (its host synchronisation included), as the reference
+                   arm times the reference's own Pipeline;
+  e2e              fz::Pipeline with host buffers: H2D of the field,
+                   compress, D2H of the container; H2D of the container,
+                   decompress, D2H of the field;
+  c3               LorenzoQuant 2-D -> Huffman on 8192^2, with the Huffman
+                   decode kernel's roofline;
+  selector         the learned per-chunk coder selector against exhaustive
+                   trial on 2 GiB of mixed fields (the metric's "ratio,
+                   learned vs exhaustive");
+  cpu_baseline     the oracle chain on the host cores, on the same field;
+  clocks           nvidia-smi samples taken during the timed region.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --workload c1|cli|c3|batch|selector|pfpl   (secondary
@@ -34,7 +48,7 @@ if ROOT not in sys.path:
 DEFAULT_DIMS = (512, 512, 512)
 EB, RADIUS, ZIGZAG, OUTLIER_CAP = 1e-3, 32768, True, 0.1
 SEED = 1002
-METRIC = "comp/decomp GB/s and % HBM roofline at fixed eb"
+METRIC = "comp/decomp GB/s and % HBM roofline at fixed eb; ratio, learned vs exhaustive"
 WORKLOAD = ("LorenzoQuant3D(REL 1e-3, r 32768, zigzag)->Bitshuffle(16384,ew2)->RZE(16384,4) "
             "on 512^3 f32 GRF k^-3 + 0.1% +-1e3 spikes")
 
@@ -129,16 +143,25 @@ def barrier(world):
 
 # ---------------------------------------------------------------- CPU side
 
-def cpu_baseline(steps: int = 1):
-    """The oracle (OpenMP C restatement of the reference stage math) on a
-    bounded sample of the workload: a 512x512x64 slab of the same field."""
-    import numpy as np
+def host_field(dims, rank: int = 0):
+    """The benchmark field as a host float32 array: generated on the GPU,
+    so it holds the same values the GPU arm compresses, when one is present."""
     import torch
 
     from fzgpumodules_b200 import fields
+    nx, ny, nz = dims
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
+    return fields.grf((nz, ny, nx), seed=SEED + rank, spike_frac=1e-3, device=dev).reshape(-1).cpu().numpy()
+
+
+def cpu_baseline(x, dims, steps: int = 1):
+    """The oracle chain (an OpenMP C restatement of the reference's stage
+    math) on the host cores, on the whole field `x` (host float32, x
+    fastest): value base, LorenzoQuant 3-D, Bitshuffle and RZE, then the
+    inverse chain; median seconds of `steps` runs."""
+    import numpy as np
+
     from oracle import oracle as O
-    x = fields.grf((64, 512, 512), seed=SEED, spike_frac=1e-3).reshape(-1).numpy()
-    dims = (512, 512, 64)
     cap = int(np.ceil(x.size * OUTLIER_CAP))
     O.lib()
     tc, td = [], []
@@ -151,7 +174,7 @@ def cpu_baseline(steps: int = 1):
         stream = O.rze_encode(O.bitshuffle(codes, 16384, 2))
         t1 = time.perf_counter()
         c2 = O.bitshuffle(O.rze_decode(stream), 16384, 2, inverse=True).view(np.uint16)
-        y = O.lq_inv(c2, err, idx, dims, e2, ZIGZAG)
+        O.lq_inv(c2, err, idx, dims, e2, ZIGZAG)
         t2 = time.perf_counter()
         tc.append(t1 - t0)
         td.append(t2 - t1)
@@ -159,8 +182,8 @@ def cpu_baseline(steps: int = 1):
     nbytes = x.size * 4
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"compress_gbs": nbytes / np.median(tc) / 1e9, "decompress_gbs": nbytes / np.median(td) / 1e9,
-            "cores": cores, "sample": "512x512x64 slab of the 512^3 field (64 MiB), oracle chain",
-            "ratio": nbytes / size}
+            "cores": cores, "sample": "the whole " + "x".join(map(str, dims)) +
+            f" field ({nbytes >> 20} MiB), oracle chain, same values as the GPU arm", "ratio": nbytes / size}
 
 
 def _cpu_2d(x2d, chain: str, eb: float, mode: int, radius: int, zigzag: bool):
@@ -227,17 +250,20 @@ CPU_WORKLOADS = {"c1": _cpu_c1, "cli": _cpu_cli, "c3": _cpu_c3}
 
 def run_reference(args, world, rank):
     """The reference arm: the reference's stage math on the host cores (the
-    reference ships no CPU implementation of this path, so the oracle port)."""
+    reference ships no CPU implementation of this path, so the oracle port),
+    on the same field and configuration as this library's arm."""
     if rank != 0:
         return
-    res = [cpu_baseline(1) for _ in range(args.warmup + args.steps)][args.warmup:]
     import numpy as np
+    dims = tuple(args.dims)
+    x = host_field(dims)
+    res = [cpu_baseline(x, dims, 1) for _ in range(args.warmup + args.steps)][args.warmup:]
     comp = float(np.median([r["compress_gbs"] for r in res]))
     dec = float(np.median([r["decompress_gbs"] for r in res]))
     line = {"metric": METRIC, "value": comp, "unit": "GB/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": WORKLOAD + " (CPU sample 512x512x64)"},
+            "data": "synthetic", "config": _config(dims, 1), "same_config": True,
             "decompress": {"value": dec, "unit": "GB/s"},
             "cpu_baseline": {"value": comp, "unit": "GB/s", "cores": res[0]["cores"], "kind": "port",
                              "sample": res[0]["sample"]},
@@ -257,7 +283,7 @@ def _reference_gpu_lq(args):
         if not torch.cuda.is_available() or not os.path.exists(path):
             return {"unavailable": "no GPU or no reference pipeline build"}
         from fzgpumodules_b200 import fields
-        nx, ny, nz = DEFAULT_DIMS
+        nx, ny, nz = tuple(args.dims)
         x = fields.grf((nz, ny, nx), seed=SEED, spike_frac=1e-3, device=torch.device("cuda", 0)).reshape(-1)
         L = C.CDLL(path)
         L.ref_pipe_last_error.restype = C.c_char_p
@@ -269,7 +295,10 @@ def _reference_gpu_lq(args):
         nbytes = 4 * x.numel()
         return {"compress_gbs": nbytes / cm.value / 1e6, "decompress_gbs": nbytes / dm.value / 1e6,
                 "compress_ms": cm.value, "decompress_ms": dm.value, "compressed_bytes": cb.value, "steps": steps,
-                "note": "Pipeline::compress / decompress calls, host synchronisation included"}
+                "dims": [nx, ny, nz],
+                "note": "the reference's fz::Pipeline::compress / decompress calls timed with CUDA events, host "
+                        "synchronisation included; the GPU arm's `pipeline` entry times this library's "
+                        "fz::Pipeline the same way"}
     except Exception as e:  # the CPU arm's line stands on its own
         return {"unavailable": str(e)[:200]}
 
@@ -285,6 +314,111 @@ def _traffic(kernel: str):
             return json.load(f)[kernel]
     except Exception:
         return None
+
+
+def _config(dims, world: int) -> dict:
+    return {"workload": WORKLOAD if tuple(dims) == DEFAULT_DIMS else WORKLOAD.replace("512^3", "x".join(map(str, dims))),
+            "dims": list(dims), "eb": EB, "eb_mode": "REL", "radius": RADIUS, "zigzag": ZIGZAG,
+            "outlier_capacity": OUTLIER_CAP,
+            "l2": "input 512 MiB > L2, plus a 256 MiB L2 flush before every timed call",
+            "parallelism": f"replicas x{world}"}
+
+
+def _pipeline(dims, n):
+    from fzgpumodules_b200 import pipeline as P
+    pl = P.Pipeline(4 * n, P.PREALLOCATE)
+    pl.setDims(*dims)
+    lq = pl.addStage(P.LorenzoQuantStage(EB, RADIUS, OUTLIER_CAP, P.REL, ZIGZAG))
+    bs = pl.addStage(P.BitshuffleStage(16384, 2))
+    rz = pl.addStage(P.RZEStage(16384, 4))
+    pl.connect(bs, lq, "codes")
+    pl.connect(rz, bs)
+    pl.finalize()
+    return pl
+
+
+def pipeline_timing(pl, x, steps: int, warmup: int, flush, world: int) -> dict:
+    """This library's fz::Pipeline::compress / decompress on the field, each
+    call bracketed by CUDA events with its host synchronisation inside, an
+    L2 flush before each: the way the reference arm times the reference's
+    own Pipeline (ref_pipeline_time_lq)."""
+    import torch
+    n = x.numel()
+    ref = pl.compress(x).clone()
+    tc = td = 0.0
+    for i in range(warmup + steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        a.record()
+        pl.compress(x)
+        b.record()
+        b.synchronize()
+        if i >= warmup:
+            tc += a.elapsed_time(b)
+        flush.zero_()
+        a.record()
+        pl.decompress(None)
+        b.record()
+        b.synchronize()
+        if i >= warmup:
+            td += a.elapsed_time(b)
+    tc = max_over_ranks(tc / steps, world)
+    td = max_over_ranks(td / steps, world)
+    y = pl.decompress(None)[:n]
+    return {"compress_gbs": world * 4 * n / tc / 1e6, "decompress_gbs": world * 4 * n / td / 1e6,
+            "compress_ms": tc, "decompress_ms": td, "compressed_bytes": int(ref.numel()),
+            "bytes_equal_fused_call": None, "values_equal_fused_call": None, "_y": y, "_comp": ref,
+            "note": "fz::Pipeline (PREALLOCATE, fused LQ->BS->RZE execution) through the Python mirror of the C ABI; "
+                    "each call includes the pipeline's host synchronisation; the reference arm's "
+                    "reference_gpu_pipeline times the reference's fz::Pipeline on the same field the same way"}
+
+
+def pipeline_e2e(pl, x, steps: int, warmup: int, world: int) -> dict:
+    """End to end through fz::Pipeline with host buffers: every step copies
+    the field from pinned host memory, compresses, copies the container back;
+    then copies the container to the device, decompresses and copies the
+    field back.  Wall clock, synchronised at the end of each direction."""
+    import torch
+    n = x.numel()
+    hx = x.cpu().pin_memory()
+    cap = int(pl.compress(x).numel())
+    hc = torch.empty(cap + (1 << 20), dtype=torch.uint8).pin_memory()
+    dc = torch.empty(cap + (1 << 20), dtype=torch.uint8, device=x.device)
+    dx = torch.empty_like(x)
+    hy = torch.empty_like(hx).pin_memory()
+    s = torch.cuda.current_stream()
+    tc, td, nb = [], [], 0
+    for it in range(warmup + steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dx.copy_(hx, non_blocking=True)
+        comp = pl.compress(dx)
+        nb = comp.numel()
+        hc[:nb].copy_(comp, non_blocking=True)
+        s.synchronize()
+        t1 = time.perf_counter()
+        dc[:nb].copy_(hc[:nb], non_blocking=True)
+        y = pl.decompress(dc[:nb])
+        hy.copy_(y[:n], non_blocking=True)
+        s.synchronize()
+        t2 = time.perf_counter()
+        if it >= warmup:
+            tc.append(t1 - t0)
+            td.append(t2 - t1)
+    ok = bool(torch.equal(hy.view(torch.int32), pl.decompress(None)[:n].cpu().view(torch.int32)))
+    t_c = max_over_ranks(sum(tc) / len(tc), world)
+    t_d = max_over_ranks(sum(td) / len(td), world)
+    return {"value": world * 4 * n / t_c / 1e9, "unit": "GB/s", "h2d_bytes_per_step": 4 * n + nb,
+            "d2h_bytes_per_step": nb + 4 * n, "compress_gbs": world * 4 * n / t_c / 1e9,
+            "decompress_gbs": world * 4 * n / t_d / 1e9, "api": "fz::Pipeline compress / decompress",
+            "values_equal_device_decompress": ok}
+
+
+def _guard(fn, *a, **k):
+    try:
+        return fn(*a, **k)
+    except Exception as e:  # an extra measurement never takes the headline line down
+        return {"error": f"{type(e).__name__}: {str(e)[:300]}"}
 
 
 def run_ours(args, world, rank, local):
@@ -363,41 +497,24 @@ def run_ours(args, world, rank, local):
     n_inv, t_inv = kern(inv_name)
     launches = sum(v[0] for v in per_kernel.values())
 
-    # end to end through the C ABI with host buffers: H2D of the field, compress,
-    # D2H of the compressed segments; H2D of the segments, decompress, D2H of the field
-    hx = x.cpu().pin_memory()
-    hy = torch.empty_like(hx).pin_memory()
-    hs = torch.empty(size, dtype=torch.uint8).pin_memory()
-    dx = torch.empty_like(x)
-    e2e_c, e2e_d = [1.0], [1.0]
-    e2e_steps = 0 if args.no_e2e else args.warmup + args.steps
-    if e2e_steps:
-        e2e_c, e2e_d = [], []
-    for it in range(e2e_steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        dx.copy_(hx, non_blocking=True)
-        o2 = kernels.lq_bs_rze_compress(dx, DIMS, EB, kernels.REL, RADIUS, ZIGZAG, OUTLIER_CAP, ws=ws, out=out)
-        sz = int(o2["rze_size"].item())  # D2H of the stream size
-        hs[:sz].copy_(o2["rze"][:sz], non_blocking=True)
-        herr = o2["err"][: n_out].to("cpu", non_blocking=True)
-        hidx = o2["idx"][: n_out].to("cpu", non_blocking=True)
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        drze = hs[:sz].to(dev, non_blocking=True)
-        derr = herr.to(dev, non_blocking=True)
-        didx = hidx.to(dev, non_blocking=True)
-        kernels.lq_bs_rze_decompress(drze, sz, derr if n_out else out["err"], didx if n_out else out["idx"],
-                                     out["count"], out["cap"], n, DIMS, abs_eb, ZIGZAG,
-                                     flags=kernels.NO_SYNC, ws=ws, out=y)
-        hy.copy_(y, non_blocking=True)
-        torch.cuda.synchronize()
-        t2 = time.perf_counter()
-        if it >= args.warmup:
-            e2e_c.append(t1 - t0)
-            e2e_d.append(t2 - t1)
-    e2e_t = max_over_ranks(float(np.mean(e2e_c)), world)
-    e2e_td = max_over_ranks(float(np.mean(e2e_d)), world)
+    # this library's fz::Pipeline, timed as the reference arm times the
+    # reference's Pipeline, and end to end with host buffers through it
+    pl = _pipeline(DIMS, n)
+    pipe = pipeline_timing(pl, x, args.steps, args.warmup, flush, world)
+    yp, cp = pipe.pop("_y"), pipe.pop("_comp").cpu().numpy()
+    pipe["values_equal_fused_call"] = bool(torch.equal(yp.view(torch.int32), y.view(torch.int32)))
+    # the container's last segment is the RZE stream: the same bytes as the fused call's
+    nseg = int(cp[:4].view(np.uint32)[0])
+    sizes = cp[4:4 + 8 * nseg].view(np.uint64).astype(np.int64)
+    off = (4 + 8 * nseg + 15) & ~15
+    for k in range(nseg - 1):
+        off += (int(sizes[k]) + 15) & ~15
+    pipe["bytes_equal_fused_call"] = bool(int(sizes[-1]) == size and np.array_equal(
+        cp[off:off + size], out["rze"][:size].cpu().numpy()))
+    del cp
+    e2e = None if args.no_e2e else pipeline_e2e(pl, x, args.steps, args.warmup, world)
+    pl.close()
+    del yp
 
     if rank != 0:
         return
@@ -407,17 +524,13 @@ def run_ours(args, world, rank, local):
     ach_c = algo_c / t_slab / 1e9 if t_slab else 0.0   # dominant compress kernel
     ach_d = algo_d / t_inv / 1e9 if t_inv else 0.0     # dominant decompress kernel
     tr_c, tr_d = _traffic(slab_name), _traffic(inv_name)
-    cpu = cpu_baseline(1) if (world == 1 and not args.no_cpu) else None
+    cpu = cpu_baseline(x.cpu().numpy(), DIMS, 1) if (world == 1 and not args.no_cpu) else None
     line = {
         "metric": METRIC, "value": world * nbytes / t_c / 1e9, "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": (t_c + t_d) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD if DIMS == DEFAULT_DIMS else WORKLOAD.replace("512^3", "x".join(map(str, DIMS))),
-                   "dims": list(DIMS), "eb": EB, "eb_mode": "REL",
-                   "radius": RADIUS, "zigzag": ZIGZAG, "outlier_capacity": OUTLIER_CAP,
-                   "l2": "input 512 MiB > L2, plus a 256 MiB L2 flush before every timed call",
-                   "parallelism": f"replicas x{world}"},
+        "config": _config(DIMS, world),
         "compress": {"gbs": nbytes / t_c / 1e9, "ms": t_c * 1e3, "ratio": nbytes / comp_bytes,
                      "compressed_bytes": comp_bytes, "outliers": n_out},
         "decompress": {"value": world * nbytes / t_d / 1e9, "unit": "GB/s", "ms": t_d * 1e3,
@@ -435,9 +548,8 @@ def run_ours(args, world, rank, local):
                      "kernel": slab_name, "kernel_ms": t_slab * 1e3, "launches": n_slab,
                      "call_frac": (algo_c / t_c / 1e9) / peak},
         "kernels_ms_per_step": {k: v[1] / args.steps for k, v in per_kernel.items()},
-        "e2e": None if args.no_e2e else {"value": world * nbytes / e2e_t / 1e9, "unit": "GB/s",
-                "h2d_bytes_per_step": nbytes + comp_bytes, "d2h_bytes_per_step": comp_bytes + nbytes + 8,
-                "compress_gbs": nbytes / e2e_t / 1e9, "decompress_gbs": nbytes / e2e_td / 1e9},
+        "pipeline": pipe,
+        "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "status": st,
@@ -447,6 +559,13 @@ def run_ours(args, world, rank, local):
         line["cpu_baseline"] = {"value": cpu["compress_gbs"], "unit": "GB/s", "cores": cpu["cores"],
                                 "kind": "port", "sample": cpu["sample"],
                                 "decompress_gbs": cpu["decompress_gbs"]}
+    if world == 1 and not args.no_extras:
+        from fzgpumodules_b200 import benchmarks
+        del flush
+        torch.cuda.empty_cache()
+        line["c3"] = _guard(benchmarks.c3_summary, dev, args.steps, args.warmup)
+        torch.cuda.empty_cache()
+        line["selector"] = _guard(benchmarks.selector_summary, dev, args.steps, args.warmup, args.train_chunks)
     print(json.dumps(line), flush=True)
 
 
@@ -500,6 +619,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--no-extras", action="store_true", help="skip the c3 and selector entries of the headline line")
+    ap.add_argument("--train-chunks", type=int, default=1 << 20,
+                    help="method-generated chunks the coder selector trains on (selector entry / workload)")
     ap.add_argument("--dims", type=int, nargs=3, default=list(DEFAULT_DIMS), metavar=("NX", "NY", "NZ"),
                     help="field extents (x fastest); the default is the 512^3 workload")
     ap.add_argument("--workload", default="chain", choices=["chain", "c1", "cli", "c3", "batch", "selector", "pfpl"],

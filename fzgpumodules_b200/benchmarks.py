@@ -115,7 +115,22 @@ def run_cli(args, dev):
                   "note": "calls include their host synchronisation, as the reference's host timing does"})
 
 
-def run_c3(args, dev):
+def _peak():
+    """Measured HBM copy bandwidth (GB/s) of this GPU pool, or None."""
+    import json as _j
+    import os as _o
+    try:
+        with open(_o.path.join(_o.path.dirname(_o.path.dirname(_o.path.abspath(__file__))), "MEASURED_PEAKS.json")) as f:
+            return float(_j.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def c3_summary(dev, steps: int, warmup: int) -> dict:
+    """C3: LorenzoQuant 2-D (ABS 1e-3, radius 512, zigzag) -> Huffman (bklen
+    1024, coarse) on the 8192^2 fractal field.  Times each step, checks the
+    decode, and gives the Huffman decode kernel's roofline: algorithmic bytes
+    = blob read + 2 B per code written, over the kernel's own event time."""
     x = F.fractal2d(8192, seed=1003, device=dev).reshape(-1)
     n = x.numel()
     dims = (8192, 8192, 1)
@@ -127,24 +142,46 @@ def run_c3(args, dev):
     freq = K.huff_histogram(codes, 1024)
     bk4, rb = K.huff_book(freq, 1024)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    t_lq = _time(lambda: K.lq_forward(x, dims, 1e-3, K.ABS, 512, True, 0.2, ws=ws), args.steps, args.warmup, flush)
-    t_hist = _time(lambda: K.huff_histogram(codes, 1024), args.steps, args.warmup, flush)
-    t_enc = _time(lambda: K.huff_encode(codes, bk4, rb, 1024, ws=hws, trim=False), args.steps, args.warmup, flush)
-    t_full = _time(lambda: K.huff_compress(codes, 1024, ws=hws, trim=False), args.steps, args.warmup, flush)
+    t_lq = _time(lambda: K.lq_forward(x, dims, 1e-3, K.ABS, 512, True, 0.2, ws=ws), steps, warmup, flush)
+    t_hist = _time(lambda: K.huff_histogram(codes, 1024), steps, warmup, flush)
+    t_enc = _time(lambda: K.huff_encode(codes, bk4, rb, 1024, ws=hws, trim=False), steps, warmup, flush)
+    t_full = _time(lambda: K.huff_compress(codes, 1024, ws=hws, trim=False), steps, warmup, flush)
     dec = torch.empty(n, dtype=torch.uint16, device=dev)
-    t_dec = _time(lambda: K.huff_decode(blob, n, 1024, ws=hws, out=dec), args.steps, args.warmup, flush)
+    t_dec = _time(lambda: K.huff_decode(blob, n, 1024, ws=hws, out=dec), steps, warmup, flush)
+    with K.Trace():
+        for _ in range(steps):
+            flush.zero_()
+            K.huff_decode(blob, n, 1024, ws=hws, out=dec)
+        torch.cuda.synchronize()
+        kern = K.Trace.kernels()
     t0 = time.perf_counter()
     for _ in range(10):
         K.huff_book(freq, 1024)
     t_book = (time.perf_counter() - t0) / 10 * 1e3
-    assert torch.equal(K.huff_decode(blob, n, 1024), codes)
+    ok = bool(torch.equal(K.huff_decode(blob, n, 1024), codes))
     comp_bytes = blob.numel() + 8 * min(int(out["count"].item()), out["cap"]) + 4
-    return _line("c3: LorenzoQuant2D(ABS 1e-3, r512, zigzag)->Huffman(1024), 8192^2 fractal", 4 * n / (t_lq + t_full) / 1e6,
-                 "GB/s", args, {"lq_ms": t_lq, "huffman_histogram_ms": t_hist, "huffman_book_host_ms": t_book,
-                                "huffman_encode_ms": t_enc, "huffman_compress_ms_with_book": t_full,
-                                "huffman_decode_ms": t_dec, "compress_gbs_without_book": 4 * n / (t_lq + t_hist + t_enc) / 1e6,
-                                "decode_gbs_codes": 2 * n / t_dec / 1e6, "ratio": 4 * n / comp_bytes,
-                                "bits_per_code": 8 * blob.numel() / n})
+    dk = next((k for k in kern if k.startswith("hf_decode")), None)
+    peak, kind = _peak()
+    roof = None
+    if dk:
+        launches, ms = kern[dk]
+        kms = ms / launches
+        algo = blob.numel() + 2 * n
+        ach = algo / kms / 1e6
+        roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "traffic": None, "algorithmic_bytes": algo, "peak_kind": kind, "kernel": dk, "kernel_ms": kms,
+                "launches": launches}
+    return {"workload": "LorenzoQuant2D(ABS 1e-3, r512, zigzag)->Huffman(1024, coarse), 8192^2 fractal",
+            "compress_gbs": 4 * n / (t_lq + t_full) / 1e6, "compress_gbs_without_book": 4 * n / (t_lq + t_hist + t_enc) / 1e6,
+            "lq_ms": t_lq, "huffman_histogram_ms": t_hist, "huffman_book_host_ms": t_book,
+            "huffman_encode_ms": t_enc, "huffman_compress_ms_with_book": t_full, "huffman_decode_ms": t_dec,
+            "decode_gbs_codes": 2 * n / t_dec / 1e6, "ratio": 4 * n / comp_bytes,
+            "bits_per_code": 8 * blob.numel() / n, "decode_identical": ok, "roofline": roof}
+
+
+def run_c3(args, dev):
+    d = c3_summary(dev, args.steps, args.warmup)
+    return _line("c3: " + d.pop("workload"), d["compress_gbs"], "GB/s", args, d)
 
 
 def batch_fields(dev, count=64, seed=1004, max_mb=256):
@@ -207,54 +244,61 @@ def run_batch(args, dev):
                                 "launches_per_batch": 5})
 
 
-def run_selector(args, dev):
+def selector_summary(dev, steps: int, warmup: int, train_chunks: int = 1 << 20) -> dict:
+    """C5: 2 GiB of mixed fields -> LorenzoQuant (REL 1e-3) codes in 64 KiB
+    chunks, coded by exhaustive trial and by the MLP selector trained on
+    `train_chunks` method-generated chunks (other seeds and field shape than
+    the test data) with the library's own kernels."""
     from . import selector as S
     kinds = ("smooth", "piecewise", "noise", "sparse")
-    # 2 GiB: 32 fields of 64 MiB (256 x 256 x 256), eight per kind
     codes = []
-    for i in range(32):
+    for i in range(32):  # 2 GiB: 32 fields of 64 MiB (256^3), eight per kind
         x = F.mixed_field(kinds[i % 4], (256, 256, 256), 1005 + i, device=dev)
         codes.append(K.lq_forward(x, (256, 256, 256), 1e-3, K.REL, 32768, True, 0.2)["codes"])
         del x
     codes = torch.cat(codes)
-    # training set: method-generated chunks (other seeds and shape), labelled
-    # by exhaustive trial; trained with the library's own MLP kernels
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    tr = S.method_codes(192, seed=500, device=dev)
-    X = S.features(tr)
-    T = S.regrets_from_sizes(S.trial_sizes(tr))
-    del tr
+    X, T = S.method_training_set(train_chunks, seed=500, device=dev)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
     sel = S.CoderSelector(seed=0, device=dev)
-    losses = sel.train(X, T, epochs=60, batch=256, lr=3e-3)
+    epochs = 60 if train_chunks <= 16384 else 12
+    batch = 256 if train_chunks <= 16384 else 4096
+    t0 = time.perf_counter()
+    losses = sel.train(X, T, epochs=epochs, batch=batch, lr=3e-3)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
+    del X, T
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    t_ex = _time(lambda: S.encode(codes, S.EXHAUSTIVE, trim=False), args.steps, args.warmup, flush)
-    t_le = _time(lambda: S.encode(codes, S.LEARNED, sel, trim=False), args.steps, args.warmup, flush)
+    t_ex = _time(lambda: S.encode(codes, S.EXHAUSTIVE, trim=False), steps, warmup, flush)
+    t_le = _time(lambda: S.encode(codes, S.LEARNED, sel, trim=False), steps, warmup, flush)
     with K.Trace():
         S.encode(codes, S.LEARNED, sel, trim=False)
         torch.cuda.synchronize()
         learned_kernels = {k: round(v[1], 3) for k, v in K.Trace.kernels().items()}
-    with K.Trace():
-        S.encode(codes, S.EXHAUSTIVE, trim=False)
-        torch.cuda.synchronize()
-        exhaustive_kernels = {k: round(v[1], 3) for k, v in K.Trace.kernels().items()}
     pre = codes[: 1 << 22]  # decode runs a host loop per chunk: check a 128-chunk prefix
     blob, _ = S.encode(pre, S.LEARNED, sel)
     ok = bool(torch.equal(S.decode(blob, pre.numel()), pre))
     r = S.compare(codes, sel)
     nbytes = codes.numel() * 2
-    return _line("selector: 2 GiB mixed fields -> LQ(REL 1e-3) codes, 64 KiB chunks, MLP 16-64-64-4",
-                 nbytes / t_le / 1e6, "GB/s", args,
-                 {"learned_ms": t_le, "exhaustive_ms": t_ex, "exhaustive_gbs": nbytes / t_ex / 1e6,
-                  "speedup_vs_exhaustive": t_ex / t_le, "ratio_learned": r["ratio_learned"],
-                  "ratio_exhaustive": r["ratio_exhaustive"], "ratio_best_fixed": r["ratio_best_fixed"],
-                  "learned_over_exhaustive": r["ratio_learned"] / r["ratio_exhaustive"],
-                  "choice_agreement": r["agreement"], "train_chunks": int(X.shape[0]), "train_seconds": t_train,
-                  "final_loss": losses[-1], "chunks": int(S.nchunks(codes.numel())),
-                  "learned_kernel_ms": learned_kernels, "exhaustive_kernel_ms": exhaustive_kernels,
-                  "decode_prefix_identical": ok,
-                  "bytes_unit": "GB/s of 16-bit codes (2 B per value)"})
+    return {"workload": "2 GiB mixed fields -> LQ(REL 1e-3) codes, 64 KiB chunks, MLP 16-64-64-4",
+            "learned_gbs": nbytes / t_le / 1e6, "exhaustive_gbs": nbytes / t_ex / 1e6,
+            "learned_ms": t_le, "exhaustive_ms": t_ex, "speedup_vs_exhaustive": t_ex / t_le,
+            "ratio_learned": r["ratio_learned"], "ratio_exhaustive": r["ratio_exhaustive"],
+            "ratio_best_fixed": r["ratio_best_fixed"],
+            "learned_over_exhaustive": r["ratio_learned"] / r["ratio_exhaustive"],
+            "gain_over_best_fixed": r["ratio_learned"] / r["ratio_best_fixed"],
+            "choice_agreement": r["agreement"], "train_chunks": int(train_chunks),
+            "train_generate_seconds": t_gen, "train_seconds": t_train, "train_epochs": epochs,
+            "final_loss": losses[-1], "held_out": "test fields use other seeds and a 256^3 shape",
+            "chunks": int(S.nchunks(codes.numel())), "learned_kernel_ms": learned_kernels,
+            "decode_prefix_identical": ok, "bytes_unit": "GB/s of 16-bit codes (2 B per value)"}
+
+
+def run_selector(args, dev):
+    d = selector_summary(dev, args.steps, args.warmup, getattr(args, "train_chunks", 1 << 20))
+    return _line("selector: " + d.pop("workload"), d["learned_gbs"], "GB/s", args, d)
 
 
 PFPL_DIMS = (512, 512, 512)

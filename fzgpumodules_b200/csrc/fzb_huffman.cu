@@ -202,15 +202,80 @@ __global__ void hf_concat_kernel(const uint32_t* __restrict__ slots, const uint3
     }
 }
 
-// One thread per partition: canonical decode (hf_kernels.cu:267-298) with a
-// 64-bit bit reader; 16 symbols are gathered before each 32-byte store.  The
-// partition length comes from the blob header (768 coarse, 1024 fine); the
-// grid covers the coarse partition count, the larger of the two.
-__global__ void __launch_bounds__(128) hf_decode_kernel(const uint8_t* __restrict__ blob, uint64_t blob_bytes,
-                                                        uint64_t n, uint32_t bklen_expect,
-                                                        uint16_t* __restrict__ out, uint32_t* err) {
-    __shared__ int s_first[32], s_entry[32];
-    extern __shared__ uint16_t s_keys[];
+// Canonical decode (hf_kernels.cu:258-312), one thread per partition as in
+// the reference, reorganised for throughput:
+//   * a per-CTA lookup table indexed by the next kHfLutBits bits gives
+//     (symbol, length) of every code of at most kHfLutBits bits in one probe;
+//     longer codes continue the canonical first[] walk from length
+//     kHfLutBits + 1.  The table is built with the walk's own comparisons
+//     (the shortest l with v >= first[l]), so both give identical symbols and
+//     error flags;
+//   * the partition's cells stream through registers in 16-byte blocks, the
+//     next block loaded while the current one is consumed, so a load has some
+//     fifty symbols of work to hide behind;
+//   * symbols are decoded 16 at a time into eight registers and leave as two
+//     16-byte stores.
+// A well-formed partition decodes its want symbols in exactly nbit bits;
+// anything else (a length past 31, a table index past the book, a bit count
+// that does not match) raises kErrMalformed.
+constexpr int kHfLutBits = 12;
+constexpr int kHfDecThreads = 256;
+
+struct HfBlockReader {
+    const uint8_t* blk;  // next 16-byte block to load
+    const uint8_t* end;  // one past the last blob byte
+    uint32_t c0, c1, c2, c3, inq;
+    uint4 nxt;
+
+    __device__ __forceinline__ uint4 load(const uint8_t* p) const {
+        if (p + 16 <= end) return __ldg(reinterpret_cast<const uint4*>(p));
+        uint32_t w[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint8_t* q = p + 4 * i;
+            w[i] = q + 4 <= end ? __ldg(reinterpret_cast<const uint32_t*>(q)) : 0u;
+        }
+        return make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    // starts at cell address a (4-byte aligned)
+    __device__ __forceinline__ void start(const uint8_t* a, const uint8_t* e) {
+        end = e;
+        const uint8_t* b0 = reinterpret_cast<const uint8_t*>(reinterpret_cast<uintptr_t>(a) & ~(uintptr_t)15);
+        const uint4 cur = load(b0);
+        nxt = load(b0 + 16);
+        blk = b0 + 32;
+        c0 = cur.x;
+        c1 = cur.y;
+        c2 = cur.z;
+        c3 = cur.w;
+        inq = 4;
+        for (uint32_t k = (uint32_t)((reinterpret_cast<uintptr_t>(a) & 15) >> 2); k; k--) take();
+    }
+    __device__ __forceinline__ uint32_t take() {
+        const uint32_t v = c0;
+        c0 = c1;
+        c1 = c2;
+        c2 = c3;
+        if (--inq == 0) {
+            c0 = nxt.x;
+            c1 = nxt.y;
+            c2 = nxt.z;
+            c3 = nxt.w;
+            inq = 4;
+            nxt = load(blk);
+            blk += 16;
+        }
+        return v;
+    }
+};
+
+__global__ void __launch_bounds__(kHfDecThreads, 4)
+    hf_decode_kernel(const uint8_t* __restrict__ blob, uint64_t blob_bytes, uint64_t n, uint32_t bklen_expect,
+                     uint16_t* __restrict__ out, uint32_t* err) {
+    __shared__ uint32_t s_first[32];
+    __shared__ int s_entry[32];
+    __shared__ uint32_t lut[1u << kHfLutBits];
+
     const uint32_t* ent = reinterpret_cast<const uint32_t*>(blob + 40);
     const uint32_t e1 = ent[1], e2 = ent[2], e3 = ent[3], e4 = ent[4], e5 = ent[5];
     const uint32_t* h32 = reinterpret_cast<const uint32_t*>(blob);
@@ -227,77 +292,109 @@ __global__ void __launch_bounds__(128) hf_decode_kernel(const uint8_t* __restric
     }
     const int* rb = reinterpret_cast<const int*>(blob + e1);
     if (threadIdx.x < 32) {
-        s_first[threadIdx.x] = rb[threadIdx.x];
+        s_first[threadIdx.x] = (uint32_t)rb[threadIdx.x];
         s_entry[threadIdx.x] = rb[32 + threadIdx.x];
     }
     const uint16_t* keys = reinterpret_cast<const uint16_t*>(blob + e1 + 256);
-    for (uint32_t i = threadIdx.x; i < bklen; i += blockDim.x) s_keys[i] = keys[i];
     __syncthreads();
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= pardeg) return;
-    const uint32_t nbit = reinterpret_cast<const uint32_t*>(blob + e2)[p];
-    const uint32_t entry = reinterpret_cast<const uint32_t*>(blob + e3)[p];
+    // lookup table: entry = symbol << 16 | bad << 8 | length (length 0: a longer code)
+    for (uint32_t u = threadIdx.x; u < (1u << kHfLutBits); u += blockDim.x) {
+        uint32_t e = 0;
+        for (int l = 1; l <= kHfLutBits; l++) {
+            const uint32_t v = u >> (kHfLutBits - l);
+            if (v >= s_first[l]) {
+                const int k = s_entry[l] + (int)v - (int)s_first[l];
+                const bool kin = k >= 0 && k < (int)bklen;
+                e = (kin ? ((uint32_t)__ldg(keys + k) << 16) : (1u << 8)) | (uint32_t)l;
+                break;
+            }
+        }
+        lut[u] = e;
+    }
+    __syncthreads();
+
+    const uint32_t* nbits_g = reinterpret_cast<const uint32_t*>(blob + e2);
+    const uint32_t* entry_g = reinterpret_cast<const uint32_t*>(blob + e3);
+    const uint8_t* cells = blob + e4;
+    const uint8_t* blob_end = blob + e5;
     const uint32_t ncells = (e5 - e4) / 4;
-    const uint32_t* bits = reinterpret_cast<const uint32_t*>(blob + e4) + entry;
-    const uint32_t avail = entry < ncells ? ncells - entry : 0u;
-    const uint64_t o0 = (uint64_t)p * sublen;
-    const uint32_t want = (uint32_t)min((uint64_t)sublen, n - o0);
-    // bit reader: buf holds the next `have` bits MSB-aligned
-    uint64_t buf = 0;
-    int have = 0;
-    uint32_t cell = 0;
-    auto refill = [&]() {
-        while (have <= 32) {
-            const uint32_t v = cell < avail ? __ldg(bits + cell) : 0u;
-            buf |= (uint64_t)v << (32 - have);
-            have += 32;
-            cell++;
-        }
-    };
     const bool aligned = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
-    uint32_t used = 0, outn = 0;
-    uint16_t stage[16];
     bool bad = false;
-    if (nbit == 0 && want > 0 && s_entry[1] == 1) {
-        // a single symbol in the book gets a zero-length code: every output
-        // is that symbol (the reference leaves this case undecoded)
-        for (uint32_t i = 0; i < want; i++) out[o0 + i] = s_keys[0];
-        return;
-    }
-    while (used < nbit && outn < want) {
-        refill();
-        uint32_t v = (uint32_t)(buf >> 63);
-        int l = 1;
-        while (l < 32 && v < (uint32_t)s_first[l]) {
-            v = (uint32_t)(buf >> (63 - l));
-            l++;
+
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pardeg; p += gridDim.x * blockDim.x) {
+        const uint32_t nbit = __ldg(nbits_g + p);
+        const uint32_t c0 = __ldg(entry_g + p);
+        const uint64_t o0 = (uint64_t)p * sublen;
+        const uint32_t want = (uint32_t)min((uint64_t)sublen, n - o0);
+        if (nbit == 0 && want > 0 && s_entry[1] == 1) {
+            // a single symbol in the book gets a zero-length code: every
+            // output is that symbol (the reference leaves this case undecoded)
+            const uint16_t k0 = __ldg(keys);
+            for (uint32_t i = 0; i < want; i++) out[o0 + i] = k0;
+            continue;
         }
-        if (l >= 32) {
-            bad = true;
-            break;
+        HfBlockReader rd;
+        rd.start(cells + 4 * (size_t)min(c0, ncells), blob_end);
+        uint64_t buf = 0;  // the next `have` bits, MSB-aligned
+        int have = 0;
+        uint32_t used = 0, eacc = 0;
+        while (have <= 32) {
+            buf |= (uint64_t)rd.take() << (32 - have);
+            have += 32;
         }
-        buf <<= l;
-        have -= l;
-        used += l;
-        const int k = s_entry[l] + (int)v - s_first[l];
-        const bool kin = k >= 0 && k < (int)bklen;
-        bad |= !kin;
-        stage[outn & 15] = kin ? s_keys[k] : (uint16_t)0;
-        outn++;
-        if ((outn & 15) == 0 && aligned) {
-            uint4* d4 = reinterpret_cast<uint4*>(out + o0 + outn - 16);
-            uint32_t w[8];
+        auto next_symbol = [&]() -> uint32_t {
+            if (have <= 32) {
+                buf |= (uint64_t)rd.take() << (32 - have);
+                have += 32;
+            }
+            const uint32_t e = lut[(uint32_t)(buf >> (64 - kHfLutBits))];
+            int l = (int)(e & 0xffu);
+            uint32_t sym;
+            if (l != 0) {
+                eacc |= e;
+                sym = e >> 16;
+            } else {  // longer than the table: continue the walk
+                l = kHfLutBits + 1;
+                uint32_t v = (uint32_t)(buf >> (64 - l));
+                while (l < 32 && v < s_first[l]) {
+                    l++;
+                    v = (uint32_t)(buf >> (64 - l));
+                }
+                if (l >= 32) {  // no code: flag it and move on by a full word
+                    bad = true;
+                    l = 31;
+                    sym = 0;
+                } else {
+                    const int k = s_entry[l] + (int)v - (int)s_first[l];
+                    const bool kin = k >= 0 && k < (int)bklen;
+                    bad |= !kin;
+                    sym = kin ? __ldg(keys + k) : 0u;
+                }
+            }
+            buf <<= l;
+            have -= l;
+            used += l;
+            return sym;
+        };
+        uint32_t i = 0;
+        if (aligned) {
+            for (; i + 16 <= want; i += 16) {
+                uint32_t w[8];
 #pragma unroll
-            for (int j = 0; j < 8; j++) w[j] = (uint32_t)stage[2 * j] | ((uint32_t)stage[2 * j + 1] << 16);
-            d4[0] = make_uint4(w[0], w[1], w[2], w[3]);
-            d4[1] = make_uint4(w[4], w[5], w[6], w[7]);
-        } else if (!aligned) {
-            out[o0 + outn - 1] = stage[(outn - 1) & 15];
+                for (int j = 0; j < 16; j++) {
+                    const uint32_t sym = next_symbol();
+                    if (j & 1) w[j >> 1] |= sym << 16;
+                    else w[j >> 1] = sym;
+                }
+                uint4* d4 = reinterpret_cast<uint4*>(out + o0 + i);
+                d4[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                d4[1] = make_uint4(w[4], w[5], w[6], w[7]);
+            }
         }
+        for (; i < want; i++) out[o0 + i] = (uint16_t)next_symbol();
+        bad |= ((eacc >> 8) & 1u) != 0 || used != nbit;
     }
-    if (aligned)
-        for (uint32_t i = outn & ~15u; i < outn; i++) out[o0 + i] = stage[i & 15];
-    if (bad || outn != want || used != nbit) atomicOr(err, kErrMalformed);
+    if (bad) atomicOr(err, kErrMalformed);
 }
 
 int launch_hf_histogram(const uint16_t* in, uint64_t n, uint32_t bklen, uint32_t* freq, int sms,
@@ -346,9 +443,13 @@ int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32
 int launch_hf_decode(const uint8_t* blob, uint64_t blob_bytes, uint64_t n, uint32_t bklen,
                      uint16_t* out, uint32_t* err, cudaStream_t s) {
     const uint32_t pardeg = (uint32_t)((n - 1) / kHfSublen + 1);  // the larger partition count
-    const int smem = 2 * (int)bklen + 16;
-    cudaFuncSetAttribute(hf_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    hf_decode_kernel<<<(pardeg + 127) / 128, 128, smem, s>>>(blob, blob_bytes, n, bklen, out, err);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t need = (pardeg + kHfDecThreads - 1) / kHfDecThreads;
+    const uint32_t grid = min(need, (uint32_t)sms * 4u);
+    TraceScope ts(s, "hf_decode");
+    hf_decode_kernel<<<grid ? grid : 1u, kHfDecThreads, 0, s>>>(blob, blob_bytes, n, bklen, out, err);
     return (int)cudaGetLastError();
 }
 

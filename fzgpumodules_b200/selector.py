@@ -200,6 +200,31 @@ def method_codes(count: int, seed: int, device, shape=(64, 128, 128), eb: float 
     return torch.cat(out)
 
 
+def method_training_set(n_chunks: int, seed: int, device, shape=(128, 256, 256), eb: float = 1e-3):
+    """Features and exhaustive-trial regrets of `n_chunks` method-generated
+    chunks: LorenzoQuant (REL eb, radius 32768, zigzag) codes of seeded
+    fields cycling through smooth / piecewise / noise / sparse, one field at
+    a time (each `shape` field is a whole number of chunks), so only the
+    16 features and 4 sizes of each chunk are kept.  Returns (X, T) on the
+    device."""
+    from . import fields as F
+    kinds = ("smooth", "piecewise", "noise", "sparse")
+    nz, ny, nx = shape
+    per = nchunks(nx * ny * nz)
+    xs, ts, have, i = [], [], 0, 0
+    while have < n_chunks:
+        x = F.mixed_field(kinds[i % 4], shape, seed + i, device=device)
+        codes = K.lq_forward(x, (nx, ny, nz), eb, K.REL, 32768, True, 0.2)["codes"]
+        del x
+        take = min(per, n_chunks - have)
+        c = codes[: take * CHUNK_CODES]
+        xs.append(features(c))
+        ts.append(regrets_from_sizes(trial_sizes(c)))
+        have += take
+        i += 1
+    return torch.cat(xs), torch.cat(ts)
+
+
 def compare(codes: torch.Tensor, sel: CoderSelector) -> dict:
     """Sizes of the exhaustive, learned and fixed-coder containers."""
     ex, tex = encode(codes, EXHAUSTIVE)
