@@ -202,79 +202,215 @@ __global__ void hf_concat_kernel(const uint32_t* __restrict__ slots, const uint3
     }
 }
 
-// Canonical decode (hf_kernels.cu:258-312), one thread per partition as in
-// the reference, reorganised for throughput:
-//   * a per-CTA lookup table indexed by the next kHfLutBits bits gives
-//     (symbol, length) of every code of at most kHfLutBits bits in one probe;
-//     longer codes continue the canonical first[] walk from length
-//     kHfLutBits + 1.  The table is built with the walk's own comparisons
-//     (the shortest l with v >= first[l]), so both give identical symbols and
-//     error flags;
-//   * the partition's cells stream through registers in 16-byte blocks, the
-//     next block loaded while the current one is consumed, so a load has some
-//     fifty symbols of work to hide behind;
-//   * symbols are decoded 16 at a time into eight registers and leave as two
-//     16-byte stores.
+// Canonical decode (hf_kernels.cu:258-312).  The reference gives each
+// partition to one thread.  Here, when the book has short codes, a warp
+// decodes one partition at a time, so every lane has work in proportion to
+// the partition's bits rather than its symbols and the output leaves in
+// coalesced 16-byte stores:
+//   * tables: each CTA builds a multi-symbol lookup table indexed by the next
+//     kHfLutBits bits.  Entry u holds up to kHfMultiMax whole codes that lie
+//     inside those bits: their symbols, their total length, their end
+//     offsets and an error flag.  A first-code table built with the canonical
+//     walk's own comparisons (the shortest l with v >= first[l]) feeds it, so
+//     symbols and error flags are identical to the walk's.  A second table
+//     gives every whole code in the window (count and end offsets) for
+//     counting.  A code longer than the table continues the walk from length
+//     kHfLutBits + 1;
+//   * count: the partition's nbit bits are cut into up to 32 equal segments
+//     of at least 32 bits.  Lane j decodes from its segment's first bit
+//     (possibly inside a code) to the first code boundary at or past the
+//     segment's end, counting codes and noting its code starts over its first
+//     64 bits (F);
+//   * synchronise: Huffman codes resynchronise.  Lane j - 1, if it decoded
+//     from a true boundary, decodes on past its end and notes the true starts
+//     (T) until one of them is also in lane j's F, at most 64 bits.  From the
+//     first shared start lane j's decode is the true decode: its count is
+//     corrected for the codes before that start, and its end is a true
+//     boundary.  A lane with no shared start inside its segment decodes again
+//     from its predecessor's true end;
+//   * emit: a warp prefix sum of the counts places each lane's symbols; each
+//     lane decodes its codes from its true start into the warp's staging
+//     strip, and the warp copies the partition out.
+// A book whose shortest code has more than kHfCoopMaxShortest bits (codes of
+// nearly one length resynchronise slowly, if ever) is decoded one partition
+// per lane instead, straight to the output.
 // A well-formed partition decodes its want symbols in exactly nbit bits;
 // anything else (a length past 31, a table index past the book, a bit count
-// that does not match) raises kErrMalformed.
+// that does not match) raises kErrMalformed.  err[kHfTicket] (zeroed with
+// the error word) hands partitions to warps.
 constexpr int kHfLutBits = 12;
-constexpr int kHfDecThreads = 256;
+constexpr uint32_t kHfLutSize = 1u << kHfLutBits;
+constexpr int kHfMultiMax = 4;
+constexpr int kHfDecWarps = 16;
+constexpr int kHfDecThreads = 32 * kHfDecWarps;
+constexpr int kHfCoopMaxShortest = 4;
+constexpr uint32_t kHfStage = kHfSublenFine;  // symbols staged per warp
+constexpr uint32_t kHfTicket = 8;
+// symbols (8 B), meta (4 B) and counts (4 B) per window, then the warps'
+// staging strips, which hold the first-code table while the CTA builds
+constexpr size_t kHfDecSmem = 16 * (size_t)kHfLutSize + 2 * (size_t)kHfStage * kHfDecWarps;
+static_assert(2 * kHfStage * kHfDecWarps >= 4 * kHfLutSize, "first-code table fits the strips");
 
-struct HfBlockReader {
-    const uint8_t* blk;  // next 16-byte block to load
-    const uint8_t* end;  // one past the last blob byte
-    uint32_t c0, c1, c2, c3, inq;
-    uint4 nxt;
-
-    __device__ __forceinline__ uint4 load(const uint8_t* p) const {
-        if (p + 16 <= end) return __ldg(reinterpret_cast<const uint4*>(p));
-        uint32_t w[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const uint8_t* q = p + 4 * i;
-            w[i] = q + 4 <= end ? __ldg(reinterpret_cast<const uint32_t*>(q)) : 0u;
-        }
-        return make_uint4(w[0], w[1], w[2], w[3]);
+// The partition's cells (MSB-first u32 words) from any bit: w0:w1 hold the
+// next 64 - off bits, w2 the word after them.
+struct HfBits {
+    const uint32_t* cells;
+    uint32_t ncells, wi, w0, w1, w2, off;
+    __device__ __forceinline__ uint32_t word(uint32_t i) const { return i < ncells ? __ldg(cells + i) : 0u; }
+    __device__ __forceinline__ void seek(uint32_t c0, uint32_t bit) {
+        const uint32_t w = c0 + (bit >> 5);
+        w0 = word(w);
+        w1 = word(w + 1);
+        w2 = word(w + 2);
+        wi = w + 3;
+        off = bit & 31u;
     }
-    // starts at cell address a (4-byte aligned)
-    __device__ __forceinline__ void start(const uint8_t* a, const uint8_t* e) {
-        end = e;
-        const uint8_t* b0 = reinterpret_cast<const uint8_t*>(reinterpret_cast<uintptr_t>(a) & ~(uintptr_t)15);
-        const uint4 cur = load(b0);
-        nxt = load(b0 + 16);
-        blk = b0 + 32;
-        c0 = cur.x;
-        c1 = cur.y;
-        c2 = cur.z;
-        c3 = cur.w;
-        inq = 4;
-        for (uint32_t k = (uint32_t)((reinterpret_cast<uintptr_t>(a) & 15) >> 2); k; k--) take();
-    }
-    __device__ __forceinline__ uint32_t take() {
-        const uint32_t v = c0;
-        c0 = c1;
-        c1 = c2;
-        c2 = c3;
-        if (--inq == 0) {
-            c0 = nxt.x;
-            c1 = nxt.y;
-            c2 = nxt.z;
-            c3 = nxt.w;
-            inq = 4;
-            nxt = load(blk);
-            blk += 16;
-        }
-        return v;
+    // the next 32 bits, MSB first
+    __device__ __forceinline__ uint32_t win() const { return __funnelshift_l(w1, w0, off); }
+    // l <= 31; moves to the next word without a branch
+    __device__ __forceinline__ void advance(uint32_t l) {
+        off += l;
+        const bool step = off >= 32;
+        const uint32_t nw = step && wi < ncells ? __ldg(cells + wi) : 0u;
+        w0 = step ? w1 : w0;
+        w1 = step ? w2 : w1;
+        w2 = step ? nw : w2;
+        wi += step ? 1u : 0u;
+        off &= 31u;
     }
 };
 
-__global__ void __launch_bounds__(kHfDecThreads, 4)
+struct HfDecTables {
+    const uint2* sym;
+    const uint32_t* meta;  // total length | count << 4 | bad << 7 | first length << 8 | end offsets << 12
+    const uint32_t* cmeta;  // every whole code in the window: total length | count << 4 | end offsets << 8
+    const uint32_t* first;
+    const int* entry;
+    const uint16_t* keys;
+    uint32_t bklen;
+};
+
+// the canonical walk from length kHfLutBits + 1 over the next 32 bits w;
+// 32 when no code matches
+__device__ __forceinline__ int hf_walk(uint32_t w, const uint32_t* first, uint32_t& v) {
+    int l = kHfLutBits + 1;
+    v = w >> (32 - l);
+    while (l < 32 && v < first[l]) {
+        l++;
+        v = w >> (32 - l);
+    }
+    return l;
+}
+
+// One probe for counting: total length, codes, end offsets (bit k-1 = a code
+// ends k bits on).  A missing code counts as one of 31 bits.
+__device__ __forceinline__ void hf_probe(uint32_t w, const HfDecTables& t, uint32_t& tot, uint32_t& c,
+                                         uint32_t& E) {
+    const uint32_t m = t.cmeta[w >> (32 - kHfLutBits)];
+    c = (m >> 4) & 15u;
+    tot = m & 15u;
+    E = m >> 8;
+    if (c == 0) {
+        uint32_t v;
+        const int l = hf_walk(w, t.first, v);
+        tot = l >= 32 ? 31u : (uint32_t)l;
+        E = 1u << (tot - 1);
+        c = 1;
+    }
+}
+
+// the code starts in a probe's window, relative to its first bit
+__device__ __forceinline__ uint32_t hf_starts(uint32_t tot, uint32_t E) {
+    return 1u | ((E << 1) & ((1u << tot) - 1u));
+}
+
+// Decodes from bit `start` to the first code boundary at or past s_end (e),
+// counting the codes (cnt); F: the code starts in [rec, rec + 64).
+__device__ __forceinline__ void hf_count(HfBits& r, const HfDecTables& t, uint32_t start, uint32_t s_end,
+                                         uint32_t rec, uint32_t& e, uint32_t& cnt, uint64_t& F) {
+    uint32_t pos = start;
+    cnt = 0;
+    F = 0;
+    while (pos < s_end) {
+        uint32_t tot, c, E;
+        hf_probe(r.win(), t, tot, c, E);
+        const uint32_t d = pos - rec;
+        if (d < 64) F |= (uint64_t)hf_starts(tot, E) << d;
+        const uint32_t rr = s_end - pos;
+        uint32_t adv = tot;
+        if (tot > rr) {  // the first code end at or past s_end
+            adv = rr - 1 + (uint32_t)__ffs(E >> (rr - 1));
+            c = (uint32_t)__popc(E & ((1u << adv) - 1u));
+        }
+        cnt += c;
+        r.advance(adv);
+        pos += adv;
+    }
+    e = pos;
+}
+
+// Decodes `count` codes from the reader, handing symbol i to put(i, s);
+// returns the bits used.
+template <class Put>
+__device__ __forceinline__ uint32_t hf_emit(HfBits& r, const HfDecTables& t, uint32_t count, uint32_t& eacc,
+                                            bool& bad, Put put) {
+    uint32_t i = 0, used = 0;
+    while (i < count) {
+        const uint32_t w = r.win();
+        const uint32_t u = w >> (32 - kHfLutBits);
+        const uint32_t m = t.meta[u];
+        const uint32_t cm = (m >> 4) & 7u;
+        uint32_t adv;
+        if (cm == 0) {
+            uint32_t v;
+            int l = hf_walk(w, t.first, v);
+            uint32_t s = 0;
+            if (l >= 32) {  // no code: flag it and move on by 31 bits
+                bad = true;
+                l = 31;
+            } else {
+                const int k = t.entry[l] + (int)v - (int)t.first[l];
+                const bool kin = k >= 0 && k < (int)t.bklen;
+                bad |= !kin;
+                s = kin ? __ldg(t.keys + k) : 0u;
+            }
+            put(i, s);
+            i++;
+            adv = (uint32_t)l;
+        } else {
+            const uint2 sy = t.sym[u];
+            const uint32_t take = min(cm, count - i);
+            put(i, sy.x);
+            if (take > 1) put(i + 1, sy.x >> 16);
+            if (take > 2) put(i + 2, sy.y);
+            if (take > 3) put(i + 3, sy.y >> 16);
+            if (take == cm) {
+                adv = m & 15u;
+            } else {  // the end of the take-th code
+                uint32_t E = m >> 12;
+                if (take > 1) E &= E - 1;
+                if (take > 2) E &= E - 1;
+                adv = (uint32_t)__ffs(E);
+            }
+            eacc |= m;
+            i += take;
+        }
+        r.advance(adv);
+        used += adv;
+    }
+    return used;
+}
+
+__global__ void __launch_bounds__(kHfDecThreads, 2)
     hf_decode_kernel(const uint8_t* __restrict__ blob, uint64_t blob_bytes, uint64_t n, uint32_t bklen_expect,
                      uint16_t* __restrict__ out, uint32_t* err) {
     __shared__ uint32_t s_first[32];
     __shared__ int s_entry[32];
-    __shared__ uint32_t lut[1u << kHfLutBits];
+    extern __shared__ __align__(16) uint8_t hf_smem[];
+    uint2* msym = reinterpret_cast<uint2*>(hf_smem);
+    uint32_t* mmeta = reinterpret_cast<uint32_t*>(hf_smem + 8 * kHfLutSize);
+    uint32_t* cmeta = reinterpret_cast<uint32_t*>(hf_smem + 12 * kHfLutSize);
+    uint8_t* strips = hf_smem + 16 * kHfLutSize;
 
     const uint32_t* ent = reinterpret_cast<const uint32_t*>(blob + 40);
     const uint32_t e1 = ent[1], e2 = ent[2], e3 = ent[3], e4 = ent[4], e5 = ent[5];
@@ -297,8 +433,9 @@ __global__ void __launch_bounds__(kHfDecThreads, 4)
     }
     const uint16_t* keys = reinterpret_cast<const uint16_t*>(blob + e1 + 256);
     __syncthreads();
-    // lookup table: entry = symbol << 16 | bad << 8 | length (length 0: a longer code)
-    for (uint32_t u = threadIdx.x; u < (1u << kHfLutBits); u += blockDim.x) {
+    // first-code table: symbol << 16 | bad << 8 | length (length 0: a longer code)
+    uint32_t* first = reinterpret_cast<uint32_t*>(strips);
+    for (uint32_t u = threadIdx.x; u < kHfLutSize; u += blockDim.x) {
         uint32_t e = 0;
         for (int l = 1; l <= kHfLutBits; l++) {
             const uint32_t v = u >> (kHfLutBits - l);
@@ -309,90 +446,221 @@ __global__ void __launch_bounds__(kHfDecThreads, 4)
                 break;
             }
         }
-        lut[u] = e;
+        first[u] = e;
     }
     __syncthreads();
+    // multi-symbol table; a code with an out-of-book index ends the entry and,
+    // as the entry's first code, is emitted as symbol 0 with the bad flag
+    for (uint32_t u = threadIdx.x; u < kHfLutSize; u += blockDim.x) {
+        uint64_t syms = 0;
+        uint32_t tot = 0, cnt = 0, bad = 0, len1 = 0, ends = 0;
+        while (cnt < (uint32_t)kHfMultiMax) {
+            const uint32_t e = first[(u << tot) & (kHfLutSize - 1)];
+            const uint32_t l = e & 0xffu;
+            if (l == 0 || tot + l > (uint32_t)kHfLutBits) break;
+            if (e & (1u << 8)) {
+                if (cnt == 0) {
+                    bad = 1;
+                    tot = len1 = l;
+                    ends = 1u << (l - 1);
+                    cnt = 1;
+                }
+                break;
+            }
+            syms |= (uint64_t)(e >> 16) << (16 * cnt);
+            if (cnt == 0) len1 = l;
+            tot += l;
+            ends |= 1u << (tot - 1);
+            cnt++;
+        }
+        msym[u] = make_uint2((uint32_t)syms, (uint32_t)(syms >> 32));
+        mmeta[u] = tot | cnt << 4 | bad << 7 | len1 << 8 | ends << 12;
+        // counting ignores the error flag and the kHfMultiMax cap
+        uint32_t ctot = 0, ccnt = 0, cends = 0;
+        while (true) {
+            const uint32_t l = first[(u << ctot) & (kHfLutSize - 1)] & 0xffu;
+            if (l == 0 || ctot + l > (uint32_t)kHfLutBits) break;
+            ctot += l;
+            cends |= 1u << (ctot - 1);
+            ccnt++;
+        }
+        cmeta[u] = ctot | ccnt << 4 | cends << 8;
+    }
+    // the shortest code length in the book (lengths l with entry[l + 1] > entry[l])
+    int shortest = 32;
+    for (int l = 30; l >= 1; l--)
+        if (s_entry[l + 1] > s_entry[l]) shortest = l;
+    __syncthreads();
 
+    const HfDecTables tb{msym, mmeta, cmeta, s_first, s_entry, keys, bklen};
     const uint32_t* nbits_g = reinterpret_cast<const uint32_t*>(blob + e2);
     const uint32_t* entry_g = reinterpret_cast<const uint32_t*>(blob + e3);
-    const uint8_t* cells = blob + e4;
-    const uint8_t* blob_end = blob + e5;
     const uint32_t ncells = (e5 - e4) / 4;
     const bool aligned = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint16_t* stage = reinterpret_cast<uint16_t*>(strips + 2 * kHfStage * warp);
+    HfBits r;
+    r.cells = reinterpret_cast<const uint32_t*>(blob + e4);
+    r.ncells = ncells;
     bool bad = false;
 
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pardeg; p += gridDim.x * blockDim.x) {
+    if (shortest > kHfCoopMaxShortest) {
+        // one partition per lane, 32 per ticket
+        while (true) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(err + kHfTicket, 32u);
+            base = __shfl_sync(~0u, base, 0);
+            if (base >= pardeg) break;
+            const uint32_t p = base + lane;
+            if (p < pardeg) {
+                const uint32_t nbit = __ldg(nbits_g + p);
+                const uint64_t o0 = (uint64_t)p * sublen;
+                const uint32_t want = (uint32_t)min((uint64_t)sublen, n - o0);
+                if (nbit == 0) {
+                    if (s_entry[1] == 1) {
+                        const uint16_t k0 = __ldg(keys);
+                        for (uint32_t i = 0; i < want; i++) out[o0 + i] = k0;
+                    } else {
+                        bad = true;
+                    }
+                } else {
+                    r.seek(min(__ldg(entry_g + p), ncells), 0);
+                    uint32_t eacc = 0;
+                    const uint32_t used =
+                        hf_emit(r, tb, want, eacc, bad, [&](uint32_t i, uint32_t s) { out[o0 + i] = (uint16_t)s; });
+                    bad |= ((eacc >> 7) & 1u) != 0 || used != nbit;
+                }
+            }
+        }
+        if (bad) atomicOr(err, kErrMalformed);
+        return;
+    }
+
+    while (true) {
+        uint32_t p = 0;
+        if (lane == 0) p = atomicAdd(err + kHfTicket, 1u);
+        p = __shfl_sync(~0u, p, 0);
+        if (p >= pardeg) break;
         const uint32_t nbit = __ldg(nbits_g + p);
-        const uint32_t c0 = __ldg(entry_g + p);
+        const uint32_t c0 = min(__ldg(entry_g + p), ncells);
         const uint64_t o0 = (uint64_t)p * sublen;
         const uint32_t want = (uint32_t)min((uint64_t)sublen, n - o0);
-        if (nbit == 0 && want > 0 && s_entry[1] == 1) {
-            // a single symbol in the book gets a zero-length code: every
-            // output is that symbol (the reference leaves this case undecoded)
-            const uint16_t k0 = __ldg(keys);
-            for (uint32_t i = 0; i < want; i++) out[o0 + i] = k0;
+        if (nbit == 0) {
+            if (s_entry[1] == 1) {
+                // a single symbol in the book gets a zero-length code: every
+                // output is that symbol (the reference leaves this case undecoded)
+                const uint16_t k0 = __ldg(keys);
+                for (uint32_t i = lane; i < want; i += 32) out[o0 + i] = k0;
+            } else {
+                bad = true;
+            }
             continue;
         }
-        HfBlockReader rd;
-        rd.start(cells + 4 * (size_t)min(c0, ncells), blob_end);
-        uint64_t buf = 0;  // the next `have` bits, MSB-aligned
-        int have = 0;
-        uint32_t used = 0, eacc = 0;
-        while (have <= 32) {
-            buf |= (uint64_t)rd.take() << (32 - have);
-            have += 32;
+        if (nbit > 31u * sublen) {  // longer than want codes of 31 bits
+            bad = true;
+            continue;
         }
-        auto next_symbol = [&]() -> uint32_t {
-            if (have <= 32) {
-                buf |= (uint64_t)rd.take() << (32 - have);
-                have += 32;
-            }
-            const uint32_t e = lut[(uint32_t)(buf >> (64 - kHfLutBits))];
-            int l = (int)(e & 0xffu);
-            uint32_t sym;
-            if (l != 0) {
-                eacc |= e;
-                sym = e >> 16;
-            } else {  // longer than the table: continue the walk
-                l = kHfLutBits + 1;
-                uint32_t v = (uint32_t)(buf >> (64 - l));
-                while (l < 32 && v < s_first[l]) {
-                    l++;
-                    v = (uint32_t)(buf >> (64 - l));
-                }
-                if (l >= 32) {  // no code: flag it and move on by a full word
-                    bad = true;
-                    l = 31;
-                    sym = 0;
-                } else {
-                    const int k = s_entry[l] + (int)v - (int)s_first[l];
-                    const bool kin = k >= 0 && k < (int)bklen;
-                    bad |= !kin;
-                    sym = kin ? __ldg(keys + k) : 0u;
+        const uint32_t seg = max(32u, (nbit + 31) / 32), nact = (nbit + seg - 1) / seg;
+        const bool act = lane < nact;
+        const uint32_t sj = min(lane * seg, nbit), send = min(sj + seg, nbit);
+        // the next lane's segment bits that a shared start may fall in
+        const uint32_t lim = min(64u, min(send + seg, nbit) - send);
+        uint32_t e = nbit, cnt = 0;
+        uint64_t F = 0, T = 0;
+        if (act) {
+            r.seek(c0, sj);
+            hf_count(r, tb, sj, send, sj, e, cnt, F);
+        }
+        const uint64_t Fn = __shfl_down_sync(~0u, F, 1);
+        // lanes in `go` decode on from their end, noting true starts for the
+        // next lane until one is in its F
+        auto extend = [&](bool go) {
+            uint32_t x = e;
+            T = 0;
+            while (__any_sync(~0u, go)) {
+                if (go) {
+                    uint32_t tot, c, E;
+                    hf_probe(r.win(), tb, tot, c, E);
+                    T |= (uint64_t)hf_starts(tot, E) << (x - send);
+                    r.advance(tot);
+                    x += tot;
+                    go = (T & Fn) == 0 && x < send + lim;
                 }
             }
-            buf <<= l;
-            have -= l;
-            used += l;
-            return sym;
         };
-        uint32_t i = 0;
-        if (aligned) {
-            for (; i + 16 <= want; i += 16) {
-                uint32_t w[8];
+        extend(act && lane + 1 < nact && e < send + lim);
+        // lane j's count from its first start shared with lane j - 1's true starts
+        auto check = [&](uint64_t tprev, uint32_t& ct) -> bool {
+            const uint64_t both = tprev & F;
+            if (!both) return false;
+            const uint32_t q = (uint32_t)__ffsll((long long)both) - 1;
+            if (sj + q >= send) return false;
+            const uint64_t below = (1ull << q) - 1ull;
+            ct = cnt - (uint32_t)__popcll(F & below) + (uint32_t)__popcll(tprev & below);
+            return true;
+        };
+        uint32_t ct = cnt;
+        bool good = true;
+        {
+            const uint64_t tprev = __shfl_up_sync(~0u, T, 1);
+            if (act && lane > 0) good = check(tprev, ct);
+        }
+        uint32_t fails = __ballot_sync(~0u, !good);
+        while (fails) {
+            const uint32_t k = (uint32_t)__ffs(fails) - 1;  // lanes below k are true
+            const uint32_t tk = __shfl_sync(~0u, e, k - 1);
+            if (lane == k) {
+                r.seek(c0, tk);
+                uint64_t Fk;
+                hf_count(r, tb, tk, send, sj, e, cnt, Fk);
+                ct = cnt;
+            }
+            extend(lane == k && k + 1 < nact && e < send + lim);
+            fails &= ~(1u << k);
+            const uint64_t tnew = __shfl_sync(~0u, T, k);
+            bool recheck_fail = false;
+            if (lane == k + 1 && act && !((fails >> lane) & 1u)) recheck_fail = !check(tnew, ct);
+            fails |= __ballot_sync(~0u, recheck_fail);
+        }
+        // place each lane's symbols
+        const uint32_t mine = act ? ct : 0u;
+        uint32_t inc = mine;
 #pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const uint32_t sym = next_symbol();
-                    if (j & 1) w[j >> 1] |= sym << 16;
-                    else w[j >> 1] = sym;
-                }
-                uint4* d4 = reinterpret_cast<uint4*>(out + o0 + i);
-                d4[0] = make_uint4(w[0], w[1], w[2], w[3]);
-                d4[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(~0u, inc, d);
+            if (lane >= (uint32_t)d) inc += y;
+        }
+        const uint32_t total = __shfl_sync(~0u, inc, 31);
+        const uint32_t elast = __shfl_sync(~0u, e, nact - 1);
+        const uint32_t tstart = __shfl_up_sync(~0u, e, 1);
+        if (total != want || elast != nbit) {
+            bad = true;
+            continue;
+        }
+        if (act) {
+            const uint32_t t0 = lane == 0 ? 0u : tstart;
+            const uint32_t off = inc - mine;
+            if (mine) {
+                r.seek(c0, t0);
+                uint32_t eacc = 0;
+                const uint32_t used =
+                    hf_emit(r, tb, mine, eacc, bad, [&](uint32_t i, uint32_t s) { stage[off + i] = (uint16_t)s; });
+                bad |= ((eacc >> 7) & 1u) != 0 || t0 + used != e;
+            } else {
+                bad |= t0 != e;
             }
         }
-        for (; i < want; i++) out[o0 + i] = (uint16_t)next_symbol();
-        bad |= ((eacc >> 8) & 1u) != 0 || used != nbit;
+        __syncwarp();
+        if (aligned) {
+            const uint32_t n8 = want >> 3;
+            uint4* d4 = reinterpret_cast<uint4*>(out + o0);
+            const uint4* s4 = reinterpret_cast<const uint4*>(stage);
+            for (uint32_t i = lane; i < n8; i += 32) d4[i] = s4[i];
+            for (uint32_t i = (n8 << 3) + lane; i < want; i += 32) out[o0 + i] = stage[i];
+        } else {
+            for (uint32_t i = lane; i < want; i += 32) out[o0 + i] = stage[i];
+        }
+        __syncwarp();
     }
     if (bad) atomicOr(err, kErrMalformed);
 }
@@ -446,10 +714,12 @@ int launch_hf_decode(const uint8_t* blob, uint64_t blob_bytes, uint64_t n, uint3
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const uint32_t need = (pardeg + kHfDecThreads - 1) / kHfDecThreads;
-    const uint32_t grid = min(need, (uint32_t)sms * 4u);
+    // two CTAs per SM, fewer for small inputs; warps take partitions from a counter
+    const uint32_t grid = max(1u, min(2u * (uint32_t)sms, (pardeg + kHfDecWarps - 1) / kHfDecWarps));
+    cudaError_t e = cudaFuncSetAttribute(hf_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHfDecSmem);
+    if (e != cudaSuccess) return (int)e;
     TraceScope ts(s, "hf_decode");
-    hf_decode_kernel<<<grid ? grid : 1u, kHfDecThreads, 0, s>>>(blob, blob_bytes, n, bklen, out, err);
+    hf_decode_kernel<<<grid, kHfDecThreads, kHfDecSmem, s>>>(blob, blob_bytes, n, bklen, out, err);
     return (int)cudaGetLastError();
 }
 
