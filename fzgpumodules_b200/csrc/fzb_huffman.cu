@@ -236,8 +236,9 @@ __global__ void hf_concat_kernel(const uint32_t* __restrict__ slots, const uint3
 // per lane instead, straight to the output.
 // A well-formed partition decodes its want symbols in exactly nbit bits;
 // anything else (a length past 31, a table index past the book, a bit count
-// that does not match) raises kErrMalformed.  err[kHfTicket] (zeroed with
-// the error word) hands partitions to warps.
+// that does not match) raises kErrMalformed.  CTA b owns partitions b, b + G,
+// b + 2G, ... (G CTAs), spread over the field, and its warps take them in
+// turn from a shared-memory counter, so no global counter is contended.
 constexpr int kHfLutBits = 12;
 constexpr uint32_t kHfLutSize = 1u << kHfLutBits;
 constexpr int kHfMultiMax = 4;
@@ -245,7 +246,6 @@ constexpr int kHfDecWarps = 16;
 constexpr int kHfDecThreads = 32 * kHfDecWarps;
 constexpr int kHfCoopMaxShortest = 4;
 constexpr uint32_t kHfStage = kHfSublenFine;  // symbols staged per warp
-constexpr uint32_t kHfTicket = 8;
 // symbols (8 B), meta (4 B) and counts (4 B) per window, then the warps'
 // staging strips, which hold the first-code table while the CTA builds
 constexpr size_t kHfDecSmem = 16 * (size_t)kHfLutSize + 2 * (size_t)kHfStage * kHfDecWarps;
@@ -331,6 +331,17 @@ __device__ __forceinline__ void hf_count(HfBits& r, const HfDecTables& t, uint32
     uint32_t pos = start;
     cnt = 0;
     F = 0;
+    // while a whole window lies before s_end every code in it counts (a
+    // longer code is a single code, so its end is the boundary sought)
+    while (pos + kHfLutBits <= s_end) {
+        uint32_t tot, c, E;
+        hf_probe(r.win(), t, tot, c, E);
+        const uint32_t d = pos - rec;
+        if (d < 64) F |= (uint64_t)hf_starts(tot, E) << d;
+        cnt += c;
+        r.advance(tot);
+        pos += tot;
+    }
     while (pos < s_end) {
         uint32_t tot, c, E;
         hf_probe(r.win(), t, tot, c, E);
@@ -355,6 +366,42 @@ template <class Put>
 __device__ __forceinline__ uint32_t hf_emit(HfBits& r, const HfDecTables& t, uint32_t count, uint32_t& eacc,
                                             bool& bad, Put put) {
     uint32_t i = 0, used = 0;
+    // while kHfMultiMax symbols remain every probe's codes are all taken, and
+    // symbols past a probe's count are overwritten by the next probe
+    while (i + kHfMultiMax <= count) {
+        const uint32_t w = r.win();
+        const uint32_t u = w >> (32 - kHfLutBits);
+        const uint32_t m = t.meta[u];
+        uint32_t cm = (m >> 4) & 7u;
+        uint32_t adv = m & 15u;
+        if (cm == 0) {
+            uint32_t v;
+            int l = hf_walk(w, t.first, v);
+            uint32_t s = 0;
+            if (l >= 32) {  // no code: flag it and move on by 31 bits
+                bad = true;
+                l = 31;
+            } else {
+                const int k = t.entry[l] + (int)v - (int)t.first[l];
+                const bool kin = k >= 0 && k < (int)t.bklen;
+                bad |= !kin;
+                s = kin ? __ldg(t.keys + k) : 0u;
+            }
+            put(i, s);
+            cm = 1;
+            adv = (uint32_t)l;
+        } else {
+            const uint2 sy = t.sym[u];
+            put(i, sy.x);
+            put(i + 1, sy.x >> 16);
+            put(i + 2, sy.y);
+            put(i + 3, sy.y >> 16);
+            eacc |= m;
+        }
+        i += cm;
+        r.advance(adv);
+        used += adv;
+    }
     while (i < count) {
         const uint32_t w = r.win();
         const uint32_t u = w >> (32 - kHfLutBits);
@@ -406,6 +453,7 @@ __global__ void __launch_bounds__(kHfDecThreads, 2)
                      uint16_t* __restrict__ out, uint32_t* err) {
     __shared__ uint32_t s_first[32];
     __shared__ int s_entry[32];
+    __shared__ uint32_t s_next;  // the CTA's next partition (or group of 32), in its own numbering
     extern __shared__ __align__(16) uint8_t hf_smem[];
     uint2* msym = reinterpret_cast<uint2*>(hf_smem);
     uint32_t* mmeta = reinterpret_cast<uint32_t*>(hf_smem + 8 * kHfLutSize);
@@ -431,6 +479,7 @@ __global__ void __launch_bounds__(kHfDecThreads, 2)
         s_first[threadIdx.x] = (uint32_t)rb[threadIdx.x];
         s_entry[threadIdx.x] = rb[32 + threadIdx.x];
     }
+    if (threadIdx.x == 0) s_next = 0;
     const uint16_t* keys = reinterpret_cast<const uint16_t*>(blob + e1 + 256);
     __syncthreads();
     // first-code table: symbol << 16 | bad << 8 | length (length 0: a longer code)
@@ -507,11 +556,11 @@ __global__ void __launch_bounds__(kHfDecThreads, 2)
     if (shortest > kHfCoopMaxShortest) {
         // one partition per lane, 32 per ticket
         while (true) {
-            uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(err + kHfTicket, 32u);
-            base = __shfl_sync(~0u, base, 0);
-            if (base >= pardeg) break;
-            const uint32_t p = base + lane;
+            uint32_t g = 0;
+            if (lane == 0) g = blockIdx.x + atomicAdd(&s_next, 1u) * gridDim.x;
+            g = __shfl_sync(~0u, g, 0);
+            if (g >= (pardeg + 31) / 32) break;
+            const uint32_t p = 32 * g + lane;
             if (p < pardeg) {
                 const uint32_t nbit = __ldg(nbits_g + p);
                 const uint64_t o0 = (uint64_t)p * sublen;
@@ -538,7 +587,7 @@ __global__ void __launch_bounds__(kHfDecThreads, 2)
 
     while (true) {
         uint32_t p = 0;
-        if (lane == 0) p = atomicAdd(err + kHfTicket, 1u);
+        if (lane == 0) p = blockIdx.x + atomicAdd(&s_next, 1u) * gridDim.x;
         p = __shfl_sync(~0u, p, 0);
         if (p >= pardeg) break;
         const uint32_t nbit = __ldg(nbits_g + p);
