@@ -787,7 +787,7 @@ int huff_encode_sub(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint
     CK(cudaMemsetAsync(w.err, 0, kCtrlBytes, s));
     return launch_hf_encode(d_in, n, d_bk4, bklen, sublen, d_revbook, static_cast<uint8_t*>(d_out),
                             reinterpret_cast<unsigned long long*>(d_out_size), w.slots, w.par_nbit,
-                            w.par_ncell, w.par_entry, w.tiles, w.ncell_total, sm_count(), s) == 0
+                            w.par_ncell, w.par_entry, w.tiles, w.ncell_total, w.err, sm_count(), s) == 0
                ? FZB_OK : FZB_E_CUDA;
 }
 

@@ -15,26 +15,27 @@
 // ReVISIT-lite kernel (hf_kernels.cu:145-250) packs four codes of at most 8
 // bits per thread and merges the shards into exactly those cells; when the
 // longest code is over 8 bits the reference deflates coarsely at sublen 1024
-// (hf_hl.cc:69-103).  Here one kernel serves both modes: a thread takes
-// sublen/256 consecutive symbols and, when they fit one 32-bit word (every
-// code at most 32/(sublen/256) bits), packs them and ORs the word into the
-// cells; otherwise each code is ORed in on its own.
+// (hf_hl.cc:69-103).  Here one kernel serves both modes: a warp codes a
+// partition, each lane sublen/32 consecutive symbols packed at its scanned
+// bit offset.
 #include "fzb_kernels.cuh"
 
 namespace fzb {
 
-constexpr int kHfThreads = 256;  // sublen / 256 symbols per thread per partition
 constexpr uint32_t kHfSmemBook = 16384;  // books up to this size are staged in shared memory
 
-// Privatised histogram: each CTA counts into shared memory, then merges.
-// Symbols >= bklen are skipped (histogram.cu:47-51).
+// Privatised histogram: each CTA counts into `copies` shared-memory copies
+// (warp w into copy w % copies, so a frequent symbol's atomics spread), then
+// merges.  A thread adds each run of equal symbols among its eight with one
+// atomic.  Symbols >= bklen are skipped (histogram.cu:47-51).
 __global__ void __launch_bounds__(512) hf_histogram_kernel(const uint16_t* __restrict__ in, uint64_t n,
-                                                           uint32_t bklen, uint32_t* __restrict__ freq) {
+                                                           uint32_t bklen, uint32_t copies,
+                                                           uint32_t* __restrict__ freq) {
     extern __shared__ uint32_t hs[];
     const bool priv = bklen <= kHfSmemBook;  // larger books count straight into freq
-    uint32_t* h = priv ? hs : freq;
+    uint32_t* h = priv ? hs + bklen * ((threadIdx.x >> 5) % copies) : freq;
     if (priv)
-        for (uint32_t i = threadIdx.x; i < bklen; i += blockDim.x) h[i] = 0;
+        for (uint32_t i = threadIdx.x; i < bklen * copies; i += blockDim.x) hs[i] = 0;
     __syncthreads();
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const bool vec = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
@@ -43,12 +44,18 @@ __global__ void __launch_bounds__(512) hf_histogram_kernel(const uint16_t* __res
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
         const uint4 v = __ldg(in8 + i);
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        uint32_t cur = w[0] & 0xffffu, run = 0;
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const uint32_t a = w[k] & 0xffffu, b = w[k] >> 16;
-            if (a < bklen) atomicAdd(&h[a], 1u);
-            if (b < bklen) atomicAdd(&h[b], 1u);
+        for (int k = 0; k < 8; k++) {
+            const uint32_t a = (w[k >> 1] >> (16 * (k & 1))) & 0xffffu;
+            if (a != cur) {
+                if (cur < bklen) atomicAdd(&h[cur], run);
+                cur = a;
+                run = 0;
+            }
+            run++;
         }
+        if (cur < bklen) atomicAdd(&h[cur], run);
     }
     for (uint64_t i = 8 * nv + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t a = in[i];
@@ -56,131 +63,127 @@ __global__ void __launch_bounds__(512) hf_histogram_kernel(const uint16_t* __res
     }
     if (!priv) return;
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < bklen; i += blockDim.x)
-        if (h[i]) atomicAdd(&freq[i], h[i]);
-}
-
-// One CTA per partition group (persistent loop): look up the codewords,
-// prefix-sum their lengths, OR the codes into shared-memory cells at their
-// bit offsets, write the cells to the partition's slot.
-template <int SUB>
-__global__ void __launch_bounds__(kHfThreads) hf_encode_kernel(const uint16_t* __restrict__ in, uint64_t n,
-                                                               const uint32_t* __restrict__ bk4, uint32_t bklen,
-                                                               uint32_t pardeg, uint32_t* __restrict__ slots,
-                                                               uint32_t* __restrict__ par_nbit,
-                                                               uint32_t* __restrict__ par_ncell) {
-    constexpr int PER = SUB / kHfThreads;  // 3 (coarse) or 4 (fine)
-    extern __shared__ uint32_t sm[];
-    const bool staged = bklen <= kHfSmemBook;
-    uint32_t* cells = sm;                             // SUB words
-    const uint32_t* book = staged ? sm + SUB : bk4;   // bklen words when staged
-    __shared__ uint32_t ws[16];
-    uint32_t lmax = 0;
-    if (staged)
-        for (uint32_t i = threadIdx.x; i < bklen; i += blockDim.x) {
-            const uint32_t v = bk4[i];
-            sm[SUB + i] = v;
-            lmax = max(lmax, v >> 27);
-        }
-    // the PER codes of a thread fit one word when every code is short enough
-    const bool packed = staged && !__syncthreads_or(lmax * PER > 32);
-    const int t = threadIdx.x;
-    for (uint32_t p = blockIdx.x; p < pardeg; p += gridDim.x) {
-        for (int i = t; i < SUB; i += kHfThreads) cells[i] = 0;
-        __syncthreads();
-        const uint64_t base = (uint64_t)p * SUB + PER * t;
-        uint32_t w[PER], bits = 0;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            w[k] = 0;
-            if (base + k < n) {
-                const uint32_t sym = in[base + k];
-                w[k] = (sym < bklen) ? book[sym] : 0u;
-            }
-            bits += w[k] >> 27;
-        }
-        uint32_t total;
-        uint32_t off = block_excl_scan(bits, ws, &total);
-        if (packed) {  // MSB-first concatenation of the thread's codes in one word
-            uint32_t acc = 0, nb = 0;
-#pragma unroll
-            for (int k = 0; k < PER; k++) {
-                const uint32_t len = w[k] >> 27;
-                if (len) acc |= (w[k] & 0x7ffffffu) << (32 - nb - len);
-                nb += len;
-            }
-            if (nb) {
-                const uint32_t cell = off >> 5, pos = off & 31;
-                atomicOr(&cells[cell], acc >> pos);
-                if (pos + nb > 32) atomicOr(&cells[cell + 1], acc << (32 - pos));
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < PER; k++) {
-                const uint32_t len = w[k] >> 27, code = w[k] & 0x7ffffffu;
-                if (len) {
-                    const uint32_t cell = off >> 5, pos = off & 31;  // pos = bits already used in the cell
-                    if (pos + len <= 32) {
-                        atomicOr(&cells[cell], code << (32 - pos - len));
-                    } else {
-                        const uint32_t spill = pos + len - 32;  // bits going to the next cell
-                        atomicOr(&cells[cell], code >> spill);
-                        atomicOr(&cells[cell + 1], code << (32 - spill));
-                    }
-                }
-                off += len;
-            }
-        }
-        __syncthreads();
-        const uint32_t ncell = (total + 31) / 32;
-        uint32_t* dst = slots + (size_t)p * SUB;
-        for (uint32_t i = t; i < ncell; i += kHfThreads) dst[i] = cells[i];
-        if (t == 0) {
-            par_nbit[p] = total;
-            par_ncell[p] = ncell;
-        }
-        __syncthreads();
+    for (uint32_t i = threadIdx.x; i < bklen; i += blockDim.x) {
+        uint32_t t = 0;
+        for (uint32_t c = 0; c < copies; c++) t += hs[c * bklen + i];
+        if (t) atomicAdd(&freq[i], t);
     }
 }
 
-// Header + revbook + par_nbit + par_entry (one CTA of 1024 threads).
-// par_entry must already hold the exclusive scan of par_ncell and
-// *ncell_total its sum.
+// Encode, a warp per partition (static interleave over all warps).  Lane l
+// codes the partition's symbols l*PER .. l*PER + PER - 1 (PER = SUB / 32):
+// it looks up their codewords, a warp scan of the code lengths gives its
+// first bit, and it packs its codes MSB-first into 32-bit words that it ORs
+// into the warp's shared-memory cells (only a lane's first and last word
+// can be shared with a neighbour).  The warp then copies the cells to the
+// partition's slot and clears them for its next partition.
+constexpr int kHfEncWarps = 8;
+
+template <int SUB>
+__global__ void __launch_bounds__(32 * kHfEncWarps) hf_encode_kernel(const uint16_t* __restrict__ in, uint64_t n,
+                                                                     const uint32_t* __restrict__ bk4, uint32_t bklen,
+                                                                     uint32_t pardeg, uint32_t* __restrict__ slots,
+                                                                     uint32_t* __restrict__ par_nbit,
+                                                                     uint32_t* __restrict__ par_ncell) {
+    constexpr int PER = SUB / 32;  // 24 (coarse) or 32 (fine)
+    static_assert(PER % 8 == 0, "whole 16-byte loads per lane");
+    extern __shared__ uint32_t sm[];
+    const bool staged = bklen <= kHfSmemBook;
+    const uint32_t* book = staged ? sm + kHfEncWarps * SUB : bk4;  // bklen words when staged
+    if (staged)
+        for (uint32_t i = threadIdx.x; i < bklen; i += blockDim.x) sm[kHfEncWarps * SUB + i] = bk4[i];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t* cells = sm + warp * SUB;
+    for (uint32_t i = lane; i < (uint32_t)SUB; i += 32) cells[i] = 0;
+    __syncthreads();
+    const bool vec = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
+    for (uint32_t p = blockIdx.x * kHfEncWarps + warp; p < pardeg; p += gridDim.x * kHfEncWarps) {
+        const uint64_t base = (uint64_t)p * SUB + (uint64_t)PER * lane;
+        uint32_t w[PER];
+        if (vec && base + PER <= n) {
+            const uint4* src = reinterpret_cast<const uint4*>(in + base);
+#pragma unroll
+            for (int q = 0; q < PER / 8; q++) {
+                const uint4 v = __ldg(src + q);
+                const uint32_t h[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    w[8 * q + 2 * k] = h[k] & 0xffffu;
+                    w[8 * q + 2 * k + 1] = h[k] >> 16;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < PER; k++) w[k] = base + k < n ? (uint32_t)in[base + k] : 0xffffffffu;
+        }
+        uint32_t bits = 0;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            w[k] = w[k] < bklen ? book[w[k]] : 0u;  // symbols past the book (or the input) are not coded
+            bits += w[k] >> 27;
+        }
+        uint32_t inc = bits;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(~0u, inc, d);
+            if (lane >= (uint32_t)d) inc += y;
+        }
+        const uint32_t total = __shfl_sync(~0u, inc, 31);
+        const uint32_t off = inc - bits;
+        uint32_t cw = off >> 5, nb = off & 31u;  // acc holds the cell's first nb bits, MSB-aligned
+        uint64_t acc = 0;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t len = w[k] >> 27;
+            if (len) acc |= (uint64_t)(w[k] & 0x7ffffffu) << (64 - nb - len);
+            nb += len;
+            if (nb >= 32) {
+                atomicOr(&cells[cw], (uint32_t)(acc >> 32));
+                cw++;
+                acc <<= 32;
+                nb -= 32;
+            }
+        }
+        if (nb) atomicOr(&cells[cw], (uint32_t)(acc >> 32));  // zero bits of other lanes OR in harmlessly
+        __syncwarp();
+        const uint32_t ncell = (total + 31) / 32;
+        uint32_t* dst = slots + (size_t)p * SUB;
+        for (uint32_t i = lane; i < ncell; i += 32) {
+            dst[i] = cells[i];
+            cells[i] = 0;
+        }
+        if (lane == 0) {
+            par_nbit[p] = total;
+            par_ncell[p] = ncell;
+        }
+        __syncwarp();
+    }
+}
+
+// Header + revbook (one CTA of 1024 threads).  hf_concat_kernel adds up the
+// total bit count and writes par_nbit and par_entry.
+// *ncell_total must already hold the cell count.
 __global__ void __launch_bounds__(1024) hf_header_kernel(uint8_t* __restrict__ out, uint32_t bklen,
                                                          uint32_t sublen, uint32_t pardeg, uint64_t n,
                                                          const uint8_t* __restrict__ revbook,
                                                          uint32_t revbook_bytes,
-                                                         const uint32_t* __restrict__ par_nbit,
-                                                         const uint32_t* __restrict__ par_entry,
                                                          const uint32_t* __restrict__ ncell_total,
                                                          unsigned long long* __restrict__ out_size) {
-    __shared__ unsigned long long part[32];
     const uint32_t e1 = 128, e2 = e1 + revbook_bytes, e3 = e2 + 4 * pardeg, e4 = e3 + 4 * pardeg;
-    unsigned long long nbit = 0;
-    for (uint32_t p = threadIdx.x; p < pardeg; p += blockDim.x) {
-        const uint32_t v = par_nbit[p];
-        nbit += v;
-        reinterpret_cast<uint32_t*>(out + e2)[p] = v;
-        reinterpret_cast<uint32_t*>(out + e3)[p] = par_entry[p];
-    }
-#pragma unroll
-    for (int d = 16; d >= 1; d >>= 1) nbit += __shfl_xor_sync(0xffffffffu, nbit, d);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = nbit;
     for (uint32_t i = threadIdx.x; i < revbook_bytes; i += blockDim.x) out[e1 + i] = revbook[i];
-    __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned long long tot = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); i++) tot += part[i];
         const uint64_t ncell = *ncell_total;
         uint32_t* h32 = reinterpret_cast<uint32_t*>(out);
         for (int i = 0; i < 32; i++) h32[i] = 0;
         h32[0] = bklen & 0xffffu;
         h32[1] = sublen;
         h32[2] = pardeg;
-        uint64_t* h64 = reinterpret_cast<uint64_t*>(out + 16);
-        h64[0] = n;
-        h64[1] = tot;
-        h64[2] = ncell;
+        // 64-bit fields as word pairs (the blob is only 4-byte aligned)
+        h32[4] = (uint32_t)n;
+        h32[5] = (uint32_t)(n >> 32);
+        h32[6] = h32[7] = 0;  // total bits, written by hf_concat_kernel
+        h32[8] = (uint32_t)ncell;
+        h32[9] = (uint32_t)(ncell >> 32);
         uint32_t* ent = reinterpret_cast<uint32_t*>(out + 40);
         ent[0] = 0;
         ent[1] = e1;
@@ -192,13 +195,74 @@ __global__ void __launch_bounds__(1024) hf_header_kernel(uint8_t* __restrict__ o
     }
 }
 
-// Partition cells from their slots to the bitstream (u32 aligned).
-__global__ void hf_concat_kernel(const uint32_t* __restrict__ slots, const uint32_t* __restrict__ par_ncell,
-                                 const uint32_t* __restrict__ par_entry, uint32_t pardeg, uint32_t sublen,
-                                 uint32_t* __restrict__ bitstream) {
-    for (uint32_t p = blockIdx.x; p < pardeg; p += gridDim.x) {
-        const uint32_t nc = par_ncell[p], e = par_entry[p];
-        for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) bitstream[e + i] = slots[(size_t)p * sublen + i];
+// Partition cells from their slots to the bitstream (u32 aligned), with
+// the par_nbit and par_entry words and the total bit count.  A warp takes 32
+// consecutive partitions, lane l holding the header of the l-th, and copies
+// four partitions at a time so that their loads are in flight together.
+constexpr int kHfCatWarps = 8;
+constexpr int kHfCatWords = 96;  // words per partition copied in the unrolled pass
+
+__global__ void __launch_bounds__(32 * kHfCatWarps) hf_concat_kernel(
+    const uint32_t* __restrict__ slots, const uint32_t* __restrict__ par_nbit,
+    const uint32_t* __restrict__ par_ncell, const uint32_t* __restrict__ par_entry, uint32_t pardeg, uint32_t sublen,
+    uint32_t* __restrict__ out_nbit, uint32_t* __restrict__ out_entry, uint32_t* __restrict__ bitstream,
+    uint32_t* __restrict__ ctrl, uint32_t* __restrict__ head_nbit) {
+    __shared__ unsigned long long s_bits[kHfCatWarps];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    unsigned long long bits = 0;
+    for (uint32_t g = blockIdx.x * kHfCatWarps + warp; 32ull * g < pardeg; g += gridDim.x * kHfCatWarps) {
+        const uint32_t pl = 32 * g + lane;
+        uint32_t nc = 0, e = 0;
+        if (pl < pardeg) {
+            const uint32_t nb = par_nbit[pl];
+            nc = par_ncell[pl];
+            e = par_entry[pl];
+            out_nbit[pl] = nb;
+            out_entry[pl] = e;
+            bits += nb;
+        }
+        for (int j = 0; j < 32; j += 4) {
+            uint32_t v[4][kHfCatWords / 32];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t ncj = __shfl_sync(~0u, nc, j + q);
+                const uint32_t* src = slots + (size_t)(32 * g + j + q) * sublen;
+#pragma unroll
+                for (int r = 0; r < kHfCatWords / 32; r++) {
+                    const uint32_t i = lane + 32 * r;
+                    v[q][r] = i < ncj ? src[i] : 0u;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t ncj = __shfl_sync(~0u, nc, j + q), ej = __shfl_sync(~0u, e, j + q);
+#pragma unroll
+                for (int r = 0; r < kHfCatWords / 32; r++) {
+                    const uint32_t i = lane + 32 * r;
+                    if (i < ncj) bitstream[ej + i] = v[q][r];
+                }
+                const uint32_t* src = slots + (size_t)(32 * g + j + q) * sublen;
+                for (uint32_t i = kHfCatWords + lane; i < ncj; i += 32) bitstream[ej + i] = src[i];
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) bits += __shfl_xor_sync(~0u, bits, d);
+    if (lane == 0) s_bits[warp] = bits;
+    __syncthreads();
+    // the CTA's bits (under 2^32) go into the 64-bit count ctrl[2] (low) /
+    // ctrl[3] (high); the last CTA writes it to the header as two words
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kHfCatWarps; w++) t += s_bits[w];
+        const uint32_t lo = (uint32_t)t, old = atomicAdd(&ctrl[2], lo);
+        if (old + lo < old) atomicAdd(&ctrl[3], 1u);
+        __threadfence();
+        if (atomicAdd(&ctrl[4], 1u) == gridDim.x - 1) {
+            __threadfence();
+            head_nbit[0] = atomicAdd(&ctrl[2], 0u);
+            head_nbit[1] = atomicAdd(&ctrl[3], 0u);
+        }
     }
 }
 
@@ -717,31 +781,33 @@ __global__ void __launch_bounds__(kHfDecThreads, 2)
 int launch_hf_histogram(const uint16_t* in, uint64_t n, uint32_t bklen, uint32_t* freq, int sms,
                         cudaStream_t s) {
     cudaMemsetAsync(freq, 0, 4 * (size_t)bklen, s);
-    const int smem = bklen <= kHfSmemBook ? 4 * (int)bklen : 0;
+    const uint32_t copies = bklen <= 4096 ? 4u : 1u;
+    const int smem = bklen <= kHfSmemBook ? 4 * (int)(bklen * copies) : 0;
     cudaFuncSetAttribute(hf_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    hf_histogram_kernel<<<2 * sms, 512, smem, s>>>(in, n, bklen, freq);
+    hf_histogram_kernel<<<2 * sms, 512, smem, s>>>(in, n, bklen, copies, freq);
     return (int)cudaGetLastError();
 }
 
 int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32_t bklen, uint32_t sublen,
                      const uint8_t* d_revbook, uint8_t* out, unsigned long long* out_size,
                      uint32_t* slots, uint32_t* par_nbit, uint32_t* par_ncell, uint32_t* par_entry,
-                     uint32_t* tiles, uint32_t* ncell_total, int sms, cudaStream_t s) {
+                     uint32_t* tiles, uint32_t* ncell_total, uint32_t* ctrl, int sms, cudaStream_t s) {
     if (sublen != (uint32_t)kHfSublen && sublen != (uint32_t)kHfSublenFine) return (int)cudaErrorInvalidValue;
     const uint32_t pardeg = (uint32_t)((n - 1) / sublen + 1);
-    const int smem = 4 * ((int)sublen + (bklen <= kHfSmemBook ? (int)bklen : 0));
-    const unsigned grid = (unsigned)min((uint64_t)pardeg, (uint64_t)8 * sms);
+    const int smem = 4 * (kHfEncWarps * (int)sublen + (bklen <= kHfSmemBook ? (int)bklen : 0));
+    const unsigned grid =
+        (unsigned)max((uint64_t)1, min((uint64_t)(pardeg + kHfEncWarps - 1) / kHfEncWarps, (uint64_t)4 * sms));
     cudaError_t e;
     if (sublen == (uint32_t)kHfSublenFine) {
         e = cudaFuncSetAttribute(hf_encode_kernel<kHfSublenFine>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return (int)e;
-        hf_encode_kernel<kHfSublenFine><<<grid, kHfThreads, smem, s>>>(in, n, bk4, bklen, pardeg, slots, par_nbit,
-                                                                       par_ncell);
+        hf_encode_kernel<kHfSublenFine><<<grid, 32 * kHfEncWarps, smem, s>>>(in, n, bk4, bklen, pardeg, slots,
+                                                                             par_nbit, par_ncell);
     } else {
         e = cudaFuncSetAttribute(hf_encode_kernel<kHfSublen>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return (int)e;
-        hf_encode_kernel<kHfSublen><<<grid, kHfThreads, smem, s>>>(in, n, bk4, bklen, pardeg, slots, par_nbit,
-                                                                   par_ncell);
+        hf_encode_kernel<kHfSublen><<<grid, 32 * kHfEncWarps, smem, s>>>(in, n, bk4, bklen, pardeg, slots, par_nbit,
+                                                                         par_ncell);
     }
     ScanSrc sc{};
     sc.base = par_ncell;
@@ -749,11 +815,13 @@ int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32
     int rc = launch_scan_u32(sc, par_entry, tiles, ncell_total, s);
     if (rc) return rc;
     const uint32_t rb = 256 + 2 * bklen;
-    hf_header_kernel<<<1, 1024, 0, s>>>(out, bklen, sublen, pardeg, n, d_revbook, rb, par_nbit, par_entry,
-                                       ncell_total, out_size);
+    hf_header_kernel<<<1, 1024, 0, s>>>(out, bklen, sublen, pardeg, n, d_revbook, rb, ncell_total, out_size);
+    uint32_t* out_nbit = reinterpret_cast<uint32_t*>(out + 128 + rb);
     uint32_t* bitstream = reinterpret_cast<uint32_t*>(out + 128 + rb + 8 * (size_t)pardeg);
-    hf_concat_kernel<<<(unsigned)min((uint64_t)pardeg, (uint64_t)8 * sms), 128, 0, s>>>(
-        slots, par_ncell, par_entry, pardeg, sublen, bitstream);
+    const uint32_t groups = (pardeg + 31) / 32;
+    hf_concat_kernel<<<(groups + kHfCatWarps - 1) / kHfCatWarps, 32 * kHfCatWarps, 0, s>>>(
+        slots, par_nbit, par_ncell, par_entry, pardeg, sublen, out_nbit, out_nbit + pardeg, bitstream, ctrl,
+        reinterpret_cast<uint32_t*>(out + 24));
     return (int)cudaGetLastError();
 }
 

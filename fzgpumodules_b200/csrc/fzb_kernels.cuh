@@ -301,7 +301,7 @@ int launch_hf_histogram(const uint16_t* in, uint64_t n, uint32_t bklen, uint32_t
 int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32_t bklen, uint32_t sublen,
                      const uint8_t* d_revbook, uint8_t* out, unsigned long long* out_size,
                      uint32_t* slots, uint32_t* par_nbit, uint32_t* par_ncell, uint32_t* par_entry,
-                     uint32_t* tiles, uint32_t* ncell_total, int sms, cudaStream_t s);
+                     uint32_t* tiles, uint32_t* ncell_total, uint32_t* ctrl, int sms, cudaStream_t s);
 int launch_hf_decode(const uint8_t* blob, uint64_t blob_bytes, uint64_t n, uint32_t bklen,
                      uint16_t* out, uint32_t* err, cudaStream_t s);
 int build_huffman_book(const uint32_t* freq, uint32_t bklen, uint32_t* bk4, uint8_t* revbook);
