@@ -126,11 +126,25 @@ def _peak():
         return 6650.0, "fallback"
 
 
+def _traffic_per_element(kernel: str):
+    """DRAM bytes per element of `kernel` from the committed ncu summary
+    (profiles/traffic.json), or None."""
+    import json as _j
+    import os as _o
+    try:
+        with open(_o.path.join(_o.path.dirname(_o.path.dirname(_o.path.abspath(__file__))), "profiles",
+                               "traffic.json")) as f:
+            return float(_j.load(f)[kernel]["bytes_per_element"])
+    except Exception:
+        return None
+
+
 def c3_summary(dev, steps: int, warmup: int) -> dict:
     """C3: LorenzoQuant 2-D (ABS 1e-3, radius 512, zigzag) -> Huffman (bklen
     1024, coarse) on the 8192^2 fractal field.  Times each step, checks the
     decode, and gives the Huffman decode kernel's roofline: algorithmic bytes
-    = blob read + 2 B per code written, over the kernel's own event time."""
+    = blob read + 2 B per code written, over the kernel's own event time;
+    traffic = the committed ncu DRAM bytes per code, scaled to n."""
     x = F.fractal2d(8192, seed=1003, device=dev).reshape(-1)
     n = x.numel()
     dims = (8192, 8192, 1)
@@ -168,9 +182,10 @@ def c3_summary(dev, steps: int, warmup: int) -> dict:
         kms = ms / launches
         algo = blob.numel() + 2 * n
         ach = algo / kms / 1e6
+        per = _traffic_per_element("hf_decode")
         roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "traffic": None, "algorithmic_bytes": algo, "peak_kind": kind, "kernel": dk, "kernel_ms": kms,
-                "launches": launches}
+                "traffic": per * n if per else None, "algorithmic_bytes": algo, "peak_kind": kind, "kernel": dk,
+                "kernel_ms": kms, "launches": launches}
     return {"workload": "LorenzoQuant2D(ABS 1e-3, r512, zigzag)->Huffman(1024, coarse), 8192^2 fractal",
             "compress_gbs": 4 * n / (t_lq + t_full) / 1e6, "compress_gbs_without_book": 4 * n / (t_lq + t_hist + t_enc) / 1e6,
             "lq_ms": t_lq, "huffman_histogram_ms": t_hist, "huffman_book_host_ms": t_book,
