@@ -165,6 +165,10 @@ def c3_summary(dev, steps: int, warmup: int) -> dict:
     with K.Trace():
         for _ in range(steps):
             flush.zero_()
+            K.huff_histogram(codes, 1024)
+            flush.zero_()
+            K.huff_encode(codes, bk4, rb, 1024, ws=hws, trim=False)
+            flush.zero_()
             K.huff_decode(blob, n, 1024, ws=hws, out=dec)
         torch.cuda.synchronize()
         kern = K.Trace.kernels()
@@ -191,7 +195,8 @@ def c3_summary(dev, steps: int, warmup: int) -> dict:
             "lq_ms": t_lq, "huffman_histogram_ms": t_hist, "huffman_book_host_ms": t_book,
             "huffman_encode_ms": t_enc, "huffman_compress_ms_with_book": t_full, "huffman_decode_ms": t_dec,
             "decode_gbs_codes": 2 * n / t_dec / 1e6, "ratio": 4 * n / comp_bytes,
-            "bits_per_code": 8 * blob.numel() / n, "decode_identical": ok, "roofline": roof}
+            "bits_per_code": 8 * blob.numel() / n, "decode_identical": ok,
+            "kernels_ms": {k: round(ms / cnt, 4) for k, (cnt, ms) in sorted(kern.items())}, "roofline": roof}
 
 
 def run_c3(args, dev):

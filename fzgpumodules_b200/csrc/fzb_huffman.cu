@@ -27,7 +27,9 @@ constexpr uint32_t kHfSmemBook = 16384;  // books up to this size are staged in 
 // Privatised histogram: each CTA counts into `copies` shared-memory copies
 // (warp w into copy w % copies, so a frequent symbol's atomics spread), then
 // merges.  A thread adds each run of equal symbols among its eight with one
-// atomic.  Symbols >= bklen are skipped (histogram.cu:47-51).
+// atomic.  (Combining equal symbols across a warp with match.any first was
+// slower: 0.109 against 0.085 ms on C3's codes.)  Symbols >= bklen are
+// skipped (histogram.cu:47-51).
 __global__ void __launch_bounds__(512) hf_histogram_kernel(const uint16_t* __restrict__ in, uint64_t n,
                                                            uint32_t bklen, uint32_t copies,
                                                            uint32_t* __restrict__ freq) {
@@ -196,10 +198,12 @@ __global__ void __launch_bounds__(1024) hf_header_kernel(uint8_t* __restrict__ o
 }
 
 // Partition cells from their slots to the bitstream (u32 aligned), with
-// the par_nbit and par_entry words and the total bit count.  A warp takes 32
-// consecutive partitions, lane l holding the header of the l-th, and copies
-// four partitions at a time so that their loads are in flight together.
+// the par_nbit and par_entry words and the total bit count.  A warp takes
+// kHfCatGroup consecutive partitions, lane l < kHfCatGroup holding the header
+// of the l-th, and copies four at a time so that their loads are in flight
+// together; small groups give enough warps to cover the load latency.
 constexpr int kHfCatWarps = 8;
+constexpr int kHfCatGroup = 8;
 constexpr int kHfCatWords = 96;  // words per partition copied in the unrolled pass
 
 __global__ void __launch_bounds__(32 * kHfCatWarps) hf_concat_kernel(
@@ -210,10 +214,11 @@ __global__ void __launch_bounds__(32 * kHfCatWarps) hf_concat_kernel(
     __shared__ unsigned long long s_bits[kHfCatWarps];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     unsigned long long bits = 0;
-    for (uint32_t g = blockIdx.x * kHfCatWarps + warp; 32ull * g < pardeg; g += gridDim.x * kHfCatWarps) {
-        const uint32_t pl = 32 * g + lane;
+    for (uint32_t g = blockIdx.x * kHfCatWarps + warp; (uint64_t)kHfCatGroup * g < pardeg;
+         g += gridDim.x * kHfCatWarps) {
+        const uint32_t pl = kHfCatGroup * g + lane;
         uint32_t nc = 0, e = 0;
-        if (pl < pardeg) {
+        if (lane < (uint32_t)kHfCatGroup && pl < pardeg) {
             const uint32_t nb = par_nbit[pl];
             nc = par_ncell[pl];
             e = par_entry[pl];
@@ -221,12 +226,13 @@ __global__ void __launch_bounds__(32 * kHfCatWarps) hf_concat_kernel(
             out_entry[pl] = e;
             bits += nb;
         }
-        for (int j = 0; j < 32; j += 4) {
+#pragma unroll
+        for (int j = 0; j < kHfCatGroup; j += 4) {
             uint32_t v[4][kHfCatWords / 32];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const uint32_t ncj = __shfl_sync(~0u, nc, j + q);
-                const uint32_t* src = slots + (size_t)(32 * g + j + q) * sublen;
+                const uint32_t* src = slots + (size_t)(kHfCatGroup * g + j + q) * sublen;
 #pragma unroll
                 for (int r = 0; r < kHfCatWords / 32; r++) {
                     const uint32_t i = lane + 32 * r;
@@ -241,7 +247,7 @@ __global__ void __launch_bounds__(32 * kHfCatWarps) hf_concat_kernel(
                     const uint32_t i = lane + 32 * r;
                     if (i < ncj) bitstream[ej + i] = v[q][r];
                 }
-                const uint32_t* src = slots + (size_t)(32 * g + j + q) * sublen;
+                const uint32_t* src = slots + (size_t)(kHfCatGroup * g + j + q) * sublen;
                 for (uint32_t i = kHfCatWords + lane; i < ncj; i += 32) bitstream[ej + i] = src[i];
             }
         }
@@ -784,6 +790,7 @@ int launch_hf_histogram(const uint16_t* in, uint64_t n, uint32_t bklen, uint32_t
     const uint32_t copies = bklen <= 4096 ? 4u : 1u;
     const int smem = bklen <= kHfSmemBook ? 4 * (int)(bklen * copies) : 0;
     cudaFuncSetAttribute(hf_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    TraceScope ts(s, "hf_histogram");
     hf_histogram_kernel<<<2 * sms, 512, smem, s>>>(in, n, bklen, copies, freq);
     return (int)cudaGetLastError();
 }
@@ -798,16 +805,20 @@ int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32
     const unsigned grid =
         (unsigned)max((uint64_t)1, min((uint64_t)(pardeg + kHfEncWarps - 1) / kHfEncWarps, (uint64_t)4 * sms));
     cudaError_t e;
-    if (sublen == (uint32_t)kHfSublenFine) {
-        e = cudaFuncSetAttribute(hf_encode_kernel<kHfSublenFine>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return (int)e;
-        hf_encode_kernel<kHfSublenFine><<<grid, 32 * kHfEncWarps, smem, s>>>(in, n, bk4, bklen, pardeg, slots,
+    {
+        TraceScope ts(s, "hf_encode");
+        if (sublen == (uint32_t)kHfSublenFine) {
+            e = cudaFuncSetAttribute(hf_encode_kernel<kHfSublenFine>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     smem);
+            if (e != cudaSuccess) return (int)e;
+            hf_encode_kernel<kHfSublenFine><<<grid, 32 * kHfEncWarps, smem, s>>>(in, n, bk4, bklen, pardeg, slots,
+                                                                                 par_nbit, par_ncell);
+        } else {
+            e = cudaFuncSetAttribute(hf_encode_kernel<kHfSublen>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess) return (int)e;
+            hf_encode_kernel<kHfSublen><<<grid, 32 * kHfEncWarps, smem, s>>>(in, n, bk4, bklen, pardeg, slots,
                                                                              par_nbit, par_ncell);
-    } else {
-        e = cudaFuncSetAttribute(hf_encode_kernel<kHfSublen>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return (int)e;
-        hf_encode_kernel<kHfSublen><<<grid, 32 * kHfEncWarps, smem, s>>>(in, n, bk4, bklen, pardeg, slots, par_nbit,
-                                                                         par_ncell);
+        }
     }
     ScanSrc sc{};
     sc.base = par_ncell;
@@ -818,7 +829,8 @@ int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32
     hf_header_kernel<<<1, 1024, 0, s>>>(out, bklen, sublen, pardeg, n, d_revbook, rb, ncell_total, out_size);
     uint32_t* out_nbit = reinterpret_cast<uint32_t*>(out + 128 + rb);
     uint32_t* bitstream = reinterpret_cast<uint32_t*>(out + 128 + rb + 8 * (size_t)pardeg);
-    const uint32_t groups = (pardeg + 31) / 32;
+    const uint32_t groups = (pardeg + kHfCatGroup - 1) / kHfCatGroup;
+    TraceScope tc(s, "hf_concat");
     hf_concat_kernel<<<(groups + kHfCatWarps - 1) / kHfCatWarps, 32 * kHfCatWarps, 0, s>>>(
         slots, par_nbit, par_ncell, par_entry, pardeg, sublen, out_nbit, out_nbit + pardeg, bitstream, ctrl,
         reinterpret_cast<uint32_t*>(out + 24));

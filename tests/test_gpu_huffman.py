@@ -116,6 +116,44 @@ def test_unaligned_output_decode(cuda):
     assert np.array_equal(buf[1:].cpu().numpy(), a)
 
 
+@pytest.mark.parametrize("fine", [False, True])
+@pytest.mark.parametrize("sigma", [0.3, 1.0, 2.0, 4.0, 8.0, 16.0, 64.0])
+def test_decode_across_code_lengths(cuda, sigma, fine):
+    """Gaussian codes from nearly one symbol to nearly flat: books whose
+    shortest code runs from 1 to 7 bits, so the decoder takes both its
+    warp-per-partition path (bit segments that resynchronise, a few lanes
+    decoding again) and its partition-per-lane path.  Blob bytes and the
+    decode are checked against the oracle."""
+    rng = np.random.default_rng(int(sigma * 10) + int(fine))
+    a = np.clip(np.round(rng.normal(512, sigma, 300_001)), 0, 1023).astype(np.uint16)
+    bklen = 1024
+    freq = _hist(a, bklen)
+    bk4, rb = O.huff_book(freq, bklen)
+    ref = O.huff_encode(a, bklen, bk4, rb, sublen=1024 if fine else 768)
+    blob, _ = K().huff_compress(torch.from_numpy(a).to(cuda), bklen, fine=fine)
+    assert np.array_equal(blob.cpu().numpy(), ref)
+    ws = K().Workspace()
+    dec = K().huff_decode(blob, a.size, bklen, ws=ws)
+    assert ws.status() == 0
+    assert np.array_equal(dec.cpu().numpy(), a)
+
+
+def test_decode_reports_corrupt_cells(cuda):
+    """Flipped bits inside the bitstream: every partition whose bit count no
+    longer decodes to its symbols is reported, whichever decode path runs."""
+    for sigma in (1.0, 64.0):
+        rng = np.random.default_rng(7)
+        a = np.clip(np.round(rng.normal(512, sigma, 200_000)), 0, 1023).astype(np.uint16)
+        blob, _ = K().huff_compress(torch.from_numpy(a).to(cuda), 1024)
+        h = blob.cpu().numpy()
+        e4, e5 = (int(v) for v in h[40:64].view(np.uint32)[4:6])
+        bad = h.copy()
+        bad[e4:e5:7] ^= 0x5A
+        ws = K().Workspace()
+        K().huff_decode(torch.from_numpy(bad).to(cuda), a.size, 1024, ws=ws)
+        assert ws.status() == -5, sigma
+
+
 # ----------------------------------------------------------- reference stage
 
 def _ref():
