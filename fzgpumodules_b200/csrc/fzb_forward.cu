@@ -262,15 +262,12 @@ __device__ __forceinline__ float qread(const float4* Q, const Win& w, long long 
 // (3-D: z, x, y -- lorenzo_quant_nd.cu:234-246; 2-D: y, x -- :72-77;
 // 1-D: x -- lorenzo_quant.cu:308-321).
 template <int NDIM>
-__device__ __forceinline__ float delta_at(const FwdArgs& a, const float4* Q, const Roles& R,
-                                          uint32_t k) {
+__device__ __forceinline__ float delta_xyz(const FwdArgs& a, const float4* Q, const Roles& R, uint32_t k,
+                                           uint32_t x, uint32_t y, uint32_t z) {
     if (NDIM == 1) {
         const float q = qread(Q, R.cur0, k);
         return (k & 1023u) ? __fsub_rn(q, qread(Q, R.cur0, (long long)k - 1)) : q;
     }
-    const uint32_t z = (NDIM == 3) ? k / a.plane : 0u;
-    const uint32_t rem = k - z * a.plane;
-    const uint32_t y = rem / a.nx, x = rem - y * a.nx;
     const Win& wc = R.cur0;
     const Win& wu = R.up0;
     const long long ku = (long long)k - a.nx;
@@ -297,6 +294,31 @@ __device__ __forceinline__ float delta_at(const FwdArgs& a, const float4* Q, con
     float b1 = A(wu, ku, kuz, wuz);
     if (tx) b1 = __fsub_rn(b1, A(wu, ku - 1, kuz - 1, wuz));
     return __fsub_rn(b0, b1);
+}
+
+// Element coordinates of field index k, and the step to k + 1 (x fastest),
+// so that a run of consecutive elements needs no divisions.
+struct Xyz {
+    uint32_t x, y, z;
+};
+template <int NDIM>
+__device__ __forceinline__ Xyz xyz_of(const FwdArgs& a, uint32_t k) {
+    if (NDIM == 1) return Xyz{k, 0u, 0u};
+    const uint32_t z = (NDIM == 3) ? k / a.plane : 0u;
+    const uint32_t rem = k - z * a.plane;
+    const uint32_t y = rem / a.nx;
+    return Xyz{rem - y * a.nx, y, z};
+}
+template <int NDIM>
+__device__ __forceinline__ void xyz_next(const FwdArgs& a, Xyz& c) {
+    if (NDIM == 1) return;
+    if (++c.x == a.nx) {
+        c.x = 0;
+        if (++c.y == a.ny && NDIM == 3) {
+            c.y = 0;
+            c.z++;
+        }
+    }
 }
 
 // Raw little-endian code words of a 32-code group from the packed form
@@ -679,17 +701,20 @@ __device__ __forceinline__ void lq_chunk_body(const FwdArgs& a, const uint32_t c
         if (zz) group_dispatch<NDIM, true>(g, tz != 0, ty != 0, x, om);
         else group_dispatch<NDIM, false>(g, tz != 0, ty != 0, x, om);
     } else if (j0 < cnt && k0 < a.nfield) {
+        // element path (rows not a multiple of 32, partial groups): coordinates
+        // step along the run; the unrolled loop keeps x[] in registers
+        Xyz cz = xyz_of<NDIM>(a, k0);
+#pragma unroll
         for (int E = 0; E < 32; E++) {
             const uint32_t k = k0 + E;
             if (j0 + E < cnt && k < a.nfield) {
-                const float cc = delta_at<NDIM>(a, Q, R, k);
+                const float cc = delta_xyz<NDIM>(a, Q, R, k, cz.x, cz.y, cz.z);
                 const bool qz = fabsf(cc) < a.radius;
                 const uint32_t code = qz ? encode_code(cc, zz) : 0u;
                 om |= (qz ? 0u : 1u) << E;
-#pragma unroll
-                for (int l = 0; l < 16; l++)
-                    if (l == (E & 15)) x[l] |= code << (16 * (E >> 4));
+                x[E & 15] |= code << (16 * (E >> 4));
             }
+            xyz_next<NDIM>(a, cz);
         }
     }
     const uint32_t nout = __popc(om);
@@ -706,10 +731,11 @@ __device__ __forceinline__ void lq_chunk_body(const FwdArgs& a, const uint32_t c
     __syncthreads();
     if (nout) {  // pass 2: recompute this thread's deltas and stage its outliers
         uint32_t pos = s_obase + ooff;
-        for (int E = 0; E < 32; E++) {
+        Xyz cz = xyz_of<NDIM>(a, k0);
+        for (int E = 0; E < 32; E++, xyz_next<NDIM>(a, cz)) {
             const uint32_t k = k0 + E;
             if (j0 + E < cnt && k < a.nfield) {
-                const float cc = delta_at<NDIM>(a, Q, R, k);
+                const float cc = delta_xyz<NDIM>(a, Q, R, k, cz.x, cz.y, cz.z);
                 if (!(fabsf(cc) < a.radius)) {
                     if (pos < a.ostage_cap) {
                         a.ostage_err[pos] = cc;
