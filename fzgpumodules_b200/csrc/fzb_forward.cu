@@ -296,6 +296,60 @@ __device__ __forceinline__ float delta_xyz(const FwdArgs& a, const float4* Q, co
     return __fsub_rn(b0, b1);
 }
 
+// Along a run of consecutive elements the x neighbour's terms are the previous
+// element's own, so the run carries them: Run::a0 = A(x, y) and a1 = A(x, y-1)
+// of the last element, with A the z-differenced value (3-D), the y-differenced
+// value (2-D, a0 only) or q itself (1-D).  delta_run gives the same float
+// operations in the same order as delta_xyz.
+struct Run {
+    float a0, a1;
+};
+template <int NDIM>
+__device__ __forceinline__ void run_terms(const FwdArgs& a, const float4* Q, const Roles& R, long long k,
+                                          uint32_t y, uint32_t z, float& a0, float& a1) {
+    if (NDIM == 1) {
+        a0 = qread(Q, R.cur0, k);
+        a1 = 0.0f;
+    } else if (NDIM == 2) {
+        a0 = qread(Q, R.cur0, k);
+        if (y & 31u) a0 = __fsub_rn(a0, qread(Q, R.up0, k - a.nx));
+        a1 = 0.0f;
+    } else {
+        const bool tz = (z & 7u) != 0;
+        a0 = qread(Q, R.cur0, k);
+        if (tz) a0 = __fsub_rn(a0, qread(Q, R.cur1, k - a.plane));
+        a1 = 0.0f;
+        if (y & 7u) {
+            a1 = qread(Q, R.up0, k - a.nx);
+            if (tz) a1 = __fsub_rn(a1, qread(Q, R.up1, k - a.nx - a.plane));
+        }
+    }
+}
+template <int NDIM>
+__device__ __forceinline__ float delta_run(const FwdArgs& a, const float4* Q, const Roles& R, uint32_t k,
+                                           uint32_t x, uint32_t y, uint32_t z, Run& run) {
+    float a0, a1;
+    run_terms<NDIM>(a, Q, R, k, y, z, a0, a1);
+    float d;
+    if (NDIM == 1) {
+        d = (k & 1023u) ? __fsub_rn(a0, run.a0) : a0;
+    } else if (NDIM == 2) {
+        d = (x & 31u) ? __fsub_rn(a0, run.a0) : a0;
+    } else {
+        const bool tx = (x & 7u) != 0;
+        const float b0 = tx ? __fsub_rn(a0, run.a0) : a0;
+        if (y & 7u) {
+            const float b1 = tx ? __fsub_rn(a1, run.a1) : a1;
+            d = __fsub_rn(b0, b1);
+        } else {
+            d = b0;
+        }
+    }
+    run.a0 = a0;
+    run.a1 = a1;
+    return d;
+}
+
 // Element coordinates of field index k, and the step to k + 1 (x fastest),
 // so that a run of consecutive elements needs no divisions.
 struct Xyz {
@@ -704,11 +758,16 @@ __device__ __forceinline__ void lq_chunk_body(const FwdArgs& a, const uint32_t c
         // element path (rows not a multiple of 32, partial groups): coordinates
         // step along the run; the unrolled loop keeps x[] in registers
         Xyz cz = xyz_of<NDIM>(a, k0);
+        Run run{0.0f, 0.0f};
+        {   // the x neighbour of the run's first element, when its tile uses it
+            const bool tx = NDIM == 1 ? (k0 & 1023u) != 0 : (cz.x & (NDIM == 2 ? 31u : 7u)) != 0;
+            if (tx) run_terms<NDIM>(a, Q, R, (long long)k0 - 1, cz.y, cz.z, run.a0, run.a1);
+        }
 #pragma unroll
         for (int E = 0; E < 32; E++) {
             const uint32_t k = k0 + E;
             if (j0 + E < cnt && k < a.nfield) {
-                const float cc = delta_xyz<NDIM>(a, Q, R, k, cz.x, cz.y, cz.z);
+                const float cc = delta_run<NDIM>(a, Q, R, k, cz.x, cz.y, cz.z, run);
                 const bool qz = fabsf(cc) < a.radius;
                 const uint32_t code = qz ? encode_code(cc, zz) : 0u;
                 om |= (qz ? 0u : 1u) << E;
