@@ -109,6 +109,25 @@ def test_lq_forward_matches_oracle(cuda, dims, mode, zz, radius, kind):
     _check_outliers(out, x, dims, mode, radius, zz, cap, cnt, idx, err)
 
 
+@pytest.mark.parametrize("dims", [(37, 19, 5), (3000, 7, 1), (33, 17, 11)])
+def test_element_path_large_prequant_values(cuda, dims):
+    """Rows that are not a multiple of 32 elements take the element path,
+    which carries each element's x-neighbour terms along the run.  With an
+    absolute bound of 1e-5 on values up to 1e3 the prequantised values reach
+    5e7, above 2^24, so float differences round and their order matters: the
+    codes and every outlier's error must still equal the oracle's."""
+    n = int(np.prod(dims))
+    rng = np.random.default_rng(23)
+    x = rng.uniform(-1e3, 1e3, n).astype(np.float32)
+    x[::7] = np.float32(0.0)
+    cap = n
+    codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-5, O.ABS, 32768, True, cap)
+    out = kern().lq_forward(_g(x, cuda), dims, 1e-5, O.ABS, 32768, True, 1.0)
+    assert np.array_equal(_h(out["codes"]), codes)
+    assert int(_h(out["count"])[0]) == cnt
+    _check_outliers(out, x, dims, O.ABS, 32768, True, cap, cnt, idx, err)
+
+
 def _check_outliers(out, x, dims, mode, radius, zz, cap, cnt, idx, err):
     k = min(cnt, cap)
     gi = _h(out["idx"])[:k].view(np.uint32)
