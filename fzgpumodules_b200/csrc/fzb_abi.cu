@@ -86,10 +86,11 @@ inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 // produce identical results; tests exercise each): 1 = 3-D fused compression
 // through the per-chunk kernel, 2 = the cp.async slab kernel instead of the
 // TMA one, 4 = the per-(slab, tile) fused inverse instead of the persistent
-// slab inverse.
+// slab inverse, 8 = codes of 2-D fields with chunk-wide rows through the
+// per-chunk kernel instead of the row walk.
 inline unsigned flags_env() {
     const char* v = getenv("FZB_DISABLE_SLAB");
-    return v ? (unsigned)strtoul(v, nullptr, 10) & 7u : 0u;
+    return v ? (unsigned)strtoul(v, nullptr, 10) & 15u : 0u;
 }
 
 #define CK(call)                                          \
@@ -246,6 +247,13 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
             TraceScope ts(s, "lq3d_slab_bs_rze");
             rc = launch_lq3d_slab(a, (unsigned)(2 * sms), s) == 0 ? FZB_OK : FZB_E_CUDA;
         }
+    } else if (!fused && g.ndim == 2 && nx % (uint32_t)kChunkCodes == 0 && g.nfield == n_total &&
+               !(flags_env() & 8)) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        TraceScope ts(s, "lq_rows");
+        rc = launch_lq_rows(a, (unsigned)sms, s) == 0 ? FZB_OK : FZB_E_CUDA;
     } else {
         TraceScope ts(s, fused ? "lq_chunk_bs_rze" : "lq_chunk");
         rc = launch_lq(g, fused, a, lq_smem_bytes(g, fused), (uint32_t)nch, s);

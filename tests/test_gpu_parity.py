@@ -281,6 +281,25 @@ def test_fused_compress_slab_and_chunk_kernels_agree(cuda, dims, kind, eb, radiu
     assert np.array_equal(decs[0], decs[2]) and np.array_equal(decs[1], decs[2])
 
 
+@pytest.mark.parametrize("dims", [(8192, 77, 1), (16384, 40, 1), (8192, 33, 1)])
+@pytest.mark.parametrize("mode,zz,radius,kind", [(O.REL, True, 32768, "spiky"), (O.ABS, True, 512, "spiky"),
+                                                 (O.NOA, False, 64, "noise")])
+def test_row_walk_codes_match_oracle(cuda, dims, mode, zz, radius, kind, monkeypatch):
+    """2-D fields whose rows are whole chunks: the row walk (each row's
+    q(k - nx) window is the previous row's q(k) window) and the per-chunk
+    kernel give the oracle's codes and outliers."""
+    n = int(np.prod(dims))
+    x = _field(n, 29, kind)
+    cap = n
+    codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-3, mode, radius, zz, cap)
+    for flag in ("0", "8"):
+        monkeypatch.setenv("FZB_DISABLE_SLAB", flag)
+        out = kern().lq_forward(_g(x, cuda), dims, 1e-3, mode, radius, zz, 1.0)
+        assert np.array_equal(_h(out["codes"]), codes), flag
+        assert int(_h(out["count"])[0]) == cnt, flag
+        _check_outliers(out, x, dims, mode, radius, zz, cap, cnt, idx, err)
+
+
 @pytest.mark.parametrize("dims", [(256, 64, 9), (512, 16, 8), (96, 40, 9)])
 def test_rounding_midpoints_match_oracle(cuda, dims, monkeypatch):
     # every element sits next to a rounding midpoint of x * ebx2_r: codes must
