@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(kHfDecThreads, 2)
     bool bad = false;
 
     if (shortest > kHfCoopMaxShortest) {
-        // one partition per lane, 32 per ticket
+        // one partition per lane, 32 per take from the counter
         while (true) {
             uint32_t g = 0;
             if (lane == 0) g = blockIdx.x + atomicAdd(&s_next, 1u) * gridDim.x;
