@@ -17,6 +17,8 @@ device time of the fused C-ABI call); beside it in the same JSON line:
                    decompress, D2H of the field;
   c3               LorenzoQuant 2-D -> Huffman on 8192^2, with the Huffman
                    decode kernel's roofline;
+  batch            64 fields of mixed rank and size as one graph-captured
+                   launch sequence, against 64 plain calls;
   selector         the learned per-chunk coder selector against exhaustive
                    trial on 2 GiB of mixed fields (the metric's "ratio,
                    learned vs exhaustive");
@@ -565,6 +567,8 @@ def run_ours(args, world, rank, local):
         torch.cuda.empty_cache()
         line["c3"] = _guard(benchmarks.c3_summary, dev, args.steps, args.warmup)
         torch.cuda.empty_cache()
+        line["batch"] = _guard(benchmarks.batch_summary, dev, args.steps, args.warmup)
+        torch.cuda.empty_cache()
         line["selector"] = _guard(benchmarks.selector_summary, dev, args.steps, args.warmup, args.train_chunks)
     print(json.dumps(line), flush=True)
 
@@ -619,7 +623,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
-    ap.add_argument("--no-extras", action="store_true", help="skip the c3 and selector entries of the headline line")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the c3, batch and selector entries of the headline line")
     ap.add_argument("--train-chunks", type=int, default=1 << 20,
                     help="method-generated chunks the coder selector trains on (selector entry / workload)")
     ap.add_argument("--dims", type=int, nargs=3, default=list(DEFAULT_DIMS), metavar=("NX", "NY", "NZ"),

@@ -227,7 +227,9 @@ def batch_fields(dev, count=64, seed=1004, max_mb=256):
     return out
 
 
-def run_batch(args, dev):
+def batch_summary(dev, steps: int, warmup: int) -> dict:
+    """C4: the 64-field batch (batch_fields) as one graph-captured launch
+    sequence against 64 plain calls, bytes compared field by field."""
     fields = batch_fields(dev)
     total = sum(f["x"].numel() * 4 for f in fields)
     b = K.Batch(fields)
@@ -240,7 +242,7 @@ def run_batch(args, dev):
         b.launch(s)
     torch.cuda.synchronize()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    t_batch = _time(lambda: g.replay(), args.steps, args.warmup, flush)
+    t_batch = _time(lambda: g.replay(), steps, warmup, flush)
     ws = K.Workspace()
     plain_out = [None] * len(fields)
 
@@ -248,7 +250,7 @@ def run_batch(args, dev):
         for i, f in enumerate(fields):
             plain_out[i] = K.lq_bs_rze_compress(f["x"], f["dims"], f["eb"], f["mode"], f["radius"], f["zigzag"],
                                                 f["outlier_capacity"], ws=ws, out=plain_out[i])
-    t_plain = _time(plain, args.steps, args.warmup, flush)
+    t_plain = _time(plain, steps, warmup, flush)
     torch.cuda.synchronize()
     same = all(int(o["rze_size"].item()) == int(p["rze_size"].item()) and
                torch.equal(o["rze"][: int(o["rze_size"].item())], p["rze"][: int(p["rze_size"].item())])
@@ -256,12 +258,16 @@ def run_batch(args, dev):
     comp = sum(int(o["rze_size"].item()) + 8 * min(int(o["count"].item()), o["cap"]) + 4 for o in b.outputs)
     del g
     b.close()
-    return _line("batch: 64 fields 1-256 MB, mixed rank, REL {1e-2,1e-3,1e-4}, LQ->BS->RZE", total / t_batch / 1e6,
-                 "GB/s", args, {"batched_ms": t_batch, "plain_ms": t_plain, "plain_gbs": total / t_plain / 1e6,
-                                "speedup_vs_plain": t_plain / t_batch, "bytes_identical": same,
-                                "tuning": {"ctas_per_sm": best.ctas_per_sm, "order": best.order},
-                                "autotune_best_ms": tune_ms, "total_bytes": total, "ratio": total / comp,
-                                "launches_per_batch": 5})
+    return {"workload": "64 fields 1-256 MB, mixed rank, REL {1e-2,1e-3,1e-4}, LQ->BS->RZE",
+            "gbs": total / t_batch / 1e6, "batched_ms": t_batch, "plain_ms": t_plain,
+            "plain_gbs": total / t_plain / 1e6, "speedup_vs_plain": t_plain / t_batch, "bytes_identical": same,
+            "tuning": {"ctas_per_sm": best.ctas_per_sm, "order": best.order}, "autotune_best_ms": tune_ms,
+            "total_bytes": total, "ratio": total / comp, "launches_per_batch": 5}
+
+
+def run_batch(args, dev):
+    d = batch_summary(dev, args.steps, args.warmup)
+    return _line("batch: " + d.pop("workload"), d.pop("gbs"), "GB/s", args, d)
 
 
 def selector_summary(dev, steps: int, warmup: int, train_chunks: int = 1 << 20) -> dict:
