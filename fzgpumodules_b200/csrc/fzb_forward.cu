@@ -350,6 +350,11 @@ __device__ __forceinline__ float delta_run(const FwdArgs& a, const float4* Q, co
     return d;
 }
 
+// The granule of 4 window values starting at k (k - gbase a multiple of 4).
+__device__ __forceinline__ float4 qread4(const float4* Q, const Win& w, long long k) {
+    return Q[w.soff + swz((int)((k - w.gbase) >> 2))];
+}
+
 // Element coordinates of field index k, and the step to k + 1 (x fastest),
 // so that a run of consecutive elements needs no divisions.
 struct Xyz {
@@ -686,6 +691,59 @@ __device__ __forceinline__ void group_dispatch(const GroupIn& g, bool tz, bool t
     }
 }
 
+// Codes of one thread's whole 32-element run when rows are a multiple of 4
+// elements but not of 32 (the element path's case): every window value of the
+// run comes in 16-byte granules (k, k - nx, k - plane and k - plane - nx are
+// all multiples of 4 from the window bases), the coordinates step along the
+// run, and the x neighbour's terms are carried as in delta_run, with the same
+// float operations in the same order.
+template <int NDIM>
+__device__ __forceinline__ void run_codes_vec(const FwdArgs& a, const float4* Q, const Roles& R, uint32_t k0,
+                                              Xyz cz, bool zz, uint32_t (&x)[16], uint32_t& om) {
+    Run run{0.0f, 0.0f};
+    if ((cz.x & (NDIM == 2 ? 31u : 7u)) != 0) run_terms<NDIM>(a, Q, R, (long long)k0 - 1, cz.y, cz.z, run.a0, run.a1);
+#pragma unroll
+    for (int g = 0; g < 8; g++) {
+        const long long kg = (long long)k0 + 4 * g;
+        const float4 c4 = qread4(Q, R.cur0, kg);
+        const float4 u4 = qread4(Q, R.up0, kg - a.nx);
+        float4 cz4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), uz4 = cz4;
+        if (NDIM == 3 && R.z) {
+            cz4 = qread4(Q, R.cur1, kg - a.plane);
+            uz4 = qread4(Q, R.up1, kg - a.plane - a.nx);
+        }
+        const float cv[4] = {c4.x, c4.y, c4.z, c4.w}, uv[4] = {u4.x, u4.y, u4.z, u4.w};
+        const float czv[4] = {cz4.x, cz4.y, cz4.z, cz4.w}, uzv[4] = {uz4.x, uz4.y, uz4.z, uz4.w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int E = 4 * g + e;
+            float a0 = cv[e], a1 = 0.0f, d;
+            if (NDIM == 2) {
+                if (cz.y & 31u) a0 = __fsub_rn(a0, uv[e]);
+                d = (cz.x & 31u) ? __fsub_rn(a0, run.a0) : a0;
+            } else {
+                const bool tz = (cz.z & 7u) != 0, tx = (cz.x & 7u) != 0;
+                if (tz) a0 = __fsub_rn(a0, czv[e]);
+                const float b0 = tx ? __fsub_rn(a0, run.a0) : a0;
+                if (cz.y & 7u) {
+                    a1 = uv[e];
+                    if (tz) a1 = __fsub_rn(a1, uzv[e]);
+                    d = __fsub_rn(b0, tx ? __fsub_rn(a1, run.a1) : a1);
+                } else {
+                    d = b0;
+                }
+            }
+            run.a0 = a0;
+            run.a1 = a1;
+            const bool qz = fabsf(d) < a.radius;
+            const uint32_t code = qz ? encode_code(d, zz) : 0u;
+            om |= (qz ? 0u : 1u) << E;
+            x[E & 15] |= code << (16 * (E >> 4));
+            xyz_next<NDIM>(a, cz);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // The chunk kernel.  FUSED=false writes codes; FUSED=true bitshuffles them
 // (16 KiB blocks, element width 2, ballot layout) and RZE-encodes the block
@@ -759,8 +817,10 @@ __device__ __forceinline__ void lq_chunk_body(const FwdArgs& a, const uint32_t c
         g.radius = a.radius;
         if (zz) group_dispatch<NDIM, true>(g, tz != 0, ty != 0, x, om);
         else group_dispatch<NDIM, false>(g, tz != 0, ty != 0, x, om);
+    } else if (NDIM >= 2 && (a.nx & 3u) == 0 && j0 + 32 <= cnt && k0 + 32 <= a.nfield) {
+        run_codes_vec<NDIM>(a, Q, R, k0, xyz_of<NDIM>(a, k0), zz, x, om);
     } else if (j0 < cnt && k0 < a.nfield) {
-        // element path (rows not a multiple of 32, partial groups): coordinates
+        // element path (rows not a multiple of 4, partial groups): coordinates
         // step along the run; the unrolled loop keeps x[] in registers
         Xyz cz = xyz_of<NDIM>(a, k0);
         Run run{0.0f, 0.0f};
