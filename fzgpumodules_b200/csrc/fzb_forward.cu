@@ -994,12 +994,16 @@ __global__ void __launch_bounds__(kThreads, 3) lq_batch_kernel(BatchArgs b) {
     __shared__ uint32_t s_ws[16];
     __shared__ uint32_t s_obase;
     __shared__ uint32_t s_unit;
+    // thread 0 takes the next unit's ticket as this one starts, so the
+    // dispenser's round trip overlaps the chunk instead of preceding it
+    uint32_t next = 0;
+    if (threadIdx.x == 0) s_unit = atomicAdd(b.counter, 1u);
     for (;;) {
-        if (threadIdx.x == 0) s_unit = atomicAdd(b.counter, 1u);
         __syncthreads();
         const uint32_t u = s_unit;
-        __syncthreads();  // s_unit is rewritten on the next iteration
+        __syncthreads();  // s_unit is rewritten at the end of this iteration
         if (u >= b.total_units) break;
+        if (threadIdx.x == 0) next = atomicAdd(b.counter, 1u);
         // field = last slot whose unit_begin <= u (fields in unit_order)
         uint32_t lo = 0, hi = b.nfields;
         while (hi - lo > 1) {
@@ -1016,7 +1020,7 @@ __global__ void __launch_bounds__(kThreads, 3) lq_batch_kernel(BatchArgs b) {
             case 3: lq_chunk_body<3, true, true>(f.a, c, Q, s_ws, s_obase); break;
             default: lq_chunk_body<3, true, false>(f.a, c, Q, s_ws, s_obase); break;
         }
-        __syncthreads();  // shared memory is reused by the next unit
+        if (threadIdx.x == 0) s_unit = next;  // read after the barrier that opens the next iteration
     }
 }
 
