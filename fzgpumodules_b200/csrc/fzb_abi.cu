@@ -267,7 +267,7 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
     CK(cudaGetLastError());
     {
         TraceScope ts(s, "assemble_copy");
-        assemble_copy_kernel<<<copy_grid(nch), 256, 0, s>>>(m);
+        CK(launch_dependent(assemble_copy_kernel, copy_grid(nch), 256, 0, s, m));
     }
     CK(cudaGetLastError());
     return FZB_OK;

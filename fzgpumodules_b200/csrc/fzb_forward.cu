@@ -100,6 +100,10 @@ __device__ __forceinline__ void minmax_body(const float* __restrict__ x, uint64_
         s_last = (atomicAdd(done, 1u) == nblk - 1);
     }
     __syncthreads();
+    // this block's share is written: a programmatic dependent (the slab
+    // compressor) may start its set-up while the last block resolves the
+    // bound, which it reads only after this grid has ended
+    asm volatile("griddepcontrol.launch_dependents;");
     if (!s_last) return;
     __threadfence();
     lo = INFINITY;
@@ -526,9 +530,14 @@ __device__ __forceinline__ void assemble_scan_body(const AsmArgs& a, uint32_t* s
     }
 }
 
+// Both assembly kernels are launched as programmatic dependents: each waits
+// for the kernel before it (the chunk sizes, then the offsets) and the scan
+// lets the copy start launching once it is done.
 __global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) {
     extern __shared__ uint32_t asm_dyn[];
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     assemble_scan_body<kAsmTile>(a, asm_dyn, asm_dyn + kAsmTile + kAsmTile / 32);
+    asm volatile("griddepcontrol.launch_dependents;");
 }
 
 int launch_assemble_scan(const AsmArgs& a, cudaStream_t s) {
@@ -536,8 +545,7 @@ int launch_assemble_scan(const AsmArgs& a, cudaStream_t s) {
     static SmemAttr attr;
     const cudaError_t e = ensure_dyn_smem(attr, (const void*)assemble_scan_kernel, smem);
     if (e != cudaSuccess) return (int)e;
-    assemble_scan_kernel<<<1, 1024, smem, s>>>(a);
-    return (int)cudaGetLastError();
+    return (int)launch_dependent(assemble_scan_kernel, 1, 1024, (size_t)smem, s, a);
 }
 
 // One chunk per group of `nth` threads (thread `tid` of the group): payload
@@ -593,6 +601,7 @@ __device__ __forceinline__ void assemble_copy_body(const AsmArgs& a, const uint3
 
 // One warp per chunk, grid-stride over the chunks.
 __global__ void __launch_bounds__(256) assemble_copy_kernel(AsmArgs a) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t nw = gridDim.x * (blockDim.x >> 5);
     for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < a.n_chunks; c += nw)

@@ -281,6 +281,32 @@ int launch_mlp_backward(const float* P, const float* X, const float* T, uint32_t
                         int kind, cudaStream_t s);
 int launch_mlp_adam(float* P, const float* G, float* M, float* V, float lr, int step, cudaStream_t s);
 
+// Launches `kernel` as a programmatic dependent of the previous kernel on
+// `s` (it may start before that kernel ends and must wait with
+// griddepcontrol.wait before reading its results); a plain launch when the
+// attribute is refused.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem,
+                                    cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
 // Per-kernel CUDA-event timing (fzb_trace.cu): a TraceScope around a launch
 // records an event pair on the launching stream while tracing is enabled.
 extern bool g_trace_on;

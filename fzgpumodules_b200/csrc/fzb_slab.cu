@@ -210,7 +210,6 @@ __global__ void __launch_bounds__(kTT, 2)
     const uint32_t nx = a.nx, R = kChunkCodes / nx, S16 = nx / 16;  // threads per row
     const bool ty = ((t / S16) & 7u) != 0;  // slab origins have y % 8 == 0
     const uint32_t tu = ty ? t - S16 : t;   // thread holding the row above
-    const float r = *a.ebx2_r;
     const float rad = a.radius;
     const uint32_t G = gridDim.x;
 
@@ -255,6 +254,11 @@ __global__ void __launch_bounds__(kTT, 2)
         issue_next(0);
         issue_next(1);
     }
+    // Launched as a programmatic dependent of the value-base scan: the set-up
+    // above and the first two plane copies (the field is not the scan's
+    // output) overlap the scan's tail; the error bound is read after it.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const float r = *a.ebx2_r;
 
     uint32_t k = 0;  // plane sequence number
     for (uint32_t uu = blockIdx.x; uu < units; uu += G) {
@@ -508,6 +512,7 @@ __global__ void __launch_bounds__(kTT, 2)
             fence_proxy_async();  // this plane's generic accesses before the buffer's next TMA fill
         }
     }
+    asm volatile("griddepcontrol.launch_dependents;");  // the assembly scan may start launching
 }
 
 }  // namespace
@@ -553,14 +558,14 @@ int launch_lq3d_tma(const FwdArgs& a, unsigned grid, cudaStream_t s) {
         static SmemAttr attr;
         e = ensure_dyn_smem(attr, (const void*)lq3d_tma_kernel<true>, (int)kSlabSmem);
         if (e != cudaSuccess) return (int)e;
-        lq3d_tma_kernel<true><<<grid, kTT, kSlabSmem, s>>>(a, map, slabs, units);
+        e = launch_dependent(lq3d_tma_kernel<true>, grid, kTT, kSlabSmem, s, a, map, slabs, units);
     } else {
         static SmemAttr attr;
         e = ensure_dyn_smem(attr, (const void*)lq3d_tma_kernel<false>, (int)kSlabSmem);
         if (e != cudaSuccess) return (int)e;
-        lq3d_tma_kernel<false><<<grid, kTT, kSlabSmem, s>>>(a, map, slabs, units);
+        e = launch_dependent(lq3d_tma_kernel<false>, grid, kTT, kSlabSmem, s, a, map, slabs, units);
     }
-    return (int)cudaGetLastError();
+    return (int)e;
 }
 
 }  // namespace fzb
