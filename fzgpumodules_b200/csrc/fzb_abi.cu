@@ -573,8 +573,8 @@ int lq_bs_rze_decompress_common(const void* d_rze, uint64_t rze_bytes, const flo
     if (fused) {
         {
             TraceScope ts(s, "outlier_ranges");
-            outlier_ranges_kernel<<<(unsigned)((nch + 256) / 256 + 1), 256, 0, s>>>(
-                d_idx, d_count, a.cap, (uint32_t)nch, w.ostart, w.err);
+            CK(launch_dependent(outlier_ranges_kernel, (unsigned)((nch + 256) / 256 + 1), 256, 0, s, d_idx, d_count,
+                                a.cap, (uint32_t)nch, w.ostart, w.err));
         }
         CK(cudaGetLastError());
         const int smem = 2 * kChunkBytes + 16 + 2048 + 256 + 32 + 4 * kChunkCodes;

@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
         in_off[n] = carry;
         if (carry > rze_bytes) atomicOr(err, kErrMalformed);
     }
+    asm volatile("griddepcontrol.launch_dependents;");  // outlier_ranges_kernel may start
 }
 
 int launch_rze_prepass(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect, uint32_t orig_expect,
@@ -114,6 +115,11 @@ __global__ void outlier_ranges_kernel(const uint32_t* __restrict__ idx, const ui
     }
     for (uint32_t i = tid; i + 1 < nout; i += stride)
         if (idx[i] >= idx[i + 1]) atomicOr(err, kErrUnsorted);
+    // launched as a programmatic dependent of the RZE prepass, whose offsets it
+    // does not read: the fused inverse may start launching now, and this grid
+    // ends only after the prepass has, so the inverse's wait covers both
+    asm volatile("griddepcontrol.launch_dependents;");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 __device__ __forceinline__ RzeDecSmem dec_smem(uint8_t* base, uint32_t* ws) {

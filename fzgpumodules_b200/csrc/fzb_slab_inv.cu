@@ -115,6 +115,9 @@ __global__ void __launch_bounds__(kThreads, kInvCtasPerSm) lq3d_inv_slab_kernel(
     __shared__ uint32_t s_first[kThreads];  // per segment: its first outlier list entry
     __shared__ uint32_t s_misc[4];          // 0 level-1 size s1, 1 malformed flag
 
+    // launched as a programmatic dependent: the prepass offsets, outlier
+    // ranges and error word are read after the kernels before have ended
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (*a.err & (kErrUnsorted | kErrMalformed)) return;
     uint8_t* base = dsm + ((kSmemAlign - (smem_u32(dsm) & (kSmemAlign - 1))) & (kSmemAlign - 1));
     uint8_t* X = base;  // x-prefixed plane, 128-byte swizzled rows (one per thread)
@@ -446,12 +449,14 @@ int launch_lq3d_inv_slab(const InvArgs& a, unsigned sms, cudaStream_t s) {
         static SmemAttr attr;
         e = ensure_dyn_smem(attr, (const void*)lq3d_inv_slab_kernel<true>, (int)kInvSmem);
         if (e != cudaSuccess) return (int)e;
-        lq3d_inv_slab_kernel<true><<<grid, kThreads, kInvSmem, s>>>(a, slabs, units);
+        e = launch_dependent(lq3d_inv_slab_kernel<true>, grid, kThreads, kInvSmem, s, a, slabs, units);
+        if (e != cudaSuccess) return (int)e;
     } else {
         static SmemAttr attr;
         e = ensure_dyn_smem(attr, (const void*)lq3d_inv_slab_kernel<false>, (int)kInvSmem);
         if (e != cudaSuccess) return (int)e;
-        lq3d_inv_slab_kernel<false><<<grid, kThreads, kInvSmem, s>>>(a, slabs, units);
+        e = launch_dependent(lq3d_inv_slab_kernel<false>, grid, kThreads, kInvSmem, s, a, slabs, units);
+        if (e != cudaSuccess) return (int)e;
     }
     return (int)cudaGetLastError();
 }
