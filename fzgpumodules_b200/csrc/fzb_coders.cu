@@ -31,6 +31,7 @@ __device__ __forceinline__ const uint32_t* scan_src(const ScanSrc& a, uint32_t* 
 }
 
 __global__ void __launch_bounds__(256) scan_tile_sums(ScanSrc a, uint32_t* __restrict__ tsum) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     uint32_t cnt;
     const uint32_t* in = scan_src(a, &cnt);
     const uint32_t b = blockIdx.x * kScanTile;
@@ -46,10 +47,12 @@ __global__ void __launch_bounds__(256) scan_tile_sums(ScanSrc a, uint32_t* __res
         for (int i = 0; i < 8; i++) t += w[i];
         tsum[blockIdx.x] = t;
     }
+    asm volatile("griddepcontrol.launch_dependents;");
 }
 
 __global__ void __launch_bounds__(1024) scan_tile_offsets(uint32_t* __restrict__ tsum, uint32_t ntiles,
                                                           uint32_t* __restrict__ total) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     __shared__ uint32_t s[1024];
     const uint32_t t = threadIdx.x, per = (ntiles + 1023) / 1024;
     const uint32_t b = t * per, e = min(ntiles, b + per);
@@ -70,10 +73,12 @@ __global__ void __launch_bounds__(1024) scan_tile_offsets(uint32_t* __restrict__
         run += v;
     }
     if (t == 1023 && total) *total = s[1023];
+    asm volatile("griddepcontrol.launch_dependents;");
 }
 
 __global__ void __launch_bounds__(256) scan_tile_apply(ScanSrc a, const uint32_t* __restrict__ toff,
                                                        uint32_t* __restrict__ out) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     __shared__ uint32_t ws[16];
     uint32_t cnt;
     const uint32_t* in = scan_src(a, &cnt);
@@ -91,16 +96,19 @@ __global__ void __launch_bounds__(256) scan_tile_apply(ScanSrc a, const uint32_t
         if (b + i < cnt) out[b + i] = run;
         run += v[i];
     }
+    asm volatile("griddepcontrol.launch_dependents;");
 }
 
 int launch_scan_u32(const ScanSrc& a, uint32_t* out, uint32_t* tile_scratch, uint32_t* total,
                     cudaStream_t s) {
     if (a.n == 0) return 0;
     const uint32_t ntiles = (a.n + kScanTile - 1) / kScanTile;
-    scan_tile_sums<<<ntiles, 256, 0, s>>>(a, tile_scratch);
-    scan_tile_offsets<<<1, 1024, 0, s>>>(tile_scratch, ntiles, total);
-    scan_tile_apply<<<ntiles, 256, 0, s>>>(a, tile_scratch, out);
-    return (int)cudaGetLastError();
+    // programmatic dependents: each waits for the kernel before it (the
+    // first for whatever produced the input) and lets the next one launch
+    cudaError_t e = launch_dependent(scan_tile_sums, ntiles, 256, 0, s, a, tile_scratch);
+    if (e == cudaSuccess) e = launch_dependent(scan_tile_offsets, 1, 1024, 0, s, tile_scratch, ntiles, total);
+    if (e == cudaSuccess) e = launch_dependent(scan_tile_apply, ntiles, 256, 0, s, a, (const uint32_t*)tile_scratch, out);
+    return (int)e;
 }
 
 // ---------------------------------------------------------------------------

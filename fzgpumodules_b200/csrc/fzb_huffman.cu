@@ -160,6 +160,7 @@ __global__ void __launch_bounds__(32 * kHfEncWarps) hf_encode_kernel(const uint1
         }
         __syncwarp();
     }
+    asm volatile("griddepcontrol.launch_dependents;");  // the cell-count scan may start launching
 }
 
 // Header + revbook (one CTA of 1024 threads).  hf_concat_kernel adds up the
@@ -171,6 +172,7 @@ __global__ void __launch_bounds__(1024) hf_header_kernel(uint8_t* __restrict__ o
                                                          uint32_t revbook_bytes,
                                                          const uint32_t* __restrict__ ncell_total,
                                                          unsigned long long* __restrict__ out_size) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // the scan's cell total
     const uint32_t e1 = 128, e2 = e1 + revbook_bytes, e3 = e2 + 4 * pardeg, e4 = e3 + 4 * pardeg;
     for (uint32_t i = threadIdx.x; i < revbook_bytes; i += blockDim.x) out[e1 + i] = revbook[i];
     if (threadIdx.x == 0) {
@@ -195,6 +197,7 @@ __global__ void __launch_bounds__(1024) hf_header_kernel(uint8_t* __restrict__ o
         ent[5] = e4 + (uint32_t)(4 * ncell);
         *out_size = e4 + 4 * ncell;
     }
+    asm volatile("griddepcontrol.launch_dependents;");
 }
 
 // Partition cells from their slots to the bitstream (u32 aligned), with
@@ -212,6 +215,7 @@ __global__ void __launch_bounds__(32 * kHfCatWarps) hf_concat_kernel(
     uint32_t* __restrict__ out_nbit, uint32_t* __restrict__ out_entry, uint32_t* __restrict__ bitstream,
     uint32_t* __restrict__ ctrl, uint32_t* __restrict__ head_nbit) {
     __shared__ unsigned long long s_bits[kHfCatWarps];
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // offsets and header of the kernels before
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     unsigned long long bits = 0;
     for (uint32_t g = blockIdx.x * kHfCatWarps + warp; (uint64_t)kHfCatGroup * g < pardeg;
@@ -826,15 +830,17 @@ int launch_hf_encode(const uint16_t* in, uint64_t n, const uint32_t* bk4, uint32
     int rc = launch_scan_u32(sc, par_entry, tiles, ncell_total, s);
     if (rc) return rc;
     const uint32_t rb = 256 + 2 * bklen;
-    hf_header_kernel<<<1, 1024, 0, s>>>(out, bklen, sublen, pardeg, n, d_revbook, rb, ncell_total, out_size);
+    cudaError_t eh = launch_dependent(hf_header_kernel, 1, 1024, 0, s, out, bklen, sublen, pardeg, n, d_revbook, rb,
+                                      (const uint32_t*)ncell_total, out_size);
+    if (eh != cudaSuccess) return (int)eh;
     uint32_t* out_nbit = reinterpret_cast<uint32_t*>(out + 128 + rb);
     uint32_t* bitstream = reinterpret_cast<uint32_t*>(out + 128 + rb + 8 * (size_t)pardeg);
     const uint32_t groups = (pardeg + kHfCatGroup - 1) / kHfCatGroup;
     TraceScope tc(s, "hf_concat");
-    hf_concat_kernel<<<(groups + kHfCatWarps - 1) / kHfCatWarps, 32 * kHfCatWarps, 0, s>>>(
-        slots, par_nbit, par_ncell, par_entry, pardeg, sublen, out_nbit, out_nbit + pardeg, bitstream, ctrl,
-        reinterpret_cast<uint32_t*>(out + 24));
-    return (int)cudaGetLastError();
+    return (int)launch_dependent(hf_concat_kernel, (groups + kHfCatWarps - 1) / kHfCatWarps, 32 * kHfCatWarps, 0, s,
+                                 (const uint32_t*)slots, (const uint32_t*)par_nbit, (const uint32_t*)par_ncell,
+                                 (const uint32_t*)par_entry, pardeg, sublen, out_nbit, out_nbit + pardeg, bitstream,
+                                 ctrl, reinterpret_cast<uint32_t*>(out + 24));
 }
 
 int launch_hf_decode(const uint8_t* blob, uint64_t blob_bytes, uint64_t n, uint32_t bklen,
