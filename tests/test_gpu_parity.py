@@ -88,6 +88,7 @@ GEOMS = [
     (9000, 3, 1),                                  # 2-D rows wider than a chunk
     (33, 17, 11), (64, 32, 16), (512, 16, 16),    # 3-D odd / row-aligned
     (96, 40, 9),                                   # 3-D chunks spanning planes
+    (20, 13, 9), (100, 24, 10),                    # 3-D rows a multiple of 4, not of 32 (16-byte runs)
 ]
 
 
@@ -109,7 +110,7 @@ def test_lq_forward_matches_oracle(cuda, dims, mode, zz, radius, kind):
     _check_outliers(out, x, dims, mode, radius, zz, cap, cnt, idx, err)
 
 
-@pytest.mark.parametrize("dims", [(37, 19, 5), (3000, 7, 1), (33, 17, 11)])
+@pytest.mark.parametrize("dims", [(37, 19, 5), (3000, 7, 1), (33, 17, 11), (20, 13, 9), (200, 9, 7)])
 def test_element_path_large_prequant_values(cuda, dims):
     """Rows that are not a multiple of 32 elements take the element path,
     which carries each element's x-neighbour terms along the run.  With an
@@ -222,7 +223,7 @@ def test_rze_matches_oracle(cuda, kind):
 
 
 FUSED_GEOMS = [(512, 16, 16), (64, 32, 24), (33, 17, 11), (256, 96, 1), (8192 * 2 + 5, 1, 1),
-               (1024, 8, 9), (96, 40, 9), (64, 256, 10)]
+               (1024, 8, 9), (96, 40, 9), (64, 256, 10), (100, 24, 10), (200, 17, 12), (1000, 9, 1)]
 
 
 @pytest.mark.parametrize("dims", FUSED_GEOMS)
