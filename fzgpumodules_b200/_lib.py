@@ -82,6 +82,12 @@ def lib():
         L.fzb_concat_bytes.argtypes = [p, i32]
         L.fzb_concat.restype = i32
         L.fzb_concat.argtypes = [p, p, i32, p, p]
+        L.fzb_concat_dev.restype = i32
+        L.fzb_concat_dev.argtypes = [p, p, p, p, p, p, i32, p, p]
+        L.fzb_gather_words.restype = i32
+        L.fzb_gather_words.argtypes = [p, p, p, i32, p, p]
+        L.fzb_status_from_bits.restype = i32
+        L.fzb_status_from_bits.argtypes = [u32, p]
         L.fzb_batch_workspace_bytes.restype = sz
         L.fzb_batch_workspace_bytes.argtypes = [p, i32]
         L.fzb_batch_create.restype = p

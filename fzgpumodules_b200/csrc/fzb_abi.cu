@@ -369,6 +369,11 @@ int fzb_workspace_status(void* d_work, void* stream) {
     return status_of(bits);
 }
 
+int fzb_status_from_bits(uint32_t bits, int* rerun_exact) {
+    if (rerun_exact) *rerun_exact = (bits & (kErrInexact | kErrUnsorted)) ? 1 : 0;
+    return status_of(bits);
+}
+
 int fzb_lq_forward(const float* d_in, uint64_t n_total, const uint32_t dims[3], float eb,
                    int eb_mode, float value_base, uint32_t radius, int zigzag, uint16_t* d_codes,
                    float* d_err, uint32_t* d_idx, uint64_t cap, uint32_t* d_count,
@@ -600,10 +605,10 @@ int lq_bs_rze_decompress_common(const void* d_rze, uint64_t rze_bytes, const flo
             a.gate_mask = kErrInexact | kErrUnsorted;
         } else {
             if (flags & FZB_NO_SYNC) return FZB_OK;
-        uint32_t bits = 0;
-        rc = read_status(w, s, &bits);
-        if (rc) return rc;
-        if (bits & (kErrMalformed | kErrLookbackTimeout)) return status_of(bits);
+            uint32_t bits = 0;
+            rc = read_status(w, s, &bits);
+            if (rc) return rc;
+            if (status_of(bits) != FZB_OK) return status_of(bits);
             if (!(bits & (kErrInexact | kErrUnsorted))) return FZB_OK;
             CK(cudaMemsetAsync(w.err, 0, 4, s));  // rerun exactly below
         }

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstring>
 #include <numeric>
 #include <queue>
 #include <stdexcept>
@@ -36,6 +37,52 @@ bool types_compatible(uint8_t a, uint8_t b) {
 }
 
 }  // namespace
+
+// ============================================================ ResultGather
+
+ResultGather::~ResultGather() {
+    if (host_) cudaFreeHost(host_);
+}
+
+bool ResultGather::enqueue(const std::vector<DeviceRead>& reads, cudaStream_t stream) {
+    if (reads.empty() || reads.size() > FZB_GATHER_MAX) return false;
+    size_t total = 0;
+    for (const auto& r : reads) total += (r.bytes + 7) & ~(size_t)7;
+    if (total > kBytes) return false;
+    if (!host_) {
+        void* h = nullptr;
+        if (cudaHostAlloc(&h, kBytes, cudaHostAllocMapped) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        void* d = nullptr;
+        if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFreeHost(h);
+            return false;
+        }
+        host_ = h;
+        dev_ = d;
+    }
+    const void* src[FZB_GATHER_MAX];
+    uint32_t bytes[FZB_GATHER_MAX];
+    uint8_t clear[FZB_GATHER_MAX];
+    for (size_t i = 0; i < reads.size(); i++) {
+        src[i] = reads[i].src;
+        bytes[i] = reads[i].bytes;
+        clear[i] = reads[i].clear ? 1 : 0;
+    }
+    return fzb_gather_words(src, bytes, clear, (int)reads.size(), dev_, stream) == FZB_OK;
+}
+
+void ResultGather::finish(const std::vector<DeviceRead>& reads) const {
+    const uint8_t* h = static_cast<const uint8_t*>(host_);
+    size_t off = 0;
+    for (const auto& r : reads) {
+        std::memcpy(r.dst, h + off, r.bytes);
+        off += (r.bytes + 7) & ~(size_t)7;
+    }
+}
 
 float PipelinePerfResult::throughput_gbs() const {
     float ms = 0.0f;
@@ -260,6 +307,7 @@ Pipeline::~Pipeline() {
     if (concat_buf_) pool_->free(concat_buf_, 0);
     if (graph_input_) pool_->free(graph_input_, 0);
     if (d_fused_size_) pool_->free(d_fused_size_, 0);
+    if (inv_work_) pool_->free(inv_work_, 0);
     dag_.reset();
     stages_.clear();
 }
@@ -708,6 +756,77 @@ void Pipeline::concatOutputs(void* d_out, size_t capacity, size_t* out_size, cud
     *out_size = total;
 }
 
+bool Pipeline::enqueueResultReads(cudaStream_t stream) {
+    reads_.clear();
+    read_stages_.clear();
+    for (auto& st : stages_) {
+        auto* r = dynamic_cast<DeviceResults*>(st.get());
+        if (!r) continue;
+        const size_t before = reads_.size();
+        r->pendingReads(reads_);
+        if (reads_.size() > before) read_stages_.push_back(r);
+    }
+    if (gather_.enqueue(reads_, stream)) return true;
+    reads_.clear();
+    read_stages_.clear();
+    return false;
+}
+
+void Pipeline::finishResultReads() {
+    gather_.finish(reads_);
+    for (auto* r : read_stages_) r->resultsFetched();
+    reads_.clear();
+    read_stages_.clear();
+}
+
+// Every output's bound (the bytes reserved for its buffer) and, where the
+// size is still on the device, the word it follows; the container is laid out
+// on the device and checked against the host's sizes after the wait.
+bool Pipeline::enqueueDeviceConcat(cudaStream_t stream) {
+    const size_t n = output_buffer_ids_.size();
+    if (n < 2 || n > FZB_CONCAT_MAX_SEGMENTS) return false;
+    const void* src[FZB_CONCAT_MAX_SEGMENTS];
+    const void* word[FZB_CONCAT_MAX_SEGMENTS];
+    uint64_t caps[FZB_CONCAT_MAX_SEGMENTS], scale[FZB_CONCAT_MAX_SEGMENTS], maxc[FZB_CONCAT_MAX_SEGMENTS];
+    uint32_t wbytes[FZB_CONCAT_MAX_SEGMENTS];
+    for (size_t i = 0; i < n; i++) {
+        DAGNode* p = output_nodes_[i];
+        const auto* r = dynamic_cast<const DeviceResults*>(p->stage);
+        if (!r) return false;  // a stage of another library: its sizes are known after the wait only
+        const BufferInfo& b = dag_->getBufferInfo(output_buffer_ids_[i]);
+        const int idx = b.producer_output_index;
+        src[i] = dag_->getBuffer(output_buffer_ids_[i]);
+        DeviceSize ds;
+        if (r->deviceOutputSize(idx, &ds)) {
+            // the bytes reserved for the output (asking the stage would read
+            // its size back, the wait this avoids)
+            caps[i] = b.allocated_size ? b.allocated_size : b.size;
+            word[i] = ds.word;
+            wbytes[i] = ds.word_bytes;
+            scale[i] = ds.scale;
+            maxc[i] = ds.max_count;
+        } else {
+            caps[i] = p->stage->getActualOutputSize(idx);
+            word[i] = nullptr;
+            wbytes[i] = 0;
+            scale[i] = 1;
+            maxc[i] = 0;
+        }
+        dev_concat_caps_[i] = caps[i];
+        dev_concat_fixed_[i] = word[i] == nullptr;
+    }
+    const size_t bound = fzb_concat_bytes(caps, (int)n);
+    if (!bound) return false;
+    if (bound > concat_bytes_) {
+        if (concat_buf_) pool_->free(concat_buf_, stream);
+        concat_bytes_ = 0;
+        concat_buf_ = pool_->allocate(bound, stream, "concat_output", true);
+        if (!concat_buf_) throw std::runtime_error("Failed to allocate concat output buffer");
+        concat_bytes_ = bound;
+    }
+    return fzb_concat_dev(src, caps, word, wbytes, scale, maxc, (int)n, concat_buf_, stream) == FZB_OK;
+}
+
 void Pipeline::compress(const void* d_input, size_t input_size, void** d_output, size_t* output_size,
                         cudaStream_t stream) {
     if (!finalized_) throw std::runtime_error("Pipeline must be finalized before execution");
@@ -744,7 +863,11 @@ void Pipeline::compress(const void* d_input, size_t input_size, void** d_output,
         runForward(stream);
     }
     const auto t2 = std::chrono::steady_clock::now();
+    // one wait: the container and the stages' results are enqueued first
+    concat_enqueued_ = enqueueDeviceConcat(stream);
+    const bool gathered = enqueueResultReads(stream);
     cuda_check(cudaStreamSynchronize(stream), "compress");
+    if (gathered) finishResultReads();
     for (auto& s : stages_) s->postStreamSync(stream);
     collectMetadata();
     if (profiling_enabled_) {
@@ -759,7 +882,20 @@ void Pipeline::compress(const void* d_input, size_t input_size, void** d_output,
                     else cudaGetLastError();
                 }
     }
-    if (meta_.size() > 1) {
+    if (concat_enqueued_) {
+        // the device laid the container out from its own sizes: a segment
+        // whose host size differs (a fixed size that changed, a device size
+        // past its buffer) is concatenated again from the host sizes
+        bool same = meta_.size() == output_buffer_ids_.size();
+        for (size_t i = 0; same && i < meta_.size(); i++)
+            same = dev_concat_fixed_[i] ? meta_[i].actual_size == dev_concat_caps_[i]
+                                        : meta_[i].actual_size <= dev_concat_caps_[i];
+        concat_enqueued_ = same;
+    }
+    if (concat_enqueued_) {
+        *output_size = concatSize();
+        *d_output = concat_buf_;
+    } else if (meta_.size() > 1) {
         const size_t need = concatSize();
         if (need > concat_bytes_) {
             if (concat_buf_) pool_->free(concat_buf_, stream);
@@ -825,6 +961,7 @@ void Pipeline::warmup(cudaStream_t stream) {
     }
     for (void* p : decomp_outputs_) pool_->free(p, stream);
     decomp_outputs_.clear();
+    decomp_output_bytes_ = 0;
     meta_.clear();
     compressed_ = false;
     cudaStreamSynchronize(stream);

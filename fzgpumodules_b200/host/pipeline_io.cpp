@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cstdio>
 #include <fstream>
+#include <functional>
 #include <stdexcept>
 #include <unordered_set>
 
@@ -28,6 +29,54 @@ struct FwdDesc {
 
 using Avail = std::unordered_map<int, std::pair<void*, size_t>>;
 
+// What a Pipeline's decompression keeps between calls: the fused inverse's
+// workspace and the mapped block its status word (and the stages' results)
+// are gathered into before the call's one wait.  Null for a one-off
+// decompression (decompressFromFile), which allocates per call and reads
+// each value with its own copy.
+struct InverseCtx {
+    ResultGather* gather = nullptr;
+    void** work = nullptr;
+    size_t* work_bytes = nullptr;
+    std::function<bool(cudaStream_t)> enqueue_reads;  // the stages' pending results
+    std::function<void()> finish_reads;
+};
+
+// The fused inverse's workspace: the context's kept buffer (grown when
+// needed), else a pool buffer that *temp receives for release.
+void* inverse_work(InverseCtx* ctx, MemoryPool* pool, size_t need, cudaStream_t stream, void** temp) {
+    *temp = nullptr;
+    if (ctx && ctx->work) {
+        if (*ctx->work && *ctx->work_bytes >= need) return *ctx->work;
+        if (*ctx->work) pool->free(*ctx->work, stream);
+        *ctx->work_bytes = 0;
+        *ctx->work = pool->allocate(need, stream, "inverse_workspace", true);
+        if (!*ctx->work) throw std::runtime_error("decompress: workspace allocation failed");
+        *ctx->work_bytes = need;
+        return *ctx->work;
+    }
+    *temp = pool->allocate(need, stream, "inverse_workspace", false);
+    if (!*temp) throw std::runtime_error("decompress: workspace allocation failed");
+    return *temp;
+}
+
+// Waits for the stream and returns the workspace status bits (cleared on the
+// device): gathered through the mapped block before the wait when the
+// context has one, else copied after it.
+uint32_t wait_status(InverseCtx* ctx, void* w, cudaStream_t stream) {
+    uint32_t bits = 0;
+    std::vector<DeviceRead> rd{{w, 4, &bits, true}};
+    const bool g = ctx && ctx->gather && ctx->gather->enqueue(rd, stream);
+    cuda_check(cudaStreamSynchronize(stream), "decompress");
+    if (g) {
+        ctx->gather->finish(rd);
+    } else {
+        cuda_check(cudaMemcpy(&bits, w, 4, cudaMemcpyDeviceToHost), "decompress status");
+        cuda_check(cudaMemset(w, 0, 4), "decompress status");
+    }
+    return bits;
+}
+
 std::string hex8(uint32_t v) {
     char b[16];
     std::snprintf(b, sizeof(b), "%08X", v);
@@ -42,7 +91,7 @@ std::string hex8(uint32_t v) {
 // inverted in one pass the same way.
 bool fused_inverse_pfpl(const std::vector<FwdDesc>& fwd, const Avail& avail, const FwdDesc* q,
                         MemoryPool* pool, void* d_result, size_t capacity, size_t* result_size,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, InverseCtx* ctx) {
     auto* qs = dynamic_cast<QuantizerStage<float, uint32_t>*>(q->stage);
     if (!qs || q->out_ids.size() != 4) return false;
     auto only = [&](int buf) -> const FwdDesc* {
@@ -87,8 +136,8 @@ bool fused_inverse_pfpl(const std::vector<FwdDesc>& fwd, const Avail& avail, con
         return t;
     };
     const size_t need = fzb_pfpl_decompress_workspace_bytes(n);
-    void* w = pool->allocate(need, stream, "inverse_workspace", false);
-    if (!w) throw std::runtime_error("decompress: workspace allocation failed");
+    void* wtemp = nullptr;
+    void* w = inverse_work(ctx, pool, need, stream, &wtemp);
     int rc = FZB_OK;
     try {
         const void* r = aligned(rze);
@@ -99,28 +148,28 @@ bool fused_inverse_pfpl(const std::vector<FwdDesc>& fwd, const Avail& avail, con
                                  static_cast<const uint32_t*>(ct), val.second / sizeof(float), n,
                                  qs->getErrorBound(), (int)qs->getErrorBoundMode(), qs->computedAbsErrorBound(),
                                  qs->getZigzagCodes() ? 1 : 0, static_cast<float*>(d_result), w, need, stream);
-        if (rc == FZB_OK) rc = fzb_workspace_status(w, stream);
+        if (rc == FZB_OK) rc = fzb_status_from_bits(wait_status(ctx, w, stream), nullptr);
     } catch (...) {
         cudaStreamSynchronize(stream);
         for (void* t : temps) pool->free(t, stream);
-        pool->free(w, stream);
+        if (wtemp) pool->free(wtemp, stream);
         throw;
     }
     cudaStreamSynchronize(stream);
     for (void* t : temps) pool->free(t, stream);
-    pool->free(w, stream);
+    if (wtemp) pool->free(wtemp, stream);
     if (rc) throw std::runtime_error(std::string("Quantizer<-Difference<-Bitshuffle<-RZE decompress: ") +
                                      fzb_status_string(rc));
     return true;
 }
 
 bool fused_inverse(const std::vector<FwdDesc>& fwd, const Avail& avail, int source_buf, MemoryPool* pool,
-                   void* d_result, size_t capacity, size_t* result_size, cudaStream_t stream) {
+                   void* d_result, size_t capacity, size_t* result_size, cudaStream_t stream, InverseCtx* ctx) {
     const FwdDesc* lq = nullptr;
     for (const auto& d : fwd)
         if (d.in_ids.size() == 1 && d.in_ids[0] == source_buf) lq = &d;
     if (!lq || lq->out_ids.size() != 4) return false;
-    if (fused_inverse_pfpl(fwd, avail, lq, pool, d_result, capacity, result_size, stream)) return true;
+    if (fused_inverse_pfpl(fwd, avail, lq, pool, d_result, capacity, result_size, stream, ctx)) return true;
     auto* lqs = dynamic_cast<LorenzoQuantStage<float, uint16_t>*>(lq->stage);
     if (!lqs) return false;
     auto consumers = [&](int buf) {
@@ -152,14 +201,27 @@ bool fused_inverse(const std::vector<FwdDesc>& fwd, const Avail& avail, int sour
     const auto d = lqs->getDims();
     uint32_t dims[3] = {(uint32_t)d[0], (uint32_t)d[1], (uint32_t)d[2]};
     const size_t need = fzb_workspace_bytes(n, 0);
-    void* w = pool->allocate(need, stream, "inverse_workspace", false);
-    if (!w) throw std::runtime_error("decompress: workspace allocation failed");
-    const int rc = fzb_lq_bs_rze_decompress(rze.first, rze.second, static_cast<const float*>(err.first),
-                                            static_cast<const uint32_t*>(idx.first),
-                                            static_cast<const uint32_t*>(cnt.first), err.second / sizeof(float), n,
-                                            dims, lqs->computedAbsErrorBound(), lqs->getZigzagCodes() ? 1 : 0,
-                                            static_cast<float*>(d_result), 0, w, need, stream);
-    pool->free(w, stream);
+    void* wtemp = nullptr;
+    void* w = inverse_work(ctx, pool, need, stream, &wtemp);
+    // the fused pass without a host wait; its status word comes back with
+    // the call's one wait, and a case it left to the exact kernels (values
+    // outside the exact-integer range, unsorted outliers) runs them after
+    auto run = [&](unsigned flags) {
+        return fzb_lq_bs_rze_decompress(rze.first, rze.second, static_cast<const float*>(err.first),
+                                        static_cast<const uint32_t*>(idx.first),
+                                        static_cast<const uint32_t*>(cnt.first), err.second / sizeof(float), n, dims,
+                                        lqs->computedAbsErrorBound(), lqs->getZigzagCodes() ? 1 : 0,
+                                        static_cast<float*>(d_result), flags, w, need, stream);
+    };
+    int rc = run(FZB_NO_SYNC);
+    if (rc == FZB_OK) {
+        int rerun = 0;
+        rc = fzb_status_from_bits(wait_status(ctx, w, stream), &rerun);
+        if (rc == FZB_OK && rerun) rc = run(FZB_FORCE_EXACT);
+    } else {
+        cudaStreamSynchronize(stream);
+    }
+    if (wtemp) pool->free(wtemp, stream);
     if (rc) throw std::runtime_error(std::string("LorenzoQuant<-Bitshuffle<-RZE decompress: ") + fzb_status_string(rc));
     return true;
 }
@@ -167,12 +229,12 @@ bool fused_inverse(const std::vector<FwdDesc>& fwd, const Avail& avail, int sour
 // Runs the inverse of every stage in reverse topological order.  d_result
 // receives the source buffer's reconstruction.
 void run_inverse(const std::vector<FwdDesc>& fwd, Avail avail, int source_buf, MemoryPool* pool, void* d_result,
-                 size_t capacity, size_t* result_size, cudaStream_t stream, bool allow_fused) {
+                 size_t capacity, size_t* result_size, cudaStream_t stream, bool allow_fused,
+                 InverseCtx* ctx = nullptr) {
     for (const auto& d : fwd) d.stage->setInverse(true);
-    if (allow_fused && fused_inverse(fwd, avail, source_buf, pool, d_result, capacity, result_size, stream)) {
-        cuda_check(cudaStreamSynchronize(stream), "decompress");
+    // the fused inverses end with the stream synchronised
+    if (allow_fused && fused_inverse(fwd, avail, source_buf, pool, d_result, capacity, result_size, stream, ctx))
         return;
-    }
     std::vector<void*> temps;
     try {
         for (auto it = fwd.rbegin(); it != fwd.rend(); ++it) {
@@ -213,7 +275,9 @@ void run_inverse(const std::vector<FwdDesc>& fwd, Avail avail, int source_buf, M
             it->stage->execute(stream, pool, in, {out}, sizes);
             avail[it->in_ids[0]] = {out, it->stage->getActualOutputSize(0)};
         }
+        const bool gathered = ctx && ctx->enqueue_reads && ctx->enqueue_reads(stream);
         cuda_check(cudaStreamSynchronize(stream), "decompress");
+        if (gathered) ctx->finish_reads();
         for (const auto& d : fwd) d.stage->postStreamSync(stream);
     } catch (...) {
         cudaStreamSynchronize(stream);
@@ -235,7 +299,14 @@ void Pipeline::runInverse(const std::unordered_map<int, std::pair<void*, size_t>
         for (auto* n : lv) fwd.push_back({n->stage, n->input_buffer_ids, n->output_buffer_ids});
     for (auto& s : stages_) s->saveState();
     try {
-        run_inverse(fwd, outputs, input_buffer_id_, pool_.get(), d_result, capacity, result_size, stream, fused_);
+        InverseCtx ctx;
+        ctx.gather = &gather_;
+        ctx.work = &inv_work_;
+        ctx.work_bytes = &inv_work_bytes_;
+        ctx.enqueue_reads = [this](cudaStream_t st) { return enqueueResultReads(st); };
+        ctx.finish_reads = [this]() { finishResultReads(); };
+        run_inverse(fwd, outputs, input_buffer_id_, pool_.get(), d_result, capacity, result_size, stream, fused_,
+                    &ctx);
     } catch (...) {
         for (auto& s : stages_) {
             s->setInverse(false);
@@ -304,12 +375,17 @@ void Pipeline::decompress(const void* d_input, size_t input_size, void** d_outpu
         return;
     }
     void* d_final = nullptr;
-    if (pool_managed_decomp_) {
+    if (pool_managed_decomp_ && decomp_outputs_.size() == 1 && decomp_output_bytes_ >= cap) {
+        // the previous call's output is released by this call: reuse it
+        d_final = decomp_outputs_[0];
+    } else if (pool_managed_decomp_) {
         for (void* p : decomp_outputs_) pool_->free(p, stream);
         decomp_outputs_.clear();
+        decomp_output_bytes_ = 0;
         d_final = pool_->allocate(cap, stream, "decomp_output", true);
         if (!d_final) throw std::runtime_error("Pool allocation for decompress output failed");
         decomp_outputs_.push_back(d_final);
+        decomp_output_bytes_ = cap;
     } else {
         cuda_check(cudaMalloc(&d_final, cap), "cudaMalloc for decompress output");
     }

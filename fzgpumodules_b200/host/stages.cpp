@@ -51,8 +51,20 @@ void StageWorkspace::release() {
 
 void StageWorkspace::checkStatus(cudaStream_t stream, const char* what) const {
     if (!ptr_) return;
-    const int st = fzb_workspace_status(ptr_, stream);
+    int st;
+    if (fetched_) {  // gathered (and cleared on the device) before the pipeline's wait
+        fetched_ = false;
+        st = fzb_status_from_bits(h_bits_, nullptr);
+    } else {
+        st = fzb_workspace_status(ptr_, stream);
+    }
     if (st != FZB_OK) throw std::runtime_error(std::string(what) + ": " + fzb_status_string(st));
+}
+
+// The status word is the workspace's first u32 (what fzb_workspace_status reads).
+void StageWorkspace::pendingStatus(std::vector<DeviceRead>& out) const {
+    if (!ptr_) return;
+    out.push_back({ptr_, 4, &h_bits_, true});
 }
 
 void* StageWorkspace::ensure(size_t bytes, MemoryPool* pool, cudaStream_t stream) {
@@ -216,8 +228,14 @@ void LorenzoQuantStage<TInput, TCode>::postStreamSync(cudaStream_t stream) {
     pending_ = false;
     uint32_t count = 0;
     float st[4] = {0, 0, 0, 0};
-    check_cuda(cudaMemcpy(&count, d_count_, 4, cudaMemcpyDeviceToHost), "LorenzoQuant outlier count");
-    check_cuda(cudaMemcpy(st, d_eb_state_, sizeof(st), cudaMemcpyDeviceToHost), "LorenzoQuant eb state");
+    if (fetched_) {  // gathered before the pipeline's wait
+        fetched_ = false;
+        count = h_count_;
+        std::memcpy(st, h_state_, sizeof(st));
+    } else {
+        check_cuda(cudaMemcpy(&count, d_count_, 4, cudaMemcpyDeviceToHost), "LorenzoQuant outlier count");
+        check_cuda(cudaMemcpy(st, d_eb_state_, sizeof(st), cudaMemcpyDeviceToHost), "LorenzoQuant eb state");
+    }
     computed_abs_eb_ = st[1];
     computed_value_base_ = (config_.eb_mode == ErrorBoundMode::ABS) ? 0.0f : st[0];
     const size_t cap = getMaxOutlierCount(num_elements_);
@@ -225,6 +243,31 @@ void LorenzoQuantStage<TInput, TCode>::postStreamSync(cudaStream_t stream) {
     actual_outlier_count_ = count;
     actual_[1] = count * sizeof(TInput);
     actual_[2] = count * sizeof(uint32_t);
+}
+
+template <typename TInput, typename TCode>
+void LorenzoQuantStage<TInput, TCode>::pendingReads(std::vector<DeviceRead>& out) {
+    if (is_inverse_) {
+        inv_ws_.pendingStatus(out);
+        return;
+    }
+    if (!pending_) return;
+    out.push_back({d_count_, 4, &h_count_, false});
+    out.push_back({d_eb_state_, sizeof(h_state_), h_state_, false});
+}
+
+template <typename TInput, typename TCode>
+void LorenzoQuantStage<TInput, TCode>::resultsFetched() {
+    if (is_inverse_) inv_ws_.statusFetched();
+    else fetched_ = pending_;
+}
+
+// The outlier lists hold min(count, capacity) entries (postStreamSync's clamp).
+template <typename TInput, typename TCode>
+bool LorenzoQuantStage<TInput, TCode>::deviceOutputSize(int index, DeviceSize* ds) const {
+    if (is_inverse_ || !pending_ || (index != 1 && index != 2)) return false;
+    *ds = {d_count_, 4, index == 1 ? sizeof(TInput) : sizeof(uint32_t), getMaxOutlierCount(num_elements_)};
+    return true;
 }
 
 template <typename TInput, typename TCode>
@@ -327,6 +370,12 @@ size_t RZEStage::estimateScratchBytes(const std::vector<size_t>& s) const {
 
 void RZEStage::readBack() const {
     if (!d_size_) return;
+    if (fetched_) {  // gathered before the pipeline's wait
+        fetched_ = false;
+        actual_ = (size_t)h_size_;
+        d_size_ = nullptr;
+        return;
+    }
     cudaStreamSynchronize(pending_stream_);
     uint64_t v = 0;
     check_cuda(cudaMemcpy(&v, d_size_, 8, cudaMemcpyDeviceToHost), "RZE size read-back");
@@ -413,6 +462,12 @@ std::vector<size_t> RLEStage<T>::estimateOutputSizes(const std::vector<size_t>& 
 template <typename T>
 void RLEStage<T>::readBack() const {
     if (!d_size_) return;
+    if (fetched_) {  // gathered before the pipeline's wait
+        fetched_ = false;
+        actual_ = (size_t)h_size_;
+        d_size_ = nullptr;
+        return;
+    }
     cudaStreamSynchronize(pending_stream_);
     uint64_t v = 0;
     check_cuda(cudaMemcpy(&v, d_size_, 8, cudaMemcpyDeviceToHost), "RLE size read-back");

@@ -183,20 +183,46 @@ template <typename TInput, typename TCode>
 void QuantizerStage<TInput, TCode>::postStreamSync(cudaStream_t stream) {
     if (is_inverse_ || !pending_) return;
     pending_ = false;
+    const bool fetched = fetched_;  // gathered before the pipeline's wait
+    fetched_ = false;
     ws_.checkStatus(stream, "QuantizerStage");
     float st[4] = {0, 0, 0, 0};
-    check_cuda(cudaMemcpy(st, d_eb_state_, sizeof(st), cudaMemcpyDeviceToHost), "Quantizer eb state");
+    if (fetched) std::memcpy(st, h_state_, sizeof(st));
+    else check_cuda(cudaMemcpy(st, d_eb_state_, sizeof(st), cudaMemcpyDeviceToHost), "Quantizer eb state");
     if (config_.eb_mode == ErrorBoundMode::NOA) {
         computed_value_base_ = st[0];
         computed_abs_eb_ = st[1];
     }
     if (d_count_) {
-        uint32_t count = 0;  // already min(outliers, capacity) on the device
-        check_cuda(cudaMemcpy(&count, d_count_, 4, cudaMemcpyDeviceToHost), "Quantizer outlier count");
+        uint32_t count = h_count_;  // already min(outliers, capacity) on the device
+        if (!fetched)
+            check_cuda(cudaMemcpy(&count, d_count_, 4, cudaMemcpyDeviceToHost), "Quantizer outlier count");
         actual_outlier_count_ = count;
         actual_[1] = count * sizeof(TInput);
         actual_[2] = count * sizeof(uint32_t);
     }
+}
+
+template <typename TInput, typename TCode>
+void QuantizerStage<TInput, TCode>::pendingReads(std::vector<DeviceRead>& out) {
+    if (is_inverse_ || !pending_) return;
+    ws_.pendingStatus(out);
+    out.push_back({d_eb_state_, sizeof(h_state_), h_state_, false});
+    if (d_count_) out.push_back({d_count_, 4, &h_count_, false});
+}
+
+template <typename TInput, typename TCode>
+void QuantizerStage<TInput, TCode>::resultsFetched() {
+    if (is_inverse_ || !pending_) return;
+    ws_.statusFetched();
+    fetched_ = true;
+}
+
+template <typename TInput, typename TCode>
+bool QuantizerStage<TInput, TCode>::deviceOutputSize(int index, DeviceSize* ds) const {
+    if (is_inverse_ || !pending_ || !d_count_ || (index != 1 && index != 2)) return false;
+    *ds = {d_count_, 4, index == 1 ? sizeof(TInput) : sizeof(uint32_t), ~0ull / sizeof(TInput)};
+    return true;
 }
 
 template <typename TInput, typename TCode>

@@ -33,6 +33,27 @@
 
 namespace fz {
 
+// Mapped pinned host block that small device results (sizes, counts, error
+// bounds, status words) are copied into by one kernel enqueued before a
+// stream wait (fzb_gather_words), instead of one blocking copy per value.
+class ResultGather {
+public:
+    ResultGather() = default;
+    ~ResultGather();
+    ResultGather(const ResultGather&) = delete;
+    ResultGather& operator=(const ResultGather&) = delete;
+    // False when nothing was enqueued (more reads than one launch takes, no
+    // mapped memory); the caller then reads the values itself.
+    bool enqueue(const std::vector<DeviceRead>& reads, cudaStream_t stream);
+    // After the wait: copies each value to its dst.
+    void finish(const std::vector<DeviceRead>& reads) const;
+
+private:
+    static constexpr size_t kBytes = 4096;
+    void* host_ = nullptr;
+    void* dev_ = nullptr;
+};
+
 enum class MemoryStrategy {
     MINIMAL,      // allocate at first use, free after the last consumer
     PREALLOCATE,  // one arena sized at finalize(); buffers with disjoint lifetimes share it
@@ -255,6 +276,14 @@ private:
     void collectMetadata();
     void concatOutputs(void* d_out, size_t capacity, size_t* out_size, cudaStream_t stream);
     size_t concatSize() const;
+    // Concatenation enqueued before the wait, with the sizes the device
+    // holds; false (nothing enqueued) when a stage's sizes are host-only.
+    bool enqueueDeviceConcat(cudaStream_t stream);
+    // The stages' pending device results, gathered into the mapped block by
+    // one kernel before the wait (false: nothing gathered, the stages read
+    // their own); distributed after it.
+    bool enqueueResultReads(cudaStream_t stream);
+    void finishResultReads();
     // Inverse over the forward topology: fwd buffer id -> (pointer, bytes).
     // Returns the reconstructed source buffer (pool- or caller-owned).
     void runInverse(const std::unordered_map<int, std::pair<void*, size_t>>& outputs, void* d_result,
@@ -313,7 +342,17 @@ private:
     void* concat_buf_ = nullptr;
     size_t concat_bytes_ = 0;
     std::vector<void*> decomp_outputs_;
+    size_t decomp_output_bytes_ = 0;  // capacity of decomp_outputs_[0]
     uint64_t* d_fused_size_ = nullptr;  // device u64 for the fused path's stream size
+    ResultGather gather_;
+    std::vector<DeviceRead> reads_;
+    std::vector<DeviceResults*> read_stages_;
+    bool concat_enqueued_ = false;
+    uint64_t dev_concat_caps_[FZM_MAX_BUFFERS] = {};
+    bool dev_concat_fixed_[FZM_MAX_BUFFERS] = {};
+    // the fused inverse's workspace, kept between decompress calls
+    void* inv_work_ = nullptr;
+    size_t inv_work_bytes_ = 0;
     PipelinePerfResult last_perf_;
 };
 

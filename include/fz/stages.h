@@ -24,6 +24,46 @@
 
 namespace fz {
 
+// A small device result that a stage reads on the host after a
+// synchronisation: a stream size, an outlier count, the resolved error
+// bound, a status word.
+struct DeviceRead {
+    const void* src = nullptr;  // device address, 4-byte aligned
+    uint32_t bytes = 0;         // a multiple of 4, at most 256
+    void* dst = nullptr;        // host destination, filled after the wait
+    bool clear = false;         // zero the device word once read (status words)
+};
+
+// Where an output's size lives on the device before the wait:
+// min(*word, max_count) * scale bytes (word a u32 or u64).
+struct DeviceSize {
+    const void* word = nullptr;
+    uint32_t word_bytes = 4;
+    uint64_t scale = 1;
+    uint64_t max_count = ~0ull;
+};
+
+// Implemented by this library's stages.  A pipeline collects the pending
+// reads of every stage, copies them into one mapped host block with one
+// kernel enqueued before its single stream wait (fzb_gather_words), fills
+// each dst and calls resultsFetched(); postStreamSync then uses the copies
+// instead of issuing its own blocking copies.  Run alone, a stage reads
+// them itself.  A pipeline whose stages all implement this also enqueues
+// its output concatenation before the wait (fzb_concat_dev), taking the
+// sizes the device holds from deviceOutputSize().
+class DeviceResults {
+public:
+    virtual ~DeviceResults() = default;
+    virtual void pendingReads(std::vector<DeviceRead>& out) { (void)out; }
+    virtual void resultsFetched() {}
+    // False when getActualOutputSize(index) is already exact on the host.
+    virtual bool deviceOutputSize(int index, DeviceSize* ds) const {
+        (void)index;
+        (void)ds;
+        return false;
+    }
+};
+
 // Device workspace owned by a stage, drawn from the pipeline's pool (or
 // cudaMalloc when the stage runs without a pool) and grown on demand.
 class StageWorkspace {
@@ -36,14 +76,20 @@ public:
     size_t size() const { return bytes_; }
     void* get() const { return ptr_; }
     // Throws when a kernel latched an error (malformed input, a bounded
-    // wait that gave up) in this workspace; clears it.
+    // wait that gave up) in this workspace; clears it.  Uses the status
+    // word a pipeline fetched (pendingStatus) when there is one.
     void checkStatus(cudaStream_t stream, const char* what) const;
+    // Adds the status word to a pipeline's gathered reads.
+    void pendingStatus(std::vector<DeviceRead>& out) const;
+    void statusFetched() const { fetched_ = ptr_ != nullptr; }
 
 private:
     void release();
     void* ptr_ = nullptr;
     size_t bytes_ = 0;
     MemoryPool* pool_ = nullptr;
+    mutable uint32_t h_bits_ = 0;
+    mutable bool fetched_ = false;
 };
 
 // ---------------------------------------------------------------------------
@@ -76,7 +122,7 @@ struct LorenzoQuantConfig {
 static_assert(sizeof(LorenzoQuantConfig) == 44, "LorenzoQuantConfig is 44 bytes");
 
 template <typename TInput = float, typename TCode = uint16_t>
-class LorenzoQuantStage : public Stage {
+class LorenzoQuantStage : public Stage, public DeviceResults {
     static_assert(std::is_same<TInput, float>::value && std::is_same<TCode, uint16_t>::value,
                   "the sm_100a kernels implement LorenzoQuantStage<float, uint16_t>");
 
@@ -100,6 +146,9 @@ public:
                  const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
     void postStreamSync(cudaStream_t stream) override;
     void onGraphReplay(cudaStream_t) override { pending_ = !is_inverse_ && d_count_ != nullptr; }
+    void pendingReads(std::vector<DeviceRead>& out) override;
+    void resultsFetched() override;
+    bool deviceOutputSize(int index, DeviceSize* ds) const override;
 
     std::string getName() const override { return "LorenzoQuant"; }
     size_t getNumInputs() const override { return is_inverse_ ? 4 : 1; }
@@ -173,6 +222,9 @@ private:
     const void* d_count_ = nullptr;  // pending read-back (forward)
     float* d_eb_state_ = nullptr;    // inside the workspace
     bool pending_ = false;
+    bool fetched_ = false;  // h_count_ / h_state_ hold the pending values
+    uint32_t h_count_ = 0;
+    float h_state_[4] = {0, 0, 0, 0};
     bool inv_dev_eb_ = false;
     StageWorkspace ws_;
     StageWorkspace inv_ws_;  // the inverse's own, so the forward eb state survives it
@@ -181,7 +233,7 @@ private:
 // ---------------------------------------------------------------------------
 // Bitshuffle (bit-plane transpose per block), size-preserving.
 // ---------------------------------------------------------------------------
-class BitshuffleStage : public Stage {
+class BitshuffleStage : public Stage, public DeviceResults {
 public:
     BitshuffleStage() = default;
     void setInverse(bool inv) override { is_inverse_ = inv; }
@@ -231,7 +283,7 @@ private:
 // ---------------------------------------------------------------------------
 // RZE (recursive zero-byte elimination over 16 KiB chunks, 4 levels).
 // ---------------------------------------------------------------------------
-class RZEStage : public Stage {
+class RZEStage : public Stage, public DeviceResults {
 public:
     RZEStage() = default;
     void setInverse(bool inv) override { is_inverse_ = inv; }
@@ -250,6 +302,19 @@ public:
         if (is_inverse_ || !last_size_) return;
         d_size_ = last_size_;
         pending_stream_ = stream;
+    }
+    void pendingReads(std::vector<DeviceRead>& out) override {
+        if (is_inverse_) ws_.pendingStatus(out);
+        else if (d_size_) out.push_back({d_size_, 8, &h_size_, false});
+    }
+    void resultsFetched() override {
+        if (is_inverse_) ws_.statusFetched();
+        else fetched_ = d_size_ != nullptr;
+    }
+    bool deviceOutputSize(int index, DeviceSize* ds) const override {
+        if (is_inverse_ || !d_size_ || index != 0) return false;
+        *ds = {d_size_, 8, 1, ~0ull};
+        return true;
     }
     std::string getName() const override { return "RZE"; }
     size_t getNumInputs() const override { return 1; }
@@ -294,6 +359,8 @@ private:
     mutable const uint64_t* d_size_ = nullptr;  // pending read-back
     const uint64_t* last_size_ = nullptr;       // where the last forward run writes its size
     mutable cudaStream_t pending_stream_ = nullptr;
+    mutable bool fetched_ = false;  // h_size_ holds *d_size_
+    uint64_t h_size_ = 0;
     Saved saved_;
     StageWorkspace ws_;
     uint64_t* d_size_own_ = nullptr;  // inside ws_
@@ -303,7 +370,7 @@ private:
 // RLE: [u32 runs][values, padded to 4 B][u32 lengths].
 // ---------------------------------------------------------------------------
 template <typename T>
-class RLEStage : public Stage {
+class RLEStage : public Stage, public DeviceResults {
     static_assert(std::is_same<T, uint8_t>::value || std::is_same<T, uint16_t>::value ||
                       std::is_same<T, uint32_t>::value || std::is_same<T, int32_t>::value,
                   "RLEStage element types: uint8_t, uint16_t, uint32_t, int32_t");
@@ -319,6 +386,19 @@ public:
         if (is_inverse_ || !last_size_) return;
         d_size_ = last_size_;
         pending_stream_ = stream;
+    }
+    void pendingReads(std::vector<DeviceRead>& out) override {
+        if (is_inverse_) ws_.pendingStatus(out);
+        else if (d_size_) out.push_back({d_size_, 8, &h_size_, false});
+    }
+    void resultsFetched() override {
+        if (is_inverse_) ws_.statusFetched();
+        else fetched_ = d_size_ != nullptr;
+    }
+    bool deviceOutputSize(int index, DeviceSize* ds) const override {
+        if (is_inverse_ || !d_size_ || index != 0) return false;
+        *ds = {d_size_, 8, 1, ~0ull};
+        return true;
     }
     std::string getName() const override { return "RLE"; }
     size_t getNumInputs() const override { return 1; }
@@ -353,6 +433,8 @@ private:
     mutable const uint64_t* d_size_ = nullptr;
     const uint64_t* last_size_ = nullptr;
     mutable cudaStream_t pending_stream_ = nullptr;
+    mutable bool fetched_ = false;  // h_size_ holds *d_size_
+    uint64_t h_size_ = 0;
     StageWorkspace ws_;
 };
 
@@ -362,7 +444,7 @@ private:
 enum class HuffmanEncodeMode { Coarse, Fine };
 
 template <typename T>
-class HuffmanStage : public Stage {
+class HuffmanStage : public Stage, public DeviceResults {
     static_assert(std::is_same<T, uint16_t>::value, "the sm_100a Huffman coder implements uint16_t symbols");
 
 public:
@@ -380,6 +462,12 @@ public:
                  const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
     void postStreamSync(cudaStream_t stream) override {
         if (is_inverse_) ws_.checkStatus(stream, "HuffmanStage (inverse)");
+    }
+    void pendingReads(std::vector<DeviceRead>& out) override {
+        if (is_inverse_) ws_.pendingStatus(out);
+    }
+    void resultsFetched() override {
+        if (is_inverse_) ws_.statusFetched();
     }
     std::string getName() const override { return "Huffman"; }
     size_t getNumInputs() const override { return 1; }
@@ -425,7 +513,7 @@ private:
 // Bitpack: low nbits of each element, nbits a power of two (or detected).
 // ---------------------------------------------------------------------------
 template <typename T>
-class BitpackStage : public Stage {
+class BitpackStage : public Stage, public DeviceResults {
     static_assert(std::is_same<T, uint8_t>::value || std::is_same<T, uint16_t>::value ||
                       std::is_same<T, uint32_t>::value,
                   "BitpackStage: T must be uint8_t, uint16_t or uint32_t");
@@ -506,7 +594,7 @@ struct QuantizerConfig {
 static_assert(sizeof(QuantizerConfig) == 36, "QuantizerConfig is 36 bytes");
 
 template <typename TInput = float, typename TCode = uint16_t>
-class QuantizerStage : public Stage {
+class QuantizerStage : public Stage, public DeviceResults {
     static_assert(std::is_same<TInput, float>::value &&
                       (std::is_same<TCode, uint16_t>::value || std::is_same<TCode, uint32_t>::value),
                   "the sm_100a kernels implement QuantizerStage<float, uint16_t / uint32_t>");
@@ -532,6 +620,9 @@ public:
                  const std::vector<void*>& outputs, const std::vector<size_t>& sizes) override;
     void postStreamSync(cudaStream_t stream) override;
     void onGraphReplay(cudaStream_t) override { pending_ = !is_inverse_ && d_eb_state_ != nullptr && ran_; }
+    void pendingReads(std::vector<DeviceRead>& out) override;
+    void resultsFetched() override;
+    bool deviceOutputSize(int index, DeviceSize* ds) const override;
 
     std::string getName() const override { return "Quantizer"; }
     size_t getNumInputs() const override { return is_inverse_ ? (isInplaceMode() ? 1 : 4) : 1; }
@@ -619,6 +710,9 @@ private:
     float computed_value_base_ = 0.0f;
     const void* d_count_ = nullptr;
     float* d_eb_state_ = nullptr;  // inside the workspace
+    bool fetched_ = false;  // h_count_ / h_state_ hold the pending values
+    uint32_t h_count_ = 0;
+    float h_state_[4] = {0, 0, 0, 0};
     Saved saved_;
     StageWorkspace ws_;
 };
@@ -628,7 +722,7 @@ private:
 // chunks; TOut the unsigned type of T's width fuses negabinary coding.
 // ---------------------------------------------------------------------------
 template <typename T, typename TOut = T>
-class DifferenceStage : public Stage {
+class DifferenceStage : public Stage, public DeviceResults {
     static_assert(std::is_integral<T>::value && sizeof(T) == sizeof(TOut) &&
                       (std::is_same<T, TOut>::value || (std::is_signed<T>::value && std::is_unsigned<TOut>::value)),
                   "the sm_100a kernels implement integer DifferenceStage<T> and <signed, unsigned> pairs");
@@ -688,7 +782,7 @@ struct LorenzoConfig {
 static_assert(sizeof(LorenzoConfig) == 16, "LorenzoConfig is 16 bytes");
 
 template <typename T>
-class LorenzoStage : public Stage {
+class LorenzoStage : public Stage, public DeviceResults {
     static_assert(std::is_integral<T>::value && std::is_signed<T>::value, "LorenzoStage requires a signed integer type");
 
 public:
@@ -737,7 +831,7 @@ private:
 // width, header [u8 TIn type][u8 TOut type].
 // ---------------------------------------------------------------------------
 template <typename TIn, typename TOut, bool NEGABINARY>
-class SignCodingStage : public Stage {
+class SignCodingStage : public Stage, public DeviceResults {
     static_assert(std::is_integral<TIn>::value && std::is_signed<TIn>::value && std::is_unsigned<TOut>::value &&
                       sizeof(TIn) == sizeof(TOut),
                   "TIn signed, TOut its unsigned counterpart");

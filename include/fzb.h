@@ -349,6 +349,36 @@ int fzb_concat(const void* const* d_srcs, const uint64_t* sizes, int n, void* d_
  * (src/pipeline/compressor_exec.cpp:198-355). */
 int fzb_concat_split(const void* d_in, uint64_t in_capacity, void* const* d_dsts, const uint64_t* capacities,
                      int n, uint32_t* d_err, void* stream);
+/* fzb_concat enqueued before the segment sizes reach the host: segment i
+ * is min(w, size_max[i]) * size_scale[i] bytes, w the u32 (size_word_bytes
+ * 4) or u64 (8) at d_size_words[i], or caps[i] bytes when d_size_words[i] is
+ * null; a length above caps[i] is cut to caps[i].  d_out holds
+ * fzb_concat_bytes(caps, n) bytes.  The header carries the device lengths,
+ * so the output equals fzb_concat of the same segments.  No counterpart in
+ * the reference, whose Pipeline::compress waits for the sizes before
+ * concatOutputs (src/pipeline/compressor_exec.cpp:119-152,
+ * compressor.cpp:853). */
+int fzb_concat_dev(const void* const* d_srcs, const uint64_t* caps, const void* const* d_size_words,
+                   const uint32_t* size_word_bytes, const uint64_t* size_scale, const uint64_t* size_max,
+                   int n, void* d_out, void* stream);
+
+/* Small device results gathered for one host wait: word i (bytes[i], a
+ * multiple of 4 up to 256, from a 4-byte aligned d_srcs[i]) is copied to
+ * dst + offset_i, offset_i the sum of the previous lengths rounded up to 8
+ * bytes each, and the source is zeroed afterwards when clear[i] (status
+ * words).  dst is memory the device can store to: mapped pinned host memory
+ * (cudaHostAlloc with cudaHostAllocMapped) read after the stream has been
+ * synchronised.  n <= FZB_GATHER_MAX; one launch.  The reference reads each
+ * such value with its own blocking copy (lorenzo_quant.cu:728-731,
+ * rze_stage.cu:853,868, rle.cu:202-204). */
+#define FZB_GATHER_MAX 32
+int fzb_gather_words(const void* const* d_srcs, const uint32_t* bytes, const uint8_t* clear, int n, void* dst,
+                     void* stream);
+/* The status fzb_workspace_status() returns for a status word read without
+ * it (through fzb_gather_words).  *rerun_exact (may be null) is set to 1
+ * when a decompression issued with FZB_NO_SYNC left a case to the exact
+ * kernels: the call is then repeated with FZB_FORCE_EXACT. */
+int fzb_status_from_bits(uint32_t bits, int* rerun_exact);
 
 /* ------------------------------------------------------------------------
  * Batched compression of many fields (no reference counterpart: it runs the

@@ -37,6 +37,30 @@ def test_invalid_arguments_rejected_before_launch():
     assert rc == -1
 
 
+def test_status_bits_and_gather_arguments():
+    L = _lib.lib()
+    rerun = C.c_int(-1)
+    # bit 1 look-back timeout, 2 malformed, 4 inexact, 8 unsorted, 16 TMA timeout
+    for bits, st, rr in [(0, 0, 0), (1, -6, 0), (2, -5, 0), (3, -5, 0), (4, 0, 1), (8, 0, 1), (16, -6, 0),
+                         (6, -5, 1)]:
+        assert L.fzb_status_from_bits(bits, C.byref(rerun)) == st
+        assert rerun.value == rr
+    assert L.fzb_status_from_bits(2, None) == -5
+    # invalid gathers are refused on the host (no pointer is dereferenced)
+    fake = 0x10000
+
+    def gather(ptrs, nbytes, dst=fake):
+        n = len(ptrs)
+        return L.fzb_gather_words((C.c_void_p * n)(*ptrs), (C.c_uint32 * n)(*nbytes), (C.c_uint8 * n)(*([0] * n)),
+                                  n, C.c_void_p(dst), None)
+    assert gather([fake], [6]) == -1          # not a multiple of 4
+    assert gather([fake], [260]) == -1        # above 256 bytes
+    assert gather([fake + 2], [4]) == -1      # misaligned source
+    assert gather([fake], [4], fake + 4) == -1  # destination not 8-byte aligned
+    assert gather([fake] * 33, [4] * 33) == -1  # more than one launch takes
+    assert L.fzb_concat_dev(None, None, None, None, None, None, 0, None, None) == -1
+
+
 def test_huffman_host_codebook_matches_oracle_and_reference():
     """fzb_huff_book is host code: it runs here and must equal the oracle's
     and (when built) the reference's phf_CPU_build_canonized_codebook_v2."""
