@@ -26,7 +26,7 @@ device time of the fused C-ABI call); beside it in the same JSON line:
   clocks           nvidia-smi samples taken during the timed region.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-  python bench.py --workload c1|cli|c3|batch|selector|pfpl   (secondary
+  python bench.py --workload c1|cli|c3|batch|selector|pfpl|timeline   (secondary
       workloads, one JSON line each; fzgpumodules_b200/benchmarks.py;
       --impl reference --workload pfpl times the reference's own pipeline)
 
@@ -635,7 +635,8 @@ def main():
                     help="method-generated chunks the coder selector trains on (selector entry / workload)")
     ap.add_argument("--dims", type=int, nargs=3, default=list(DEFAULT_DIMS), metavar=("NX", "NY", "NZ"),
                     help="field extents (x fastest); the default is the 512^3 workload")
-    ap.add_argument("--workload", default="chain", choices=["chain", "c1", "cli", "c3", "batch", "selector", "pfpl"],
+    ap.add_argument("--workload", default="chain",
+                    choices=["chain", "c1", "cli", "c3", "batch", "selector", "pfpl", "timeline"],
                     help="chain: the headline LQ3D->BS->RZE line; others: secondary workloads (1 GPU)")
     args = ap.parse_args()
     if args.workload == "pfpl" and args.impl == "reference":

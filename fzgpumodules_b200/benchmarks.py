@@ -15,7 +15,10 @@ as one JSON line with the same keys as the headline line:
 * ``selector``  2 GiB of mixed fields -> LorenzoQuant (REL 1e-3) codes in 64 KiB
                 chunks, coded by exhaustive trial and by the trained MLP selector;
 * ``pfpl``      the pfpl preset, Quantizer (REL 1e-3) -> Difference -> Bitshuffle
-                -> RZE, on a 512^3 field, as kernels and through fz::Pipeline.
+                -> RZE, on a 512^3 field, as kernels and through fz::Pipeline;
+* ``timeline``  a CUPTI timeline (torch.profiler) of fz::Pipeline calls on the
+                512^3 chain: host time, GPU busy time, idle gaps and blocking
+                calls per call.
 
 Timing: CUDA events on the launching stream after warm-up; inputs larger than
 L2 or an L2 flush between timed iterations.
@@ -453,5 +456,103 @@ def run_pfpl(args, dev):
                           "back; pipeline_* through fz::Pipeline (which runs the one-pass chain; host syncs included)"})
 
 
+def _kname(name: str) -> str:
+    """A kernel's name without its return type, namespaces' anonymous parts
+    and parameter list."""
+    n = name.replace("void ", "").replace("(anonymous namespace)::", "")
+    return n.split("(")[0][:60].strip()
+
+
+def pipeline_timeline(dev, calls: int = 3) -> dict:
+    """Where the time of a fz::Pipeline call goes, from a CUPTI timeline
+    (torch.profiler) of `calls` compress and decompress calls of the 512^3
+    LQ3D(REL 1e-3) -> Bitshuffle -> RZE chain (PREALLOCATE), each after an L2
+    flush: per call its host duration, the host time before the first GPU
+    operation, the GPU busy time and the idle gaps between GPU operations,
+    the time from the last GPU operation's end to the call's return, and the
+    blocking calls it made (stream / device synchronisations, synchronous
+    copies).  Kernel names and durations are listed for the last call."""
+    from torch.profiler import ProfilerActivity, profile, record_function
+
+    from .pipeline import PREALLOCATE, REL, BitshuffleStage, LorenzoQuantStage, Pipeline, RZEStage
+    x = F.grf((512, 512, 512), seed=1002, spike_frac=1e-3, device=dev).reshape(-1)
+    n = x.numel()
+    pl = Pipeline(4 * n, PREALLOCATE)
+    pl.setDims(512, 512, 512)
+    lq = pl.addStage(LorenzoQuantStage(1e-3, 32768, 0.1, REL, True))
+    bs = pl.addStage(BitshuffleStage(16384, 2))
+    rz = pl.addStage(RZEStage(16384, 4))
+    pl.connect(bs, lq, "codes")
+    pl.connect(rz, bs)
+    pl.finalize()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(3):
+        pl.compress(x)
+        pl.decompress(None)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CPU, ProfilerActivity.CUDA]) as prof:
+        for i in range(calls):
+            flush.zero_()
+            torch.cuda.synchronize()
+            with record_function(f"call:compress:{i}"):
+                pl.compress(x)
+            flush.zero_()
+            torch.cuda.synchronize()
+            with record_function(f"call:decompress:{i}"):
+                pl.decompress(None)
+    pl.close()
+    import os
+    import tempfile
+    fd, path = tempfile.mkstemp(suffix=".json")
+    os.close(fd)
+    try:
+        prof.export_chrome_trace(path)
+        with open(path) as f:
+            trace = json.load(f)
+    finally:
+        os.remove(path)
+    ev = [e for e in trace.get("traceEvents", []) if e.get("ph") == "X"]
+    calls_ev = [e for e in ev if str(e.get("name", "")).startswith("call:")]
+    gpu = sorted((e["ts"], e["ts"] + e["dur"], e["name"]) for e in ev
+                 if e.get("cat") in ("kernel", "gpu_memcpy", "gpu_memset"))
+    api = [(e["ts"], e["ts"] + e["dur"], e["name"]) for e in ev if e.get("cat") == "cuda_runtime"]
+    out = {}
+    for c in sorted(calls_ev, key=lambda e: e["ts"]):
+        kind = c["name"].split(":")[1]
+        t0, t1 = c["ts"], c["ts"] + c["dur"]
+        g = [k for k in gpu if t0 <= k[0] < t1]
+        if not g:
+            continue
+        busy = sum(k[1] - k[0] for k in g)
+        gaps, end = 0.0, g[0][1]
+        for k in g[1:]:
+            gaps += max(0.0, k[0] - end)
+            end = max(end, k[1])
+        blocking = [a[2] for a in api if t0 <= a[0] < t1 and ("Synchronize" in a[2] or a[2] == "cudaMemcpy")]
+        rec = {"call_us": t1 - t0, "host_before_first_gpu_op_us": g[0][0] - t0, "gpu_busy_us": busy,
+               "gpu_gaps_us": gaps, "last_gpu_end_to_return_us": t1 - end,
+               "gpu_ops": len(g), "blocking_calls": {b: blocking.count(b) for b in sorted(set(blocking))},
+               "kernels_us": [[_kname(k[2]), round(k[1] - k[0], 1)] for k in g]}
+        out.setdefault(kind, []).append(rec)
+    summary = {}
+    for kind, recs in out.items():
+        m = {k: float(np.mean([r[k] for r in recs])) for k in
+             ("call_us", "host_before_first_gpu_op_us", "gpu_busy_us", "gpu_gaps_us", "last_gpu_end_to_return_us")}
+        m["gpu_ops"] = recs[-1]["gpu_ops"]
+        m["blocking_calls"] = recs[-1]["blocking_calls"]
+        m["kernels_us_last_call"] = recs[-1]["kernels_us"]
+        m["gbs_by_call"] = 4 * n / m["call_us"] / 1e3
+        summary[kind] = m
+    return summary
+
+
+def run_timeline(args, dev):
+    d = pipeline_timeline(dev, max(1, min(args.steps, 5)))
+    v = d.get("compress", {}).get("gbs_by_call", 0.0)
+    return _line("timeline: fz::Pipeline LQ3D(REL 1e-3)->Bitshuffle->RZE 512^3, CUPTI timeline of each call",
+                 v, "GB/s", args, {"calls": d, "note": "host clock of the profiled calls (profiler overhead "
+                                   "included); the breakdown, not the value, is the point"})
+
+
 WORKLOADS = {"c1": run_c1, "cli": run_cli, "c3": run_c3, "batch": run_batch, "selector": run_selector,
-             "pfpl": run_pfpl}
+             "pfpl": run_pfpl, "timeline": run_timeline}
