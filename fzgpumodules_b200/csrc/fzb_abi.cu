@@ -248,7 +248,7 @@ int forward_common(bool fused, const float* d_in, uint64_t n_total, const uint32
             rc = launch_lq3d_slab(a, (unsigned)(2 * sms), s) == 0 ? FZB_OK : FZB_E_CUDA;
         }
     } else if (!fused && g.ndim == 2 && nx % (uint32_t)kChunkCodes == 0 && g.nfield == n_total &&
-               !(flags_env() & 8)) {
+               lq_rows_supported(a) && !(flags_env() & 8)) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

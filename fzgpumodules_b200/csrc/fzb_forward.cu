@@ -931,68 +931,6 @@ __global__ void __launch_bounds__(kThreads, 3) lq_chunk_kernel(FwdArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Codes of a 2-D field whose rows are whole chunks (nx a multiple of 8192):
-// a CTA walks down a run of rows of one chunk column.  The window of
-// q(k - nx) a row needs is the previous row's window of q(k), already
-// quantised in shared memory, so each row after the run's first loads and
-// quantises one window instead of the chunk kernel's two.  Units are (chunk
-// column, run of rpr rows); the codes and outliers equal lq_chunk_kernel's.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 3) lq_rows_kernel(FwdArgs a, uint32_t m, uint32_t rpr, uint32_t units) {
-    extern __shared__ float4 Q[];
-    __shared__ uint32_t s_ws[16];
-    __shared__ uint32_t s_obase;
-    const bool vec_ok = (reinterpret_cast<uintptr_t>(a.in) & 15) == 0;
-    const float r = *a.ebx2_r;
-    const uint32_t ny = a.nfield / a.nx;
-    for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
-        const uint32_t col = u % m, y0 = (u / m) * rpr, y1 = min(ny, y0 + rpr);
-        int up_off = 0, cur_off = 0;
-        for (uint32_t y = y0; y < y1; y++) {
-            const uint32_t c = y * m + col;
-            const long long s0 = (long long)c * kChunkCodes, e0 = s0 + kChunkCodes;
-            int so = 0;
-            Roles R;
-            R.two = true;
-            R.z = false;
-            R.up0 = make_win(s0 - (long long)a.nx - 1, e0 - (long long)a.nx, so);
-            R.cur0 = make_win(s0 - 1, e0, so);
-            if (y == y0) {
-                up_off = R.up0.soff;
-                cur_off = R.cur0.soff;
-                load_window(Q, R.up0, a.in, a.nfield, r, vec_ok);
-            } else {  // the previous row's q(k) window serves as this row's q(k - nx)
-                const int t = up_off;
-                up_off = cur_off;
-                cur_off = t;
-            }
-            R.up0.soff = up_off;
-            R.cur0.soff = cur_off;
-            R.cur1 = R.cur0;
-            R.up1 = R.up0;
-            load_window(Q, R.cur0, a.in, a.nfield, r, vec_ok);
-            __syncthreads();
-            lq_chunk_body<2, false, true>(a, c, Q, s_ws, s_obase, &R);
-            __syncthreads();  // every read of this row's windows is done before the next load
-        }
-    }
-}
-
-int launch_lq_rows(const FwdArgs& a, unsigned sms, cudaStream_t s) {
-    const uint32_t m = a.nx / (uint32_t)kChunkCodes, ny = a.nfield / a.nx;
-    const uint32_t want = 3u * sms;
-    uint32_t rpr = (uint32_t)(((uint64_t)m * ny + want - 1) / want);
-    if (rpr < 1) rpr = 1;
-    const uint32_t runs = (ny + rpr - 1) / rpr, units = m * runs;
-    const uint32_t gran = ((((uint32_t)kChunkCodes + 1 + 3) / 4 + 1) + 7) & ~7u;
-    const size_t smem = (size_t)2 * gran * 16;
-    cudaError_t e = cudaFuncSetAttribute(lq_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return (int)e;
-    lq_rows_kernel<<<units < want ? units : want, kThreads, smem, s>>>(a, m, rpr, units);
-    return (int)cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
 // Batched fused compression: many fields, one persistent launch.  CTAs take
 // (field, chunk) units from a global counter in the order `unit_order`
 // lists the fields; every unit runs the same chunk body as the single-field

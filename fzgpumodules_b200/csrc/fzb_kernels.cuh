@@ -147,7 +147,9 @@ int launch_lq_chunk(int ndim, bool fused, bool rowal, const FwdArgs& a, size_t s
 // Slab-column fused 3-D kernel (see fzb_forward.cu); `grid` persistent CTAs.
 int launch_lq3d_slab(const FwdArgs& a, unsigned grid, cudaStream_t s);
 // Codes of a 2-D field whose rows are whole chunks (nx % 8192 == 0, no
-// padding past the field), rows walked down chunk columns.
+// padding past the field), rows walked down chunk columns (fzb_rows2d.cu);
+// needs a 16-byte aligned input, 8-byte aligned codes and radius <= 2^21.
+bool lq_rows_supported(const FwdArgs& a);
 int launch_lq_rows(const FwdArgs& a, unsigned sms, cudaStream_t s);
 // TMA-fed slab kernel (fzb_slab.cu): same applicability and bytes, plus a
 // 16-byte aligned input and radius <= 2^21.

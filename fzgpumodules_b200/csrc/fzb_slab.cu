@@ -42,14 +42,6 @@ namespace {
 constexpr int kOBytes = kChunkBytes + 128;    // level payload (+ slack for the second atomic word)
 constexpr size_t kSlabSmem = kSmemAlign + 2 * kStageBytes + kOBytes + kChunkBytes + 256;
 
-// Round half away from zero of y: trunc(y + copysign(0.49999997, y)) with the
-// add rounded to nearest equals round(y) for every float (for |y| >= 2^23 y is
-// already integral and the add returns y).  `sv` supplies the sign (of v, the
-// same as y's since the scale is positive).
-__device__ __forceinline__ uint32_t half_bits(float sv) {
-    return (__float_as_uint(sv) & 0x80000000u) | 0x3effffffu;
-}
-
 }  // namespace
 
 namespace {

@@ -90,6 +90,14 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) {
 
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: c + kMagic holds integer c in its low bits
 
+// Round half away from zero of y: trunc(y + copysign(0.49999997, y)) with the
+// add rounded to nearest equals round(y) for every float (for |y| >= 2^23 y is
+// already integral and the add returns y).  `sv` supplies the sign (of v, the
+// same as y's since the scale is positive).
+__device__ __forceinline__ uint32_t half_bits(float sv) {
+    return (__float_as_uint(sv) & 0x80000000u) | 0x3effffffu;
+}
+
 // Byte offset in a 128-byte-swizzled buffer of 16-byte granule g of row `row`
 // (the TMA SWIZZLE_128B layout: granule index XOR row % 8).  Thread t of a
 // slab kernel owns row t (32 floats).

@@ -110,7 +110,7 @@ def test_lq_forward_matches_oracle(cuda, dims, mode, zz, radius, kind):
     _check_outliers(out, x, dims, mode, radius, zz, cap, cnt, idx, err)
 
 
-@pytest.mark.parametrize("dims", [(37, 19, 5), (3000, 7, 1), (33, 17, 11), (20, 13, 9), (200, 9, 7)])
+@pytest.mark.parametrize("dims", [(37, 19, 5), (3000, 7, 1), (33, 17, 11), (20, 13, 9), (200, 9, 7), (8192, 6, 1)])
 def test_element_path_large_prequant_values(cuda, dims):
     """Rows that are not a multiple of 32 elements take the element path,
     which carries each element's x-neighbour terms along the run.  With an
@@ -299,6 +299,21 @@ def test_row_walk_codes_match_oracle(cuda, dims, mode, zz, radius, kind, monkeyp
         assert np.array_equal(_h(out["codes"]), codes), flag
         assert int(_h(out["count"])[0]) == cnt, flag
         _check_outliers(out, x, dims, mode, radius, zz, cap, cnt, idx, err)
+
+
+@pytest.mark.parametrize("dims", [(8192, 40, 1), (16384, 9, 1)])
+def test_row_walk_rounding_midpoints(cuda, dims, monkeypatch):
+    # the 2-D row walk quantizes in registers (round half away from zero as
+    # trunc(y + copysign(0.49999997, y))): next to every rounding midpoint
+    # its codes equal the oracle's and the per-chunk kernel's
+    n = int(np.prod(dims))
+    x = _midpoint_field(n, 37, 1e-3)
+    codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-3, O.ABS, 32768, True, n)
+    for flag in ("0", "8"):
+        monkeypatch.setenv("FZB_DISABLE_SLAB", flag)
+        out = kern().lq_forward(_g(x, cuda), dims, 1e-3, O.ABS, 32768, True, 1.0)
+        assert np.array_equal(_h(out["codes"]), codes), flag
+        assert int(_h(out["count"])[0]) == cnt, flag
 
 
 @pytest.mark.parametrize("dims", [(256, 64, 9), (512, 16, 8), (96, 40, 9)])
