@@ -804,6 +804,67 @@ int huff_encode_sub(const uint16_t* d_in, uint64_t n, uint32_t bklen, const uint
                ? FZB_OK : FZB_E_CUDA;
 }
 
+// Pinned host staging of the codebook round trip, one per host thread: the
+// histogram comes back and the book goes out with asynchronous copies (a
+// pageable copy stages through a driver buffer and blocks).  `done` marks
+// the end of the last upload, waited for before the buffers are rewritten.
+struct HfHostStage {
+    uint32_t* freq = nullptr;
+    uint32_t* bk4 = nullptr;
+    uint8_t* revbook = nullptr;
+    uint32_t bklen = 0;
+    int dev = -1;  // the device `done` belongs to
+    cudaEvent_t done = nullptr;
+    bool pending = false;
+    ~HfHostStage() { release(); }
+    void release() {
+        if (done) {
+            if (pending) cudaEventSynchronize(done);
+            cudaEventDestroy(done);
+        }
+        if (freq) cudaFreeHost(freq);
+        freq = nullptr;
+        bk4 = nullptr;
+        revbook = nullptr;
+        done = nullptr;
+        pending = false;
+        bklen = 0;
+        dev = -1;
+    }
+    // false: no pinned memory (the caller stages through vectors)
+    bool ensure(uint32_t n) {
+        int d = 0;
+        if (cudaGetDevice(&d) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        if (freq && bklen >= n && d == dev) {
+            if (pending) cudaEventSynchronize(done);
+            pending = false;
+            return true;
+        }
+        release();
+        const size_t bytes = 8 * (size_t)n + hf_revbook_bytes(n);
+        void* h = nullptr;
+        if (cudaHostAlloc(&h, bytes, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFreeHost(h);
+            done = nullptr;
+            return false;
+        }
+        dev = d;
+        freq = static_cast<uint32_t*>(h);
+        bk4 = freq + n;
+        revbook = reinterpret_cast<uint8_t*>(bk4 + n);
+        bklen = n;
+        return true;
+    }
+};
+
 int huff_compress_sub(const uint16_t* d_in, uint64_t n, uint32_t bklen, uint32_t sublen, void* d_out,
                       uint64_t* d_out_size, void* d_work, size_t work_bytes, void* stream) {
     if (!d_in || !d_out || !d_out_size || !hf_args_ok(n, bklen)) return FZB_E_INVALID;
@@ -813,17 +874,36 @@ int huff_compress_sub(const uint16_t* d_in, uint64_t n, uint32_t bklen, uint32_t
     cudaStream_t s = S(stream);
     int rc = fzb_huff_histogram(d_in, n, bklen, w.freq, stream);
     if (rc) return rc;
-    std::vector<uint32_t> freq(bklen), bk4(bklen);
-    std::vector<uint8_t> revbook(hf_revbook_bytes(bklen));
-    CK(cudaMemcpyAsync(freq.data(), w.freq, 4 * (size_t)bklen, cudaMemcpyDeviceToHost, s));
+    static thread_local HfHostStage stage;
+    std::vector<uint32_t> vfreq, vbk4;
+    std::vector<uint8_t> vrev;
+    uint32_t *freq, *bk4;
+    uint8_t* revbook;
+    const bool pinned = stage.ensure(bklen);
+    if (pinned) {
+        freq = stage.freq;
+        bk4 = stage.bk4;
+        revbook = stage.revbook;
+    } else {
+        vfreq.resize(bklen);
+        vbk4.resize(bklen);
+        vrev.resize(hf_revbook_bytes(bklen));
+        freq = vfreq.data();
+        bk4 = vbk4.data();
+        revbook = vrev.data();
+    }
+    CK(cudaMemcpyAsync(freq, w.freq, 4 * (size_t)bklen, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     uint64_t sum = 0;
     for (uint32_t i = 0; i < bklen; i++) sum += freq[i];
     if (sum != n) return FZB_E_RANGE;
-    if (build_huffman_book(freq.data(), bklen, bk4.data(), revbook.data()) != 0) return FZB_E_INVALID;
-    // pageable sources: each copy has read its host buffer when the call returns
-    CK(cudaMemcpyAsync(w.bk4, bk4.data(), 4 * (size_t)bklen, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(w.revbook, revbook.data(), revbook.size(), cudaMemcpyHostToDevice, s));
+    if (build_huffman_book(freq, bklen, bk4, revbook) != 0) return FZB_E_INVALID;
+    CK(cudaMemcpyAsync(w.bk4, bk4, 4 * (size_t)bklen, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(w.revbook, revbook, hf_revbook_bytes(bklen), cudaMemcpyHostToDevice, s));
+    if (pinned) {  // the uploads read the pinned buffers until they have run
+        CK(cudaEventRecord(stage.done, s));
+        stage.pending = true;
+    }
     return huff_encode_sub(d_in, n, bklen, w.bk4, w.revbook, sublen, d_out, d_out_size, d_work, work_bytes,
                            stream);
 }

@@ -26,10 +26,12 @@ constexpr uint32_t kHfSmemBook = 16384;  // books up to this size are staged in 
 
 // Privatised histogram: each CTA counts into `copies` shared-memory copies
 // (warp w into copy w % copies, so a frequent symbol's atomics spread), then
-// merges.  A thread adds each run of equal symbols among its eight with one
-// atomic.  (Combining equal symbols across a warp with match.any first was
-// slower: 0.109 against 0.085 ms on C3's codes.)  Symbols >= bklen are
-// skipped (histogram.cu:47-51).
+// merges.  Symbols 0..3 -- the small deltas, most of a zigzag code stream --
+// are counted in registers (16-bit fields, two to a word) and added once per
+// warp at the end; a thread adds each run of equal other symbols among its
+// eight with one atomic, four 16-byte loads in flight.  (Combining equal
+// symbols across a warp with match.any first was slower: 0.109 against 0.085
+// ms on C3's codes.)  Symbols >= bklen are skipped (histogram.cu:47-51).
 __global__ void __launch_bounds__(512) hf_histogram_kernel(const uint16_t* __restrict__ in, uint64_t n,
                                                            uint32_t bklen, uint32_t copies,
                                                            uint32_t* __restrict__ freq) {
@@ -43,21 +45,58 @@ __global__ void __launch_bounds__(512) hf_histogram_kernel(const uint16_t* __res
     const bool vec = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
     const uint64_t nv = vec ? n / 8 : 0;
     const uint4* in8 = reinterpret_cast<const uint4*>(in);
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
-        const uint4 v = __ldg(in8 + i);
-        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-        uint32_t cur = w[0] & 0xffffu, run = 0;
+    // symbols 0..3 (the small deltas of zigzag codes) count in registers, two
+    // 16-bit fields per word, flushed before a field can wrap; the others go
+    // to the shared copies, equal neighbours merged into one add
+    uint32_t c01 = 0, c23 = 0, since = 0;
+    const bool small_ok = bklen >= 4;
+    constexpr int kU = 4;  // 16-byte loads in flight per thread
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < nv; i0 += kU * stride) {
+        uint4 v[kU];
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const uint32_t a = (w[k >> 1] >> (16 * (k & 1))) & 0xffffu;
-            if (a != cur) {
-                if (cur < bklen) atomicAdd(&h[cur], run);
-                cur = a;
-                run = 0;
+        for (int u = 0; u < kU; u++) v[u] = i0 + u * stride < nv ? __ldg(in8 + i0 + u * stride) : make_uint4(~0u, ~0u, ~0u, ~0u);
+#pragma unroll
+        for (int u = 0; u < kU; u++) {
+            if (i0 + u * stride >= nv) break;
+            const uint32_t w[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+            uint32_t cur = 0xffffffffu, run = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const uint32_t a = (w[k >> 1] >> (16 * (k & 1))) & 0xffffu;
+                if (small_ok && a < 4u) {
+                    const uint32_t inc = 1u << ((a & 1u) << 4);
+                    if (a < 2u) c01 += inc;
+                    else c23 += inc;
+                    continue;
+                }
+                if (a != cur) {
+                    if (cur < bklen) atomicAdd(&h[cur], run);
+                    cur = a;
+                    run = 0;
+                }
+                run++;
             }
-            run++;
+            if (cur < bklen) atomicAdd(&h[cur], run);
+            since += 8;
         }
-        if (cur < bklen) atomicAdd(&h[cur], run);
+        if (since >= 65536 - 8 * kU) {  // a 16-bit field could wrap in the next round
+            atomicAdd(&h[0], c01 & 0xffffu);
+            atomicAdd(&h[1], c01 >> 16);
+            atomicAdd(&h[2], c23 & 0xffffu);
+            atomicAdd(&h[3], c23 >> 16);
+            c01 = c23 = since = 0;
+        }
+    }
+    if (small_ok) {  // every lane of the block reaches this point
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t t0 = __reduce_add_sync(0xffffffffu, c01 & 0xffffu), t1 = __reduce_add_sync(0xffffffffu, c01 >> 16);
+        const uint32_t t2 = __reduce_add_sync(0xffffffffu, c23 & 0xffffu), t3 = __reduce_add_sync(0xffffffffu, c23 >> 16);
+        if (lane == 0) {
+            if (t0) atomicAdd(&h[0], t0);
+            if (t1) atomicAdd(&h[1], t1);
+            if (t2) atomicAdd(&h[2], t2);
+            if (t3) atomicAdd(&h[3], t3);
+        }
     }
     for (uint64_t i = 8 * nv + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t a = in[i];
