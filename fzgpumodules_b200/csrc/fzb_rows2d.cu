@@ -30,38 +30,11 @@ constexpr int kRowThreads = 256;
 constexpr int kRowGran = kChunkCodes / 4 / kRowThreads;  // granules a thread owns per chunk (8)
 constexpr int kRowCtasPerSm = 2;
 
-struct Q4 {
-    float2 a, b;  // elements 0,1 and 2,3 of a granule
-};
-
-// q of a granule: round half away from zero of v * r.
-__device__ __forceinline__ Q4 quant4(float4 v, float r) {
-    // scalar products: a packed multiply followed by the packed add could be
-    // contracted into one fused multiply-add, which rounds differently
-    const float2 y0 = f2(__fmul_rn(v.x, r), __fmul_rn(v.y, r));
-    const float2 y1 = f2(__fmul_rn(v.z, r), __fmul_rn(v.w, r));
-    const float2 s0 = __fadd2_rn(y0, f2(__uint_as_float(half_bits(v.x)), __uint_as_float(half_bits(v.y))));
-    const float2 s1 = __fadd2_rn(y1, f2(__uint_as_float(half_bits(v.z)), __uint_as_float(half_bits(v.w))));
-    return {f2(truncf(s0.x), truncf(s0.y)), f2(truncf(s1.x), truncf(s1.y))};
-}
-
 // Deltas of a granule from its q, the row above's q (ty) and the previous
 // element's y difference `left` (0 at a tile start): c = (q - q_up) - left.
 __device__ __forceinline__ Q4 deltas4(Q4 q, Q4 qu, bool ty, float left) {
     const Q4 v = ty ? Q4{sub2(q.a, qu.a), sub2(q.b, qu.b)} : q;
     return {sub2(v.a, f2(left, v.a.x)), sub2(v.b, f2(v.a.y, v.b.x))};
-}
-
-template <bool ZZ>
-__device__ __forceinline__ uint32_t code_pair(float2 c) {
-    const float2 m = __fadd2_rn(c, f2(kMagic, kMagic));
-    uint32_t p = __byte_perm(__float_as_uint(m.x), __float_as_uint(m.y), 0x5410);
-    if (ZZ) {
-        uint32_t s;
-        asm("prmt.b32 %0, %1, %1, 0xBB99;" : "=r"(s) : "r"(p));  // per-half sign mask
-        p = ((p << 1) & 0xfffefffeu) ^ s;
-    }
-    return p;
 }
 
 // The y-differenced value of the element before granule g's first (lane - 1

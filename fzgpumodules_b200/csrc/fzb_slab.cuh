@@ -98,6 +98,36 @@ __device__ __forceinline__ uint32_t half_bits(float sv) {
     return (__float_as_uint(sv) & 0x80000000u) | 0x3effffffu;
 }
 
+struct Q4 {
+    float2 a, b;  // elements 0,1 and 2,3 of a granule
+};
+
+// q of a granule: round half away from zero of v * r.
+__device__ __forceinline__ Q4 quant4(float4 v, float r) {
+    // scalar products: a packed multiply followed by the packed add could be
+    // contracted into one fused multiply-add, which rounds differently
+    const float2 y0 = f2(__fmul_rn(v.x, r), __fmul_rn(v.y, r));
+    const float2 y1 = f2(__fmul_rn(v.z, r), __fmul_rn(v.w, r));
+    const float2 s0 = __fadd2_rn(y0, f2(__uint_as_float(half_bits(v.x)), __uint_as_float(half_bits(v.y))));
+    const float2 s1 = __fadd2_rn(y1, f2(__uint_as_float(half_bits(v.z)), __uint_as_float(half_bits(v.w))));
+    return {f2(truncf(s0.x), truncf(s0.y)), f2(truncf(s1.x), truncf(s1.y))};
+}
+
+// Codes of two integer-valued deltas |c| < 2^22 packed as c0 | c1 << 16
+// (int16 or zigzag), through the magic-number add: c + 1.5 * 2^23 holds c in
+// its low mantissa bits.
+template <bool ZZ>
+__device__ __forceinline__ uint32_t code_pair(float2 c) {
+    const float2 m = __fadd2_rn(c, f2(kMagic, kMagic));
+    uint32_t p = __byte_perm(__float_as_uint(m.x), __float_as_uint(m.y), 0x5410);
+    if (ZZ) {
+        uint32_t s;
+        asm("prmt.b32 %0, %1, %1, 0xBB99;" : "=r"(s) : "r"(p));  // per-half sign mask
+        p = ((p << 1) & 0xfffefffeu) ^ s;
+    }
+    return p;
+}
+
 // Byte offset in a 128-byte-swizzled buffer of 16-byte granule g of row `row`
 // (the TMA SWIZZLE_128B layout: granule index XOR row % 8).  Thread t of a
 // slab kernel owns row t (32 floats).

@@ -110,7 +110,8 @@ def test_lq_forward_matches_oracle(cuda, dims, mode, zz, radius, kind):
     _check_outliers(out, x, dims, mode, radius, zz, cap, cnt, idx, err)
 
 
-@pytest.mark.parametrize("dims", [(37, 19, 5), (3000, 7, 1), (33, 17, 11), (20, 13, 9), (200, 9, 7), (8192, 6, 1)])
+@pytest.mark.parametrize("dims", [(37, 19, 5), (3000, 7, 1), (33, 17, 11), (20, 13, 9), (200, 9, 7), (8192, 6, 1),
+                                  (40000, 1, 1)])
 def test_element_path_large_prequant_values(cuda, dims):
     """Rows that are not a multiple of 32 elements take the element path,
     which carries each element's x-neighbour terms along the run.  With an
@@ -301,11 +302,12 @@ def test_row_walk_codes_match_oracle(cuda, dims, mode, zz, radius, kind, monkeyp
         _check_outliers(out, x, dims, mode, radius, zz, cap, cnt, idx, err)
 
 
-@pytest.mark.parametrize("dims", [(8192, 40, 1), (16384, 9, 1)])
-def test_row_walk_rounding_midpoints(cuda, dims, monkeypatch):
-    # the 2-D row walk quantizes in registers (round half away from zero as
-    # trunc(y + copysign(0.49999997, y))): next to every rounding midpoint
-    # its codes equal the oracle's and the per-chunk kernel's
+@pytest.mark.parametrize("dims", [(8192, 40, 1), (16384, 9, 1), (65536, 1, 1)])
+def test_register_paths_rounding_midpoints(cuda, dims, monkeypatch):
+    # the 2-D row walk and the 1-D register front end quantize in registers
+    # (round half away from zero as trunc(y + copysign(0.49999997, y))): next
+    # to every rounding midpoint their codes equal the oracle's and the
+    # per-chunk kernel's
     n = int(np.prod(dims))
     x = _midpoint_field(n, 37, 1e-3)
     codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-3, O.ABS, 32768, True, n)
