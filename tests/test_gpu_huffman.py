@@ -44,6 +44,24 @@ def _hist(a, bklen):
     return np.bincount(a[a < bklen], minlength=bklen).astype(np.uint32)
 
 
+@pytest.mark.parametrize("bklen", [1, 2, 3, 4, 5, 1024, 20000])
+def test_histogram_counts(cuda, bklen):
+    """Symbols 0..3 counted in registers (SIMD compares on code pairs), the
+    others through shared-memory copies (global counts past 16384 symbols):
+    every count exact, symbols >= bklen skipped, with tails past the last
+    16-byte word and a misaligned start."""
+    rng = np.random.default_rng(bklen)
+    for n in (1, 7, 8, 9, 1000003):
+        small = rng.integers(0, 4, n)
+        wide = rng.integers(0, max(2 * bklen, 8), n)
+        a = np.where(rng.random(n) < 0.7, small, wide).astype(np.uint16)
+        a[rng.random(n) < 0.01] = 65535
+        d = torch.from_numpy(np.concatenate([[np.uint16(1)], a])).to(cuda)
+        for view, ref in ((d[1:], a), (d, np.concatenate([[np.uint16(1)], a]))):
+            freq = K().huff_histogram(view, bklen).cpu().numpy().view(np.uint32)
+            assert np.array_equal(freq, _hist(ref, bklen)), (bklen, n)
+
+
 @pytest.mark.parametrize("case", list(_cases()))
 def test_histogram_book_blob_decode(cuda, case):
     a = _cases()[case]
