@@ -541,7 +541,65 @@ __global__ void __launch_bounds__(1024) assemble_scan_kernel(AsmArgs a) {
     asm volatile("griddepcontrol.launch_dependents;");
 }
 
+// The same scans for up to kTiledScanMax chunks, a CTA per 1024 chunks:
+// each CTA first sums the payload sizes, staged outlier counts and outlier
+// counts of every chunk before its tile (at most 63 K words each, from L2),
+// then scans its own tile; the last CTA writes the stream header's totals.
+__global__ void __launch_bounds__(1024) assemble_scan_tiles_kernel(AsmArgs a) {
+    __shared__ uint32_t ws[66];
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const uint32_t n = a.n_chunks, t = threadIdx.x, base = blockIdx.x * 1024u;
+    const bool last = base + 1024u >= n;
+    auto staged = [&](uint32_t i) -> uint32_t {
+        const uint32_t b0 = a.obase[i], n0 = a.ocnt[i];
+        return b0 >= a.ostage_cap ? 0u : min(n0, a.ostage_cap - b0);
+    };
+    uint32_t sp = 0, so = 0, sc = 0;  // before the tile: payload bytes, staged outliers, outliers found
+    for (uint32_t i = t; i < base; i += 1024u) {
+        if (a.sizes) sp += a.sizes[i] & 0x7fffffffu;
+        if (a.ocnt) {
+            so += staged(i);
+            sc += a.ocnt[i];
+        }
+    }
+    const uint32_t i = base + t;
+    const bool in = i < n;
+    const uint32_t vs = (in && a.sizes) ? a.sizes[i] : 0u;
+    const uint32_t vo = (in && a.ocnt) ? staged(i) : 0u;
+    const uint32_t vc = (in && a.ocnt) ? a.ocnt[i] : 0u;
+    uint32_t e0, e1, SP, SO, ep, eo, TP, TO;
+    block_scan2_1024(sp, so, e0, e1, SP, SO, ws);  // SP, SO: the sums before the tile
+    block_scan2_1024(vs & 0x7fffffffu, vo, ep, eo, TP, TO, ws);
+    uint32_t* hdr = reinterpret_cast<uint32_t*>(a.out);
+    if (in) {
+        if (a.sizes) {
+            a.pay_off[i] = (unsigned long long)SP + ep;
+            hdr[2 + i] = vs;  // the stream's size table
+        }
+        if (a.ocnt) a.ofin[i] = SO + eo;
+    }
+    if (last) {
+        uint32_t c0, c1, SC, TC;
+        block_scan2_1024(sc, vc, c0, c1, SC, TC, ws);
+        if (t == 0) {
+            if (a.sizes) {
+                hdr[0] = a.orig_bytes;
+                hdr[1] = n;
+                const unsigned long long total = 8ull + 4ull * n + (unsigned long long)SP + TP;
+                const unsigned long long padded = (total + 3) & ~3ull;
+                for (unsigned long long k = total; k < padded; k++) a.out[k] = 0;
+                *a.out_size = padded;
+            }
+            if (a.ocnt) *a.out_count = SC + TC;
+        }
+    }
+    asm volatile("griddepcontrol.launch_dependents;");
+}
+
 int launch_assemble_scan(const AsmArgs& a, cudaStream_t s) {
+    if (a.n_chunks <= kTiledScanMax)
+        return (int)launch_dependent(assemble_scan_tiles_kernel, (a.n_chunks + 1023u) / 1024u + (a.n_chunks == 0),
+                                     1024, 0, s, a);
     const int smem = (int)(2 * (kAsmTile + kAsmTile / 32) * sizeof(uint32_t));
     static SmemAttr attr;
     const cudaError_t e = ensure_dyn_smem(attr, (const void*)assemble_scan_kernel, smem);

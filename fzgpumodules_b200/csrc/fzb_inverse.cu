@@ -86,8 +86,50 @@ __global__ void __launch_bounds__(1024) rze_prepass_kernel(const uint8_t* __rest
     asm volatile("griddepcontrol.launch_dependents;");  // outlier_ranges_kernel may start
 }
 
+// The same offsets for up to kTiledScanMax chunks, a CTA per 1024 chunks,
+// each summing the size words before its tile itself (no CTA waits for
+// another); the last CTA writes the end offset and checks it.
+__global__ void __launch_bounds__(1024) rze_prepass_tiles_kernel(const uint8_t* __restrict__ rze,
+                                                                 uint64_t rze_bytes, uint32_t n_expect,
+                                                                 uint32_t orig_expect,
+                                                                 unsigned long long* __restrict__ in_off,
+                                                                 uint32_t* err) {
+    __shared__ uint32_t ws[66];
+    const uint32_t* h = reinterpret_cast<const uint32_t*>(rze);
+    const uint32_t n = n_expect, t = threadIdx.x, base = blockIdx.x * 1024u;
+    const bool last = base + 1024u >= n;
+    const uint64_t hdr = 8ull + 4ull * n;
+    if (h[0] != orig_expect || h[1] != n_expect || hdr > rze_bytes) {
+        // inconsistent header: flag it and point every chunk at the header end
+        if (blockIdx.x == 0 && t == 0) atomicOr(err, kErrMalformed);
+        if (base + t < n) in_off[base + t] = rze_bytes + 1;
+        if (last && t == 0) in_off[n] = rze_bytes + 1;
+        asm volatile("griddepcontrol.launch_dependents;");
+        return;
+    }
+    uint32_t sp = 0;  // bytes of the chunks before the tile (at most 2^30)
+    for (uint32_t i = t; i < base; i += 1024u) sp += h[2 + i] & 0x7fffffffu;
+    const uint32_t i = base + t;
+    const uint32_t v = i < n ? h[2 + i] & 0x7fffffffu : 0u;
+    uint32_t e0, e1, SP, S1, ev, e2, TV, T2;
+    block_scan2_1024(sp, 0u, e0, e1, SP, S1, ws);
+    block_scan2_1024(v, 0u, ev, e2, TV, T2, ws);
+    if (i < n) in_off[i] = hdr + SP + ev;
+    if (last && t == 0) {
+        const unsigned long long end = hdr + (unsigned long long)SP + TV;
+        in_off[n] = end;
+        if (end > rze_bytes) atomicOr(err, kErrMalformed);
+    }
+    asm volatile("griddepcontrol.launch_dependents;");  // outlier_ranges_kernel may start
+}
+
 int launch_rze_prepass(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect, uint32_t orig_expect,
                        unsigned long long* in_off, uint32_t* err, cudaStream_t s) {
+    if (n_expect <= kTiledScanMax) {
+        rze_prepass_tiles_kernel<<<(n_expect + 1023u) / 1024u + (n_expect == 0), 1024, 0, s>>>(
+            rze, rze_bytes, n_expect, orig_expect, in_off, err);
+        return (int)cudaGetLastError();
+    }
     const int smem = (int)((kAsmTile + kAsmTile / 32) * sizeof(uint32_t));
     static SmemAttr attr;
     const cudaError_t e = ensure_dyn_smem(attr, (const void*)rze_prepass_kernel, smem);

@@ -166,6 +166,57 @@ __global__ void assemble_scan_kernel(AsmArgs a);
 // Shared-memory index with one pad word per 32 entries: thread t touching
 // entries k*t + j (k a power of two up to 32) stays free of bank conflicts.
 __device__ __forceinline__ uint32_t pad32(uint32_t i) { return i + (i >> 5); }
+
+// Fields of up to this many chunks take the tiled scans (assemble_scan,
+// rze_prepass): one CTA per 1024 chunks, each summing the chunks before its
+// tile itself, so no CTA waits for another.
+constexpr uint32_t kTiledScanMax = 65536;
+
+// Exclusive scans of two values over a block of 1024 threads, with their
+// totals (ws: 64 words of shared memory).
+__device__ __forceinline__ void block_scan2_1024(uint32_t a, uint32_t b, uint32_t& ea, uint32_t& eb, uint32_t& ta,
+                                                 uint32_t& tb, uint32_t* ws) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t ia = a, ib = b;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t na = __shfl_up_sync(0xffffffffu, ia, d), nb = __shfl_up_sync(0xffffffffu, ib, d);
+        if (lane >= (uint32_t)d) {
+            ia += na;
+            ib += nb;
+        }
+    }
+    if (lane == 31) {
+        ws[warp] = ia;
+        ws[32 + warp] = ib;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t va = ws[lane], vb = ws[32 + lane];
+        uint32_t xa = va, xb = vb;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t na = __shfl_up_sync(0xffffffffu, xa, d), nb = __shfl_up_sync(0xffffffffu, xb, d);
+            if (lane >= (uint32_t)d) {
+                xa += na;
+                xb += nb;
+            }
+        }
+        __syncwarp();
+        ws[lane] = xa - va;
+        ws[32 + lane] = xb - vb;
+        if (lane == 31) {
+            ws[64] = xa;
+            ws[65] = xb;
+        }
+    }
+    __syncthreads();
+    ea = ws[warp] + ia - a;
+    eb = ws[32 + warp] + ib - b;
+    ta = ws[64];
+    tb = ws[65];
+    __syncthreads();  // ws may be reused
+}
 constexpr uint32_t kAsmTile = 16384;  // chunks per tile of the single-CTA assembly scan (shared memory: 2 words each)
 int launch_assemble_scan(const AsmArgs& a, cudaStream_t s);
 __global__ void assemble_copy_kernel(AsmArgs a);  // one warp per chunk, grid-stride
