@@ -952,9 +952,10 @@ int fzb_huff_decode(const void* d_in, uint64_t in_bytes, uint64_t n, uint32_t bk
 
 // ---------------------------------------------------------------------------
 // Batched LorenzoQuant -> Bitshuffle -> RZE over many fields: one reset
-// kernel, one value-base kernel for every field, one persistent chunk
-// kernel over every (field, chunk) unit and two assembly kernels -- five
-// launches whatever the field count, capturable in a CUDA graph.
+// kernel, one value-base kernel for every field, the slab kernel of each
+// field the single-field call codes with one, one persistent chunk kernel
+// over the (field, chunk) units of the others and two assembly kernels,
+// capturable in a CUDA graph.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -963,7 +964,17 @@ struct BatchPlan {
     uint32_t mm_grid_x;
     unsigned lq_grid;
     size_t smem;
+    std::vector<FwdArgs> slab;  // fields coded by a slab kernel (host copies of their arguments)
+    unsigned sms = 148;
 };
+
+// A field the single-field call would code with a slab kernel (3-D, nx a
+// power of two in [32, 1024], whole-row chunks, no padding).
+bool batch_slab_field(const Geometry& g, uint64_t n_total) {
+    const uint32_t nx = g.nx;
+    return g.ndim == 3 && nx >= 32 && nx <= 1024 && (nx & (nx - 1)) == 0 &&
+           g.ny % ((uint32_t)kChunkCodes / nx) == 0 && g.nfield == n_total;
+}
 
 struct BatchLayout {
     size_t desc_bytes;
@@ -1018,6 +1029,7 @@ void* fzb_batch_create(const fzb_batch_field* fields, int nfields, const fzb_bat
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     uint8_t* base = static_cast<uint8_t*>(d_work);
     std::vector<BatchField> hf((size_t)nfields);
+    std::vector<char> is_slab((size_t)nfields, 0);
     size_t smem = 0;
     uint32_t mm_grid = 1;
     for (int i = 0; i < nfields; i++) {
@@ -1051,23 +1063,29 @@ void* fzb_batch_create(const fzb_batch_field* fields, int nfields, const fzb_bat
         const bool rowal = (g.ndim == 1) || (g.nx % 32 == 0);
         b.kind = g.ndim == 1 ? 0u : g.ndim == 2 ? (rowal ? 1u : 2u) : (rowal ? 3u : 4u);
         b.n_chunks = (uint32_t)chunks_of(f.n_total);
-        const size_t sm = lq_smem_bytes(g, true);
-        if (sm > smem) smem = sm;
+        is_slab[i] = batch_slab_field(g, f.n_total) && !(flags_env() & 1);
+        if (!is_slab[i]) {
+            const size_t sm = lq_smem_bytes(g, true);
+            if (sm > smem) smem = sm;
+        }
     }
     if ((int)smem > max_smem) {
         *st = FZB_E_INVALID;
         return nullptr;
     }
-    // field order of the unit ranges
+    // field order of the unit ranges: the chunk kernel's fields first (in
+    // the tuned order), the slab kernels' fields after them
     std::vector<uint32_t> order((size_t)nfields), begin((size_t)nfields);
     for (int i = 0; i < nfields; i++) order[i] = (uint32_t)i;
     if (tuning && tuning->order == 1)
         std::stable_sort(order.begin(), order.end(),
                          [&](uint32_t x, uint32_t y) { return hf[x].n_chunks > hf[y].n_chunks; });
-    uint64_t units = 0;
+    std::stable_partition(order.begin(), order.end(), [&](uint32_t x) { return !is_slab[x]; });
+    uint64_t units = 0, lq_units = 0;
     for (int i = 0; i < nfields; i++) {
         begin[i] = (uint32_t)units;
         units += hf[order[i]].n_chunks;
+        if (!is_slab[order[i]]) lq_units = units;
     }
     if (units >= (1ull << 31)) return nullptr;
     // descriptors: [BatchField x n][order x n][begin x n][counter]
@@ -1092,11 +1110,15 @@ void* fzb_batch_create(const fzb_batch_field* fields, int nfields, const fzb_bat
     p->args.unit_order = reinterpret_cast<const uint32_t*>(base + o_order);
     p->args.unit_begin = reinterpret_cast<const uint32_t*>(base + o_order + 4ull * nfields);
     p->args.total_units = (uint32_t)units;
+    p->args.lq_units = (uint32_t)lq_units;
     p->args.counter = reinterpret_cast<uint32_t*>(base + o_counter);
     p->mm_grid_x = mm_grid;
+    p->sms = (unsigned)sms;
+    for (int i = 0; i < nfields; i++)
+        if (is_slab[order[i]]) p->slab.push_back(hf[order[i]].a);
     const int per_sm = (tuning && tuning->ctas_per_sm > 0) ? tuning->ctas_per_sm : 2;
     const uint64_t grid = (uint64_t)per_sm * (uint64_t)sms;
-    p->lq_grid = (unsigned)(grid < units ? grid : units);
+    p->lq_grid = (unsigned)(grid < lq_units ? grid : lq_units);
     if (p->lq_grid == 0) p->lq_grid = 1;
     p->smem = smem;
     *st = FZB_OK;
@@ -1108,7 +1130,13 @@ int fzb_batch_launch(void* batch, void* stream) {
     const BatchPlan* p = static_cast<const BatchPlan*>(batch);
     cudaStream_t s = S(stream);
     TraceScope ts(s, "batch_lq_bs_rze");
-    return launch_batch(p->args, p->mm_grid_x, p->lq_grid, p->smem, s) == 0 ? FZB_OK : FZB_E_CUDA;
+    if (launch_batch_scan(p->args, p->mm_grid_x, s) != 0) return FZB_E_CUDA;
+    for (const FwdArgs& a : p->slab) {  // the slab kernels of the single-field call
+        const int rc = (lq3d_tma_supported(a) && !(flags_env() & 2)) ? launch_lq3d_tma(a, 2 * p->sms, s)
+                                                                      : launch_lq3d_slab(a, 2 * p->sms, s);
+        if (rc != 0) return FZB_E_CUDA;
+    }
+    return launch_batch_code(p->args, p->lq_grid, p->smem, s) == 0 ? FZB_OK : FZB_E_CUDA;
 }
 
 void fzb_batch_destroy(void* batch) { delete static_cast<BatchPlan*>(batch); }

@@ -1075,7 +1075,7 @@ __global__ void __launch_bounds__(kThreads, 3) lq_batch_kernel(BatchArgs b) {
         __syncthreads();
         const uint32_t u = s_unit;
         __syncthreads();  // s_unit is rewritten at the end of this iteration
-        if (u >= b.total_units) break;
+        if (u >= b.lq_units) break;
         if (threadIdx.x == 0) next = atomicAdd(b.counter, 1u);
         // field = last slot whose unit_begin <= u (fields in unit_order)
         uint32_t lo = 0, hi = b.nfields;
@@ -1136,12 +1136,18 @@ __global__ void batch_reset_kernel(BatchArgs b) {
     }
 }
 
-int launch_batch(const BatchArgs& b, uint32_t mm_grid_x, unsigned lq_grid, size_t smem, cudaStream_t s) {
+int launch_batch_scan(const BatchArgs& b, uint32_t mm_grid_x, cudaStream_t s) {
     batch_reset_kernel<<<b.nfields, 32, 0, s>>>(b);
     batch_minmax_kernel<<<dim3(mm_grid_x, b.nfields), 256, 0, s>>>(b);
-    cudaError_t e = cudaFuncSetAttribute(lq_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return (int)e;
-    lq_batch_kernel<<<lq_grid, kThreads, smem, s>>>(b);
+    return (int)cudaGetLastError();
+}
+
+int launch_batch_code(const BatchArgs& b, unsigned lq_grid, size_t smem, cudaStream_t s) {
+    if (b.lq_units) {
+        cudaError_t e = cudaFuncSetAttribute(lq_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        lq_batch_kernel<<<lq_grid, kThreads, smem, s>>>(b);
+    }
     batch_assemble_scan_kernel<<<b.nfields, 1024, 0, s>>>(b);
     batch_assemble_copy_kernel<<<b.total_units, 256, 0, s>>>(b);
     return (int)cudaGetLastError();

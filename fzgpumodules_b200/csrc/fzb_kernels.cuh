@@ -288,12 +288,17 @@ struct BatchArgs {
     const BatchField* fields;
     uint32_t nfields;
     const uint32_t* unit_order;  // field index per slot
-    const uint32_t* unit_begin;  // first unit of each slot
-    uint32_t total_units;
+    const uint32_t* unit_begin;  // first unit (chunk) of each slot
+    uint32_t total_units;        // chunks of every field (the assembly's units)
+    uint32_t lq_units;           // the chunk kernel's units: the leading slots, slab fields excluded
     uint32_t* counter;           // unit dispenser
 };
 
-int launch_batch(const BatchArgs& b, uint32_t mm_grid_x, unsigned lq_grid, size_t smem, cudaStream_t s);
+// Reset and the value-base scan of every field; then the chunk kernel over
+// the first lq_units units and the assembly of every field.  Fields that take
+// a slab kernel are launched between the two.
+int launch_batch_scan(const BatchArgs& b, uint32_t mm_grid_x, cudaStream_t s);
+int launch_batch_code(const BatchArgs& b, unsigned lq_grid, size_t smem, cudaStream_t s);
 
 // Per-chunk coding with a learned selector (fzb_select.cu).
 constexpr int kSelCodes = 32768;            // codes per 64 KiB chunk

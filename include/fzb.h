@@ -384,8 +384,10 @@ int fzb_status_from_bits(uint32_t bits, int* rerun_exact);
  * Batched compression of many fields (no reference counterpart: it runs the
  * chain of fzb_lq_bs_rze_compress for every field in five launches --
  * reset, one value-base scan over all fields, one persistent chunk kernel
- * over every (field, chunk) unit, two assembly kernels -- so a batch is one
- * CUDA graph node group regardless of its size).  Each field's outputs are
+ * over every (field, chunk) unit, two assembly kernels -- plus one slab
+ * kernel launch per field the single-field call codes with a slab kernel
+ * (3-D, nx a power of two in [32, 1024], whole-row chunks), so a batch is one
+ * CUDA graph node group).  Each field's outputs are
  * byte-identical to its own fzb_lq_bs_rze_compress call.
  *
  * fzb_batch_create validates the fields, writes the descriptors into
