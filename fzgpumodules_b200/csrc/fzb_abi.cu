@@ -88,11 +88,6 @@ inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 // TMA one, 4 = the per-(slab, tile) fused inverse instead of the persistent
 // slab inverse, 8 = codes of 2-D fields with chunk-wide rows through the
 // per-chunk kernel instead of the row walk.
-inline unsigned flags_env() {
-    const char* v = getenv("FZB_DISABLE_SLAB");
-    return v ? (unsigned)strtoul(v, nullptr, 10) & 15u : 0u;
-}
-
 #define CK(call)                                          \
     do {                                                  \
         if ((call) != cudaSuccess) return FZB_E_CUDA;     \

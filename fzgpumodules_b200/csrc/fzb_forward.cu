@@ -597,7 +597,7 @@ __global__ void __launch_bounds__(1024) assemble_scan_tiles_kernel(AsmArgs a) {
 }
 
 int launch_assemble_scan(const AsmArgs& a, cudaStream_t s) {
-    if (a.n_chunks <= kTiledScanMax)
+    if (a.n_chunks <= kTiledScanMax && !(flags_env() & 16))
         return (int)launch_dependent(assemble_scan_tiles_kernel, (a.n_chunks + 1023u) / 1024u + (a.n_chunks == 0),
                                      1024, 0, s, a);
     const int smem = (int)(2 * (kAsmTile + kAsmTile / 32) * sizeof(uint32_t));

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(1024) rze_prepass_tiles_kernel(const uint8_t* 
 
 int launch_rze_prepass(const uint8_t* rze, uint64_t rze_bytes, uint32_t n_expect, uint32_t orig_expect,
                        unsigned long long* in_off, uint32_t* err, cudaStream_t s) {
-    if (n_expect <= kTiledScanMax) {
+    if (n_expect <= kTiledScanMax && !(flags_env() & 16)) {
         rze_prepass_tiles_kernel<<<(n_expect + 1023u) / 1024u + (n_expect == 0), 1024, 0, s>>>(
             rze, rze_bytes, n_expect, orig_expect, in_off, err);
         return (int)cudaGetLastError();

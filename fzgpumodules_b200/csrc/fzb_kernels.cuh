@@ -5,6 +5,7 @@
 #include "fzb_rze.cuh"
 
 #include <atomic>
+#include <cstdlib>
 
 namespace fzb {
 
@@ -171,6 +172,16 @@ __device__ __forceinline__ uint32_t pad32(uint32_t i) { return i + (i >> 5); }
 // rze_prepass): one CTA per 1024 chunks, each summing the chunks before its
 // tile itself, so no CTA waits for another.
 constexpr uint32_t kTiledScanMax = 65536;
+
+// FZB_DISABLE_SLAB (a test and measurement switch, default 0): bit 1 codes
+// slab-shaped 3-D fields with the chunk kernel, 2 takes the cp.async slab
+// kernel instead of the TMA one, 4 the per-tile fused inverse instead of the
+// inverse slab kernel, 8 2-D codes with the chunk kernel instead of the row
+// walk, 16 the single-CTA assembly scan and prepass instead of the tiled ones.
+inline unsigned flags_env() {
+    const char* v = getenv("FZB_DISABLE_SLAB");
+    return v ? (unsigned)strtoul(v, nullptr, 10) & 31u : 0u;
+}
 
 // Exclusive scans of two values over a block of 1024 threads, with their
 // totals (ws: 64 words of shared memory).

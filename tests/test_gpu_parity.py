@@ -250,6 +250,32 @@ def test_fused_compress_matches_oracle_chain(cuda, dims, mode, zz, radius, kind)
         assert np.array_equal(_h(dec).view(np.uint32), y.view(np.uint32)), f"flags={flags}"
 
 
+@pytest.mark.parametrize("dims", [(8192 * 1024 + 5, 1, 1), (256, 256, 130), (37, 19, 5)])
+def test_tiled_and_single_cta_scans_agree(cuda, dims, monkeypatch):
+    # the assembly scan and the inverse prepass: a CTA per 1024 chunks (each
+    # summing the chunks before its tile) and the single-CTA scans equal the
+    # oracle's stream, outlier lists and reconstruction (1025 chunks: two tiles)
+    n = int(np.prod(dims))
+    x = _field(n, 41, "spiky")
+    cap = int(np.ceil(n * 0.1))
+    codes, err, idx, cnt, abs_eb, r, e2, _ = _oracle_forward(x, dims, 1e-3, O.ABS, 512, True, cap)
+    stream = O.rze_encode(O.bitshuffle(codes, 16384, 2))
+    y = O.lq_inv(codes, err, idx, dims, e2, True)
+    for flag in ("0", "16"):
+        monkeypatch.setenv("FZB_DISABLE_SLAB", flag)
+        out = kern().lq_bs_rze_compress(_g(x, cuda), dims, 1e-3, O.ABS, 512, True, 0.1)
+        size = int(_h(out["rze_size"])[0])
+        assert size == stream.size and np.array_equal(_h(out["rze"])[:size], stream), flag
+        assert int(_h(out["count"])[0]) == cnt, flag
+        _check_outliers(out, x, dims, O.ABS, 512, True, cap, cnt, idx, err)
+        dec = kern().lq_bs_rze_decompress(out["rze"], size, out["err"], out["idx"], out["count"],
+                                          out["cap"], n, dims, float(abs_eb), True)
+        assert np.array_equal(_h(dec).view(np.uint32), y.view(np.uint32)), flag
+        got = kern().lq_forward(_g(x, cuda), dims, 1e-3, O.ABS, 512, True, 0.1)
+        assert np.array_equal(_h(got["codes"]), codes), flag
+        _check_outliers(got, x, dims, O.ABS, 512, True, cap, cnt, idx, err)
+
+
 @pytest.mark.parametrize("dims", [(512, 32, 16), (64, 256, 10), (32, 256, 9), (1024, 16, 17), (128, 64, 3)])
 @pytest.mark.parametrize("kind,eb,radius,zz", [("spiky", 1e-3, 512, True), ("noise", 1e-3, 32768, False),
                                                ("blocks", 1e-3, 32768, True), ("special", 1e-3, 64, True)])
