@@ -42,11 +42,23 @@ class _DeviceView:
                                          "version": 3, "strides": None}
 
 
-def _view(ptr: int, nbytes: int, device) -> torch.Tensor:
+def _view(ptr: int, nbytes: int, device, cache: dict | None = None) -> torch.Tensor:
+    """A uint8 tensor over `nbytes` pipeline-owned device bytes at `ptr`.  A
+    pipeline reuses its output buffers from call to call, so its views are
+    kept by (pointer, size) in `cache` (a few entries) instead of being built
+    again through __cuda_array_interface__ on every call."""
     if nbytes == 0 or not ptr:
         return torch.empty(0, dtype=torch.uint8, device=device)
+    key = (ptr, nbytes)
+    if cache is not None and key in cache:
+        return cache[key]
     with torch.cuda.device(device):
-        return torch.as_tensor(_DeviceView(ptr, nbytes), device=device)
+        t = torch.as_tensor(_DeviceView(ptr, nbytes), device=device)
+    if cache is not None:
+        if len(cache) >= 4:
+            cache.pop(next(iter(cache)))
+        cache[key] = t
+    return t
 
 
 def _stream(device) -> C.c_void_p:
@@ -258,6 +270,7 @@ class Pipeline:
         self._streams, self._bounds = 1, False
         self._h = None
         self._last_in = 0
+        self._views: dict = {}  # (pointer, bytes) -> view of pipeline-owned output memory
 
     # builder ---------------------------------------------------------------
     def loadConfig(self, path: str):
@@ -386,7 +399,7 @@ class Pipeline:
             _check(lib().fzb_pipeline_compress(self._h, C.c_void_p(src.data_ptr()), src.numel(), C.byref(out),
                                                C.byref(nb), _stream(self.device)), "compress")
         self._last_in = src.numel()
-        return _view(out.value or 0, nb.value, self.device)
+        return _view(out.value or 0, nb.value, self.device, self._views)
 
     def decompress(self, compressed: torch.Tensor | None = None, dtype=torch.float32) -> torch.Tensor:
         """Pool-owned reconstruction (``compressed=None`` decompresses the
@@ -397,7 +410,7 @@ class Pipeline:
         with torch.cuda.device(self.device):
             _check(lib().fzb_pipeline_decompress(self._h, ptr, n, C.byref(out), C.byref(nb), _stream(self.device)),
                    "decompress")
-        return _view(out.value or 0, nb.value, self.device).view(dtype)
+        return _view(out.value or 0, nb.value, self.device, self._views).view(dtype)
 
     def decompressInto(self, compressed: torch.Tensor | None, out: torch.Tensor) -> int:
         nb = C.c_uint64()
@@ -433,6 +446,7 @@ class Pipeline:
         return t.view(dtype)
 
     def close(self):
+        self._views = {}
         if self._h is not None:
             torch.cuda.synchronize(self.device)
             lib().fzb_pipeline_destroy(self._h)
