@@ -61,8 +61,34 @@ def _view(ptr: int, nbytes: int, device, cache: dict | None = None) -> torch.Ten
     return t
 
 
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
 def _stream(device) -> C.c_void_p:
+    if _raw_stream is not None:  # the current stream's handle without a Stream object
+        idx = device.index if device.index is not None else torch.cuda.current_device()
+        return C.c_void_p(_raw_stream(idx))
     return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+class _OnDevice:
+    """torch.cuda.device(d), skipped when d is already current."""
+
+    __slots__ = ("idx", "prev")
+
+    def __init__(self, device):
+        self.idx = device.index
+        self.prev = None
+
+    def __enter__(self):
+        cur = torch.cuda.current_device()
+        if cur != self.idx:
+            self.prev = cur
+            torch.cuda.set_device(self.idx)
+
+    def __exit__(self, *exc):
+        if self.prev is not None:
+            torch.cuda.set_device(self.prev)
 
 
 # ------------------------------------------------------------------ stages
@@ -262,6 +288,8 @@ class Pipeline:
     def __init__(self, input_data_size: int = 0, strategy: int = MINIMAL, pool_multiplier: float = 3.0,
                  device=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        if self.device.index is None:  # "cuda": the current device, by index
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self._hint, self._strategy, self._mult = int(input_data_size), int(strategy), float(pool_multiplier)
         self._stages: list[Stage] = []
         self._conns: list[tuple[Stage, Stage, str]] = []
@@ -393,21 +421,25 @@ class Pipeline:
     # execution -------------------------------------------------------------
     def compress(self, data: torch.Tensor) -> torch.Tensor:
         """Returns a view of the pipeline-owned compressed bytes."""
-        src = data.contiguous().view(torch.uint8).reshape(-1)
+        if not data.is_contiguous():
+            data = data.contiguous()
+        nbytes = data.numel() * data.element_size()
         out, nb = C.c_void_p(), C.c_uint64()
-        with torch.cuda.device(self.device):
-            _check(lib().fzb_pipeline_compress(self._h, C.c_void_p(src.data_ptr()), src.numel(), C.byref(out),
+        with _OnDevice(self.device):
+            _check(lib().fzb_pipeline_compress(self._h, C.c_void_p(data.data_ptr()), nbytes, C.byref(out),
                                                C.byref(nb), _stream(self.device)), "compress")
-        self._last_in = src.numel()
+        self._last_in = nbytes
         return _view(out.value or 0, nb.value, self.device, self._views)
 
     def decompress(self, compressed: torch.Tensor | None = None, dtype=torch.float32) -> torch.Tensor:
         """Pool-owned reconstruction (``compressed=None`` decompresses the
         pipeline's own last outputs)."""
         out, nb = C.c_void_p(), C.c_uint64()
+        if compressed is not None and not compressed.is_contiguous():
+            compressed = compressed.contiguous()
         ptr = C.c_void_p(compressed.data_ptr()) if compressed is not None else C.c_void_p()
         n = compressed.numel() * compressed.element_size() if compressed is not None else 0
-        with torch.cuda.device(self.device):
+        with _OnDevice(self.device):
             _check(lib().fzb_pipeline_decompress(self._h, ptr, n, C.byref(out), C.byref(nb), _stream(self.device)),
                    "decompress")
         return _view(out.value or 0, nb.value, self.device, self._views).view(dtype)
