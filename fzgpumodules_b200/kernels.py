@@ -23,7 +23,17 @@ def _ptr(t: torch.Tensor | None):
     return C.c_void_p(t.data_ptr()) if t is not None else None
 
 
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
 def _stream(device=None):
+    """The current stream's handle (without building a Stream object when
+    torch offers the raw accessor)."""
+    if _raw_stream is not None:
+        if isinstance(device, str):
+            device = torch.device(device)
+        idx = device.index if isinstance(device, torch.device) else device
+        return C.c_void_p(_raw_stream(torch.cuda.current_device() if idx is None else int(idx)))
     return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
 
 
