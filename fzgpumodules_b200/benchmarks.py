@@ -271,7 +271,8 @@ def batch_summary(dev, steps: int, warmup: int) -> dict:
     return {"workload": "64 fields 1-256 MB, mixed rank, REL {1e-2,1e-3,1e-4}, LQ->BS->RZE",
             "gbs": total / t_batch / 1e6, "batched_ms": t_batch, "plain_ms": t_plain,
             "plain_gbs": total / t_plain / 1e6, "speedup_vs_plain": t_plain / t_batch, "bytes_identical": same,
-            "tuning": {"ctas_per_sm": best.ctas_per_sm, "order": best.order}, "autotune_best_ms": tune_ms,
+            "tuning": {"ctas_per_sm": best.ctas_per_sm, "order": best.order, "flat_tiles": best.flat_tiles,
+                       "scan_parts": best.scan_parts}, "autotune_best_ms": tune_ms,
             "total_bytes": total, "ratio": total / comp, "launches_per_batch": 5 + sum(map(_slab_field, fields))}
 
 

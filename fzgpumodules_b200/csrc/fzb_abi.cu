@@ -1049,8 +1049,9 @@ void* fzb_batch_create(const fzb_batch_field* fields, int nfields, const fzb_bat
         b.user_eb = f.eb;
         b.vb_given = f.value_base;
         b.scan = (f.eb_mode != FZB_ABS && !(f.value_base > 0.0f)) ? 1u : 0u;
+        const uint64_t per_sm_parts = (tuning && tuning->scan_parts > 0) ? (uint64_t)tuning->scan_parts : 4u;
         uint64_t want = (f.n_total / 4 + 255) / 256;
-        uint64_t parts = want < (uint64_t)(4 * sms) ? want : (uint64_t)(4 * sms);
+        uint64_t parts = want < per_sm_parts * sms ? want : per_sm_parts * sms;
         if (parts < 1) parts = 1;
         if (parts > (uint64_t)kMaxParts) parts = kMaxParts;
         b.mm_parts = b.scan ? (uint32_t)parts : 1u;
@@ -1058,7 +1059,7 @@ void* fzb_batch_create(const fzb_batch_field* fields, int nfields, const fzb_bat
         const bool rowal = (g.ndim == 1) || (g.nx % 32 == 0);
         b.kind = g.ndim == 1 ? 0u : g.ndim == 2 ? (rowal ? 1u : 2u) : (rowal ? 3u : 4u);
         b.n_chunks = (uint32_t)chunks_of(f.n_total);
-        is_slab[i] = batch_slab_field(g, f.n_total) && !(flags_env() & 1);
+        is_slab[i] = batch_slab_field(g, f.n_total) && !(flags_env() & 1) && !(tuning && tuning->flat_tiles);
         if (!is_slab[i]) {
             const size_t sm = lq_smem_bytes(g, true);
             if (sm > smem) smem = sm;
@@ -1145,31 +1146,47 @@ int fzb_batch_autotune(const fzb_batch_field* fields, int nfields, void* d_work,
     CK(cudaEventCreate(&e1));
     float best_t = 1e30f;
     int rc = FZB_OK;
-    for (int order = 0; order < 2 && rc == FZB_OK; order++)
-        for (int per_sm = 1; per_sm <= 3 && rc == FZB_OK; per_sm++) {
-            fzb_batch_tuning t{per_sm, order};
-            int st = 0;
-            void* p = fzb_batch_create(fields, nfields, &t, d_work, work_bytes, &st);
-            if (!p) {
-                rc = st;
-                break;
-            }
-            float tmin = 1e30f;
-            for (int rep = 0; rep < 3 && rc == FZB_OK; rep++) {  // first run warms up
-                if (cudaEventRecord(e0, s) != cudaSuccess) rc = FZB_E_CUDA;
-                if (rc == FZB_OK) rc = fzb_batch_launch(p, stream);
-                if (rc == FZB_OK && cudaEventRecord(e1, s) != cudaSuccess) rc = FZB_E_CUDA;
-                if (rc == FZB_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = FZB_E_CUDA;
-                float ms = 0;
-                if (rc == FZB_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = FZB_E_CUDA;
-                if (rc == FZB_OK && rep > 0 && ms < tmin) tmin = ms;
-            }
-            fzb_batch_destroy(p);
-            if (rc == FZB_OK && tmin < best_t) {
-                best_t = tmin;
-                *best = t;
-            }
+    auto trial = [&](const fzb_batch_tuning& t) {
+        if (rc != FZB_OK) return;
+        int st = 0;
+        void* p = fzb_batch_create(fields, nfields, &t, d_work, work_bytes, &st);
+        if (!p) {
+            rc = st;
+            return;
         }
+        float tmin = 1e30f;
+        for (int rep = 0; rep < 3 && rc == FZB_OK; rep++) {  // first run warms up
+            if (cudaEventRecord(e0, s) != cudaSuccess) rc = FZB_E_CUDA;
+            if (rc == FZB_OK) rc = fzb_batch_launch(p, stream);
+            if (rc == FZB_OK && cudaEventRecord(e1, s) != cudaSuccess) rc = FZB_E_CUDA;
+            if (rc == FZB_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = FZB_E_CUDA;
+            float ms = 0;
+            if (rc == FZB_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = FZB_E_CUDA;
+            if (rc == FZB_OK && rep > 0 && ms < tmin) tmin = ms;
+        }
+        fzb_batch_destroy(p);
+        if (rc == FZB_OK && tmin < best_t) {
+            best_t = tmin;
+            *best = t;
+        }
+    };
+    // coordinate search: CTAs per SM x order, then the tile shape, then the
+    // scan granularity, each from the best shape so far
+    for (int order = 0; order < 2; order++)
+        for (int per_sm = 1; per_sm <= 3; per_sm++) trial(fzb_batch_tuning{per_sm, order, 0, 4});
+    if (rc == FZB_OK) {
+        fzb_batch_tuning t = *best;
+        t.flat_tiles = 1;
+        trial(t);
+    }
+    if (rc == FZB_OK) {
+        const fzb_batch_tuning b = *best;
+        for (int parts : {1, 2, 8}) {
+            fzb_batch_tuning t = b;
+            t.scan_parts = parts;
+            trial(t);
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (best_ms) *best_ms = best_t;

@@ -515,10 +515,13 @@ class _BatchField(C.Structure):
 
 
 class BatchTuning(C.Structure):
-    _fields_ = [("ctas_per_sm", C.c_int), ("order", C.c_int)]
+    """fzb_batch_tuning: CTAs per SM, dispatch order, flat tiles for
+    slab-shaped fields, value-base scan blocks per SM (0 = default)."""
+    _fields_ = [("ctas_per_sm", C.c_int), ("order", C.c_int), ("flat_tiles", C.c_int), ("scan_parts", C.c_int)]
 
     def __repr__(self):
-        return f"BatchTuning(ctas_per_sm={self.ctas_per_sm}, order={self.order})"
+        return (f"BatchTuning(ctas_per_sm={self.ctas_per_sm}, order={self.order}, flat_tiles={self.flat_tiles}, "
+                f"scan_parts={self.scan_parts})")
 
 
 class Batch:

@@ -416,9 +416,19 @@ typedef struct fzb_batch_field {
     float* d_eb_state;
 } fzb_batch_field;
 
+/* Launch shape of a batch (zero fields take the defaults):
+ * ctas_per_sm  CTAs per SM of the persistent chunk kernel (default 2);
+ * order        1: the chunk kernel dispenses the largest fields first;
+ * flat_tiles   1: slab-shaped 3-D fields go through the chunk kernel's flat
+ *              8192-element chunks instead of the slab kernel's R-row x
+ *              8-plane units (the tile shape);
+ * scan_parts   value-base scan granularity, blocks per SM per field (default
+ *              4; the scan of a field has at most scan_parts x SMs blocks). */
 typedef struct fzb_batch_tuning {
     int ctas_per_sm;
     int order;
+    int flat_tiles;
+    int scan_parts;
 } fzb_batch_tuning;
 
 size_t fzb_batch_workspace_bytes(const fzb_batch_field* fields, int nfields);
@@ -426,6 +436,9 @@ void* fzb_batch_create(const fzb_batch_field* fields, int nfields, const fzb_bat
                        size_t work_bytes, int* status);
 int fzb_batch_launch(void* batch, void* stream);
 void fzb_batch_destroy(void* batch);
+/* Times launch shapes with CUDA events and returns the fastest: every CTAs
+ * per SM (1-3) x dispatch order, then, from the best of those, the other
+ * tile shape and scan granularities 1, 2 and 8. */
 int fzb_batch_autotune(const fzb_batch_field* fields, int nfields, void* d_work, size_t work_bytes, void* stream,
                        fzb_batch_tuning* best, float* best_ms);
 

@@ -36,6 +36,11 @@ def _fields(dev, count=24, seed=1004):
         abs_case = i % 5 == 0  # ABS with a small radius: outliers occur
         out.append(dict(x=x, dims=dims, eb=1e-3 if abs_case else float(rng.choice([1e-2, 1e-3, 1e-4])),
                         mode=K().ABS if abs_case else K().REL, radius=512 if abs_case else 32768, zigzag=True))
+    # two slab-shaped fields (the batch gives them the slab kernels)
+    for j, dims in enumerate([(128, 64, 9), (256, 32, 17)]):
+        x = F.grf(tuple(reversed(dims)), seed=seed + count + j, spike_frac=1e-3, device=dev).reshape(-1).contiguous()
+        out.append(dict(x=x, dims=dims, eb=1e-3, mode=K().ABS if j else K().REL, radius=512 if j else 32768,
+                        zigzag=True))
     return out
 
 
@@ -67,17 +72,20 @@ def test_batch_matches_single_field_calls(cuda):
     b.close()
 
 
-@pytest.mark.parametrize("ctas,order", [(1, 0), (3, 1), (2, 1)])
-def test_batch_tuning_does_not_change_bytes(cuda, ctas, order):
+@pytest.mark.parametrize("ctas,order,flat,parts", [(1, 0, 0, 0), (3, 1, 1, 1), (2, 1, 0, 8), (2, 0, 1, 2)])
+def test_batch_tuning_does_not_change_bytes(cuda, ctas, order, flat, parts):
+    # CTAs per SM, dispatch order, tile shape (slab units or flat chunks for
+    # slab-shaped fields) and scan granularity change the launch, not the bytes
     fields = _fields(cuda, count=12, seed=77)
     ref = [_expected(f) for f in fields]
-    b = K().Batch(fields, K().BatchTuning(ctas, order))
+    b = K().Batch(fields, K().BatchTuning(ctas, order, flat, parts))
     b.launch()
     torch.cuda.synchronize()
     for o, r in zip(b.outputs, ref):
         _same(o, r)
     best, ms = b.autotune()
     assert 1 <= best.ctas_per_sm <= 3 and best.order in (0, 1) and ms > 0
+    assert best.flat_tiles in (0, 1) and best.scan_parts in (1, 2, 4, 8)
     b.launch()
     torch.cuda.synchronize()
     for o, r in zip(b.outputs, ref):
