@@ -14,7 +14,8 @@ device time of the fused C-ABI call); beside it in the same JSON line:
                    arm times the reference's own Pipeline;
   e2e              fz::Pipeline with host buffers: H2D of the field,
                    compress, D2H of the container; H2D of the container,
-                   decompress, D2H of the field;
+                   decompress, D2H of the field; streamed (step k+1's
+                   upload overlaps step k's coding and read-back);
   c3               LorenzoQuant 2-D -> Huffman on 8192^2, with the Huffman
                    decode kernel's roofline;
   batch            64 fields of mixed rank and size as one graph-captured
@@ -382,43 +383,100 @@ def pipeline_timing(pl, x, steps: int, warmup: int, flush, world: int) -> dict:
 
 
 def pipeline_e2e(pl, x, steps: int, warmup: int, world: int) -> dict:
-    """End to end through fz::Pipeline with host buffers: every step copies
-    the field from pinned host memory, compresses, copies the container back;
-    then copies the container to the device, decompresses and copies the
-    field back.  Wall clock, synchronised at the end of each direction."""
+    """End to end through fz::Pipeline with host buffers, streamed as a
+    service would run it: every step uploads its field from pinned host
+    memory, compresses it and reads the container back, and step k+1's upload
+    (a second device buffer, its own stream) overlaps step k's compression
+    and read-back.  Then the reverse: every step uploads a container,
+    decompresses it into one of two device buffers and reads the field back,
+    step k+1's upload and decompression overlapping step k's read-back.  Wall
+    clock over all steps of a direction, the pipeline fill included."""
     import torch
     n = x.numel()
+    dev = x.device
     hx = x.cpu().pin_memory()
     cap = int(pl.compress(x).numel())
     hc = torch.empty(cap + (1 << 20), dtype=torch.uint8).pin_memory()
-    dc = torch.empty(cap + (1 << 20), dtype=torch.uint8, device=x.device)
-    dx = torch.empty_like(x)
     hy = torch.empty_like(hx).pin_memory()
-    s = torch.cuda.current_stream()
-    tc, td, nb = [], [], 0
-    for it in range(warmup + steps):
+    dxs = [torch.empty_like(x) for _ in range(2)]
+    dcs = [torch.empty(cap + (1 << 20), dtype=torch.uint8, device=dev) for _ in range(2)]
+    ys = [torch.empty_like(x) for _ in range(2)]
+    main = torch.cuda.current_stream()
+    up, down = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    nb = 0
+
+    def compress_run(k_steps: int) -> float:
+        nonlocal nb
+        free = [torch.cuda.Event() for _ in range(2)]   # dxs[b] read by its compression
+        ready = [torch.cuda.Event() for _ in range(2)]  # dxs[b] uploaded
+        for e in free:
+            e.record(main)
+
+        def upload(k):
+            b = k & 1
+            up.wait_event(free[b])
+            with torch.cuda.stream(up):
+                dxs[b].copy_(hx, non_blocking=True)
+            ready[b].record(up)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        dx.copy_(hx, non_blocking=True)
-        comp = pl.compress(dx)
-        nb = comp.numel()
-        hc[:nb].copy_(comp, non_blocking=True)
-        s.synchronize()
-        t1 = time.perf_counter()
-        dc[:nb].copy_(hc[:nb], non_blocking=True)
-        y = pl.decompress(dc[:nb])
-        hy.copy_(y[:n], non_blocking=True)
-        s.synchronize()
-        t2 = time.perf_counter()
-        if it >= warmup:
-            tc.append(t1 - t0)
-            td.append(t2 - t1)
+        upload(0)
+        for k in range(k_steps):
+            if k + 1 < k_steps:
+                upload(k + 1)
+            b = k & 1
+            main.wait_event(ready[b])
+            comp = pl.compress(dxs[b])  # the pipeline's one wait: this compression
+            free[b].record(main)
+            nb = comp.numel()
+            hc[:nb].copy_(comp, non_blocking=True)  # the next compression follows it on `main`
+        main.synchronize()
+        return time.perf_counter() - t0
+
+    def decompress_run(k_steps: int) -> float:
+        used = [torch.cuda.Event() for _ in range(2)]   # dcs[b] consumed
+        ready = [torch.cuda.Event() for _ in range(2)]  # dcs[b] uploaded
+        done = [torch.cuda.Event() for _ in range(2)]   # ys[b] written
+        free = [torch.cuda.Event() for _ in range(2)]   # ys[b] read back
+        for e in used + free:
+            e.record(main)
+
+        def upload(k):
+            b = k & 1
+            up.wait_event(used[b])
+            with torch.cuda.stream(up):
+                dcs[b][:nb].copy_(hc[:nb], non_blocking=True)
+            ready[b].record(up)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        upload(0)
+        for k in range(k_steps):
+            if k + 1 < k_steps:
+                upload(k + 1)
+            b = k & 1
+            main.wait_event(ready[b])
+            main.wait_event(free[b])
+            pl.decompressInto(dcs[b][:nb], ys[b])  # the pipeline's one wait: this decompression
+            used[b].record(main)
+            done[b].record(main)
+            down.wait_event(done[b])
+            with torch.cuda.stream(down):
+                hy.copy_(ys[b], non_blocking=True)
+            free[b].record(down)
+        down.synchronize()
+        main.synchronize()
+        return time.perf_counter() - t0
+
+    compress_run(max(warmup, 1))
+    t_c = max_over_ranks(compress_run(steps) / steps, world)
+    decompress_run(max(warmup, 1))
+    t_d = max_over_ranks(decompress_run(steps) / steps, world)
     ok = bool(torch.equal(hy.view(torch.int32), pl.decompress(None)[:n].cpu().view(torch.int32)))
-    t_c = max_over_ranks(sum(tc) / len(tc), world)
-    t_d = max_over_ranks(sum(td) / len(td), world)
     return {"value": world * 4 * n / t_c / 1e9, "unit": "GB/s", "h2d_bytes_per_step": 4 * n + nb,
             "d2h_bytes_per_step": nb + 4 * n, "compress_gbs": world * 4 * n / t_c / 1e9,
-            "decompress_gbs": world * 4 * n / t_d / 1e9, "api": "fz::Pipeline compress / decompress",
+            "decompress_gbs": world * 4 * n / t_d / 1e9, "api": "fz::Pipeline compress / decompressInto",
+            "streamed": "step k+1's upload overlaps step k's coding and read-back (two device buffers, "
+                        "upload / read-back streams); wall clock over all steps, pipeline fill included",
             "values_equal_device_decompress": ok}
 
 
