@@ -31,43 +31,53 @@ struct Node {
     uint32_t sym = 0;
 };
 
+// The heap keeps each node's frequency beside its id, so a comparison reads
+// one slot instead of following the id into the node array; the order of
+// comparisons, and so every tie, is unchanged.
 class MinHeap {
 public:
-    explicit MinHeap(const std::vector<Node>& nodes) : nodes_(nodes) { slots_.push_back(-1); }
+    MinHeap() { slots_.push_back({0, -1}); }
+    void reserve(size_t n) { slots_.reserve(n + 1); }
     size_t size() const { return slots_.size() - 1; }
-    void push(int id) {
-        slots_.push_back(id);
+    void push(int id, uint64_t freq) {
+        slots_.push_back({freq, id});
         size_t i = slots_.size() - 1;
         while (i > 1) {
             const size_t parent = i >> 1;
-            if (nodes_[slots_[parent]].freq <= nodes_[id].freq) break;
+            if (slots_[parent].freq <= freq) break;
             slots_[i] = slots_[parent];
             i = parent;
         }
-        slots_[i] = id;
+        slots_[i] = {freq, id};
     }
     int pop() {
-        const int top = slots_[1];
-        slots_[1] = slots_.back();
+        const int top = slots_[1].id;
+        const Slot moved = slots_.back();
         slots_.pop_back();
         const size_t end = slots_.size();
+        if (end <= 1) return top;
         size_t i = 1;
+        Slot* h = slots_.data();
         while (2 * i < end) {
             size_t c = 2 * i;
-            if (c + 1 < end && nodes_[slots_[c + 1]].freq < nodes_[slots_[c]].freq) c++;
-            if (nodes_[slots_[i]].freq > nodes_[slots_[c]].freq) {
-                std::swap(slots_[i], slots_[c]);
-                i = c;
-            } else {
-                break;
-            }
+            // the right child only when strictly smaller (a select, not a branch)
+            const uint64_t fl = h[c].freq;
+            const uint64_t fr = c + 1 < end ? h[c + 1].freq : fl;
+            c += fr < fl ? 1 : 0;
+            if (!(moved.freq > h[c].freq)) break;
+            h[i] = h[c];
+            i = c;
         }
+        h[i] = moved;
         return top;
     }
 
 private:
-    const std::vector<Node>& nodes_;
-    std::vector<int> slots_;
+    struct Slot {
+        uint64_t freq;
+        int id;
+    };
+    std::vector<Slot> slots_;
 };
 
 }  // namespace
@@ -85,8 +95,9 @@ int build_huffman_book(const uint32_t* freq, uint32_t bklen, uint32_t* bk4, uint
             nd.sym = s;
             nodes.push_back(nd);
         }
-    MinHeap heap(nodes);
-    for (int i = 0; i < (int)nodes.size(); i++) heap.push(i);
+    MinHeap heap;
+    heap.reserve(nodes.size());
+    for (int i = 0; i < (int)nodes.size(); i++) heap.push(i, nodes[i].freq);
     while (heap.size() > 1) {
         const int right = heap.pop();
         const int left = heap.pop();
@@ -95,7 +106,7 @@ int build_huffman_book(const uint32_t* freq, uint32_t bklen, uint32_t* bk4, uint
         nd.right = right;
         nd.freq = nodes[left].freq + nodes[right].freq;
         nodes.push_back(nd);
-        heap.push((int)nodes.size() - 1);
+        heap.push((int)nodes.size() - 1, nd.freq);
     }
 
     std::vector<uint64_t> bk8(bklen, ~0ull);

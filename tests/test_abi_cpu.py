@@ -86,6 +86,12 @@ def test_huffman_host_codebook_matches_oracle_and_reference():
     f = np.zeros(1024, np.uint32)
     f[7] = 100  # a single symbol
     cases.append((f, 1024))
+    # ties everywhere: which equal-frequency node the heap pops decides the tree
+    cases.append((np.full(1024, 5, np.uint32), 1024))
+    cases.append((rng.integers(1, 4, 1024).astype(np.uint32), 1024))
+    f = (np.exp(-0.012 * np.arange(1024)) * 1e5).astype(np.uint32)
+    f[:4] *= 200  # C3-like: a few dominant symbols over a long geometric tail
+    cases.append((f, 1024))
     for f, bk in cases:
         a = K.huff_book(f, bk)
         b = O.huff_book(f, bk)
