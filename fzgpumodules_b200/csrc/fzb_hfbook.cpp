@@ -3,8 +3,8 @@
 // hf_bk_impl1.cc:73-163, hf_bk_internal.cc:59-101, hf_canon.cc:86-131).
 //
 // The reference builds this table on the host from the device histogram;
-// so does this library (a few hundred symbols, microseconds of CPU).  The
-// steps that fix the output bits:
+// so does this library (tens of microseconds for a thousand symbols: the
+// heap's dependent loads set the pace).  The steps that fix the output bits:
 //   * a 1-indexed binary min-heap: insertion stops at a parent whose
 //     frequency is <= the new node's; removal moves the last node to the
 //     root and sinks it, taking the right child only when strictly smaller
