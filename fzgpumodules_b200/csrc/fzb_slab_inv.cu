@@ -49,12 +49,16 @@ __constant__ uint32_t kExpandInit[16] = {
 __device__ __forceinline__ void cp_async4(uint32_t* dst, const uint32_t* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async16s(uint32_t* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Stages chunk c's payload words (from the 4-byte boundary at or below its
-// first byte) into Cw.  Returns the header word in e, the first byte's offset
-// in the first word in lead, and ok = the payload lies inside the stream.
+// Stages chunk c's payload (from the 16-byte boundary at or below its first
+// byte when the stream is 16-byte aligned, else the 4-byte one) into Cw.
+// Returns the header word in e, the first byte's offset from that boundary in
+// lead, and ok = the payload lies inside the stream.
 __device__ __forceinline__ void stage_chunk(const InvArgs& a, uint32_t c, uint32_t* Cw, uint32_t& e,
                                             uint32_t& lead, bool& ok) {
     e = reinterpret_cast<const uint32_t*>(a.rze + 8)[c];
@@ -62,10 +66,33 @@ __device__ __forceinline__ void stage_chunk(const InvArgs& a, uint32_t c, uint32
     const uint32_t comp = e & 0x7fffffffu;
     ok = off + comp <= a.rze_bytes;
     const uint8_t* src = a.rze + (ok ? off : 0);
-    lead = (uint32_t)(reinterpret_cast<uintptr_t>(src) & 3u);
     const uint32_t ncopy = ok ? min(comp, (uint32_t)kChunkBytes) : 0u;
-    const uint32_t nw = (lead + ncopy + 3) >> 2;
     const uint8_t* end = a.rze + a.rze_bytes;
+    if ((reinterpret_cast<uintptr_t>(a.rze) & 15u) == 0) {
+        // a 16-byte aligned stream: 16-byte copies from the 16-byte boundary
+        // at or below the first byte (never below the stream's start)
+        lead = (uint32_t)(reinterpret_cast<uintptr_t>(src) & 15u);
+        const uint32_t ng = (lead + ncopy + 15) >> 4;
+        const uint8_t* g0 = src - lead;
+        for (uint32_t i = threadIdx.x; i < ng; i += kThreads) {
+            const uint8_t* p = g0 + 16u * i;
+            if (p + 16 <= end) {
+                cp_async16s(Cw + 4u * i, p);
+            } else {  // the stream's last bytes: only those inside it
+#pragma unroll
+                for (int w = 0; w < 4; w++) {
+                    uint32_t v = 0;
+                    for (int b = 0; b < 4; b++)
+                        if (p + 4 * w + b < end) v |= (uint32_t)p[4 * w + b] << (8 * b);
+                    Cw[4u * i + w] = v;
+                }
+            }
+        }
+        cp_async_commit();
+        return;
+    }
+    lead = (uint32_t)(reinterpret_cast<uintptr_t>(src) & 3u);
+    const uint32_t nw = (lead + ncopy + 3) >> 2;
     const uint32_t* gw = reinterpret_cast<const uint32_t*>(src - lead);
     for (uint32_t i = threadIdx.x; i < nw; i += kThreads) {
         const uint8_t* p = reinterpret_cast<const uint8_t*>(gw + i);
