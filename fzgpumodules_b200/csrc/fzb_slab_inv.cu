@@ -4,8 +4,9 @@
 // units plane by plane, mirroring the slab compressor (fzb_slab.cu).
 //
 // Per chunk (= one slab plane):
-//   * the chunk's payload is staged into shared memory with 4-byte cp.async
-//     one plane ahead (double buffer);
+//   * the chunk's payload is staged into shared memory with 16-byte cp.async
+//     copies (4-byte ones for a stream that is not 16-byte aligned) one plane
+//     ahead (double buffer);
 //   * warp 0 rebuilds RZE levels 4 -> 2 (bm3, bm2 and the per-byte prefix
 //     counts of bm2), all threads rebuild bm1 (rze_stage.cu:871-994);
 //   * thread t owns chunk elements 32t..32t+31: its 16 plane nibbles come
