@@ -393,29 +393,53 @@ __global__ void __launch_bounds__(kThreads, kInvCtasPerSm) lq3d_inv_slab_kernel(
             }
             transpose16x2(x);
 
-            // codes -> deltas (u - 32768 through 1.5*2^23 + u), outliers, x prefix
-            float d[32];
-            {
-                const float2 nb2 = f2(-(kMagic + 32768.0f), -(kMagic + 32768.0f));
+            // codes -> deltas (u - 32768 through 1.5*2^23 + u), outliers, x prefix.
+            // Words x[8h..8h+7] hold elements 8h..8h+7 (low halves) and
+            // 16+8h..23+8h (high halves): one x-prefix group each, so only
+            // sixteen deltas are live at a time.
+            const float2 nb2 = f2(-(kMagic + 32768.0f), -(kMagic + 32768.0f));
+            auto deltas = [&](int h, float (&lo)[8], float (&hi)[8]) {
 #pragma unroll
-                for (int kk = 0; kk < 16; kk += 2) {
-                    const uint32_t p0 = biased_pair<ZZ>(x[kk]), p1 = biased_pair<ZZ>(x[kk + 1]);
-                    const float2 lo = __fadd2_rn(f2(__uint_as_float(__byte_perm(p0, 0x4b400000u, 0x7610)),
-                                                    __uint_as_float(__byte_perm(p1, 0x4b400000u, 0x7610))), nb2);
-                    const float2 hi = __fadd2_rn(f2(__uint_as_float(__byte_perm(p0, 0x4b400000u, 0x7632)),
-                                                    __uint_as_float(__byte_perm(p1, 0x4b400000u, 0x7632))), nb2);
-                    d[kk] = lo.x;
-                    d[kk + 1] = lo.y;
-                    d[16 + kk] = hi.x;
-                    d[17 + kk] = hi.y;
+                for (int kk = 0; kk < 8; kk += 2) {
+                    const uint32_t p0 = biased_pair<ZZ>(x[8 * h + kk]), p1 = biased_pair<ZZ>(x[8 * h + kk + 1]);
+                    const float2 l = __fadd2_rn(f2(__uint_as_float(__byte_perm(p0, 0x4b400000u, 0x7610)),
+                                                   __uint_as_float(__byte_perm(p1, 0x4b400000u, 0x7610))), nb2);
+                    const float2 u = __fadd2_rn(f2(__uint_as_float(__byte_perm(p0, 0x4b400000u, 0x7632)),
+                                                   __uint_as_float(__byte_perm(p1, 0x4b400000u, 0x7632))), nb2);
+                    lo[kk] = l.x;
+                    lo[kk + 1] = l.y;
+                    hi[kk] = u.x;
+                    hi[kk + 1] = u.y;
                 }
-            }
-            const bool checked = o1 > o0;  // uniform: the chunk carries outliers
-            if (checked) {  // add them through the thread's own row of X
+            };
+            // group i (elements 8i..8i+7) <-> granules 2i, 2i+1 of the thread's row of X
+            auto put = [&](int i, const float (&v)[8]) {
+                *reinterpret_cast<float4*>(X + swz_off(t, 2 * i)) = make_float4(v[0], v[1], v[2], v[3]);
+                *reinterpret_cast<float4*>(X + swz_off(t, 2 * i + 1)) = make_float4(v[4], v[5], v[6], v[7]);
+            };
+            auto scan8 = [](float (&v)[8]) {
 #pragma unroll
-                for (int g = 0; g < 8; g++)
-                    *reinterpret_cast<float4*>(X + swz_off(t, g)) =
-                        make_float4(d[4 * g], d[4 * g + 1], d[4 * g + 2], d[4 * g + 3]);
+                for (int jj = 1; jj < 8; jj++) v[jj] = __fadd_rn(v[jj], v[jj - 1]);
+            };
+            const bool checked = o1 > o0;  // uniform: the chunk carries outliers
+            if (!checked) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    float lo[8], hi[8];
+                    deltas(h, lo, hi);
+                    scan8(lo);
+                    scan8(hi);
+                    put(h, lo);
+                    put(2 + h, hi);
+                }
+            } else {  // add the outliers through the thread's own row of X
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    float lo[8], hi[8];
+                    deltas(h, lo, hi);
+                    put(h, lo);
+                    put(2 + h, hi);
+                }
                 const uint32_t om = s_om[t];
                 if (om) {
                     s_om[t] = 0;
@@ -428,28 +452,19 @@ __global__ void __launch_bounds__(kThreads, kInvCtasPerSm) lq3d_inv_slab_kernel(
                         if (!(fabsf(v) < kExact)) inexact = true;
                     }
                 }
-#pragma unroll
-                for (int g = 0; g < 8; g++) {
-                    const float4 v = *reinterpret_cast<const float4*>(X + swz_off(t, g));
-                    d[4 * g] = v.x;
-                    d[4 * g + 1] = v.y;
-                    d[4 * g + 2] = v.z;
-                    d[4 * g + 3] = v.w;
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int jj = 1; jj < 8; jj++) d[8 * i + jj] = __fadd_rn(d[8 * i + jj], d[8 * i + jj - 1]);
-            if (checked) {
                 float mx = 0.0f;
 #pragma unroll
-                for (int kk = 0; kk < 32; kk++) mx = max_nan(mx, fabsf(d[kk]));
+                for (int i = 0; i < 4; i++) {
+                    const float4 v0 = *reinterpret_cast<const float4*>(X + swz_off(t, 2 * i));
+                    const float4 v1 = *reinterpret_cast<const float4*>(X + swz_off(t, 2 * i + 1));
+                    float v[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+                    scan8(v);
+#pragma unroll
+                    for (int jj = 0; jj < 8; jj++) mx = max_nan(mx, fabsf(v[jj]));
+                    put(i, v);
+                }
                 if (!(mx < kExact)) inexact = true;
             }
-#pragma unroll
-            for (int g = 0; g < 8; g++)
-                *reinterpret_cast<float4*>(X + swz_off(t, g)) = make_float4(d[4 * g], d[4 * g + 1], d[4 * g + 2], d[4 * g + 3]);
             // this plane's output pass runs after the next B0
             pend = true;
             pz = z;
